@@ -1,0 +1,115 @@
+/*
+ * tetfit.h -- C ABI of the B200-native TetFIT leapfrog time-stepping path.
+ *
+ * The entry points replace the two calls a TetFIT driver makes
+ * (src/DGA/main/dga_main.cpp:52-62):
+ *   Discretization(std::string inputfile)            Discretization.hpp:45-211
+ *   RunSimulation(const Simulation&, const uint32_t&) Discretization.hpp:289-2303
+ * and expose the hot loop stepwise so that a caller can drive it, sample it and
+ * read the state back.  All buffers passed in are host memory owned by the
+ * caller; device memory is owned by the context.  Every function returns 0 on
+ * success or a negative TF_E* code; tf_last_error() gives the message (for
+ * script errors the reference's own text, "Input file error at line N: ...",
+ * Utilities.hpp:371-375).  One context per host thread; a context is not
+ * re-entrant.  Nothing throws across this boundary.
+ */
+#ifndef TETFIT_H
+#define TETFIT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define TF_API __attribute__((visibility("default")))
+#else
+#define TF_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct tf_ctx tf_ctx;
+
+enum {
+  TF_OK = 0,
+  TF_E_SCRIPT = -1,      /* script / mesh / solids file error (MyThrow text)        */
+  TF_E_ARG = -2,         /* bad argument, unknown simulation label, buffer too small */
+  TF_E_CUDA = -3,        /* CUDA runtime error or no usable sm_100 device           */
+  TF_E_UNSUPPORTED = -4, /* feature outside the time-stepping path (e.g. PML, silo)  */
+  TF_E_STATE = -5,       /* call out of order (e.g. tf_step before tf_prepare)       */
+  TF_E_SOLVER = -6       /* iterative solve hit its iteration limit                 */
+};
+
+enum { TF_FP64 = 0, TF_FP32 = 1 };
+
+typedef struct tf_opts {
+  int32_t precision;    /* TF_FP64 (default) or TF_FP32 field state                     */
+  int32_t device;       /* CUDA device ordinal                                          */
+  int32_t write_files;  /* tf_run: write <name><label>_probe_E/H.dat and poynting.dat   */
+  int32_t verbose;      /* print the reference's parameter banner and stats            */
+  int32_t graph_steps;  /* steps per captured CUDA graph (0: automatic)                */
+  int32_t reserved[11];
+} tf_opts;
+
+typedef struct tf_info {
+  uint64_t n_edges, n_faces, n_cells;  /* dofs: edges (U) and faces (B)           */
+  uint64_t n_probes, n_steps;          /* probes inside the mesh; loop length     */
+  uint64_t step_index;                 /* steps already taken                     */
+  uint32_t nx, ny, nz;                 /* Cartesian cells per axis (0 for tets)   */
+  int32_t method;                      /* 0 fdtd, 1 dga, 2 gfdtd                  */
+  double dt, dt_estimate;              /* step used; courant x stability estimate */
+  int32_t possibly_unstable;           /* SET step exceeded the estimate          */
+  int32_t precision;
+  uint64_t device_bytes;               /* device memory held by the context       */
+  uint32_t kernels_per_step;           /* kernel launches one leapfrog step makes */
+  uint32_t n_sources;                  /* sources of the simulation (label order) */
+  uint64_t reserved[7];
+} tf_info;
+
+/* Parse a .fdtd script (Discretization(std::string), Discretization.hpp:45-211). */
+TF_API int tf_open(const char* fdtd_path, tf_ctx** out);
+/* Simulation labels in ascending order (the order dga_main.cpp:52-62 runs them). */
+TF_API int tf_simulations(tf_ctx* ctx, uint32_t* labels, uint32_t cap, uint32_t* n);
+/* Build mesh, operators and device state for one simulation
+ * (RunSimulation up to the time loop, Discretization.hpp:289-428, 4347-5690). */
+TF_API int tf_prepare(tf_ctx* ctx, uint32_t sim_label, const tf_opts* opts);
+TF_API int tf_get_info(tf_ctx* ctx, tf_info* info);
+/* Advance up to nsteps leapfrog steps (Discretization.hpp:1840-1933). */
+TF_API int tf_step(tf_ctx* ctx, uint64_t nsteps, uint64_t* done);
+/* Probe series so far: times[n], values[n][n_probes][6] = Ex Ey Ez Hx Hy Hz
+ * (ExportFitFields, Discretization.hpp:3096-3158).  *n_samples is always set. */
+TF_API int tf_get_probes(tf_ctx* ctx, double* times, double* values, size_t cap_samples, size_t* n_samples);
+/* Probe coordinates [n_probes][3] and containing cell index (reference numbering). */
+TF_API int tf_get_probe_points(tf_ctx* ctx, double* xyz, uint64_t* cells, size_t cap);
+/* Field state in the reference's numbering: U[n_edges], B[n_faces], F[n_faces]
+ * (any pointer may be NULL).  Values are converted to double. */
+TF_API int tf_get_state(tf_ctx* ctx, double* U, size_t nU, double* B, size_t nB, double* F, size_t nF);
+/* Overwrite U and F (reference numbering); B is derived as F / M_nu on the H grid. */
+TF_API int tf_set_state(tf_ctx* ctx, const double* U, size_t nU, const double* F, size_t nF);
+/* Per-step boundary flux 0.5 (U_old + U) . curl_fb (Discretization.hpp:1901). */
+TF_API int tf_get_flux(tf_ctx* ctx, double* flux, size_t cap, size_t* n);
+/* Discrete leapfrog energy 0.5 U.Me U + 0.5 B_prev.Mnu B (FP64 accumulation). */
+TF_API int tf_energy(tf_ctx* ctx, double* energy);
+/* One step driven from host memory: carrier_in[n_sources] replaces the script
+ * waveform's value for this step (NULL keeps it); probe_out[n_probes*6]
+ * receives the sample this step exports, if it exports one (NULL skips). */
+TF_API int tf_step_io(tf_ctx* ctx, const double* carrier_in, double* probe_out, uint64_t* done);
+/* Runs up to nsteps steps with CUDA events between kernels and returns the
+ * device milliseconds spent per phase: ms[0] sources/BC edges, ms[1] E update,
+ * ms[2] source scatter + boundary flux, ms[3] probe export, ms[4] H update
+ * (the reference's per-phase averages, Discretization.hpp:2286-2302). */
+TF_API int tf_phase_times(tf_ctx* ctx, uint64_t nsteps, double* ms5, uint64_t* done);
+/* Whole simulation as RunSimulation does it: prepare, every step, output files. */
+TF_API int tf_run(tf_ctx* ctx, uint32_t sim_label, const tf_opts* opts);
+/* Device time of the last tf_step call, from CUDA events on the context stream. */
+TF_API int tf_last_step_ms(tf_ctx* ctx, double* ms);
+TF_API const char* tf_last_error(tf_ctx* ctx);
+TF_API void tf_close(tf_ctx* ctx);
+/* Fills *opts with defaults (FP64, device 0, no files, quiet, automatic graphs). */
+TF_API void tf_default_opts(tf_opts* opts);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TETFIT_H */

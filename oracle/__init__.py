@@ -1,0 +1,116 @@
+"""CPU oracle — TEST INFRASTRUCTURE ONLY.
+
+An FP64 C++ restatement of TetFIT's time-stepping path (see the headers of
+oracle/*.cpp for the reference lines each part follows), loaded with ctypes.
+Only tests/, bench.py's cpu_baseline / reference leg and
+__graft_entry__.smoke() may use it, and only as the checker or the timed CPU
+baseline; the product (tetfit_b200/) never imports it.
+
+Parity is pinned against fixtures generated by this restatement and against
+size-independent properties (energy conservation, analytic waveguide); the
+reference ships no tests or golden vectors and cannot be compiled here, so
+parity against the reference binary itself is unpinned.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .build import LIB, LIB_OMP, build
+
+_libs = {}
+
+
+def lib(omp: bool = False):
+    path = LIB_OMP if omp else LIB
+    if path not in _libs:
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        P = ctypes.c_void_p
+        L.orc_fit_open.restype = P
+        L.orc_fit_open.argtypes = [ctypes.c_char_p, ctypes.c_uint, ctypes.c_char_p, ctypes.c_int]
+        L.orc_fit_close.argtypes = [P]
+        L.orc_fit_info.argtypes = [P, P, P]
+        L.orc_fit_step.restype = ctypes.c_longlong
+        L.orc_fit_step.argtypes = [P, ctypes.c_longlong]
+        L.orc_fit_nsamples.restype = ctypes.c_longlong
+        L.orc_fit_nsamples.argtypes = [P]
+        L.orc_fit_probes.argtypes = [P, P, P, P, P]
+        L.orc_fit_state.argtypes = [P, P, P, P]
+        L.orc_fit_flux.argtypes = [P, P]
+        L.orc_fit_topology.argtypes = [P, P, P, P, P]
+        _libs[path] = L
+    return _libs[path]
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class FitOracle:
+    """FP64 CPU restatement of one Cartesian FIT simulation."""
+
+    def __init__(self, script: str, label: int = 1, omp: bool = False):
+        self.L = lib(omp)
+        err = ctypes.create_string_buffer(1024)
+        self.h = self.L.orc_fit_open(os.fsencode(script), label, err, 1024)
+        if not self.h:
+            raise RuntimeError(err.value.decode())
+        iv = np.zeros(16, dtype=np.int64)
+        dv = np.zeros(16)
+        self.L.orc_fit_info(self.h, _p(iv), _p(dv))
+        self.nE, self.nF, self.nV, self.n_probes, self.n_steps = (int(x) for x in iv[:5])
+        self.N = tuple(int(x) for x in iv[5:8])
+        self.possibly_unstable = bool(iv[8])
+        self.dt, self.dt_estimate = float(dv[0]), float(dv[1])
+        self.steps_done = 0
+
+    def step(self, n: int) -> int:
+        d = int(self.L.orc_fit_step(self.h, n))
+        self.steps_done += d
+        return d
+
+    def run(self) -> int:
+        return self.step(self.n_steps)
+
+    def probes(self):
+        ns = int(self.L.orc_fit_nsamples(self.h))
+        t = np.zeros(ns)
+        v = np.zeros((ns, self.n_probes, 6))
+        pts = np.zeros((self.n_probes, 3))
+        el = np.zeros(self.n_probes, dtype=np.int64)
+        self.L.orc_fit_probes(self.h, _p(t), _p(v), _p(pts), _p(el))
+        return t, v, pts, el
+
+    def state(self):
+        U, F, B = np.zeros(self.nE), np.zeros(self.nF), np.zeros(self.nF)
+        self.L.orc_fit_state(self.h, _p(U), _p(F), _p(B))
+        return U, B, F
+
+    def flux(self):
+        f = np.zeros(self.steps_done)
+        self.L.orc_fit_flux(self.h, _p(f))
+        return f
+
+    def topology(self):
+        en = np.zeros((self.nE, 2), dtype=np.uint32)
+        npts = self.nV * 8
+        xyz = np.zeros((npts, 3))
+        fe = np.zeros((self.nF, 4), dtype=np.uint32)
+        cl = np.zeros(self.nE, dtype=np.uint32)
+        n = self.L.orc_fit_topology(self.h, _p(en), _p(xyz), _p(fe), _p(cl))
+        return en, xyz[:n], fe, cl
+
+    def close(self):
+        if self.h:
+            self.L.orc_fit_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

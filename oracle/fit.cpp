@@ -1,0 +1,589 @@
+// ORACLE — test infrastructure only.
+// FP64 CPU restatement of TetFIT's Cartesian FIT ("method fdtd") path:
+//   ReadStructuredMesh   src/DGA/Discretization.hpp:4347-5690
+//   probe location       Discretization.hpp:397-428, FindFitProbe :3590-3643
+//   dipole (j) edges     Discretization.hpp:466-502
+//   leapfrog loop        Discretization.hpp:1791-1943
+//   sources/BC           Discretization.hpp:3899-4202, Source.hpp:313-567
+//   probe sampling       GetFitElectricField/GetFitMagneticField :3555-3588,
+//                        ExportFitFields :3096-3158
+// Element, face, edge and node numbering follow the reference's cube sweep
+// (k, then j, then i) with the per-cube sharing rules of :4615-4934, so state
+// vectors come out in the reference's own order.
+//
+// Documented divergences (each an undefined-behaviour corner of the reference):
+//  * an interface face between materials a != b gets the label matad(a,b)
+//    (:5102-5104) which the reference truncates to 8 bits and uses to index the
+//    100-slot BndToBC table (:5401-5405); here the full label is kept and a
+//    label >= 100 carries no boundary condition;
+//  * an edge on a boundary face that is neither PEC nor a source surface has
+//    3 faces but is sent to the 4-face common stencil (:1869-1876, out-of-range
+//    read); here it is updated with its explicit signed faces and no source
+//    term (a natural boundary);
+//  * PML boundary conditions (:4411-4555, "under development" in README.md:144)
+//    are rejected.
+#include "fit.hpp"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <stdexcept>
+
+#include "lanczos.hpp"
+
+namespace orc {
+
+// Local cube topology of the reference (Discretization.hpp:4615-5280).
+// Nodes: bit0 = +x, bit1 = +y, bit2 = +z.
+static const int kEdgeNodes[12][2] = {{0, 1}, {0, 2}, {0, 4}, {1, 3}, {1, 5}, {2, 3},
+                                      {2, 6}, {3, 7}, {4, 5}, {4, 6}, {5, 7}, {6, 7}};
+static const int kEdgeAxis[12] = {0, 1, 2, 1, 2, 0, 2, 2, 0, 1, 1, 0};
+static const int kDualCurl[3] = {1, -1, 1};  // by edge axis (:4953-5067)
+// Faces: 0 z-, 1 y-, 2 x-, 3 x+, 4 y+, 5 z+.
+static const int kFaceEdges[6][4] = {{0, 1, 3, 5}, {0, 2, 4, 8}, {1, 2, 6, 9},
+                                     {3, 4, 7, 10}, {5, 6, 7, 11}, {8, 9, 10, 11}};
+static const int kFaceCurl[6] = {1, -1, 1, 1, -1, 1};
+static const int kFaceLabel[6] = {1, 5, 2, 4, 3, 6};   // first-touch labels (:5084-5232)
+static const int kFaceNormal[6] = {2, 1, 0, 0, 1, 2};
+// Sharing with the previously swept neighbours (bottom = k-1, left = j-1,
+// back = i-1): {my position, neighbour position}.
+static const int kShareEdgeBottom[4][2] = {{0, 8}, {1, 9}, {3, 10}, {5, 11}};
+static const int kShareEdgeLeft[4][2] = {{0, 5}, {2, 6}, {4, 7}, {8, 11}};
+static const int kShareEdgeBack[4][2] = {{1, 3}, {2, 4}, {6, 7}, {9, 10}};
+static const int kShareNodeBottom[4][2] = {{0, 4}, {1, 5}, {2, 6}, {3, 7}};
+static const int kShareNodeLeft[4][2] = {{0, 2}, {1, 3}, {4, 6}, {5, 7}};
+static const int kShareNodeBack[4][2] = {{0, 1}, {2, 3}, {4, 5}, {6, 7}};
+
+static const uint32_t NONE = 0xffffffffu;
+
+void FitOracle::build_mesh() {
+  // Discretization.hpp:4347-4583
+  const Mesh& msh = sc.meshes[sim.mesh];
+  for (auto& b : sc.bcs)
+    if (b.second.type == "pml") throw std::runtime_error("PML boundary conditions are not supported");
+  solids = read_solids(msh.file);
+  double scale = msh.scale;
+  xmin = scale * msh.xmin; ymin = scale * msh.ymin; zmin = scale * msh.zmin;
+  xmax = scale * msh.xmax; ymax = scale * msh.ymax; zmax = scale * msh.zmax;
+  Lx = scale * msh.xstep; Ly = scale * msh.ystep; Lz = scale * msh.zstep;
+  Nx = (uint32_t)(std::fabs(xmax - xmin) / Lx);
+  Ny = (uint32_t)(std::fabs(ymax - ymin) / Ly);
+  Nz = (uint32_t)(std::fabs(zmax - zmin) / Lz);
+
+  // material-pair labels (Discretization.hpp:330-347)
+  if (sc.materials.empty()) throw std::runtime_error("no material defined");
+  uint32_t maxmat = sc.materials.rbegin()->first;
+  matad.assign((size_t)(maxmat + 1) * (maxmat + 1), 0);
+  uint64_t ml = 6;
+  for (uint32_t i = 0; i <= maxmat; i++)
+    for (uint32_t j = i + 1; j <= maxmat; j++) {
+      ++ml;
+      matad[(size_t)i * (maxmat + 1) + j] = matad[(size_t)j * (maxmat + 1) + i] = ml;
+    }
+  auto mat_adj = [&](uint32_t a, uint32_t b) -> uint64_t {
+    if (a > maxmat || b > maxmat) throw std::runtime_error("solid material label without a material definition");
+    return matad[(size_t)a * (maxmat + 1) + b];
+  };
+
+  const size_t ncell = (size_t)Nx * Ny * Nz;
+  const double area_z = Lx * Ly, area_x = Ly * Lz, area_y = Lx * Lz;
+  const double da[3] = {area_x / 4, area_y / 4, area_z / 4};
+  const double L[3] = {Lx, Ly, Lz};
+  D.reserve(ncell); Ecl.reserve(ncell); Pcl.reserve(ncell); vol_material.reserve(ncell);
+  std::vector<double> avg_eps, avg_sigma, avg_ni, avg_msig, edge_len, face_area;
+  std::vector<uint8_t> ele_lossy, mag_lossy;
+  uint32_t nv = 0, nf = 0, ne = 0, np = 0;
+  double pz = zmin;
+  for (uint32_t k = 0; k < Nz; ++k) {
+    double py = ymin;
+    for (uint32_t j = 0; j < Ny; ++j) {
+      double px = xmin;
+      for (uint32_t i = 0; i < Nx; ++i) {
+        uint32_t m = which_solid(px + 0.5 * Lx, py + 0.5 * Ly, pz + 0.5 * Lz);
+        vol_material.push_back(m);
+        const Material& mat = sc.materials[m];  // map insertion of a default material, as the reference
+        std::array<uint32_t, 6> d;
+        std::array<uint32_t, 12> e;
+        std::array<uint32_t, 8> p;
+        d.fill(NONE); e.fill(NONE); p.fill(NONE);
+        // neighbour existence by coordinate comparison (:4619-4633)
+        uint32_t bottom = pz > zmin ? nv - Nx * Ny : NONE;
+        uint32_t left = py > ymin ? nv - Nx : NONE;
+        uint32_t back = px > xmin ? nv - 1 : NONE;
+        // shared entities; the reference's case table takes, per slot, the
+        // same global entity from whichever neighbour it names
+        if (bottom != NONE) {
+          d[0] = D[bottom][5];
+          for (auto& s : kShareEdgeBottom) e[s[0]] = Ecl[bottom][s[1]];
+          for (auto& s : kShareNodeBottom) p[s[0]] = Pcl[bottom][s[1]];
+        }
+        if (left != NONE) {
+          d[1] = D[left][4];
+          for (auto& s : kShareEdgeLeft) e[s[0]] = Ecl[left][s[1]];
+          for (auto& s : kShareNodeLeft) p[s[0]] = Pcl[left][s[1]];
+        }
+        if (back != NONE) {
+          d[2] = D[back][3];
+          for (auto& s : kShareEdgeBack) e[s[0]] = Ecl[back][s[1]];
+          for (auto& s : kShareNodeBack) p[s[0]] = Pcl[back][s[1]];
+        }
+        // new entities numbered in slot order
+        for (int q = 0; q < 6; q++)
+          if (d[q] == NONE) {
+            d[q] = nf++;
+            Dt.emplace_back();
+            C.push_back({NONE, NONE, NONE, NONE});
+            curl.push_back(1);
+            boundary_face.push_back(0);
+            tbc_flag.push_back(0);
+            avg_ni.push_back(0); avg_msig.push_back(0); mag_lossy.push_back(0); face_area.push_back(0);
+          }
+        for (int q = 0; q < 12; q++)
+          if (e[q] == NONE) {
+            e[q] = ne++;
+            Ct.emplace_back();
+            G.push_back({NONE, NONE});
+            dual_curl.push_back(0);
+            avg_eps.push_back(0); avg_sigma.push_back(0); ele_lossy.push_back(0); edge_len.push_back(0);
+          }
+        for (int q = 0; q < 8; q++)
+          if (p[q] == NONE) {
+            p[q] = np++;
+            pts.push_back({px + ((q & 1) ? Lx : 0), py + ((q & 2) ? Ly : 0), pz + ((q & 4) ? Lz : 0)});
+          }
+        D.push_back(d); Ecl.push_back(e); Pcl.push_back(p);
+        // incidence volume->face (:4938-4943)
+        for (int q = 0; q < 6; q++) Dt[d[q]].push_back({nv, q < 3 ? -1 : 1});
+        // first visit of an edge fixes its nodes, length and dual-curl sign (:4945-5068)
+        for (int q = 0; q < 12; q++)
+          if (G[e[q]][0] == NONE) {
+            G[e[q]] = {p[kEdgeNodes[q][0]], p[kEdgeNodes[q][1]]};
+            edge_len[e[q]] = L[kEdgeAxis[q]];
+            dual_curl[e[q]] = kDualCurl[kEdgeAxis[q]];
+          }
+        // faces: first visit fills C and Ct, second visit relabels (:5070-5232)
+        for (int q = 0; q < 6; q++) {
+          uint32_t f = d[q];
+          if (C[f][0] == NONE) {
+            for (int r = 0; r < 4; r++) {
+              C[f][r] = e[kFaceEdges[q][r]];
+              int sg = kFaceCurl[q] * ((r % 2) ? -1 : 1);
+              Ct[e[kFaceEdges[q][r]]].push_back({f, (int8_t)sg});
+            }
+            curl[f] = kFaceCurl[q];
+            face_area[f] = kFaceNormal[q] == 2 ? area_z : (kFaceNormal[q] == 1 ? area_y : area_x);
+            boundary_face[f] = kFaceLabel[q];
+            tbc_flag[f] = m != 0;
+          } else {
+            boundary_face[f] = mat_adj(vol_material[Dt[f][0].first], vol_material[Dt[f][1].first]);
+            tbc_flag[f] = tbc_flag[f] || m != 0;
+          }
+        }
+        // material averages (:5234-5330)
+        const int face_of_axis[3][2] = {{2, 3}, {1, 4}, {0, 5}};
+        const int edges_of_axis[3][4] = {{0, 5, 8, 11}, {1, 3, 9, 10}, {2, 4, 6, 7}};
+        for (int a = 0; a < 3; a++)
+          if (mat.mu.m[a][a] != 0)
+            for (int s = 0; s < 2; s++) avg_ni[d[face_of_axis[a][s]]] += L[a] / 2 / mat.mu.m[a][a];
+        for (int a = 0; a < 3; a++)
+          if (mat.chi.m[a][a] != 0)
+            for (int s = 0; s < 2; s++) {
+              avg_msig[d[face_of_axis[a][s]]] += L[a] / 2 / mat.chi.m[a][a];
+              mag_lossy[d[face_of_axis[a][s]]]++;
+            }
+        for (int a = 0; a < 3; a++)
+          if (mat.eps.m[a][a] != 0)
+            for (int s = 0; s < 4; s++) avg_eps[e[edges_of_axis[a][s]]] += da[a] * mat.eps.m[a][a];
+        for (int a = 0; a < 3; a++)
+          if (mat.sigma.m[a][a] != 0)
+            for (int s = 0; s < 4; s++) {
+              avg_sigma[e[edges_of_axis[a][s]]] += da[a] * mat.sigma.m[a][a];
+              ele_lossy[e[edges_of_axis[a][s]]]++;
+            }
+        nv++;
+        px += Lx;
+      }
+      py += Ly;
+    }
+    pz += Lz;
+  }
+  nE = ne; nF = nf; nV = nv;
+
+  // edge sources/BC bookkeeping and classification (:5353-5468)
+  edge_src.assign(nE, {});
+  std::vector<uint32_t> H_dummy;
+  for (uint32_t f = 0; f < nF; f++)
+    if (tbc_flag[f]) tbc.push_back(f);
+  for (uint32_t i = 0; i < nE; i++) {
+    uint32_t in_b = 0, brk = 0;
+    for (auto& sf : Ct[i]) {
+      uint64_t bid = boundary_face[sf.first];
+      if (bid == 0) continue;
+      const BoundaryCondition* bc = bid < 100 ? &sc.bcs[sc.bnd_to_bc[bid]] : nullptr;
+      if (bc && bc->type == "pec") {
+        in_b++;
+        edge_src[i].clear();
+        bc_edges.push_back(i);
+        if (brk == 1) src_edges.pop_back();
+        else if (brk == 2) uncommon_edges.pop_back();
+        break;
+      }
+      for (uint32_t sl : sim.sources) {
+        Source& src = sc.sources[sl];
+        if (std::find(src.surfaces.begin(), src.surfaces.end(), (uint32_t)bid) == src.surfaces.end()) continue;
+        in_b++;
+        if (src.st == "e") {
+          if (brk == 2) break;
+          if (std::find(edge_src[i].begin(), edge_src[i].end(), sl) == edge_src[i].end()) {
+            edge_src[i].push_back(sl);
+            brk = 1;
+            if (src_edges.empty() || src_edges.back() != i) src_edges.push_back(i);
+          }
+        } else if (src.st == "h") {
+          if (brk == 1) break;
+          if (std::find(edge_src[i].begin(), edge_src[i].end(), sl) == edge_src[i].end()) {
+            edge_src[i].push_back(sl);
+            brk = 2;
+            if (uncommon_edges.empty() || uncommon_edges.back() != i) uncommon_edges.push_back(i);
+          }
+        }
+      }
+    }
+    if (in_b == 0) {
+      if (Ct[i].size() == 4) common_edges.push_back(i);
+      else uncommon_edges.push_back(i);  // natural boundary edge (divergence, see header)
+    }
+  }
+
+  // time step (:5472-5483)
+  std::vector<double> Nvec(nF), Hvec(nE);
+  for (uint32_t f = 0; f < nF; f++) Nvec[f] = avg_ni[f] / face_area[f];
+  for (uint32_t e = 0; e < nE; e++) Hvec[e] = edge_len[e] / avg_eps[e];
+  // TF_ORACLE_SKIP_DT=1 (timing runs only): skip the eigen-estimate and take a
+  // pinned step as given.
+  const char* skip = std::getenv("TF_ORACLE_SKIP_DT");
+  if (skip && skip[0] == '1' && sim.step != 0) dt_estimate = sim.step;
+  else dt_estimate = sim.courant * fdtd_time_step(Nvec, Hvec);
+  dt = dt_estimate;
+  possibly_unstable = false;
+  if (sim.step != 0) {
+    if (sim.step > dt) possibly_unstable = true;
+    else dt = sim.step;
+  }
+
+  // coefficients (:5485-5649); pml factors are 1 without PML
+  for (uint32_t f = 0; f < nF; f++) {
+    if (avg_ni[f] != 0) {
+      if (mag_lossy[f]) {
+        M_nu.push_back(1 / (face_area[f] * (1 / avg_ni[f] + 0.5 * dt / avg_msig[f])));
+        M_mu.push_back(face_area[f] * (1 / avg_ni[f] - 0.5 * dt / avg_msig[f]));
+      } else {
+        M_nu.push_back(avg_ni[f] / face_area[f]);
+        M_mu.push_back(face_area[f] / avg_ni[f]);
+      }
+    } else {
+      M_nu.push_back(0);
+      M_mu.push_back(0);
+    }
+  }
+  for (uint32_t i = 0; i < nE; i++) {
+    if (!edge_src[i].empty()) {  // source consistency filter (:5576-5589)
+      std::vector<uint32_t> keep;
+      uint32_t first = edge_src[i][0];
+      std::string ftype = sc.sources[first].st;
+      uint32_t fsurf = sc.sources[first].surfaces.empty() ? 0 : sc.sources[first].surfaces[0];
+      for (auto k : edge_src[i]) {
+        Source& s = sc.sources[k];
+        if (s.st == ftype && (s.surfaces.empty() ? 0 : s.surfaces[0]) == fsurf) keep.push_back(k);
+      }
+      edge_src[i] = keep;
+    }
+    if (avg_eps[i] != 0) {
+      if (ele_lossy[i]) {
+        M_h.push_back(edge_len[i] / (avg_eps[i] + 0.5 * dt * avg_sigma[i]));
+        M_q.push_back((avg_eps[i] - 0.5 * dt * avg_sigma[i]) / edge_len[i]);
+      } else {
+        M_h.push_back(edge_len[i] / avg_eps[i]);
+        M_q.push_back(avg_eps[i] / edge_len[i]);
+      }
+    } else {
+      M_h.push_back(0);
+      M_q.push_back(0);
+    }
+  }
+  bnd_dual.assign(nE, {0, 0, 0});
+}
+
+uint32_t FitOracle::which_solid(double x, double y, double z) {
+  // Discretization.hpp:10110-10122: first solid in ascending label order
+  for (auto& s : solids)
+    if (s.second.rule(x, y, z)) return s.second.material;
+  return 0;
+}
+
+double FitOracle::fdtd_time_step(const std::vector<double>& Nvec, const std::vector<double>& Hvec) {
+  // Operator of Discretization.hpp:7058-7084, A = Einv C^T N C, symmetrised as
+  // Einv^1/2 C^T N C Einv^1/2; dt = 2/sqrt(lambda_max) (:7118).
+  std::vector<double> sq(nE), Fb(nF), tmp(nE);
+  for (uint32_t e = 0; e < nE; e++) sq[e] = std::sqrt(Hvec[e]);
+  auto apply = [&](const double* x, double* y) {
+    for (uint32_t e = 0; e < nE; e++) tmp[e] = sq[e] * x[e];
+    for (uint32_t f = 0; f < nF; f++)
+      Fb[f] = Nvec[f] * curl[f] * (tmp[C[f][0]] - tmp[C[f][1]] + tmp[C[f][2]] - tmp[C[f][3]]);
+    for (uint32_t e = 0; e < nE; e++) {
+      double s = 0;
+      if (Ct[e].size() < 4) {
+        for (auto& sf : Ct[e]) s += Fb[sf.first] * sf.second;
+      } else {
+        s = dual_curl[e] * (Fb[Ct[e][0].first] - Fb[Ct[e][1].first] + Fb[Ct[e][2].first] - Fb[Ct[e][3].first]);
+      }
+      y[e] = sq[e] * s;
+    }
+  };
+  double lam = lanczos_max(nE, apply);
+  return 2.0 / std::sqrt(lam);
+}
+
+std::array<double, 3> FitOracle::edge_bar(uint32_t e) const {
+  // Discretization.hpp:10528-10540
+  const auto &a = pts[G[e][0]], &b = pts[G[e][1]];
+  return {(a[0] + b[0]) / 2, (a[1] + b[1]) / 2, (a[2] + b[2]) / 2};
+}
+
+std::array<double, 3> FitOracle::face_bar(uint32_t f) const {
+  // Discretization.hpp:10455-10469
+  double bc[3] = {0, 0, 0};
+  for (int r = 0; r < 4; r++)
+    for (int s = 0; s < 2; s++) {
+      const auto& p = pts[G[C[f][r]][s]];
+      for (int a = 0; a < 3; a++) bc[a] += 0.5 * p[a];
+    }
+  return {bc[0] / 4, bc[1] / 4, bc[2] / 4};
+}
+
+std::array<double, 3> FitOracle::vol_bar(uint32_t v) const {
+  // Discretization.hpp:10485-10490
+  double bc[3] = {0, 0, 0};
+  for (int q = 0; q < 8; q++)
+    for (int a = 0; a < 3; a++) bc[a] += pts[Pcl[v][q]][a];
+  return {bc[0] / 8, bc[1] / 8, bc[2] / 8};
+}
+
+uint32_t FitOracle::find_probe(const std::array<double, 3>& pv) {
+  // Discretization.hpp:3590-3643: breadth-first walk from the last hit; the
+  // first cube whose closed box (tolerance 1e-12) holds the point wins.
+  const double tol = 1e-12;
+  std::vector<uint8_t> colour(nV, 0);
+  std::vector<uint32_t> q;
+  q.push_back(root);
+  colour[0]++;
+  size_t k = 0;
+  while (k < q.size()) {
+    uint32_t v = q[k];
+    const auto& pp = pts[Pcl[v][0]];
+    double d0 = pv[0] - pp[0], d1 = pv[1] - pp[1], d2 = pv[2] - pp[2];
+    if (d0 >= -tol && d0 < Lx + tol && d1 >= -tol && d1 < Ly + tol && d2 >= -tol && d2 < Lz + tol) {
+      root = v;
+      return v;
+    }
+    for (uint32_t f : D[v]) {
+      uint32_t n = Dt[f].front().first;
+      if (n == v) n = Dt[f].back().first;
+      if (colour[n] == 0) {
+        q.push_back(n);
+        colour[n]++;
+      }
+    }
+    if (colour[v] < 255) colour[v]++;
+    k++;
+  }
+  return nV;
+}
+
+void FitOracle::prepare(uint32_t label) {
+  // Discretization.hpp:289-428 (setup of one simulation)
+  sim_label = label;
+  sim = sc.simulations.at(label);
+  const Mesh& msh = sc.meshes[sim.mesh];
+  if (msh.type != "cartesian") throw std::runtime_error("FIT oracle needs a cartesian mesh");
+  if (sim.method != "fdtd") throw std::runtime_error("FIT oracle needs method fdtd");
+  out = sc.outputs[sim.output];
+  out.initialize();
+  root = 0;
+  build_mesh();
+  U.assign(nE, 0); I.assign(nE, 0); curl_fb.assign(nE, 0);
+  F.assign(nF, 0); B.assign(nF, 0);
+  probe_elem.clear(); probe_pts.clear();
+  if (out.mode == "probepoint") {
+    for (auto& pv : out.probes) {
+      uint32_t v = find_probe(pv);
+      if (v < nV) {
+        probe_elem.push_back(v);
+        probe_pts.push_back(pv);
+      }
+    }
+    // point dipoles (:466-502)
+    for (uint32_t sl : sim.sources) {
+      Source& s = sc.sources[sl];
+      if (s.st != "j") continue;
+      uint32_t v = find_probe(s.location);
+      if (v >= nV) continue;
+      uint32_t best = Ecl[v][0];
+      auto eb = edge_bar(best);
+      double bd = std::sqrt(std::pow(eb[0] - s.location[0], 2) + std::pow(eb[1] - s.location[1], 2) +
+                            std::pow(eb[2] - s.location[2], 2));
+      for (int q = 1; q < 12; q++) {
+        auto b = edge_bar(Ecl[v][q]);
+        double d = std::sqrt(std::pow(b[0] - s.location[0], 2) + std::pow(b[1] - s.location[1], 2) +
+                             std::pow(b[2] - s.location[2], 2));
+        if (d < bd) { bd = d; best = Ecl[v][q]; }
+      }
+      if (edge_src[best].empty()) src_edges.push_back(best);
+      edge_src[best].push_back(sl);
+    }
+  }
+  times.clear(); samples.clear(); flux.clear();
+  step_index = 0;
+  nsteps_total = 0;
+  while ((double)nsteps_total * dt <= sim.duration) nsteps_total++;
+}
+
+double FitOracle::efield_source(uint32_t e, double t) {
+  // ComputeEfieldSource, Discretization.hpp:3907-3940
+  if (t < 0) return 0;
+  auto eb = edge_bar(e);
+  double v[3] = {0, 0, 0};
+  for (auto s : edge_src[e])
+    if (sc.sources[s].st == "e") {
+      auto r = sc.sources[s].compute(eb[0], eb[1], eb[2], t);
+      for (int a = 0; a < 3; a++) v[a] += r[a];
+    }
+  const auto &p0 = pts[G[e][0]], &p1 = pts[G[e][1]];
+  return v[0] * (p1[0] - p0[0]) + v[1] * (p1[1] - p0[1]) + v[2] * (p1[2] - p0[2]);
+}
+
+double FitOracle::current_source(uint32_t e, double t) {
+  // ComputeCurrentSource, Discretization.hpp:3994-4028
+  if (t < 0) return 0;
+  auto eb = edge_bar(e);
+  double v[3] = {0, 0, 0};
+  for (auto s : edge_src[e])
+    if (sc.sources[s].st == "j") {
+      auto r = sc.sources[s].compute(eb[0], eb[1], eb[2], t);
+      for (int a = 0; a < 3; a++) v[a] += r[a];
+    }
+  const auto &p0 = pts[G[e][0]], &p1 = pts[G[e][1]];
+  double ev[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+  double n = std::sqrt(ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2]);
+  return (1.0 / n) * (v[0] * ev[0] + v[1] * ev[1] + v[2] * ev[2]);
+}
+
+double FitOracle::hfield_source(uint32_t e, double t) {
+  // ComputeHfieldSource, Cartesian branch, Discretization.hpp:4088-4202
+  if (t < 0) return 0;
+  auto eb = edge_bar(e);
+  double v[3] = {0, 0, 0};
+  for (auto s : edge_src[e])
+    if (sc.sources[s].st == "h") {
+      auto r = sc.sources[s].compute(eb[0], eb[1], eb[2], t);
+      for (int a = 0; a < 3; a++) v[a] += r[a];
+    }
+  auto& bd = bnd_dual[e];
+  if (bd[0] == 0 && bd[1] == 0 && bd[2] == 0) {
+    // lazily built dual edge on the boundary (:4150-4196)
+    int nf = 0, ni = 0;
+    std::array<double, 3> vb{0, 0, 0}, backup{0, 0, 0};
+    for (auto& sf : Ct[e]) {
+      uint32_t f = sf.first;
+      auto fb = face_bar(f);
+      if (boundary_face[f] > 0) {
+        ++nf;
+        auto vbar = vol_bar(Dt[f][0].first);
+        backup = {vbar[0] - eb[0], vbar[1] - eb[1], vbar[2] - eb[2]};
+        if (nf == 1) bd = fb;
+        else if (nf == 2) bd = {fb[0] - bd[0], fb[1] - bd[1], fb[2] - bd[2]};
+      } else {
+        vb = {fb[0] - eb[0], fb[1] - eb[1], fb[2] - eb[2]};
+        ni++;
+      }
+    }
+    if (!ni) vb = backup;
+    const auto &p0 = pts[G[e][0]], &p1 = pts[G[e][1]];
+    double ev[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+    double cr[3] = {ev[1] * bd[2] - ev[2] * bd[1], ev[2] * bd[0] - ev[0] * bd[2], ev[0] * bd[1] - ev[1] * bd[0]};
+    if (cr[0] * vb[0] + cr[1] * vb[1] + cr[2] * vb[2] < 0) bd = {-bd[0], -bd[1], -bd[2]};
+  }
+  return v[0] * bd[0] + v[1] * bd[1] + v[2] * bd[2];
+}
+
+void FitOracle::export_probes(double t) {
+  // ExportFitFields "probepoint" (:3096-3158) with GetFitElectricField /
+  // GetFitMagneticField (:3555-3588).  mu^-1 is taken as 1/mu on the diagonal
+  // (the reference inverts the 3x3 matrix by cofactors: <= 2 ulp apart).
+  const double vol = Lx * Ly * Lz;
+  const double dax = Ly * Lz / 4, day = Lx * Lz / 4, daz = Lx * Ly / 4;
+  for (size_t p = 0; p < probe_elem.size(); p++) {
+    uint32_t c = probe_elem[p];
+    const auto& e = Ecl[c];
+    double Ex = (U[e[0]] * dax + U[e[5]] * dax + U[e[8]] * dax + U[e[11]] * dax) / vol;
+    double Ey = (U[e[1]] * day + U[e[3]] * day + U[e[9]] * day + U[e[10]] * day) / vol;
+    double Ez = (U[e[2]] * daz + U[e[4]] * daz + U[e[6]] * daz + U[e[7]] * daz) / vol;
+    const auto& d = D[c];
+    const Material& m = sc.materials[vol_material[c]];
+    double hx = B[d[2]] * (0.5 * Lx) + B[d[3]] * (0.5 * Lx);
+    double hy = B[d[1]] * (0.5 * Ly) + B[d[4]] * (0.5 * Ly);
+    double hz = B[d[0]] * (0.5 * Lz) + B[d[5]] * (0.5 * Lz);
+    double Hx = (1.0 / m.mu.m[0][0]) * hx / vol;
+    double Hy = (1.0 / m.mu.m[1][1]) * hy / vol;
+    double Hz = (1.0 / m.mu.m[2][2]) * hz / vol;
+    samples.push_back(Ex); samples.push_back(Ey); samples.push_back(Ez);
+    samples.push_back(Hx); samples.push_back(Hy); samples.push_back(Hz);
+  }
+  times.push_back(t);
+}
+
+uint64_t FitOracle::step(uint64_t n) {
+  // Discretization.hpp:1840-1933, one iteration per step
+  uint64_t done = 0;
+  std::vector<double> U_old;
+  for (; done < n && step_index < nsteps_total; done++, step_index++) {
+    const double t = (double)step_index * dt;
+    U_old = U;
+    // PEC edges hold the PEC value 0 (BoundaryCondition.hpp:61-68).  The
+    // reference reads it through BCs[BndToBC[edge_bcs[e]]] (:3904, :5407), a
+    // double lookup that can land on a default BC with an unset value.
+    for (auto j : bc_edges) U[j] = 0.0;
+    for (auto j : src_edges) {
+      if (sc.sources[edge_src[j][0]].st == "j") I[j] = current_source(j, t);
+      else U[j] = efield_source(j, t);
+    }
+#pragma omp parallel for schedule(static)
+    for (size_t q = 0; q < common_edges.size(); q++) {
+      const uint32_t j = common_edges[q];
+      const auto& c = Ct[j];
+      U[j] = M_h[j] * (M_q[j] * U_old[j] +
+                       dt * (dual_curl[j] * (F[c[0].first] - F[c[1].first] + F[c[2].first] - F[c[3].first]) - I[j]));
+    }
+    for (auto j : uncommon_edges) {
+      curl_fb[j] = edge_src[j].empty() ? 0.0 : hfield_source(j, t - 0.5 * dt);
+      double s = 0;
+      for (auto& sf : Ct[j]) s += F[sf.first] * sf.second;
+      U[j] = M_h[j] * (M_q[j] * U_old[j] + dt * (s + curl_fb[j] - I[j]));
+    }
+    double fl = 0;
+    for (uint32_t e = 0; e < nE; e++) fl += (U_old[e] + U[e]) * curl_fb[e];
+    flux.push_back(0.5 * fl);
+#pragma omp parallel for schedule(static)
+    for (size_t q = 0; q < tbc.size(); q++) {
+      const uint32_t j = tbc[q];
+      const auto& c = C[j];
+      B[j] = M_mu[j] * F[j] - dt * curl[j] * (U[c[0]] - U[c[1]] + U[c[2]] - U[c[3]]);
+      F[j] = M_nu[j] * B[j];
+    }
+    if (out.mode == "probepoint" && out.allow_print(t)) export_probes(t);
+  }
+  return done;
+}
+
+}  // namespace orc

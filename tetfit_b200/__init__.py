@@ -1,0 +1,234 @@
+"""B200-native TetFIT leapfrog time-stepping path.
+
+The product is the shared library `libtetfit_b200.so` (C ABI declared in
+include/tetfit.h: C++ host code driving sm_100a CUDA kernels).  This module is
+a thin ctypes mirror of the reference's driver interface
+(src/DGA/Discretization.hpp:45-211 `Discretization(inputfile)`, :289
+`RunSimulation(sim, label)`, src/DGA/main/dga_main.cpp:52-62), plus stepwise
+access used by tests and the benchmark.  There is no CPU fallback: importing
+raises if the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtetfit_b200.so")
+
+TF_OK, TF_E_SCRIPT, TF_E_ARG, TF_E_CUDA, TF_E_UNSUPPORTED, TF_E_STATE, TF_E_SOLVER = 0, -1, -2, -3, -4, -5, -6
+FP64, FP32 = 0, 1
+METHODS = {0: "fdtd", 1: "dga", 2: "gfdtd"}
+
+
+class TetfitError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+        self.message = message
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int32), ("device", ctypes.c_int32), ("write_files", ctypes.c_int32),
+                ("verbose", ctypes.c_int32), ("graph_steps", ctypes.c_int32), ("reserved", ctypes.c_int32 * 11)]
+
+
+class Info(ctypes.Structure):
+    _fields_ = [("n_edges", ctypes.c_uint64), ("n_faces", ctypes.c_uint64), ("n_cells", ctypes.c_uint64),
+                ("n_probes", ctypes.c_uint64), ("n_steps", ctypes.c_uint64), ("step_index", ctypes.c_uint64),
+                ("nx", ctypes.c_uint32), ("ny", ctypes.c_uint32), ("nz", ctypes.c_uint32),
+                ("method", ctypes.c_int32), ("dt", ctypes.c_double), ("dt_estimate", ctypes.c_double),
+                ("possibly_unstable", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("device_bytes", ctypes.c_uint64), ("kernels_per_step", ctypes.c_uint32),
+                ("n_sources", ctypes.c_uint32), ("reserved", ctypes.c_uint64 * 7)]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        d["method"] = METHODS.get(d["method"], d["method"])
+        return d
+
+
+_lib = None
+
+# name -> (restype, argtypes); every symbol declared in include/tetfit.h
+_P = ctypes.c_void_p
+_SIGS = {
+    "tf_open": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_P)]),
+    "tf_simulations": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32,
+                                      ctypes.POINTER(ctypes.c_uint32)]),
+    "tf_prepare": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(Opts)]),
+    "tf_get_info": (ctypes.c_int, [_P, ctypes.POINTER(Info)]),
+    "tf_step": (ctypes.c_int, [_P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
+    "tf_get_probes": (ctypes.c_int, [_P, _P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "tf_get_probe_points": (ctypes.c_int, [_P, _P, _P, ctypes.c_size_t]),
+    "tf_get_state": (ctypes.c_int, [_P, _P, ctypes.c_size_t, _P, ctypes.c_size_t, _P, ctypes.c_size_t]),
+    "tf_set_state": (ctypes.c_int, [_P, _P, ctypes.c_size_t, _P, ctypes.c_size_t]),
+    "tf_get_flux": (ctypes.c_int, [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "tf_energy": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double)]),
+    "tf_step_io": (ctypes.c_int, [_P, _P, _P, ctypes.POINTER(ctypes.c_uint64)]),
+    "tf_phase_times": (ctypes.c_int, [_P, ctypes.c_uint64, _P, ctypes.POINTER(ctypes.c_uint64)]),
+    "tf_run": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(Opts)]),
+    "tf_last_step_ms": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double)]),
+    "tf_last_error": (ctypes.c_char_p, [_P]),
+    "tf_close": (None, [_P]),
+    "tf_default_opts": (None, [ctypes.POINTER(Opts)]),
+}
+
+
+def lib():
+    """Load the native library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m tetfit_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+class Discretization:
+    """Mirror of TetFIT's `Discretization` driver for one `.fdtd` script.
+
+    `Discretization(path)` parses the script like Discretization.hpp:45-211;
+    `run_simulation(label)` runs one simulation end to end like
+    RunSimulation (Discretization.hpp:289-2303), writing the same probe and
+    poynting files when `write_files=True`.  Script errors raise TetfitError
+    whose message is the reference's "Input file error at line N: ..." text.
+    """
+
+    def __init__(self, path: str):
+        L = lib()
+        self._h = _P()
+        rc = L.tf_open(os.fsencode(path), ctypes.byref(self._h))
+        if rc != TF_OK:
+            msg = L.tf_last_error(self._h).decode()
+            L.tf_close(self._h)
+            self._h = None
+            raise TetfitError(rc, msg)
+
+    def _check(self, rc):
+        if rc != TF_OK:
+            raise TetfitError(rc, lib().tf_last_error(self._h).decode())
+
+    @property
+    def simulations(self) -> list:
+        n = ctypes.c_uint32()
+        self._check(lib().tf_simulations(self._h, None, 0, ctypes.byref(n)))
+        arr = (ctypes.c_uint32 * max(n.value, 1))()
+        self._check(lib().tf_simulations(self._h, arr, n.value, ctypes.byref(n)))
+        return list(arr)[: n.value]
+
+    @staticmethod
+    def _opts(precision="fp64", device=0, write_files=False, verbose=False, graph_steps=0) -> Opts:
+        o = Opts()
+        lib().tf_default_opts(ctypes.byref(o))
+        o.precision = {"fp64": FP64, "fp32": FP32}[precision] if isinstance(precision, str) else int(precision)
+        o.device, o.write_files, o.verbose, o.graph_steps = device, int(write_files), int(verbose), graph_steps
+        return o
+
+    def prepare(self, label: int, **opts) -> dict:
+        o = self._opts(**opts)
+        self._check(lib().tf_prepare(self._h, label, ctypes.byref(o)))
+        return self.info()
+
+    def run_simulation(self, label: int, **opts) -> dict:
+        o = self._opts(**opts)
+        self._check(lib().tf_run(self._h, label, ctypes.byref(o)))
+        return self.info()
+
+    def info(self) -> dict:
+        i = Info()
+        self._check(lib().tf_get_info(self._h, ctypes.byref(i)))
+        return i.as_dict()
+
+    def step(self, n: int) -> int:
+        done = ctypes.c_uint64()
+        self._check(lib().tf_step(self._h, n, ctypes.byref(done)))
+        return done.value
+
+    def step_io(self, carrier_in=None, probe_out=None) -> int:
+        """One step with this step's carrier values from host memory and the
+        exported probe sample read back (see tf_step_io)."""
+        done = ctypes.c_uint64()
+        self._check(lib().tf_step_io(self._h, _ptr(carrier_in), _ptr(probe_out), ctypes.byref(done)))
+        return done.value
+
+    def phase_times(self, n: int):
+        """Device ms per phase over n steps: sources/BC, E, scatter+flux, probes, H."""
+        ms = np.zeros(5)
+        done = ctypes.c_uint64()
+        self._check(lib().tf_phase_times(self._h, n, _ptr(ms), ctypes.byref(done)))
+        return ms, done.value
+
+    def last_step_ms(self) -> float:
+        ms = ctypes.c_double()
+        self._check(lib().tf_last_step_ms(self._h, ctypes.byref(ms)))
+        return ms.value
+
+    def probes(self):
+        """(times[n], values[n, n_probes, 6]) with columns Ex Ey Ez Hx Hy Hz."""
+        n = ctypes.c_size_t()
+        self._check(lib().tf_get_probes(self._h, None, None, 0, ctypes.byref(n)))
+        np_ = self.info()["n_probes"]
+        t = np.zeros(n.value)
+        v = np.zeros((n.value, np_, 6))
+        self._check(lib().tf_get_probes(self._h, _ptr(t), _ptr(v), n.value, ctypes.byref(n)))
+        return t, v
+
+    def probe_points(self):
+        np_ = self.info()["n_probes"]
+        xyz = np.zeros((np_, 3))
+        cells = np.zeros(np_, dtype=np.uint64)
+        self._check(lib().tf_get_probe_points(self._h, _ptr(xyz), _ptr(cells), np_))
+        return xyz, cells
+
+    def state(self):
+        """(U[n_edges], B[n_faces], F[n_faces]) in the reference's numbering."""
+        i = self.info()
+        U, B, F = np.zeros(i["n_edges"]), np.zeros(i["n_faces"]), np.zeros(i["n_faces"])
+        self._check(lib().tf_get_state(self._h, _ptr(U), U.size, _ptr(B), B.size, _ptr(F), F.size))
+        return U, B, F
+
+    def set_state(self, U, F):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        F = np.ascontiguousarray(F, dtype=np.float64)
+        self._check(lib().tf_set_state(self._h, _ptr(U), U.size, _ptr(F), F.size))
+
+    def flux(self):
+        n = ctypes.c_size_t()
+        self._check(lib().tf_get_flux(self._h, None, 0, ctypes.byref(n)))
+        f = np.zeros(n.value)
+        self._check(lib().tf_get_flux(self._h, _ptr(f), n.value, ctypes.byref(n)))
+        return f
+
+    def energy(self) -> float:
+        e = ctypes.c_double()
+        self._check(lib().tf_energy(self._h, ctypes.byref(e)))
+        return e.value
+
+    def close(self):
+        if self._h:
+            lib().tf_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,296 @@
+// extern "C" boundary (include/tetfit.h).  Maps C++ exceptions to status
+// codes; nothing throws across the ABI.
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <memory>
+#include <sstream>
+#include <string>
+
+#include "../../include/tetfit.h"
+#include "cuda_util.hpp"
+#include "fit.hpp"
+#include "script.hpp"
+
+struct tf_ctx {
+  tf::Script sc;
+  std::string path, err;
+  std::unique_ptr<tf::FitSim> fit;
+  uint32_t label = 0;
+  tf_opts opts{};
+};
+
+namespace {
+
+int fail(tf_ctx* c, int code, const std::string& m) {
+  if (c) c->err = m;
+  return code;
+}
+
+template <typename F>
+int guarded(tf_ctx* c, F&& f) {
+  try {
+    return f();
+  } catch (const tf::ScriptError& e) {
+    return fail(c, TF_E_SCRIPT, e.what());
+  } catch (const tf::CudaError& e) {
+    return fail(c, TF_E_CUDA, e.what());
+  } catch (const tf::UnsupportedError& e) {
+    return fail(c, TF_E_UNSUPPORTED, e.what());
+  } catch (const tf::SolverError& e) {
+    return fail(c, TF_E_SOLVER, e.what());
+  } catch (const std::invalid_argument& e) {
+    return fail(c, TF_E_ARG, e.what());
+  } catch (const std::exception& e) {
+    return fail(c, TF_E_ARG, e.what());
+  }
+}
+
+// Output files of Discretization.hpp:1948-2010 (probe series) and :1936-1941
+// (poynting.dat): std::setw(15), default stream precision.
+void write_outputs(tf_ctx* c) {
+  tf::FitSim& f = *c->fit;
+  const tf::Output& o = f.output();
+  if (o.mode == "probepoint") {
+    size_t ns = f.n_samples(), np = f.n_probes();
+    std::vector<double> t(ns), v(ns * np * 6), xyz(np * 3);
+    f.get_probes(t.data(), v.data(), ns);
+    f.probe_points(xyz.data(), nullptr, np);
+    std::stringstream se, sh;
+    se << o.name << std::setw(5) << std::setfill('0') << c->label << "_probe_E.dat";
+    sh << o.name << std::setw(5) << std::setfill('0') << c->label << "_probe_H.dat";
+    std::ofstream os(se.str()), osh(sh.str());
+    for (size_t k = 0; k < ns; k++)
+      for (size_t p = 0; p < np; p++) {
+        const double* s = &v[(k * np + p) * 6];
+        os << std::setw(15) << xyz[3 * p] << " " << std::setw(15) << xyz[3 * p + 1] << " " << std::setw(15)
+           << xyz[3 * p + 2] << " " << std::setw(15) << t[k] << " " << std::setw(15) << s[0] << " "
+           << std::setw(15) << s[1] << " " << std::setw(15) << s[2] << std::endl;
+        osh << std::setw(15) << xyz[3 * p] << " " << std::setw(15) << xyz[3 * p + 1] << " " << std::setw(15)
+            << xyz[3 * p + 2] << " " << std::setw(15) << t[k] - 0.5 * f.dt() << " " << std::setw(15) << s[3]
+            << " " << std::setw(15) << s[4] << " " << std::setw(15) << s[5] << std::endl;
+      }
+  }
+  size_t n = 0;
+  f.get_flux(nullptr, 0, &n);
+  std::vector<double> fl(n);
+  f.get_flux(fl.data(), n, &n);
+  std::ofstream pf("poynting.dat");
+  for (size_t k = 0; k < n; k++) pf << double(k + 0.5) * f.dt() << "\t" << fl[k] << "\t" << 0.0 << std::endl;
+}
+
+void banner(tf_ctx* c) {
+  tf::FitSim& f = *c->fit;
+  std::cout << std::endl << "Simulation parameters:" << std::endl;
+  std::cout << std::setw(20) << "Method: " << std::setw(20) << "fdtd" << std::endl;
+  std::cout << std::setw(20) << "Simulation time: " << std::setw(20) << f.simulation().duration << " sec"
+            << std::endl;
+  std::cout << std::setw(20) << "Time step: " << std::setw(20) << f.dt() << " sec" << std::endl;
+  std::cout << std::setw(20) << "Elements: " << std::setw(20) << f.n_cells() << std::endl;
+  std::cout << std::setw(20) << "Surfaces: " << std::setw(20) << f.n_faces() << std::endl;
+  std::cout << std::setw(20) << "Edges:    " << std::setw(20) << f.n_edges() << std::endl;
+  std::cout << std::setw(20) << "Unknowns: " << std::setw(20) << f.n_edges() + f.n_faces() << std::endl;
+  if (f.possibly_unstable())
+    std::cout << "WARNING: the time step size chosen by the user is possibly unstable! (Upper stable limit will "
+                 "be used instead...)"
+              << std::endl;
+}
+
+}  // namespace
+
+extern "C" {
+
+void tf_default_opts(tf_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->precision = TF_FP64;
+}
+
+int tf_open(const char* path, tf_ctx** out) {
+  if (!out || !path) return TF_E_ARG;
+  *out = nullptr;
+  auto* c = new tf_ctx();
+  c->path = path;
+  tf_default_opts(&c->opts);
+  int rc = guarded(c, [&]() -> int {
+    c->sc.parse(path);
+    return TF_OK;
+  });
+  *out = c;  // the context carries the error message even on failure
+  return rc;
+}
+
+int tf_simulations(tf_ctx* c, uint32_t* labels, uint32_t cap, uint32_t* n) {
+  if (!c) return TF_E_ARG;
+  uint32_t k = 0;
+  for (auto& kv : c->sc.simulations) {
+    if (labels && k < cap) labels[k] = kv.first;
+    k++;
+  }
+  if (n) *n = k;
+  return TF_OK;
+}
+
+int tf_prepare(tf_ctx* c, uint32_t label, const tf_opts* opts) {
+  if (!c) return TF_E_ARG;
+  return guarded(c, [&]() -> int {
+    c->fit.reset();
+    if (opts) c->opts = *opts;
+    auto it = c->sc.simulations.find(label);
+    if (it == c->sc.simulations.end()) return fail(c, TF_E_ARG, "unknown simulation label " + std::to_string(label));
+    const std::string& meth = it->second.method;
+    const std::string mtype = c->sc.meshes[it->second.mesh].type;
+    // Discretization.hpp:313-316
+    if ((mtype == "tetrahedral" && meth == "fdtd") || (mtype == "cartesian" && meth != "fdtd" && meth != "fdtdo2"))
+      throw tf::ScriptError("Input file error at line 0: If mesh type is tetrahedral, method must be fem or dga. If "
+                            "mesh type is cartesian, method must be fdtd");
+    tf::RunOptions ro;
+    ro.precision = c->opts.precision;
+    ro.device = c->opts.device;
+    ro.graph_steps = c->opts.graph_steps;
+    ro.verbose = c->opts.verbose != 0;
+    if (meth == "fdtd") {
+      c->fit.reset(new tf::FitSim(c->sc, label, ro));
+    } else {
+      return fail(c, TF_E_UNSUPPORTED, "method " + meth + " is not available in this build");
+    }
+    c->label = label;
+    if (ro.verbose) banner(c);
+    return TF_OK;
+  });
+}
+
+int tf_get_info(tf_ctx* c, tf_info* info) {
+  if (!c || !info) return TF_E_ARG;
+  if (!c->fit) return fail(c, TF_E_STATE, "tf_get_info before tf_prepare");
+  std::memset(info, 0, sizeof(*info));
+  tf::FitSim& f = *c->fit;
+  info->n_edges = f.n_edges();
+  info->n_faces = f.n_faces();
+  info->n_cells = f.n_cells();
+  info->n_probes = f.n_probes();
+  info->n_steps = f.n_steps();
+  info->step_index = f.step_index();
+  info->nx = f.nx(); info->ny = f.ny(); info->nz = f.nz();
+  info->method = 0;
+  info->dt = f.dt();
+  info->dt_estimate = f.dt_estimate();
+  info->possibly_unstable = f.possibly_unstable();
+  info->precision = f.precision();
+  info->device_bytes = f.device_bytes();
+  info->kernels_per_step = (uint32_t)f.kernels_per_step();
+  info->n_sources = (uint32_t)f.n_sources();
+  return TF_OK;
+}
+
+int tf_step(tf_ctx* c, uint64_t n, uint64_t* done) {
+  if (!c) return TF_E_ARG;
+  if (!c->fit) return fail(c, TF_E_STATE, "tf_step before tf_prepare");
+  return guarded(c, [&]() -> int {
+    uint64_t d = c->fit->step(n);
+    if (done) *done = d;
+    return TF_OK;
+  });
+}
+
+int tf_step_io(tf_ctx* c, const double* carrier_in, double* probe_out, uint64_t* done) {
+  if (!c) return TF_E_ARG;
+  if (!c->fit) return fail(c, TF_E_STATE, "tf_step_io before tf_prepare");
+  return guarded(c, [&]() -> int {
+    uint64_t d = c->fit->step_io(carrier_in, probe_out);
+    if (done) *done = d;
+    return TF_OK;
+  });
+}
+
+int tf_phase_times(tf_ctx* c, uint64_t n, double* ms5, uint64_t* done) {
+  if (!c || !ms5) return TF_E_ARG;
+  if (!c->fit) return fail(c, TF_E_STATE, "tf_phase_times before tf_prepare");
+  return guarded(c, [&]() -> int {
+    uint64_t d = c->fit->phase_times(n, ms5);
+    if (done) *done = d;
+    return TF_OK;
+  });
+}
+
+int tf_get_probes(tf_ctx* c, double* times, double* values, size_t cap, size_t* n) {
+  if (!c) return TF_E_ARG;
+  if (!c->fit) return fail(c, TF_E_STATE, "tf_get_probes before tf_prepare");
+  return guarded(c, [&]() -> int {
+    size_t ns = c->fit->n_samples();
+    if (n) *n = ns;
+    c->fit->get_probes(times, values, cap);
+    return TF_OK;
+  });
+}
+
+int tf_get_probe_points(tf_ctx* c, double* xyz, uint64_t* cells, size_t cap) {
+  if (!c) return TF_E_ARG;
+  if (!c->fit) return fail(c, TF_E_STATE, "tf_get_probe_points before tf_prepare");
+  c->fit->probe_points(xyz, cells, cap);
+  return TF_OK;
+}
+
+int tf_get_state(tf_ctx* c, double* U, size_t nU, double* B, size_t nB, double* F, size_t nF) {
+  if (!c) return TF_E_ARG;
+  if (!c->fit) return fail(c, TF_E_STATE, "tf_get_state before tf_prepare");
+  if ((U && nU < c->fit->n_edges()) || (B && nB < c->fit->n_faces()) || (F && nF < c->fit->n_faces()))
+    return fail(c, TF_E_ARG, "state buffer too small");
+  return guarded(c, [&]() -> int {
+    c->fit->get_state(U, B, F);
+    return TF_OK;
+  });
+}
+
+int tf_set_state(tf_ctx* c, const double* U, size_t nU, const double* F, size_t nF) {
+  if (!c) return TF_E_ARG;
+  if (!c->fit) return fail(c, TF_E_STATE, "tf_set_state before tf_prepare");
+  if ((U && nU < c->fit->n_edges()) || (F && nF < c->fit->n_faces()))
+    return fail(c, TF_E_ARG, "state buffer too small");
+  return guarded(c, [&]() -> int {
+    c->fit->set_state(U, F);
+    return TF_OK;
+  });
+}
+
+int tf_get_flux(tf_ctx* c, double* flux, size_t cap, size_t* n) {
+  if (!c) return TF_E_ARG;
+  if (!c->fit) return fail(c, TF_E_STATE, "tf_get_flux before tf_prepare");
+  return guarded(c, [&]() -> int {
+    c->fit->get_flux(flux, cap, n);
+    return TF_OK;
+  });
+}
+
+int tf_energy(tf_ctx* c, double* e) {
+  if (!c || !e) return TF_E_ARG;
+  if (!c->fit) return fail(c, TF_E_STATE, "tf_energy before tf_prepare");
+  return guarded(c, [&]() -> int {
+    *e = c->fit->energy();
+    return TF_OK;
+  });
+}
+
+int tf_run(tf_ctx* c, uint32_t label, const tf_opts* opts) {
+  int rc = tf_prepare(c, label, opts);
+  if (rc) return rc;
+  return guarded(c, [&]() -> int {
+    while (c->fit->step_index() < c->fit->n_steps()) c->fit->step(c->fit->n_steps() - c->fit->step_index());
+    if (c->opts.write_files) write_outputs(c);
+    return TF_OK;
+  });
+}
+
+int tf_last_step_ms(tf_ctx* c, double* ms) {
+  if (!c || !ms) return TF_E_ARG;
+  if (!c->fit) return fail(c, TF_E_STATE, "no simulation prepared");
+  *ms = c->fit->last_step_ms();
+  return TF_OK;
+}
+
+const char* tf_last_error(tf_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+void tf_close(tf_ctx* c) { delete c; }
+
+}  // extern "C"

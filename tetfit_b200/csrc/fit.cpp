@@ -1,0 +1,1278 @@
+// Cartesian FIT host setup (Yee index space) and device runtime.
+//
+// The reference builds its Cartesian complex by sweeping cubes and numbering
+// entities as it meets them (Discretization.hpp:4347-5690).  Here the complex
+// is implicit: an edge or face is addressed by (component, i, j, k) in the
+// padded layout of fit_kernels.cuh, materials live per cell, and only the
+// edges whose update is not the interior 4-face stencil are listed.  The
+// reference's numbering is reproduced on demand (build_ref_maps) so that state
+// can be exchanged in the order a TetFIT caller expects.
+#include "fit.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <stdexcept>
+#include <unordered_map>
+
+#include "cuda_util.hpp"
+
+namespace tf {
+
+template <typename T>
+void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const ProbeSet& pr, int* step_counter,
+                     double* flux, cudaStream_t st, cudaEvent_t* ev);
+int fit_kernels_per_step(int n_special, int n_probes);
+template <typename T>
+size_t fit_launch_energy(const FitGrid<T>& g, double* part, cudaStream_t st);
+
+namespace {
+
+// Largest eigenvalue of the Lanczos tridiagonal (diagonal a, off-diagonal b)
+// by Sturm-sequence bisection.
+double tridiag_max(const std::vector<double>& a, const std::vector<double>& bfull) {
+  const size_t m = a.size();
+  std::vector<double> b(bfull.begin(), bfull.begin() + (m > 0 ? m - 1 : 0));
+  double lo = a[0], hi = a[0];
+  for (size_t i = 0; i < m; i++) {
+    double r = (i > 0 ? std::fabs(b[i - 1]) : 0) + (i + 1 < m ? std::fabs(b[i]) : 0);
+    lo = std::fmin(lo, a[i] - r);
+    hi = std::fmax(hi, a[i] + r);
+  }
+  for (int it = 0; it < 200 && hi - lo > 1e-15 * std::fabs(hi); it++) {
+    double x = 0.5 * (lo + hi), d = 1;
+    int below = 0;
+    for (size_t i = 0; i < m; i++) {
+      d = a[i] - x - (i > 0 ? b[i - 1] * b[i - 1] / d : 0);
+      if (d == 0) d = 1e-300;
+      if (d < 0) below++;
+    }
+    if (below >= (int)m) hi = x;
+    else lo = x;
+  }
+  return hi;
+}
+
+// face (normal axis n, Yee indices)
+struct FaceRef {
+  int n, i, j, k, sign;
+};
+
+const int kFaceSlotLow[3] = {2, 1, 0};   // x-, y-, z- slot in the reference cube
+const int kFaceSlotHigh[3] = {3, 4, 5};  // x+, y+, z+
+const int kLabelLow[3] = {2, 5, 1};      // domain-surface labels (Discretization.hpp:5084-5232)
+const int kLabelHigh[3] = {4, 3, 6};
+
+}  // namespace
+
+// ------------------------------------------------------------------ set-up
+FitSim::FitSim(Script& sc, uint32_t label, const RunOptions& opt) : sc_(sc), opt_(opt), label_(label) {
+  auto it = sc_.simulations.find(label);
+  if (it == sc_.simulations.end()) throw std::invalid_argument("unknown simulation label " + std::to_string(label));
+  sim_ = it->second;
+  out_ = sc_.outputs[sim_.output];
+  out_.initialize();
+  src_labels_ = sim_.sources;
+  setup_grid();
+  classify_edges();
+  dt_est_ = sim_.courant * estimate_dt();
+  dt_ = dt_est_;
+  if (sim_.step != 0) {  // Discretization.hpp:5476-5483
+    if (sim_.step > dt_) unstable_ = true;
+    else dt_ = sim_.step;
+  }
+  build_tables();
+  locate_probes_and_dipoles();
+  nsteps_ = 0;
+  while ((double)nsteps_ * dt_ <= sim_.duration) nsteps_++;  // Discretization.hpp:1840
+  // print schedule (Output::AllowPrint, Output.hpp:300-310)
+  slot_of_step_.assign(nsteps_, -1);
+  if (out_.mode == "probepoint") {
+    Output o = out_;
+    for (uint64_t i = 0; i < nsteps_; i++) {
+      double t = (double)i * dt_;
+      if (o.allow_print(t)) {
+        slot_of_step_[i] = nslots_++;
+        sample_times_.push_back(t);
+      }
+    }
+  }
+  alloc_device();
+  upload();
+}
+
+FitSim::~FitSim() {
+  if (pinned_) cudaFreeHost(pinned_);
+  if (graph_) cudaGraphExecDestroy(graph_);
+  for (void* p : allocs_) cudaFree(p);
+  if (ev0_) cudaEventDestroy(ev0_);
+  if (ev1_) cudaEventDestroy(ev1_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void FitSim::setup_grid() {
+  const Mesh& msh = sc_.meshes[sim_.mesh];
+  if (msh.type != "cartesian") throw std::invalid_argument("method fdtd needs a cartesian mesh");
+  for (auto& b : sc_.bcs)
+    if (b.second.type == "pml") throw UnsupportedError("PML boundary conditions are outside the supported path");
+  solids_ = read_solids(msh.file);
+  const double sc = msh.scale;
+  lo_[0] = sc * msh.xmin; lo_[1] = sc * msh.ymin; lo_[2] = sc * msh.zmin;
+  const double hi[3] = {sc * msh.xmax, sc * msh.ymax, sc * msh.zmax};
+  L_[0] = sc * msh.xstep; L_[1] = sc * msh.ystep; L_[2] = sc * msh.zstep;
+  int* N[3] = {&Nx_, &Ny_, &Nz_};
+  for (int a = 0; a < 3; a++) {
+    *N[a] = (int)(uint32_t)(std::fabs(hi[a] - lo_[a]) / L_[a]);  // Discretization.hpp:4557-4559
+    if (*N[a] < 1) throw std::invalid_argument("cartesian grid with no cells");
+    xs_[a].resize(*N[a] + 1);
+    xs_[a][0] = lo_[a];
+    for (int q = 0; q < *N[a]; q++) xs_[a][q + 1] = xs_[a][q] + L_[a];
+  }
+  sx_ = ((int64_t)Nx_ + 1 + 7) / 8 * 8;
+  sxy_ = sx_ * (Ny_ + 1);
+  nslot_ = sxy_ * (Nz_ + 1);
+  nE_ = (uint64_t)Nx_ * (Ny_ + 1) * (Nz_ + 1) + (uint64_t)(Nx_ + 1) * Ny_ * (Nz_ + 1) +
+        (uint64_t)(Nx_ + 1) * (Ny_ + 1) * Nz_;
+  nF_ = (uint64_t)Nx_ * Ny_ * (Nz_ + 1) + (uint64_t)Nx_ * (Ny_ + 1) * Nz_ + (uint64_t)(Nx_ + 1) * Ny_ * Nz_;
+  if (sc_.materials.empty()) throw std::invalid_argument("no material defined");
+  maxmat_ = sc_.materials.rbegin()->first;
+
+  // Cell materials: the first solid in label order whose rule holds at the
+  // cell centre (WhichSolid, Discretization.hpp:10110-10122).  Solids are
+  // visited in label order over their bounding boxes; a cell keeps the first
+  // match.
+  const size_t ncell = (size_t)Nx_ * Ny_ * Nz_;
+  std::vector<uint32_t> lab(ncell, 0);
+  std::vector<uint8_t> done(ncell, 0);
+  auto center = [&](int a, int q) { return xs_[a][q] + 0.5 * L_[a]; };
+  for (auto& kv : solids_) {
+    const Solid& s = kv.second;
+    double bmin[3], bmax[3];
+    if (s.type == "sphere") {
+      double r = std::sqrt(s.sqr);
+      for (int a = 0; a < 3; a++) { bmin[a] = s.center[a] - r; bmax[a] = s.center[a] + r; }
+    } else if (s.type == "box") {
+      for (int a = 0; a < 3; a++) { bmin[a] = s.corner[a]; bmax[a] = s.corner[a] + s.size[a]; }
+    } else if (s.type == "cylinder") {
+      double r = std::sqrt(s.sqr);
+      for (int a = 0; a < 3; a++) {
+        bmin[a] = std::fmin(s.center[a], s.center[a] + s.size[a]) - r;
+        bmax[a] = std::fmax(s.center[a], s.center[a] + s.size[a]) + r;
+      }
+    } else {
+      continue;
+    }
+    int q0[3], q1[3];
+    for (int a = 0; a < 3; a++) {
+      const int Na = a == 0 ? Nx_ : (a == 1 ? Ny_ : Nz_);
+      double f0 = (bmin[a] - lo_[a]) / L_[a] - 2.0, f1 = (bmax[a] - lo_[a]) / L_[a] + 2.0;
+      q0[a] = f0 < 0 ? 0 : (f0 > Na - 1 ? Na : (int)f0);
+      q1[a] = f1 > Na - 1 ? Na - 1 : (f1 < 0 ? -1 : (int)f1);
+    }
+    for (int k = q0[2]; k <= q1[2]; k++)
+      for (int j = q0[1]; j <= q1[1]; j++)
+        for (int i = q0[0]; i <= q1[0]; i++) {
+          size_t c = (size_t)i + (size_t)Nx_ * ((size_t)j + (size_t)Ny_ * k);
+          if (done[c]) continue;
+          if (s.rule(center(0, i), center(1, j), center(2, k))) {
+            lab[c] = s.material;
+            done[c] = 1;
+          }
+        }
+  }
+  // compact material indices
+  std::vector<uint32_t> used;
+  {
+    std::vector<uint8_t> seen;
+    for (size_t c = 0; c < ncell; c++) {
+      uint32_t l = lab[c];
+      if (l > maxmat_) throw std::invalid_argument("solid material " + std::to_string(l) + " is not defined");
+      if (l >= seen.size()) seen.resize(l + 1, 0);
+      seen[l] = 1;
+    }
+    for (uint32_t l = 0; l < seen.size(); l++)
+      if (seen[l]) used.push_back(l);
+  }
+  if (used.size() > 256) throw UnsupportedError("more than 256 distinct materials in one cartesian grid");
+  std::vector<int> idx(maxmat_ + 1, -1);
+  for (size_t q = 0; q < used.size(); q++) idx[used[q]] = (int)q;
+  mat_label_ = used;
+  mat_.resize(ncell);
+  for (size_t c = 0; c < ncell; c++) mat_[c] = (uint8_t)idx[lab[c]];
+}
+
+// material-pair label of an interior face (Discretization.hpp:330-347)
+static uint64_t pair_label(uint32_t a, uint32_t b, uint32_t M) {
+  if (a == b) return 0;
+  if (a > b) std::swap(a, b);
+  return 6 + (uint64_t)a * M - (uint64_t)a * (a - 1) / 2 + (b - a);
+}
+
+namespace {
+struct EdgeFaces {
+  int n = 0;
+  FaceRef f[4];
+};
+}  // namespace
+
+// The faces of edge (axis a, node i,j,k) in the order the reference lists them
+// in Ct_vec: faces sorted by (creating cube, slot in that cube), with the
+// right-handed circulation sign of the edge in each face.
+static EdgeFaces faces_of_edge(int a, int i, int j, int k, int Nx, int Ny, int Nz) {
+  EdgeFaces ef;
+  const int N[3] = {Nx, Ny, Nz};
+  const int e[3] = {i, j, k};
+  struct Key { int64_t cube; int slot; FaceRef fr; };
+  Key keys[4];
+  int nk = 0;
+  for (int n = 0; n < 3; n++) {
+    if (n == a) continue;
+    const int m = 3 - a - n;        // the other in-face axis
+    for (int d = 0; d < 2; d++) {   // face at m-index e[m]-1 (edge on its high side) or e[m]
+      int fi[3] = {e[0], e[1], e[2]};
+      fi[m] = e[m] - 1 + d;
+      if (fi[m] < 0 || fi[m] >= N[m]) continue;
+      // face exists; its sign: basis (u,v) = the two in-face axes, u < v;
+      // orientation +1 when u x v = +n, i.e. cyclic (n, u, v)
+      const int u = std::min(a, m), v = std::max(a, m);
+      const int cyc = ((u == (n + 1) % 3) && (v == (n + 2) % 3)) ? 1 : -1;
+      int sgn;
+      if (a == u) sgn = (d == 1) ? 1 : -1;   // u-edge at v-low (face index == edge index) -> +
+      else sgn = (d == 1) ? -1 : 1;          // v-edge at u-low -> -, at u-high -> +
+      sgn *= cyc;
+      // creating cube: lower cell along n if it exists, else the upper one
+      int ci[3] = {fi[0], fi[1], fi[2]};
+      int slot;
+      if (fi[n] > 0) { ci[n] = fi[n] - 1; slot = kFaceSlotHigh[n]; }
+      else { slot = kFaceSlotLow[n]; }
+      if (fi[n] > N[n]) continue;
+      int64_t cube = (int64_t)ci[0] + (int64_t)Nx * ((int64_t)ci[1] + (int64_t)Ny * ci[2]);
+      keys[nk++] = {cube, slot, {n, fi[0], fi[1], fi[2], sgn}};
+    }
+  }
+  std::sort(keys, keys + nk, [](const Key& x, const Key& y) {
+    return x.cube != y.cube ? x.cube < y.cube : x.slot < y.slot;
+  });
+  ef.n = nk;
+  for (int q = 0; q < nk; q++) ef.f[q] = keys[q].fr;
+  return ef;
+}
+
+void FitSim::classify_edges() {
+  // Edge classes of Discretization.hpp:5391-5468: PEC faces win, then the
+  // first source type met (face order, then source label order) decides.
+  auto pec_label = [&](uint64_t L) {
+    if (L == 0 || L >= 100) return false;
+    auto it = sc_.bcs.find(sc_.bnd_to_bc[L]);
+    return it != sc_.bcs.end() && it->second.type == "pec";
+  };
+  std::vector<uint64_t> active;  // labels that carry a BC or a source
+  for (uint64_t L = 1; L < 100; L++)
+    if (pec_label(L)) active.push_back(L);
+  for (uint32_t sl : src_labels_)
+    for (uint32_t L : sc_.sources[sl].surfaces) active.push_back(L);
+  bool interface_active = false;
+  for (uint64_t L : active)
+    if (L > 6) interface_active = true;
+
+  auto cell_label = [&](int i, int j, int k) {
+    return mat_label_[mat_[(size_t)i + (size_t)Nx_ * ((size_t)j + (size_t)Ny_ * k)]];
+  };
+  const int N[3] = {Nx_, Ny_, Nz_};
+  auto face_label = [&](const FaceRef& f) -> uint64_t {
+    const int p = f.n == 0 ? f.i : (f.n == 1 ? f.j : f.k);
+    if (p == 0) return kLabelLow[f.n];
+    if (p == N[f.n]) return kLabelHigh[f.n];
+    int li = f.i - (f.n == 0), lj = f.j - (f.n == 1), lk = f.k - (f.n == 2);
+    return pair_label(cell_label(li, lj, lk), cell_label(f.i, f.j, f.k), maxmat_);
+  };
+  auto slot_of = [&](int i, int j, int k) { return (int64_t)i + sx_ * j + sxy_ * k; };
+
+  auto classify = [&](int a, int i, int j, int k, bool interior) {
+    EdgeFaces ef = faces_of_edge(a, i, j, k, Nx_, Ny_, Nz_);
+    uint64_t lab[4];
+    bool pec = false;
+    for (int q = 0; q < ef.n; q++) {
+      lab[q] = face_label(ef.f[q]);
+      if (pec_label(lab[q])) pec = true;
+    }
+    HostSpecial hs;
+    hs.comp = a;
+    hs.slot = slot_of(i, j, k);
+    if (pec) {
+      if (!interior) return;  // never written: holds 0
+      hs.op = 0; hs.kind = 0;
+      special_.push_back(hs);
+      return;
+    }
+    int in_b = 0, brk = 0;
+    std::vector<uint32_t> esrc;
+    for (int q = 0; q < ef.n; q++) {
+      if (lab[q] == 0) continue;
+      for (uint32_t sl : src_labels_) {
+        Source& s = sc_.sources[sl];
+        if (std::find(s.surfaces.begin(), s.surfaces.end(), (uint32_t)lab[q]) == s.surfaces.end()) continue;
+        in_b++;
+        if (s.st == "e") {
+          if (brk == 2) break;
+          if (std::find(esrc.begin(), esrc.end(), sl) == esrc.end()) { esrc.push_back(sl); brk = 1; }
+        } else if (s.st == "h") {
+          if (brk == 1) break;
+          if (std::find(esrc.begin(), esrc.end(), sl) == esrc.end()) { esrc.push_back(sl); brk = 2; }
+        }
+      }
+    }
+    if (!esrc.empty()) {  // source consistency filter (Discretization.hpp:5576-5589)
+      const Source& f = sc_.sources[esrc[0]];
+      uint32_t fs = f.surfaces.empty() ? 0 : f.surfaces[0];
+      std::vector<uint32_t> keep;
+      for (uint32_t s : esrc) {
+        const Source& x = sc_.sources[s];
+        if (x.st == f.st && (x.surfaces.empty() ? 0 : x.surfaces[0]) == fs) keep.push_back(s);
+      }
+      esrc = keep;
+    }
+    if (in_b == 0) {
+      if (ef.n == 4) return;  // interior stencil
+      hs.op = 1; hs.kind = 0;  // natural boundary edge
+    } else if (esrc.empty()) {
+      if (!interior) return;   // never written
+      hs.op = 0; hs.kind = 0;
+    } else if (sc_.sources[esrc[0]].st == "e") {
+      hs.op = 0; hs.kind = 1;
+    } else {
+      hs.op = 1; hs.kind = 2;
+    }
+    hs.srcs = esrc;
+    if (hs.op == 1) {
+      hs.nface = ef.n;
+      for (int q = 0; q < ef.n; q++) {
+        hs.fcomp[q] = ef.f[q].n;
+        hs.fslot[q] = slot_of(ef.f[q].i, ef.f[q].j, ef.f[q].k);
+        hs.fsign[q] = ef.f[q].sign;
+      }
+    }
+    special_.push_back(hs);
+  };
+
+  // domain-surface edges
+  for (int a = 0; a < 3; a++) {
+    const int b = (a + 1) % 3, c = (a + 2) % 3;
+    for (int ka = 0; ka < N[a]; ka++)
+      for (int kb = 0; kb <= N[b]; kb++)
+        for (int kc = 0; kc <= N[c]; kc++) {
+          bool surf = kb == 0 || kb == N[b] || kc == 0 || kc == N[c];
+          if (!surf) continue;
+          int e[3];
+          e[a] = ka; e[b] = kb; e[c] = kc;
+          classify(a, e[0], e[1], e[2], false);
+        }
+  }
+  // interface edges, only when a BC or source names an interface label
+  if (interface_active) {
+    for (int a = 0; a < 3; a++) {
+      const int b = (a + 1) % 3, c = (a + 2) % 3;
+      for (int ka = 0; ka < N[a]; ka++)
+        for (int kb = 1; kb < N[b]; kb++)
+          for (int kc = 1; kc < N[c]; kc++) {
+            int e[3];
+            e[a] = ka; e[b] = kb; e[c] = kc;
+            // cells around the edge: an interface edge has two different materials
+            int ci[3] = {e[0], e[1], e[2]};
+            uint32_t first = 0;
+            bool mixed = false;
+            for (int q = 0; q < 4; q++) {
+              ci[b] = e[b] - 1 + (q & 1);
+              ci[c] = e[c] - 1 + (q >> 1);
+              uint32_t l = cell_label(ci[0], ci[1], ci[2]);
+              if (q == 0) first = l;
+              else if (l != first) mixed = true;
+            }
+            if (mixed) classify(a, e[0], e[1], e[2], true);
+          }
+    }
+  }
+}
+
+// Per-material tables, special-edge coefficients and geometric source data.
+void FitSim::build_tables() {
+  const size_t nm = mat_label_.size();
+  const double da[3] = {L_[1] * L_[2] / 4, L_[0] * L_[2] / 4, L_[0] * L_[1] / 4};
+  const double area[3] = {L_[1] * L_[2], L_[0] * L_[2], L_[0] * L_[1]};
+  P_.assign(3 * nm, 0); S_.assign(3 * nm, 0); R_.assign(3 * nm, 0); X_.assign(3 * nm, 0);
+  mh_pure_.assign(3 * nm, 0); mq_pure_.assign(3 * nm, 0); mnu_pure_.assign(3 * nm, 0); mmu_pure_.assign(3 * nm, 0);
+  inv_mu_.assign(3 * nm, 0);
+  live_.assign(nm, 0);
+  for (size_t m = 0; m < nm; m++) {
+    const Material& mt = sc_.materials[mat_label_[m]];  // default material when undefined
+    live_[m] = mat_label_[m] != 0;
+    for (int a = 0; a < 3; a++) {
+      P_[3 * m + a] = mt.eps.m[a][a] != 0 ? da[a] * mt.eps.m[a][a] : 0.0;
+      S_[3 * m + a] = mt.sigma.m[a][a] != 0 ? da[a] * mt.sigma.m[a][a] : 0.0;
+      R_[3 * m + a] = mt.mu.m[a][a] != 0 ? L_[a] / 2 / mt.mu.m[a][a] : 0.0;
+      X_[3 * m + a] = mt.chi.m[a][a] != 0 ? L_[a] / 2 / mt.chi.m[a][a] : 0.0;
+      inv_mu_[3 * m + a] = 1.0 / mt.mu.m[a][a];
+    }
+  }
+  auto edge_coef = [&](int a, const int* ms, int n, double& mh, double& mq) {
+    double eps = 0, sig = 0;
+    bool lossy = false;
+    for (int q = 0; q < n; q++) {
+      eps += P_[3 * ms[q] + a];
+      if (S_[3 * ms[q] + a] != 0) { sig += S_[3 * ms[q] + a]; lossy = true; }
+    }
+    if (eps != 0) {
+      if (lossy) {
+        double hs = 0.5 * dt_ * sig;
+        mh = L_[a] / (eps + hs);
+        mq = (eps - hs) / L_[a];
+      } else {
+        mh = L_[a] / eps;
+        mq = eps / L_[a];
+      }
+    } else {
+      mh = mq = 0;
+    }
+  };
+  auto face_coef = [&](int a, const int* ms, int n, double& mnu, double& mmu) {
+    double ni = 0, msg = 0;
+    bool lossy = false;
+    for (int q = 0; q < n; q++) {
+      ni += R_[3 * ms[q] + a];
+      if (X_[3 * ms[q] + a] != 0) { msg += X_[3 * ms[q] + a]; lossy = true; }
+    }
+    if (ni != 0) {
+      if (lossy) {
+        double hd = 0.5 * dt_ / msg;
+        mnu = 1 / (area[a] * (1 / ni + hd));
+        mmu = area[a] * (1 / ni - hd);
+      } else {
+        mnu = ni / area[a];
+        mmu = area[a] / ni;
+      }
+    } else {
+      mnu = mmu = 0;
+    }
+  };
+  for (size_t m = 0; m < nm; m++)
+    for (int a = 0; a < 3; a++) {
+      int ms[4] = {(int)m, (int)m, (int)m, (int)m};
+      edge_coef(a, ms, 4, mh_pure_[3 * m + a], mq_pure_[3 * m + a]);
+      face_coef(a, ms, 2, mnu_pure_[3 * m + a], mmu_pure_[3 * m + a]);
+    }
+  // special edges: coefficients from the cells that exist, in sweep order
+  auto cell_m = [&](int i, int j, int k) { return (int)mat_[(size_t)i + (size_t)Nx_ * ((size_t)j + (size_t)Ny_ * k)]; };
+  const int N[3] = {Nx_, Ny_, Nz_};
+  for (auto& hs : special_) {
+    int a = hs.comp;
+    int64_t s = hs.slot;
+    int k = (int)(s / sxy_), j = (int)((s % sxy_) / sx_), i = (int)(s % sx_);
+    int e[3] = {i, j, k};
+    const int b = a == 0 ? 1 : 0, c = a == 2 ? 1 : 2;  // the two other axes, b < c
+    int ms[4], nmq = 0;
+    for (int qc = 0; qc < 2; qc++)       // sweep order: higher axis slowest
+      for (int qb = 0; qb < 2; qb++) {
+        int ci[3] = {e[0], e[1], e[2]};
+        ci[b] = e[b] - 1 + qb;
+        ci[c] = e[c] - 1 + qc;
+        if (ci[b] < 0 || ci[b] >= N[b] || ci[c] < 0 || ci[c] >= N[c]) continue;
+        ms[nmq++] = cell_m(ci[0], ci[1], ci[2]);
+      }
+    edge_coef(a, ms, nmq, hs.mh, hs.mq);
+  }
+}
+
+double FitSim::estimate_dt() {
+  // dt = 2 / sqrt(lambda_max(Einv C^T N C)) (Discretization.hpp:7036-7119),
+  // lambda_max by Lanczos on Einv^1/2 C^T N C Einv^1/2 over all edges/faces.
+  // The reference uses Spectra Arnoldi at tolerance 2e-2; `SET step` pins dt.
+  if (nE_ > (uint64_t)30000000) {
+    // Large grids: the uniform-medium Yee bound 1 / (c sqrt(sum 1/L^2)) of the
+    // fastest material present, which is 2/sqrt(lambda_max) for a uniform grid.
+    double best = 1e300;
+    for (size_t m = 0; m < mat_label_.size(); m++) {
+      const Material& mt = sc_.materials[mat_label_[m]];
+      double s = 0;
+      for (int a = 0; a < 3; a++) s += 1.0 / (L_[a] * L_[a] * mt.mu.m[a][a] * mt.eps.m[a][a]);
+      best = std::fmin(best, 1.0 / std::sqrt(s));
+    }
+    return best;
+  }
+  const int N[3] = {Nx_, Ny_, Nz_};
+  const size_t ncomp = (size_t)nslot_;
+  std::vector<double> H(3 * ncomp, 0.0), Nv(3 * ncomp, 0.0);
+  std::vector<uint8_t> valid(3 * ncomp, 0);
+  const double da[3] = {L_[1] * L_[2] / 4, L_[0] * L_[2] / 4, L_[0] * L_[1] / 4};
+  const double area[3] = {L_[1] * L_[2], L_[0] * L_[2], L_[0] * L_[1]};
+  auto cm = [&](int i, int j, int k) -> const Material& {
+    return sc_.materials[mat_label_[mat_[(size_t)i + (size_t)Nx_ * ((size_t)j + (size_t)Ny_ * k)]]];
+  };
+  for (int k = 0; k <= Nz_; k++)
+    for (int j = 0; j <= Ny_; j++)
+      for (int i = 0; i <= Nx_; i++) {
+        int e[3] = {i, j, k};
+        int64_t s = i + sx_ * j + sxy_ * k;
+        for (int a = 0; a < 3; a++) {
+          if (e[a] >= N[a]) continue;
+          int b = (a + 1) % 3, c = (a + 2) % 3;
+          if (e[b] > N[b] || e[c] > N[c]) continue;
+          double eps = 0;
+          for (int q = 0; q < 4; q++) {
+            int ci[3] = {e[0], e[1], e[2]};
+            ci[b] = e[b] - 1 + (q & 1);
+            ci[c] = e[c] - 1 + (q >> 1);
+            if (ci[b] < 0 || ci[b] >= N[b] || ci[c] < 0 || ci[c] >= N[c]) continue;
+            eps += da[a] * cm(ci[0], ci[1], ci[2]).eps.m[a][a];
+          }
+          valid[a * ncomp + s] = 1;
+          H[a * ncomp + s] = std::sqrt(L_[a] / eps);
+        }
+        for (int n = 0; n < 3; n++) {
+          int b = (n + 1) % 3, c = (n + 2) % 3;
+          if (e[n] > N[n] || e[b] >= N[b] || e[c] >= N[c]) continue;
+          double ni = 0;
+          if (e[n] > 0) {
+            int ci[3] = {e[0], e[1], e[2]};
+            ci[n]--;
+            ni += L_[n] / 2 / cm(ci[0], ci[1], ci[2]).mu.m[n][n];
+          }
+          if (e[n] < N[n]) ni += L_[n] / 2 / cm(e[0], e[1], e[2]).mu.m[n][n];
+          Nv[n * ncomp + s] = ni / area[n];
+        }
+      }
+  std::vector<double> tmp(3 * ncomp), Fb(3 * ncomp);
+  const int64_t st[3] = {1, sx_, sxy_};
+  auto apply = [&](const double* x, double* y) {
+    for (size_t q = 0; q < 3 * ncomp; q++) tmp[q] = H[q] * x[q];
+    // faces: circulation of the 4 edges (u at v-low +, v at u-high +, u at v-high -, v at u-low -)
+    for (int n = 0; n < 3; n++) {
+      int u = (n + 1) % 3, v = (n + 2) % 3;
+      for (size_t s = 0; s < ncomp; s++) {
+        int64_t ss = (int64_t)s;
+        int kk = (int)(ss / sxy_), jj = (int)((ss % sxy_) / sx_), ii = (int)(ss % sx_);
+        int e[3] = {ii, jj, kk};
+        if (e[n] > N[n] || e[u] >= N[u] || e[v] >= N[v]) { Fb[n * ncomp + s] = 0; continue; }
+        double val = tmp[u * ncomp + s] + tmp[v * ncomp + s + st[u]] - tmp[u * ncomp + s + st[v]] - tmp[v * ncomp + s];
+        Fb[n * ncomp + s] = Nv[n * ncomp + s] * val;
+      }
+    }
+    for (int a = 0; a < 3; a++) {
+      int b = (a + 1) % 3, c = (a + 2) % 3;  // faces with normal c hold the a-edge as their u (a==(c+1)%3)
+      for (size_t s = 0; s < ncomp; s++) {
+        if (!valid[a * ncomp + s]) { y[a * ncomp + s] = 0; continue; }
+        int64_t ss = (int64_t)s;
+        int kk = (int)(ss / sxy_), jj = (int)((ss % sxy_) / sx_), ii = (int)(ss % sx_);
+        int e[3] = {ii, jj, kk};
+        double acc = 0;
+        // normal c: a == (c+1)%3 is u  -> + at v-low (face v-index == e[b]), - at v-high (face at e[b]-1)
+        if (e[b] < N[b]) acc += Fb[c * ncomp + s];
+        if (e[b] > 0) acc -= Fb[c * ncomp + s - st[b]];
+        // normal b: a == (b+2)%3 is v -> + at u-high (face u-index == e[c]-1), - at u-low (face at e[c])
+        if (e[c] > 0) acc += Fb[b * ncomp + s - st[c]];
+        if (e[c] < N[c]) acc -= Fb[b * ncomp + s];
+        y[a * ncomp + s] = H[a * ncomp + s] * acc;
+      }
+    }
+  };
+  // Lanczos on the valid sub-space
+  std::vector<double> v(3 * ncomp, 0), w(3 * ncomp), vp(3 * ncomp, 0);
+  uint64_t rs = 0x9E3779B97F4A7C15ull;
+  double nrm = 0;
+  for (size_t q = 0; q < 3 * ncomp; q++) {
+    rs ^= rs << 13; rs ^= rs >> 7; rs ^= rs << 17;
+    v[q] = valid[q] ? (double)(rs >> 11) / 9007199254740992.0 - 0.5 : 0.0;
+    nrm += v[q] * v[q];
+  }
+  nrm = std::sqrt(nrm);
+  for (auto& x : v) x /= nrm;
+  std::vector<double> al, be;
+  double beta = 0, last = 0, lam = 0;
+  for (int it = 0; it < 300; it++) {
+    apply(v.data(), w.data());
+    double alpha = 0;
+    for (size_t q = 0; q < 3 * ncomp; q++) alpha += w[q] * v[q];
+    for (size_t q = 0; q < 3 * ncomp; q++) w[q] -= alpha * v[q] + beta * vp[q];
+    al.push_back(alpha);
+    double nb = 0;
+    for (size_t q = 0; q < 3 * ncomp; q++) nb += w[q] * w[q];
+    nb = std::sqrt(nb);
+    if (it % 10 == 9 || nb == 0 || it == 299) {
+      lam = tridiag_max(al, be);
+      if (nb == 0 || std::fabs(lam - last) <= 1e-9 * std::fabs(lam)) break;
+      last = lam;
+    }
+    be.push_back(nb);
+    beta = nb;
+    vp.swap(v);
+    for (size_t q = 0; q < 3 * ncomp; q++) v[q] = w[q] / nb;
+  }
+  return 2.0 / std::sqrt(lam);
+}
+
+void FitSim::locate_probes_and_dipoles() {
+  // FindFitProbe (Discretization.hpp:3590-3643): breadth-first from the last
+  // hit, neighbours in face-slot order z-, y-, x-, x+, y+, z+; cube 0 starts
+  // marked.  The first cube whose box (tolerance 1e-12) holds the point wins.
+  const size_t ncell = (size_t)Nx_ * Ny_ * Nz_;
+  std::vector<uint8_t> colour(ncell, 0);
+  std::vector<size_t> touched;
+  size_t root = 0;
+  auto find = [&](const std::array<double, 3>& pv) -> int64_t {
+    for (size_t t : touched) colour[t] = 0;
+    touched.clear();
+    std::vector<size_t> q;
+    q.push_back(root);
+    colour[0] = 1;
+    touched.push_back(0);
+    const double tol = 1e-12;
+    for (size_t h = 0; h < q.size(); h++) {
+      size_t v = q[h];
+      int i = (int)(v % Nx_), j = (int)((v / Nx_) % Ny_), k = (int)(v / ((size_t)Nx_ * Ny_));
+      double d0 = pv[0] - xs_[0][i], d1 = pv[1] - xs_[1][j], d2 = pv[2] - xs_[2][k];
+      if (d0 >= -tol && d0 < L_[0] + tol && d1 >= -tol && d1 < L_[1] + tol && d2 >= -tol && d2 < L_[2] + tol) {
+        root = v;
+        return (int64_t)v;
+      }
+      const int nb[6][3] = {{0, 0, -1}, {0, -1, 0}, {-1, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+      for (auto& d : nb) {
+        int ii = i + d[0], jj = j + d[1], kk = k + d[2];
+        size_t n;
+        if (ii < 0 || ii >= Nx_ || jj < 0 || jj >= Ny_ || kk < 0 || kk >= Nz_) n = v;  // boundary face
+        else n = (size_t)ii + (size_t)Nx_ * ((size_t)jj + (size_t)Ny_ * kk);
+        if (!colour[n]) {
+          q.push_back(n);
+          colour[n] = 1;
+          touched.push_back(n);
+        }
+      }
+      if (!colour[v]) { colour[v] = 1; touched.push_back(v); }
+    }
+    return -1;
+  };
+  if (out_.mode == "probepoint") {
+    for (auto& pv : out_.probes) {
+      int64_t v = find(pv);
+      if (v < 0) continue;
+      int i = (int)(v % Nx_), j = (int)((v / Nx_) % Ny_), k = (int)(v / ((int64_t)Nx_ * Ny_));
+      probe_cell_.push_back({i, j, k});
+      probe_pts_.push_back(pv);
+    }
+    // point dipoles (Discretization.hpp:466-502): nearest of the cube's 12 edges
+    std::unordered_map<int64_t, size_t> where;
+    for (size_t q = 0; q < special_.size(); q++) where[special_[q].slot * 4 + special_[q].comp] = q;
+    static const int kEdgeAxis[12] = {0, 1, 2, 1, 2, 0, 2, 2, 0, 1, 1, 0};
+    static const int kEdgeNode0[12] = {0, 0, 0, 1, 1, 2, 2, 3, 4, 4, 5, 6};
+    for (uint32_t sl : src_labels_) {
+      Source& s = sc_.sources[sl];
+      if (s.st != "j") continue;
+      int64_t v = find(s.location);
+      if (v < 0) continue;
+      int ci = (int)(v % Nx_), cj = (int)((v / Nx_) % Ny_), ck = (int)(v / ((int64_t)Nx_ * Ny_));
+      int best = -1;
+      double bd = 0;
+      for (int q = 0; q < 12; q++) {
+        int a = kEdgeAxis[q], n0 = kEdgeNode0[q];
+        int e[3] = {ci + (n0 & 1), cj + ((n0 >> 1) & 1), ck + ((n0 >> 2) & 1)};
+        double b[3];
+        for (int x = 0; x < 3; x++) {
+          double p0 = xs_[x][e[x]], p1 = x == a ? xs_[x][e[x] + 1] : p0;
+          b[x] = (p0 + p1) / 2;
+        }
+        double d = std::sqrt((b[0] - s.location[0]) * (b[0] - s.location[0]) +
+                             (b[1] - s.location[1]) * (b[1] - s.location[1]) +
+                             (b[2] - s.location[2]) * (b[2] - s.location[2]));
+        if (best < 0 || d < bd) { bd = d; best = q; }
+      }
+      int a = kEdgeAxis[best], n0 = kEdgeNode0[best];
+      int e[3] = {ci + (n0 & 1), cj + ((n0 >> 1) & 1), ck + ((n0 >> 2) & 1)};
+      int64_t slot = e[0] + sx_ * e[1] + sxy_ * e[2];
+      auto it = where.find(slot * 4 + a);
+      EdgeFaces ef = faces_of_edge(a, e[0], e[1], e[2], Nx_, Ny_, Nz_);
+      if (it == where.end()) {
+        // edge not special: a 4-face interior edge (common), or a PEC / frozen
+        // boundary edge whose value stays 0
+        if (ef.n != 4) continue;
+        bool on_surface = false;
+        for (int x = 0; x < 3; x++)
+          if (x != a && (e[x] == 0 || e[x] == (x == 0 ? Nx_ : (x == 1 ? Ny_ : Nz_)))) on_surface = true;
+        if (on_surface) continue;
+        HostSpecial hs;
+        hs.comp = a; hs.slot = slot; hs.op = 2; hs.kind = 3;
+        hs.nface = 4;
+        for (int q = 0; q < 4; q++) {
+          hs.fcomp[q] = ef.f[q].n;
+          hs.fslot[q] = ef.f[q].i + sx_ * ef.f[q].j + sxy_ * ef.f[q].k;
+        }
+        hs.fsign[0] = a == 1 ? -1 : 1;  // dual curl sign of the edge axis
+        hs.srcs.push_back(sl);
+        // coefficients of a common edge
+        const int b = a == 0 ? 1 : 0, c = a == 2 ? 1 : 2;
+        int ms[4], nmq = 0;
+        for (int qc = 0; qc < 2; qc++)
+          for (int qb = 0; qb < 2; qb++) {
+            int cc[3] = {e[0], e[1], e[2]};
+            cc[b] = e[b] - 1 + qb;
+            cc[c] = e[c] - 1 + qc;
+            ms[nmq++] = mat_[(size_t)cc[0] + (size_t)Nx_ * ((size_t)cc[1] + (size_t)Ny_ * cc[2])];
+          }
+        double eps = 0, sig = 0;
+        bool lossy = false;
+        for (int q = 0; q < 4; q++) {
+          eps += P_[3 * ms[q] + a];
+          if (S_[3 * ms[q] + a] != 0) { sig += S_[3 * ms[q] + a]; lossy = true; }
+        }
+        if (eps != 0) {
+          if (lossy) { double hsg = 0.5 * dt_ * sig; hs.mh = L_[a] / (eps + hsg); hs.mq = (eps - hsg) / L_[a]; }
+          else { hs.mh = L_[a] / eps; hs.mq = eps / L_[a]; }
+        }
+        where[slot * 4 + a] = special_.size();
+        special_.push_back(hs);
+      } else {
+        HostSpecial& hs = special_[it->second];
+        if (hs.kind == 3) hs.srcs.push_back(sl);                         // second dipole on the edge
+        else if (hs.srcs.empty() && hs.op == 1) { hs.kind = 3; hs.srcs.push_back(sl); }  // natural edge
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ device
+template <typename T>
+void FitSim::fill_grid(FitGrid<T>& g, SpecialEdges<T>& s) {
+  g.Ux = (T*)dU_[0]; g.Uy = (T*)dU_[1]; g.Uz = (T*)dU_[2];
+  g.Fx = (T*)dF_[0]; g.Fy = (T*)dF_[1]; g.Fz = (T*)dF_[2];
+  g.mat = dmat_;
+  g.Nx = Nx_; g.Ny = Ny_; g.Nz = Nz_;
+  g.sx = sx_; g.sxy = sxy_;
+  g.dt = dt_;
+  g.P = dP_; g.S = dS_; g.R = dR_; g.X = dX_;
+  g.mh_pure = (const T*)dmh_; g.mq_pure = (const T*)dmq_; g.mnu_pure = (const T*)dmnu_; g.mmu_pure = (const T*)dmmu_;
+  g.live = dlive_;
+  for (int a = 0; a < 3; a++) g.len[a] = L_[a];
+  g.area[0] = L_[1] * L_[2]; g.area[1] = L_[0] * L_[2]; g.area[2] = L_[0] * L_[1];
+  s.n = (int)special_.size();
+  s.slot = dsp_slot_; s.comp = dsp_comp_; s.op = dsp_op_; s.nface = dsp_nface_; s.fcomp = dsp_fcomp_;
+  s.fslot = dsp_fslot_; s.fsign = dsp_fsign_; s.mh = dsp_mh_; s.mq = dsp_mq_;
+  s.src_begin = dsp_begin_; s.pair_src = dsp_psrc_; s.pair_fac = dsp_pfac_; s.pair_vec = dsp_vec_; s.post = dsp_post_;
+  s.pair_dir = dsp_pdir_; s.src_amp = dsrc_amp_; s.carrier = dcarrier_; s.src_kind = dsrc_kind_;
+  s.nsrc = (int)src_labels_.size();
+  s.out = (T*)dsp_out_;
+  s.flux_part = dflux_part_;
+}
+
+void FitSim::alloc_device() {
+  CU(cudaSetDevice(opt_.device));
+  int major = 0;
+  CU(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, opt_.device));
+  if (major != 10) throw CudaError("device " + std::to_string(opt_.device) + " is not an sm_100 (B200) GPU");
+  CU(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  CU(cudaEventCreate(&ev0_));
+  CU(cudaEventCreate(&ev1_));
+  const size_t es = opt_.precision == 1 ? sizeof(float) : sizeof(double);
+  auto dalloc = [&](size_t bytes) -> void* {
+    void* p = nullptr;
+    if (bytes == 0) bytes = 16;
+    CU(cudaMalloc(&p, bytes));
+    allocs_.push_back(p);
+    dev_bytes_ += bytes;
+    return p;
+  };
+  for (int a = 0; a < 3; a++) {
+    dU_[a] = dalloc(nslot_ * es);
+    dF_[a] = dalloc(nslot_ * es);
+    CU(cudaMemsetAsync(dU_[a], 0, nslot_ * es, stream_));
+    CU(cudaMemsetAsync(dF_[a], 0, nslot_ * es, stream_));
+  }
+  dmat_ = (uint8_t*)dalloc(mat_.size());
+  const size_t nm3 = 3 * mat_label_.size();
+  dP_ = (double*)dalloc(nm3 * 8); dS_ = (double*)dalloc(nm3 * 8);
+  dR_ = (double*)dalloc(nm3 * 8); dX_ = (double*)dalloc(nm3 * 8);
+  dmh_ = dalloc(nm3 * es); dmq_ = dalloc(nm3 * es); dmnu_ = dalloc(nm3 * es); dmmu_ = dalloc(nm3 * es);
+  dlive_ = (uint8_t*)dalloc(mat_label_.size());
+  dstep_ = (int*)dalloc(sizeof(int));
+  dflux_ = (double*)dalloc(nsteps_ * 8);
+  const size_t ns = special_.size();
+  nflux_part_ = (int)((ns + 255) / 256);
+  dflux_part_ = (double*)dalloc((nflux_part_ + 1) * 8);
+  dsp_slot_ = (int64_t*)dalloc(ns * 8); dsp_comp_ = (int8_t*)dalloc(ns); dsp_op_ = (int8_t*)dalloc(ns);
+  dsp_nface_ = (int8_t*)dalloc(ns); dsp_fcomp_ = (int8_t*)dalloc(4 * ns); dsp_fsign_ = (int8_t*)dalloc(4 * ns);
+  dsp_fslot_ = (int64_t*)dalloc(4 * ns * 8); dsp_mh_ = (double*)dalloc(ns * 8); dsp_mq_ = (double*)dalloc(ns * 8);
+  dsp_vec_ = (double*)dalloc(3 * ns * 8); dsp_post_ = (double*)dalloc(ns * 8);
+  dsp_begin_ = (int*)dalloc((ns + 1) * 4);
+  size_t npairs = 0;
+  for (auto& h : special_) npairs += h.srcs.size();
+  dsp_psrc_ = (int*)dalloc(npairs * 4); dsp_pfac_ = (double*)dalloc(4 * npairs * 8); dsp_pdir_ = (int8_t*)dalloc(npairs);
+  const size_t nsrc = src_labels_.size();
+  dsrc_amp_ = (double*)dalloc(nsrc * 8); dsrc_kind_ = (int8_t*)dalloc(nsrc);
+  dcarrier_ = (double*)dalloc(nsteps_ * nsrc * 8);
+  dsp_out_ = dalloc(ns * es);
+  const size_t np = probe_cell_.size();
+  dpi_ = (int*)dalloc(np * 4); dpj_ = (int*)dalloc(np * 4); dpk_ = (int*)dalloc(np * 4);
+  dinvmu_ = (double*)dalloc(3 * np * 8);
+  dslot_ = (int*)dalloc(nsteps_ * 4);
+  dsamples_ = (double*)dalloc((size_t)nslots_ * np * 6 * 8);
+}
+
+// geometry helpers for the dual edge of a boundary H-source edge
+void FitSim::upload() {
+  const size_t es = opt_.precision == 1 ? sizeof(float) : sizeof(double);
+  auto put = [&](void* d, const void* h, size_t b) {
+    if (b) CU(cudaMemcpyAsync(d, h, b, cudaMemcpyHostToDevice, stream_));
+  };
+  auto conv = [&](const std::vector<double>& v) {
+    std::vector<char> buf(v.size() * es);
+    if (es == 8) std::memcpy(buf.data(), v.data(), v.size() * 8);
+    else for (size_t q = 0; q < v.size(); q++) ((float*)buf.data())[q] = (float)v[q];
+    return buf;
+  };
+  put(dmat_, mat_.data(), mat_.size());
+  put(dP_, P_.data(), P_.size() * 8); put(dS_, S_.data(), S_.size() * 8);
+  put(dR_, R_.data(), R_.size() * 8); put(dX_, X_.data(), X_.size() * 8);
+  auto b1 = conv(mh_pure_), b2 = conv(mq_pure_), b3 = conv(mnu_pure_), b4 = conv(mmu_pure_);
+  put(dmh_, b1.data(), b1.size()); put(dmq_, b2.data(), b2.size());
+  put(dmnu_, b3.data(), b3.size()); put(dmmu_, b4.data(), b4.size());
+  put(dlive_, live_.data(), live_.size());
+  CU(cudaMemsetAsync(dstep_, 0, sizeof(int), stream_));
+  CU(cudaMemsetAsync(dflux_, 0, nsteps_ * 8, stream_));
+
+  // sources: amplitude, kind and the carrier table (Source.hpp:313-325)
+  const size_t nsrc = src_labels_.size();
+  std::vector<double> amp(nsrc), carrier(nsteps_ * nsrc, 0.0);
+  std::vector<int8_t> kind(nsrc, -1);
+  for (size_t q = 0; q < nsrc; q++) {
+    const Source& s = sc_.sources[src_labels_[q]];
+    amp[q] = s.st == "j" ? s.amp * s.impedance : s.amp;
+    kind[q] = s.st == "e" ? 0 : (s.st == "h" ? 1 : (s.st == "j" ? 2 : -1));
+    for (uint64_t i = 0; i < nsteps_; i++) {
+      double t = (double)i * dt_;
+      if (s.st == "h") t = t - 0.5 * dt_;  // ComputeHfieldSource at t - dt/2 (Discretization.hpp:1882)
+      double c = 0.0;
+      if (t >= 0) {
+        if (s.carrier == "sin") c = std::sin((double)(2 * PI_L * s.freq * (t - s.delay)));
+        else if (s.carrier == "cos") c = s.amp * std::cos((double)(2 * PI_L * s.freq * (t - s.delay)));
+        else if (s.carrier == "gaussian") c = std::exp(-std::pow(t - s.delay, 2) / std::pow(s.width, 2));
+        else if (s.carrier == "ricker") {
+          double a = (double)(PI_L * s.freq * (t - s.delay));
+          c = (1 - 2 * std::pow(a, 2)) * std::exp(-std::pow(a, 2));
+        } else c = 1.0;
+      }
+      carrier[i * nsrc + q] = c;
+    }
+  }
+  put(dsrc_amp_, amp.data(), nsrc * 8); put(dsrc_kind_, kind.data(), nsrc);
+  put(dcarrier_, carrier.data(), carrier.size() * 8);
+
+  // special edges
+  const size_t ns = special_.size();
+  std::vector<int64_t> slot(ns), fslot(4 * ns);
+  std::vector<int8_t> comp(ns), op(ns), nface(ns), fcomp(4 * ns), fsign(4 * ns);
+  std::vector<double> mh(ns), mq(ns), vec(3 * ns, 0.0), post(ns, 1.0);
+  std::vector<int> begin(ns + 1, 0), psrc;
+  std::vector<double> pfac;
+  std::vector<int8_t> pdir;
+  std::vector<int> srcidx(1, 0);
+  auto src_index = [&](uint32_t l) {
+    for (size_t q = 0; q < nsrc; q++)
+      if (src_labels_[q] == l) return (int)q;
+    return -1;
+  };
+  const int N[3] = {Nx_, Ny_, Nz_};
+  for (size_t e = 0; e < ns; e++) {
+    const HostSpecial& h = special_[e];
+    slot[e] = h.slot; comp[e] = (int8_t)h.comp; op[e] = (int8_t)h.op; nface[e] = (int8_t)h.nface;
+    for (int q = 0; q < 4; q++) { fcomp[4 * e + q] = (int8_t)h.fcomp[q]; fslot[4 * e + q] = h.fslot[q]; fsign[4 * e + q] = (int8_t)h.fsign[q]; }
+    mh[e] = h.mh; mq[e] = h.mq;
+    begin[e] = (int)psrc.size();
+    const int a = h.comp;
+    int k = (int)(h.slot / sxy_), j = (int)((h.slot % sxy_) / sx_), i = (int)(h.slot % sx_);
+    int ei[3] = {i, j, k};
+    double p0[3], p1[3], eb[3];
+    for (int x = 0; x < 3; x++) {
+      p0[x] = xs_[x][ei[x]];
+      p1[x] = x == a ? xs_[x][ei[x] + 1] : p0[x];
+      eb[x] = (p0[x] + p1[x]) / 2;  // edge barycenter (Discretization.hpp:10528-10540)
+    }
+    double ev[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+    if (h.kind == 1 || h.kind == 3) {
+      for (int x = 0; x < 3; x++) vec[3 * e + x] = ev[x];
+      if (h.kind == 3) post[e] = 1.0 / std::sqrt(ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2]);
+    } else if (h.kind == 2) {
+      // dual edge on the boundary, built as ComputeHfieldSource does lazily
+      // (Discretization.hpp:4150-4196)
+      EdgeFaces ef = faces_of_edge(a, i, j, k, Nx_, Ny_, Nz_);
+      auto face_bar = [&](const FaceRef& f, double* out) {
+        // sum over the face's 4 edges (reference C_vec order), 0.5 x each node, / 4
+        const int n = f.n, u = n == 0 ? 1 : 0, v = n == 2 ? 1 : 2;
+        int fi[3] = {f.i, f.j, f.k};
+        // edges: u-edge at v-low, v-edge at u-low, v-edge at u-high, u-edge at v-high
+        int ed[4][3];  // {axis, du, dv}
+        int tab[4][3] = {{u, 0, 0}, {v, 0, 0}, {v, 1, 0}, {u, 0, 1}};
+        std::memcpy(ed, tab, sizeof(tab));
+        double bc[3] = {0, 0, 0};
+        for (int r = 0; r < 4; r++) {
+          int ax = ed[r][0];
+          int base[3] = {fi[0], fi[1], fi[2]};
+          if (ax == v) base[u] += ed[r][1];
+          else base[v] += ed[r][2];
+          for (int nd = 0; nd < 2; nd++) {
+            int pt[3] = {base[0], base[1], base[2]};
+            if (nd) pt[ax]++;
+            for (int x = 0; x < 3; x++) bc[x] += 0.5 * xs_[x][pt[x]];
+          }
+        }
+        for (int x = 0; x < 3; x++) out[x] = bc[x] / 4;
+      };
+      auto flabel = [&](const FaceRef& f) -> uint64_t {
+        const int p = f.n == 0 ? f.i : (f.n == 1 ? f.j : f.k);
+        if (p == 0) return kLabelLow[f.n];
+        if (p == N[f.n]) return kLabelHigh[f.n];
+        auto cl = [&](int ii, int jj, int kk) {
+          return mat_label_[mat_[(size_t)ii + (size_t)Nx_ * ((size_t)jj + (size_t)Ny_ * kk)]];
+        };
+        return pair_label(cl(f.i - (f.n == 0), f.j - (f.n == 1), f.k - (f.n == 2)), cl(f.i, f.j, f.k), maxmat_);
+      };
+      double bd[3] = {0, 0, 0}, vb[3] = {0, 0, 0}, backup[3] = {0, 0, 0};
+      int nfb = 0, ni = 0;
+      for (int q = 0; q < ef.n; q++) {
+        double fb[3];
+        face_bar(ef.f[q], fb);
+        if (flabel(ef.f[q]) > 0) {
+          ++nfb;
+          // first cell of the face (the creating cube): lower along n if it exists
+          int ci[3] = {ef.f[q].i, ef.f[q].j, ef.f[q].k};
+          const int n = ef.f[q].n;
+          if (ci[n] > 0) ci[n]--;
+          double vbar[3] = {0, 0, 0};
+          for (int c = 0; c < 8; c++) {
+            int pt[3] = {ci[0] + (c & 1), ci[1] + ((c >> 1) & 1), ci[2] + ((c >> 2) & 1)};
+            for (int x = 0; x < 3; x++) vbar[x] += xs_[x][pt[x]];
+          }
+          for (int x = 0; x < 3; x++) backup[x] = vbar[x] / 8 - eb[x];
+          if (nfb == 1) for (int x = 0; x < 3; x++) bd[x] = fb[x];
+          else if (nfb == 2) for (int x = 0; x < 3; x++) bd[x] = fb[x] - bd[x];
+        } else {
+          for (int x = 0; x < 3; x++) vb[x] = fb[x] - eb[x];
+          ni++;
+        }
+      }
+      if (!ni) for (int x = 0; x < 3; x++) vb[x] = backup[x];
+      double cr[3] = {ev[1] * bd[2] - ev[2] * bd[1], ev[2] * bd[0] - ev[0] * bd[2], ev[0] * bd[1] - ev[1] * bd[0]};
+      if (cr[0] * vb[0] + cr[1] * vb[1] + cr[2] * vb[2] < 0)
+        for (int x = 0; x < 3; x++) bd[x] = -bd[x];
+      for (int x = 0; x < 3; x++) vec[3 * e + x] = bd[x];
+    }
+    for (uint32_t sl : h.srcs) {
+      const Source& s = sc_.sources[sl];
+      int si = src_index(sl);
+      if (si < 0) continue;
+      // spatial factors in the order Source::Compute applies them
+      double f[4] = {1.0, 1.0, 1.0, 1.0};
+      if (s.decay != 0)
+        f[0] = std::pow(std::pow(eb[0] - s.center[0], 2) + std::pow(eb[1] - s.center[1], 2) +
+                            std::pow(eb[2] - s.center[2], 2),
+                        -0.5 * s.decay);
+      if (s.prof == "gaussian") {
+        double ex = -((std::pow(eb[0] - s.center[0], 2) + std::pow(eb[1] - s.center[1], 2) +
+                       std::pow(eb[2] - s.center[2], 2)) /
+                      std::pow(s.radius, 2));
+        f[1] = std::exp(ex);
+      } else if (s.prof == "wave") {
+        for (int x = 0; x < 3; x++) {
+          if (s.bfuncs[x] == "sin") f[1 + x] = std::sin((double)(2 * PI_L * s.kvec[x] * (eb[x] - s.center[x])));
+          else if (s.bfuncs[x] == "cos") f[1 + x] = std::cos((double)(2 * PI_L * s.kvec[x] * (eb[x] - s.center[x])));
+        }
+      }
+      psrc.push_back(si);
+      for (int q = 0; q < 4; q++) pfac.push_back(f[q]);
+      pdir.push_back((int8_t)(s.dir == "x" ? 0 : (s.dir == "y" ? 1 : 2)));
+    }
+  }
+  begin[ns] = (int)psrc.size();
+  put(dsp_slot_, slot.data(), ns * 8); put(dsp_comp_, comp.data(), ns); put(dsp_op_, op.data(), ns);
+  put(dsp_nface_, nface.data(), ns); put(dsp_fcomp_, fcomp.data(), 4 * ns); put(dsp_fsign_, fsign.data(), 4 * ns);
+  put(dsp_fslot_, fslot.data(), 4 * ns * 8); put(dsp_mh_, mh.data(), ns * 8); put(dsp_mq_, mq.data(), ns * 8);
+  put(dsp_vec_, vec.data(), 3 * ns * 8); put(dsp_post_, post.data(), ns * 8);
+  put(dsp_begin_, begin.data(), (ns + 1) * 4);
+  put(dsp_psrc_, psrc.data(), psrc.size() * 4); put(dsp_pfac_, pfac.data(), pfac.size() * 8);
+  put(dsp_pdir_, pdir.data(), pdir.size());
+  // probes
+  const size_t np = probe_cell_.size();
+  std::vector<int> pi(np), pj(np), pk(np);
+  std::vector<double> im(3 * np);
+  for (size_t p = 0; p < np; p++) {
+    pi[p] = probe_cell_[p][0]; pj[p] = probe_cell_[p][1]; pk[p] = probe_cell_[p][2];
+    size_t c = (size_t)pi[p] + (size_t)Nx_ * ((size_t)pj[p] + (size_t)Ny_ * pk[p]);
+    for (int a = 0; a < 3; a++) im[3 * p + a] = inv_mu_[3 * mat_[c] + a];
+  }
+  put(dpi_, pi.data(), np * 4); put(dpj_, pj.data(), np * 4); put(dpk_, pk.data(), np * 4);
+  put(dinvmu_, im.data(), 3 * np * 8);
+  put(dslot_, slot_of_step_.data(), nsteps_ * 4);
+  CU(cudaStreamSynchronize(stream_));
+}
+
+void FitSim::launch_steps(int n, cudaEvent_t* ev) {
+  ProbeSet pr;
+  pr.n = (int)probe_cell_.size();
+  pr.ci = dpi_; pr.cj = dpj_; pr.ck = dpk_;
+  pr.inv_mu = dinvmu_; pr.samples = dsamples_; pr.slot_of_step = dslot_;
+  if (opt_.precision == 1) {
+    FitGrid<float> g; SpecialEdges<float> s;
+    fill_grid(g, s);
+    for (int q = 0; q < n; q++) fit_launch_step<float>(g, s, pr, dstep_, dflux_, stream_, ev);
+  } else {
+    FitGrid<double> g; SpecialEdges<double> s;
+    fill_grid(g, s);
+    for (int q = 0; q < n; q++) fit_launch_step<double>(g, s, pr, dstep_, dflux_, stream_, ev);
+  }
+}
+
+uint64_t FitSim::step(uint64_t n) {
+  if (step_ + n > nsteps_) n = nsteps_ - step_;
+  if (n == 0) { last_ms_ = 0; return 0; }
+  int glen = opt_.graph_steps;
+  if (glen <= 0) glen = n_cells() < 4000000 ? 64 : 1;  // small grids are launch bound: replay graphs
+  CU(cudaEventRecord(ev0_, stream_));
+  uint64_t left = n;
+  if (glen > 1) {
+    if (!graph_ || graph_len_ != glen) {
+      if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
+      cudaGraph_t gr;
+      CU(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+      launch_steps(glen);
+      CU(cudaStreamEndCapture(stream_, &gr));
+      CU(cudaGraphInstantiate(&graph_, gr, 0));
+      CU(cudaGraphDestroy(gr));
+      graph_len_ = glen;
+    }
+    while (left >= (uint64_t)glen) {
+      CU(cudaGraphLaunch(graph_, stream_));
+      left -= glen;
+    }
+  }
+  if (left) launch_steps((int)left);
+  CU(cudaGetLastError());
+  CU(cudaEventRecord(ev1_, stream_));
+  CU(cudaEventSynchronize(ev1_));
+  float ms = 0;
+  CU(cudaEventElapsedTime(&ms, ev0_, ev1_));
+  last_ms_ = ms;
+  step_ += n;
+  return n;
+}
+
+int FitSim::kernels_per_step() const {
+  return fit_kernels_per_step((int)special_.size(), (int)probe_cell_.size());
+}
+
+// Per-phase device time over n steps (sources/BC, E, scatter+flux, probes, H),
+// the counterpart of the reference's per-phase averages (Discretization.hpp
+// :2286-2302), from CUDA events recorded between the kernels on the stream.
+uint64_t FitSim::phase_times(uint64_t n, double* ms5) {
+  if (step_ + n > nsteps_) n = nsteps_ - step_;
+  for (int q = 0; q < 5; q++) ms5[q] = 0;
+  cudaEvent_t ev[6];
+  for (auto& e : ev) CU(cudaEventCreate(&e));
+  for (uint64_t i = 0; i < n; i++) {
+    launch_steps(1, ev);
+    CU(cudaEventSynchronize(ev[5]));
+    for (int q = 0; q < 5; q++) {
+      float ms = 0;
+      CU(cudaEventElapsedTime(&ms, ev[q], ev[q + 1]));
+      ms5[q] += ms;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  step_ += n;
+  return n;
+}
+
+// One step driven from the host: the carrier values of this step come from
+// `carrier_in` (one per simulation source, in source-label order; NULL keeps
+// the script's waveform) through a pinned staging buffer, and the probe
+// sample the step produces is read back into `probe_out` (NULL: none).
+uint64_t FitSim::step_io(const double* carrier_in, double* probe_out) {
+  if (step_ >= nsteps_) return 0;
+  const size_t nsrc = src_labels_.size(), np = probe_cell_.size();
+  if (!pinned_) {
+    CU(cudaHostAlloc((void**)&pinned_, (nsrc + 6 * np + 1) * sizeof(double), cudaHostAllocDefault));
+  }
+  if (carrier_in && nsrc) {
+    std::memcpy(pinned_, carrier_in, nsrc * sizeof(double));
+    CU(cudaMemcpyAsync(dcarrier_ + step_ * nsrc, pinned_, nsrc * sizeof(double), cudaMemcpyHostToDevice, stream_));
+  }
+  launch_steps(1, nullptr);
+  const int slot = slot_of_step_[step_];
+  if (probe_out && slot >= 0 && np) {
+    CU(cudaMemcpyAsync(pinned_ + nsrc, dsamples_ + (size_t)slot * np * 6, np * 6 * sizeof(double),
+                       cudaMemcpyDeviceToHost, stream_));
+  }
+  CU(cudaStreamSynchronize(stream_));
+  if (probe_out && slot >= 0 && np) std::memcpy(probe_out, pinned_ + nsrc, np * 6 * sizeof(double));
+  step_++;
+  return 1;
+}
+
+size_t FitSim::n_samples() const {
+  size_t c = 0;
+  for (uint64_t i = 0; i < step_; i++)
+    if (slot_of_step_[i] >= 0) c++;
+  return c;
+}
+
+void FitSim::get_probes(double* times, double* values, size_t cap) const {
+  size_t ns = n_samples();
+  if (ns > cap) ns = cap;
+  const size_t np = probe_cell_.size();
+  if (times) std::memcpy(times, sample_times_.data(), ns * 8);
+  if (values && ns && np) CU(cudaMemcpy(values, dsamples_, ns * np * 6 * 8, cudaMemcpyDeviceToHost));
+}
+
+void FitSim::probe_points(double* xyz, uint64_t* cells, size_t cap) const {
+  for (size_t p = 0; p < probe_cell_.size() && p < cap; p++) {
+    if (xyz) for (int a = 0; a < 3; a++) xyz[3 * p + a] = probe_pts_[p][a];
+    if (cells)
+      cells[p] = (uint64_t)probe_cell_[p][0] +
+                 (uint64_t)Nx_ * ((uint64_t)probe_cell_[p][1] + (uint64_t)Ny_ * probe_cell_[p][2]);
+  }
+}
+
+void FitSim::get_flux(double* flux, size_t cap, size_t* n) const {
+  size_t m = step_ < cap ? step_ : cap;
+  if (flux && m) CU(cudaMemcpy(flux, dflux_, m * 8, cudaMemcpyDeviceToHost));
+  if (n) *n = step_;
+}
+
+// The reference's numbering of the Cartesian complex: cubes swept k, j, i;
+// each cube numbers the edges and faces not shared with its bottom (k-1),
+// left (j-1) and back (i-1) neighbours, in slot order
+// (Discretization.hpp:4583-4934).
+void FitSim::build_ref_maps() {
+  if (!edge_map_.empty()) return;
+  static const int kEdgeAxis[12] = {0, 1, 2, 1, 2, 0, 2, 2, 0, 1, 1, 0};
+  static const int kEdgeNode0[12] = {0, 0, 0, 1, 1, 2, 2, 3, 4, 4, 5, 6};
+  static const int kShBottom[4] = {0, 1, 3, 5}, kShLeft[4] = {0, 2, 4, 8}, kShBack[4] = {1, 2, 6, 9};
+  static const int kFaceN[6] = {2, 1, 0, 0, 1, 2};
+  static const int kFaceOff[6][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  edge_map_.reserve(nE_);
+  face_map_.reserve(nF_);
+  for (int k = 0; k < Nz_; k++)
+    for (int j = 0; j < Ny_; j++)
+      for (int i = 0; i < Nx_; i++) {
+        bool shared[12] = {false};
+        if (k > 0) for (int q : kShBottom) shared[q] = true;
+        if (j > 0) for (int q : kShLeft) shared[q] = true;
+        if (i > 0) for (int q : kShBack) shared[q] = true;
+        bool fsh[6] = {k > 0, j > 0, i > 0, false, false, false};
+        for (int q = 0; q < 6; q++) {
+          if (fsh[q]) continue;
+          int64_t s = (i + kFaceOff[q][0]) + sx_ * (j + kFaceOff[q][1]) + sxy_ * (k + kFaceOff[q][2]);
+          face_map_.push_back(((int64_t)kFaceN[q] << 60) | s);
+        }
+        for (int q = 0; q < 12; q++) {
+          if (shared[q]) continue;
+          int n0 = kEdgeNode0[q];
+          int64_t s = (i + (n0 & 1)) + sx_ * (j + ((n0 >> 1) & 1)) + sxy_ * (k + ((n0 >> 2) & 1));
+          edge_map_.push_back(((int64_t)kEdgeAxis[q] << 60) | s);
+        }
+      }
+}
+
+void FitSim::get_state(double* U, double* B, double* F) {
+  build_ref_maps();
+  const size_t es = opt_.precision == 1 ? 4 : 8;
+  std::vector<char> hu[3], hf[3];
+  for (int a = 0; a < 3; a++) {
+    hu[a].resize(nslot_ * es);
+    hf[a].resize(nslot_ * es);
+    CU(cudaMemcpy(hu[a].data(), dU_[a], nslot_ * es, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(hf[a].data(), dF_[a], nslot_ * es, cudaMemcpyDeviceToHost));
+  }
+  auto rd = [&](const std::vector<char>& v, int64_t s) {
+    return es == 8 ? ((const double*)v.data())[s] : (double)((const float*)v.data())[s];
+  };
+  const int64_t mask = ((int64_t)1 << 60) - 1;
+  if (U)
+    for (size_t e = 0; e < edge_map_.size(); e++) U[e] = rd(hu[edge_map_[e] >> 60], edge_map_[e] & mask);
+  if (F)
+    for (size_t f = 0; f < face_map_.size(); f++) F[f] = rd(hf[face_map_[f] >> 60], face_map_[f] & mask);
+  if (B) {
+    // B = F / M_nu on live faces (the H update keeps F = M_nu B)
+    const int N[3] = {Nx_, Ny_, Nz_};
+    const double area[3] = {L_[1] * L_[2], L_[0] * L_[2], L_[0] * L_[1]};
+    for (size_t f = 0; f < face_map_.size(); f++) {
+      int n = (int)(face_map_[f] >> 60);
+      int64_t s = face_map_[f] & mask;
+      int k = (int)(s / sxy_), j = (int)((s % sxy_) / sx_), i = (int)(s % sx_);
+      int e[3] = {i, j, k};
+      int ms[2], nm = 0;
+      bool live = false;
+      if (e[n] > 0) {
+        int c[3] = {i, j, k};
+        c[n]--;
+        ms[nm++] = mat_[(size_t)c[0] + (size_t)Nx_ * ((size_t)c[1] + (size_t)Ny_ * c[2])];
+      }
+      if (e[n] < N[n]) ms[nm++] = mat_[(size_t)i + (size_t)Nx_ * ((size_t)j + (size_t)Ny_ * k)];
+      double ni = 0, msg = 0;
+      bool lossy = false;
+      for (int q = 0; q < nm; q++) {
+        live = live || live_[ms[q]];
+        ni += R_[3 * ms[q] + n];
+        if (X_[3 * ms[q] + n] != 0) { msg += X_[3 * ms[q] + n]; lossy = true; }
+      }
+      double mnu = 0;
+      if (ni != 0) mnu = lossy ? 1 / (area[n] * (1 / ni + 0.5 * dt_ / msg)) : ni / area[n];
+      double fv = rd(hf[n], s);
+      B[f] = (live && mnu != 0) ? fv / mnu : 0.0;
+    }
+  }
+}
+
+void FitSim::set_state(const double* U, const double* F) {
+  build_ref_maps();
+  const size_t es = opt_.precision == 1 ? 4 : 8;
+  const int64_t mask = ((int64_t)1 << 60) - 1;
+  std::vector<char> hu[3], hf[3];
+  for (int a = 0; a < 3; a++) {
+    hu[a].assign(nslot_ * es, 0);
+    hf[a].assign(nslot_ * es, 0);
+  }
+  auto wr = [&](std::vector<char>& v, int64_t s, double x) {
+    if (es == 8) ((double*)v.data())[s] = x;
+    else ((float*)v.data())[s] = (float)x;
+  };
+  for (size_t e = 0; e < edge_map_.size(); e++) wr(hu[edge_map_[e] >> 60], edge_map_[e] & mask, U ? U[e] : 0.0);
+  for (size_t f = 0; f < face_map_.size(); f++) wr(hf[face_map_[f] >> 60], face_map_[f] & mask, F ? F[f] : 0.0);
+  for (int a = 0; a < 3; a++) {
+    CU(cudaMemcpy(dU_[a], hu[a].data(), nslot_ * es, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(dF_[a], hf[a].data(), nslot_ * es, cudaMemcpyHostToDevice));
+  }
+}
+
+double FitSim::energy() {
+  size_t nb;
+  double* part = nullptr;
+  if (opt_.precision == 1) {
+    FitGrid<float> g; SpecialEdges<float> s;
+    fill_grid(g, s);
+    nb = fit_launch_energy<float>(g, nullptr, stream_);
+    CU(cudaMallocAsync((void**)&part, nb * 8, stream_));
+    fit_launch_energy<float>(g, part, stream_);
+  } else {
+    FitGrid<double> g; SpecialEdges<double> s;
+    fill_grid(g, s);
+    nb = fit_launch_energy<double>(g, nullptr, stream_);
+    CU(cudaMallocAsync((void**)&part, nb * 8, stream_));
+    fit_launch_energy<double>(g, part, stream_);
+  }
+  std::vector<double> h(nb);
+  CU(cudaMemcpyAsync(h.data(), part, nb * 8, cudaMemcpyDeviceToHost, stream_));
+  CU(cudaFreeAsync(part, stream_));
+  CU(cudaStreamSynchronize(stream_));
+  double acc = 0;
+  for (double x : h) acc += x;
+  return acc;
+}
+
+}  // namespace tf

@@ -1,0 +1,492 @@
+// Cartesian FIT (Yee) leapfrog kernels for sm_100a.
+//
+//   fit_e_kernel        interior E update  (Discretization.hpp:1869-1876)
+//   fit_special_pre     boundary / source / interface edges, into a side buffer
+//                       (Discretization.hpp:1850-1863, 1880-1895, 3899-4202)
+//   fit_special_post    scatter of the side buffer + per-step boundary flux
+//                       (Discretization.hpp:1901)
+//   fit_probe_kernel    E and H at probe cells (Discretization.hpp:3555-3588)
+//   fit_h_kernel        H update (Discretization.hpp:1908-1915)
+//
+// The update arithmetic uses explicitly rounded operations (no contraction to
+// FMA) in the reference's operation order, so the FP64 path reproduces the
+// CPU reference arithmetic exactly; the FP32 path runs the same code on
+// float state with coefficients rounded from their double values.
+#include <cuda_runtime.h>
+
+#include "fit_kernels.cuh"
+
+namespace tf {
+
+template <typename T>
+struct Ar;
+template <>
+struct Ar<double> {
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+};
+template <>
+struct Ar<float> {
+  static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+  static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+  static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+};
+
+__device__ __forceinline__ int64_t cell_index(int i, int j, int k, int Nx, int Ny) {
+  return (int64_t)i + (int64_t)Nx * ((int64_t)j + (int64_t)Ny * k);
+}
+
+// Edge coefficients from the materials of its cells, listed in sweep order
+// (Discretization.hpp:5294-5330 accumulation, :5591-5609 M_h/M_q).
+template <typename T>
+__device__ void edge_coef(const FitGrid<T>& g, int a, const uint8_t* m, int nm, double& mh, double& mq) {
+  double eps = 0.0, sig = 0.0;
+  bool lossy = false;
+  for (int q = 0; q < nm; q++) {
+    eps = __dadd_rn(eps, g.P[3 * m[q] + a]);
+    double s = g.S[3 * m[q] + a];
+    if (s != 0.0) {
+      sig = __dadd_rn(sig, s);
+      lossy = true;
+    }
+  }
+  const double len = g.len[a];
+  if (eps != 0.0) {
+    if (lossy) {
+      double hs = __dmul_rn(__dmul_rn(0.5, g.dt), sig);
+      mh = len / __dadd_rn(eps, hs);
+      mq = __dsub_rn(eps, hs) / len;
+    } else {
+      mh = len / eps;
+      mq = eps / len;
+    }
+  } else {
+    mh = 0.0;
+    mq = 0.0;
+  }
+}
+
+// Face coefficients (Discretization.hpp:5270-5292 accumulation, :5488-5514).
+template <typename T>
+__device__ void face_coef(const FitGrid<T>& g, int a, const uint8_t* m, int nm, double& mnu, double& mmu) {
+  double ni = 0.0, ms = 0.0;
+  bool lossy = false;
+  for (int q = 0; q < nm; q++) {
+    ni = __dadd_rn(ni, g.R[3 * m[q] + a]);
+    double x = g.X[3 * m[q] + a];
+    if (x != 0.0) {
+      ms = __dadd_rn(ms, x);
+      lossy = true;
+    }
+  }
+  const double area = g.area[a];
+  if (ni != 0.0) {
+    if (lossy) {
+      double hd = __dmul_rn(0.5, g.dt) / ms;
+      mnu = 1.0 / __dmul_rn(area, __dadd_rn(1.0 / ni, hd));
+      mmu = __dmul_rn(area, __dsub_rn(1.0 / ni, hd));
+    } else {
+      mnu = ni / area;
+      mmu = area / ni;
+    }
+  } else {
+    mnu = 0.0;
+    mmu = 0.0;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void edge_coef_t(const FitGrid<T>& g, int a, const uint8_t* m, T& mh, T& mq) {
+  if (m[0] == m[1] && m[0] == m[2] && m[0] == m[3]) {
+    mh = g.mh_pure[3 * m[0] + a];
+    mq = g.mq_pure[3 * m[0] + a];
+  } else {
+    double h, q;
+    edge_coef(g, a, m, 4, h, q);
+    mh = (T)h;
+    mq = (T)q;
+  }
+}
+
+// Face (axis a) at slot s whose lower cell is (il,jl,kl) and upper cell (i,j,k).
+template <typename T>
+__device__ __forceinline__ bool face_coef_t(const FitGrid<T>& g, int a, bool has_lo, bool has_hi, uint8_t mlo,
+                                            uint8_t mhi, T& mnu, T& mmu) {
+  if (!((has_lo && g.live[mlo]) || (has_hi && g.live[mhi]))) return false;
+  if (has_lo && has_hi && mlo == mhi) {
+    mnu = g.mnu_pure[3 * mlo + a];
+    mmu = g.mmu_pure[3 * mlo + a];
+  } else {
+    uint8_t m[2];
+    int nm = 0;
+    if (has_lo) m[nm++] = mlo;
+    if (has_hi) m[nm++] = mhi;
+    double nu, mu;
+    face_coef(g, a, m, nm, nu, mu);
+    mnu = (T)nu;
+    mmu = (T)mu;
+  }
+  return true;
+}
+
+// Interior E update: one thread per node slot (i,j,k) updates the x, y and z
+// edges leaving that node, when they have all four faces.
+template <typename T>
+__global__ void __launch_bounds__(256) fit_e_kernel(FitGrid<T> g) {
+  using A = Ar<T>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i > g.Nx || j > g.Ny) return;
+  const int64_t s = (int64_t)i + g.sx * j + g.sxy * k;
+  const T dt = (T)g.dt;
+  const bool xin = i > 0 && i < g.Nx, yin = j > 0 && j < g.Ny, zin = k > 0 && k < g.Nz;
+  // materials of the 8 cells around the node: c[dz][dy][dx], d=0 is the lower cell
+  uint8_t c[2][2][2];
+#pragma unroll
+  for (int dz = 0; dz < 2; dz++)
+#pragma unroll
+    for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+      for (int dx = 0; dx < 2; dx++) {
+        int ci = i - 1 + dx, cj = j - 1 + dy, ck = k - 1 + dz;
+        bool ok = ci >= 0 && ci < g.Nx && cj >= 0 && cj < g.Ny && ck >= 0 && ck < g.Nz;
+        c[dz][dy][dx] = ok ? g.mat[cell_index(ci, cj, ck, g.Nx, g.Ny)] : 0;
+      }
+  if (i < g.Nx && yin && zin) {  // x-edge: faces Fy(k-1), Fz(j-1), Fz, Fy (Ct order)
+    uint8_t m[4] = {c[0][0][1], c[0][1][1], c[1][0][1], c[1][1][1]};
+    T mh, mq;
+    edge_coef_t(g, 0, m, mh, mq);
+    T cf = A::sub(A::add(A::sub(g.Fy[s - g.sxy], g.Fz[s - g.sx]), g.Fz[s]), g.Fy[s]);
+    g.Ux[s] = A::mul(mh, A::add(A::mul(mq, g.Ux[s]), A::mul(dt, cf)));
+  }
+  if (j < g.Ny && xin && zin) {  // y-edge: faces Fx(k-1), Fz(i-1), Fz, Fx; dual curl -1
+    uint8_t m[4] = {c[0][1][0], c[0][1][1], c[1][1][0], c[1][1][1]};
+    T mh, mq;
+    edge_coef_t(g, 1, m, mh, mq);
+    T cf = -A::sub(A::add(A::sub(g.Fx[s - g.sxy], g.Fz[s - 1]), g.Fz[s]), g.Fx[s]);
+    g.Uy[s] = A::mul(mh, A::add(A::mul(mq, g.Uy[s]), A::mul(dt, cf)));
+  }
+  if (k < g.Nz && xin && yin) {  // z-edge: faces Fx(j-1), Fy(i-1), Fy, Fx
+    uint8_t m[4] = {c[1][0][0], c[1][0][1], c[1][1][0], c[1][1][1]};
+    T mh, mq;
+    edge_coef_t(g, 2, m, mh, mq);
+    T cf = A::sub(A::add(A::sub(g.Fx[s - g.sx], g.Fy[s - 1]), g.Fy[s]), g.Fx[s]);
+    g.Uz[s] = A::mul(mh, A::add(A::mul(mq, g.Uz[s]), A::mul(dt, cf)));
+  }
+}
+
+// New flux B of a face from F (old) and U (new); F_new = M_nu B.
+template <typename T>
+__device__ __forceinline__ T face_flux(T mmu, T Fold, T dtc, T cs) {
+  using A = Ar<T>;
+  return A::sub(A::mul(mmu, Fold), A::mul(dtc, cs));
+}
+
+template <typename T>
+__device__ __forceinline__ T curl_x(const FitGrid<T>& g, int64_t s) {  // Fx at slot s
+  using A = Ar<T>;
+  return A::sub(A::add(A::sub(g.Uy[s], g.Uz[s]), g.Uz[s + g.sx]), g.Uy[s + g.sxy]);
+}
+template <typename T>
+__device__ __forceinline__ T curl_y(const FitGrid<T>& g, int64_t s) {
+  using A = Ar<T>;
+  return A::sub(A::add(A::sub(g.Ux[s], g.Uz[s]), g.Uz[s + 1]), g.Ux[s + g.sxy]);
+}
+template <typename T>
+__device__ __forceinline__ T curl_z(const FitGrid<T>& g, int64_t s) {
+  using A = Ar<T>;
+  return A::sub(A::add(A::sub(g.Ux[s], g.Uy[s]), g.Uy[s + 1]), g.Ux[s + g.sx]);
+}
+
+template <typename T>
+__device__ __forceinline__ uint8_t cell_mat(const FitGrid<T>& g, int i, int j, int k) {
+  return g.mat[cell_index(i, j, k, g.Nx, g.Ny)];
+}
+
+// B of face (axis a) at (i,j,k) recomputed from the current F and U; returns
+// false (B = 0) for faces the H update leaves alone.
+template <typename T>
+__device__ bool face_B(const FitGrid<T>& g, int a, int i, int j, int k, T& B, T& mnu, T* mmu_out = nullptr) {
+  const int64_t s = (int64_t)i + g.sx * j + g.sxy * k;
+  const T dt = (T)g.dt;
+  int li = i, lj = j, lk = k;
+  bool has_lo, has_hi;
+  if (a == 0) { li = i - 1; has_lo = i > 0; has_hi = i < g.Nx; }
+  else if (a == 1) { lj = j - 1; has_lo = j > 0; has_hi = j < g.Ny; }
+  else { lk = k - 1; has_lo = k > 0; has_hi = k < g.Nz; }
+  uint8_t mlo = has_lo ? cell_mat(g, li, lj, lk) : 0, mhi = has_hi ? cell_mat(g, i, j, k) : 0;
+  T mmu;
+  if (!face_coef_t(g, a, has_lo, has_hi, mlo, mhi, mnu, mmu)) {
+    B = (T)0;
+    return false;
+  }
+  if (mmu_out) *mmu_out = mmu;
+  if (a == 0) B = face_flux(mmu, g.Fx[s], dt, curl_x(g, s));
+  else if (a == 1) B = face_flux(mmu, g.Fy[s], -dt, curl_y(g, s));
+  else B = face_flux(mmu, g.Fz[s], dt, curl_z(g, s));
+  return true;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) fit_h_kernel(FitGrid<T> g, int* step_counter) {
+  using A = Ar<T>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (step_counter && i == 0 && j == 0 && k == 0) atomicAdd(step_counter, 1);
+  if (i > g.Nx || j > g.Ny) return;
+  const int64_t s = (int64_t)i + g.sx * j + g.sxy * k;
+  const T dt = (T)g.dt;
+  const bool ci = i < g.Nx, cj = j < g.Ny, ck = k < g.Nz;
+  const uint8_t m0 = (ci && cj && ck) ? cell_mat(g, i, j, k) : 0;
+  T mnu, mmu;
+  if (cj && ck) {  // Fx(i,j,k): cells (i-1,j,k), (i,j,k)
+    uint8_t ml = i > 0 ? cell_mat(g, i - 1, j, k) : 0;
+    if (face_coef_t(g, 0, i > 0, ci, ml, m0, mnu, mmu)) {
+      T B = face_flux(mmu, g.Fx[s], dt, curl_x(g, s));
+      g.Fx[s] = A::mul(mnu, B);
+    }
+  }
+  if (ci && ck) {  // Fy(i,j,k): cells (i,j-1,k), (i,j,k); curl -1
+    uint8_t ml = j > 0 ? cell_mat(g, i, j - 1, k) : 0;
+    if (face_coef_t(g, 1, j > 0, cj, ml, m0, mnu, mmu)) {
+      T B = face_flux(mmu, g.Fy[s], -dt, curl_y(g, s));
+      g.Fy[s] = A::mul(mnu, B);
+    }
+  }
+  if (ci && cj) {  // Fz(i,j,k): cells (i,j,k-1), (i,j,k)
+    uint8_t ml = k > 0 ? cell_mat(g, i, j, k - 1) : 0;
+    if (face_coef_t(g, 2, k > 0, ck, ml, m0, mnu, mmu)) {
+      T B = face_flux(mmu, g.Fz[s], dt, curl_z(g, s));
+      g.Fz[s] = A::mul(mnu, B);
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T* comp_ptr(T* x, T* y, T* z, int c) {
+  return c == 0 ? x : (c == 1 ? y : z);
+}
+
+// Special edges: new values into sp.out, flux partial sums per block.
+template <typename T>
+__global__ void __launch_bounds__(256) fit_special_pre(FitGrid<T> g, SpecialEdges<T> sp, const int* step_counter) {
+  using A = Ar<T>;
+  __shared__ double red[256];
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int step = *step_counter;
+  double contrib = 0.0;
+  if (e < sp.n) {
+    T* U = comp_ptr(g.Ux, g.Uy, g.Uz, sp.comp[e]);
+    const int64_t slot = sp.slot[e];
+    const T Uo = U[slot];
+    // source value: sum of source vectors, dotted with the projection vector
+    double v[3] = {0.0, 0.0, 0.0};
+    int kind = 0;
+    for (int p = sp.src_begin[e]; p < sp.src_begin[e + 1]; p++) {
+      const int si = sp.pair_src[p];
+      kind = sp.src_kind[si] + 1;
+      double ret = __dmul_rn(sp.src_amp[si], sp.carrier[(int64_t)step * sp.nsrc + si]);
+      ret = __dmul_rn(ret, sp.pair_fac[4 * p + 0]);
+      ret = __dmul_rn(ret, sp.pair_fac[4 * p + 1]);
+      ret = __dmul_rn(ret, sp.pair_fac[4 * p + 2]);
+      ret = __dmul_rn(ret, sp.pair_fac[4 * p + 3]);
+      const int d = sp.pair_dir[p];
+      v[d] = __dadd_rn(v[d], ret);
+    }
+    double val = 0.0;
+    if (kind) {
+      const double* w = sp.pair_vec + 3 * (int64_t)e;
+      val = __dadd_rn(__dadd_rn(__dmul_rn(v[0], w[0]), __dmul_rn(v[1], w[1])), __dmul_rn(v[2], w[2]));
+      val = __dmul_rn(sp.post[e], val);
+    }
+    const int op = sp.op[e];
+    T Un;
+    if (op == 0) {
+      Un = kind == 1 ? (T)val : (T)0;
+    } else {
+      const T dt = (T)g.dt;
+      T f[4];
+      const int nf = sp.nface[e];
+      for (int q = 0; q < 4; q++) {
+        f[q] = (T)0;
+        if (q < nf) {
+          const T* F = comp_ptr(g.Fx, g.Fy, g.Fz, sp.fcomp[4 * e + q]);
+          f[q] = F[sp.fslot[4 * e + q]];
+        }
+      }
+      const T I = kind == 3 ? (T)val : (T)0;
+      const T mh = (T)sp.mh[e], mq = (T)sp.mq[e];
+      T cf;
+      if (op == 1) {  // explicit signed faces, Eigen 3-vector dot order
+        T acc = A::add(A::mul(f[0], (T)sp.fsign[4 * e]), A::mul(f[1], (T)sp.fsign[4 * e + 1]));
+        acc = A::add(acc, A::mul(f[2], (T)sp.fsign[4 * e + 2]));
+        if (nf > 3) acc = A::add(acc, A::mul(f[3], (T)sp.fsign[4 * e + 3]));
+        const T cfb = kind == 2 ? (T)val : (T)0;
+        cf = A::sub(A::add(acc, cfb), I);
+        Un = A::mul(mh, A::add(A::mul(mq, Uo), A::mul(dt, cf)));
+        contrib = __dmul_rn(__dadd_rn((double)Uo, (double)Un), (double)cfb);
+      } else {  // interior stencil with a dipole current
+        T st = A::sub(A::add(A::sub(f[0], f[1]), f[2]), f[3]);
+        cf = A::sub(A::mul((T)sp.fsign[4 * e], st), I);
+        Un = A::mul(mh, A::add(A::mul(mq, Uo), A::mul(dt, cf)));
+      }
+    }
+    sp.out[e] = Un;
+  }
+  red[threadIdx.x] = contrib;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] = __dadd_rn(red[threadIdx.x], red[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) sp.flux_part[blockIdx.x] = red[0];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) fit_special_post(FitGrid<T> g, SpecialEdges<T> sp, const int* step_counter,
+                                                         double* flux, int nparts) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < sp.n) {
+    T* U = comp_ptr(g.Ux, g.Uy, g.Uz, sp.comp[e]);
+    U[sp.slot[e]] = sp.out[e];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    double acc = 0.0;
+    for (int b = 0; b < nparts; b++) acc = __dadd_rn(acc, sp.flux_part[b]);
+    flux[*step_counter] = __dmul_rn(0.5, acc);
+  }
+}
+
+template <typename T>
+__global__ void fit_probe_kernel(FitGrid<T> g, ProbeSet pr, const int* step_counter) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= pr.n) return;
+  const int slotn = pr.slot_of_step[*step_counter];
+  if (slotn < 0) return;
+  const int i = pr.ci[p], j = pr.cj[p], k = pr.ck[p];
+  const double Lx = g.len[0], Ly = g.len[1], Lz = g.len[2];
+  const double vol = __dmul_rn(__dmul_rn(Lx, Ly), Lz);
+  const double dax = __dmul_rn(Ly, Lz) / 4, day = __dmul_rn(Lx, Lz) / 4, daz = __dmul_rn(Lx, Ly) / 4;
+  auto U = [&](const T* a, int ii, int jj, int kk) { return (double)a[(int64_t)ii + g.sx * jj + g.sxy * kk]; };
+  auto sum4 = [&](double a, double b, double c, double d, double w) {
+    return __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(a, w), __dmul_rn(b, w)), __dmul_rn(c, w)), __dmul_rn(d, w));
+  };
+  double* out = pr.samples + ((int64_t)slotn * pr.n + p) * 6;
+  out[0] = sum4(U(g.Ux, i, j, k), U(g.Ux, i, j + 1, k), U(g.Ux, i, j, k + 1), U(g.Ux, i, j + 1, k + 1), dax) / vol;
+  out[1] = sum4(U(g.Uy, i, j, k), U(g.Uy, i + 1, j, k), U(g.Uy, i, j, k + 1), U(g.Uy, i + 1, j, k + 1), day) / vol;
+  out[2] = sum4(U(g.Uz, i, j, k), U(g.Uz, i + 1, j, k), U(g.Uz, i, j + 1, k), U(g.Uz, i + 1, j + 1, k), daz) / vol;
+  const double half[3] = {__dmul_rn(0.5, Lx), __dmul_rn(0.5, Ly), __dmul_rn(0.5, Lz)};
+  for (int a = 0; a < 3; a++) {
+    T B0, B1, nu;
+    face_B(g, a, i, j, k, B0, nu);
+    face_B(g, a, i + (a == 0), j + (a == 1), k + (a == 2), B1, nu);
+    double h = __dadd_rn(__dmul_rn((double)B0, half[a]), __dmul_rn((double)B1, half[a]));
+    out[3 + a] = __dmul_rn(pr.inv_mu[3 * p + a], h) / vol;
+  }
+}
+
+// ---------------------------------------------------------------- launchers
+template <typename T>
+void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const ProbeSet& pr, int* step_counter,
+                     double* flux, cudaStream_t st, cudaEvent_t* ev) {
+  // ev (optional): 6 events recorded around the 5 phases, for per-phase timing
+  dim3 blk(32, 8, 1);
+  dim3 grd((unsigned)((g.Nx + 1 + 31) / 32), (unsigned)((g.Ny + 1 + 7) / 8), (unsigned)(g.Nz + 1));
+  const int nsb = (sp.n + 255) / 256;
+  if (ev) cudaEventRecord(ev[0], st);
+  if (sp.n > 0) fit_special_pre<T><<<nsb, 256, 0, st>>>(g, sp, step_counter);
+  if (ev) cudaEventRecord(ev[1], st);
+  fit_e_kernel<T><<<grd, blk, 0, st>>>(g);
+  if (ev) cudaEventRecord(ev[2], st);
+  fit_special_post<T><<<nsb > 0 ? nsb : 1, 256, 0, st>>>(g, sp, step_counter, flux, nsb);
+  if (ev) cudaEventRecord(ev[3], st);
+  if (pr.n > 0) fit_probe_kernel<T><<<(pr.n + 127) / 128, 128, 0, st>>>(g, pr, step_counter);
+  if (ev) cudaEventRecord(ev[4], st);
+  fit_h_kernel<T><<<grd, blk, 0, st>>>(g, step_counter);
+  if (ev) cudaEventRecord(ev[5], st);
+}
+
+int fit_kernels_per_step(int n_special, int n_probes) { return 3 + (n_special > 0) + (n_probes > 0); }
+
+template void fit_launch_step<double>(const FitGrid<double>&, const SpecialEdges<double>&, const ProbeSet&, int*,
+                                      double*, cudaStream_t, cudaEvent_t*);
+template void fit_launch_step<float>(const FitGrid<float>&, const SpecialEdges<float>&, const ProbeSet&, int*,
+                                     double*, cudaStream_t, cudaEvent_t*);
+
+// Discrete leapfrog energy: 0.5 sum M_e U^2 + 0.5 sum M_mu F_old F_new, with
+// F_new recomputed (not stored) from the current U.  FP64 accumulation, one
+// partial per block.
+template <typename T>
+__global__ void __launch_bounds__(256) fit_energy_kernel(FitGrid<T> g, double* part) {
+  __shared__ double red[256];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  double acc = 0.0;
+  if (i <= g.Nx && j <= g.Ny) {
+    const int64_t s = (int64_t)i + g.sx * j + g.sxy * k;
+    uint8_t c[2][2][2];
+    for (int dz = 0; dz < 2; dz++)
+      for (int dy = 0; dy < 2; dy++)
+        for (int dx = 0; dx < 2; dx++) {
+          int ci = i - 1 + dx, cj = j - 1 + dy, ck = k - 1 + dz;
+          bool ok = ci >= 0 && ci < g.Nx && cj >= 0 && cj < g.Ny && ck >= 0 && ck < g.Nz;
+          c[dz][dy][dx] = ok ? g.mat[cell_index(ci, cj, ck, g.Nx, g.Ny)] : 255;
+        }
+    // electric part: M_e = avg_eps / len over the edge's existing cells
+    const T* Us[3] = {g.Ux, g.Uy, g.Uz};
+    const bool valid[3] = {i < g.Nx, j < g.Ny, k < g.Nz};
+    for (int a = 0; a < 3; a++) {
+      if (!valid[a]) continue;
+      uint8_t m[4];
+      int nm = 0;
+      for (int q = 0; q < 4; q++) {
+        int b0 = q & 1, b1 = (q >> 1) & 1;
+        uint8_t cm;
+        if (a == 0) cm = c[b1][b0][1];
+        else if (a == 1) cm = c[b1][1][b0];
+        else cm = c[1][b1][b0];
+        if (cm != 255) m[nm++] = cm;
+      }
+      double eps = 0.0;
+      for (int q = 0; q < nm; q++) eps += g.P[3 * m[q] + a];
+      double u = (double)Us[a][s];
+      acc += 0.5 * (eps / g.len[a]) * u * u;
+    }
+    for (int a = 0; a < 3; a++) {
+      T B, nu;
+      if ((a == 0 && j < g.Ny && k < g.Nz) || (a == 1 && i < g.Nx && k < g.Nz) || (a == 2 && i < g.Nx && j < g.Ny)) {
+        const T* Fs = a == 0 ? g.Fx : (a == 1 ? g.Fy : g.Fz);
+        double Fold = (double)Fs[s];
+        T mmu;
+        if (face_B(g, a, i, j, k, B, nu, &mmu)) {
+          double Fnew = (double)nu * (double)B;
+          acc += 0.5 * ((double)mmu * Fold) * Fnew;
+        }
+      }
+    }
+  }
+  red[tid] = acc;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (tid < w) red[tid] += red[tid + w];
+    __syncthreads();
+  }
+  if (tid == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * (uint64_t)blockIdx.z)] = red[0];
+}
+
+template <typename T>
+size_t fit_launch_energy(const FitGrid<T>& g, double* part, cudaStream_t st) {
+  dim3 blk(32, 8, 1);
+  dim3 grd((unsigned)((g.Nx + 1 + 31) / 32), (unsigned)((g.Ny + 1 + 7) / 8), (unsigned)(g.Nz + 1));
+  if (part) fit_energy_kernel<T><<<grd, blk, 0, st>>>(g, part);
+  return (size_t)grd.x * grd.y * grd.z;
+}
+template size_t fit_launch_energy<double>(const FitGrid<double>&, double*, cudaStream_t);
+template size_t fit_launch_energy<float>(const FitGrid<float>&, double*, cudaStream_t);
+
+}  // namespace tf
