@@ -41,6 +41,7 @@ WORKLOADS = {
     # name: (cells per axis, spheres, precision, steps in the script)
     "fit512": (512, 200, "fp32", 5000),
     "fit64": (64, 0, "fp64", 2000),
+    "fit256": (256, 200, "fp32", 2000),   # profiling size: state 400 MB > L2
 }
 
 
@@ -164,8 +165,9 @@ def run_ours(args, rank, world, local_rank):
     probe = np.zeros(max(info["n_probes"], 1) * 6)
     barrier()
     t0 = time.perf_counter()
+    s0 = d.info()["step_index"]
     for i in range(K2):
-        s = info["step_index"] + i
+        s = s0 + i
         carrier[:] = np.sin(2 * np.pi * case.frequency * (s * info["dt"] - 0.5 * info["dt"]))
         d.step_io(carrier, probe)
     e2e_s = time.perf_counter() - t0

@@ -114,3 +114,104 @@ class FitOracle:
             self.close()
         except Exception:
             pass
+
+
+class TetOracle:
+    """FP64 CPU restatement of one tetrahedral simulation (dga or gfdtd)."""
+
+    def __init__(self, script: str, label: int = 1, omp: bool = False, consistent_mass: bool = False):
+        self.L = lib(omp)
+        L = self.L
+        P = ctypes.c_void_p
+        if not getattr(L, "_tet_sigs", False):
+            L.orc_tet_open.restype = P
+            L.orc_tet_open.argtypes = [ctypes.c_char_p, ctypes.c_uint, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+            L.orc_tet_close.argtypes = [P]
+            L.orc_tet_info.argtypes = [P, P, P]
+            L.orc_tet_step.restype = ctypes.c_longlong
+            L.orc_tet_step.argtypes = [P, ctypes.c_longlong]
+            L.orc_tet_nsamples.restype = ctypes.c_longlong
+            L.orc_tet_nsamples.argtypes = [P]
+            L.orc_tet_probes.argtypes = [P, P, P, P, P]
+            L.orc_tet_state.argtypes = [P, P, P, P]
+            L.orc_tet_flux.argtypes = [P, P]
+            L.orc_tet_cg.argtypes = [P, P, P]
+            L.orc_tet_topology.argtypes = [P, P, P, P, P]
+            L.orc_tet_matrix.restype = ctypes.c_longlong
+            L.orc_tet_matrix.argtypes = [P, ctypes.c_int, P, P, P]
+            L._tet_sigs = True
+        err = ctypes.create_string_buffer(1024)
+        self.h = L.orc_tet_open(os.fsencode(script), label, int(consistent_mass), err, 1024)
+        if not self.h:
+            raise RuntimeError(err.value.decode())
+        iv = np.zeros(16, dtype=np.int64)
+        dv = np.zeros(16)
+        L.orc_tet_info(self.h, _p(iv), _p(dv))
+        (self.nE, self.nF, self.nT, self.nN, self.n_probes, self.n_steps, self.method, self.n_free,
+         self.n_bnd) = (int(x) for x in iv[:9])
+        self.possibly_unstable = bool(iv[9])
+        self.dt, self.dt_estimate = float(dv[0]), float(dv[1])
+        self.steps_done = 0
+
+    def step(self, n: int) -> int:
+        d = int(self.L.orc_tet_step(self.h, n))
+        self.steps_done += d
+        return d
+
+    def run(self) -> int:
+        return self.step(self.n_steps)
+
+    def probes(self):
+        ns = int(self.L.orc_tet_nsamples(self.h))
+        t = np.zeros(ns)
+        v = np.zeros((ns, self.n_probes, 6))
+        pts = np.zeros((self.n_probes, 3))
+        el = np.zeros(self.n_probes, dtype=np.int64)
+        self.L.orc_tet_probes(self.h, _p(t), _p(v), _p(pts), _p(el))
+        return t, v, pts, el
+
+    def state(self):
+        U, F, B = np.zeros(self.nE), np.zeros(self.nF), np.zeros(self.nF)
+        self.L.orc_tet_state(self.h, _p(U), _p(F), _p(B))
+        return U, B, F
+
+    def flux(self):
+        f = np.zeros(self.steps_done)
+        self.L.orc_tet_flux(self.h, _p(f))
+        return f
+
+    def cg(self):
+        it = np.zeros(self.steps_done, dtype=np.int32)
+        er = np.zeros(self.steps_done)
+        self.L.orc_tet_cg(self.h, _p(it), _p(er))
+        return it, er
+
+    def topology(self):
+        e = np.zeros((self.nE, 2), dtype=np.uint32)
+        f = np.zeros((self.nF, 3), dtype=np.uint32)
+        c = np.zeros(self.nE, dtype=np.uint8)
+        b = np.zeros(self.nE, dtype=np.int32)
+        self.L.orc_tet_topology(self.h, _p(e), _p(f), _p(c), _p(b))
+        return e, f, c, b
+
+    def matrix(self, which: str):
+        """CSR (ptr, col, val) of one operator: C, N, H (dga), E or A (gfdtd)."""
+        w = {"C": 0, "N": 1, "H": 2, "E": 3, "A": 4}[which]
+        nnz = int(self.L.orc_tet_matrix(self.h, w, None, None, None))
+        nrows = {0: self.nF, 1: self.nF, 2: self.nE, 3: self.nE, 4: self.n_free}[w]
+        ptr = np.zeros(nrows + 1, dtype=np.uint64)
+        col = np.zeros(nnz, dtype=np.uint32)
+        val = np.zeros(nnz)
+        self.L.orc_tet_matrix(self.h, w, _p(ptr), _p(col), _p(val))
+        return ptr, col, val
+
+    def close(self):
+        if self.h:
+            self.L.orc_tet_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -13,7 +13,7 @@ import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_build")
-SOURCES = ["script.cpp", "fit.cpp", "capi.cpp"]
+SOURCES = ["script.cpp", "fit.cpp", "tet.cpp", "capi.cpp"]
 LIB = os.path.join(OUT_DIR, "libtf_oracle.so")
 LIB_OMP = os.path.join(OUT_DIR, "libtf_oracle_omp.so")
 

@@ -5,6 +5,7 @@
 #include <string>
 
 #include "fit.hpp"
+#include "tet.hpp"
 
 using orc::FitOracle;
 
@@ -93,6 +94,96 @@ int orc_fit_topology(void* h, unsigned* edge_nodes, double* node_xyz, unsigned* 
     for (auto e : o->uncommon_edges) classes[e] = 3;
   }
   return (int)o->pts.size();
+}
+
+// ---------------------------------------------------------------- tets
+void* orc_tet_open(const char* script, unsigned label, int flags, char* err, int errlen) {
+  auto* o = new orc::TetOracle();
+  o->consistent_mass = (flags & 1) != 0;
+  try {
+    o->sc.parse(script);
+    o->prepare(label);
+    return o;
+  } catch (const std::exception& e) {
+    put_err(err, errlen, e.what());
+    delete o;
+    return nullptr;
+  }
+}
+
+void orc_tet_close(void* h) { delete static_cast<orc::TetOracle*>(h); }
+
+// ints: nE nF nV(tets) nNodes nprobes nsteps method nfree nbnd possibly_unstable
+// dbls: dt dt_estimate
+int orc_tet_info(void* h, long long* iv, double* dv) {
+  auto* o = static_cast<orc::TetOracle*>(h);
+  iv[0] = (long long)o->edges.size(); iv[1] = (long long)o->faces.size(); iv[2] = (long long)o->vols.size();
+  iv[3] = (long long)o->pts.size(); iv[4] = (long long)o->probe_elem.size(); iv[5] = (long long)o->nsteps_total;
+  iv[6] = o->method; iv[7] = (long long)o->free_edges.size(); iv[8] = (long long)o->bnd_dual.size();
+  iv[9] = o->possibly_unstable;
+  dv[0] = o->dt; dv[1] = o->dt_estimate;
+  return 0;
+}
+
+long long orc_tet_step(void* h, long long n) { return (long long)static_cast<orc::TetOracle*>(h)->step((uint64_t)n); }
+long long orc_tet_nsamples(void* h) { return (long long)static_cast<orc::TetOracle*>(h)->times.size(); }
+
+int orc_tet_probes(void* h, double* times, double* samples, double* points, long long* elems) {
+  auto* o = static_cast<orc::TetOracle*>(h);
+  if (times) std::memcpy(times, o->times.data(), o->times.size() * sizeof(double));
+  if (samples) std::memcpy(samples, o->samples.data(), o->samples.size() * sizeof(double));
+  for (size_t p = 0; p < o->probe_elem.size(); p++) {
+    if (points) for (int a = 0; a < 3; a++) points[3 * p + a] = o->probe_pts[p][a];
+    if (elems) elems[p] = o->probe_elem[p];
+  }
+  return 0;
+}
+
+int orc_tet_state(void* h, double* U, double* F, double* B) {
+  auto* o = static_cast<orc::TetOracle*>(h);
+  if (U) std::memcpy(U, o->U.data(), o->U.size() * sizeof(double));
+  if (F) std::memcpy(F, o->F.data(), o->F.size() * sizeof(double));
+  if (B) std::memcpy(B, o->B.data(), o->B.size() * sizeof(double));
+  return 0;
+}
+
+int orc_tet_flux(void* h, double* flux) {
+  auto* o = static_cast<orc::TetOracle*>(h);
+  std::memcpy(flux, o->flux.data(), o->flux.size() * sizeof(double));
+  return (int)o->flux.size();
+}
+
+int orc_tet_cg(void* h, int* iters, double* errs) {
+  auto* o = static_cast<orc::TetOracle*>(h);
+  for (size_t k = 0; k < o->cg_iters.size(); k++) {
+    if (iters) iters[k] = o->cg_iters[k];
+    if (errs) errs[k] = o->cg_err[k];
+  }
+  return (int)o->cg_iters.size();
+}
+
+// topology: edges [nE][2] (node ids), faces [nF][3], classes [nE], bnd index [nE]
+int orc_tet_topology(void* h, unsigned* edges, unsigned* faces, unsigned char* cls, int* bnd) {
+  auto* o = static_cast<orc::TetOracle*>(h);
+  for (size_t e = 0; e < o->edges.size(); e++) {
+    if (edges) { edges[2 * e] = o->edges[e][0]; edges[2 * e + 1] = o->edges[e][1]; }
+    if (cls) cls[e] = o->cls[e];
+    if (bnd) bnd[e] = o->bnd_edges[e];
+  }
+  if (faces)
+    for (size_t f = 0; f < o->faces.size(); f++)
+      for (int a = 0; a < 3; a++) faces[3 * f + a] = o->faces[f][a];
+  return 0;
+}
+
+// CSR export of an operator: which 0 C, 1 N, 2 H, 3 E, 4 A; returns nnz
+long long orc_tet_matrix(void* h, int which, unsigned long long* ptr, unsigned* col, double* val) {
+  auto* o = static_cast<orc::TetOracle*>(h);
+  const orc::Csr* m = which == 0 ? &o->C : which == 1 ? &o->N : which == 2 ? &o->H : which == 3 ? &o->E : &o->A;
+  if (ptr) for (size_t i = 0; i < m->ptr.size(); i++) ptr[i] = m->ptr[i];
+  if (col) std::memcpy(col, m->col.data(), m->col.size() * sizeof(unsigned));
+  if (val) std::memcpy(val, m->val.data(), m->val.size() * sizeof(double));
+  return (long long)m->val.size();
 }
 
 }  // extern "C"

@@ -1,0 +1,108 @@
+// ORACLE — test infrastructure only.  FP64 CPU restatement of TetFIT's
+// tetrahedral DGA paths ("method dga" explicit and "method gfdtd" with the
+// Jacobi-PCG mass solve); see tet.cpp for the reference lines followed.
+#pragma once
+#include <array>
+#include <cstdint>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "script.hpp"
+
+namespace orc {
+
+// Compressed sparse rows with duplicates summed in insertion order, the way
+// Eigen's setFromTriplets(..., add) assembles (columns ascending per row).
+struct Csr {
+  uint32_t nrows = 0, ncols = 0;
+  std::vector<uint64_t> ptr;
+  std::vector<uint32_t> col;
+  std::vector<double> val;
+  struct Trip {
+    uint32_t r, c;
+    double v;
+  };
+  static Csr build(uint32_t nr, uint32_t nc, const std::vector<Trip>& t);
+  void mul(const double* x, double* y) const;          // y = A x
+  void mul_t(const double* x, double* y) const;        // y = A^T x (A^T built on the fly)
+  double diag(uint32_t i) const;
+};
+
+struct TetOracle {
+  Script sc;
+  Simulation sim;
+  Output out;
+  uint32_t sim_label = 0;
+  int method = 1;  // 1 dga, 2 gfdtd
+  // mesh and complex (reference numbering: sorted unique faces/edges)
+  std::vector<std::array<double, 3>> pts;
+  std::vector<std::array<uint32_t, 4>> vols;
+  std::vector<uint32_t> vol_mat;
+  std::vector<double> cell_vol;
+  std::vector<std::array<uint32_t, 3>> faces;
+  std::vector<std::array<uint32_t, 2>> edges;
+  std::vector<std::array<std::pair<uint32_t, int>, 4>> vtf;
+  std::vector<std::vector<std::pair<uint32_t, int>>> ftv;
+  std::vector<std::array<std::pair<uint32_t, int>, 3>> fte;
+  std::vector<std::vector<std::pair<uint32_t, int>>> nte;
+  std::vector<std::vector<uint32_t>> node_vols;
+  std::vector<uint64_t> boundary_face;
+  std::vector<int32_t> bnd_edges;
+  std::vector<std::array<double, 3>> bnd_dual;
+  std::vector<uint32_t> edge_bcs;
+  std::vector<std::vector<uint32_t>> edge_src;
+  std::vector<uint8_t> is_pec, cls;  // cls: 1 interior dof, 4 Dirichlet (PEC or e-source)
+  Csr C;                               // F x E, +-1
+  // operators
+  Csr N;                               // F x F
+  Csr H;                               // E x E, rows of class-1 edges (dga)
+  Csr E;                               // E x E eps mass (gfdtd)
+  Csr A, RHS1;                         // free x free system; E(free rows, Dirichlet cols)
+  std::vector<int64_t> free_index;     // edge -> compressed free index or -1
+  std::vector<uint32_t> free_edges;
+  std::vector<double> jacobi;
+  double dt = 0, dt_estimate = 0;
+  bool possibly_unstable = false;
+  // state
+  std::vector<double> U, I, F, B, Fb, Fb_old, U_old, SrcFld, solution;
+  uint32_t root = 0;
+  std::vector<uint32_t> probe_elem;
+  std::vector<std::array<double, 3>> probe_pts;
+  std::vector<double> times, samples, flux;
+  std::vector<int> cg_iters;
+  std::vector<double> cg_err;
+  uint64_t step_index = 0, nsteps_total = 0;
+  int cg_maxiter = 100;
+  bool consistent_mass = false;  // gfdtd: corrected eps-mass (see tet.cpp)
+
+  void prepare(uint32_t label);
+  uint64_t step(uint64_t n);
+  // helpers shared with the C ABI
+  std::array<double, 3> edge_bar(uint32_t e) const;
+  std::array<double, 3> face_bar(uint32_t f) const;
+  std::array<double, 3> vol_bar(uint32_t v) const;
+
+ private:
+  void read_mesh();
+  void build_dga();
+  void build_gfdtd();
+  std::array<uint32_t, 6> vol_edges(uint32_t v) const;
+  std::array<std::array<double, 3>, 6> dual_area_vectors(uint32_t v) const;
+  std::array<std::array<double, 3>, 4> primal_area_vectors(uint32_t v) const;
+  void local_M(uint32_t v, double M[4][4]) const;
+  Csr assemble_N() const;
+  uint32_t find_probe(const std::array<double, 3>& pv);
+  double efield_source(uint32_t e, double t);
+  double current_source(uint32_t e, double t);
+  double hfield_source(uint32_t e, double t);
+  void apply_K(const double* x, double* y, std::vector<double>& tf) const;
+  int cg_solve(const Csr& M, const std::vector<double>& pre, const double* b, double* x, double tol, int maxit,
+               double* err) const;
+  void export_probes(double t);
+  void dga_step(double t);
+  void gfdtd_step(double t, double t_prev);
+  std::vector<std::array<double, 16>> whitney_;
+};
+
+}  // namespace orc

@@ -10,8 +10,8 @@ benchmark are generated here from seeds:
   (z = zmin), surfaces 2-6 PEC, probe grid {0.1,0.1,0.6} x {0.5,1,0.5} x
   {0,0.04,1.05} (156 probes inside the box), optionally with seeded random
   spheres of lossy dielectric over vacuum.
-* `kuhn_box` (tetrahedral) -- n^3 cubes cut into 6 Kuhn tetrahedra with
-  seeded interior-vertex jitter; see `write_netgen_kuhn`.
+* `kuhn_mesh` / `write_tet_case` (tetrahedral) -- n^3 cubes cut into 6 Kuhn
+  tetrahedra with seeded interior-vertex jitter, written in netgen format.
 
 Surface labels on the Cartesian grid follow the reference code
 (Discretization.hpp:5084-5232): 1 z-, 2 x-, 3 y+, 4 x+, 5 y-, 6 z+.
@@ -52,7 +52,7 @@ class FitCase:
 
     def dt(self) -> float:
         if self.step is not None:
-            return self.step
+            return float(self.step)
         h = 1.0 / self.n
         return 0.95 * self.courant * h / (C0 * math.sqrt(3.0))
 
@@ -72,8 +72,8 @@ def write_fit_cavity(directory: str, case: FitCase, name: str = "cavity") -> str
         f.write(f"DEFINE solid {nmat}\n   SET material {nmat}\n   SET type box\n")
         f.write("   SET corner {0,0,0}\n   SET size {1,1,1}\n")
         f.write(f"END solid {nmat}\n")
-    dt = case.dt()
-    duration = (case.steps - 1) * dt
+    dt = float(case.dt())
+    duration = float((case.steps - 1) * dt)
     h = 1.0 / case.n
     lines = []
     lines += ["DEFINE mesh 1", "   SET type cartesian",
@@ -113,3 +113,129 @@ def random_spheres(count: int, seed: int) -> list:
         out.append(Sphere(center=tuple(rng.uniform(0.0, 1.0, 3)), radius=float(rng.uniform(0.02, 0.1)),
                           eps_r=float(rng.uniform(1.0, 10.0)), sigma=float(10 ** rng.uniform(-4, 0))))
     return out
+
+
+# --------------------------------------------------------------- tetrahedral
+# Kuhn (Freudenthal) subdivision of a cube into 6 tetrahedra sharing the main
+# diagonal; node bits: 1 = +x, 2 = +y, 4 = +z.  The same split in every cube
+# keeps the mesh conforming.
+KUHN_TETS = ((0, 1, 3, 7), (0, 1, 5, 7), (0, 2, 3, 7), (0, 2, 6, 7), (0, 4, 5, 7), (0, 4, 6, 7))
+# domain-surface labels of the generated meshes: 1 z-, 2 x-, 3 y-, 4 x+, 5 y+, 6 z+
+SURFACE_LABELS = {("z", 0): 1, ("x", 0): 2, ("y", 0): 3, ("x", 1): 4, ("y", 1): 5, ("z", 1): 6}
+
+
+def kuhn_mesh(n: int, jitter: float = 0.15, seed: int = 0x7E7F17, material=None):
+    """Points [(n+1)^3, 3], tets [6 n^3, 4] (0-based), tet materials, boundary
+    triangles [(12 n^2), 3] and their labels, for the unit cube cut into n^3
+    cubes of 6 Kuhn tetrahedra.  Interior vertices are moved by
+    U[-jitter*h, jitter*h]^3 (seeded); boundary vertices stay on the box.
+    `material(centroids) -> labels` assigns tet materials (default 1)."""
+    h = 1.0 / n
+    g = np.arange(n + 1) * h
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    pts = np.stack([X.ravel(order="F"), Y.ravel(order="F"), Z.ravel(order="F")], axis=1)
+    idx = np.arange((n + 1) ** 3).reshape((n + 1, n + 1, n + 1), order="F")  # idx[i,j,k]
+    rng = np.random.default_rng(seed)
+    interior = np.ones((n + 1,) * 3, dtype=bool)
+    interior[[0, -1], :, :] = False
+    interior[:, [0, -1], :] = False
+    interior[:, :, [0, -1]] = False
+    inter = interior.ravel(order="F")
+    shift = rng.uniform(-jitter * h, jitter * h, size=(int(inter.sum()), 3))
+    pts[inter] += shift
+    i, j, k = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    i, j, k = i.ravel(order="F"), j.ravel(order="F"), k.ravel(order="F")
+    corner = [idx[i + (b & 1), j + ((b >> 1) & 1), k + ((b >> 2) & 1)] for b in range(8)]
+    tets = np.stack([np.stack([corner[a], corner[b], corner[c], corner[d]], 1) for (a, b, c, d) in KUHN_TETS],
+                    1).reshape(-1, 4)
+    cent = pts[tets].mean(axis=1)
+    mats = np.ones(len(tets), dtype=np.int64) if material is None else np.asarray(material(cent), dtype=np.int64)
+    # boundary triangles: the Kuhn faces lying on the box
+    tris, labels = [], []
+    faces = np.concatenate([tets[:, [0, 1, 2]], tets[:, [0, 1, 3]], tets[:, [0, 2, 3]], tets[:, [1, 2, 3]]])
+    fp = pts[faces]
+    for axis, name in enumerate("xyz"):
+        for side in (0, 1):
+            on = np.all(np.abs(fp[:, :, axis] - side) < 1e-12, axis=1)
+            tris.append(faces[on])
+            labels.append(np.full(int(on.sum()), SURFACE_LABELS[(name, side)]))
+    return pts, tets, mats, np.concatenate(tris), np.concatenate(labels)
+
+
+def write_netgen(path: str, pts, tets, mats, tris, labels) -> str:
+    """Netgen neutral format as TetFIT reads it (Discretization.hpp:5924-6101,
+    6612-6654): point count + coordinates, tetrahedron count + `mat p1..p4`,
+    triangle count + `label p1 p2 p3`, all node indices 1-based."""
+    with open(path, "w") as f:
+        f.write(f"{len(pts)}\n")
+        np.savetxt(f, pts, fmt="%.17g")
+        f.write(f"{len(tets)}\n")
+        np.savetxt(f, np.column_stack([mats, tets + 1]), fmt="%d")
+        f.write(f"{len(tris)}\n")
+        np.savetxt(f, np.column_stack([labels, tris + 1]), fmt="%d")
+    return path
+
+
+@dataclass
+class TetCase:
+    n: int = 24
+    method: str = "gfdtd"            # "dga" (explicit) or "gfdtd" (PCG)
+    steps: int = 200
+    courant: float = 0.98
+    step: float | None = None        # pinned time step; default from the Kuhn-mesh bound below
+    tolerance: float = 1e-8
+    frequency: float = 2e8
+    jitter: float = 0.15
+    seed: int = 0x7E7F17
+    eps: tuple = (1.0,)              # eps_r per material label 1, 2, ...
+    split_x: bool = False            # material 1 for x < 0.5, 2 for x >= 0.5
+    pec_surfaces: tuple = (2, 3, 4, 5, 6)
+    source_surface: int = 1
+    source_type: str = "h"
+    carrier: str = "sin"
+    probes: bool = True
+    mat_field: object = None         # optional callable centroids -> labels
+
+    def dt(self) -> float:
+        if self.step is not None:
+            return float(self.step)
+        # 0.25 h / c0: below the stability limit of the jittered Kuhn meshes
+        return 0.25 * (1.0 / self.n) / C0
+
+
+def write_tet_case(directory: str, case: TetCase, name: str = "box") -> str:
+    os.makedirs(directory, exist_ok=True)
+    if case.mat_field is not None:
+        material = case.mat_field
+    elif case.split_x:
+        material = lambda c: np.where(c[:, 0] < 0.5, 1, 2)
+    else:
+        material = None
+    mesh = write_netgen(os.path.join(directory, f"{name}.mesh"),
+                        *kuhn_mesh(case.n, case.jitter, case.seed, material))
+    dt = float(case.dt())
+    duration = float((case.steps - 1) * dt if case.method == "dga" else case.steps * dt)
+    lines = ["DEFINE mesh 1", "   SET type tetrahedral", "   SET mesher netgen",
+             f"   SET file {os.path.basename(mesh)}", "   SET name box", "   SET scalefactor 1", "END mesh 1"]
+    for m, e in enumerate(case.eps, start=1):
+        lines += [f"DEFINE material {m}", f"   SET epsilon {e!r}", "   SET mu 1", "   SET sigma 0", "   SET chi 0",
+                  f"END material {m}"]
+    lines += ["DEFINE bc 1"] + [f"   SET surface {s}" for s in case.pec_surfaces] + ["   SET type pec", "END bc 1"]
+    lines += ["DEFINE source 1", f"   SET surface {case.source_surface}", f"   SET type {case.source_type}",
+              "   SET profile wave", "   SET mode { sin , cos , cos }", "   SET center {0, 0, 0}",
+              "   SET direction x", "   SET amplitude 1", f"   SET frequency {case.frequency!r}",
+              f"   SET carrier {case.carrier}", "   SET wavevector { 0.5, 0, 0 }", "END source 1"]
+    if case.probes:
+        lines += ["DEFINE output 1", "   SET name zsections", "   SET mode probepoint",
+                  "   SET xgrid { 0.1, 0.1,0.6}", "   SET ygrid { 0.5, 1, 0.5}", "   SET zgrid { 0, 0.04, 1.05}",
+                  "   SET grid on", "   SET period 0", "END output 1"]
+    lines += ["DEFINE simulation 1", f"   SET method {case.method}", "   SET solver cg",
+              f"   SET tolerance {case.tolerance!r}", "   SET mesh 1", "   SET source 1",
+              f"   SET duration {duration!r}", f"   SET step {dt!r}", f"   SET courant {case.courant!r}"]
+    if case.probes:
+        lines += ["   SET output 1"]
+    lines += ["END simulation 1"]
+    script = os.path.join(directory, f"{name}.fdtd")
+    with open(script, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return script
