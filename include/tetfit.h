@@ -49,7 +49,12 @@ typedef struct tf_opts {
   int32_t write_files;  /* tf_run: write <name><label>_probe_E/H.dat and poynting.dat   */
   int32_t verbose;      /* print the reference's parameter banner and stats            */
   int32_t graph_steps;  /* steps per captured CUDA graph (0: automatic)                */
-  int32_t reserved[11];
+  int32_t mass_model;   /* gfdtd eps-mass: 0 as the reference builds it, 1 consistent  */
+  int32_t warm_start;   /* gfdtd CG guess: 0 previous solution (reference), 1 zero,
+                           2 polynomial extrapolation, 3 learned per-edge MLP        */
+  int32_t cg_criterion; /* 0 ||r||/||r0|| <= tol (reference), 1 ||r|| <= tol ||b||   */
+  int32_t cg_maxiter;   /* 0: 100, the reference's limit                             */
+  int32_t reserved[7];
 } tf_opts;
 
 typedef struct tf_info {
@@ -102,6 +107,9 @@ TF_API int tf_step_io(tf_ctx* ctx, const double* carrier_in, double* probe_out, 
 TF_API int tf_phase_times(tf_ctx* ctx, uint64_t nsteps, double* ms5, uint64_t* done);
 /* Whole simulation as RunSimulation does it: prepare, every step, output files. */
 TF_API int tf_run(tf_ctx* ctx, uint32_t sim_label, const tf_opts* opts);
+/* gfdtd: CG iterations and final relative residual of every step taken so far
+ * (the reference's "mean solver iterations", Discretization.hpp:2286-2302). */
+TF_API int tf_solver_stats(tf_ctx* ctx, int32_t* iters, double* resid, size_t cap, size_t* n);
 /* Device time of the last tf_step call, from CUDA events on the context stream. */
 TF_API int tf_last_step_ms(tf_ctx* ctx, double* ms);
 TF_API const char* tf_last_error(tf_ctx* ctx);

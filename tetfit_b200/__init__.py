@@ -32,7 +32,9 @@ class TetfitError(RuntimeError):
 
 class Opts(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("device", ctypes.c_int32), ("write_files", ctypes.c_int32),
-                ("verbose", ctypes.c_int32), ("graph_steps", ctypes.c_int32), ("reserved", ctypes.c_int32 * 11)]
+                ("verbose", ctypes.c_int32), ("graph_steps", ctypes.c_int32), ("mass_model", ctypes.c_int32),
+                ("warm_start", ctypes.c_int32), ("cg_criterion", ctypes.c_int32), ("cg_maxiter", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 7)]
 
 
 class Info(ctypes.Structure):
@@ -70,6 +72,7 @@ _SIGS = {
     "tf_step_io": (ctypes.c_int, [_P, _P, _P, ctypes.POINTER(ctypes.c_uint64)]),
     "tf_phase_times": (ctypes.c_int, [_P, ctypes.c_uint64, _P, ctypes.POINTER(ctypes.c_uint64)]),
     "tf_run": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(Opts)]),
+    "tf_solver_stats": (ctypes.c_int, [_P, _P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "tf_last_step_ms": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double)]),
     "tf_last_error": (ctypes.c_char_p, [_P]),
     "tf_close": (None, [_P]),
@@ -128,12 +131,19 @@ class Discretization:
         self._check(lib().tf_simulations(self._h, arr, n.value, ctypes.byref(n)))
         return list(arr)[: n.value]
 
+    WARM_STARTS = {"previous": 0, "zero": 1, "extrapolate": 2, "learned": 3}
+
     @staticmethod
-    def _opts(precision="fp64", device=0, write_files=False, verbose=False, graph_steps=0) -> Opts:
+    def _opts(precision="fp64", device=0, write_files=False, verbose=False, graph_steps=0, mass="reference",
+              warm_start="previous", cg_criterion="reference", cg_maxiter=0) -> Opts:
         o = Opts()
         lib().tf_default_opts(ctypes.byref(o))
         o.precision = {"fp64": FP64, "fp32": FP32}[precision] if isinstance(precision, str) else int(precision)
         o.device, o.write_files, o.verbose, o.graph_steps = device, int(write_files), int(verbose), graph_steps
+        o.mass_model = {"reference": 0, "consistent": 1}[mass]
+        o.warm_start = Discretization.WARM_STARTS[warm_start] if isinstance(warm_start, str) else int(warm_start)
+        o.cg_criterion = {"reference": 0, "rhs": 1}[cg_criterion]
+        o.cg_maxiter = cg_maxiter
         return o
 
     def prepare(self, label: int, **opts) -> dict:
@@ -169,6 +179,15 @@ class Discretization:
         done = ctypes.c_uint64()
         self._check(lib().tf_phase_times(self._h, n, _ptr(ms), ctypes.byref(done)))
         return ms, done.value
+
+    def solver_stats(self):
+        """gfdtd: (iterations[n_steps_done], final relative residual[n_steps_done])."""
+        n = ctypes.c_size_t()
+        self._check(lib().tf_solver_stats(self._h, None, None, 0, ctypes.byref(n)))
+        it = np.zeros(n.value, dtype=np.int32)
+        rs = np.zeros(n.value)
+        self._check(lib().tf_solver_stats(self._h, _ptr(it), _ptr(rs), n.value, ctypes.byref(n)))
+        return it, rs
 
     def last_step_ms(self) -> float:
         ms = ctypes.c_double()

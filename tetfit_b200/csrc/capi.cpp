@@ -12,11 +12,13 @@
 #include "cuda_util.hpp"
 #include "fit.hpp"
 #include "script.hpp"
+#include "sim.hpp"
+#include "tet.hpp"
 
 struct tf_ctx {
   tf::Script sc;
   std::string path, err;
-  std::unique_ptr<tf::FitSim> fit;
+  std::unique_ptr<tf::Sim> fit;
   uint32_t label = 0;
   tf_opts opts{};
 };
@@ -50,7 +52,7 @@ int guarded(tf_ctx* c, F&& f) {
 // Output files of Discretization.hpp:1948-2010 (probe series) and :1936-1941
 // (poynting.dat): std::setw(15), default stream precision.
 void write_outputs(tf_ctx* c) {
-  tf::FitSim& f = *c->fit;
+  tf::Sim& f = *c->fit;
   const tf::Output& o = f.output();
   if (o.mode == "probepoint") {
     size_t ns = f.n_samples(), np = f.n_probes();
@@ -68,7 +70,7 @@ void write_outputs(tf_ctx* c) {
            << xyz[3 * p + 2] << " " << std::setw(15) << t[k] << " " << std::setw(15) << s[0] << " "
            << std::setw(15) << s[1] << " " << std::setw(15) << s[2] << std::endl;
         osh << std::setw(15) << xyz[3 * p] << " " << std::setw(15) << xyz[3 * p + 1] << " " << std::setw(15)
-            << xyz[3 * p + 2] << " " << std::setw(15) << t[k] - 0.5 * f.dt() << " " << std::setw(15) << s[3]
+            << xyz[3 * p + 2] << " " << std::setw(15) << t[k] + f.sample_time_shift() << " " << std::setw(15) << s[3]
             << " " << std::setw(15) << s[4] << " " << std::setw(15) << s[5] << std::endl;
       }
   }
@@ -76,14 +78,18 @@ void write_outputs(tf_ctx* c) {
   f.get_flux(nullptr, 0, &n);
   std::vector<double> fl(n);
   f.get_flux(fl.data(), n, &n);
+  // poynting.dat: times (k + 1/2) dt for fdtd/dga (:1936-1941, :945-950),
+  // (k + 1) dt for gfdtd (:1570-1574)
   std::ofstream pf("poynting.dat");
-  for (size_t k = 0; k < n; k++) pf << double(k + 0.5) * f.dt() << "\t" << fl[k] << "\t" << 0.0 << std::endl;
+  const double off = f.method() == 2 ? 1.0 : 0.5;
+  for (size_t k = 0; k < n; k++) pf << double(k + off) * f.dt() << "\t" << fl[k] << "\t" << 0.0 << std::endl;
 }
 
 void banner(tf_ctx* c) {
-  tf::FitSim& f = *c->fit;
+  tf::Sim& f = *c->fit;
+  static const char* kNames[3] = {"fdtd", "dga", "gfdtd"};
   std::cout << std::endl << "Simulation parameters:" << std::endl;
-  std::cout << std::setw(20) << "Method: " << std::setw(20) << "fdtd" << std::endl;
+  std::cout << std::setw(20) << "Method: " << std::setw(20) << kNames[f.method()] << std::endl;
   std::cout << std::setw(20) << "Simulation time: " << std::setw(20) << f.simulation().duration << " sec"
             << std::endl;
   std::cout << std::setw(20) << "Time step: " << std::setw(20) << f.dt() << " sec" << std::endl;
@@ -150,10 +156,16 @@ int tf_prepare(tf_ctx* c, uint32_t label, const tf_opts* opts) {
     ro.device = c->opts.device;
     ro.graph_steps = c->opts.graph_steps;
     ro.verbose = c->opts.verbose != 0;
+    ro.consistent_mass = c->opts.mass_model == 1;
+    ro.warm_start = c->opts.warm_start;
+    ro.cg_criterion = c->opts.cg_criterion;
+    if (c->opts.cg_maxiter > 0) ro.cg_maxiter = c->opts.cg_maxiter;
     if (meth == "fdtd") {
       c->fit.reset(new tf::FitSim(c->sc, label, ro));
+    } else if (meth == "dga" || meth == "gfdtd") {
+      c->fit.reset(new tf::TetSim(c->sc, label, ro));
     } else {
-      return fail(c, TF_E_UNSUPPORTED, "method " + meth + " is not available in this build");
+      return fail(c, TF_E_UNSUPPORTED, "method " + meth + " is outside the time-stepping path (fdtd, dga, gfdtd)");
     }
     c->label = label;
     if (ro.verbose) banner(c);
@@ -165,7 +177,7 @@ int tf_get_info(tf_ctx* c, tf_info* info) {
   if (!c || !info) return TF_E_ARG;
   if (!c->fit) return fail(c, TF_E_STATE, "tf_get_info before tf_prepare");
   std::memset(info, 0, sizeof(*info));
-  tf::FitSim& f = *c->fit;
+  tf::Sim& f = *c->fit;
   info->n_edges = f.n_edges();
   info->n_faces = f.n_faces();
   info->n_cells = f.n_cells();
@@ -173,7 +185,7 @@ int tf_get_info(tf_ctx* c, tf_info* info) {
   info->n_steps = f.n_steps();
   info->step_index = f.step_index();
   info->nx = f.nx(); info->ny = f.ny(); info->nz = f.nz();
-  info->method = 0;
+  info->method = f.method();
   info->dt = f.dt();
   info->dt_estimate = f.dt_estimate();
   info->possibly_unstable = f.possibly_unstable();
@@ -278,6 +290,16 @@ int tf_run(tf_ctx* c, uint32_t label, const tf_opts* opts) {
   return guarded(c, [&]() -> int {
     while (c->fit->step_index() < c->fit->n_steps()) c->fit->step(c->fit->n_steps() - c->fit->step_index());
     if (c->opts.write_files) write_outputs(c);
+    return TF_OK;
+  });
+}
+
+int tf_solver_stats(tf_ctx* c, int32_t* iters, double* resid, size_t cap, size_t* n) {
+  if (!c) return TF_E_ARG;
+  if (!c->fit) return fail(c, TF_E_STATE, "no simulation prepared");
+  return guarded(c, [&]() -> int {
+    size_t k = c->fit->solver_stats(iters, resid, cap);
+    if (n) *n = k;
     return TF_OK;
   });
 }

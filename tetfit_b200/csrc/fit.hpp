@@ -11,15 +11,9 @@
 
 #include "fit_kernels.cuh"
 #include "script.hpp"
+#include "sim.hpp"
 
 namespace tf {
-
-struct RunOptions {
-  int precision = 0;  // 0 fp64, 1 fp32
-  int device = 0;
-  int graph_steps = 0;
-  bool verbose = false;
-};
 
 // One special edge as built on the host (see SpecialEdges for the device form).
 struct HostSpecial {
@@ -35,40 +29,42 @@ struct HostSpecial {
   std::vector<uint32_t> srcs;  // source labels in the reference's edge_src order
 };
 
-class FitSim {
+class FitSim : public Sim {
  public:
   FitSim(Script& sc, uint32_t label, const RunOptions& opt);
-  ~FitSim();
-  uint64_t step(uint64_t n);
+  ~FitSim() override;
+  int method() const override { return 0; }
+  uint64_t step(uint64_t n) override;
   // accessors
-  uint64_t n_edges() const { return nE_; }
-  uint64_t n_faces() const { return nF_; }
-  uint64_t n_cells() const { return (uint64_t)Nx_ * Ny_ * Nz_; }
-  uint64_t n_probes() const { return probe_cell_.size(); }
-  uint64_t n_steps() const { return nsteps_; }
-  uint64_t step_index() const { return step_; }
-  int nx() const { return Nx_; }
-  int ny() const { return Ny_; }
-  int nz() const { return Nz_; }
-  double dt() const { return dt_; }
-  double dt_estimate() const { return dt_est_; }
-  bool possibly_unstable() const { return unstable_; }
-  int precision() const { return opt_.precision; }
-  uint64_t device_bytes() const { return dev_bytes_; }
-  double last_step_ms() const { return last_ms_; }
-  const Output& output() const { return out_; }
-  size_t n_samples() const;
-  void get_probes(double* times, double* values, size_t cap) const;
-  void probe_points(double* xyz, uint64_t* cells, size_t cap) const;
-  void get_state(double* U, double* B, double* F);
-  void set_state(const double* U, const double* F);
-  void get_flux(double* flux, size_t cap, size_t* n) const;
-  double energy();
-  uint64_t phase_times(uint64_t n, double* ms5);
-  uint64_t step_io(const double* carrier_in, double* probe_out);
-  int kernels_per_step() const;
-  size_t n_sources() const { return src_labels_.size(); }
-  const Simulation& simulation() const { return sim_; }
+  uint64_t n_edges() const override { return nE_; }
+  uint64_t n_faces() const override { return nF_; }
+  uint64_t n_cells() const override { return (uint64_t)Nx_ * Ny_ * Nz_; }
+  uint64_t n_probes() const override { return probe_cell_.size(); }
+  uint64_t n_steps() const override { return nsteps_; }
+  uint64_t step_index() const override { return step_; }
+  int nx() const override { return Nx_; }
+  int ny() const override { return Ny_; }
+  int nz() const override { return Nz_; }
+  double dt() const override { return dt_; }
+  double dt_estimate() const override { return dt_est_; }
+  bool possibly_unstable() const override { return unstable_; }
+  int precision() const override { return opt_.precision; }
+  uint64_t device_bytes() const override { return dev_bytes_; }
+  double last_step_ms() const override { return last_ms_; }
+  const Output& output() const override { return out_; }
+  size_t n_samples() const override;
+  double sample_time_shift() const override { return -0.5 * dt_; }
+  void get_probes(double* times, double* values, size_t cap) const override;
+  void probe_points(double* xyz, uint64_t* cells, size_t cap) const override;
+  void get_state(double* U, double* B, double* F) override;
+  void set_state(const double* U, const double* F) override;
+  void get_flux(double* flux, size_t cap, size_t* n) const override;
+  double energy() override;
+  uint64_t phase_times(uint64_t n, double* ms5) override;
+  uint64_t step_io(const double* carrier_in, double* probe_out) override;
+  int kernels_per_step() const override;
+  size_t n_sources() const override { return src_labels_.size(); }
+  const Simulation& simulation() const override { return sim_; }
 
  private:
   void setup_grid();

@@ -177,6 +177,86 @@ __global__ void __launch_bounds__(256) fit_e_kernel(FitGrid<T> g) {
   }
 }
 
+// Interior E update, z-marching form: a thread owns the node column (i,j)
+// over planes [k0, k1) and carries the z-1 faces and cell materials of the
+// previous plane in registers, so each plane costs 7 face loads, 3 edge
+// loads/stores and 4 material bytes.  Same arithmetic as fit_e_kernel.
+template <typename T>
+__global__ void __launch_bounds__(256) fit_e_march(FitGrid<T> g, int kchunk) {
+  using A = Ar<T>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k0 = blockIdx.z * kchunk;
+  if (i > g.Nx || j > g.Ny || k0 > g.Nz) return;
+  const int k1 = min(k0 + kchunk, g.Nz + 1);
+  const T dt = (T)g.dt;
+  const bool xin = i > 0 && i < g.Nx, yin = j > 0 && j < g.Ny;
+  const bool xe = i < g.Nx && yin, ye = j < g.Ny && xin, ze = xin && yin;  // column has x/y/z edges
+  const bool ci0 = i > 0, ci1 = i < g.Nx, cj0 = j > 0, cj1 = j < g.Ny;
+  int64_t s = (int64_t)i + g.sx * j + g.sxy * k0;
+  const int64_t cb = (int64_t)(i - 1) + (int64_t)g.Nx * (j - 1);  // cell (i-1,j-1) in a plane
+  const int64_t cplane = (int64_t)g.Nx * g.Ny;
+  // materials of the plane below, c[dy][dx]
+  uint8_t lo[2][2] = {{0, 0}, {0, 0}};
+  if (k0 > 0) {
+    const uint8_t* m = g.mat + cb + cplane * (k0 - 1);
+    lo[0][0] = (ci0 && cj0) ? m[0] : 0;
+    lo[0][1] = (ci1 && cj0) ? m[1] : 0;
+    lo[1][0] = (ci0 && cj1) ? m[g.Nx] : 0;
+    lo[1][1] = (ci1 && cj1) ? m[g.Nx + 1] : 0;
+  }
+  T fy_lo = (k0 > 0 && xe) ? g.Fy[s - g.sxy] : (T)0;
+  T fx_lo = (k0 > 0 && ye) ? g.Fx[s - g.sxy] : (T)0;
+  for (int k = k0; k < k1; k++, s += g.sxy) {
+    const bool zin = k > 0 && k < g.Nz;
+    uint8_t hi[2][2] = {{0, 0}, {0, 0}};
+    if (k < g.Nz) {
+      const uint8_t* m = g.mat + cb + cplane * k;
+      hi[0][0] = (ci0 && cj0) ? m[0] : 0;
+      hi[0][1] = (ci1 && cj0) ? m[1] : 0;
+      hi[1][0] = (ci0 && cj1) ? m[g.Nx] : 0;
+      hi[1][1] = (ci1 && cj1) ? m[g.Nx + 1] : 0;
+    }
+    const T fx = (j < g.Ny && k < g.Nz) ? g.Fx[s] : (T)0;
+    const T fy = (i < g.Nx && k < g.Nz) ? g.Fy[s] : (T)0;
+    if (zin) {
+      const T fz = g.Fz[s];
+      const bool same = lo[0][0] == lo[0][1] && lo[0][0] == lo[1][0] && lo[0][0] == lo[1][1] &&
+                        lo[0][0] == hi[0][0] && lo[0][0] == hi[0][1] && lo[0][0] == hi[1][0] &&
+                        lo[0][0] == hi[1][1];
+      if (xe) {  // x-edge: faces Fy(k-1), Fz(j-1), Fz, Fy
+        T mh, mq;
+        if (same) { mh = g.mh_pure[3 * lo[0][0]]; mq = g.mq_pure[3 * lo[0][0]]; }
+        else { uint8_t m[4] = {lo[0][1], lo[1][1], hi[0][1], hi[1][1]}; edge_coef_t(g, 0, m, mh, mq); }
+        const T cf = A::sub(A::add(A::sub(fy_lo, g.Fz[s - g.sx]), fz), fy);
+        g.Ux[s] = A::mul(mh, A::add(A::mul(mq, g.Ux[s]), A::mul(dt, cf)));
+      }
+      if (ye) {  // y-edge: faces Fx(k-1), Fz(i-1), Fz, Fx; dual curl -1
+        T mh, mq;
+        if (same) { mh = g.mh_pure[3 * lo[0][0] + 1]; mq = g.mq_pure[3 * lo[0][0] + 1]; }
+        else { uint8_t m[4] = {lo[1][0], lo[1][1], hi[1][0], hi[1][1]}; edge_coef_t(g, 1, m, mh, mq); }
+        const T cf = -A::sub(A::add(A::sub(fx_lo, g.Fz[s - 1]), fz), fx);
+        g.Uy[s] = A::mul(mh, A::add(A::mul(mq, g.Uy[s]), A::mul(dt, cf)));
+      }
+    }
+    if (ze && k < g.Nz) {  // z-edge: faces Fx(j-1), Fy(i-1), Fy, Fx
+      T mh, mq;
+      if (hi[0][0] == hi[0][1] && hi[0][0] == hi[1][0] && hi[0][0] == hi[1][1]) {
+        mh = g.mh_pure[3 * hi[0][0] + 2];
+        mq = g.mq_pure[3 * hi[0][0] + 2];
+      } else {
+        uint8_t m[4] = {hi[0][0], hi[0][1], hi[1][0], hi[1][1]};
+        edge_coef_t(g, 2, m, mh, mq);
+      }
+      const T cf = A::sub(A::add(A::sub(g.Fx[s - g.sx], g.Fy[s - 1]), fy), fx);
+      g.Uz[s] = A::mul(mh, A::add(A::mul(mq, g.Uz[s]), A::mul(dt, cf)));
+    }
+    fy_lo = fy;
+    fx_lo = fx;
+    lo[0][0] = hi[0][0]; lo[0][1] = hi[0][1]; lo[1][0] = hi[1][0]; lo[1][1] = hi[1][1];
+  }
+}
+
 // New flux B of a face from F (old) and U (new); F_new = M_nu B.
 template <typename T>
 __device__ __forceinline__ T face_flux(T mmu, T Fold, T dtc, T cs) {
@@ -262,6 +342,57 @@ __global__ void __launch_bounds__(256) fit_h_kernel(FitGrid<T> g, int* step_coun
       T B = face_flux(mmu, g.Fz[s], dt, curl_z(g, s));
       g.Fz[s] = A::mul(mnu, B);
     }
+  }
+}
+
+// H update, z-marching form: the thread owns face column (i,j) over planes
+// [k0, k1), carrying Ux, Uy at plane k+1 (needed again as plane k of the next
+// iteration) and the cell material below.  Same arithmetic as fit_h_kernel.
+template <typename T>
+__global__ void __launch_bounds__(256) fit_h_march(FitGrid<T> g, int kchunk, int* step_counter) {
+  using A = Ar<T>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k0 = blockIdx.z * kchunk;
+  if (step_counter && i == 0 && j == 0 && k0 == 0) atomicAdd(step_counter, 1);
+  if (i > g.Nx || j > g.Ny || k0 > g.Nz) return;
+  const int k1 = min(k0 + kchunk, g.Nz + 1);
+  const T dt = (T)g.dt;
+  const bool ci = i < g.Nx, cj = j < g.Ny;
+  int64_t s = (int64_t)i + g.sx * j + g.sxy * k0;
+  const int64_t cplane = (int64_t)g.Nx * g.Ny;
+  const int64_t cc = (int64_t)i + (int64_t)g.Nx * j;
+  T ux = (ci) ? g.Ux[s] : (T)0, uy = (cj) ? g.Uy[s] : (T)0;
+  uint8_t m_lo = (ci && cj && k0 > 0) ? g.mat[cc + cplane * (k0 - 1)] : 0;
+  for (int k = k0; k < k1; k++, s += g.sxy) {
+    const bool ck = k < g.Nz;
+    const uint8_t m0 = (ci && cj && ck) ? g.mat[cc + cplane * k] : 0;
+    const T ux1 = (ci && ck) ? g.Ux[s + g.sxy] : (T)0;
+    const T uy1 = (cj && ck) ? g.Uy[s + g.sxy] : (T)0;
+    T mnu, mmu;
+    if (cj && ck) {  // Fx(i,j,k): cells (i-1,j,k), (i,j,k)
+      const uint8_t ml = i > 0 ? g.mat[cc - 1 + cplane * k] : 0;
+      if (face_coef_t(g, 0, i > 0, ci, ml, m0, mnu, mmu)) {
+        const T cs = A::sub(A::add(A::sub(uy, g.Uz[s]), g.Uz[s + g.sx]), uy1);
+        g.Fx[s] = A::mul(mnu, face_flux(mmu, g.Fx[s], dt, cs));
+      }
+    }
+    if (ci && ck) {  // Fy(i,j,k): cells (i,j-1,k), (i,j,k); curl -1
+      const uint8_t ml = j > 0 ? g.mat[cc - g.Nx + cplane * k] : 0;
+      if (face_coef_t(g, 1, j > 0, cj, ml, m0, mnu, mmu)) {
+        const T cs = A::sub(A::add(A::sub(ux, g.Uz[s]), g.Uz[s + 1]), ux1);
+        g.Fy[s] = A::mul(mnu, face_flux(mmu, g.Fy[s], -dt, cs));
+      }
+    }
+    if (ci && cj) {  // Fz(i,j,k): cells (i,j,k-1), (i,j,k)
+      if (face_coef_t(g, 2, k > 0, ck, m_lo, m0, mnu, mmu)) {
+        const T cs = A::sub(A::add(A::sub(ux, uy), g.Uy[s + 1]), g.Ux[s + g.sx]);
+        g.Fz[s] = A::mul(mnu, face_flux(mmu, g.Fz[s], dt, cs));
+      }
+    }
+    ux = ux1;
+    uy = uy1;
+    m_lo = m0;
   }
 }
 
@@ -353,10 +484,18 @@ __global__ void __launch_bounds__(256) fit_special_post(FitGrid<T> g, SpecialEdg
     T* U = comp_ptr(g.Ux, g.Uy, g.Uz, sp.comp[e]);
     U[sp.slot[e]] = sp.out[e];
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (blockIdx.x == 0) {
+    // fixed-order reduction of the per-block flux partials
+    __shared__ double red[256];
     double acc = 0.0;
-    for (int b = 0; b < nparts; b++) acc = __dadd_rn(acc, sp.flux_part[b]);
-    flux[*step_counter] = __dmul_rn(0.5, acc);
+    for (int b = threadIdx.x; b < nparts; b += blockDim.x) acc = __dadd_rn(acc, sp.flux_part[b]);
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+      if (threadIdx.x < w) red[threadIdx.x] = __dadd_rn(red[threadIdx.x], red[threadIdx.x + w]);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) flux[*step_counter] = __dmul_rn(0.5, red[0]);
   }
 }
 
@@ -399,13 +538,16 @@ void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const Probe
   if (ev) cudaEventRecord(ev[0], st);
   if (sp.n > 0) fit_special_pre<T><<<nsb, 256, 0, st>>>(g, sp, step_counter);
   if (ev) cudaEventRecord(ev[1], st);
-  fit_e_kernel<T><<<grd, blk, 0, st>>>(g);
+  const int kchunk = 16;
+  dim3 mblk(32, 8, 1);
+  dim3 mgrd((unsigned)((g.Nx + 1 + 31) / 32), (unsigned)((g.Ny + 1 + 7) / 8), (unsigned)((g.Nz + 1 + kchunk - 1) / kchunk));
+  fit_e_march<T><<<mgrd, mblk, 0, st>>>(g, kchunk);
   if (ev) cudaEventRecord(ev[2], st);
   fit_special_post<T><<<nsb > 0 ? nsb : 1, 256, 0, st>>>(g, sp, step_counter, flux, nsb);
   if (ev) cudaEventRecord(ev[3], st);
   if (pr.n > 0) fit_probe_kernel<T><<<(pr.n + 127) / 128, 128, 0, st>>>(g, pr, step_counter);
   if (ev) cudaEventRecord(ev[4], st);
-  fit_h_kernel<T><<<grd, blk, 0, st>>>(g, step_counter);
+  fit_h_march<T><<<mgrd, mblk, 0, st>>>(g, kchunk, step_counter);
   if (ev) cudaEventRecord(ev[5], st);
 }
 

@@ -1,0 +1,1181 @@
+// Tetrahedral DGA simulations: host set-up and device runtime.
+//
+// The complex is numbered as TetFIT numbers it (Discretization.hpp:5868-6926):
+// tets, faces and edges sorted lexicographically by their sorted node tuples,
+// so every state vector is already in the reference's order.  Numbering is
+// done with packed 64-bit keys and one sort per entity kind.  The material
+// operators follow ConstructCodecasaMaterialMatrices (Discretization.hpp
+// :8694-9513, dga) and ConstructGFDTDMaterialMatrices (:8132-8692, gfdtd) and
+// are uploaded as CSR; the time loop runs entirely on the device
+// (tet_kernels.cu).  Lossless materials only (sigma = chi = 0).
+#include "tet.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <functional>
+#include <numeric>
+#include <sstream>
+#include <stdexcept>
+
+#include "cuda_util.hpp"
+
+namespace tf {
+
+template <typename T>
+cudaError_t tet_launch_step(const DevPtrs& d, int method, int cg_blocks, cudaStream_t st, cudaEvent_t* ev);
+template <typename T>
+int tet_cg_blocks(int device);
+template <typename T>
+void tet_launch_initial_probes(const DevPtrs& d, cudaStream_t st);
+
+namespace {
+using V3 = std::array<double, 3>;
+V3 sub(const V3& a, const V3& b) { return {a[0] - b[0], a[1] - b[1], a[2] - b[2]}; }
+V3 cross(const V3& a, const V3& b) {
+  return {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+}
+double dot(const V3& a, const V3& b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+V3 scale(const V3& a, double s) { return {a[0] * s, a[1] * s, a[2] * s}; }
+V3 mv(const Mat3& m, const V3& v) {
+  V3 r;
+  for (int i = 0; i < 3; i++) r[i] = m.m[i][0] * v[0] + m.m[i][1] * v[1] + m.m[i][2] * v[2];
+  return r;
+}
+bool is_zero(const Mat3& m) {
+  for (auto& r : m.m)
+    for (double x : r)
+      if (x != 0) return false;
+  return true;
+}
+
+// inverse of a small SPD matrix by Cholesky
+void spd_inv(std::vector<double>& a, int n) {
+  std::vector<double> L(n * n, 0.0), inv(n * n), y(n);
+  for (int k = 0; k < n; k++) {
+    double x = a[k * n + k];
+    for (int j = 0; j < k; j++) x -= L[k * n + j] * L[k * n + j];
+    if (!(x > 0)) throw std::runtime_error("local mass matrix is not positive definite (degenerate element?)");
+    L[k * n + k] = std::sqrt(x);
+    for (int i = k + 1; i < n; i++) {
+      double v = a[i * n + k];
+      for (int j = 0; j < k; j++) v -= L[i * n + j] * L[k * n + j];
+      L[i * n + k] = v / L[k * n + k];
+    }
+  }
+  for (int c = 0; c < n; c++) {
+    for (int i = 0; i < n; i++) {
+      double s = i == c ? 1.0 : 0.0;
+      for (int j = 0; j < i; j++) s -= L[i * n + j] * y[j];
+      y[i] = s / L[i * n + i];
+    }
+    for (int i = n - 1; i >= 0; i--) {
+      double s = y[i];
+      for (int j = i + 1; j < n; j++) s -= L[j * n + i] * inv[j * n + c];
+      inv[i * n + c] = s / L[i * n + i];
+    }
+  }
+  a.swap(inv);
+}
+
+double tridiag_max(const std::vector<double>& a, const std::vector<double>& bf) {
+  const size_t m = a.size();
+  double lo = a[0], hi = a[0];
+  for (size_t i = 0; i < m; i++) {
+    double r = (i > 0 ? std::fabs(bf[i - 1]) : 0) + (i + 1 < m ? std::fabs(bf[i]) : 0);
+    lo = std::fmin(lo, a[i] - r);
+    hi = std::fmax(hi, a[i] + r);
+  }
+  for (int it = 0; it < 200 && hi - lo > 1e-15 * std::fabs(hi); it++) {
+    double x = 0.5 * (lo + hi), d = 1;
+    int below = 0;
+    for (size_t i = 0; i < m; i++) {
+      d = a[i] - x - (i > 0 ? bf[i - 1] * bf[i - 1] / d : 0);
+      if (d == 0) d = 1e-300;
+      if (d < 0) below++;
+    }
+    if (below >= (int)m) hi = x;
+    else lo = x;
+  }
+  return hi;
+}
+}  // namespace
+
+HostCsr HostCsr::build(uint32_t nr, uint32_t nc, std::vector<Trip>& t) {
+  HostCsr m;
+  m.nrows = nr;
+  m.ncols = nc;
+  std::stable_sort(t.begin(), t.end(), [](const Trip& a, const Trip& b) { return a.r != b.r ? a.r < b.r : a.c < b.c; });
+  m.ptr.assign(nr + 1, 0);
+  for (size_t k = 0; k < t.size(); k++) {
+    if (k > 0 && t[k].r == t[k - 1].r && t[k].c == t[k - 1].c) {
+      m.val.back() += t[k].v;
+      continue;
+    }
+    m.col.push_back((int32_t)t[k].c);
+    m.val.push_back(t[k].v);
+    m.ptr[t[k].r + 1]++;
+  }
+  for (uint32_t r = 0; r < nr; r++) m.ptr[r + 1] += m.ptr[r];
+  return m;
+}
+
+void HostCsr::mul(const double* x, double* y) const {
+  for (uint32_t r = 0; r < nrows; r++) {
+    double s = 0;
+    for (int64_t k = ptr[r]; k < ptr[r + 1]; k++) s += val[k] * x[col[k]];
+    y[r] = s;
+  }
+}
+
+// ------------------------------------------------------------------ set-up
+TetSim::TetSim(Script& sc, uint32_t label, const RunOptions& opt) : sc_(sc), opt_(opt), label_(label) {
+  sim_ = sc_.simulations.at(label);
+  out_ = sc_.outputs[sim_.output];
+  out_.initialize();
+  method_ = sim_.method == "dga" ? 1 : 2;
+  src_labels_ = sim_.sources;
+  read_mesh();
+  classify();
+  build_ops();
+  locate_probes();
+  // loop length: i = 1 .. while i dt <= duration (Discretization.hpp:810, 1459)
+  nsteps_ = 0;
+  while ((double)(nsteps_ + 1) * dt_ <= sim_.duration) nsteps_++;
+  // print schedule: dga exports t = 0 and after every step (index i <-> i dt),
+  // gfdtd exports U^{i-1} inside step i (index i-1 <-> (i-1) dt)
+  const uint64_t nsched = method_ == 1 ? nsteps_ + 1 : nsteps_;
+  slot_of_step_.assign(nsched + 1, -1);
+  if (out_.mode == "probepoint") {
+    Output o = out_;
+    for (uint64_t i = 0; i < nsched; i++) {
+      // gfdtd stamps the export of loop step i+1 as current_time - t_step
+      // (Discretization.hpp:1470-1471), which is not always (double)i * dt
+      double t = method_ == 1 ? (double)i * dt_ : (double)(i + 1) * dt_ - dt_;
+      if (o.allow_print(t)) {
+        slot_of_step_[i] = nslots_++;
+        sample_times_.push_back(t);
+      }
+    }
+  }
+  alloc_and_upload();
+}
+
+TetSim::~TetSim() {
+  if (pinned_) cudaFreeHost(pinned_);
+  for (void* p : allocs_) cudaFree(p);
+  if (ev0_) cudaEventDestroy(ev0_);
+  if (ev1_) cudaEventDestroy(ev1_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void TetSim::read_mesh() {
+  // netgen neutral reader (Discretization.hpp:5924-6101)
+  const Mesh& msh = sc_.meshes[sim_.mesh];
+  if (msh.mesher == "gmsh") throw UnsupportedError("gmsh meshes are outside the supported path (use netgen)");
+  std::ifstream fin(msh.file.c_str(), std::ios::binary);
+  if (!fin.is_open()) throw ScriptError("Invalid mesh file name");
+  std::stringstream ss;
+  ss << fin.rdbuf();
+  const std::string buf = ss.str();
+  const char* p = buf.c_str();
+  if (*p < '0' || *p > '9') my_throw(0, "Undefined mesh type! Available: tetrahedral, cartesian");
+  char* end;
+  const uint32_t np = (uint32_t)std::strtoul(p, &end, 10);
+  pts_.resize(np);
+  for (uint32_t i = 0; i < np; i++) {
+    double x = std::strtod(end, &end), y = std::strtod(end, &end), z = std::strtod(end, &end);
+    pts_[i] = {msh.scale * x, msh.scale * y, msh.scale * z};
+  }
+  const uint32_t nt = (uint32_t)std::strtoul(end, &end, 10);
+  std::vector<std::array<int32_t, 5>> tt;  // 4 sorted nodes + material
+  tt.reserve(nt);
+  for (uint32_t i = 0; i < nt; i++) {
+    int32_t m = (int32_t)std::strtoul(end, &end, 10);
+    std::array<int32_t, 4> q;
+    for (int k = 0; k < 4; k++) q[k] = (int32_t)std::strtoul(end, &end, 10) - 1;
+    std::sort(q.begin(), q.end());
+    if (m != 7) tt.push_back({q[0], q[1], q[2], q[3], m});
+  }
+  std::stable_sort(tt.begin(), tt.end(), [](const auto& a, const auto& b) {
+    return std::lexicographical_compare(a.begin(), a.begin() + 4, b.begin(), b.begin() + 4);
+  });
+  const uint32_t L = (uint32_t)tt.size();
+  vols_.resize(L);
+  vol_mat_.resize(L);
+  cell_vol_.resize(L);
+  for (uint32_t k = 0; k < L; k++) {
+    vols_[k] = {tt[k][0], tt[k][1], tt[k][2], tt[k][3]};
+    vol_mat_[k] = (uint32_t)tt[k][4];
+    const auto& t = vols_[k];
+    V3 v1 = sub(pts_[t[1]], pts_[t[0]]), v2 = sub(pts_[t[2]], pts_[t[0]]), v3 = sub(pts_[t[3]], pts_[t[0]]);
+    cell_vol_[k] = dot(v1, cross(v2, v3)) / 6.0;
+    const Material& mt = sc_.materials[vol_mat_[k]];
+    if (!is_zero(mt.sigma) || !is_zero(mt.chi))
+      throw UnsupportedError("lossy materials (sigma or chi) on tetrahedra are outside the supported path");
+  }
+  // faces: packed keys when node ids fit in 21 bits, else tuple order
+  const bool packed = np < (1u << 21);
+  auto fkey = [](int32_t a, int32_t b, int32_t c) {
+    return ((uint64_t)a << 42) | ((uint64_t)b << 21) | (uint64_t)c;
+  };
+  std::vector<std::pair<uint64_t, uint32_t>> fk(4 * (size_t)L);
+  std::vector<std::array<int32_t, 3>> ftup;
+  if (!packed) ftup.resize(4 * (size_t)L);
+  for (uint32_t k = 0; k < L; k++) {
+    const auto& t = vols_[k];
+    const int32_t tri[4][3] = {{t[0], t[1], t[2]}, {t[0], t[1], t[3]}, {t[0], t[2], t[3]}, {t[1], t[2], t[3]}};
+    for (int q = 0; q < 4; q++) {
+      size_t slot = k + (size_t)q * L;
+      fk[slot] = {packed ? fkey(tri[q][0], tri[q][1], tri[q][2]) : slot, (uint32_t)slot};
+      if (!packed) ftup[slot] = {tri[q][0], tri[q][1], tri[q][2]};
+    }
+  }
+  if (packed) std::sort(fk.begin(), fk.end());
+  else
+    std::stable_sort(fk.begin(), fk.end(), [&](const auto& a, const auto& b) { return ftup[a.first] < ftup[b.first]; });
+  std::vector<int32_t> flab(4 * (size_t)L);
+  auto face_tuple = [&](size_t slot) -> std::array<int32_t, 3> {
+    uint32_t k = (uint32_t)(slot % L);
+    int q = (int)(slot / L);
+    const auto& t = vols_[k];
+    const int32_t tri[4][3] = {{t[0], t[1], t[2]}, {t[0], t[1], t[3]}, {t[0], t[2], t[3]}, {t[1], t[2], t[3]}};
+    return {tri[q][0], tri[q][1], tri[q][2]};
+  };
+  for (size_t q = 0; q < fk.size(); q++) {
+    auto tup = face_tuple(fk[q].second);
+    if (faces_.empty() || faces_.back() != tup) faces_.push_back(tup);
+    flab[fk[q].second] = (int32_t)faces_.size() - 1;
+  }
+  fk.clear();
+  fk.shrink_to_fit();
+  const uint32_t NF = (uint32_t)faces_.size();
+  ftv_.assign(NF, {-1, -1});
+  vtf_.resize(L);
+  for (uint32_t k = 0; k < L; k++) {
+    const int32_t f0 = flab[k], f1 = flab[k + L], f2 = flab[k + 2 * (size_t)L], f3 = flab[k + 3 * (size_t)L];
+    for (int32_t f : {f0, f1, f2, f3}) {
+      if (ftv_[f][0] < 0) ftv_[f][0] = (int32_t)k;
+      else ftv_[f][1] = (int32_t)k;
+    }
+    vtf_[k] = {f3, f2, f1, f0};  // opposite nodes 0..3 (Discretization.hpp:6239-6267)
+  }
+  // edges
+  std::vector<uint64_t> ek(3 * (size_t)NF);
+  for (uint32_t f = 0; f < NF; f++) {
+    const auto& s = faces_[f];
+    ek[f] = ((uint64_t)s[0] << 32) | (uint32_t)s[1];
+    ek[f + NF] = ((uint64_t)s[0] << 32) | (uint32_t)s[2];
+    ek[f + 2 * (size_t)NF] = ((uint64_t)s[1] << 32) | (uint32_t)s[2];
+  }
+  std::vector<uint64_t> eu(ek);
+  std::sort(eu.begin(), eu.end());
+  eu.erase(std::unique(eu.begin(), eu.end()), eu.end());
+  edges_.resize(eu.size());
+  for (size_t e = 0; e < eu.size(); e++) edges_[e] = {(int32_t)(eu[e] >> 32), (int32_t)(eu[e] & 0xffffffffu)};
+  auto eid = [&](uint64_t key) { return (int32_t)(std::lower_bound(eu.begin(), eu.end(), key) - eu.begin()); };
+  fte_.resize(NF);
+  for (uint32_t f = 0; f < NF; f++) fte_[f] = {eid(ek[f]), eid(ek[f + NF]), eid(ek[f + 2 * (size_t)NF])};
+  const uint32_t NE = (uint32_t)edges_.size();
+  // node stars (edges ascending) and node -> tets (ascending)
+  star_ptr_.assign(np + 1, 0);
+  for (auto& e : edges_) { star_ptr_[e[0] + 1]++; star_ptr_[e[1] + 1]++; }
+  for (uint32_t i = 0; i < np; i++) star_ptr_[i + 1] += star_ptr_[i];
+  star_edge_.resize(star_ptr_[np]);
+  {
+    std::vector<int64_t> pos(star_ptr_.begin(), star_ptr_.end() - 1);
+    for (uint32_t e = 0; e < NE; e++) {
+      star_edge_[pos[edges_[e][0]]++] = (int32_t)e;
+      star_edge_[pos[edges_[e][1]]++] = (int32_t)e;
+    }
+  }
+  nvol_ptr_.assign(np + 1, 0);
+  for (auto& t : vols_)
+    for (int32_t n : t) nvol_ptr_[n + 1]++;
+  for (uint32_t i = 0; i < np; i++) nvol_ptr_[i + 1] += nvol_ptr_[i];
+  nvol_.resize(nvol_ptr_[np]);
+  {
+    std::vector<int64_t> pos(nvol_ptr_.begin(), nvol_ptr_.end() - 1);
+    for (uint32_t k = 0; k < L; k++)
+      for (int32_t n : vols_[k]) nvol_[pos[n]++] = (int32_t)k;
+  }
+  // C^T: edge -> faces ascending, sign in bit 31
+  {
+    std::vector<HostCsr::Trip> t;
+    t.reserve(3 * (size_t)NF);
+    for (uint32_t f = 0; f < NF; f++) {
+      t.push_back({(uint32_t)fte_[f][0], f, 1.0});
+      t.push_back({(uint32_t)fte_[f][1], f, -1.0});
+      t.push_back({(uint32_t)fte_[f][2], f, 1.0});
+    }
+    Ct_ = HostCsr::build(NE, NF, t);
+  }
+  // boundary faces and their dual edges (Discretization.hpp:6380-6489)
+  bnd_edge_.assign(NE, -1);
+  auto fbar = [&](uint32_t f) {
+    const auto &a = pts_[faces_[f][0]], &b = pts_[faces_[f][1]], &c = pts_[faces_[f][2]];
+    return V3{(a[0] + b[0] + c[0]) / 3.0, (a[1] + b[1] + c[1]) / 3.0, (a[2] + b[2] + c[2]) / 3.0};
+  };
+  auto vbar = [&](int32_t v) {
+    V3 r{0, 0, 0};
+    for (int q = 0; q < 4; q++)
+      for (int a = 0; a < 3; a++) r[a] += pts_[vols_[v][q]][a];
+    return V3{r[0] / 4.0, r[1] / 4.0, r[2] / 4.0};
+  };
+  for (uint32_t f = 0; f < NF; f++) {
+    if (ftv_[f][0] < 0) throw std::invalid_argument("Conductor boundary cannot be on mesh boundary!");
+    if (ftv_[f][1] >= 0) continue;
+    for (int32_t e : fte_[f]) {
+      if (bnd_edge_[e] < 0) {
+        bnd_edge_[e] = (int32_t)bnd_dual_.size();
+        bnd_dual_.push_back(fbar(f));
+      } else {
+        V3& bd = bnd_dual_[bnd_edge_[e]];
+        bd = sub(fbar(f), bd);
+        V3 ev = sub(pts_[edges_[e][1]], pts_[edges_[e][0]]);
+        V3 fv = cross(sub(pts_[faces_[f][1]], pts_[faces_[f][0]]), sub(pts_[faces_[f][2]], pts_[faces_[f][0]]));
+        if (dot(fv, sub(vbar(ftv_[f][0]), fbar(f))) >= 0) fv = scale(fv, -1);
+        if (dot(cross(ev, fv), bd) > 0) bd = scale(bd, -1);
+        bd = scale(bd, -1);
+      }
+    }
+  }
+  // boundary triangles: PEC and source surfaces (Discretization.hpp:6612-6754)
+  const uint32_t ntri = (uint32_t)std::strtoul(end, &end, 10);
+  std::vector<uint32_t> edge_bc(NE, 0);
+  pec_.assign(NE, 0);
+  edge_src_.assign(NE, {});
+  for (uint32_t i = 0; i < ntri; i++) {
+    uint32_t bid = (uint32_t)std::strtoul(end, &end, 10);
+    std::array<int32_t, 3> s;
+    for (int k = 0; k < 3; k++) s[k] = (int32_t)std::strtoul(end, &end, 10) - 1;
+    std::sort(s.begin(), s.end());
+    auto it = std::lower_bound(faces_.begin(), faces_.end(), s);
+    if (it == faces_.end() || *it != s) continue;
+    const uint32_t f = (uint32_t)(it - faces_.begin());
+    const uint32_t which = bid < 100 ? sc_.bnd_to_bc[bid] : 0;
+    if (which != 0) {
+      auto bc = sc_.bcs.find(which);
+      if (bc != sc_.bcs.end() && bc->second.type == "pec")
+        for (int32_t e : fte_[f]) {
+          edge_bc[e] = which;
+          edge_src_[e].clear();
+          pec_[e] = 1;
+          if (bnd_edge_[e] >= 0) {
+            bnd_dual_[bnd_edge_[e]] = {0, 0, 0};
+            bnd_edge_[e] = -1;
+          }
+        }
+    } else {
+      for (uint32_t sl : src_labels_) {
+        Source& src = sc_.sources[sl];
+        if (std::find(src.surfaces.begin(), src.surfaces.end(), bid) == src.surfaces.end() || src.st == "b") continue;
+        for (int32_t e : fte_[f])
+          if (!pec_[e] && std::find(edge_src_[e].begin(), edge_src_[e].end(), sl) == edge_src_[e].end())
+            edge_src_[e].push_back(sl);
+      }
+    }
+  }
+}
+
+void TetSim::classify() {
+  // source consistency filter and edge classes (Discretization.hpp:6758-6859)
+  const uint32_t NE = (uint32_t)edges_.size();
+  cls_.assign(NE, 1);
+  for (uint32_t e = 0; e < NE; e++) {
+    auto& es = edge_src_[e];
+    if (!es.empty()) {
+      const Source& f = sc_.sources[es[0]];
+      uint32_t fs = f.surfaces.empty() ? 0 : f.surfaces[0];
+      std::vector<uint32_t> keep;
+      for (uint32_t s : es) {
+        const Source& x = sc_.sources[s];
+        if (x.st == f.st && (x.surfaces.empty() ? 0 : x.surfaces[0]) == fs) keep.push_back(s);
+      }
+      es.swap(keep);
+    }
+    bool dir = pec_[e] != 0;
+    for (uint32_t s : es)
+      if (sc_.sources[s].st == "e") dir = true;
+    if (dir) cls_[e] = 4;
+  }
+}
+
+std::array<int32_t, 6> TetSim::vol_edges(uint32_t v) const {
+  // local order ab, bc, ac, ad, bd, cd: the sorted edges of the tet after
+  // the reference's two swaps (Discretization.hpp:10309-10314)
+  std::array<int32_t, 6> es;
+  int n = 0;
+  for (int q = 0; q < 4; q++)
+    for (int32_t e : fte_[vtf_[v][q]]) {
+      bool seen = false;
+      for (int k = 0; k < n; k++) seen = seen || es[k] == e;
+      if (!seen) es[n++] = e;
+    }
+  std::sort(es.begin(), es.end());
+  std::swap(es[1], es[2]);
+  std::swap(es[1], es[3]);
+  return es;
+}
+
+void TetSim::build_ops() {
+  const uint32_t NE = (uint32_t)edges_.size(), NF = (uint32_t)faces_.size(), L = (uint32_t)vols_.size();
+  auto ebar = [&](int32_t e) {
+    const auto &a = pts_[edges_[e][0]], &b = pts_[edges_[e][1]];
+    return V3{0.5 * (a[0] + b[0]), 0.5 * (a[1] + b[1]), 0.5 * (a[2] + b[2])};
+  };
+  auto fbar = [&](int32_t f) {
+    const auto &a = pts_[faces_[f][0]], &b = pts_[faces_[f][1]], &c = pts_[faces_[f][2]];
+    return V3{(a[0] + b[0] + c[0]) / 3.0, (a[1] + b[1] + c[1]) / 3.0, (a[2] + b[2] + c[2]) / 3.0};
+  };
+  // N = sum of per-tet inverse magnetic blocks (Discretization.hpp:8754-8807, 9158-9255)
+  {
+    std::vector<HostCsr::Trip> t;
+    t.reserve(16 * (size_t)L);
+    for (uint32_t v = 0; v < L; v++) {
+      auto es = vol_edges(v);
+      V3 eb[6], fb[4];
+      for (int i = 0; i < 6; i++) eb[i] = ebar(es[i]);
+      for (int i = 0; i < 4; i++) fb[i] = fbar(vtf_[v][i]);
+      V3 vb{0, 0, 0};
+      for (int q = 0; q < 4; q++)
+        for (int a = 0; a < 3; a++) vb[a] += pts_[vols_[v][q]][a];
+      vb = {vb[0] / 4.0, vb[1] / 4.0, vb[2] / 4.0};
+      const double sgn = cell_vol_[v] < 0 ? -0.5 : 0.5;
+      const V3 fv[6] = {scale(cross(sub(vb, eb[0]), sub(fb[2], fb[3])), sgn),
+                        scale(cross(sub(vb, eb[1]), sub(fb[0], fb[3])), sgn),
+                        scale(cross(sub(vb, eb[2]), sub(fb[3], fb[1])), sgn),
+                        scale(cross(sub(vb, eb[3]), sub(fb[1], fb[2])), sgn),
+                        scale(cross(sub(vb, eb[4]), sub(fb[2], fb[0])), sgn),
+                        scale(cross(sub(vb, eb[5]), sub(fb[0], fb[1])), sgn)};
+      const Mat3& mu = sc_.materials.at(vol_mat_[v]).mu;
+      auto d = [&](int a, int b) { return dot(fv[a], mv(mu, fv[b])); };
+      const double c = 36.0 / std::fabs(cell_vol_[v]);
+      std::vector<double> M = {(d(0, 0) + d(2, 2) + d(3, 3)) * c, (-d(1, 2) - d(3, 4)) * c,
+                               (-d(0, 1) + d(3, 5)) * c,          (d(0, 4) + d(2, 5)) * c,
+                               0, (d(0, 0) + d(1, 1) + d(4, 4)) * c, (-d(0, 2) - d(4, 5)) * c, (d(0, 3) - d(1, 5)) * c,
+                               0, 0, (d(1, 1) + d(2, 2) + d(5, 5)) * c, (-d(2, 3) - d(1, 4)) * c,
+                               0, 0, 0, (d(3, 3) + d(4, 4) + d(5, 5)) * c};
+      for (int i = 0; i < 4; i++)
+        for (int j = 0; j < i; j++) M[4 * i + j] = M[4 * j + i];
+      spd_inv(M, 4);
+      for (int j = 0; j < 4; j++)
+        for (int k = 0; k < 4; k++)
+          if (M[4 * j + k] != 0) t.push_back({(uint32_t)vtf_[v][j], (uint32_t)vtf_[v][k], M[4 * j + k]});
+    }
+    N_ = HostCsr::build(NF, NF, t);
+  }
+  auto primal_area = [&](uint32_t v) {
+    const auto& n = vols_[v];
+    V3 e[6] = {sub(pts_[n[1]], pts_[n[0]]), sub(pts_[n[2]], pts_[n[1]]), sub(pts_[n[2]], pts_[n[0]]),
+               sub(pts_[n[3]], pts_[n[0]]), sub(pts_[n[3]], pts_[n[1]]), sub(pts_[n[3]], pts_[n[2]])};
+    return std::array<V3, 4>{scale(cross(e[1], e[4]), 0.5), scale(cross(e[2], e[3]), 0.5),
+                             scale(cross(e[0], e[3]), 0.5), scale(cross(e[0], e[2]), 0.5)};
+  };
+  // node -> local position of the three incident tet edges
+  static const int kEd[4][3] = {{0, 2, 3}, {0, 1, 4}, {1, 2, 5}, {3, 4, 5}};
+  if (method_ == 1) {
+    // node-star eps-matrices (Discretization.hpp:8856-9123) and their inverses
+    static const int kFv[4][3] = {{1, 2, 3}, {0, 2, 3}, {1, 0, 3}, {0, 1, 2}};
+    static const double kSg[4][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {1, 1, 1}};
+    static const int kVtfSign[4] = {1, -1, 1, -1};  // vtf signs (Discretization.hpp:6239-6267)
+    std::vector<HostCsr::Trip> einv_t, h_t;
+    for (uint32_t nid = 0; nid < pts_.size(); nid++) {
+      const int64_t b0 = star_ptr_[nid];
+      const int n = (int)(star_ptr_[nid + 1] - b0);
+      std::vector<double> E(n * n, 0.0);
+      for (int64_t q = nvol_ptr_[nid]; q < nvol_ptr_[nid + 1]; q++) {
+        const int32_t vv = nvol_[q];
+        auto el = vol_edges(vv);
+        auto fv = primal_area(vv);
+        const double V = std::fabs(cell_vol_[vv]);
+        const Mat3& eps = sc_.materials.at(vol_mat_[vv]).eps;
+        int k = 0;
+        while (vols_[vv][k] != (int32_t)nid) k++;
+        int li[3];
+        V3 w[3];
+        for (int a = 0; a < 3; a++) {
+          li[a] = (int)(std::lower_bound(star_edge_.begin() + b0, star_edge_.begin() + b0 + n, el[kEd[k][a]]) -
+                        (star_edge_.begin() + b0));
+          w[a] = scale(fv[kFv[k][a]], kSg[k][a] * 2.0 / 3.0 / V * kVtfSign[kFv[k][a]]);
+        }
+        for (int a = 0; a < 3; a++)
+          for (int b = a; b < 3; b++) {
+            double val = dot(w[a], mv(eps, w[b])) * V / 4;
+            E[li[a] * n + li[b]] += val;
+            if (a != b) E[li[b] * n + li[a]] = E[li[a] * n + li[b]];
+          }
+      }
+      std::vector<double> Hl = E;
+      spd_inv(Hl, n);
+      for (int j = 0; j < n; j++)
+        for (int k = j; k < n; k++)
+          if (Hl[j * n + k] != 0) {
+            einv_t.push_back({(uint32_t)star_edge_[b0 + j], (uint32_t)star_edge_[b0 + k], Hl[j * n + k]});
+            if (j != k) einv_t.push_back({(uint32_t)star_edge_[b0 + k], (uint32_t)star_edge_[b0 + j], Hl[j * n + k]});
+          }
+      // masked inverse (Discretization.hpp:9263-9333)
+      for (int j = 0; j < n; j++)
+        if (cls_[star_edge_[b0 + j]] == 4) {
+          for (int k = 0; k < n; k++) E[j * n + k] = E[k * n + j] = 0;
+          E[j * n + j] = 1;
+        }
+      spd_inv(E, n);
+      for (int j = 0; j < n; j++) {
+        const int32_t ej = star_edge_[b0 + j];
+        if (cls_[ej] != 1) continue;
+        for (int k = j; k < n; k++) {
+          const int32_t ek = star_edge_[b0 + k];
+          if (cls_[ek] == 4 || E[j * n + k] == 0) continue;
+          h_t.push_back({(uint32_t)ej, (uint32_t)ek, E[j * n + k]});
+          if (j != k) h_t.push_back({(uint32_t)ek, (uint32_t)ej, E[j * n + k]});
+        }
+      }
+    }
+    HostCsr Einv = HostCsr::build(NE, NE, einv_t);
+    H_ = HostCsr::build(NE, NE, h_t);
+    dt_est_ = sim_.courant * estimate_dt(Einv, false);
+  } else {
+    // gfdtd eps-mass from the node dual bases (Discretization.hpp:8357-8621)
+    std::vector<HostCsr::Trip> t;
+    for (uint32_t nid = 0; nid < pts_.size(); nid++)
+      for (int64_t q = nvol_ptr_[nid]; q < nvol_ptr_[nid + 1]; q++) {
+        const int32_t vv = nvol_[q];
+        auto el = vol_edges(vv);
+        const double om = std::fabs(cell_vol_[vv]) / 4.0;
+        const Mat3& eps = sc_.materials.at(vol_mat_[vv]).eps;
+        int k = 0;
+        while (vols_[vv][k] != (int32_t)nid) k++;
+        int32_t e[3] = {el[kEd[k][0]], el[kEd[k][1]], el[kEd[k][2]]};
+        V3 a1 = sub(ebar(e[0]), pts_[nid]), a2 = sub(ebar(e[1]), pts_[nid]), a3 = sub(ebar(e[2]), pts_[nid]);
+        const double nc = std::pow(dot(a1, cross(a2, a3)), -1);
+        const V3 f[3] = {scale(cross(a2, a3), nc), scale(cross(a3, a1), nc), scale(cross(a1, a2), nc)};
+        Mat3 oe;
+        for (int i = 0; i < 3; i++)
+          for (int j = 0; j < 3; j++) oe.m[i][j] = om * eps.m[i][j];
+        // reference form: half-edge duals, no 1/4, no orientation signs;
+        // consistent form: both applied
+        double sg[3] = {1, 1, 1}, quarter = 1;
+        if (opt_.consistent_mass) {
+          for (int a = 0; a < 3; a++) sg[a] = edges_[e[a]][1] == (int32_t)nid ? -1.0 : 1.0;
+          quarter = 0.25;
+        }
+        static const int kPair[9][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {1, 0}, {0, 2}, {2, 0}, {1, 2}, {2, 1}};
+        for (auto& pq : kPair)
+          t.push_back({(uint32_t)e[pq[0]], (uint32_t)e[pq[1]],
+                       quarter * sg[pq[0]] * sg[pq[1]] * dot(f[pq[0]], mv(oe, f[pq[1]]))});
+      }
+    E_ = HostCsr::build(NE, NE, t);
+    std::vector<int32_t> fidx(NE, -1);
+    for (uint32_t e = 0; e < NE; e++) {
+      if (cls_[e] != 4) {
+        fidx[e] = (int32_t)free_edges_.size();
+        free_edges_.push_back((int32_t)e);
+      } else {
+        dir_edges_.push_back((int32_t)e);
+      }
+    }
+    std::vector<HostCsr::Trip> at, rt;
+    for (uint32_t r = 0; r < NE; r++) {
+      if (fidx[r] < 0) continue;
+      for (int64_t k = E_.ptr[r]; k < E_.ptr[r + 1]; k++) {
+        const int32_t c = E_.col[k];
+        if (fidx[c] < 0) rt.push_back({(uint32_t)fidx[r], (uint32_t)c, E_.val[k]});
+        else at.push_back({(uint32_t)fidx[r], (uint32_t)fidx[c], E_.val[k]});
+      }
+    }
+    const uint32_t nf = (uint32_t)free_edges_.size();
+    A_ = HostCsr::build(nf, nf, at);
+    R_ = HostCsr::build(nf, NE, rt);
+    jacobi_.resize(nf);
+    for (uint32_t i = 0; i < nf; i++) {
+      double dg = 0;
+      for (int64_t k = A_.ptr[i]; k < A_.ptr[i + 1]; k++)
+        if (A_.col[k] == (int32_t)i) dg = A_.val[k];
+      jacobi_[i] = dg != 0 ? 1.0 / dg : 1.0;  // ConjugateGradientSolver.hpp:119-127
+    }
+    dt_est_ = sim_.courant * estimate_dt(E_, true);
+  }
+  dt_ = dt_est_;
+  if (sim_.step != 0) {  // Discretization.hpp:9146-9153, 8634-8641
+    if (sim_.step > dt_) unstable_ = true;
+    else dt_ = sim_.step;
+  }
+}
+
+// Largest eigenvalue of Minv K (dga, Minv = node-star inverses) or of the
+// pencil K x = lambda E x (gfdtd), K = C^T N C, by Lanczos in the K inner
+// product; dt = 2 / sqrt(lambda).  Meshes above 3 M edges with a pinned step
+// skip the estimate and take the step as given.
+double TetSim::estimate_dt(const HostCsr& M, bool generalized) {
+  const size_t n = edges_.size(), nf = faces_.size();
+  if (sim_.step != 0 && n > 3000000) return sim_.step / sim_.courant;
+  std::vector<double> cu(nf), ncu(nf);
+  auto K = [&](const double* x, double* y) {
+    for (size_t f = 0; f < nf; f++) cu[f] = x[fte_[f][0]] - x[fte_[f][1]] + x[fte_[f][2]];
+    N_.mul(cu.data(), ncu.data());
+    for (size_t e = 0; e < n; e++) {
+      double s = 0;
+      for (int64_t k = Ct_.ptr[e]; k < Ct_.ptr[e + 1]; k++) s += Ct_.val[k] * ncu[Ct_.col[k]];
+      y[e] = s;
+    }
+  };
+  std::vector<double> pre(n), r(n), z(n), p(n), q(n);
+  if (generalized)
+    for (size_t i = 0; i < n; i++) {
+      double dg = 0;
+      for (int64_t k = M.ptr[i]; k < M.ptr[i + 1]; k++)
+        if (M.col[k] == (int32_t)i) dg = M.val[k];
+      pre[i] = dg != 0 ? 1.0 / dg : 1.0;
+    }
+  auto Minv = [&](const double* x, double* y) {
+    if (!generalized) {
+      M.mul(x, y);
+      return;
+    }
+    // y = E^-1 x by Jacobi-PCG from zero
+    std::fill(y, y + n, 0.0);
+    double rr0 = 0, rz = 0;
+    for (size_t i = 0; i < n; i++) { r[i] = x[i]; rr0 += r[i] * r[i]; z[i] = pre[i] * r[i]; rz += r[i] * z[i]; p[i] = z[i]; }
+    for (int it = 0; it < 1000 && rr0 > 0; it++) {
+      M.mul(p.data(), q.data());
+      double pq = 0;
+      for (size_t i = 0; i < n; i++) pq += p[i] * q[i];
+      double a = rz / pq, rr = 0, rz2 = 0;
+      for (size_t i = 0; i < n; i++) { y[i] += a * p[i]; r[i] -= a * q[i]; rr += r[i] * r[i]; z[i] = pre[i] * r[i]; rz2 += r[i] * z[i]; }
+      if (std::sqrt(rr / rr0) < 1e-12) break;
+      for (size_t i = 0; i < n; i++) p[i] = z[i] + rz2 / rz * p[i];
+      rz = rz2;
+    }
+  };
+  std::vector<double> x(n), v(n), Kv(n), w(n), Kw(n), vp(n, 0.0);
+  uint64_t s = 0x2545F4914F6CDD1Dull;
+  for (size_t i = 0; i < n; i++) {
+    s ^= s << 13; s ^= s >> 7; s ^= s << 17;
+    x[i] = (double)(s >> 11) / 9007199254740992.0 - 0.5;
+  }
+  K(x.data(), Kv.data());
+  Minv(Kv.data(), v.data());
+  K(v.data(), Kv.data());
+  double nrm = 0;
+  for (size_t i = 0; i < n; i++) nrm += v[i] * Kv[i];
+  nrm = std::sqrt(nrm);
+  for (size_t i = 0; i < n; i++) { v[i] /= nrm; Kv[i] /= nrm; }
+  std::vector<double> al, be;
+  double beta = 0, last = 0, lam = 0;
+  for (int it = 0; it < 400; it++) {
+    Minv(Kv.data(), w.data());
+    double alpha = 0;
+    for (size_t i = 0; i < n; i++) alpha += w[i] * Kv[i];
+    for (size_t i = 0; i < n; i++) w[i] -= alpha * v[i] + beta * vp[i];
+    al.push_back(alpha);
+    K(w.data(), Kw.data());
+    double nb = 0;
+    for (size_t i = 0; i < n; i++) nb += w[i] * Kw[i];
+    nb = nb > 0 ? std::sqrt(nb) : 0;
+    if (it % 10 == 9 || nb == 0 || it == 399) {
+      lam = tridiag_max(al, be);
+      if (nb == 0 || std::fabs(lam - last) <= 1e-9 * std::fabs(lam)) break;
+      last = lam;
+    }
+    be.push_back(nb);
+    beta = nb;
+    vp.swap(v);
+    for (size_t i = 0; i < n; i++) { v[i] = w[i] / nb; Kv[i] = Kw[i] / nb; }
+  }
+  return 2.0 / std::sqrt(lam);
+}
+
+void TetSim::locate_probes() {
+  // FindProbe (Discretization.hpp:3645-3747)
+  auto det4 = [](const double m[4][4]) {
+    double a = m[2][2] * m[3][3] - m[2][3] * m[3][2], b = m[2][1] * m[3][3] - m[2][3] * m[3][1];
+    double c = m[2][1] * m[3][2] - m[2][2] * m[3][1], d = m[2][0] * m[3][3] - m[2][3] * m[3][0];
+    double e = m[2][0] * m[3][2] - m[2][2] * m[3][0], f = m[2][0] * m[3][1] - m[2][1] * m[3][0];
+    return m[0][0] * (m[1][1] * a - m[1][2] * b + m[1][3] * c) - m[0][1] * (m[1][0] * a - m[1][2] * d + m[1][3] * e) +
+           m[0][2] * (m[1][0] * b - m[1][1] * d + m[1][3] * f) - m[0][3] * (m[1][0] * c - m[1][1] * e + m[1][2] * f);
+  };
+  const uint32_t L = (uint32_t)vols_.size();
+  std::vector<uint8_t> colour(L, 0);
+  std::vector<uint32_t> touched;
+  uint32_t root = 0;
+  auto find = [&](const std::array<double, 3>& pv) -> int64_t {
+    for (uint32_t t : touched) colour[t] = 0;
+    touched.clear();
+    std::vector<uint32_t> q{root};
+    colour[0] = 1;
+    touched.push_back(0);
+    const double tol = 1e-12;
+    for (size_t h = 0; h < q.size(); h++) {
+      const uint32_t v = q[h];
+      double rows[4][4];
+      for (int r = 0; r < 4; r++) {
+        for (int a = 0; a < 3; a++) rows[r][a] = pts_[vols_[v][r]][a];
+        rows[r][3] = 1;
+      }
+      const double d0 = det4(rows);
+      bool ok = true;
+      for (int r = 0; r < 4 && ok; r++) {
+        double m[4][4];
+        std::memcpy(m, rows, sizeof(m));
+        for (int a = 0; a < 3; a++) m[r][a] = pv[a];
+        const double d1 = det4(m);
+        ok = (d0 >= -tol && d1 >= -tol) || (d0 <= tol && d1 <= tol);
+      }
+      if (ok) {
+        root = v;
+        return v;
+      }
+      for (int32_t f : vtf_[v]) {
+        int32_t n = ftv_[f][0];
+        if (n == (int32_t)v) n = ftv_[f][1] >= 0 ? ftv_[f][1] : n;
+        if (!colour[n]) {
+          colour[n] = 1;
+          touched.push_back(n);
+          q.push_back(n);
+        }
+      }
+      if (!colour[v]) { colour[v] = 1; touched.push_back(v); }
+    }
+    return -1;
+  };
+  if (out_.mode == "probepoint") {
+    for (auto& pv : out_.probes) {
+      int64_t v = find(pv);
+      if (v < 0) continue;
+      probe_tet_.push_back((int32_t)v);
+      probe_pts_.push_back(pv);
+      // Whitney weights: lambda = [x 1] G with G the inverse of the node matrix
+      double W[4][8];
+      for (int i = 0; i < 4; i++) {
+        for (int a = 0; a < 3; a++) W[i][a] = pts_[vols_[v][i]][a];
+        W[i][3] = 1;
+        for (int j = 0; j < 4; j++) W[i][4 + j] = i == j ? 1.0 : 0.0;
+      }
+      for (int c = 0; c < 4; c++) {
+        int piv = c;
+        for (int r = c + 1; r < 4; r++)
+          if (std::fabs(W[r][c]) > std::fabs(W[piv][c])) piv = r;
+        for (int j = 0; j < 8; j++) std::swap(W[c][j], W[piv][j]);
+        const double dd = W[c][c];
+        for (int j = 0; j < 8; j++) W[c][j] /= dd;
+        for (int r = 0; r < 4; r++)
+          if (r != c) {
+            const double fct = W[r][c];
+            for (int j = 0; j < 8; j++) W[r][j] -= fct * W[c][j];
+          }
+      }
+      double lam[4], grad[4][3];
+      for (int i = 0; i < 4; i++) {
+        lam[i] = pv[0] * W[0][4 + i] + pv[1] * W[1][4 + i] + pv[2] * W[2][4 + i] + W[3][4 + i];
+        for (int a = 0; a < 3; a++) grad[i][a] = W[a][4 + i];
+      }
+      static const int kE[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
+      for (int q = 0; q < 6; q++)
+        for (int a = 0; a < 3; a++)
+          probe_we_.push_back(lam[kE[q][0]] * grad[kE[q][1]][a] - lam[kE[q][1]] * grad[kE[q][0]][a]);
+      // H = 1/4 mu^-1 (sum of face-flux weighted primal edge combinations)/(3 V)
+      // (GetMagneticField, Discretization.hpp:3877-3897)
+      const auto& n = vols_[v];
+      V3 pev[6] = {sub(pts_[n[1]], pts_[n[0]]), sub(pts_[n[2]], pts_[n[1]]), sub(pts_[n[2]], pts_[n[0]]),
+                   sub(pts_[n[3]], pts_[n[0]]), sub(pts_[n[3]], pts_[n[1]]), sub(pts_[n[3]], pts_[n[2]])};
+      const double vv = 3 * cell_vol_[v];
+      const Mat3& mu = sc_.materials.at(vol_mat_[v]).mu;
+      V3 hq[4];
+      for (int a = 0; a < 3; a++) {
+        hq[0][a] = pev[0][a] + pev[2][a] + pev[3][a];
+        hq[1][a] = pev[0][a] - pev[1][a] - pev[4][a];
+        hq[2][a] = -pev[2][a] - pev[1][a] + pev[5][a];
+        hq[3][a] = pev[3][a] + pev[4][a] + pev[5][a];
+      }
+      for (int q = 0; q < 4; q++)
+        for (int a = 0; a < 3; a++) probe_hf_.push_back(0.25 * (1.0 / mu.m[a][a]) * hq[q][a] / vv);
+    }
+    // current dipoles: nearest edge of the star of the tet's first node
+    // (Discretization.hpp:436-464)
+    for (uint32_t sl : src_labels_) {
+      Source& s = sc_.sources[sl];
+      if (s.st != "j") continue;
+      int64_t v = find(s.location);
+      if (v < 0) continue;
+      const int32_t node = vols_[v][0];
+      int32_t best = -1;
+      double bd = 0;
+      for (int64_t q = star_ptr_[node]; q < star_ptr_[node + 1]; q++) {
+        const int32_t e = star_edge_[q];
+        const auto &a = pts_[edges_[e][0]], &b = pts_[edges_[e][1]];
+        V3 d{0.5 * (a[0] + b[0]) - s.location[0], 0.5 * (a[1] + b[1]) - s.location[1],
+             0.5 * (a[2] + b[2]) - s.location[2]};
+        const double dd = std::sqrt(dot(d, d));
+        if (best < 0 || dd < bd) { bd = dd; best = e; }
+      }
+      edge_src_[best].push_back(sl);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ device
+template <typename T>
+static std::vector<T> as(const std::vector<double>& v) {
+  return std::vector<T>(v.begin(), v.end());
+}
+
+void TetSim::alloc_and_upload() {
+  CU(cudaSetDevice(opt_.device));
+  int major = 0;
+  CU(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, opt_.device));
+  if (major != 10) throw CudaError("device " + std::to_string(opt_.device) + " is not an sm_100 (B200) GPU");
+  CU(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  CU(cudaEventCreate(&ev0_));
+  CU(cudaEventCreate(&ev1_));
+  const bool f32 = opt_.precision == 1;
+  const size_t es = f32 ? 4 : 8;
+  auto dalloc = [&](size_t bytes) -> void* {
+    void* p = nullptr;
+    CU(cudaMalloc(&p, bytes ? bytes : 16));
+    allocs_.push_back(p);
+    dev_bytes_ += bytes;
+    return p;
+  };
+  auto up = [&](const void* h, size_t bytes) -> void* {
+    void* p = dalloc(bytes);
+    if (bytes) CU(cudaMemcpyAsync(p, h, bytes, cudaMemcpyHostToDevice, stream_));
+    return p;
+  };
+  auto upT = [&](const std::vector<double>& v) -> void* {
+    if (!f32) return up(v.data(), v.size() * 8);
+    auto f = as<float>(v);
+    void* p = up(f.data(), f.size() * 4);
+    CU(cudaStreamSynchronize(stream_));
+    return p;
+  };
+  auto zeros = [&](size_t n) -> void* {
+    void* p = dalloc(n * es);
+    CU(cudaMemsetAsync(p, 0, n * es, stream_));
+    return p;
+  };
+  DevPtrs& d = dp_;
+  const size_t NE = edges_.size(), NF = faces_.size();
+  d.nE = (int)NE;
+  d.nF = (int)NF;
+  d.dt = dt_;
+  d.U = zeros(NE); d.F = zeros(NF); d.B = zeros(NF); d.cu = zeros(NF); d.cf = zeros(NE);
+  d.I = zeros(NE); d.cb = zeros(NE); d.src = zeros(NE);
+  d.fte = (const int32_t*)up(fte_.data(), NF * 3 * 4);
+  {
+    std::vector<int32_t> cc(Ct_.col.size());
+    for (size_t k = 0; k < cc.size(); k++) cc[k] = Ct_.val[k] < 0 ? (int32_t)((uint32_t)Ct_.col[k] | 0x80000000u) : Ct_.col[k];
+    d.ct_ptr = (const int64_t*)up(Ct_.ptr.data(), Ct_.ptr.size() * 8);
+    d.ct_col = (const int32_t*)up(cc.data(), cc.size() * 4);
+  }
+  auto upcsr = [&](const HostCsr& m, const int64_t*& ptr, const int32_t*& col, const void*& val) {
+    ptr = (const int64_t*)up(m.ptr.data(), m.ptr.size() * 8);
+    col = (const int32_t*)up(m.col.data(), m.col.size() * 4);
+    val = upT(m.val);
+  };
+  upcsr(N_, d.n_ptr, d.n_col, d.n_val);
+  if (method_ == 1) {
+    upcsr(H_, d.h_ptr, d.h_col, d.h_val);
+  } else {
+    upcsr(E_, d.e_ptr, d.e_col, d.e_val);
+    upcsr(A_, d.a_ptr, d.a_col, d.a_val);
+    upcsr(R_, d.r_ptr, d.r_col, d.r_val);
+    d.jac = upT(jacobi_);
+    d.nfree = (int)free_edges_.size();
+    d.ndir = (int)dir_edges_.size();
+    d.free_edges = (const int32_t*)up(free_edges_.data(), free_edges_.size() * 4);
+    d.dir_edges = (const int32_t*)up(dir_edges_.data(), dir_edges_.size() * 4);
+    d.x = zeros(d.nfree); d.r = zeros(d.nfree); d.p = zeros(d.nfree); d.q = zeros(d.nfree);
+    d.rhs = zeros(d.nfree); d.xh1 = zeros(d.nfree); d.xh2 = zeros(d.nfree); d.xh3 = zeros(d.nfree);
+    cg_blocks_ = f32 ? tet_cg_blocks<float>(opt_.device) : tet_cg_blocks<double>(opt_.device);
+    if (cg_blocks_ < 1) throw CudaError("no co-resident blocks for the cooperative CG kernel");
+    d.part_a = (double*)dalloc((size_t)cg_blocks_ * 8);
+    d.part_b = (double*)dalloc((size_t)cg_blocks_ * 3 * 8);
+    d.cg_iters = (int32_t*)dalloc((nsteps_ + 1) * 4);
+    d.cg_resid = (double*)dalloc((nsteps_ + 1) * 8);
+    d.cg_maxiter = opt_.cg_maxiter;
+    d.cg_criterion = opt_.cg_criterion;
+    d.warm_start = opt_.warm_start;
+    d.tol = sim_.tol;
+  }
+  // source edges and pairs
+  const size_t nsrc = src_labels_.size();
+  auto src_index = [&](uint32_t l) {
+    for (size_t q = 0; q < nsrc; q++)
+      if (src_labels_[q] == l) return (int)q;
+    return -1;
+  };
+  std::vector<double> init_U(NE, 0.0), init_I(NE, 0.0), init_src(NE, 0.0);
+  for (size_t e = 0; e < NE; e++) {
+    if (edge_src_[e].empty() || pec_[e]) continue;
+    const std::string ty = sc_.sources[edge_src_[e][0]].st;
+    int kind = ty == "e" ? 1 : (ty == "h" ? 2 : (ty == "j" ? 3 : 0));
+    if (kind == 0 || (kind == 2 && bnd_edge_[e] < 0)) continue;
+    const auto &a = pts_[edges_[e][0]], &b = pts_[edges_[e][1]];
+    const V3 eb{0.5 * (a[0] + b[0]), 0.5 * (a[1] + b[1]), 0.5 * (a[2] + b[2])};
+    const V3 ev = sub(b, a);
+    V3 vec = kind == 2 ? bnd_dual_[bnd_edge_[e]] : ev;
+    double post = kind == 3 ? 1.0 / std::sqrt(dot(ev, ev)) : 1.0;
+    src_begin_.push_back((int)pair_src_.size());
+    src_edge_.push_back((int32_t)e);
+    src_kind_e_.push_back((int8_t)kind);
+    for (int q = 0; q < 3; q++) src_vec_.push_back(vec[q]);
+    src_post_.push_back(post);
+    double v0[3] = {0, 0, 0};
+    for (uint32_t sl : edge_src_[e]) {
+      const Source& s = sc_.sources[sl];
+      if (s.st != ty) continue;  // each evaluator sums only its own type
+      const int si = src_index(sl);
+      double f[4] = {1, 1, 1, 1};
+      if (s.decay != 0)
+        f[0] = std::pow(std::pow(eb[0] - s.center[0], 2) + std::pow(eb[1] - s.center[1], 2) +
+                            std::pow(eb[2] - s.center[2], 2), -0.5 * s.decay);
+      if (s.prof == "gaussian")
+        f[1] = std::exp(-((std::pow(eb[0] - s.center[0], 2) + std::pow(eb[1] - s.center[1], 2) +
+                           std::pow(eb[2] - s.center[2], 2)) / std::pow(s.radius, 2)));
+      else if (s.prof == "wave")
+        for (int x = 0; x < 3; x++) {
+          if (s.bfuncs[x] == "sin") f[1 + x] = std::sin((double)(2 * PI_L * s.kvec[x] * (eb[x] - s.center[x])));
+          else if (s.bfuncs[x] == "cos") f[1 + x] = std::cos((double)(2 * PI_L * s.kvec[x] * (eb[x] - s.center[x])));
+        }
+      pair_src_.push_back(si);
+      for (int q = 0; q < 4; q++) pair_fac_.push_back(f[q]);
+      const int dir = s.dir == "x" ? 0 : (s.dir == "y" ? 1 : 2);
+      pair_dir_.push_back((int8_t)dir);
+      // value at t = 0 for the initial state
+      auto r0 = s.compute(eb[0], eb[1], eb[2], 0.0);
+      for (int x = 0; x < 3; x++) v0[x] += r0[x];
+    }
+    const double val0 = post * ((v0[0] * vec[0] + v0[1] * vec[1]) + v0[2] * vec[2]);
+    if (kind == 1) { init_U[e] = val0; init_src[e] = val0; }
+    else if (kind == 3 && method_ == 2) init_I[e] = val0;
+  }
+  src_begin_.push_back((int)pair_src_.size());
+  src_amp_.resize(nsrc);
+  carrier_.assign(nsteps_ * nsrc + 1, 0.0);
+  for (size_t q = 0; q < nsrc; q++) {
+    const Source& s = sc_.sources[src_labels_[q]];
+    src_amp_[q] = s.st == "j" ? s.amp * s.impedance : s.amp;
+    for (uint64_t i = 0; i < nsteps_; i++) {
+      double t = (double)(i + 1) * dt_;
+      if (s.st == "h") t = t - 0.5 * dt_;
+      double c = 0.0;
+      if (t >= 0) {
+        if (s.carrier == "sin") c = std::sin((double)(2 * PI_L * s.freq * (t - s.delay)));
+        else if (s.carrier == "cos") c = s.amp * std::cos((double)(2 * PI_L * s.freq * (t - s.delay)));
+        else if (s.carrier == "gaussian") c = std::exp(-std::pow(t - s.delay, 2) / std::pow(s.width, 2));
+        else if (s.carrier == "ricker") {
+          double a = (double)(PI_L * s.freq * (t - s.delay));
+          c = (1 - 2 * std::pow(a, 2)) * std::exp(-std::pow(a, 2));
+        } else c = 1.0;
+      }
+      carrier_[i * nsrc + q] = c;
+    }
+  }
+  d.nse = (int)src_edge_.size();
+  d.nsrc = (int)nsrc;
+  d.se_edge = (const int32_t*)up(src_edge_.data(), src_edge_.size() * 4);
+  d.se_kind = (const int8_t*)up(src_kind_e_.data(), src_kind_e_.size());
+  d.se_begin = (const int*)up(src_begin_.data(), src_begin_.size() * 4);
+  d.pair_src = (const int*)up(pair_src_.data(), pair_src_.size() * 4);
+  d.pair_fac = (const double*)up(pair_fac_.data(), pair_fac_.size() * 8);
+  d.pair_dir = (const int8_t*)up(pair_dir_.data(), pair_dir_.size());
+  d.se_vec = (const double*)up(src_vec_.data(), src_vec_.size() * 8);
+  d.se_post = (const double*)up(src_post_.data(), src_post_.size() * 8);
+  d.src_amp = (const double*)up(src_amp_.data(), src_amp_.size() * 8);
+  d.carrier = (const double*)up(carrier_.data(), carrier_.size() * 8);
+  d.flux = (double*)dalloc((nsteps_ + 1) * 8);
+  CU(cudaMemsetAsync(d.flux, 0, (nsteps_ + 1) * 8, stream_));
+  d.nflux_part = method_ == 1 ? (int)((NE + 255) / 256) : (int)((src_edge_.size() + 255) / 256);
+  if (d.nflux_part < 1) d.nflux_part = 1;
+  d.flux_part = (double*)dalloc((size_t)d.nflux_part * 8);
+  CU(cudaMemsetAsync(d.flux_part, 0, (size_t)d.nflux_part * 8, stream_));
+  // probes
+  const size_t np = probe_tet_.size();
+  std::vector<int32_t> pe(6 * np), pf(4 * np);
+  for (size_t p = 0; p < np; p++) {
+    auto el = vol_edges(probe_tet_[p]);
+    for (int q = 0; q < 6; q++) pe[6 * p + q] = el[q];
+    for (int q = 0; q < 4; q++) pf[4 * p + q] = vtf_[probe_tet_[p]][q];
+  }
+  d.np = (int)np;
+  d.p_edges = (const int32_t*)up(pe.data(), pe.size() * 4);
+  d.p_faces = (const int32_t*)up(pf.data(), pf.size() * 4);
+  d.p_we = (const double*)up(probe_we_.data(), probe_we_.size() * 8);
+  d.p_hf = (const double*)up(probe_hf_.data(), probe_hf_.size() * 8);
+  d.samples = (double*)dalloc((size_t)nslots_ * np * 6 * 8);
+  d.slot_of_step = (const int*)up(slot_of_step_.data(), slot_of_step_.size() * 4);
+  d.step = (int*)dalloc(sizeof(int));
+  CU(cudaMemsetAsync(d.step, 0, sizeof(int), stream_));
+  // initial state (t = 0 sources, dga :671-791, gfdtd :1425-1445)
+  auto put_state = [&](void* dst, const std::vector<double>& v) {
+    if (!f32) CU(cudaMemcpyAsync(dst, v.data(), v.size() * 8, cudaMemcpyHostToDevice, stream_));
+    else {
+      auto f = as<float>(v);
+      CU(cudaMemcpyAsync(dst, f.data(), f.size() * 4, cudaMemcpyHostToDevice, stream_));
+      CU(cudaStreamSynchronize(stream_));
+    }
+  };
+  put_state(d.U, init_U);
+  put_state(d.I, init_I);
+  put_state(d.src, init_src);
+  if (method_ == 1) {
+    if (f32) tet_launch_initial_probes<float>(d, stream_);
+    else tet_launch_initial_probes<double>(d, stream_);
+  }
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(stream_));
+}
+
+void TetSim::launch_steps(int n, cudaEvent_t* ev) {
+  for (int q = 0; q < n; q++) {
+    cudaError_t e = opt_.precision == 1 ? tet_launch_step<float>(dp_, method_, cg_blocks_, stream_, ev)
+                                        : tet_launch_step<double>(dp_, method_, cg_blocks_, stream_, ev);
+    CU(e);
+  }
+}
+
+uint64_t TetSim::step(uint64_t n) {
+  if (step_ + n > nsteps_) n = nsteps_ - step_;
+  if (n == 0) { last_ms_ = 0; return 0; }
+  CU(cudaEventRecord(ev0_, stream_));
+  launch_steps((int)n, nullptr);
+  CU(cudaEventRecord(ev1_, stream_));
+  CU(cudaEventSynchronize(ev1_));
+  float ms = 0;
+  CU(cudaEventElapsedTime(&ms, ev0_, ev1_));
+  last_ms_ = ms;
+  step_ += n;
+  return n;
+}
+
+uint64_t TetSim::phase_times(uint64_t n, double* ms5) {
+  if (step_ + n > nsteps_) n = nsteps_ - step_;
+  for (int q = 0; q < 5; q++) ms5[q] = 0;
+  cudaEvent_t ev[6];
+  for (auto& e : ev) CU(cudaEventCreate(&e));
+  for (uint64_t i = 0; i < n; i++) {
+    launch_steps(1, ev);
+    CU(cudaEventSynchronize(ev[5]));
+    for (int q = 0; q < 5; q++) {
+      float ms = 0;
+      CU(cudaEventElapsedTime(&ms, ev[q], ev[q + 1]));
+      ms5[q] += ms;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  step_ += n;
+  return n;
+}
+
+uint64_t TetSim::step_io(const double* carrier_in, double* probe_out) {
+  if (step_ >= nsteps_) return 0;
+  const size_t nsrc = src_labels_.size(), np = probe_tet_.size();
+  if (!pinned_) CU(cudaHostAlloc((void**)&pinned_, (nsrc + 6 * np + 1) * sizeof(double), cudaHostAllocDefault));
+  if (carrier_in && nsrc) {
+    std::memcpy(pinned_, carrier_in, nsrc * sizeof(double));
+    CU(cudaMemcpyAsync((double*)dp_.carrier + step_ * nsrc, pinned_, nsrc * sizeof(double), cudaMemcpyHostToDevice,
+                       stream_));
+  }
+  launch_steps(1, nullptr);
+  const uint64_t sched = method_ == 1 ? step_ + 1 : step_;
+  const int slot = slot_of_step_[sched];
+  if (probe_out && slot >= 0 && np)
+    CU(cudaMemcpyAsync(pinned_ + nsrc, dp_.samples + (size_t)slot * np * 6, np * 6 * sizeof(double),
+                       cudaMemcpyDeviceToHost, stream_));
+  CU(cudaStreamSynchronize(stream_));
+  if (probe_out && slot >= 0 && np) std::memcpy(probe_out, pinned_ + nsrc, np * 6 * sizeof(double));
+  step_++;
+  return 1;
+}
+
+size_t TetSim::n_samples() const {
+  size_t c = 0;
+  const uint64_t upto = method_ == 1 ? step_ + 1 : step_;
+  for (uint64_t i = 0; i < upto && i < slot_of_step_.size(); i++)
+    if (slot_of_step_[i] >= 0) c++;
+  return c;
+}
+
+void TetSim::get_probes(double* times, double* values, size_t cap) const {
+  size_t ns = n_samples();
+  if (ns > cap) ns = cap;
+  const size_t np = probe_tet_.size();
+  if (times) std::memcpy(times, sample_times_.data(), ns * 8);
+  if (values && ns && np) CU(cudaMemcpy(values, dp_.samples, ns * np * 6 * 8, cudaMemcpyDeviceToHost));
+}
+
+void TetSim::probe_points(double* xyz, uint64_t* cells, size_t cap) const {
+  for (size_t p = 0; p < probe_tet_.size() && p < cap; p++) {
+    if (xyz) for (int a = 0; a < 3; a++) xyz[3 * p + a] = probe_pts_[p][a];
+    if (cells) cells[p] = (uint64_t)probe_tet_[p];
+  }
+}
+
+static void fetch(const void* d, size_t n, bool f32, double* out) {
+  if (!out) return;
+  if (!f32) {
+    CU(cudaMemcpy(out, d, n * 8, cudaMemcpyDeviceToHost));
+    return;
+  }
+  std::vector<float> tmp(n);
+  CU(cudaMemcpy(tmp.data(), d, n * 4, cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < n; i++) out[i] = tmp[i];
+}
+
+void TetSim::get_state(double* U, double* B, double* F) {
+  const bool f32 = opt_.precision == 1;
+  CU(cudaStreamSynchronize(stream_));
+  fetch(dp_.U, edges_.size(), f32, U);
+  fetch(dp_.B, faces_.size(), f32, B);
+  fetch(dp_.F, faces_.size(), f32, F);
+}
+
+void TetSim::set_state(const double* U, const double* F) {
+  const bool f32 = opt_.precision == 1;
+  auto put = [&](void* dst, const double* src, size_t n) {
+    if (!src) return;
+    if (!f32) CU(cudaMemcpy(dst, src, n * 8, cudaMemcpyHostToDevice));
+    else {
+      std::vector<float> t(src, src + n);
+      CU(cudaMemcpy(dst, t.data(), n * 4, cudaMemcpyHostToDevice));
+    }
+  };
+  put(dp_.U, U, edges_.size());
+  put(dp_.F, F, faces_.size());
+}
+
+void TetSim::get_flux(double* flux, size_t cap, size_t* n) const {
+  size_t m = step_ < cap ? step_ : cap;
+  if (flux && m) CU(cudaMemcpy(flux, dp_.flux, m * 8, cudaMemcpyDeviceToHost));
+  if (n) *n = step_;
+}
+
+size_t TetSim::solver_stats(int32_t* iters, double* resid, size_t cap) const {
+  if (method_ != 2) return 0;
+  size_t m = step_ < cap ? step_ : cap;
+  if (iters && m) CU(cudaMemcpy(iters, dp_.cg_iters, m * 4, cudaMemcpyDeviceToHost));
+  if (resid && m) CU(cudaMemcpy(resid, dp_.cg_resid, m * 8, cudaMemcpyDeviceToHost));
+  return step_;
+}
+
+double TetSim::energy() {
+  // 0.5 U.E U + 0.5 B.N B on the host in FP64 (gfdtd mass; dga returns the
+  // magnetic part plus 0.5 U.(Einv^-1 restricted) is not formed: magnetic only)
+  std::vector<double> U(edges_.size()), B(faces_.size()), F(faces_.size()), t;
+  get_state(U.data(), B.data(), F.data());
+  double w = 0;
+  t.resize(faces_.size());
+  N_.mul(B.data(), t.data());
+  for (size_t f = 0; f < B.size(); f++) w += 0.5 * B[f] * t[f];
+  if (method_ == 2) {
+    t.resize(edges_.size());
+    E_.mul(U.data(), t.data());
+    for (size_t e = 0; e < U.size(); e++) w += 0.5 * U[e] * t[e];
+  }
+  return w;
+}
+
+}  // namespace tf

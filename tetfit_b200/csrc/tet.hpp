@@ -1,0 +1,146 @@
+// Tetrahedral DGA simulations ("method dga" explicit, "method gfdtd" with the
+// conjugate-gradient eps-mass solve): host set-up of the complex and operators
+// and the device runtime driving tet_kernels.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "script.hpp"
+#include "sim.hpp"
+#include "tet_kernels.cuh"
+
+namespace tf {
+
+// CSR on the host (int32 columns, double values), duplicates summed in
+// insertion order.
+struct HostCsr {
+  uint32_t nrows = 0, ncols = 0;
+  std::vector<int64_t> ptr;
+  std::vector<int32_t> col;
+  std::vector<double> val;
+  struct Trip {
+    uint32_t r, c;
+    double v;
+  };
+  static HostCsr build(uint32_t nr, uint32_t nc, std::vector<Trip>& t);
+  void mul(const double* x, double* y) const;
+};
+
+class TetSim : public Sim {
+ public:
+  TetSim(Script& sc, uint32_t label, const RunOptions& opt);
+  ~TetSim() override;
+  int method() const override { return method_; }
+  uint64_t step(uint64_t n) override;
+  uint64_t n_edges() const override { return edges_.size(); }
+  uint64_t n_faces() const override { return faces_.size(); }
+  uint64_t n_cells() const override { return vols_.size(); }
+  uint64_t n_probes() const override { return probe_tet_.size(); }
+  uint64_t n_steps() const override { return nsteps_; }
+  uint64_t step_index() const override { return step_; }
+  double dt() const override { return dt_; }
+  double dt_estimate() const override { return dt_est_; }
+  bool possibly_unstable() const override { return unstable_; }
+  int precision() const override { return opt_.precision; }
+  uint64_t device_bytes() const override { return dev_bytes_; }
+  double last_step_ms() const override { return last_ms_; }
+  const Output& output() const override { return out_; }
+  const Simulation& simulation() const override { return sim_; }
+  size_t n_samples() const override;
+  double sample_time_shift() const override { return method_ == 2 ? 0.5 * dt_ : -0.5 * dt_; }
+  void get_probes(double* times, double* values, size_t cap) const override;
+  void probe_points(double* xyz, uint64_t* cells, size_t cap) const override;
+  void get_state(double* U, double* B, double* F) override;
+  void set_state(const double* U, const double* F) override;
+  void get_flux(double* flux, size_t cap, size_t* n) const override;
+  double energy() override;
+  uint64_t phase_times(uint64_t n, double* ms5) override;
+  uint64_t step_io(const double* carrier_in, double* probe_out) override;
+  int kernels_per_step() const override {
+    const int np = probe_tet_.empty() ? 0 : 1;
+    return method_ == 1 ? 6 + np + (src_edge_.empty() ? 0 : 1) : 9 + np;
+  }
+  size_t n_sources() const override { return src_labels_.size(); }
+  size_t solver_stats(int32_t* iters, double* resid, size_t cap) const override;
+  uint64_t n_free() const { return free_edges_.size(); }
+  uint64_t nnz_A() const { return A_.val.size(); }
+
+ private:
+  void read_mesh();
+  void classify();
+  void build_ops();
+  double estimate_dt(const HostCsr& Minv_or_E, bool generalized);
+  void locate_probes();
+  void alloc_and_upload();
+  void launch_steps(int n, cudaEvent_t* ev);
+  template <typename T>
+  void fill(TetDev<T>& d) const;
+  std::array<int32_t, 6> vol_edges(uint32_t v) const;
+
+  Script& sc_;
+  Simulation sim_;
+  Output out_;
+  RunOptions opt_;
+  uint32_t label_;
+  int method_ = 2;
+  // complex
+  std::vector<std::array<double, 3>> pts_;
+  std::vector<std::array<int32_t, 4>> vols_;
+  std::vector<uint32_t> vol_mat_;
+  std::vector<double> cell_vol_;
+  std::vector<std::array<int32_t, 3>> faces_;      // sorted node triples
+  std::vector<std::array<int32_t, 2>> edges_;      // sorted node pairs
+  std::vector<std::array<int32_t, 4>> vtf_;        // faces opposite nodes 0..3 (bcd, acd, abd, abc)
+  std::vector<std::array<int32_t, 2>> ftv_;        // tets of a face (-1 if none)
+  std::vector<std::array<int32_t, 3>> fte_;        // edges p0p1, p0p2, p1p2 (signs +, -, +)
+  std::vector<int64_t> star_ptr_;                  // node -> incident edges (ascending)
+  std::vector<int32_t> star_edge_;
+  std::vector<int64_t> nvol_ptr_;                  // node -> incident tets (ascending)
+  std::vector<int32_t> nvol_;
+  std::vector<int32_t> bnd_edge_;                  // edge -> boundary dual index or -1
+  std::vector<std::array<double, 3>> bnd_dual_;
+  std::vector<uint8_t> cls_;                       // 1 interior dof, 4 Dirichlet
+  std::vector<uint8_t> pec_;
+  std::vector<std::vector<uint32_t>> edge_src_;
+  // operators
+  HostCsr Ct_;                                     // E x F, +-1 (C transposed)
+  HostCsr N_, H_, E_, A_, R_;                      // R_: eps-mass, free rows x Dirichlet cols
+  std::vector<int32_t> free_edges_, dir_edges_;
+  std::vector<double> jacobi_;
+  // sources
+  std::vector<uint32_t> src_labels_;
+  std::vector<int32_t> src_edge_;                  // source-driven edges
+  std::vector<int8_t> src_kind_e_;                 // 1 e, 2 h, 3 j
+  std::vector<int> src_begin_;
+  std::vector<int> pair_src_;
+  std::vector<double> pair_fac_;
+  std::vector<int8_t> pair_dir_;
+  std::vector<double> src_vec_, src_post_;
+  std::vector<double> carrier_, src_amp_;
+  std::vector<int8_t> src_kind_;
+  // probes
+  std::vector<int32_t> probe_tet_;
+  std::vector<std::array<double, 3>> probe_pts_;
+  std::vector<double> probe_we_, probe_hf_;        // [p][6][3] Whitney weights, [p][4][3] flux weights
+  std::vector<int> slot_of_step_;
+  std::vector<double> sample_times_;
+  int nslots_ = 0;
+  double dt_ = 0, dt_est_ = 0;
+  bool unstable_ = false;
+  uint64_t nsteps_ = 0, step_ = 0;
+  double last_ms_ = 0;
+  uint64_t dev_bytes_ = 0;
+  // device
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  std::vector<void*> allocs_;
+  DevPtrs dp_{};
+  int cg_blocks_ = 0;
+  double* pinned_ = nullptr;
+};
+
+}  // namespace tf
