@@ -110,8 +110,33 @@ TF_API int tf_run(tf_ctx* ctx, uint32_t sim_label, const tf_opts* opts);
 /* gfdtd: CG iterations and final relative residual of every step taken so far
  * (the reference's "mean solver iterations", Discretization.hpp:2286-2302). */
 TF_API int tf_solver_stats(tf_ctx* ctx, int32_t* iters, double* resid, size_t cap, size_t* n);
+/* Standalone Jacobi-PCG solve of a symmetric positive definite CSR system held
+ * in device memory, with the persistent kernel of the gfdtd path
+ * (ConjugateGradientSolver.hpp:52-129: Jacobi preconditioner 1/diag, stop on
+ * ||r||/||r0|| <= tol (criterion 0) or ||r|| <= tol ||b|| (criterion 1), at
+ * most maxiter iterations, 0 meaning 100).  x holds the initial guess and
+ * receives the solution.  Returns TF_E_SOLVER when the iteration limit is hit
+ * first (x then holds the last iterate).  Allocates its work space (4 n + a
+ * few hundred doubles) on the device for the duration of the call.  Errors are
+ * reported through tf_last_error(NULL). */
+typedef struct tf_pcg_args {
+  int32_t n;                 /* rows = columns                                  */
+  int32_t device;
+  const int64_t* row_ptr;    /* device, n + 1 entries                           */
+  const int32_t* col;        /* device                                          */
+  const double* val;         /* device                                          */
+  const double* b;           /* device, n                                       */
+  double* x;                 /* device, n: initial guess in, solution out       */
+  double tol;
+  int32_t maxiter;
+  int32_t criterion;
+  void* stream;              /* cudaStream_t, or NULL for the default stream    */
+} tf_pcg_args;
+TF_API int tf_pcg_solve(const tf_pcg_args* args, int32_t* iters, double* rel_resid);
 /* Device time of the last tf_step call, from CUDA events on the context stream. */
 TF_API int tf_last_step_ms(tf_ctx* ctx, double* ms);
+/* Message of the last failure on ctx; with ctx == NULL, of the last
+ * context-free call (tf_pcg_solve) on this host thread. */
 TF_API const char* tf_last_error(tf_ctx* ctx);
 TF_API void tf_close(tf_ctx* ctx);
 /* Fills *opts with defaults (FP64, device 0, no files, quiet, automatic graphs). */

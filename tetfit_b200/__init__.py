@@ -54,6 +54,13 @@ class Info(ctypes.Structure):
 
 _lib = None
 
+
+class PcgArgs(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int32), ("device", ctypes.c_int32), ("row_ptr", ctypes.c_void_p),
+                ("col", ctypes.c_void_p), ("val", ctypes.c_void_p), ("b", ctypes.c_void_p), ("x", ctypes.c_void_p),
+                ("tol", ctypes.c_double), ("maxiter", ctypes.c_int32), ("criterion", ctypes.c_int32),
+                ("stream", ctypes.c_void_p)]
+
 # name -> (restype, argtypes); every symbol declared in include/tetfit.h
 _P = ctypes.c_void_p
 _SIGS = {
@@ -73,6 +80,8 @@ _SIGS = {
     "tf_phase_times": (ctypes.c_int, [_P, ctypes.c_uint64, _P, ctypes.POINTER(ctypes.c_uint64)]),
     "tf_run": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(Opts)]),
     "tf_solver_stats": (ctypes.c_int, [_P, _P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "tf_pcg_solve": (ctypes.c_int, [ctypes.POINTER(PcgArgs), ctypes.POINTER(ctypes.c_int32),
+                                    ctypes.POINTER(ctypes.c_double)]),
     "tf_last_step_ms": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double)]),
     "tf_last_error": (ctypes.c_char_p, [_P]),
     "tf_close": (None, [_P]),
@@ -93,6 +102,26 @@ def lib():
             fn.argtypes = args
         _lib = L
     return _lib
+
+
+def pcg_solve(row_ptr, col, val, b, x, tol=1e-8, maxiter=0, criterion=0, device=0, stream=None):
+    """Jacobi-PCG on a CSR system in device memory (tf_pcg_solve).  Arguments
+    are device pointers (ints) or objects with a `data_ptr()` method (e.g.
+    torch tensors: int64 row_ptr, int32 col, float64 val/b/x).  Returns
+    (status, iterations, relative residual); x is overwritten."""
+    def dp(t):
+        return t.data_ptr() if hasattr(t, "data_ptr") else int(t)
+    n = (len(row_ptr) - 1) if hasattr(row_ptr, "__len__") else None
+    a = PcgArgs(n=int(n if n is not None else len(b)), device=device, row_ptr=dp(row_ptr), col=dp(col),
+                val=dp(val), b=dp(b), x=dp(x), tol=tol, maxiter=maxiter, criterion=criterion, stream=stream)
+    it = ctypes.c_int32()
+    rs = ctypes.c_double()
+    rc = lib().tf_pcg_solve(ctypes.byref(a), ctypes.byref(it), ctypes.byref(rs))
+    return rc, it.value, rs.value
+
+
+def last_thread_error() -> str:
+    return lib().tf_last_error(None).decode()
 
 
 def _ptr(a):

@@ -23,6 +23,12 @@ struct tf_ctx {
   tf_opts opts{};
 };
 
+namespace tf {
+// message of the last context-free call on this host thread
+static thread_local std::string g_thread_error;
+void set_thread_error(const std::string& m) { g_thread_error = m; }
+}  // namespace tf
+
 namespace {
 
 int fail(tf_ctx* c, int code, const std::string& m) {
@@ -311,7 +317,7 @@ int tf_last_step_ms(tf_ctx* c, double* ms) {
   return TF_OK;
 }
 
-const char* tf_last_error(tf_ctx* c) { return c ? c->err.c_str() : "null context"; }
+const char* tf_last_error(tf_ctx* c) { return c ? c->err.c_str() : tf::g_thread_error.c_str(); }
 
 void tf_close(tf_ctx* c) { delete c; }
 

@@ -314,6 +314,10 @@ __global__ void __launch_bounds__(kBlock) tet_cg(DevPtrs d) {
     const int step = *d.step;
     d.cg_iters[step] = it;
     d.cg_resid[step] = res / res0;
+    if (d.cg_limit) {
+      const bool unmet = d.cg_criterion == 0 ? res / res0 > d.tol : res > d.tol * bnorm;
+      d.cg_limit[step] = unmet ? 1 : 0;
+    }
   }
 }
 
@@ -411,6 +415,28 @@ cudaError_t tet_launch_step(const DevPtrs& d, int method, int cg_blocks, cudaStr
     bump_step<<<1, 1, 0, st>>>(d.step);
     if (ev) cudaEventRecord(ev[5], st);
   }
+  return cudaGetLastError();
+}
+
+// Jacobi preconditioner from the CSR diagonal (1 where the diagonal is
+// missing or zero, ConjugateGradientSolver.hpp:119-127)
+__global__ void jacobi_from_csr(const int64_t* ptr, const int32_t* col, const double* val, double* pre, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double dg = 0.0;
+  for (int64_t k = ptr[i]; k < ptr[i + 1]; k++)
+    if (col[k] == i) dg = val[k];
+  pre[i] = dg != 0.0 ? 1.0 / dg : 1.0;
+}
+
+// Standalone FP64 solve: preconditioner, then the persistent PCG kernel.
+cudaError_t pcg_launch_solve(DevPtrs d, int blocks, cudaStream_t st) {
+  jacobi_from_csr<<<nblk(d.nfree), kBlock, 0, st>>>(d.a_ptr, d.a_col, (const double*)d.a_val, (double*)d.jac,
+                                                    d.nfree);
+  cudaMemsetAsync(d.step, 0, sizeof(int), st);
+  void* args[] = {(void*)&d};
+  cudaError_t err = cudaLaunchCooperativeKernel((void*)tet_cg<double>, dim3(blocks), dim3(kBlock), args, 0, st);
+  if (err != cudaSuccess) return err;
   return cudaGetLastError();
 }
 

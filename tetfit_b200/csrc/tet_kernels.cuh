@@ -34,6 +34,7 @@ struct DevPtrs {
   double *part_a = nullptr, *part_b = nullptr;
   int32_t* cg_iters = nullptr;
   double* cg_resid = nullptr;
+  int32_t* cg_limit = nullptr;  // optional: 1 when the iteration limit stopped the solve
   int cg_maxiter = 100, cg_criterion = 0, warm_start = 0;
   double tol = 1e-8;
   // sources
