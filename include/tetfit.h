@@ -133,6 +133,20 @@ typedef struct tf_pcg_args {
   void* stream;              /* cudaStream_t, or NULL for the default stream    */
 } tf_pcg_args;
 TF_API int tf_pcg_solve(const tf_pcg_args* args, int32_t* iters, double* rel_resid);
+/* tf_pcg_solve without any device allocation.  This entry point has no
+ * counterpart in the reference; it serves callers that cannot allocate device
+ * memory while they solve: a host whose own pool allocator already holds the
+ * GPU's memory (a cudaMalloc there fails or fragments the pool), or a loop that
+ * must not stall other streams, since cudaMalloc and cudaFree can synchronize
+ * the device.  The work space is a file-scope device array sized for at most
+ * 262,144 unknowns (about 8 MiB); every GPU that loads the library holds it
+ * until the process exits, and larger n is rejected with TF_E_ARG.  The first
+ * call on a device looks up the array's device address (once per device, that
+ * device current); make that first call before any stream capture.  All calls
+ * share the one array: calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller.  Same arguments, results
+ * and status codes as tf_pcg_solve. */
+TF_API int tf_pcg_solve_noalloc(const tf_pcg_args* args, int32_t* iters, double* rel_resid);
 /* Device time of the last tf_step call, from CUDA events on the context stream. */
 TF_API int tf_last_step_ms(tf_ctx* ctx, double* ms);
 /* Message of the last failure on ctx; with ctx == NULL, of the last

@@ -82,6 +82,8 @@ _SIGS = {
     "tf_solver_stats": (ctypes.c_int, [_P, _P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "tf_pcg_solve": (ctypes.c_int, [ctypes.POINTER(PcgArgs), ctypes.POINTER(ctypes.c_int32),
                                     ctypes.POINTER(ctypes.c_double)]),
+    "tf_pcg_solve_noalloc": (ctypes.c_int, [ctypes.POINTER(PcgArgs), ctypes.POINTER(ctypes.c_int32),
+                                            ctypes.POINTER(ctypes.c_double)]),
     "tf_last_step_ms": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double)]),
     "tf_last_error": (ctypes.c_char_p, [_P]),
     "tf_close": (None, [_P]),

@@ -5,6 +5,7 @@
 // iteration limit).
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <string>
 
 #include "../../include/tetfit.h"
@@ -107,4 +108,86 @@ extern "C" int tf_pcg_solve(const tf_pcg_args* a, int32_t* iters, double* rel_re
   rc = finish(st, d, iters, rel_resid);
   cudaFree(work);
   return rc;
+}
+
+// ---------------------------------------------------------------------------
+// tf_pcg_solve_noalloc: the same solve with its work space in a file-scope
+// device array instead of cudaMalloc.  For callers that cannot allocate device
+// memory while they solve: a host whose own pool allocator already holds the
+// GPU's memory (a cudaMalloc there fails or fragments the pool), or a loop
+// that must not stall other streams (cudaMalloc and cudaFree can synchronize
+// the device).  The array holds kNoAllocMaxN unknowns (4 vectors of 8 B each,
+// 8 MiB plus reduction slots) and stays resident on every GPU that loads the
+// library until the process exits.
+namespace {
+
+constexpr int kNoAllocMaxN = 1 << 18;   // 262,144 unknowns
+constexpr int kNoAllocMaxBlocks = 1024; // reduction slots for the cooperative grid
+
+__device__ __align__(256) double g_pcg_scratch[4 * (size_t)kNoAllocMaxN + 4 * kNoAllocMaxBlocks + 4];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+double* g_scratch_addr[kMaxDevices] = {nullptr};
+int g_scratch_blocks[kMaxDevices] = {0};
+
+// Device address of the array on `device` (which must be current), looked
+// up once per device: in host code the symbol name is only a host-side handle.
+int scratch_for(int device, double** addr, int* blocks) {
+  if (device < 0 || device >= kMaxDevices) {
+    tf::set_thread_error("tf_pcg_solve_noalloc: device ordinal out of range");
+    return TF_E_ARG;
+  }
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (!g_scratch_addr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_pcg_scratch);
+    if (e != cudaSuccess) {
+      tf::set_thread_error(std::string("tf_pcg_solve_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      return TF_E_CUDA;
+    }
+    int b = tf::tet_cg_blocks<double>(device);
+    if (b < 1) {
+      tf::set_thread_error("tf_pcg_solve_noalloc: no co-resident blocks for the cooperative kernel");
+      return TF_E_CUDA;
+    }
+    g_scratch_blocks[device] = b < kNoAllocMaxBlocks ? b : kNoAllocMaxBlocks;
+    g_scratch_addr[device] = (double*)p;
+  }
+  *addr = g_scratch_addr[device];
+  *blocks = g_scratch_blocks[device];
+  return TF_OK;
+}
+
+}  // namespace
+
+extern "C" int tf_pcg_solve_noalloc(const tf_pcg_args* a, int32_t* iters, double* rel_resid) {
+  int rc = check_args(a);
+  if (rc) return rc;
+  if (a->n > kNoAllocMaxN) {
+    tf::set_thread_error("tf_pcg_solve_noalloc: n = " + std::to_string(a->n) +
+                         " exceeds the static work space of " + std::to_string(kNoAllocMaxN) + " unknowns");
+    return TF_E_ARG;
+  }
+  cudaError_t e = cudaSetDevice(a->device);
+  if (e != cudaSuccess) {
+    tf::set_thread_error(std::string("tf_pcg_solve_noalloc: ") + cudaGetErrorString(e));
+    return TF_E_CUDA;
+  }
+  double* work = nullptr;
+  int blocks = 0;
+  rc = scratch_for(a->device, &work, &blocks);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)a->stream;
+  // the layout places the n-sized vectors first; the reduction slots and
+  // counters sit after 4 * n, inside the array for any n <= kNoAllocMaxN.
+  // Every value the kernel reads is written earlier in the same call (the
+  // step counter is cleared by pcg_launch_solve).
+  DevPtrs d = make_ptrs(a, work, blocks);
+  e = tf::pcg_launch_solve(d, blocks, st);
+  if (e != cudaSuccess) {
+    tf::set_thread_error(std::string("tf_pcg_solve_noalloc: ") + cudaGetErrorString(e));
+    return TF_E_CUDA;
+  }
+  return finish(st, d, iters, rel_resid);
 }
