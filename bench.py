@@ -38,10 +38,15 @@ MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
 WORKLOADS = {
-    # name: (cells per axis, spheres, precision, steps in the script)
-    "fit512": (512, 200, "fp32", 5000),
-    "fit64": (64, 0, "fp64", 2000),
-    "fit256": (256, 200, "fp32", 2000),   # profiling size: state 400 MB > L2
+    # Cartesian FIT cavities (SURVEY cfg0 / cfg2)
+    "fit512": dict(kind="fit", n=512, spheres=200, prec="fp32", steps=5000),
+    "fit64": dict(kind="fit", n=64, spheres=0, prec="fp64", steps=2000),
+    "fit256": dict(kind="fit", n=256, spheres=200, prec="fp32", steps=2000),  # profiling size, state > L2
+    # tetrahedral box, jittered Kuhn mesh (SURVEY cfg1 at 24^3, cfg4 size at 96^3)
+    "gfdtd24": dict(kind="tet", method="gfdtd", n=24, prec="fp64", steps=1200, cpu_n=24),
+    "dga24": dict(kind="tet", method="dga", n=24, prec="fp64", steps=1200, cpu_n=24),
+    "gfdtd96": dict(kind="tet", method="gfdtd", n=96, prec="fp32", steps=5000, grf=True, cpu_n=24),
+    "gfdtd96_fp64": dict(kind="tet", method="gfdtd", n=96, prec="fp64", steps=5000, grf=True, cpu_n=24),
 }
 
 
@@ -104,14 +109,26 @@ class ClockSampler:
 
 
 def make_case(workdir: str, workload: str, n_override: int | None = None):
-    from tetfit_b200.cases import FitCase, random_spheres, write_fit_cavity
-    n, nsph, prec, steps = WORKLOADS[workload]
-    spheres = random_spheres(nsph, seed=2026) if nsph else []
-    case = FitCase(n=n, steps=steps, spheres=spheres)
+    """Write the workload's script (and solids file or netgen mesh); return
+    (script path, precision, case object)."""
+    w = WORKLOADS[workload]
+    if w["kind"] == "fit":
+        from tetfit_b200.cases import FitCase, random_spheres, write_fit_cavity
+        spheres = random_spheres(w["spheres"], seed=2026) if w["spheres"] else []
+        case = FitCase(n=w["n"], steps=w["steps"], spheres=spheres)
+        if n_override:
+            # same scene and time step, coarser grid (bounded CPU sample)
+            case = FitCase(n=n_override, steps=w["steps"], spheres=spheres, step=case.dt())
+        return write_fit_cavity(workdir, case), w["prec"], case
+    from tetfit_b200.cases import TetCase, grf_materials, write_tet_case
+    kw = {}
+    if w.get("grf"):
+        mat, table, _ = grf_materials()
+        kw = dict(mat_field=mat, eps=table)
+    case = TetCase(n=w["n"], method=w["method"], steps=w["steps"], **kw)
     if n_override:
-        # same scene and time step, coarser grid (bounded CPU sample)
-        case = FitCase(n=n_override, steps=steps, spheres=spheres, step=case.dt())
-    return write_fit_cavity(workdir, case), prec, case
+        case = TetCase(n=n_override, method=w["method"], steps=w["steps"], step=case.dt(), **kw)
+    return write_tet_case(workdir, case), w["prec"], case
 
 
 def fit_bytes(info: dict, es: int):
@@ -122,6 +139,58 @@ def fit_bytes(info: dict, es: int):
     e_bytes = es * (2 * nE + nF) + nc
     h_bytes = es * (2 * nF + nE) + nc
     return e_bytes, h_bytes
+
+
+def phase_names(info):
+    if info["method"] == "fdtd":
+        return ["sources_bc", "e_update", "scatter_flux", "probes", "h_update"]
+    if info["method"] == "dga":
+        return ["sources", "e_update", "flux", "h_update", "probes"]
+    return ["h_update_probes", "sources_rhs", "cg_solve", "scatter", "step_end"]
+
+
+def describe(name, case, prec, info):
+    if WORKLOADS[name]["kind"] == "fit":
+        return (f"{name}: FIT cavity {case.n}^3 cells, {len(case.spheres)} lossy spheres, PEC surfaces 2-6, "
+                f"H-wave source on surface 1, {prec} state, {info['n_probes']} probes every step")
+    mats = "GRF eps_r in [1,12], 24 levels" if WORKLOADS[name].get("grf") else "vacuum"
+    extra = f", CG tol {case.tolerance:g} (reference criterion), previous-solution guess" \
+        if case.method == "gfdtd" else ""
+    return (f"{name}: {case.method} on a jittered Kuhn box {case.n}^3 x 6 = {info['n_cells']} tets, {mats}, "
+            f"PEC surfaces 2-6, H-wave source on surface 1, {prec} state{extra}")
+
+
+def l2_note(info, es):
+    state = (info["n_edges"] + 2 * info["n_faces"]) * es + info.get("nnz_operators", 0) * (4 + es) \
+        + info.get("nnz_system", 0) * (4 + es)
+    if state > 126e6:
+        return f"state + operators {state / 1e6:.0f} MB > 126 MB L2 (no flush needed)"
+    return f"state + operators {state / 1e6:.1f} MB fit in the 126 MB L2 (L2-resident workload, no flush)"
+
+
+def roofline_kernel(d, info, es, ms5, nph):
+    """(kernel name, algorithmic bytes per launch, launch ms, extra config)."""
+    if info["method"] == "fdtd":
+        e_bytes, h_bytes = fit_bytes(info, es)
+        e_ms, h_ms = ms5[1] / nph, ms5[4] / nph
+        if e_ms >= h_ms:
+            return "fit_e_kernel", e_bytes, e_ms, {}
+        return "fit_h_kernel", h_bytes, h_ms, {}
+    if info["method"] == "dga":
+        # tet_curl_f + tet_h_update: C^T F gather and the H SpMV
+        # bytes: C^T F gather (int32 per entry, F once, cb, I, cf written),
+        # then the H SpMV (int32 + value per entry, cf once, U read/write)
+        nE, nF = info["n_edges"], info["n_faces"]
+        nnz_ct, nnz_h = 3 * nF, info["nnz_operators"]
+        b = (nnz_ct * 4 + nE * 8 + nF * es + nE * 3 * es) + (nnz_h * (4 + es) + nE * (8 + 3 * es))
+        return "tet_curl_f+tet_h_update", b, ms5[1] / nph, {}
+    it, _ = d.solver_stats()
+    its = it[-nph:]
+    n, nnz = info["n_free"], info["nnz_system"]
+    per_iter = nnz * (4 + es) + n * (13 * es + 8)
+    setup = nnz * (4 + es) + n * (8 + 4 * es)
+    b = float(its.mean()) * per_iter + setup
+    return "tet_cg", b, ms5[2] / nph, {"cg_iterations_mean": float(its.mean()), "n_free": n, "nnz_A": nnz}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -137,7 +206,8 @@ def run_ours(args, rank, world, local_rank):
     script, prec, case = make_case(work, args.workload)
     d = tb.Discretization(script)
     t0 = time.time()
-    info = d.prepare(1, precision=prec, device=local_rank, graph_steps=1 if case.n >= 256 else 0)
+    info = d.prepare(1, precision=prec, device=local_rank,
+                     graph_steps=1 if WORKLOADS[args.workload]["kind"] == "fit" and case.n >= 256 else 0)
     setup_s = time.time() - t0
     K, W = args.steps, args.warmup
     need = W + K + min(K, 50) + 20
@@ -166,8 +236,10 @@ def run_ours(args, rank, world, local_rank):
     barrier()
     t0 = time.perf_counter()
     s0 = d.info()["step_index"]
+    # the script's own waveform for these steps, supplied from the host
+    tshift = 0.5 if WORKLOADS[args.workload]["kind"] == "fit" else -0.5
     for i in range(K2):
-        s = s0 + i
+        s = s0 + i + (0 if tshift > 0 else 1)
         carrier[:] = np.sin(2 * np.pi * case.frequency * (s * info["dt"] - 0.5 * info["dt"]))
         d.step_io(carrier, probe)
     e2e_s = time.perf_counter() - t0
@@ -184,10 +256,7 @@ def run_ours(args, rank, world, local_rank):
     result = None
     if rank == 0:
         es = 4 if prec == "fp32" else 8
-        e_bytes, h_bytes = fit_bytes(info, es)
-        e_ms, h_ms = ms5[1] / nph, ms5[4] / nph
-        dom = "fit_e_kernel" if e_ms >= h_ms else "fit_h_kernel"
-        dom_bytes, dom_ms = (e_bytes, e_ms) if dom == "fit_e_kernel" else (h_bytes, h_ms)
+        dom, dom_bytes, dom_ms, extra = roofline_kernel(d, info, es, ms5, nph)
         peak, peak_kind = hbm_peak()
         achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
         value = world * dofs * K / (max_ms * 1e-3)
@@ -195,16 +264,13 @@ def run_ours(args, rank, world, local_rank):
             "metric": "dof-steps/s", "value": value, "unit": "dof-steps/s", "n_gpus": world, "steps": K,
             "warmup": W, "ms_per_step": max_ms / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if prec == "fp32" else "f64", "data": "synthetic",
-            "config": {"workload": f"{args.workload}: FIT cavity {case.n}^3 cells, {len(case.spheres)} lossy "
-                                   f"spheres, PEC surfaces 2-6, H-wave source on surface 1, "
-                                   f"{prec} state, 156 probes every step",
+            "config": {"workload": describe(args.workload, case, prec, info),
                        "dofs": dofs, "cells": info["n_cells"], "parallelism": f"replicas x{world}",
-                       "l2": "state 6 arrays >> 126 MB L2 (no flush needed)", "setup_s": round(setup_s, 2)},
+                       "l2": l2_note(info, es), "setup_s": round(setup_s, 2), **extra},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
                          "algorithmic_bytes": dom_bytes, "launch_ms": dom_ms},
-            "phases_ms_per_step": {k: v / nph for k, v in
-                                   zip(["sources_bc", "e_update", "scatter_flux", "probes", "h_update"], ms5)},
+            "phases_ms_per_step": {k: v / nph for k, v in zip(phase_names(info), ms5)},
             "e2e": {"value": world * dofs * K2 / max_e2e, "unit": "dof-steps/s",
                     "h2d_bytes_per_step": 8 * n_src, "d2h_bytes_per_step": 8 * 6 * info["n_probes"],
                     "api": "tf_step_io"},
@@ -224,12 +290,12 @@ def cpu_baseline(args, seconds=15.0, threads=None):
     """FP64 CPU restatement of the reference on a bounded sample of the scene."""
     import oracle
     work = tempfile.mkdtemp(prefix="tfcpu_")
-    n_sample = 96 if args.workload == "fit512" else WORKLOADS[args.workload][0]
+    n_sample = sample_size(args.workload)
     script, _, _ = make_case(work, args.workload, n_override=n_sample)
     if threads:
         os.environ["OMP_NUM_THREADS"] = str(threads)
     os.environ["TF_ORACLE_SKIP_DT"] = "1"  # the step is pinned; skip the setup-only eigen-estimate
-    o = oracle.FitOracle(script, omp=True)
+    o = open_oracle(args.workload, script)
     dofs = o.nE + o.nF
     o.step(2)
     t0 = time.perf_counter()
@@ -238,10 +304,31 @@ def cpu_baseline(args, seconds=15.0, threads=None):
         n += o.step(10)
     el = time.perf_counter() - t0
     o.close()
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    cores = oracle_threads(args.workload)
     return {"value": dofs * n / el, "unit": "dof-steps/s", "cores": cores, "kind": "port",
             "sample": f"{n_sample}^3 grid of the same scene (FP64), {n} steps, {el:.1f} s, "
-                      f"OpenMP threads={cores}", "cpu": _cpu_model()}
+                      f"threads={cores}", "cpu": _cpu_model()}
+
+
+def sample_size(workload):
+    w = WORKLOADS[workload]
+    if w["kind"] == "fit":
+        return 96 if w["n"] > 96 else w["n"]
+    return w.get("cpu_n", w["n"])
+
+
+def open_oracle(workload, script):
+    import oracle
+    if WORKLOADS[workload]["kind"] == "fit":
+        return oracle.FitOracle(script, omp=True)
+    return oracle.TetOracle(script, omp=True)
+
+
+def oracle_threads(workload):
+    # the tetrahedral restatement is single-threaded, as the reference
+    if WORKLOADS[workload]["kind"] != "fit":
+        return 1
+    return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
 
 
 def _cpu_model():
@@ -260,10 +347,10 @@ def run_reference(args, rank):
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
     import oracle
     work = tempfile.mkdtemp(prefix="tfref_")
-    n_sample = 96 if args.workload == "fit512" else WORKLOADS[args.workload][0]
+    n_sample = sample_size(args.workload)
     script, _, _ = make_case(work, args.workload, n_override=n_sample)
     os.environ["TF_ORACLE_SKIP_DT"] = "1"  # the step is pinned; skip the setup-only eigen-estimate
-    o = oracle.FitOracle(script, omp=True)
+    o = open_oracle(args.workload, script)
     dofs = o.nE + o.nF
     o.step(args.warmup)
     t0 = time.perf_counter()
@@ -271,7 +358,7 @@ def run_reference(args, rank):
     el = time.perf_counter() - t0
     o.close()
     v = dofs * args.steps / el
-    cores = int(os.environ["OMP_NUM_THREADS"])
+    cores = oracle_threads(args.workload)
     sample = (f"{n_sample}^3 grid of the {args.workload} scene, FP64 C++ restatement of the reference "
               f"(reference needs Eigen/Spectra/GSL/Silo, not buildable here), {args.steps} steps")
     return {"impl": "reference", "metric": "dof-steps/s", "value": v, "unit": "dof-steps/s", "n_gpus": 1,

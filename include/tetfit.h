@@ -69,7 +69,9 @@ typedef struct tf_info {
   uint64_t device_bytes;               /* device memory held by the context       */
   uint32_t kernels_per_step;           /* kernel launches one leapfrog step makes */
   uint32_t n_sources;                  /* sources of the simulation (label order) */
-  uint64_t reserved[7];
+  uint64_t n_free, nnz_system;         /* gfdtd: CG unknowns and nonzeros of A    */
+  uint64_t nnz_operators;              /* nonzeros of H (dga) or of E (gfdtd)     */
+  uint64_t reserved[4];
 } tf_info;
 
 /* Parse a .fdtd script (Discretization(std::string), Discretization.hpp:45-211). */

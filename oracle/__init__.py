@@ -42,6 +42,7 @@ def lib(omp: bool = False):
         L.orc_fit_state.argtypes = [P, P, P, P]
         L.orc_fit_flux.argtypes = [P, P]
         L.orc_fit_topology.argtypes = [P, P, P, P, P]
+        L.orc_fit_coeffs.argtypes = [P, P, P, P, P]
         _libs[path] = L
     return _libs[path]
 
@@ -94,6 +95,12 @@ class FitOracle:
         f = np.zeros(self.steps_done)
         self.L.orc_fit_flux(self.h, _p(f))
         return f
+
+    def coeffs(self):
+        """(M_h, M_q, M_nu, M_mu) in the reference numbering."""
+        mh, mq, mnu, mmu = np.zeros(self.nE), np.zeros(self.nE), np.zeros(self.nF), np.zeros(self.nF)
+        self.L.orc_fit_coeffs(self.h, _p(mh), _p(mq), _p(mnu), _p(mmu))
+        return mh, mq, mnu, mmu
 
     def topology(self):
         en = np.zeros((self.nE, 2), dtype=np.uint32)

@@ -75,6 +75,14 @@ int orc_fit_flux(void* h, double* flux) {
   return 0;
 }
 
+// Material coefficients in the reference numbering: M_h, M_q (edges), M_nu, M_mu (faces).
+int orc_fit_coeffs(void* h, double* mh, double* mq, double* mnu, double* mmu) {
+  auto* o = static_cast<FitOracle*>(h);
+  for (uint32_t e = 0; e < o->nE; e++) { if (mh) mh[e] = o->M_h[e]; if (mq) mq[e] = o->M_q[e]; }
+  for (uint32_t f = 0; f < o->nF; f++) { if (mnu) mnu[f] = o->M_nu[f]; if (mmu) mmu[f] = o->M_mu[f]; }
+  return 0;
+}
+
 // Edge nodes (2 per edge) and node coordinates, to relate orderings by geometry.
 int orc_fit_topology(void* h, unsigned* edge_nodes, double* node_xyz, unsigned* face_edges, unsigned* classes) {
   auto* o = static_cast<FitOracle*>(h);

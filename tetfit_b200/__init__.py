@@ -44,7 +44,8 @@ class Info(ctypes.Structure):
                 ("method", ctypes.c_int32), ("dt", ctypes.c_double), ("dt_estimate", ctypes.c_double),
                 ("possibly_unstable", ctypes.c_int32), ("precision", ctypes.c_int32),
                 ("device_bytes", ctypes.c_uint64), ("kernels_per_step", ctypes.c_uint32),
-                ("n_sources", ctypes.c_uint32), ("reserved", ctypes.c_uint64 * 7)]
+                ("n_sources", ctypes.c_uint32), ("n_free", ctypes.c_uint64), ("nnz_system", ctypes.c_uint64),
+                ("nnz_operators", ctypes.c_uint64), ("reserved", ctypes.c_uint64 * 4)]
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

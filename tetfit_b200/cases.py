@@ -49,6 +49,8 @@ class FitCase:
     source_surface: int = 1
     pec_surfaces: tuple = (2, 3, 4, 5, 6)
     carrier: str = "sin"
+    width: float | None = None       # gaussian carrier width (s)
+    delay: float | None = None       # carrier delay (s)
 
     def dt(self) -> float:
         if self.step is not None:
@@ -88,7 +90,12 @@ def write_fit_cavity(directory: str, case: FitCase, name: str = "cavity") -> str
     lines += ["DEFINE source 1", f"   SET surface {case.source_surface}", f"   SET type {case.source_type}",
               "   SET profile wave", "   SET mode { sin , cos , cos }", "   SET center {0, 0, 0}",
               "   SET direction x", "   SET amplitude 1", f"   SET frequency {case.frequency!r}",
-              f"   SET carrier {case.carrier}", "   SET wavevector { 0.5, 0, 0 }", "END source 1"]
+              f"   SET carrier {case.carrier}", "   SET wavevector { 0.5, 0, 0 }"]
+    if case.width is not None:
+        lines += [f"   SET width {float(case.width)!r}"]
+    if case.delay is not None:
+        lines += [f"   SET delay {float(case.delay)!r}"]
+    lines += ["END source 1"]
     if case.probes:
         lines += ["DEFINE output 1", f"   SET name {case.output_name}", "   SET mode probepoint",
                   "   SET xgrid { 0.1, 0.1,0.6}", "   SET ygrid { 0.5, 1, 0.5}", "   SET zgrid { 0, 0.04, 1.05}",
@@ -187,7 +194,7 @@ class TetCase:
     frequency: float = 2e8
     jitter: float = 0.15
     seed: int = 0x7E7F17
-    eps: tuple = (1.0,)              # eps_r per material label 1, 2, ...
+    eps: object = (1.0,)             # eps_r per material label 1, 2, ... (tuple) or {label: eps_r}
     split_x: bool = False            # material 1 for x < 0.5, 2 for x >= 0.5
     pec_surfaces: tuple = (2, 3, 4, 5, 6)
     source_surface: int = 1
@@ -195,6 +202,8 @@ class TetCase:
     carrier: str = "sin"
     probes: bool = True
     mat_field: object = None         # optional callable centroids -> labels
+    width: float | None = None       # gaussian carrier width (s)
+    delay: float | None = None       # carrier delay (s)
 
     def dt(self) -> float:
         if self.step is not None:
@@ -217,14 +226,20 @@ def write_tet_case(directory: str, case: TetCase, name: str = "box") -> str:
     duration = float((case.steps - 1) * dt if case.method == "dga" else case.steps * dt)
     lines = ["DEFINE mesh 1", "   SET type tetrahedral", "   SET mesher netgen",
              f"   SET file {os.path.basename(mesh)}", "   SET name box", "   SET scalefactor 1", "END mesh 1"]
-    for m, e in enumerate(case.eps, start=1):
-        lines += [f"DEFINE material {m}", f"   SET epsilon {e!r}", "   SET mu 1", "   SET sigma 0", "   SET chi 0",
-                  f"END material {m}"]
+    eps_items = case.eps.items() if isinstance(case.eps, dict) else enumerate(case.eps, start=1)
+    for m, e in eps_items:
+        lines += [f"DEFINE material {m}", f"   SET epsilon {float(e)!r}", "   SET mu 1", "   SET sigma 0",
+                  "   SET chi 0", f"END material {m}"]
     lines += ["DEFINE bc 1"] + [f"   SET surface {s}" for s in case.pec_surfaces] + ["   SET type pec", "END bc 1"]
     lines += ["DEFINE source 1", f"   SET surface {case.source_surface}", f"   SET type {case.source_type}",
               "   SET profile wave", "   SET mode { sin , cos , cos }", "   SET center {0, 0, 0}",
               "   SET direction x", "   SET amplitude 1", f"   SET frequency {case.frequency!r}",
-              f"   SET carrier {case.carrier}", "   SET wavevector { 0.5, 0, 0 }", "END source 1"]
+              f"   SET carrier {case.carrier}", "   SET wavevector { 0.5, 0, 0 }"]
+    if case.width is not None:
+        lines += [f"   SET width {float(case.width)!r}"]
+    if case.delay is not None:
+        lines += [f"   SET delay {float(case.delay)!r}"]
+    lines += ["END source 1"]
     if case.probes:
         lines += ["DEFINE output 1", "   SET name zsections", "   SET mode probepoint",
                   "   SET xgrid { 0.1, 0.1,0.6}", "   SET ygrid { 0.5, 1, 0.5}", "   SET zgrid { 0, 0.04, 1.05}",
@@ -239,3 +254,35 @@ def write_tet_case(directory: str, case: TetCase, name: str = "box") -> str:
     with open(script, "w") as f:
         f.write("\n".join(lines) + "\n")
     return script
+
+
+def grf_materials(k_levels: int = 24, corr: float = 0.1, seed: int = 4242, grid: int = 64,
+                  lo: float = 1.0, hi: float = 12.0):
+    """Seeded 3-D Gaussian random field on the unit cube (Gaussian covariance
+    of correlation length `corr`, by FFT filtering of white noise on a
+    periodic `grid`^3 lattice), mapped affinely to [lo, hi] and quantised to
+    `k_levels` materials.  Returns (material(centroids) -> labels,
+    {label: eps_r}, max quantisation error).  Labels skip 7, which TetFIT
+    drops (Discretization.hpp:6091), and stay below 100."""
+    assert k_levels <= 97
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal((grid,) * 3)
+    f = np.fft.fftfreq(grid, d=1.0 / grid)
+    kx, ky, kz = np.meshgrid(f, f, f, indexing="ij")
+    filt = np.exp(-0.5 * (2 * np.pi) ** 2 * (kx ** 2 + ky ** 2 + kz ** 2) * (corr ** 2) / 2)
+    field = np.real(np.fft.ifftn(np.fft.fftn(w) * filt))
+    field = (field - field.min()) / (field.max() - field.min())
+    eps = lo + (hi - lo) * field
+    edges = np.linspace(lo, hi, k_levels + 1)
+    centres = 0.5 * (edges[:-1] + edges[1:])
+    labels = [l for l in range(1, k_levels + 2) if l != 7][:k_levels]
+    table = {labels[q]: float(centres[q]) for q in range(k_levels)}
+    qerr = float((hi - lo) / k_levels / 2)
+
+    def material(cent):
+        ijk = np.clip((cent * grid).astype(int), 0, grid - 1)
+        e = eps[ijk[:, 0], ijk[:, 1], ijk[:, 2]]
+        q = np.clip(((e - lo) / (hi - lo) * k_levels).astype(int), 0, k_levels - 1)
+        return np.asarray(labels)[q]
+
+    return material, table, qerr

@@ -199,6 +199,9 @@ int tf_get_info(tf_ctx* c, tf_info* info) {
   info->device_bytes = f.device_bytes();
   info->kernels_per_step = (uint32_t)f.kernels_per_step();
   info->n_sources = (uint32_t)f.n_sources();
+  info->n_free = f.n_free();
+  info->nnz_system = f.nnz_system();
+  info->nnz_operators = f.nnz_operators();
   return TF_OK;
 }
 

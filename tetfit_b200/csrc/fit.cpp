@@ -23,7 +23,7 @@ namespace tf {
 
 template <typename T>
 void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const ProbeSet& pr, int* step_counter,
-                     double* flux, cudaStream_t st, cudaEvent_t* ev);
+                     double* flux, cudaStream_t st, cudaEvent_t* ev, int e_variant, int h_variant);
 int fit_kernels_per_step(int n_special, int n_probes);
 template <typename T>
 size_t fit_launch_energy(const FitGrid<T>& g, double* part, cudaStream_t st);
@@ -813,6 +813,9 @@ void FitSim::alloc_device() {
   dinvmu_ = (double*)dalloc(3 * np * 8);
   dslot_ = (int*)dalloc(nsteps_ * 4);
   dsamples_ = (double*)dalloc((size_t)nslots_ * np * 6 * 8);
+  // pinned staging for tf_step_io, allocated here so the stepping path
+  // allocates nothing
+  CU(cudaHostAlloc((void**)&pinned_, (src_labels_.size() + 6 * np + 1) * sizeof(double), cudaHostAllocDefault));
 }
 
 // geometry helpers for the dual edge of a boundary H-source edge
@@ -1020,17 +1023,60 @@ void FitSim::launch_steps(int n, cudaEvent_t* ev) {
   if (opt_.precision == 1) {
     FitGrid<float> g; SpecialEdges<float> s;
     fill_grid(g, s);
-    for (int q = 0; q < n; q++) fit_launch_step<float>(g, s, pr, dstep_, dflux_, stream_, ev);
+    for (int q = 0; q < n; q++) fit_launch_step<float>(g, s, pr, dstep_, dflux_, stream_, ev, e_var_, h_var_);
   } else {
     FitGrid<double> g; SpecialEdges<double> s;
     fill_grid(g, s);
-    for (int q = 0; q < n; q++) fit_launch_step<double>(g, s, pr, dstep_, dflux_, stream_, ev);
+    for (int q = 0; q < n; q++) fit_launch_step<double>(g, s, pr, dstep_, dflux_, stream_, ev, e_var_, h_var_);
   }
+}
+
+// Project autotuner: on grids of at least 2 M cells the first steps of a run
+// cycle through the E and H kernel variants (bit-identical results), timing
+// each with events, and keep the fastest of each for the rest of the run.
+void FitSim::autotune(uint64_t& n) {
+  if (tuned_ || n_cells() < 2000000) { tuned_ = true; return; }
+  const int kVariants = 3, kReps = 2;
+  cudaEvent_t ev[6];
+  for (auto& e : ev) CU(cudaEventCreate(&e));
+  while (tune_pos_ < kVariants * kReps && n > 0) {
+    const int v = tune_pos_ / kReps;
+    e_var_ = h_var_ = v;
+    launch_steps(1, ev);
+    CU(cudaEventSynchronize(ev[5]));
+    float a = 0, b = 0;
+    CU(cudaEventElapsedTime(&a, ev[1], ev[2]));
+    CU(cudaEventElapsedTime(&b, ev[4], ev[5]));
+    tune_e_[v] += a;
+    tune_h_[v] += b;
+    step_++;
+    n--;
+    tune_pos_++;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (tune_pos_ < kVariants * kReps) return;  // continue on the next call
+  int be = 0, bh = 0;
+  for (int v = 1; v < kVariants; v++) {
+    if (tune_e_[v] < tune_e_[be]) be = v;
+    if (tune_h_[v] < tune_h_[bh]) bh = v;
+  }
+  e_var_ = be;
+  h_var_ = bh;
+  tuned_ = true;
+  if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
 }
 
 uint64_t FitSim::step(uint64_t n) {
   if (step_ + n > nsteps_) n = nsteps_ - step_;
   if (n == 0) { last_ms_ = 0; return 0; }
+  if (!tuned_) {
+    uint64_t before = n;
+    autotune(n);
+    if (n == 0) { last_ms_ = 0; return before; }
+    uint64_t done_tuning = before - n;
+    uint64_t rest = step(n);
+    return done_tuning + rest;
+  }
   int glen = opt_.graph_steps;
   if (glen <= 0) glen = n_cells() < 4000000 ? 64 : 1;  // small grids are launch bound: replay graphs
   CU(cudaEventRecord(ev0_, stream_));

@@ -63,6 +63,8 @@ class FitSim : public Sim {
   uint64_t phase_times(uint64_t n, double* ms5) override;
   uint64_t step_io(const double* carrier_in, double* probe_out) override;
   int kernels_per_step() const override;
+  int e_variant() const { return e_var_; }
+  int h_variant() const { return h_var_; }
   size_t n_sources() const override { return src_labels_.size(); }
   const Simulation& simulation() const override { return sim_; }
 
@@ -76,6 +78,7 @@ class FitSim : public Sim {
   void upload();
   void build_ref_maps();
   void launch_steps(int n, cudaEvent_t* ev = nullptr);
+  void autotune(uint64_t& n);
   template <typename T>
   void fill_grid(FitGrid<T>& g, SpecialEdges<T>& s);
 
@@ -137,6 +140,10 @@ class FitSim : public Sim {
   int *dpi_ = nullptr, *dpj_ = nullptr, *dpk_ = nullptr, *dslot_ = nullptr;
   double *dinvmu_ = nullptr, *dsamples_ = nullptr;
   double* pinned_ = nullptr;  // host staging for step_io
+  int e_var_ = 2, h_var_ = 2; // kernel variants (see fit_launch_step)
+  bool tuned_ = false;
+  int tune_pos_ = 0;
+  double tune_e_[3] = {0, 0, 0}, tune_h_[3] = {0, 0, 0};
   // graphs
   cudaGraphExec_t graph_ = nullptr;
   int graph_len_ = 0;

@@ -190,6 +190,14 @@ __global__ void __launch_bounds__(256) fit_e_march(FitGrid<T> g, int kchunk) {
   if (i > g.Nx || j > g.Ny || k0 > g.Nz) return;
   const int k1 = min(k0 + kchunk, g.Nz + 1);
   const T dt = (T)g.dt;
+  // the E half only reads F and the materials: read-only, non-aliasing loads
+  const T* __restrict__ Fx = g.Fx;
+  const T* __restrict__ Fy = g.Fy;
+  const T* __restrict__ Fz = g.Fz;
+  T* __restrict__ Ux = g.Ux;
+  T* __restrict__ Uy = g.Uy;
+  T* __restrict__ Uz = g.Uz;
+  const uint8_t* __restrict__ mat = g.mat;
   const bool xin = i > 0 && i < g.Nx, yin = j > 0 && j < g.Ny;
   const bool xe = i < g.Nx && yin, ye = j < g.Ny && xin, ze = xin && yin;  // column has x/y/z edges
   const bool ci0 = i > 0, ci1 = i < g.Nx, cj0 = j > 0, cj1 = j < g.Ny;
@@ -199,28 +207,28 @@ __global__ void __launch_bounds__(256) fit_e_march(FitGrid<T> g, int kchunk) {
   // materials of the plane below, c[dy][dx]
   uint8_t lo[2][2] = {{0, 0}, {0, 0}};
   if (k0 > 0) {
-    const uint8_t* m = g.mat + cb + cplane * (k0 - 1);
-    lo[0][0] = (ci0 && cj0) ? m[0] : 0;
-    lo[0][1] = (ci1 && cj0) ? m[1] : 0;
-    lo[1][0] = (ci0 && cj1) ? m[g.Nx] : 0;
-    lo[1][1] = (ci1 && cj1) ? m[g.Nx + 1] : 0;
+    const uint8_t* m = mat + cb + cplane * (k0 - 1);
+    lo[0][0] = (ci0 && cj0) ? __ldg(m) : 0;
+    lo[0][1] = (ci1 && cj0) ? __ldg(m + 1) : 0;
+    lo[1][0] = (ci0 && cj1) ? __ldg(m + g.Nx) : 0;
+    lo[1][1] = (ci1 && cj1) ? __ldg(m + g.Nx + 1) : 0;
   }
-  T fy_lo = (k0 > 0 && xe) ? g.Fy[s - g.sxy] : (T)0;
-  T fx_lo = (k0 > 0 && ye) ? g.Fx[s - g.sxy] : (T)0;
+  T fy_lo = (k0 > 0 && xe) ? __ldg(Fy + s - g.sxy) : (T)0;
+  T fx_lo = (k0 > 0 && ye) ? __ldg(Fx + s - g.sxy) : (T)0;
   for (int k = k0; k < k1; k++, s += g.sxy) {
     const bool zin = k > 0 && k < g.Nz;
     uint8_t hi[2][2] = {{0, 0}, {0, 0}};
     if (k < g.Nz) {
-      const uint8_t* m = g.mat + cb + cplane * k;
-      hi[0][0] = (ci0 && cj0) ? m[0] : 0;
-      hi[0][1] = (ci1 && cj0) ? m[1] : 0;
-      hi[1][0] = (ci0 && cj1) ? m[g.Nx] : 0;
-      hi[1][1] = (ci1 && cj1) ? m[g.Nx + 1] : 0;
+      const uint8_t* m = mat + cb + cplane * k;
+      hi[0][0] = (ci0 && cj0) ? __ldg(m) : 0;
+      hi[0][1] = (ci1 && cj0) ? __ldg(m + 1) : 0;
+      hi[1][0] = (ci0 && cj1) ? __ldg(m + g.Nx) : 0;
+      hi[1][1] = (ci1 && cj1) ? __ldg(m + g.Nx + 1) : 0;
     }
-    const T fx = (j < g.Ny && k < g.Nz) ? g.Fx[s] : (T)0;
-    const T fy = (i < g.Nx && k < g.Nz) ? g.Fy[s] : (T)0;
+    const T fx = (j < g.Ny && k < g.Nz) ? __ldg(Fx + s) : (T)0;
+    const T fy = (i < g.Nx && k < g.Nz) ? __ldg(Fy + s) : (T)0;
     if (zin) {
-      const T fz = g.Fz[s];
+      const T fz = __ldg(Fz + s);
       const bool same = lo[0][0] == lo[0][1] && lo[0][0] == lo[1][0] && lo[0][0] == lo[1][1] &&
                         lo[0][0] == hi[0][0] && lo[0][0] == hi[0][1] && lo[0][0] == hi[1][0] &&
                         lo[0][0] == hi[1][1];
@@ -228,15 +236,15 @@ __global__ void __launch_bounds__(256) fit_e_march(FitGrid<T> g, int kchunk) {
         T mh, mq;
         if (same) { mh = g.mh_pure[3 * lo[0][0]]; mq = g.mq_pure[3 * lo[0][0]]; }
         else { uint8_t m[4] = {lo[0][1], lo[1][1], hi[0][1], hi[1][1]}; edge_coef_t(g, 0, m, mh, mq); }
-        const T cf = A::sub(A::add(A::sub(fy_lo, g.Fz[s - g.sx]), fz), fy);
-        g.Ux[s] = A::mul(mh, A::add(A::mul(mq, g.Ux[s]), A::mul(dt, cf)));
+        const T cf = A::sub(A::add(A::sub(fy_lo, __ldg(Fz + s - g.sx)), fz), fy);
+        Ux[s] = A::mul(mh, A::add(A::mul(mq, Ux[s]), A::mul(dt, cf)));
       }
       if (ye) {  // y-edge: faces Fx(k-1), Fz(i-1), Fz, Fx; dual curl -1
         T mh, mq;
         if (same) { mh = g.mh_pure[3 * lo[0][0] + 1]; mq = g.mq_pure[3 * lo[0][0] + 1]; }
         else { uint8_t m[4] = {lo[1][0], lo[1][1], hi[1][0], hi[1][1]}; edge_coef_t(g, 1, m, mh, mq); }
-        const T cf = -A::sub(A::add(A::sub(fx_lo, g.Fz[s - 1]), fz), fx);
-        g.Uy[s] = A::mul(mh, A::add(A::mul(mq, g.Uy[s]), A::mul(dt, cf)));
+        const T cf = -A::sub(A::add(A::sub(fx_lo, __ldg(Fz + s - 1)), fz), fx);
+        Uy[s] = A::mul(mh, A::add(A::mul(mq, Uy[s]), A::mul(dt, cf)));
       }
     }
     if (ze && k < g.Nz) {  // z-edge: faces Fx(j-1), Fy(i-1), Fy, Fx
@@ -248,8 +256,8 @@ __global__ void __launch_bounds__(256) fit_e_march(FitGrid<T> g, int kchunk) {
         uint8_t m[4] = {hi[0][0], hi[0][1], hi[1][0], hi[1][1]};
         edge_coef_t(g, 2, m, mh, mq);
       }
-      const T cf = A::sub(A::add(A::sub(g.Fx[s - g.sx], g.Fy[s - 1]), fy), fx);
-      g.Uz[s] = A::mul(mh, A::add(A::mul(mq, g.Uz[s]), A::mul(dt, cf)));
+      const T cf = A::sub(A::add(A::sub(__ldg(Fx + s - g.sx), __ldg(Fy + s - 1)), fy), fx);
+      Uz[s] = A::mul(mh, A::add(A::mul(mq, Uz[s]), A::mul(dt, cf)));
     }
     fy_lo = fy;
     fx_lo = fx;
@@ -359,35 +367,43 @@ __global__ void __launch_bounds__(256) fit_h_march(FitGrid<T> g, int kchunk, int
   const int k1 = min(k0 + kchunk, g.Nz + 1);
   const T dt = (T)g.dt;
   const bool ci = i < g.Nx, cj = j < g.Ny;
+  // the H half only reads U and the materials
+  const T* __restrict__ Ux = g.Ux;
+  const T* __restrict__ Uy = g.Uy;
+  const T* __restrict__ Uz = g.Uz;
+  T* __restrict__ Fx = g.Fx;
+  T* __restrict__ Fy = g.Fy;
+  T* __restrict__ Fz = g.Fz;
+  const uint8_t* __restrict__ mat = g.mat;
   int64_t s = (int64_t)i + g.sx * j + g.sxy * k0;
   const int64_t cplane = (int64_t)g.Nx * g.Ny;
   const int64_t cc = (int64_t)i + (int64_t)g.Nx * j;
-  T ux = (ci) ? g.Ux[s] : (T)0, uy = (cj) ? g.Uy[s] : (T)0;
-  uint8_t m_lo = (ci && cj && k0 > 0) ? g.mat[cc + cplane * (k0 - 1)] : 0;
+  T ux = (ci) ? __ldg(Ux + s) : (T)0, uy = (cj) ? __ldg(Uy + s) : (T)0;
+  uint8_t m_lo = (ci && cj && k0 > 0) ? __ldg(mat + cc + cplane * (k0 - 1)) : 0;
   for (int k = k0; k < k1; k++, s += g.sxy) {
     const bool ck = k < g.Nz;
-    const uint8_t m0 = (ci && cj && ck) ? g.mat[cc + cplane * k] : 0;
-    const T ux1 = (ci && ck) ? g.Ux[s + g.sxy] : (T)0;
-    const T uy1 = (cj && ck) ? g.Uy[s + g.sxy] : (T)0;
+    const uint8_t m0 = (ci && cj && ck) ? __ldg(mat + cc + cplane * k) : 0;
+    const T ux1 = (ci && ck) ? __ldg(Ux + s + g.sxy) : (T)0;
+    const T uy1 = (cj && ck) ? __ldg(Uy + s + g.sxy) : (T)0;
     T mnu, mmu;
     if (cj && ck) {  // Fx(i,j,k): cells (i-1,j,k), (i,j,k)
-      const uint8_t ml = i > 0 ? g.mat[cc - 1 + cplane * k] : 0;
+      const uint8_t ml = i > 0 ? __ldg(mat + cc - 1 + cplane * k) : 0;
       if (face_coef_t(g, 0, i > 0, ci, ml, m0, mnu, mmu)) {
-        const T cs = A::sub(A::add(A::sub(uy, g.Uz[s]), g.Uz[s + g.sx]), uy1);
-        g.Fx[s] = A::mul(mnu, face_flux(mmu, g.Fx[s], dt, cs));
+        const T cs = A::sub(A::add(A::sub(uy, __ldg(Uz + s)), __ldg(Uz + s + g.sx)), uy1);
+        Fx[s] = A::mul(mnu, face_flux(mmu, Fx[s], dt, cs));
       }
     }
     if (ci && ck) {  // Fy(i,j,k): cells (i,j-1,k), (i,j,k); curl -1
-      const uint8_t ml = j > 0 ? g.mat[cc - g.Nx + cplane * k] : 0;
+      const uint8_t ml = j > 0 ? __ldg(mat + cc - g.Nx + cplane * k) : 0;
       if (face_coef_t(g, 1, j > 0, cj, ml, m0, mnu, mmu)) {
-        const T cs = A::sub(A::add(A::sub(ux, g.Uz[s]), g.Uz[s + 1]), ux1);
-        g.Fy[s] = A::mul(mnu, face_flux(mmu, g.Fy[s], -dt, cs));
+        const T cs = A::sub(A::add(A::sub(ux, __ldg(Uz + s)), __ldg(Uz + s + 1)), ux1);
+        Fy[s] = A::mul(mnu, face_flux(mmu, Fy[s], -dt, cs));
       }
     }
     if (ci && cj) {  // Fz(i,j,k): cells (i,j,k-1), (i,j,k)
       if (face_coef_t(g, 2, k > 0, ck, m_lo, m0, mnu, mmu)) {
-        const T cs = A::sub(A::add(A::sub(ux, uy), g.Uy[s + 1]), g.Ux[s + g.sx]);
-        g.Fz[s] = A::mul(mnu, face_flux(mmu, g.Fz[s], dt, cs));
+        const T cs = A::sub(A::add(A::sub(ux, uy), __ldg(Uy + s + 1)), __ldg(Ux + s + g.sx));
+        Fz[s] = A::mul(mnu, face_flux(mmu, Fz[s], dt, cs));
       }
     }
     ux = ux1;
@@ -528,35 +544,45 @@ __global__ void fit_probe_kernel(FitGrid<T> g, ProbeSet pr, const int* step_coun
 }
 
 // ---------------------------------------------------------------- launchers
+// Kernel variants for the E and H halves (all compute bit-identical results):
+// 0 one thread per node slot, 1 z-march over 4 planes, 2 z-march over 16.
 template <typename T>
 void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const ProbeSet& pr, int* step_counter,
-                     double* flux, cudaStream_t st, cudaEvent_t* ev) {
+                     double* flux, cudaStream_t st, cudaEvent_t* ev, int e_variant, int h_variant) {
   // ev (optional): 6 events recorded around the 5 phases, for per-phase timing
   dim3 blk(32, 8, 1);
   dim3 grd((unsigned)((g.Nx + 1 + 31) / 32), (unsigned)((g.Ny + 1 + 7) / 8), (unsigned)(g.Nz + 1));
+  auto mgrid = [&](int kc) {
+    return dim3((unsigned)((g.Nx + 1 + 31) / 32), (unsigned)((g.Ny + 1 + 7) / 8), (unsigned)((g.Nz + 1 + kc - 1) / kc));
+  };
   const int nsb = (sp.n + 255) / 256;
   if (ev) cudaEventRecord(ev[0], st);
   if (sp.n > 0) fit_special_pre<T><<<nsb, 256, 0, st>>>(g, sp, step_counter);
   if (ev) cudaEventRecord(ev[1], st);
-  const int kchunk = 16;
-  dim3 mblk(32, 8, 1);
-  dim3 mgrd((unsigned)((g.Nx + 1 + 31) / 32), (unsigned)((g.Ny + 1 + 7) / 8), (unsigned)((g.Nz + 1 + kchunk - 1) / kchunk));
-  fit_e_march<T><<<mgrd, mblk, 0, st>>>(g, kchunk);
+  if (e_variant == 0) fit_e_kernel<T><<<grd, blk, 0, st>>>(g);
+  else {
+    const int kc = e_variant == 1 ? 4 : 16;
+    fit_e_march<T><<<mgrid(kc), blk, 0, st>>>(g, kc);
+  }
   if (ev) cudaEventRecord(ev[2], st);
   fit_special_post<T><<<nsb > 0 ? nsb : 1, 256, 0, st>>>(g, sp, step_counter, flux, nsb);
   if (ev) cudaEventRecord(ev[3], st);
   if (pr.n > 0) fit_probe_kernel<T><<<(pr.n + 127) / 128, 128, 0, st>>>(g, pr, step_counter);
   if (ev) cudaEventRecord(ev[4], st);
-  fit_h_march<T><<<mgrd, mblk, 0, st>>>(g, kchunk, step_counter);
+  if (h_variant == 0) fit_h_kernel<T><<<grd, blk, 0, st>>>(g, step_counter);
+  else {
+    const int kc = h_variant == 1 ? 4 : 16;
+    fit_h_march<T><<<mgrid(kc), blk, 0, st>>>(g, kc, step_counter);
+  }
   if (ev) cudaEventRecord(ev[5], st);
 }
 
 int fit_kernels_per_step(int n_special, int n_probes) { return 3 + (n_special > 0) + (n_probes > 0); }
 
 template void fit_launch_step<double>(const FitGrid<double>&, const SpecialEdges<double>&, const ProbeSet&, int*,
-                                      double*, cudaStream_t, cudaEvent_t*);
+                                      double*, cudaStream_t, cudaEvent_t*, int, int);
 template void fit_launch_step<float>(const FitGrid<float>&, const SpecialEdges<float>&, const ProbeSet&, int*,
-                                     double*, cudaStream_t, cudaEvent_t*);
+                                     double*, cudaStream_t, cudaEvent_t*, int, int);
 
 // Discrete leapfrog energy: 0.5 sum M_e U^2 + 0.5 sum M_mu F_old F_new, with
 // F_new recomputed (not stored) from the current U.  FP64 accumulation, one

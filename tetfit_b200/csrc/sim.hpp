@@ -53,6 +53,9 @@ class Sim {
   virtual uint64_t step_io(const double* carrier_in, double* probe_out) = 0;
   virtual int kernels_per_step() const = 0;
   virtual size_t n_sources() const = 0;
+  virtual uint64_t n_free() const { return 0; }
+  virtual uint64_t nnz_system() const { return 0; }
+  virtual uint64_t nnz_operators() const { return 0; }
   // iterative solver statistics (gfdtd): iterations and final residual per step
   virtual size_t solver_stats(int32_t* iters, double* resid, size_t cap) const {
     (void)iters; (void)resid; (void)cap;

@@ -1009,6 +1009,7 @@ void TetSim::alloc_and_upload() {
   d.slot_of_step = (const int*)up(slot_of_step_.data(), slot_of_step_.size() * 4);
   d.step = (int*)dalloc(sizeof(int));
   CU(cudaMemsetAsync(d.step, 0, sizeof(int), stream_));
+  CU(cudaHostAlloc((void**)&pinned_, (nsrc + 6 * np + 1) * sizeof(double), cudaHostAllocDefault));
   // initial state (t = 0 sources, dga :671-791, gfdtd :1425-1445)
   auto put_state = [&](void* dst, const std::vector<double>& v) {
     if (!f32) CU(cudaMemcpyAsync(dst, v.data(), v.size() * 8, cudaMemcpyHostToDevice, stream_));

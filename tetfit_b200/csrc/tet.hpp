@@ -66,8 +66,10 @@ class TetSim : public Sim {
   }
   size_t n_sources() const override { return src_labels_.size(); }
   size_t solver_stats(int32_t* iters, double* resid, size_t cap) const override;
-  uint64_t n_free() const { return free_edges_.size(); }
-  uint64_t nnz_A() const { return A_.val.size(); }
+  uint64_t n_free() const override { return free_edges_.size(); }
+  uint64_t nnz_system() const override { return A_.val.size(); }
+  // nonzeros of the step's main operator: H (dga) or E (gfdtd)
+  uint64_t nnz_operators() const override { return method_ == 1 ? H_.val.size() : E_.val.size(); }
 
  private:
   void read_mesh();
