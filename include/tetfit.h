@@ -54,7 +54,10 @@ typedef struct tf_opts {
                            2 polynomial extrapolation, 3 learned per-edge MLP        */
   int32_t cg_criterion; /* 0 ||r||/||r0|| <= tol (reference), 1 ||r|| <= tol ||b||   */
   int32_t cg_maxiter;   /* 0: 100, the reference's limit                             */
-  int32_t reserved[7];
+  int32_t batch_mode;   /* tf_batch_open: 0 all members advance together in one
+                           group, 1 each member alone (one after another)       */
+  int32_t host_threads; /* tf_batch_open: host threads building members, 0 all  */
+  int32_t reserved[5];
 } tf_opts;
 
 typedef struct tf_info {
@@ -71,7 +74,9 @@ typedef struct tf_info {
   uint32_t n_sources;                  /* sources of the simulation (label order) */
   uint64_t n_free, nnz_system;         /* gfdtd: CG unknowns and nonzeros of A    */
   uint64_t nnz_operators;              /* nonzeros of H (dga) or of E (gfdtd)     */
-  uint64_t reserved[4];
+  uint32_t cg_blocks;                  /* gfdtd: blocks of the persistent CG kernel */
+  int32_t cg_variant;                  /* gfdtd: CG variant the autotuner picked   */
+  uint64_t reserved[3];
 } tf_info;
 
 /* Parse a .fdtd script (Discretization(std::string), Discretization.hpp:45-211). */
@@ -149,6 +154,42 @@ TF_API int tf_pcg_solve(const tf_pcg_args* args, int32_t* iters, double* rel_res
  * threads) race and must be serialised by the caller.  Same arguments, results
  * and status codes as tf_pcg_solve. */
 TF_API int tf_pcg_solve_noalloc(const tf_pcg_args* args, int32_t* iters, double* rel_resid);
+/* ---- Batches: many gfdtd simulations advanced together ---------------------
+ * The reference runs the simulations of a script one after another
+ * (dga_main.cpp:52-62), each with its own mesh, materials, sources and time
+ * step.  A batch holds n such simulations (scripts[i], simulation label
+ * labels[i], method gfdtd) built on the host in parallel and laid out in one
+ * device image: one launch sequence and one persistent CG kernel per step
+ * advance every member (batch_mode 0), each member keeping its own time step,
+ * tolerance, stopping test, probes and statistics.  batch_mode 1 keeps every
+ * member in its own device image and steps them one after another (the
+ * reference's order).  Members are numbered 0..n-1 in argument order.  Errors
+ * are reported through tf_batch_last_error. */
+typedef struct tf_batch tf_batch;
+TF_API int tf_batch_open(const char* const* scripts, const uint32_t* labels, uint32_t n, const tf_opts* opts,
+                         tf_batch** out);
+TF_API int tf_batch_info(tf_batch* b, uint32_t member, tf_info* info);
+/* Advance every unfinished member by up to nsteps steps; *done = the most any member took. */
+TF_API int tf_batch_step(tf_batch* b, uint64_t nsteps, uint64_t* done);
+/* tf_phase_times over the batch: ms5 = H update + probes, sources + rhs, CG, scatter, step end. */
+TF_API int tf_batch_phase_times(tf_batch* b, uint64_t nsteps, double* ms5, uint64_t* done);
+/* One step of every member from host memory: carriers_in holds n_sources values
+ * per member in member order (NULL keeps the scripts' waveforms); probes_out
+ * receives n_probes * 6 values per member in member order for the members that
+ * export a sample this step (others' slots are left untouched). */
+TF_API int tf_batch_step_io(tf_batch* b, const double* carriers_in, double* probes_out, uint64_t* done);
+TF_API int tf_batch_get_probes(tf_batch* b, uint32_t member, double* times, double* values, size_t cap_samples,
+                               size_t* n_samples);
+TF_API int tf_batch_get_probe_points(tf_batch* b, uint32_t member, double* xyz, uint64_t* cells, size_t cap);
+TF_API int tf_batch_get_state(tf_batch* b, uint32_t member, double* U, size_t nU, double* B, size_t nB, double* F,
+                              size_t nF);
+TF_API int tf_batch_get_flux(tf_batch* b, uint32_t member, double* flux, size_t cap, size_t* n);
+TF_API int tf_batch_solver_stats(tf_batch* b, uint32_t member, int32_t* iters, double* resid, size_t cap,
+                                 size_t* n);
+/* Device time of the last tf_batch_step (summed over members in batch_mode 1). */
+TF_API int tf_batch_last_step_ms(tf_batch* b, double* ms);
+TF_API const char* tf_batch_last_error(tf_batch* b);
+TF_API void tf_batch_close(tf_batch* b);
 /* Device time of the last tf_step call, from CUDA events on the context stream. */
 TF_API int tf_last_step_ms(tf_ctx* ctx, double* ms);
 /* Message of the last failure on ctx; with ctx == NULL, of the last

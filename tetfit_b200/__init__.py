@@ -34,7 +34,7 @@ class Opts(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("device", ctypes.c_int32), ("write_files", ctypes.c_int32),
                 ("verbose", ctypes.c_int32), ("graph_steps", ctypes.c_int32), ("mass_model", ctypes.c_int32),
                 ("warm_start", ctypes.c_int32), ("cg_criterion", ctypes.c_int32), ("cg_maxiter", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 7)]
+                ("batch_mode", ctypes.c_int32), ("host_threads", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
 
 
 class Info(ctypes.Structure):
@@ -45,7 +45,8 @@ class Info(ctypes.Structure):
                 ("possibly_unstable", ctypes.c_int32), ("precision", ctypes.c_int32),
                 ("device_bytes", ctypes.c_uint64), ("kernels_per_step", ctypes.c_uint32),
                 ("n_sources", ctypes.c_uint32), ("n_free", ctypes.c_uint64), ("nnz_system", ctypes.c_uint64),
-                ("nnz_operators", ctypes.c_uint64), ("reserved", ctypes.c_uint64 * 4)]
+                ("nnz_operators", ctypes.c_uint64), ("cg_blocks", ctypes.c_uint32), ("cg_variant", ctypes.c_int32),
+                ("reserved", ctypes.c_uint64 * 3)]
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -85,6 +86,23 @@ _SIGS = {
                                     ctypes.POINTER(ctypes.c_double)]),
     "tf_pcg_solve_noalloc": (ctypes.c_int, [ctypes.POINTER(PcgArgs), ctypes.POINTER(ctypes.c_int32),
                                             ctypes.POINTER(ctypes.c_double)]),
+    "tf_batch_open": (ctypes.c_int, [ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_uint32),
+                                     ctypes.c_uint32, ctypes.POINTER(Opts), ctypes.POINTER(_P)]),
+    "tf_batch_info": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(Info)]),
+    "tf_batch_step": (ctypes.c_int, [_P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
+    "tf_batch_phase_times": (ctypes.c_int, [_P, ctypes.c_uint64, _P, ctypes.POINTER(ctypes.c_uint64)]),
+    "tf_batch_step_io": (ctypes.c_int, [_P, _P, _P, ctypes.POINTER(ctypes.c_uint64)]),
+    "tf_batch_get_probes": (ctypes.c_int, [_P, ctypes.c_uint32, _P, _P, ctypes.c_size_t,
+                                           ctypes.POINTER(ctypes.c_size_t)]),
+    "tf_batch_get_probe_points": (ctypes.c_int, [_P, ctypes.c_uint32, _P, _P, ctypes.c_size_t]),
+    "tf_batch_get_state": (ctypes.c_int, [_P, ctypes.c_uint32, _P, ctypes.c_size_t, _P, ctypes.c_size_t, _P,
+                                          ctypes.c_size_t]),
+    "tf_batch_get_flux": (ctypes.c_int, [_P, ctypes.c_uint32, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "tf_batch_solver_stats": (ctypes.c_int, [_P, ctypes.c_uint32, _P, _P, ctypes.c_size_t,
+                                             ctypes.POINTER(ctypes.c_size_t)]),
+    "tf_batch_last_step_ms": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double)]),
+    "tf_batch_last_error": (ctypes.c_char_p, [_P]),
+    "tf_batch_close": (None, [_P]),
     "tf_last_step_ms": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double)]),
     "tf_last_error": (ctypes.c_char_p, [_P]),
     "tf_close": (None, [_P]),
@@ -167,7 +185,7 @@ class Discretization:
 
     @staticmethod
     def _opts(precision="fp64", device=0, write_files=False, verbose=False, graph_steps=0, mass="reference",
-              warm_start="previous", cg_criterion="reference", cg_maxiter=0) -> Opts:
+              warm_start="previous", cg_criterion="reference", cg_maxiter=0, batch_mode=0, host_threads=0) -> Opts:
         o = Opts()
         lib().tf_default_opts(ctypes.byref(o))
         o.precision = {"fp64": FP64, "fp32": FP32}[precision] if isinstance(precision, str) else int(precision)
@@ -176,6 +194,8 @@ class Discretization:
         o.warm_start = Discretization.WARM_STARTS[warm_start] if isinstance(warm_start, str) else int(warm_start)
         o.cg_criterion = {"reference": 0, "rhs": 1}[cg_criterion]
         o.cg_maxiter = cg_maxiter
+        o.batch_mode = {"group": 0, "serial": 1}[batch_mode] if isinstance(batch_mode, str) else int(batch_mode)
+        o.host_threads = host_threads
         return o
 
     def prepare(self, label: int, **opts) -> dict:
@@ -270,6 +290,115 @@ class Discretization:
     def close(self):
         if self._h:
             lib().tf_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many gfdtd simulations advanced together (tf_batch_*).
+
+    `Batch([(script, label), ...], batch_mode="group")` builds every member on
+    the host in parallel and lays them out in one device image: each step is
+    one launch sequence and one persistent CG kernel for all members, each
+    member with its own time step, tolerance, probes and statistics.
+    `batch_mode="serial"` keeps each member in its own image and steps them
+    one after another, the way the reference runs a script's simulations
+    (dga_main.cpp:52-62).  Options as `Discretization.prepare`.
+    """
+
+    def __init__(self, members, **opts):
+        L = lib()
+        members = list(members)
+        o = Discretization._opts(**opts)
+        paths = (ctypes.c_char_p * len(members))(*[os.fsencode(p) for p, _ in members])
+        labels = (ctypes.c_uint32 * len(members))(*[int(l) for _, l in members])
+        self._h = _P()
+        rc = L.tf_batch_open(paths, labels, len(members), ctypes.byref(o), ctypes.byref(self._h))
+        if rc != TF_OK:
+            msg = L.tf_batch_last_error(self._h).decode()
+            L.tf_batch_close(self._h)
+            self._h = None
+            raise TetfitError(rc, msg)
+        self.size = len(members)
+
+    def _check(self, rc):
+        if rc != TF_OK:
+            raise TetfitError(rc, lib().tf_batch_last_error(self._h).decode())
+
+    def info(self, m: int) -> dict:
+        i = Info()
+        self._check(lib().tf_batch_info(self._h, m, ctypes.byref(i)))
+        return i.as_dict()
+
+    def step(self, n: int) -> int:
+        done = ctypes.c_uint64()
+        self._check(lib().tf_batch_step(self._h, n, ctypes.byref(done)))
+        return done.value
+
+    def phase_times(self, n: int):
+        ms = np.zeros(5)
+        done = ctypes.c_uint64()
+        self._check(lib().tf_batch_phase_times(self._h, n, _ptr(ms), ctypes.byref(done)))
+        return ms, done.value
+
+    def step_io(self, carriers_in=None, probes_out=None) -> int:
+        done = ctypes.c_uint64()
+        self._check(lib().tf_batch_step_io(self._h, _ptr(carriers_in), _ptr(probes_out), ctypes.byref(done)))
+        return done.value
+
+    def last_step_ms(self) -> float:
+        ms = ctypes.c_double()
+        self._check(lib().tf_batch_last_step_ms(self._h, ctypes.byref(ms)))
+        return ms.value
+
+    def probes(self, m: int):
+        n = ctypes.c_size_t()
+        self._check(lib().tf_batch_get_probes(self._h, m, None, None, 0, ctypes.byref(n)))
+        np_ = self.info(m)["n_probes"]
+        t, v = np.zeros(n.value), np.zeros((n.value, np_, 6))
+        self._check(lib().tf_batch_get_probes(self._h, m, _ptr(t), _ptr(v), n.value, ctypes.byref(n)))
+        return t, v
+
+    def probe_points(self, m: int):
+        np_ = self.info(m)["n_probes"]
+        xyz, cells = np.zeros((np_, 3)), np.zeros(np_, dtype=np.uint64)
+        self._check(lib().tf_batch_get_probe_points(self._h, m, _ptr(xyz), _ptr(cells), np_))
+        return xyz, cells
+
+    def state(self, m: int):
+        i = self.info(m)
+        U, B, F = np.zeros(i["n_edges"]), np.zeros(i["n_faces"]), np.zeros(i["n_faces"])
+        self._check(lib().tf_batch_get_state(self._h, m, _ptr(U), U.size, _ptr(B), B.size, _ptr(F), F.size))
+        return U, B, F
+
+    def flux(self, m: int):
+        n = ctypes.c_size_t()
+        self._check(lib().tf_batch_get_flux(self._h, m, None, 0, ctypes.byref(n)))
+        f = np.zeros(n.value)
+        self._check(lib().tf_batch_get_flux(self._h, m, _ptr(f), n.value, ctypes.byref(n)))
+        return f
+
+    def solver_stats(self, m: int):
+        n = ctypes.c_size_t()
+        self._check(lib().tf_batch_solver_stats(self._h, m, None, None, 0, ctypes.byref(n)))
+        it, rs = np.zeros(n.value, dtype=np.int32), np.zeros(n.value)
+        self._check(lib().tf_batch_solver_stats(self._h, m, _ptr(it), _ptr(rs), n.value, ctypes.byref(n)))
+        return it, rs
+
+    def close(self):
+        if self._h:
+            lib().tf_batch_close(self._h)
             self._h = None
 
     def __enter__(self):

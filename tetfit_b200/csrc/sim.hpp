@@ -17,6 +17,9 @@ struct RunOptions {
   int warm_start = 0;       // gfdtd CG initial guess: 0 previous solution, 1 zero, 2 extrapolation, 3 learned
   int cg_criterion = 0;     // 0 ||r||/||r0|| <= tol (reference), 1 ||r|| <= tol ||b||
   int cg_maxiter = 100;
+  // run the stability estimate even when the script pins the step (batches
+  // turn it off: with a pinned step it only sets the possibly-unstable flag)
+  bool estimate_pinned = true;
 };
 
 class Sim {

@@ -11,6 +11,8 @@
 #include "tet.hpp"
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -131,16 +133,27 @@ void HostCsr::mul(const double* x, double* y) const {
 }
 
 // ------------------------------------------------------------------ set-up
-TetSim::TetSim(Script& sc, uint32_t label, const RunOptions& opt) : sc_(sc), opt_(opt), label_(label) {
+TetSim::TetSim(Script& sc, uint32_t label, const RunOptions& opt, bool device)
+    : sc_(sc), opt_(opt), label_(label) {
   sim_ = sc_.simulations.at(label);
   out_ = sc_.outputs[sim_.output];
   out_.initialize();
   method_ = sim_.method == "dga" ? 1 : 2;
   src_labels_ = sim_.sources;
+  auto t0 = std::chrono::steady_clock::now();
+  auto lap = [&](const char* what) {
+    auto t1 = std::chrono::steady_clock::now();
+    if (opt_.verbose) std::printf("  set-up %-14s %8.3f s\n", what, std::chrono::duration<double>(t1 - t0).count());
+    t0 = t1;
+  };
   read_mesh();
+  lap("mesh");
   classify();
+  lap("classes");
   build_ops();
+  lap("operators");
   locate_probes();
+  lap("probes");
   // loop length: i = 1 .. while i dt <= duration (Discretization.hpp:810, 1459)
   nsteps_ = 0;
   while ((double)(nsteps_ + 1) * dt_ <= sim_.duration) nsteps_++;
@@ -160,7 +173,20 @@ TetSim::TetSim(Script& sc, uint32_t label, const RunOptions& opt) : sc_(sc), opt
       }
     }
   }
-  alloc_and_upload();
+  build_sources();
+  if (device) alloc_and_upload();
+}
+
+void TetSim::release_host() {
+  auto drop = [](auto& v) { std::remove_reference_t<decltype(v)>().swap(v); };
+  for (HostCsr* m : {&Ct_, &N_, &H_, &E_, &A_, &R_}) {
+    drop(m->ptr);
+    drop(m->col);
+    drop(m->val);
+  }
+  drop(vtf_); drop(ftv_); drop(fte_); drop(star_ptr_); drop(star_edge_); drop(nvol_ptr_); drop(nvol_);
+  drop(bnd_edge_); drop(bnd_dual_); drop(edge_src_); drop(carrier_); drop(init_U_); drop(init_I_);
+  drop(init_src_); drop(jacobi_); drop(cls_); drop(pec_);
 }
 
 TetSim::~TetSim() {
@@ -596,7 +622,11 @@ void TetSim::build_ops() {
         if (A_.col[k] == (int32_t)i) dg = A_.val[k];
       jacobi_[i] = dg != 0 ? 1.0 / dg : 1.0;  // ConjugateGradientSolver.hpp:119-127
     }
+    auto te = std::chrono::steady_clock::now();
     dt_est_ = sim_.courant * estimate_dt(E_, true);
+    if (opt_.verbose)
+      std::printf("  set-up %-14s %8.3f s\n", "(dt estimate)",
+                  std::chrono::duration<double>(std::chrono::steady_clock::now() - te).count());
   }
   dt_ = dt_est_;
   if (sim_.step != 0) {  // Discretization.hpp:9146-9153, 8634-8641
@@ -607,11 +637,12 @@ void TetSim::build_ops() {
 
 // Largest eigenvalue of Minv K (dga, Minv = node-star inverses) or of the
 // pencil K x = lambda E x (gfdtd), K = C^T N C, by Lanczos in the K inner
-// product; dt = 2 / sqrt(lambda).  Meshes above 3 M edges with a pinned step
-// skip the estimate and take the step as given.
+// product; dt = 2 / sqrt(lambda).  Meshes above 3 M edges with a pinned step,
+// and batch members with a pinned step, skip the estimate and take the step
+// as given.
 double TetSim::estimate_dt(const HostCsr& M, bool generalized) {
   const size_t n = edges_.size(), nf = faces_.size();
-  if (sim_.step != 0 && n > 3000000) return sim_.step / sim_.courant;
+  if (sim_.step != 0 && (n > 3000000 || !opt_.estimate_pinned)) return sim_.step / sim_.courant;
   std::vector<double> cu(nf), ncu(nf);
   auto K = [&](const double* x, double* y) {
     for (size_t f = 0; f < nf; f++) cu[f] = x[fte_[f][0]] - x[fte_[f][1]] + x[fte_[f][2]];
@@ -822,6 +853,89 @@ static std::vector<T> as(const std::vector<double>& v) {
   return std::vector<T>(v.begin(), v.end());
 }
 
+// Source-driven edges, their (source, profile factor) pairs, the carrier
+// table per step and the t = 0 state (Discretization.hpp:3899-4202,
+// Source.hpp:313-567).
+void TetSim::build_sources() {
+  const size_t NE = edges_.size();
+  // source edges and pairs
+  const size_t nsrc = src_labels_.size();
+  auto src_index = [&](uint32_t l) {
+    for (size_t q = 0; q < nsrc; q++)
+      if (src_labels_[q] == l) return (int)q;
+    return -1;
+  };
+  init_U_.assign(NE, 0.0);
+  init_I_.assign(NE, 0.0);
+  init_src_.assign(NE, 0.0);
+  for (size_t e = 0; e < NE; e++) {
+    if (edge_src_[e].empty() || pec_[e]) continue;
+    const std::string ty = sc_.sources[edge_src_[e][0]].st;
+    int kind = ty == "e" ? 1 : (ty == "h" ? 2 : (ty == "j" ? 3 : 0));
+    if (kind == 0 || (kind == 2 && bnd_edge_[e] < 0)) continue;
+    const auto &a = pts_[edges_[e][0]], &b = pts_[edges_[e][1]];
+    const V3 eb{0.5 * (a[0] + b[0]), 0.5 * (a[1] + b[1]), 0.5 * (a[2] + b[2])};
+    const V3 ev = sub(b, a);
+    V3 vec = kind == 2 ? bnd_dual_[bnd_edge_[e]] : ev;
+    double post = kind == 3 ? 1.0 / std::sqrt(dot(ev, ev)) : 1.0;
+    src_begin_.push_back((int)pair_src_.size());
+    src_edge_.push_back((int32_t)e);
+    src_kind_e_.push_back((int8_t)kind);
+    for (int q = 0; q < 3; q++) src_vec_.push_back(vec[q]);
+    src_post_.push_back(post);
+    double v0[3] = {0, 0, 0};
+    for (uint32_t sl : edge_src_[e]) {
+      const Source& s = sc_.sources[sl];
+      if (s.st != ty) continue;  // each evaluator sums only its own type
+      const int si = src_index(sl);
+      double f[4] = {1, 1, 1, 1};
+      if (s.decay != 0)
+        f[0] = std::pow(std::pow(eb[0] - s.center[0], 2) + std::pow(eb[1] - s.center[1], 2) +
+                            std::pow(eb[2] - s.center[2], 2), -0.5 * s.decay);
+      if (s.prof == "gaussian")
+        f[1] = std::exp(-((std::pow(eb[0] - s.center[0], 2) + std::pow(eb[1] - s.center[1], 2) +
+                           std::pow(eb[2] - s.center[2], 2)) / std::pow(s.radius, 2)));
+      else if (s.prof == "wave")
+        for (int x = 0; x < 3; x++) {
+          if (s.bfuncs[x] == "sin") f[1 + x] = std::sin((double)(2 * PI_L * s.kvec[x] * (eb[x] - s.center[x])));
+          else if (s.bfuncs[x] == "cos") f[1 + x] = std::cos((double)(2 * PI_L * s.kvec[x] * (eb[x] - s.center[x])));
+        }
+      pair_src_.push_back(si);
+      for (int q = 0; q < 4; q++) pair_fac_.push_back(f[q]);
+      const int dir = s.dir == "x" ? 0 : (s.dir == "y" ? 1 : 2);
+      pair_dir_.push_back((int8_t)dir);
+      // value at t = 0 for the initial state
+      auto r0 = s.compute(eb[0], eb[1], eb[2], 0.0);
+      for (int x = 0; x < 3; x++) v0[x] += r0[x];
+    }
+    const double val0 = post * ((v0[0] * vec[0] + v0[1] * vec[1]) + v0[2] * vec[2]);
+    if (kind == 1) { init_U_[e] = val0; init_src_[e] = val0; }
+    else if (kind == 3 && method_ == 2) init_I_[e] = val0;
+  }
+  src_begin_.push_back((int)pair_src_.size());
+  src_amp_.resize(nsrc);
+  carrier_.assign(nsteps_ * nsrc + 1, 0.0);
+  for (size_t q = 0; q < nsrc; q++) {
+    const Source& s = sc_.sources[src_labels_[q]];
+    src_amp_[q] = s.st == "j" ? s.amp * s.impedance : s.amp;
+    for (uint64_t i = 0; i < nsteps_; i++) {
+      double t = (double)(i + 1) * dt_;
+      if (s.st == "h") t = t - 0.5 * dt_;
+      double c = 0.0;
+      if (t >= 0) {
+        if (s.carrier == "sin") c = std::sin((double)(2 * PI_L * s.freq * (t - s.delay)));
+        else if (s.carrier == "cos") c = s.amp * std::cos((double)(2 * PI_L * s.freq * (t - s.delay)));
+        else if (s.carrier == "gaussian") c = std::exp(-std::pow(t - s.delay, 2) / std::pow(s.width, 2));
+        else if (s.carrier == "ricker") {
+          double a = (double)(PI_L * s.freq * (t - s.delay));
+          c = (1 - 2 * std::pow(a, 2)) * std::exp(-std::pow(a, 2));
+        } else c = 1.0;
+      }
+      carrier_[i * nsrc + q] = c;
+    }
+  }
+}
+
 void TetSim::alloc_and_upload() {
   CU(cudaSetDevice(opt_.device));
   int major = 0;
@@ -900,80 +1014,7 @@ void TetSim::alloc_and_upload() {
     d.warm_start = opt_.warm_start;
     d.tol = sim_.tol;
   }
-  // source edges and pairs
   const size_t nsrc = src_labels_.size();
-  auto src_index = [&](uint32_t l) {
-    for (size_t q = 0; q < nsrc; q++)
-      if (src_labels_[q] == l) return (int)q;
-    return -1;
-  };
-  std::vector<double> init_U(NE, 0.0), init_I(NE, 0.0), init_src(NE, 0.0);
-  for (size_t e = 0; e < NE; e++) {
-    if (edge_src_[e].empty() || pec_[e]) continue;
-    const std::string ty = sc_.sources[edge_src_[e][0]].st;
-    int kind = ty == "e" ? 1 : (ty == "h" ? 2 : (ty == "j" ? 3 : 0));
-    if (kind == 0 || (kind == 2 && bnd_edge_[e] < 0)) continue;
-    const auto &a = pts_[edges_[e][0]], &b = pts_[edges_[e][1]];
-    const V3 eb{0.5 * (a[0] + b[0]), 0.5 * (a[1] + b[1]), 0.5 * (a[2] + b[2])};
-    const V3 ev = sub(b, a);
-    V3 vec = kind == 2 ? bnd_dual_[bnd_edge_[e]] : ev;
-    double post = kind == 3 ? 1.0 / std::sqrt(dot(ev, ev)) : 1.0;
-    src_begin_.push_back((int)pair_src_.size());
-    src_edge_.push_back((int32_t)e);
-    src_kind_e_.push_back((int8_t)kind);
-    for (int q = 0; q < 3; q++) src_vec_.push_back(vec[q]);
-    src_post_.push_back(post);
-    double v0[3] = {0, 0, 0};
-    for (uint32_t sl : edge_src_[e]) {
-      const Source& s = sc_.sources[sl];
-      if (s.st != ty) continue;  // each evaluator sums only its own type
-      const int si = src_index(sl);
-      double f[4] = {1, 1, 1, 1};
-      if (s.decay != 0)
-        f[0] = std::pow(std::pow(eb[0] - s.center[0], 2) + std::pow(eb[1] - s.center[1], 2) +
-                            std::pow(eb[2] - s.center[2], 2), -0.5 * s.decay);
-      if (s.prof == "gaussian")
-        f[1] = std::exp(-((std::pow(eb[0] - s.center[0], 2) + std::pow(eb[1] - s.center[1], 2) +
-                           std::pow(eb[2] - s.center[2], 2)) / std::pow(s.radius, 2)));
-      else if (s.prof == "wave")
-        for (int x = 0; x < 3; x++) {
-          if (s.bfuncs[x] == "sin") f[1 + x] = std::sin((double)(2 * PI_L * s.kvec[x] * (eb[x] - s.center[x])));
-          else if (s.bfuncs[x] == "cos") f[1 + x] = std::cos((double)(2 * PI_L * s.kvec[x] * (eb[x] - s.center[x])));
-        }
-      pair_src_.push_back(si);
-      for (int q = 0; q < 4; q++) pair_fac_.push_back(f[q]);
-      const int dir = s.dir == "x" ? 0 : (s.dir == "y" ? 1 : 2);
-      pair_dir_.push_back((int8_t)dir);
-      // value at t = 0 for the initial state
-      auto r0 = s.compute(eb[0], eb[1], eb[2], 0.0);
-      for (int x = 0; x < 3; x++) v0[x] += r0[x];
-    }
-    const double val0 = post * ((v0[0] * vec[0] + v0[1] * vec[1]) + v0[2] * vec[2]);
-    if (kind == 1) { init_U[e] = val0; init_src[e] = val0; }
-    else if (kind == 3 && method_ == 2) init_I[e] = val0;
-  }
-  src_begin_.push_back((int)pair_src_.size());
-  src_amp_.resize(nsrc);
-  carrier_.assign(nsteps_ * nsrc + 1, 0.0);
-  for (size_t q = 0; q < nsrc; q++) {
-    const Source& s = sc_.sources[src_labels_[q]];
-    src_amp_[q] = s.st == "j" ? s.amp * s.impedance : s.amp;
-    for (uint64_t i = 0; i < nsteps_; i++) {
-      double t = (double)(i + 1) * dt_;
-      if (s.st == "h") t = t - 0.5 * dt_;
-      double c = 0.0;
-      if (t >= 0) {
-        if (s.carrier == "sin") c = std::sin((double)(2 * PI_L * s.freq * (t - s.delay)));
-        else if (s.carrier == "cos") c = s.amp * std::cos((double)(2 * PI_L * s.freq * (t - s.delay)));
-        else if (s.carrier == "gaussian") c = std::exp(-std::pow(t - s.delay, 2) / std::pow(s.width, 2));
-        else if (s.carrier == "ricker") {
-          double a = (double)(PI_L * s.freq * (t - s.delay));
-          c = (1 - 2 * std::pow(a, 2)) * std::exp(-std::pow(a, 2));
-        } else c = 1.0;
-      }
-      carrier_[i * nsrc + q] = c;
-    }
-  }
   d.nse = (int)src_edge_.size();
   d.nsrc = (int)nsrc;
   d.se_edge = (const int32_t*)up(src_edge_.data(), src_edge_.size() * 4);
@@ -1019,9 +1060,9 @@ void TetSim::alloc_and_upload() {
       CU(cudaStreamSynchronize(stream_));
     }
   };
-  put_state(d.U, init_U);
-  put_state(d.I, init_I);
-  put_state(d.src, init_src);
+  put_state(d.U, init_U_);
+  put_state(d.I, init_I_);
+  put_state(d.src, init_src_);
   if (method_ == 1) {
     if (f32) tet_launch_initial_probes<float>(d, stream_);
     else tet_launch_initial_probes<double>(d, stream_);

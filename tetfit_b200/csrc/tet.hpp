@@ -32,7 +32,9 @@ struct HostCsr {
 
 class TetSim : public Sim {
  public:
-  TetSim(Script& sc, uint32_t label, const RunOptions& opt);
+  // device = false builds the complex, operators, probes and source tables on
+  // the host only (a batch lays several of them out in one device image)
+  TetSim(Script& sc, uint32_t label, const RunOptions& opt, bool device = true);
   ~TetSim() override;
   int method() const override { return method_; }
   uint64_t step(uint64_t n) override;
@@ -70,6 +72,8 @@ class TetSim : public Sim {
   uint64_t nnz_system() const override { return A_.val.size(); }
   // nonzeros of the step's main operator: H (dga) or E (gfdtd)
   uint64_t nnz_operators() const override { return method_ == 1 ? H_.val.size() : E_.val.size(); }
+  // frees the complex and operator arrays once a group has laid them out
+  void release_host();
 
  private:
   void read_mesh();
@@ -77,7 +81,9 @@ class TetSim : public Sim {
   void build_ops();
   double estimate_dt(const HostCsr& Minv_or_E, bool generalized);
   void locate_probes();
+  void build_sources();
   void alloc_and_upload();
+  friend class TetGroup;
   void launch_steps(int n, cudaEvent_t* ev);
   template <typename T>
   void fill(TetDev<T>& d) const;
@@ -124,6 +130,7 @@ class TetSim : public Sim {
   std::vector<double> src_vec_, src_post_;
   std::vector<double> carrier_, src_amp_;
   std::vector<int8_t> src_kind_;
+  std::vector<double> init_U_, init_I_, init_src_;  // state at t = 0
   // probes
   std::vector<int32_t> probe_tet_;
   std::vector<std::array<double, 3>> probe_pts_;

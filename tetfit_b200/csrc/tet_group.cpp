@@ -1,0 +1,598 @@
+// Host side of a gfdtd simulation group: lays S host-built simulations out in
+// one device image (tet_group_kernels.cuh), partitions the CG rows among the
+// persistent kernel's blocks and drives the step loop.
+#include "tet_group.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <string>
+
+#include "cuda_util.hpp"
+
+namespace tf {
+
+namespace {
+
+constexpr int kTuneSteps = 10;  // 2 warm-up steps, then 4 timed steps per CG variant
+int64_t up32(int64_t n) { return (n + 31) & ~int64_t(31); }
+
+// SELL-32 under construction (global slice offsets across simulations)
+template <typename T>
+struct SellHost {
+  std::vector<int64_t> ptr{0};
+  std::vector<int32_t> col;
+  std::vector<T> val;
+  // rows [0, nrows) of one simulation, nrows % 32 == 0; rows p >= nreal are
+  // padding.  len(p): entries of row p; ent(p, j, c, v): entry j; pad(p):
+  // column of a padding entry.
+  template <typename L, typename E, typename P>
+  void append(int64_t nrows, int64_t nreal, L len, E ent, P pad, bool values) {
+    for (int64_t s0 = 0; s0 < nrows; s0 += 32) {
+      int ml = 0;
+      for (int l = 0; l < 32; l++)
+        if (s0 + l < nreal) ml = std::max(ml, (int)len(s0 + l));
+      const size_t base = col.size();
+      col.resize(base + 32 * (size_t)ml);
+      if (values) val.resize(base + 32 * (size_t)ml);
+      for (int l = 0; l < 32; l++) {
+        const int64_t p = s0 + l;
+        const int n = p < nreal ? (int)len(p) : 0;
+        for (int j = 0; j < ml; j++) {
+          int32_t c = 0;
+          double v = 0.0;
+          if (j < n) ent(p, j, c, v);
+          else c = pad(p);
+          col[base + 32 * (size_t)j + l] = c;
+          if (values) val[base + 32 * (size_t)j + l] = (T)v;
+        }
+      }
+      ptr.push_back((int64_t)col.size());
+    }
+  }
+};
+
+}  // namespace
+
+void* TetGroup::dalloc(size_t bytes) {
+  void* p = nullptr;
+  CU(cudaMalloc(&p, bytes ? bytes : 16));
+  allocs_.push_back(p);
+  dev_bytes_ += bytes;
+  return p;
+}
+
+template <typename V>
+void* TetGroup::upload(const std::vector<V>& v) {
+  void* p = dalloc(v.size() * sizeof(V));
+  if (!v.empty()) CU(cudaMemcpy(p, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice));
+  return p;
+}
+
+TetGroup::TetGroup(std::vector<TetSim*> sims, const RunOptions& opt, bool release_host) : opt_(opt) {
+  if (sims.empty()) throw std::invalid_argument("empty simulation group");
+  if (sims.size() > (size_t)kMaxGroup)
+    throw std::invalid_argument("a group holds at most " + std::to_string(kMaxGroup) + " simulations");
+  for (TetSim* t : sims)
+    if (t->method() != 2) throw std::invalid_argument("simulation groups run method gfdtd only");
+  CU(cudaSetDevice(opt_.device));
+  int major = 0;
+  CU(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, opt_.device));
+  if (major != 10) throw CudaError("device " + std::to_string(opt_.device) + " is not an sm_100 (B200) GPU");
+  CU(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  CU(cudaEventCreate(&ev0_));
+  CU(cudaEventCreate(&ev1_));
+  if (opt_.precision == 1) build<float>(sims, release_host);
+  else build<double>(sims, release_host);
+}
+
+TetGroup::~TetGroup() {
+  if (pinned_) cudaFreeHost(pinned_);
+  for (void* p : allocs_) cudaFree(p);
+  if (ev0_) cudaEventDestroy(ev0_);
+  if (ev1_) cudaEventDestroy(ev1_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+template <typename T>
+void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
+  const int S = (int)sims.size();
+  SellHost<T> A, Ef, N, Ct;
+  std::vector<int32_t> fte, free_edge, dir_edge;
+  std::vector<T> pre, U0, I0, Src0;
+  std::vector<uint16_t> slice_sim, fslice_sim;
+  std::vector<double> dt(S), tol(S);
+  std::vector<int> nsteps(S);
+  std::vector<int64_t> stat_off(S), samp_off(S), sched_off(S), car_off(S);
+  std::vector<int> nsrc(S), src_off(S), sim_se(S + 1), sim_probe(S + 1);
+  std::vector<int32_t> se_edge;
+  std::vector<int8_t> se_kind, pair_dir;
+  std::vector<int> se_begin, pair_src, probe_sim, sched;
+  std::vector<double> pair_fac, se_vec, se_post, src_amp, carrier, p_we, p_hf;
+  std::vector<int32_t> p_edges, p_faces;
+  int64_t eoff = 0, foff = 0, roff = 0, stat = 0, samp = 0;
+  meta_.resize(S);
+  for (int s = 0; s < S; s++) {
+    TetSim& t = *sims[s];
+    Meta& m = meta_[s];
+    const int64_t NE = (int64_t)t.edges_.size(), NF = (int64_t)t.faces_.size();
+    const int64_t nf = (int64_t)t.free_edges_.size();
+    const int64_t NFp = up32(NF), nfp = up32(nf);
+    m.nE = NE;
+    m.nF = NF;
+    m.nsteps = t.nsteps_;
+    m.eoff = eoff;
+    m.foff = foff;
+    m.roff = roff;
+    dofs_ += (uint64_t)(NE + NF);
+    nnz_a_real_ += t.A_.val.size();
+    // Free rows grouped by stencil: rows whose column offsets (col - row) are
+    // the same form a class, classes in order of first appearance, rows of a
+    // class in their own order.  On meshes with repeated local structure the
+    // 32 rows of a slice then gather their j-th entries from consecutive
+    // positions; each class has one row length, so slices carry little
+    // padding.
+    std::vector<int32_t> old_of_new(nf), pos(nf), cls(nf);
+    auto alen_old = [&](int32_t k) { return t.A_.ptr[k + 1] - t.A_.ptr[k]; };
+    {
+      std::map<std::vector<int32_t>, int32_t> classes;
+      std::vector<int32_t> key;
+      for (int64_t k = 0; k < nf; k++) {
+        key.clear();
+        for (int64_t q = t.A_.ptr[k]; q < t.A_.ptr[k + 1]; q++) key.push_back((int32_t)(t.A_.col[q] - k));
+        cls[k] = classes.emplace(key, (int32_t)classes.size()).first->second;
+      }
+    }
+    std::iota(old_of_new.begin(), old_of_new.end(), 0);
+    std::stable_sort(old_of_new.begin(), old_of_new.end(), [&](int32_t a, int32_t b) { return cls[a] < cls[b]; });
+    for (int64_t p = 0; p < nf; p++) pos[old_of_new[p]] = (int32_t)p;
+    A.append(
+        nfp, nf, [&](int64_t p) { return alen_old(old_of_new[p]); },
+        [&](int64_t p, int j, int32_t& c, double& v) {
+          const int64_t q = t.A_.ptr[old_of_new[p]] + j;
+          c = (int32_t)(roff + pos[t.A_.col[q]]);
+          v = t.A_.val[q];
+        },
+        [&](int64_t p) { return (int32_t)(roff + p); }, true);
+    auto erow = [&](int64_t p) { return (int64_t)t.free_edges_[old_of_new[p]]; };
+    Ef.append(
+        nfp, nf, [&](int64_t p) { return t.E_.ptr[erow(p) + 1] - t.E_.ptr[erow(p)]; },
+        [&](int64_t p, int j, int32_t& c, double& v) {
+          const int64_t q = t.E_.ptr[erow(p)] + j;
+          c = (int32_t)(eoff + t.E_.col[q]);
+          v = t.E_.val[q];
+        },
+        [&](int64_t) { return (int32_t)eoff; }, true);
+    Ct.append(
+        nfp, nf, [&](int64_t p) { return t.Ct_.ptr[erow(p) + 1] - t.Ct_.ptr[erow(p)]; },
+        [&](int64_t p, int j, int32_t& c, double& v) {
+          const int64_t q = t.Ct_.ptr[erow(p)] + j;
+          c = (int32_t)(foff + t.Ct_.col[q]);
+          if (t.Ct_.val[q] < 0) c = (int32_t)((uint32_t)c | 0x80000000u);
+          v = 0.0;
+        },
+        [&](int64_t) { return kPadCol; }, false);
+    N.append(
+        NFp, NF, [&](int64_t f) { return t.N_.ptr[f + 1] - t.N_.ptr[f]; },
+        [&](int64_t f, int j, int32_t& c, double& v) {
+          const int64_t q = t.N_.ptr[f] + j;
+          c = (int32_t)(foff + t.N_.col[q]);
+          v = t.N_.val[q];
+        },
+        [&](int64_t f) { return (int32_t)(foff + f); }, true);
+    for (int64_t f = 0; f < NFp; f++)
+      for (int k = 0; k < 3; k++) fte.push_back(f < NF ? (int32_t)(eoff + t.fte_[f][k]) : -1);
+    for (int64_t p = 0; p < nfp; p++) {
+      pre.push_back(p < nf ? (T)t.jacobi_[old_of_new[p]] : (T)0);
+      free_edge.push_back(p < nf ? (int32_t)(eoff + t.free_edges_[old_of_new[p]]) : -1);
+    }
+    for (int32_t e : t.dir_edges_) dir_edge.push_back((int32_t)(eoff + e));
+    slice_sim.insert(slice_sim.end(), nfp / 32, (uint16_t)s);
+    fslice_sim.insert(fslice_sim.end(), NFp / 32, (uint16_t)s);
+    for (int64_t e = 0; e < NE; e++) {
+      U0.push_back((T)t.init_U_[e]);
+      I0.push_back((T)t.init_I_[e]);
+      Src0.push_back((T)t.init_src_[e]);
+    }
+    dt[s] = t.dt_;
+    tol[s] = t.sim_.tol;
+    nsteps[s] = (int)t.nsteps_;
+    // sources
+    m.nsrc = t.src_labels_.size();
+    nsrc[s] = (int)m.nsrc;
+    src_off[s] = (int)src_amp.size();
+    car_off[s] = (int64_t)carrier.size();
+    m.car_off = car_off[s];
+    sim_se[s] = (int)se_edge.size();
+    const int pair_base = (int)pair_src.size();
+    for (size_t k = 0; k < t.src_edge_.size(); k++) {
+      se_edge.push_back((int32_t)(eoff + t.src_edge_[k]));
+      se_kind.push_back(t.src_kind_e_[k]);
+      se_begin.push_back(pair_base + t.src_begin_[k]);
+      for (int a = 0; a < 3; a++) se_vec.push_back(t.src_vec_[3 * k + a]);
+      se_post.push_back(t.src_post_[k]);
+    }
+    for (size_t p = 0; p < t.pair_src_.size(); p++) {
+      pair_src.push_back(src_off[s] + t.pair_src_[p]);
+      pair_dir.push_back(t.pair_dir_[p]);
+      for (int a = 0; a < 4; a++) pair_fac.push_back(t.pair_fac_[4 * p + a]);
+    }
+    src_amp.insert(src_amp.end(), t.src_amp_.begin(), t.src_amp_.end());
+    carrier.insert(carrier.end(), t.carrier_.begin(), t.carrier_.end());
+    // probes
+    m.np = t.probe_tet_.size();
+    sim_probe[s] = (int)probe_sim.size();
+    for (size_t p = 0; p < m.np; p++) {
+      const int32_t v = t.probe_tet_[p];
+      auto el = t.vol_edges(v);
+      probe_sim.push_back(s);
+      for (int q = 0; q < 6; q++) p_edges.push_back((int32_t)(eoff + el[q]));
+      for (int q = 0; q < 4; q++) p_faces.push_back((int32_t)(foff + t.vtf_[v][q]));
+      for (int q = 0; q < 18; q++) p_we.push_back(t.probe_we_[18 * p + q]);
+      for (int q = 0; q < 12; q++) p_hf.push_back(t.probe_hf_[12 * p + q]);
+    }
+    m.nslots = t.nslots_;
+    m.slot_of_step = t.slot_of_step_;
+    m.sample_times = t.sample_times_;
+    samp_off[s] = samp;
+    m.samp_off = samp;
+    samp += (int64_t)m.nslots * (int64_t)m.np * 6;
+    sched_off[s] = (int64_t)sched.size();
+    sched.insert(sched.end(), t.slot_of_step_.begin(), t.slot_of_step_.end());
+    stat_off[s] = stat;
+    m.stat_off = stat;
+    stat += (int64_t)t.nsteps_ + 1;
+    eoff += NE;
+    foff += NFp;
+    roff += nfp;
+    if (eoff >= INT32_MAX || foff >= INT32_MAX || roff >= INT32_MAX)
+      throw std::invalid_argument("simulation group exceeds 2^31 edges, faces or rows");
+    if (release_host) t.release_host();
+  }
+  sim_se[S] = (int)se_edge.size();
+  se_begin.push_back((int)pair_src.size());
+  sim_probe[S] = (int)probe_sim.size();
+  carrier_host_ = carrier;
+  nnz_a_ = A.col.size();
+
+  GroupDev& d = dev_;
+  d.S = S;
+  d.nE = eoff;
+  d.nF = foff;
+  d.nrow = roff;
+  d.ndir = (int64_t)dir_edge.size();
+  d.nse = (int64_t)se_edge.size();
+  d.np = (int64_t)probe_sim.size();
+  d.dt = (const double*)upload(dt);
+  d.tol = (const double*)upload(tol);
+  d.nsteps = (const int*)upload(nsteps);
+  d.step = (int*)dalloc(sizeof(int) * S);
+  CU(cudaMemset(d.step, 0, sizeof(int) * S));
+  d.fslice_sim = (const uint16_t*)upload(fslice_sim);
+  d.slice_sim = (const uint16_t*)upload(slice_sim);
+  const size_t es = sizeof(T);
+  auto zeros = [&](int64_t n) {
+    void* p = dalloc((size_t)n * es);
+    CU(cudaMemset(p, 0, (size_t)n * es));
+    return p;
+  };
+  d.U = upload(U0);
+  d.I = upload(I0);
+  d.src = upload(Src0);
+  d.F = zeros(d.nF);
+  d.B = zeros(d.nF);
+  d.cb = zeros(d.nE);
+  d.fte = (const int32_t*)upload(fte);
+  auto put = [&](SellHost<T>& m, SellDev& o, bool values) {
+    o.ptr = (const int64_t*)upload(m.ptr);
+    o.col = (const int32_t*)upload(m.col);
+    o.val = values ? upload(m.val) : nullptr;
+    std::vector<int64_t>().swap(m.ptr);
+    std::vector<int32_t>().swap(m.col);
+    std::vector<T>().swap(m.val);
+  };
+  put(N, d.N, true);
+  put(Ef, d.Ef, true);
+  put(Ct, d.Ct, false);
+  put(A, d.A, true);
+  d.pre = upload(pre);
+  d.free_edge = (const int32_t*)upload(free_edge);
+  d.dir_edge = (const int32_t*)upload(dir_edge);
+  d.x = zeros(d.nrow);
+  d.r = zeros(d.nrow);
+  d.p0 = zeros(d.nrow);
+  d.p1 = zeros(d.nrow);
+  d.q = zeros(d.nrow);
+  d.rhs = zeros(d.nrow);
+  if (opt_.warm_start == 2) {
+    d.xh1 = zeros(d.nrow);
+    d.xh2 = zeros(d.nrow);
+    d.xh3 = zeros(d.nrow);
+  }
+  d.cg_maxiter = opt_.cg_maxiter > 0 ? opt_.cg_maxiter : 100;
+  d.cg_criterion = opt_.cg_criterion;
+  d.warm_start = opt_.warm_start;
+  d.cg_iters = (int32_t*)dalloc(sizeof(int32_t) * stat);
+  d.cg_resid = (double*)dalloc(sizeof(double) * stat);
+  d.cg_limit = (int32_t*)dalloc(sizeof(int32_t) * stat);
+  d.flux = (double*)dalloc(sizeof(double) * stat);
+  CU(cudaMemset(d.cg_iters, 0, sizeof(int32_t) * stat));
+  CU(cudaMemset(d.cg_resid, 0, sizeof(double) * stat));
+  CU(cudaMemset(d.cg_limit, 0, sizeof(int32_t) * stat));
+  CU(cudaMemset(d.flux, 0, sizeof(double) * stat));
+  d.stat_off = (const int64_t*)upload(stat_off);
+  d.sim_se = (const int*)upload(sim_se);
+  d.se_edge = (const int32_t*)upload(se_edge);
+  d.se_kind = (const int8_t*)upload(se_kind);
+  d.se_begin = (const int*)upload(se_begin);
+  d.pair_src = (const int*)upload(pair_src);
+  d.pair_fac = (const double*)upload(pair_fac);
+  d.pair_dir = (const int8_t*)upload(pair_dir);
+  d.se_vec = (const double*)upload(se_vec);
+  d.se_post = (const double*)upload(se_post);
+  d.src_amp = (const double*)upload(src_amp);
+  d.carrier = (const double*)upload(carrier);
+  d.car_off = (const int64_t*)upload(car_off);
+  d.nsrc = (const int*)upload(nsrc);
+  d.src_off = (const int*)upload(src_off);
+  d.probe_sim = (const int*)upload(probe_sim);
+  d.sim_probe = (const int*)upload(sim_probe);
+  d.p_edges = (const int32_t*)upload(p_edges);
+  d.p_faces = (const int32_t*)upload(p_faces);
+  d.p_we = (const double*)upload(p_we);
+  d.p_hf = (const double*)upload(p_hf);
+  d.samples = (double*)dalloc(sizeof(double) * (size_t)std::max<int64_t>(samp, 1));
+  d.samp_off = (const int64_t*)upload(samp_off);
+  d.sched = (const int*)upload(sched);
+  d.sched_off = (const int64_t*)upload(sched_off);
+  cg_blocks_ = opt_.precision == 1 ? group_cg_blocks<float>(opt_.device, S, &cg_smem_)
+                                   : group_cg_blocks<double>(opt_.device, S, &cg_smem_);
+  if (cg_blocks_ < 1) throw CudaError("no co-resident blocks for the cooperative CG kernel");
+  partition();
+  for (const Meta& m : meta_) {
+    io_src_ += m.nsrc;
+    io_probe_ += 6 * m.np;
+  }
+  const size_t mp = io_src_ + io_probe_ + 1;
+  pinned_len_ = mp;
+  CU(cudaHostAlloc((void**)&pinned_, mp * sizeof(double), cudaHostAllocDefault));
+  CU(cudaDeviceSynchronize());
+}
+
+// Contiguous slice ranges of about equal work (stored entries of A plus the
+// vector passes) for the CG blocks, cut at simulation boundaries into
+// segments.  The block count follows the problem size (at most one slice per
+// warp and pass) so that small systems keep their grid barriers cheap.
+void TetGroup::partition() {
+  GroupDev& d = dev_;
+  const int64_t nslice = d.nrow / 32;
+  std::vector<int64_t> aptr(nslice + 1);
+  CU(cudaMemcpy(aptr.data(), d.A.ptr, sizeof(int64_t) * (nslice + 1), cudaMemcpyDeviceToHost));
+  std::vector<uint16_t> ssim(nslice);
+  if (nslice) CU(cudaMemcpy(ssim.data(), d.slice_sim, sizeof(uint16_t) * nslice, cudaMemcpyDeviceToHost));
+  int64_t want = (nslice + kCgWarps - 1) / kCgWarps;
+  int G = (int)std::max<int64_t>(1, std::min<int64_t>(cg_blocks_, want));
+  std::vector<double> cum(nslice + 1, 0.0);
+  for (int64_t s = 0; s < nslice; s++) cum[s + 1] = cum[s] + (double)((aptr[s + 1] - aptr[s]) >> 5) + 8.0;
+  std::vector<int64_t> cut(G + 1, 0);
+  cut[G] = nslice;
+  for (int b = 1; b < G; b++) {
+    const double target = cum[nslice] * b / G;
+    cut[b] = std::lower_bound(cum.begin(), cum.end(), target) - cum.begin();
+    cut[b] = std::max(cut[b], cut[b - 1]);
+  }
+  std::vector<int> blk_seg(G + 1, 0), seg_sim, sim_seg(d.S + 1, 0);
+  std::vector<int64_t> seg_s0, seg_s1;
+  for (int b = 0; b < G; b++) {
+    blk_seg[b] = (int)seg_sim.size();
+    int64_t s = cut[b];
+    while (s < cut[b + 1]) {
+      int64_t e = s;
+      while (e < cut[b + 1] && ssim[e] == ssim[s]) e++;
+      seg_sim.push_back(ssim[s]);
+      seg_s0.push_back(s);
+      seg_s1.push_back(e);
+      s = e;
+    }
+    if ((int)seg_sim.size() - blk_seg[b] > kMaxSeg)
+      throw std::invalid_argument("CG block spans more than " + std::to_string(kMaxSeg) + " simulations");
+  }
+  blk_seg[G] = (int)seg_sim.size();
+  // segments of a simulation are consecutive
+  for (size_t g = 0; g < seg_sim.size(); g++) sim_seg[seg_sim[g] + 1]++;
+  for (int s = 0; s < d.S; s++) sim_seg[s + 1] += sim_seg[s];
+  for (size_t g = 1; g < seg_sim.size(); g++)
+    if (seg_sim[g] < seg_sim[g - 1]) throw std::logic_error("CG segments out of simulation order");
+  cg_blocks_ = G;
+  blk_seg_.assign(blk_seg.begin(), blk_seg.end());
+  d.blk_seg = (const int*)upload(blk_seg);
+  d.seg_sim = (const int*)upload(seg_sim);
+  d.seg_s0 = (const int64_t*)upload(seg_s0);
+  d.seg_s1 = (const int64_t*)upload(seg_s1);
+  d.sim_seg = (const int*)upload(sim_seg);
+  d.part = (double*)dalloc(sizeof(double) * 3 * std::max<size_t>(seg_sim.size(), 1));
+}
+
+void TetGroup::launch(int n, cudaEvent_t* ev) {
+  for (int k = 0; k < n; k++) {
+    cudaError_t e = opt_.precision == 1
+                        ? group_launch_step<float>(dev_, cg_blocks_, cg_variant_, cg_smem_, stream_, ev)
+                        : group_launch_step<double>(dev_, cg_blocks_, cg_variant_, cg_smem_, stream_, ev);
+    CU(e);
+  }
+}
+
+uint64_t TetGroup::step(uint64_t n) {
+  uint64_t left = 0;
+  for (const Meta& m : meta_) left = std::max(left, m.nsteps - m.step);
+  n = std::min(n, left);
+  if (n == 0) {
+    last_ms_ = 0;
+    return 0;
+  }
+  float total = 0;
+  uint64_t done = 0;
+  // the first steps alternate the two CG variants (bitwise identical
+  // iterates) and keep the one with the smaller total CG time
+  while (done < n && tune_pos_ < kTuneSteps) {
+    cudaEvent_t ev[6];
+    for (auto& e : ev) CU(cudaEventCreate(&e));
+    cg_variant_ = tune_pos_ & 1;
+    launch(1, ev);
+    CU(cudaEventSynchronize(ev[5]));
+    float a = 0, c = 0;
+    CU(cudaEventElapsedTime(&a, ev[2], ev[3]));
+    CU(cudaEventElapsedTime(&c, ev[0], ev[5]));
+    if (tune_pos_ >= 2) tune_ms_[cg_variant_] += a;  // first pair is warm-up
+    total += c;
+    for (auto& e : ev) cudaEventDestroy(e);
+    tune_pos_++;
+    done++;
+    if (tune_pos_ == kTuneSteps) cg_variant_ = tune_ms_[0] <= tune_ms_[1] ? 0 : 1;
+  }
+  if (done < n) {
+    CU(cudaEventRecord(ev0_, stream_));
+    launch((int)(n - done), nullptr);
+    CU(cudaEventRecord(ev1_, stream_));
+    CU(cudaEventSynchronize(ev1_));
+    float ms = 0;
+    CU(cudaEventElapsedTime(&ms, ev0_, ev1_));
+    total += ms;
+  }
+  last_ms_ = total;
+  for (Meta& m : meta_) m.step = std::min(m.nsteps, m.step + n);
+  return n;
+}
+
+uint64_t TetGroup::phase_times(uint64_t n, double* ms5) {
+  uint64_t left = 0;
+  for (const Meta& m : meta_) left = std::max(left, m.nsteps - m.step);
+  n = std::min(n, left);
+  for (int q = 0; q < 5; q++) ms5[q] = 0;
+  cudaEvent_t ev[6];
+  for (auto& e : ev) CU(cudaEventCreate(&e));
+  for (uint64_t i = 0; i < n; i++) {
+    launch(1, ev);
+    CU(cudaEventSynchronize(ev[5]));
+    for (int q = 0; q < 5; q++) {
+      float ms = 0;
+      CU(cudaEventElapsedTime(&ms, ev[q], ev[q + 1]));
+      ms5[q] += ms;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (Meta& m : meta_) m.step = std::min(m.nsteps, m.step + n);
+  return n;
+}
+
+uint64_t TetGroup::step_io(const double* car_in, double* probe_out) {
+  uint64_t left = 0;
+  for (const Meta& m : meta_) left = std::max(left, m.nsteps - m.step);
+  if (left == 0) return 0;
+  double* hin = pinned_;
+  double* hout = pinned_ + io_src_;
+  if (car_in && io_src_) {
+    std::memcpy(hin, car_in, io_src_ * sizeof(double));
+    size_t o = 0;
+    for (const Meta& m : meta_) {
+      if (m.nsrc && m.step < m.nsteps)
+        CU(cudaMemcpyAsync((double*)dev_.carrier + m.car_off + m.step * m.nsrc, hin + o, m.nsrc * sizeof(double),
+                           cudaMemcpyHostToDevice, stream_));
+      o += m.nsrc;
+    }
+  }
+  launch(1, nullptr);
+  size_t o = 0;
+  std::vector<char> got(meta_.size(), 0);
+  for (size_t s = 0; s < meta_.size(); s++) {
+    const Meta& m = meta_[s];
+    const int slot = m.step < m.nsteps ? m.slot_of_step[m.step] : -1;
+    if (probe_out && slot >= 0 && m.np) {
+      CU(cudaMemcpyAsync(hout + o, dev_.samples + m.samp_off + (size_t)slot * m.np * 6, m.np * 6 * sizeof(double),
+                         cudaMemcpyDeviceToHost, stream_));
+      got[s] = 1;
+    }
+    o += m.np * 6;
+  }
+  CU(cudaStreamSynchronize(stream_));
+  o = 0;
+  for (size_t s = 0; s < meta_.size(); s++) {
+    if (got[s]) std::memcpy(probe_out + o, hout + o, meta_[s].np * 6 * sizeof(double));
+    o += meta_[s].np * 6;
+  }
+  for (Meta& m : meta_) m.step = std::min(m.nsteps, m.step + 1);
+  return 1;
+}
+
+size_t TetGroup::n_samples(int s) const {
+  const Meta& m = meta_[s];
+  size_t c = 0;
+  for (uint64_t i = 0; i < m.step && i < m.slot_of_step.size(); i++)
+    if (m.slot_of_step[i] >= 0) c++;
+  return c;
+}
+
+void TetGroup::get_probes(int s, double* times, double* values, size_t cap) const {
+  const Meta& m = meta_[s];
+  size_t ns = std::min(n_samples(s), cap);
+  if (times) std::memcpy(times, m.sample_times.data(), ns * 8);
+  if (values && ns && m.np)
+    CU(cudaMemcpy(values, dev_.samples + m.samp_off, ns * m.np * 6 * 8, cudaMemcpyDeviceToHost));
+}
+
+static void fetch_range(const void* base, int64_t off, size_t n, bool f32, double* out) {
+  if (!out || !n) return;
+  if (!f32) {
+    CU(cudaMemcpy(out, (const double*)base + off, n * 8, cudaMemcpyDeviceToHost));
+    return;
+  }
+  std::vector<float> tmp(n);
+  CU(cudaMemcpy(tmp.data(), (const float*)base + off, n * 4, cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < n; i++) out[i] = tmp[i];
+}
+
+void TetGroup::get_state(int s, double* U, double* B, double* F) {
+  const Meta& m = meta_[s];
+  const bool f32 = opt_.precision == 1;
+  CU(cudaStreamSynchronize(stream_));
+  fetch_range(dev_.U, m.eoff, m.nE, f32, U);
+  fetch_range(dev_.B, m.foff, m.nF, f32, B);
+  fetch_range(dev_.F, m.foff, m.nF, f32, F);
+}
+
+void TetGroup::set_state(int s, const double* U, const double* F) {
+  const Meta& m = meta_[s];
+  const bool f32 = opt_.precision == 1;
+  auto put = [&](void* base, int64_t off, const double* src, size_t n) {
+    if (!src) return;
+    if (!f32) CU(cudaMemcpy((double*)base + off, src, n * 8, cudaMemcpyHostToDevice));
+    else {
+      std::vector<float> t(src, src + n);
+      CU(cudaMemcpy((float*)base + off, t.data(), n * 4, cudaMemcpyHostToDevice));
+    }
+  };
+  CU(cudaStreamSynchronize(stream_));
+  put(dev_.U, m.eoff, U, m.nE);
+  put(dev_.F, m.foff, F, m.nF);
+}
+
+size_t TetGroup::solver_stats(int s, int32_t* iters, double* resid, size_t cap) const {
+  const Meta& m = meta_[s];
+  const size_t n = std::min<size_t>(m.step, cap);
+  if (iters && n) CU(cudaMemcpy(iters, dev_.cg_iters + m.stat_off, n * 4, cudaMemcpyDeviceToHost));
+  if (resid && n) CU(cudaMemcpy(resid, dev_.cg_resid + m.stat_off, n * 8, cudaMemcpyDeviceToHost));
+  return m.step;
+}
+
+void TetGroup::get_flux(int s, double* flux, size_t cap, size_t* n) const {
+  const Meta& m = meta_[s];
+  const size_t k = std::min<size_t>(m.step, cap);
+  if (flux && k) CU(cudaMemcpy(flux, dev_.flux + m.stat_off, k * 8, cudaMemcpyDeviceToHost));
+  if (n) *n = m.step;
+}
+
+template void TetGroup::build<float>(std::vector<TetSim*>&, bool);
+template void TetGroup::build<double>(std::vector<TetSim*>&, bool);
+
+}  // namespace tf

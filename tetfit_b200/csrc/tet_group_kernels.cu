@@ -1,0 +1,523 @@
+// Kernels of a group of gfdtd simulations (Discretization.hpp:1459-1565 per
+// simulation), all simulations advanced by the same launches:
+//
+//   grp_curl_u     B -= dt C U on the faces (3 signed edges per face)
+//   grp_nmul       F = N B (SELL-32)
+//   grp_probes     Whitney E and face-flux H at the probe points (:3768-3897)
+//   grp_sources    one block per simulation: source-edge values from the
+//                  carrier table, boundary flux of the step (:1478-1504)
+//   grp_rhs        Psi = E (U_old - Src) - dt I + dt C^T F + dt Ctb Fb on the
+//                  free rows (:1516-1523) and the CG initial guess
+//   grp_cg         persistent cooperative Jacobi-PCG over every simulation's
+//                  system at once (ConjugateGradientSolver.hpp:52-103), each
+//                  simulation with its own scalars and stopping test
+//   grp_scatter    U[free] = x, U[Dirichlet] = source values (:1540-1541)
+//   grp_bump       step counters of the running simulations
+//
+// CG arithmetic.  Iteration j of the reference computes q = A p_j, alpha_j =
+// rz / p_j.q, x += alpha_j p_j, r -= alpha_j q, z = pre r, beta = rz'/rz,
+// p_{j+1} = z + beta p_j.  Here p alternates between two buffers, and the x
+// update of iteration j is applied while p_{j+1} is formed (p_j is read there
+// anyway), with one final update after the loop.  In the fused variant the
+// SpMV forms p_{j+1} at every gathered column from (pre, r, p_j) with the same
+// explicitly rounded operations the row's owner uses, so p_{j+1} needs no
+// barrier before the SpMV: two grid barriers per iteration instead of three.
+// Both variants give bitwise identical iterates.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include "tet_group_kernels.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace tf {
+
+constexpr int kGB = 256;
+
+__device__ __forceinline__ float fmaT(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmaT(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float mulT(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mulT(double a, double b) { return __dmul_rn(a, b); }
+
+__device__ __forceinline__ bool running(const GroupDev& d, int s) { return d.step[s] < d.nsteps[s]; }
+
+// sum over the row's entries, in stored order, of val * g(col).  Entries
+// are taken 8 at a time: the index and value loads of a chunk are all issued
+// before its gathers, so a row costs about two memory latencies instead of
+// one per entry group.
+template <typename T, typename G>
+__device__ __forceinline__ T sell_dot(const SellDev& m, int64_t row, G g) {
+  constexpr int CH = 8;
+  const int64_t sl = row >> 5;
+  const int64_t b = m.ptr[sl];
+  const int len = (int)((m.ptr[sl + 1] - b) >> 5);
+  const int32_t* col = m.col + b + (row & 31);
+  const T* val = (const T*)m.val + b + (row & 31);
+  T s = 0;
+  for (int j0 = 0; j0 < len; j0 += CH) {
+    int32_t c[CH];
+    T v[CH];
+#pragma unroll
+    for (int k = 0; k < CH; k++)
+      if (j0 + k < len) {
+        c[k] = __ldg(col + 32 * (j0 + k));
+        v[k] = __ldg(val + 32 * (j0 + k));
+      }
+#pragma unroll
+    for (int k = 0; k < CH; k++)
+      if (j0 + k < len) s += v[k] * g(c[k]);
+  }
+  return s;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// deterministic block sum of one double (all threads get the result)
+__device__ double grp_block_sum(double v, double* sh) {
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    s = warp_sum(s);
+    if (threadIdx.x == 0) sh[32] = s;
+  }
+  __syncthreads();
+  return sh[32];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kGB) grp_curl_u(GroupDev d) {
+  const int64_t f = (int64_t)blockIdx.x * kGB + threadIdx.x;
+  if (f >= d.nF) return;
+  const int s = d.fslice_sim[f >> 5];
+  if (!running(d, s)) return;
+  const int32_t* e = d.fte + 3 * f;
+  const int32_t e0 = e[0];
+  if (e0 < 0) return;
+  const T* U = (const T*)d.U;
+  const T c = U[e0] - U[e[1]] + U[e[2]];
+  T* B = (T*)d.B;
+  B[f] = B[f] - (T)d.dt[s] * c;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kGB) grp_nmul(GroupDev d) {
+  const int64_t f = (int64_t)blockIdx.x * kGB + threadIdx.x;
+  if (f >= d.nF) return;
+  if (!running(d, d.fslice_sim[f >> 5])) return;
+  const T* B = (const T*)d.B;
+  ((T*)d.F)[f] = sell_dot<T>(d.N, f, [&](int32_t c) { return B[c]; });
+}
+
+// gfdtd exports U^{i-1} and B^{i-1/2} inside step i (Discretization.hpp:1469-1475)
+template <typename T>
+__global__ void grp_probes(GroupDev d) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= d.np) return;
+  const int s = d.probe_sim[p];
+  if (!running(d, s)) return;
+  const int slot = d.sched[d.sched_off[s] + d.step[s]];
+  if (slot < 0) return;
+  const T* U = (const T*)d.U;
+  const T* B = (const T*)d.B;
+  double E[3] = {0, 0, 0}, H[3] = {0, 0, 0};
+  for (int q = 0; q < 6; q++) {
+    const double u = (double)U[d.p_edges[6 * p + q]];
+    for (int a = 0; a < 3; a++) E[a] += d.p_we[18 * p + 3 * q + a] * u;
+  }
+  for (int q = 0; q < 4; q++) {
+    const double b = (double)B[d.p_faces[4 * p + q]];
+    for (int a = 0; a < 3; a++) H[a] += d.p_hf[12 * p + 3 * q + a] * b;
+  }
+  const int64_t nps = d.sim_probe[s + 1] - d.sim_probe[s];
+  double* out = d.samples + d.samp_off[s] + ((int64_t)slot * nps + (p - d.sim_probe[s])) * 6;
+  for (int a = 0; a < 3; a++) {
+    out[a] = E[a];
+    out[3 + a] = H[a];
+  }
+}
+
+// One block per simulation.  E sources write the Dirichlet values, H sources
+// the boundary dual-edge term, currents I; the step's flux sum is
+// U_prev . 0.5 (Fb(t) + Fb(t - dt)) over the H-source edges.
+template <typename T>
+__global__ void __launch_bounds__(kGB) grp_sources(GroupDev d) {
+  __shared__ double sh[33];
+  const int s = blockIdx.x;
+  if (!running(d, s)) return;
+  const int step = d.step[s];
+  const int ns = d.nsrc[s];
+  const double* car = d.carrier + d.car_off[s];
+  const int s0 = d.src_off[s];
+  double fl = 0.0;
+  for (int k = d.sim_se[s] + threadIdx.x; k < d.sim_se[s + 1]; k += kGB) {
+    auto value = [&](int row) {
+      double v[3] = {0.0, 0.0, 0.0};
+      for (int p = d.se_begin[k]; p < d.se_begin[k + 1]; p++) {
+        const int si = d.pair_src[p];
+        double ret = d.src_amp[si] * car[(int64_t)row * ns + (si - s0)];
+        ret *= d.pair_fac[4 * p + 0];
+        ret *= d.pair_fac[4 * p + 1];
+        ret *= d.pair_fac[4 * p + 2];
+        ret *= d.pair_fac[4 * p + 3];
+        v[d.pair_dir[p]] += ret;
+      }
+      const double* w = d.se_vec + 3 * (int64_t)k;
+      return d.se_post[k] * ((v[0] * w[0] + v[1] * w[1]) + v[2] * w[2]);
+    };
+    const int e = d.se_edge[k];
+    const int kind = d.se_kind[k];
+    const double val = value(step);
+    if (kind == 1) {
+      ((T*)d.src)[e] = (T)val;
+    } else if (kind == 2) {
+      ((T*)d.cb)[e] = (T)val;
+      const double prev = step > 0 ? value(step - 1) : 0.0;
+      fl += (double)((const T*)d.U)[e] * (0.5 * (val + prev));
+    } else if (kind == 3) {
+      ((T*)d.I)[e] = (T)val;
+    }
+  }
+  fl = grp_block_sum(fl, sh);
+  if (threadIdx.x == 0) d.flux[d.stat_off[s] + step] = fl;
+}
+
+// Right-hand side on the free rows and the initial guess: 0 previous
+// solution (x kept), 1 zero, 2 quadratic extrapolation from the last three
+// solutions (history shifted here).
+template <typename T>
+__global__ void __launch_bounds__(kGB) grp_rhs(GroupDev d) {
+  const int64_t i = (int64_t)blockIdx.x * kGB + threadIdx.x;
+  if (i >= d.nrow) return;
+  const int s = d.slice_sim[i >> 5];
+  if (!running(d, s)) return;
+  const int32_t e = d.free_edge[i];
+  if (e < 0) return;
+  const T* U = (const T*)d.U;
+  const T* S = (const T*)d.src;
+  const T* F = (const T*)d.F;
+  const T eu = sell_dot<T>(d.Ef, i, [&](int32_t c) { return U[c] - S[c]; });
+  T cf = 0;
+  {
+    const int64_t sl = i >> 5;
+    const int64_t b = d.Ct.ptr[sl];
+    const int len = (int)((d.Ct.ptr[sl + 1] - b) >> 5);
+    const int32_t* col = d.Ct.col + b + (i & 31);
+    for (int j = 0; j < len; j++) {
+      const int32_t c = __ldg(col + 32 * j);
+      if (c == kPadCol) break;
+      const T v = F[c & 0x7fffffff];
+      cf = c < 0 ? cf - v : cf + v;
+    }
+  }
+  const T dt = (T)d.dt[s];
+  ((T*)d.rhs)[i] = eu - dt * ((const T*)d.I)[e] + dt * cf + dt * ((const T*)d.cb)[e];
+  T* x = (T*)d.x;
+  if (d.warm_start == 1) {
+    x[i] = 0;
+  } else if (d.warm_start == 2) {
+    T* h1 = (T*)d.xh1;
+    T* h2 = (T*)d.xh2;
+    T* h3 = (T*)d.xh3;
+    const int step = d.step[s];
+    const T a = x[i], b = h1[i], c = h2[i];
+    h3[i] = c;
+    h2[i] = b;
+    h1[i] = a;
+    if (step >= 3) x[i] = (T)3 * a - (T)3 * b + c;
+    else if (step >= 2) x[i] = (T)2 * a - b;
+  }
+}
+
+struct SimCg {
+  double rz, res0, bnorm, res, alpha, beta;
+  int it, active;
+};
+
+// p_{j+1} at one row, rounded the same way wherever it is formed
+template <typename T>
+__device__ __forceinline__ T p_next(T pre, T r, T pold, T beta, bool first) {
+  const T z = mulT(pre, r);
+  return first ? z : fmaT(beta, pold, z);
+}
+
+template <typename T, bool kFused>
+__global__ void __launch_bounds__(kCgThreads, 2) grp_cg(GroupDev d) {
+  cg::grid_group grid = cg::this_grid();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SimCg* st = reinterpret_cast<SimCg*>(smem_raw);
+  double* wp = reinterpret_cast<double*>(smem_raw + sizeof(SimCg) * d.S);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g0 = d.blk_seg[blockIdx.x], g1 = d.blk_seg[blockIdx.x + 1];
+  T* x = (T*)d.x;
+  T* r = (T*)d.r;
+  T* q = (T*)d.q;
+  const T* b = (const T*)d.rhs;
+  const T* pre = (const T*)d.pre;
+  auto pbuf = [&](int k) { return (k & 1) ? (T*)d.p1 : (T*)d.p0; };
+
+  auto flush = [&](int g, double a0, double a1, double a2) {
+    a0 = warp_sum(a0);
+    a1 = warp_sum(a1);
+    a2 = warp_sum(a2);
+    if (lane == 0) {
+      double* w = wp + ((g - g0) * kCgWarps + warp) * 3;
+      w[0] = a0;
+      w[1] = a1;
+      w[2] = a2;
+    }
+  };
+  auto publish = [&](int nq) {
+    __syncthreads();
+    for (int gl = threadIdx.x; gl < g1 - g0; gl += kCgThreads)
+      for (int k = 0; k < nq; k++) {
+        double a = 0.0;
+        for (int w = 0; w < kCgWarps; w++) a += wp[(gl * kCgWarps + w) * 3 + k];
+        d.part[3 * (int64_t)(g0 + gl) + k] = a;
+      }
+  };
+  // per-simulation totals of the published partials: one warp per
+  // simulation, lanes over its segments, then a fixed shuffle tree; f(s, t)
+  // runs on lane 0 with the nq totals t[]
+  auto totals = [&](int nq, auto&& f) {
+    for (int s = warp; s < d.S; s += kCgWarps) {
+      double t[3] = {0.0, 0.0, 0.0};
+      for (int g = d.sim_seg[s] + lane; g < d.sim_seg[s + 1]; g += 32)
+        for (int k = 0; k < nq; k++) t[k] += d.part[3 * (int64_t)g + k];
+      for (int k = 0; k < nq; k++) t[k] = warp_sum(t[k]);
+      if (lane == 0) f(s, t);
+    }
+  };
+  auto go_on = [&](const SimCg& c, int s) {
+    if (c.it >= d.cg_maxiter) return false;
+    if (d.cg_criterion == 0) return c.res / c.res0 > d.tol[s];  // NaN (res0 = 0) stops, as the reference
+    return c.res > d.tol[s] * c.bnorm;
+  };
+
+  // r = b - A x; rr = r.r, rz = r.(pre r), bb = b.b
+  for (int g = g0; g < g1; g++) {
+    const int s = d.seg_sim[g];
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    if (running(d, s))
+      for (int64_t sl = d.seg_s0[g] + warp; sl < d.seg_s1[g]; sl += kCgWarps) {
+        const int64_t i = sl * 32 + lane;
+        const T ri = b[i] - sell_dot<T>(d.A, i, [&](int32_t c) { return x[c]; });
+        r[i] = ri;
+        const double rd = (double)ri;
+        a0 += rd * rd;
+        a1 += rd * (double)(pre[i] * ri);
+        a2 += (double)b[i] * (double)b[i];
+      }
+    flush(g, a0, a1, a2);
+  }
+  publish(3);
+  grid.sync();
+  totals(3, [&](int s, const double* t) {
+    SimCg c;
+    c.res0 = sqrt(t[0]);
+    c.rz = t[1];
+    c.bnorm = sqrt(t[2]);
+    c.res = c.res0;
+    c.alpha = c.beta = 0.0;
+    c.it = 0;
+    c.active = running(d, s) && go_on(c, s);
+    st[s] = c;
+  });
+  __syncthreads();
+
+  for (;;) {
+    int any = 0;
+    for (int s = threadIdx.x; s < d.S; s += kCgThreads) any |= st[s].active;
+    if (!__syncthreads_or(any)) break;
+    // p_{j+1} = z + beta p_j, x += alpha_j p_j (lazy), and in the fused
+    // variant q = A p_{j+1} with p.q partials
+    for (int g = g0; g < g1; g++) {
+      const int s = d.seg_sim[g];
+      const SimCg c = st[s];
+      double a0 = 0.0;
+      if (c.active) {
+        const bool first = c.it == 0;
+        const T beta = (T)c.beta, alpha = (T)c.alpha;
+        const T* pold = pbuf(c.it + 1);
+        T* pn = pbuf(c.it);
+        for (int64_t sl = d.seg_s0[g] + warp; sl < d.seg_s1[g]; sl += kCgWarps) {
+          const int64_t i = sl * 32 + lane;
+          const T po = first ? (T)0 : pold[i];
+          const T pi = p_next<T>(pre[i], r[i], po, beta, first);
+          if (!first) x[i] = fmaT(alpha, po, x[i]);
+          pn[i] = pi;
+          if (kFused) {
+            const T qi = sell_dot<T>(d.A, i, [&](int32_t cc) {
+              return p_next<T>(__ldg(pre + cc), r[cc], first ? (T)0 : pold[cc], beta, first);
+            });
+            q[i] = qi;
+            a0 += (double)pi * (double)qi;
+          }
+        }
+      }
+      if (kFused) flush(g, a0, 0.0, 0.0);
+    }
+    if (!kFused) {
+      grid.sync();
+      for (int g = g0; g < g1; g++) {
+        const int s = d.seg_sim[g];
+        const SimCg c = st[s];
+        double a0 = 0.0;
+        if (c.active) {
+          const T* pn = pbuf(c.it);
+          for (int64_t sl = d.seg_s0[g] + warp; sl < d.seg_s1[g]; sl += kCgWarps) {
+            const int64_t i = sl * 32 + lane;
+            const T qi = sell_dot<T>(d.A, i, [&](int32_t cc) { return pn[cc]; });
+            q[i] = qi;
+            a0 += (double)pn[i] * (double)qi;
+          }
+        }
+        flush(g, a0, 0.0, 0.0);
+      }
+    }
+    publish(1);
+    grid.sync();
+    totals(1, [&](int s, const double* t) {
+      if (st[s].active) st[s].alpha = st[s].rz / t[0];
+    });
+    __syncthreads();
+    // r -= alpha q; rr, rz partials
+    for (int g = g0; g < g1; g++) {
+      const int s = d.seg_sim[g];
+      double a0 = 0.0, a1 = 0.0;
+      if (st[s].active) {
+        const T alpha = (T)st[s].alpha;
+        for (int64_t sl = d.seg_s0[g] + warp; sl < d.seg_s1[g]; sl += kCgWarps) {
+          const int64_t i = sl * 32 + lane;
+          const T ri = r[i] - alpha * q[i];
+          r[i] = ri;
+          const double rd = (double)ri;
+          a0 += rd * rd;
+          a1 += rd * (double)(pre[i] * ri);
+        }
+      }
+      flush(g, a0, a1, 0.0);
+    }
+    publish(2);
+    grid.sync();
+    totals(2, [&](int s, const double* t) {
+      SimCg c = st[s];
+      if (!c.active) return;
+      const double rz_prev = c.rz;
+      c.res = sqrt(t[0]);
+      c.rz = t[1];
+      c.it++;
+      c.beta = c.rz / rz_prev;
+      c.active = go_on(c, s);
+      st[s] = c;
+    });
+    __syncthreads();
+  }
+  // the last x update, x += alpha_{J-1} p_{J-1}
+  for (int g = g0; g < g1; g++) {
+    const int s = d.seg_sim[g];
+    const SimCg c = st[s];
+    if (!running(d, s) || c.it == 0) continue;
+    const T alpha = (T)c.alpha;
+    const T* pl = pbuf(c.it - 1);
+    for (int64_t sl = d.seg_s0[g] + warp; sl < d.seg_s1[g]; sl += kCgWarps) {
+      const int64_t i = sl * 32 + lane;
+      x[i] = fmaT(alpha, pl[i], x[i]);
+    }
+  }
+  if (blockIdx.x == 0)
+    for (int s = threadIdx.x; s < d.S; s += kCgThreads) {
+      if (!running(d, s)) continue;
+      const SimCg c = st[s];
+      const int64_t k = d.stat_off[s] + d.step[s];
+      d.cg_iters[k] = c.it;
+      d.cg_resid[k] = c.res / c.res0;
+      const bool unmet = d.cg_criterion == 0 ? c.res / c.res0 > d.tol[s] : c.res > d.tol[s] * c.bnorm;
+      d.cg_limit[k] = unmet ? 1 : 0;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kGB) grp_scatter(GroupDev d) {
+  const int64_t k = (int64_t)blockIdx.x * kGB + threadIdx.x;
+  T* U = (T*)d.U;
+  if (k < d.nrow) {
+    const int32_t e = d.free_edge[k];
+    if (e >= 0) U[e] = ((const T*)d.x)[k];
+  }
+  if (k < d.ndir) {
+    const int32_t e = d.dir_edge[k];
+    U[e] = ((const T*)d.src)[e];
+  }
+}
+
+__global__ void grp_bump(GroupDev d) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < d.S && d.step[s] < d.nsteps[s]) d.step[s] += 1;
+}
+
+// ------------------------------------------------------------------ launch
+static inline unsigned gblk(int64_t n) { return (unsigned)(n > 0 ? (n + kGB - 1) / kGB : 1); }
+
+static size_t cg_smem(int S) { return sizeof(SimCg) * (size_t)S + sizeof(double) * kMaxSeg * kCgWarps * 3; }
+
+template <typename T>
+int group_cg_blocks(int device, int S, size_t* smem) {
+  const size_t sm = cg_smem(S);
+  if (smem) *smem = sm;
+  int sms = 0, a = 0, b = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (cudaFuncSetAttribute(grp_cg<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess ||
+      cudaFuncSetAttribute(grp_cg<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+    return 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, grp_cg<T, true>, kCgThreads, sm);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, grp_cg<T, false>, kCgThreads, sm);
+  return (a < b ? a : b) * sms;
+}
+
+// One step of every running simulation.  ev (optional, 6 events) brackets:
+// H update + probes, sources + rhs, CG, scatter, step end.
+template <typename T>
+cudaError_t group_launch_step(const GroupDev& d, int cg_blocks, int cg_variant, size_t smem, cudaStream_t st,
+                              cudaEvent_t* ev) {
+  if (ev) cudaEventRecord(ev[0], st);
+  grp_curl_u<T><<<gblk(d.nF), kGB, 0, st>>>(d);
+  grp_nmul<T><<<gblk(d.nF), kGB, 0, st>>>(d);
+  if (d.np) grp_probes<T><<<(unsigned)((d.np + 127) / 128), 128, 0, st>>>(d);
+  if (ev) cudaEventRecord(ev[1], st);
+  grp_sources<T><<<d.S, kGB, 0, st>>>(d);
+  grp_rhs<T><<<gblk(d.nrow), kGB, 0, st>>>(d);
+  if (ev) cudaEventRecord(ev[2], st);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cg_blocks);
+  cfg.blockDim = dim3(kCgThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t err = cg_variant == 0 ? cudaLaunchKernelEx(&cfg, grp_cg<T, true>, d)
+                                    : cudaLaunchKernelEx(&cfg, grp_cg<T, false>, d);
+  if (err != cudaSuccess) return err;
+  if (ev) cudaEventRecord(ev[3], st);
+  grp_scatter<T><<<gblk(d.nrow > d.ndir ? d.nrow : d.ndir), kGB, 0, st>>>(d);
+  if (ev) cudaEventRecord(ev[4], st);
+  grp_bump<<<(d.S + 127) / 128, 128, 0, st>>>(d);
+  if (ev) cudaEventRecord(ev[5], st);
+  return cudaGetLastError();
+}
+
+template cudaError_t group_launch_step<double>(const GroupDev&, int, int, size_t, cudaStream_t, cudaEvent_t*);
+template cudaError_t group_launch_step<float>(const GroupDev&, int, int, size_t, cudaStream_t, cudaEvent_t*);
+template int group_cg_blocks<double>(int, int, size_t*);
+template int group_cg_blocks<float>(int, int, size_t*);
+
+}  // namespace tf
