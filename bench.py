@@ -1,10 +1,16 @@
 """Benchmark of the leapfrog time-stepping path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload fit512|fit64]
+                    [--workload batch128|fit512|gfdtd24|...]
 
 A step is one leapfrog step (E half, sources, probe export, H half) over the
-whole workload.  Default workload `fit512`: the 512^3-cell Cartesian FIT cavity
+whole workload.  Default workload `batch128`: 128 independent gfdtd
+simulations (Kuhn meshes of 8^3..48^3 cubes, own materials, sources and time
+steps) advanced together in one device image, FP32 fields with FP64 CG
+reductions, CG to ||r|| <= 1e-8 ||b||; the JSON line also carries the plain
+FP64 arm (the same members one at a time, previous-solution guess) and the
+probe error of small members against the FP64 CPU oracle.  Workload `fit512`:
+the 512^3-cell Cartesian FIT cavity
 with 200 seeded lossy dielectric spheres over vacuum, PEC on surfaces 2-6 and
 the H-wave source on surface 1, FP32 field state (807,667,200 edge+face dofs;
 the field arrays, 3.3 GB, are far larger than the 126 MB L2, so no flush is
@@ -47,6 +53,11 @@ WORKLOADS = {
     "dga24": dict(kind="tet", method="dga", n=24, prec="fp64", steps=1200, cpu_n=24),
     "gfdtd96": dict(kind="tet", method="gfdtd", n=96, prec="fp32", steps=5000, grf=True, cpu_n=24),
     "gfdtd96_fp64": dict(kind="tet", method="gfdtd", n=96, prec="fp64", steps=5000, grf=True, cpu_n=24),
+    # batched gfdtd (SURVEY cfg3): 128 members, n ~ U{8..48}, FP32 fields, FP64 CG reductions, CG to
+    # ||r|| <= 1e-8 ||b||; the plain arm runs the same members one at a time in FP64 with the
+    # reference's previous-solution guess
+    "batch128": dict(kind="batch", members=128, n_lo=8, n_hi=48, steps=1000, seed=31337, prec="fp32",
+                     warm="extrapolate", crit="rhs", plain_steps=10),
 }
 
 
@@ -286,6 +297,193 @@ def run_ours(args, rank, world, local_rank):
     return result
 
 
+def cg_bytes_per_launch(infos, its, es):
+    """Algorithmic bytes of one grp_cg launch: per member and iteration the
+    stored entries of A (int32 column + value) and 11 row-vector accesses
+    (p-update/SpMV phase: z, r, p_old, x read, x, p_new, q written; residual
+    phase: r, q, pre read, r written), plus the initial residual (A once and
+    b, x, pre, r) and the final x update (x, p read, x written)."""
+    total = 0.0
+    for info, it in zip(infos, its):
+        nnz, n = info["nnz_system"], info["n_free"]
+        total += it * (nnz * (4 + es) + 11 * es * n) + nnz * (4 + es) + 4 * es * n + 3 * es * n
+    return total
+
+
+def member_carriers(infos, cases, steps_done):
+    """The scripts' own H-wave carrier values (sin, source amplitude applied
+    on the device) for each member's next step: t = (i + 1) dt - dt / 2."""
+    out = []
+    for info, case, i in zip(infos, cases, steps_done):
+        t = (i + 1) * info["dt"] - 0.5 * info["dt"]
+        out += [np.sin(2 * np.pi * case.frequency * t)] * info["n_sources"]
+    return np.asarray(out if out else [0.0])
+
+
+def run_batch(args, rank, world, local_rank):
+    import tetfit_b200 as tb
+    from tetfit_b200.cases import batch_cases, write_batch
+    w = WORKLOADS[args.workload]
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist_
+        dist = dist_
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+
+    def barrier():
+        if dist:
+            import torch
+            torch.cuda.synchronize()
+            dist.barrier()
+
+    # every rank runs its own batch of members (independent replicas)
+    cases = batch_cases(w["members"], w["n_lo"], w["n_hi"], steps=w["steps"], seed=w["seed"] + rank)
+    work = tempfile.mkdtemp(prefix=f"tfbatch{rank}_")
+    t0 = time.time()
+    members = write_batch(work, cases)
+    write_s = time.time() - t0
+    es = 4 if w["prec"] == "fp32" else 8
+    t0 = time.time()
+    b = tb.Batch(members, precision=w["prec"], cg_criterion=w["crit"], warm_start=w["warm"], device=local_rank)
+    setup_s = time.time() - t0
+    infos = [b.info(m) for m in range(b.size)]
+    dofs = sum(i["n_edges"] + i["n_faces"] for i in infos)
+    K, W = args.steps, args.warmup
+    nph = min(K, 10)
+    K2 = min(K, 20)
+    need = W + nph + K + K2
+    if need > w["steps"]:
+        raise SystemExit(f"batch members have {w['steps']} steps, bench needs {need}")
+    b.step(W)
+    ms5, _ = b.phase_times(nph)
+    its_ph = [b.solver_stats(m)[0][W:W + nph].mean() for m in range(b.size)]
+    cg_bytes = cg_bytes_per_launch(infos, its_ph, es)
+    cg_ms = ms5[2] / nph
+    barrier()
+    with ClockSampler(local_rank) as clk:
+        b.step(K)
+        dev_ms = b.last_step_ms()
+    barrier()
+    stats = [b.solver_stats(m)[0] for m in range(b.size)]
+    it_timed = float(np.mean([s[W + nph:W + nph + K].mean() for s in stats]))
+    # e2e: tf_batch_step_io, every member's carrier values H2D and probe samples D2H each step
+    n_src = sum(i["n_sources"] for i in infos)
+    n_probe_vals = 6 * sum(i["n_probes"] for i in infos)
+    probes = np.zeros(max(n_probe_vals, 1))
+    done = [W + nph + K] * b.size
+    barrier()
+    t0 = time.perf_counter()
+    for k in range(K2):
+        b.step_io(member_carriers(infos, cases, [d_ + k for d_ in done]), probes)
+    e2e_s = time.perf_counter() - t0
+    barrier()
+    # probe error of the small members against the FP64 CPU oracle over all steps taken
+    perr = []
+    if rank == 0:
+        import oracle
+        small = [m for m in range(b.size) if cases[m].n <= 10][:2]
+        for m in small:
+            t_, v_ = b.probes(m)
+            o = oracle.TetOracle(members[m][0])
+            o.step(len(t_))
+            vo = o.probes()[1]
+            o.close()
+            perr.append(float(np.linalg.norm(v_ - vo) / max(np.linalg.norm(vo), 1e-300)))
+    kps = infos[0]["kernels_per_step"]
+    b.close()
+    # plain arm: the same members one at a time in FP64, previous-solution guess
+    t0 = time.time()
+    p = tb.Batch(members, precision="fp64", batch_mode="serial", cg_criterion=w["crit"], warm_start="previous",
+                 device=local_rank)
+    plain_setup_s = time.time() - t0
+    p.step(3)
+    Kp = w["plain_steps"]
+    barrier()
+    p.step(Kp)
+    plain_ms = p.last_step_ms()
+    barrier()
+    plain_it = float(np.mean([p.solver_stats(m)[0][3:3 + Kp].mean() for m in range(p.size)]))
+    p.close()
+    max_ms, max_e2e, max_plain = dev_ms, e2e_s, plain_ms
+    if dist:
+        import torch
+        t = torch.tensor([dev_ms, e2e_s, plain_ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        max_ms, max_e2e, max_plain = (float(x) for x in t)
+    result = None
+    if rank == 0:
+        peak, peak_kind = hbm_peak()
+        achieved = cg_bytes / (cg_ms * 1e-3) / 1e9
+        value = world * dofs * K / (max_ms * 1e-3)
+        plain_value = world * dofs * Kp / (max_plain * 1e-3)
+        ns = sorted(c.n for c in cases)
+        result = {
+            "metric": "dof-steps/s", "value": value, "unit": "dof-steps/s", "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": max_ms / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if es == 4 else "f64", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: {w['members']} gfdtd members in one group, Kuhn meshes "
+                                   f"n ~ U{{{w['n_lo']}..{w['n_hi']}}} (min {ns[0]}, median {ns[len(ns) // 2]}, "
+                                   f"max {ns[-1]}) x 6 tets, eps_r ~ U[1,4] per x-half, f ~ U[1e8,4e8] Hz, "
+                                   f"{w['prec']} fields, FP64 CG reductions, CG tol 1e-8 (||r|| <= tol ||b||), "
+                                   f"{w['warm']} warm start",
+                       "members": w["members"], "dofs": dofs, "parallelism": f"replicas x{world}",
+                       "l2": f"CG working set {cg_bytes / max(it_timed, 1) / 1e6:.0f} MB per iteration > 126 MB L2 "
+                             f"(no flush needed)",
+                       "setup_s": round(setup_s, 1), "mesh_write_s": round(write_s, 1),
+                       "cg_iterations_mean": it_timed, "cg_variant": infos[0]["cg_variant"],
+                       "cg_blocks": infos[0]["cg_blocks"]},
+            "roofline": {"bound": "hbm", "kernel": "grp_cg", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                         "algorithmic_bytes": cg_bytes, "launch_ms": cg_ms},
+            "phases_ms_per_step": {k: v / nph for k, v in zip(
+                ["h_update_probes", "sources_rhs", "cg_solve", "scatter", "step_end"], ms5)},
+            "plain_fp64": {"value": plain_value, "unit": "dof-steps/s", "ms_per_step": max_plain / Kp,
+                           "steps": Kp, "cg_iterations_mean": plain_it, "setup_s": round(plain_setup_s, 1),
+                           "mode": "members one at a time, FP64, previous-solution guess, same CG tolerance",
+                           "speedup": value / plain_value},
+            "probe_error_vs_fp64_oracle": {"members": len(perr), "max_rel_l2": max(perr) if perr else None},
+            "e2e": {"value": world * dofs * K2 / max_e2e, "unit": "dof-steps/s",
+                    "h2d_bytes_per_step": 8 * n_src, "d2h_bytes_per_step": 8 * n_probe_vals,
+                    "api": "tf_batch_step_io"},
+            "gpu_launches": kps * K,
+            "clocks": clk.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            result["cpu_baseline"] = batch_cpu_baseline(cases, members, seconds=args.cpu_seconds)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def batch_cpu_baseline(cases, members, seconds=15.0):
+    """FP64 CPU restatement, single thread, stepping members in order for a
+    bounded time (the reference runs a script's simulations one by one)."""
+    import oracle
+    os.environ["TF_ORACLE_SKIP_DT"] = "1"
+    t_all, dofs_steps, used = 0.0, 0.0, 0
+    for (script, _), case in zip(members, cases):
+        if t_all >= seconds:
+            break
+        o = oracle.TetOracle(script)
+        dofs = o.nE + o.nF
+        o.step(1)
+        t0 = time.perf_counter()
+        k = 0
+        while time.perf_counter() - t0 < max(seconds - t_all, 0.5) / 2 and k < 200:
+            k += o.step(1)
+        el = time.perf_counter() - t0
+        o.close()
+        t_all += el
+        dofs_steps += dofs * k
+        used += 1
+    return {"value": dofs_steps / t_all, "unit": "dof-steps/s", "cores": 1, "kind": "port",
+            "sample": f"first {used} batch members stepped one after another (FP64), {t_all:.1f} s",
+            "cpu": _cpu_model()}
+
+
 def cpu_baseline(args, seconds=15.0, threads=None):
     """FP64 CPU restatement of the reference on a bounded sample of the scene."""
     import oracle
@@ -370,13 +568,60 @@ def run_reference(args, rank):
             "e2e": {"value": v, "unit": "dof-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def _ref_member(arg):
+    """Worker: the FP64 restatement of the reference on one batch member."""
+    script, warm, steps = arg
+    os.environ["TF_ORACLE_SKIP_DT"] = "1"
+    os.environ["OMP_NUM_THREADS"] = "1"
+    import oracle
+    o = oracle.TetOracle(script)
+    dofs = o.nE + o.nF
+    o.step(warm)
+    t0 = time.perf_counter()
+    o.step(steps)
+    el = time.perf_counter() - t0
+    o.close()
+    return dofs, el
+
+
+def run_batch_reference(args, rank):
+    """The reference's CPU path on the batch: members are independent
+    simulations, so every host thread runs one member (one process each);
+    the sample is the first members of the batch with n <= 24, one per host
+    thread, each advanced warmup + steps steps."""
+    if rank != 0:
+        return None
+    import multiprocessing as mp
+    from tetfit_b200.cases import batch_cases, write_batch
+    w = WORKLOADS[args.workload]
+    cases = batch_cases(w["members"], w["n_lo"], w["n_hi"], steps=w["steps"], seed=w["seed"])
+    threads = os.cpu_count() or 1
+    pick = [i for i, c in enumerate(cases) if c.n <= 24][:threads]
+    work = tempfile.mkdtemp(prefix="tfbref_")
+    members = write_batch(work, [cases[i] for i in pick])
+    with mp.get_context("spawn").Pool(len(members)) as pool:
+        res = pool.map(_ref_member, [(m[0], args.warmup, args.steps) for m in members], chunksize=1)
+    el = max(r[1] for r in res)
+    dofs = sum(r[0] for r in res)
+    v = dofs * args.steps / el
+    sample = (f"{len(members)} batch members with n <= 24 (one per host thread), FP64 C++ restatement of the "
+              f"reference (reference needs Eigen/Spectra/GSL/Silo, not buildable here), {args.steps} steps each")
+    return {"impl": "reference", "metric": "dof-steps/s", "value": v, "unit": "dof-steps/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": f"{args.workload} (bounded CPU sample)"},
+            "cpu_baseline": {"value": v, "unit": "dof-steps/s", "cores": len(members), "kind": "port",
+                             "sample": sample, "cpu": _cpu_model()},
+            "e2e": {"value": v, "unit": "dof-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="fit512", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="batch128", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()
@@ -385,7 +630,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
-        out = run_reference(args, rank)
+        out = run_reference(args, rank) if WORKLOADS[args.workload]["kind"] != "batch" \
+            else run_batch_reference(args, rank)
+    elif WORKLOADS[args.workload]["kind"] == "batch":
+        out = run_batch(args, rank, world, local_rank)
     else:
         out = run_ours(args, rank, world, local_rank)
     if rank == 0 and out is not None:

@@ -286,3 +286,40 @@ def grf_materials(k_levels: int = 24, corr: float = 0.1, seed: int = 4242, grid:
         return np.asarray(labels)[q]
 
     return material, table, qerr
+
+
+def batch_cases(count: int = 128, n_lo: int = 8, n_hi: int = 48, steps: int = 1000, seed: int = 31337,
+                tolerance: float = 1e-8, probes: bool = True) -> list:
+    """Independent gfdtd runs for a batch: mesh n ~ U{n_lo..n_hi} cubes per
+    side (6 Kuhn tetrahedra each, interior vertices jittered +-0.15 h by a
+    per-member seed), eps_r ~ U[1,4] on each x-half (materials 1 and 2), PEC on
+    surfaces 2-6, an H-wave source on surface 1 with f ~ U[1e8,4e8] Hz, the
+    member's own pinned step 0.25 h / c0 and `steps` steps each."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(rng.integers(n_lo, n_hi + 1))
+        e1, e2 = (float(v) for v in rng.uniform(1.0, 4.0, 2))
+        f = float(rng.uniform(1e8, 4e8))
+        out.append(TetCase(n=n, method="gfdtd", steps=steps, split_x=True, eps=(e1, e2), frequency=f,
+                           seed=int(rng.integers(1, 2 ** 31)), tolerance=tolerance, probes=probes))
+    return out
+
+
+def _write_member(arg):
+    directory, i, case = arg
+    return write_tet_case(os.path.join(directory, f"m{i:04d}"), case)
+
+
+def write_batch(directory: str, cases: list, processes: int = 0) -> list:
+    """Write every member's mesh and script (in parallel worker processes);
+    return [(script path, simulation label 1), ...] in member order."""
+    import multiprocessing as mp
+    args = [(directory, i, c) for i, c in enumerate(cases)]
+    procs = processes or min(len(cases), os.cpu_count() or 1, 32)
+    if procs <= 1:
+        paths = [_write_member(a) for a in args]
+    else:
+        with mp.get_context("spawn").Pool(procs) as pool:
+            paths = pool.map(_write_member, args, chunksize=1)
+    return [(p, 1) for p in paths]

@@ -153,7 +153,7 @@ int tf_batch_info(tf_batch* b, uint32_t m, tf_info* info) {
   info->kernels_per_step = (uint32_t)grp.kernels_per_step();
   info->n_sources = (uint32_t)t.n_sources();
   info->n_free = t.n_free();
-  info->nnz_system = grp.nnz_A();
+  info->nnz_system = grp.nnz_A(k);
   info->cg_blocks = (uint32_t)grp.cg_blocks();
   info->cg_variant = grp.cg_variant();
   return TF_OK;

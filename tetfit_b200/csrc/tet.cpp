@@ -23,6 +23,7 @@
 #include <stdexcept>
 
 #include "cuda_util.hpp"
+#include "tet_group.hpp"
 
 namespace tf {
 
@@ -174,7 +175,17 @@ TetSim::TetSim(Script& sc, uint32_t label, const RunOptions& opt, bool device)
     }
   }
   build_sources();
-  if (device) alloc_and_upload();
+  if (!device) return;
+  if (method_ == 2) group_.reset(new TetGroup({this}, opt_, false));
+  else alloc_and_upload();
+}
+
+uint64_t TetSim::device_bytes() const { return group_ ? group_->device_bytes() : dev_bytes_; }
+double TetSim::last_step_ms() const { return group_ ? group_->last_step_ms() : last_ms_; }
+int TetSim::kernels_per_step() const {
+  if (group_) return group_->kernels_per_step();
+  const int np = probe_tet_.empty() ? 0 : 1;
+  return 6 + np + (src_edge_.empty() ? 0 : 1);
 }
 
 void TetSim::release_host() {
@@ -190,6 +201,7 @@ void TetSim::release_host() {
 }
 
 TetSim::~TetSim() {
+  group_.reset();
   if (pinned_) cudaFreeHost(pinned_);
   for (void* p : allocs_) cudaFree(p);
   if (ev0_) cudaEventDestroy(ev0_);
@@ -1080,6 +1092,11 @@ void TetSim::launch_steps(int n, cudaEvent_t* ev) {
 }
 
 uint64_t TetSim::step(uint64_t n) {
+  if (group_) {
+    const uint64_t k = group_->step(n);
+    step_ = group_->step_index(0);
+    return k;
+  }
   if (step_ + n > nsteps_) n = nsteps_ - step_;
   if (n == 0) { last_ms_ = 0; return 0; }
   CU(cudaEventRecord(ev0_, stream_));
@@ -1094,6 +1111,11 @@ uint64_t TetSim::step(uint64_t n) {
 }
 
 uint64_t TetSim::phase_times(uint64_t n, double* ms5) {
+  if (group_) {
+    const uint64_t k = group_->phase_times(n, ms5);
+    step_ = group_->step_index(0);
+    return k;
+  }
   if (step_ + n > nsteps_) n = nsteps_ - step_;
   for (int q = 0; q < 5; q++) ms5[q] = 0;
   cudaEvent_t ev[6];
@@ -1113,6 +1135,11 @@ uint64_t TetSim::phase_times(uint64_t n, double* ms5) {
 }
 
 uint64_t TetSim::step_io(const double* carrier_in, double* probe_out) {
+  if (group_) {
+    const uint64_t k = group_->step_io(carrier_in, probe_out);
+    step_ = group_->step_index(0);
+    return k;
+  }
   if (step_ >= nsteps_) return 0;
   const size_t nsrc = src_labels_.size(), np = probe_tet_.size();
   if (!pinned_) CU(cudaHostAlloc((void**)&pinned_, (nsrc + 6 * np + 1) * sizeof(double), cudaHostAllocDefault));
@@ -1134,6 +1161,7 @@ uint64_t TetSim::step_io(const double* carrier_in, double* probe_out) {
 }
 
 size_t TetSim::n_samples() const {
+  if (group_) return group_->n_samples(0);
   size_t c = 0;
   const uint64_t upto = method_ == 1 ? step_ + 1 : step_;
   for (uint64_t i = 0; i < upto && i < slot_of_step_.size(); i++)
@@ -1142,6 +1170,7 @@ size_t TetSim::n_samples() const {
 }
 
 void TetSim::get_probes(double* times, double* values, size_t cap) const {
+  if (group_) return group_->get_probes(0, times, values, cap);
   size_t ns = n_samples();
   if (ns > cap) ns = cap;
   const size_t np = probe_tet_.size();
@@ -1168,6 +1197,7 @@ static void fetch(const void* d, size_t n, bool f32, double* out) {
 }
 
 void TetSim::get_state(double* U, double* B, double* F) {
+  if (group_) return group_->get_state(0, U, B, F);
   const bool f32 = opt_.precision == 1;
   CU(cudaStreamSynchronize(stream_));
   fetch(dp_.U, edges_.size(), f32, U);
@@ -1176,6 +1206,7 @@ void TetSim::get_state(double* U, double* B, double* F) {
 }
 
 void TetSim::set_state(const double* U, const double* F) {
+  if (group_) return group_->set_state(0, U, F);
   const bool f32 = opt_.precision == 1;
   auto put = [&](void* dst, const double* src, size_t n) {
     if (!src) return;
@@ -1190,12 +1221,14 @@ void TetSim::set_state(const double* U, const double* F) {
 }
 
 void TetSim::get_flux(double* flux, size_t cap, size_t* n) const {
+  if (group_) return group_->get_flux(0, flux, cap, n);
   size_t m = step_ < cap ? step_ : cap;
   if (flux && m) CU(cudaMemcpy(flux, dp_.flux, m * 8, cudaMemcpyDeviceToHost));
   if (n) *n = step_;
 }
 
 size_t TetSim::solver_stats(int32_t* iters, double* resid, size_t cap) const {
+  if (group_) return group_->solver_stats(0, iters, resid, cap);
   if (method_ != 2) return 0;
   size_t m = step_ < cap ? step_ : cap;
   if (iters && m) CU(cudaMemcpy(iters, dp_.cg_iters, m * 4, cudaMemcpyDeviceToHost));

@@ -6,6 +6,7 @@
 
 #include <array>
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -14,6 +15,8 @@
 #include "tet_kernels.cuh"
 
 namespace tf {
+
+class TetGroup;
 
 // CSR on the host (int32 columns, double values), duplicates summed in
 // insertion order.
@@ -48,8 +51,8 @@ class TetSim : public Sim {
   double dt_estimate() const override { return dt_est_; }
   bool possibly_unstable() const override { return unstable_; }
   int precision() const override { return opt_.precision; }
-  uint64_t device_bytes() const override { return dev_bytes_; }
-  double last_step_ms() const override { return last_ms_; }
+  uint64_t device_bytes() const override;
+  double last_step_ms() const override;
   const Output& output() const override { return out_; }
   const Simulation& simulation() const override { return sim_; }
   size_t n_samples() const override;
@@ -62,10 +65,7 @@ class TetSim : public Sim {
   double energy() override;
   uint64_t phase_times(uint64_t n, double* ms5) override;
   uint64_t step_io(const double* carrier_in, double* probe_out) override;
-  int kernels_per_step() const override {
-    const int np = probe_tet_.empty() ? 0 : 1;
-    return method_ == 1 ? 6 + np + (src_edge_.empty() ? 0 : 1) : 9 + np;
-  }
+  int kernels_per_step() const override;
   size_t n_sources() const override { return src_labels_.size(); }
   size_t solver_stats(int32_t* iters, double* resid, size_t cap) const override;
   uint64_t n_free() const override { return free_edges_.size(); }
@@ -150,6 +150,8 @@ class TetSim : public Sim {
   DevPtrs dp_{};
   int cg_blocks_ = 0;
   double* pinned_ = nullptr;
+  // gfdtd runs on the group engine (a group of one simulation)
+  std::unique_ptr<TetGroup> group_;
 };
 
 }  // namespace tf

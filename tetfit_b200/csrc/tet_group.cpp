@@ -127,6 +127,7 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
     m.roff = roff;
     dofs_ += (uint64_t)(NE + NF);
     nnz_a_real_ += t.A_.val.size();
+    m.nnz_a = t.A_.val.size();
     // Free rows grouped by stencil: rows whose column offsets (col - row) are
     // the same form a class, classes in order of first appearance, rows of a
     // class in their own order.  On meshes with repeated local structure the
@@ -301,6 +302,7 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
   d.dir_edge = (const int32_t*)upload(dir_edge);
   d.x = zeros(d.nrow);
   d.r = zeros(d.nrow);
+  d.z = zeros(d.nrow);
   d.p0 = zeros(d.nrow);
   d.p1 = zeros(d.nrow);
   d.q = zeros(d.nrow);

@@ -38,6 +38,7 @@ class TetGroup {
   double last_step_ms() const { return last_ms_; }
   uint64_t step_index(int s) const { return meta_[s].step; }
   uint64_t n_steps(int s) const { return meta_[s].nsteps; }
+  uint64_t nnz_A(int s) const { return meta_[s].nnz_a; }
   void get_state(int s, double* U, double* B, double* F);
   void set_state(int s, const double* U, const double* F);
   size_t n_samples(int s) const;
@@ -56,7 +57,7 @@ class TetGroup {
 
  private:
   struct Meta {
-    uint64_t nE = 0, nF = 0, nsteps = 0, step = 0, np = 0, nsrc = 0;
+    uint64_t nE = 0, nF = 0, nsteps = 0, step = 0, np = 0, nsrc = 0, nnz_a = 0;
     int64_t eoff = 0, foff = 0, roff = 0, stat_off = 0, samp_off = 0, car_off = 0;
     int nslots = 0;
     std::vector<int> slot_of_step;

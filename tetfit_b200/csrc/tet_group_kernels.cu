@@ -18,10 +18,11 @@
 // rz / p_j.q, x += alpha_j p_j, r -= alpha_j q, z = pre r, beta = rz'/rz,
 // p_{j+1} = z + beta p_j.  Here p alternates between two buffers, and the x
 // update of iteration j is applied while p_{j+1} is formed (p_j is read there
-// anyway), with one final update after the loop.  In the fused variant the
-// SpMV forms p_{j+1} at every gathered column from (pre, r, p_j) with the same
-// explicitly rounded operations the row's owner uses, so p_{j+1} needs no
-// barrier before the SpMV: two grid barriers per iteration instead of three.
+// anyway), with one final update after the loop.  The residual phase stores
+// z = pre r.  In the fused variant the SpMV forms p_{j+1} at every gathered
+// column from (z, p_j) with the same explicitly rounded operation the row's
+// owner uses, so p_{j+1} needs no barrier before the SpMV: two grid barriers
+// per iteration instead of three.
 // Both variants give bitwise identical iterates.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
@@ -240,10 +241,10 @@ struct SimCg {
   int it, active;
 };
 
-// p_{j+1} at one row, rounded the same way wherever it is formed
+// p_{j+1} at one row from z = pre r (stored by the residual phase), rounded
+// the same way wherever it is formed
 template <typename T>
-__device__ __forceinline__ T p_next(T pre, T r, T pold, T beta, bool first) {
-  const T z = mulT(pre, r);
+__device__ __forceinline__ T p_next(T z, T pold, T beta, bool first) {
   return first ? z : fmaT(beta, pold, z);
 }
 
@@ -260,6 +261,7 @@ __global__ void __launch_bounds__(kCgThreads, 2) grp_cg(GroupDev d) {
   T* q = (T*)d.q;
   const T* b = (const T*)d.rhs;
   const T* pre = (const T*)d.pre;
+  T* z = (T*)d.z;
   auto pbuf = [&](int k) { return (k & 1) ? (T*)d.p1 : (T*)d.p0; };
 
   auto flush = [&](int g, double a0, double a1, double a2) {
@@ -309,9 +311,11 @@ __global__ void __launch_bounds__(kCgThreads, 2) grp_cg(GroupDev d) {
         const int64_t i = sl * 32 + lane;
         const T ri = b[i] - sell_dot<T>(d.A, i, [&](int32_t c) { return x[c]; });
         r[i] = ri;
+        const T zi = mulT(pre[i], ri);
+        z[i] = zi;
         const double rd = (double)ri;
         a0 += rd * rd;
-        a1 += rd * (double)(pre[i] * ri);
+        a1 += rd * (double)zi;
         a2 += (double)b[i] * (double)b[i];
       }
     flush(g, a0, a1, a2);
@@ -349,12 +353,12 @@ __global__ void __launch_bounds__(kCgThreads, 2) grp_cg(GroupDev d) {
         for (int64_t sl = d.seg_s0[g] + warp; sl < d.seg_s1[g]; sl += kCgWarps) {
           const int64_t i = sl * 32 + lane;
           const T po = first ? (T)0 : pold[i];
-          const T pi = p_next<T>(pre[i], r[i], po, beta, first);
+          const T pi = p_next<T>(z[i], po, beta, first);
           if (!first) x[i] = fmaT(alpha, po, x[i]);
           pn[i] = pi;
           if (kFused) {
             const T qi = sell_dot<T>(d.A, i, [&](int32_t cc) {
-              return p_next<T>(__ldg(pre + cc), r[cc], first ? (T)0 : pold[cc], beta, first);
+              return p_next<T>(z[cc], first ? (T)0 : pold[cc], beta, first);
             });
             q[i] = qi;
             a0 += (double)pi * (double)qi;
@@ -397,9 +401,11 @@ __global__ void __launch_bounds__(kCgThreads, 2) grp_cg(GroupDev d) {
           const int64_t i = sl * 32 + lane;
           const T ri = r[i] - alpha * q[i];
           r[i] = ri;
+          const T zi = mulT(pre[i], ri);
+          z[i] = zi;
           const double rd = (double)ri;
           a0 += rd * rd;
-          a1 += rd * (double)(pre[i] * ri);
+          a1 += rd * (double)zi;
         }
       }
       flush(g, a0, a1, 0.0);

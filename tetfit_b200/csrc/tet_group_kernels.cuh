@@ -61,7 +61,7 @@ struct GroupDev {
   const int32_t* free_edge = nullptr;
   const int32_t* dir_edge = nullptr;
   // CG
-  void *x = nullptr, *r = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr, *rhs = nullptr;
+  void *x = nullptr, *r = nullptr, *z = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr, *rhs = nullptr;
   void *xh1 = nullptr, *xh2 = nullptr, *xh3 = nullptr;
   const int* blk_seg = nullptr;  // [G + 1]
   const int* seg_sim = nullptr;
