@@ -57,7 +57,9 @@ typedef struct tf_opts {
   int32_t batch_mode;   /* tf_batch_open: 0 all members advance together in one
                            group, 1 each member alone (one after another)       */
   int32_t host_threads; /* tf_batch_open: host threads building members, 0 all  */
-  int32_t reserved[5];
+  int32_t learn_steps;  /* warm_start 3: steps whose solutions train the network
+                           (0: 500); the extrapolation is used meanwhile         */
+  int32_t reserved[4];
 } tf_opts;
 
 typedef struct tf_info {
@@ -117,6 +119,12 @@ TF_API int tf_run(tf_ctx* ctx, uint32_t sim_label, const tf_opts* opts);
 /* gfdtd: CG iterations and final relative residual of every step taken so far
  * (the reference's "mean solver iterations", Discretization.hpp:2286-2302). */
 TF_API int tf_solver_stats(tf_ctx* ctx, int32_t* iters, double* resid, size_t cap, size_t* n);
+/* warm_start 3: per step taken, 1 when the CG kept the network's guess and 0
+ * when the polynomial extrapolation had the smaller initial residual (or the
+ * network was still training). */
+TF_API int tf_guess_stats(tf_ctx* ctx, int8_t* kept, size_t cap, size_t* n);
+/* warm_start 3: training loss of every Adam step so far. */
+TF_API int tf_training_loss(tf_ctx* ctx, float* loss, size_t cap, size_t* n);
 /* Standalone Jacobi-PCG solve of a symmetric positive definite CSR system held
  * in device memory, with the persistent kernel of the gfdtd path
  * (ConjugateGradientSolver.hpp:52-129: Jacobi preconditioner 1/diag, stop on
@@ -186,10 +194,33 @@ TF_API int tf_batch_get_state(tf_batch* b, uint32_t member, double* U, size_t nU
 TF_API int tf_batch_get_flux(tf_batch* b, uint32_t member, double* flux, size_t cap, size_t* n);
 TF_API int tf_batch_solver_stats(tf_batch* b, uint32_t member, int32_t* iters, double* resid, size_t cap,
                                  size_t* n);
+TF_API int tf_batch_guess_stats(tf_batch* b, uint32_t member, int8_t* kept, size_t cap, size_t* n);
+/* Training loss of the network that member's group learns (one network per group). */
+TF_API int tf_batch_training_loss(tf_batch* b, uint32_t member, float* loss, size_t cap, size_t* n);
+/* Current parameters of that network (tf_mlp_param_count() floats). */
+TF_API int tf_batch_mlp_params(tf_batch* b, uint32_t member, float* params);
 /* Device time of the last tf_batch_step (summed over members in batch_mode 1). */
 TF_API int tf_batch_last_step_ms(tf_batch* b, double* ms);
 TF_API const char* tf_batch_last_error(tf_batch* b);
 TF_API void tf_batch_close(tf_batch* b);
+/* ---- Learned CG warm start network ------------------------------------------
+ * The per-edge network of warm_start 3 (no counterpart in the reference, whose
+ * CG starts from the previous solution, Discretization.hpp:1536): 6 inputs ->
+ * 64 -> 64 -> 1 with SiLU, BF16 weights and activations on the tensor cores,
+ * FP32 accumulation and FP32 master parameters.  The parameter vector holds
+ * tf_mlp_param_count() floats: W1[64][16] (inputs 6..15 zero), b1[64],
+ * W2[64][64], b2[64], W3[64], b3, W[n][k] the weight from input k to output n.
+ * These calls run the group engine's own kernels on host buffers (current
+ * device); errors through tf_last_error(NULL). */
+TF_API int tf_mlp_param_count(void);
+/* He-uniform initial parameters (output layer scaled by 0.1) from a seed. */
+TF_API int tf_mlp_init(uint64_t seed, float* params);
+/* outputs[n] of inputs[n][6]. */
+TF_API int tf_mlp_forward(const float* params, int64_t n, const float* inputs, float* outputs);
+/* Gradient of sum_i w_i (y_i - t_i)^2 / n with respect to the parameters
+ * (weights NULL: all 1), and that loss; n <= 2^24. */
+TF_API int tf_mlp_gradient(const float* params, int64_t n, const float* inputs, const float* targets,
+                           const float* weights, float* grad, float* loss);
 /* Device time of the last tf_step call, from CUDA events on the context stream. */
 TF_API int tf_last_step_ms(tf_ctx* ctx, double* ms);
 /* Message of the last failure on ctx; with ctx == NULL, of the last

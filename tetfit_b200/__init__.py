@@ -34,7 +34,8 @@ class Opts(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("device", ctypes.c_int32), ("write_files", ctypes.c_int32),
                 ("verbose", ctypes.c_int32), ("graph_steps", ctypes.c_int32), ("mass_model", ctypes.c_int32),
                 ("warm_start", ctypes.c_int32), ("cg_criterion", ctypes.c_int32), ("cg_maxiter", ctypes.c_int32),
-                ("batch_mode", ctypes.c_int32), ("host_threads", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
+                ("batch_mode", ctypes.c_int32), ("host_threads", ctypes.c_int32), ("learn_steps", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 4)]
 
 
 class Info(ctypes.Structure):
@@ -82,6 +83,12 @@ _SIGS = {
     "tf_phase_times": (ctypes.c_int, [_P, ctypes.c_uint64, _P, ctypes.POINTER(ctypes.c_uint64)]),
     "tf_run": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(Opts)]),
     "tf_solver_stats": (ctypes.c_int, [_P, _P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "tf_guess_stats": (ctypes.c_int, [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "tf_training_loss": (ctypes.c_int, [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "tf_batch_guess_stats": (ctypes.c_int, [_P, ctypes.c_uint32, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "tf_batch_training_loss": (ctypes.c_int, [_P, ctypes.c_uint32, _P, ctypes.c_size_t,
+                                              ctypes.POINTER(ctypes.c_size_t)]),
+    "tf_batch_mlp_params": (ctypes.c_int, [_P, ctypes.c_uint32, _P]),
     "tf_pcg_solve": (ctypes.c_int, [ctypes.POINTER(PcgArgs), ctypes.POINTER(ctypes.c_int32),
                                     ctypes.POINTER(ctypes.c_double)]),
     "tf_pcg_solve_noalloc": (ctypes.c_int, [ctypes.POINTER(PcgArgs), ctypes.POINTER(ctypes.c_int32),
@@ -103,6 +110,10 @@ _SIGS = {
     "tf_batch_last_step_ms": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double)]),
     "tf_batch_last_error": (ctypes.c_char_p, [_P]),
     "tf_batch_close": (None, [_P]),
+    "tf_mlp_param_count": (ctypes.c_int, []),
+    "tf_mlp_init": (ctypes.c_int, [ctypes.c_uint64, _P]),
+    "tf_mlp_forward": (ctypes.c_int, [_P, ctypes.c_int64, _P, _P]),
+    "tf_mlp_gradient": (ctypes.c_int, [_P, ctypes.c_int64, _P, _P, _P, _P, _P]),
     "tf_last_step_ms": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double)]),
     "tf_last_error": (ctypes.c_char_p, [_P]),
     "tf_close": (None, [_P]),
@@ -139,6 +150,38 @@ def pcg_solve(row_ptr, col, val, b, x, tol=1e-8, maxiter=0, criterion=0, device=
     rs = ctypes.c_double()
     rc = lib().tf_pcg_solve(ctypes.byref(a), ctypes.byref(it), ctypes.byref(rs))
     return rc, it.value, rs.value
+
+
+def mlp_init(seed: int = 1) -> np.ndarray:
+    """Initial parameters of the warm-start network (tf_mlp_init)."""
+    p = np.zeros(lib().tf_mlp_param_count(), dtype=np.float32)
+    lib().tf_mlp_init(seed, _ptr(p))
+    return p
+
+
+def mlp_forward(params, inputs) -> np.ndarray:
+    """Network outputs [n] for inputs [n, 6] (tf_mlp_forward, tensor-core kernel)."""
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    inputs = np.ascontiguousarray(inputs, dtype=np.float32)
+    out = np.zeros(len(inputs), dtype=np.float32)
+    rc = lib().tf_mlp_forward(_ptr(params), len(inputs), _ptr(inputs), _ptr(out))
+    if rc != TF_OK:
+        raise TetfitError(rc, last_thread_error())
+    return out
+
+
+def mlp_gradient(params, inputs, targets, weights=None):
+    """(gradient[n_params], loss) of sum w (y - t)^2 / n (tf_mlp_gradient)."""
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    inputs = np.ascontiguousarray(inputs, dtype=np.float32)
+    targets = np.ascontiguousarray(targets, dtype=np.float32)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float32)
+    g = np.zeros_like(params)
+    loss = np.zeros(1, dtype=np.float32)
+    rc = lib().tf_mlp_gradient(_ptr(params), len(inputs), _ptr(inputs), _ptr(targets), _ptr(w), _ptr(g), _ptr(loss))
+    if rc != TF_OK:
+        raise TetfitError(rc, last_thread_error())
+    return g, float(loss[0])
 
 
 def last_thread_error() -> str:
@@ -185,7 +228,8 @@ class Discretization:
 
     @staticmethod
     def _opts(precision="fp64", device=0, write_files=False, verbose=False, graph_steps=0, mass="reference",
-              warm_start="previous", cg_criterion="reference", cg_maxiter=0, batch_mode=0, host_threads=0) -> Opts:
+              warm_start="previous", cg_criterion="reference", cg_maxiter=0, batch_mode=0, host_threads=0,
+              learn_steps=0) -> Opts:
         o = Opts()
         lib().tf_default_opts(ctypes.byref(o))
         o.precision = {"fp64": FP64, "fp32": FP32}[precision] if isinstance(precision, str) else int(precision)
@@ -196,6 +240,7 @@ class Discretization:
         o.cg_maxiter = cg_maxiter
         o.batch_mode = {"group": 0, "serial": 1}[batch_mode] if isinstance(batch_mode, str) else int(batch_mode)
         o.host_threads = host_threads
+        o.learn_steps = learn_steps
         return o
 
     def prepare(self, label: int, **opts) -> dict:
@@ -245,6 +290,21 @@ class Discretization:
         ms = ctypes.c_double()
         self._check(lib().tf_last_step_ms(self._h, ctypes.byref(ms)))
         return ms.value
+
+    def guess_stats(self):
+        """warm_start "learned": per step 1 when the network's guess was kept."""
+        n = ctypes.c_size_t()
+        self._check(lib().tf_guess_stats(self._h, None, 0, ctypes.byref(n)))
+        k = np.zeros(n.value, dtype=np.int8)
+        self._check(lib().tf_guess_stats(self._h, _ptr(k), n.value, ctypes.byref(n)))
+        return k
+
+    def training_loss(self):
+        n = ctypes.c_size_t()
+        self._check(lib().tf_training_loss(self._h, None, 0, ctypes.byref(n)))
+        v = np.zeros(n.value, dtype=np.float32)
+        self._check(lib().tf_training_loss(self._h, _ptr(v), n.value, ctypes.byref(n)))
+        return v
 
     def probes(self):
         """(times[n], values[n, n_probes, 6]) with columns Ex Ey Ez Hx Hy Hz."""
@@ -388,6 +448,25 @@ class Batch:
         f = np.zeros(n.value)
         self._check(lib().tf_batch_get_flux(self._h, m, _ptr(f), n.value, ctypes.byref(n)))
         return f
+
+    def guess_stats(self, m: int):
+        n = ctypes.c_size_t()
+        self._check(lib().tf_batch_guess_stats(self._h, m, None, 0, ctypes.byref(n)))
+        k = np.zeros(n.value, dtype=np.int8)
+        self._check(lib().tf_batch_guess_stats(self._h, m, _ptr(k), n.value, ctypes.byref(n)))
+        return k
+
+    def training_loss(self, m: int = 0):
+        n = ctypes.c_size_t()
+        self._check(lib().tf_batch_training_loss(self._h, m, None, 0, ctypes.byref(n)))
+        v = np.zeros(n.value, dtype=np.float32)
+        self._check(lib().tf_batch_training_loss(self._h, m, _ptr(v), n.value, ctypes.byref(n)))
+        return v
+
+    def mlp_params(self, m: int = 0):
+        p = np.zeros(lib().tf_mlp_param_count(), dtype=np.float32)
+        self._check(lib().tf_batch_mlp_params(self._h, m, _ptr(p)))
+        return p
 
     def solver_stats(self, m: int):
         n = ctypes.c_size_t()

@@ -166,6 +166,7 @@ int tf_prepare(tf_ctx* c, uint32_t label, const tf_opts* opts) {
     ro.warm_start = c->opts.warm_start;
     ro.cg_criterion = c->opts.cg_criterion;
     if (c->opts.cg_maxiter > 0) ro.cg_maxiter = c->opts.cg_maxiter;
+    if (c->opts.learn_steps > 0) ro.learn_steps = c->opts.learn_steps;
     if (meth == "fdtd") {
       c->fit.reset(new tf::FitSim(c->sc, label, ro));
     } else if (meth == "dga" || meth == "gfdtd") {
@@ -308,6 +309,26 @@ int tf_solver_stats(tf_ctx* c, int32_t* iters, double* resid, size_t cap, size_t
   if (!c->fit) return fail(c, TF_E_STATE, "no simulation prepared");
   return guarded(c, [&]() -> int {
     size_t k = c->fit->solver_stats(iters, resid, cap);
+    if (n) *n = k;
+    return TF_OK;
+  });
+}
+
+int tf_guess_stats(tf_ctx* c, int8_t* kept, size_t cap, size_t* n) {
+  if (!c) return TF_E_ARG;
+  if (!c->fit) return fail(c, TF_E_STATE, "tf_guess_stats before tf_prepare");
+  return guarded(c, [&]() -> int {
+    const size_t k = c->fit->guess_stats(kept, cap);
+    if (n) *n = k;
+    return TF_OK;
+  });
+}
+
+int tf_training_loss(tf_ctx* c, float* loss, size_t cap, size_t* n) {
+  if (!c) return TF_E_ARG;
+  if (!c->fit) return fail(c, TF_E_STATE, "tf_training_loss before tf_prepare");
+  return guarded(c, [&]() -> int {
+    const size_t k = c->fit->training_loss(loss, cap);
     if (n) *n = k;
     return TF_OK;
   });

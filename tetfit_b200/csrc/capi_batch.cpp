@@ -78,6 +78,7 @@ int tf_batch_open(const char* const* scripts, const uint32_t* labels, uint32_t n
     ro.warm_start = o.warm_start;
     ro.cg_criterion = o.cg_criterion;
     if (o.cg_maxiter > 0) ro.cg_maxiter = o.cg_maxiter;
+    if (o.learn_steps > 0) ro.learn_steps = o.learn_steps;
     ro.estimate_pinned = false;
     b->mode = o.batch_mode;
     if (b->mode != 0 && b->mode != 1) return bfail(b, TF_E_ARG, "batch_mode must be 0 or 1");
@@ -249,6 +250,35 @@ int tf_batch_solver_stats(tf_batch* b, uint32_t m, int32_t* iters, double* resid
     const auto [g, k] = b->where[m];
     const size_t s = b->groups[g]->solver_stats(k, iters, resid, cap);
     if (n) *n = s;
+    return TF_OK;
+  });
+}
+
+int tf_batch_guess_stats(tf_batch* b, uint32_t m, int8_t* kept, size_t cap, size_t* n) {
+  if (int rc = member_ok(b, m)) return rc;
+  return bguarded(b, [&]() -> int {
+    const auto [g, k] = b->where[m];
+    const size_t s = b->groups[g]->guess_stats(k, kept, cap);
+    if (n) *n = s;
+    return TF_OK;
+  });
+}
+
+int tf_batch_training_loss(tf_batch* b, uint32_t m, float* loss, size_t cap, size_t* n) {
+  if (int rc = member_ok(b, m)) return rc;
+  return bguarded(b, [&]() -> int {
+    const size_t s = b->groups[b->where[m].first]->training_loss(loss, cap);
+    if (n) *n = s;
+    return TF_OK;
+  });
+}
+
+int tf_batch_mlp_params(tf_batch* b, uint32_t m, float* params) {
+  if (int rc = member_ok(b, m)) return rc;
+  if (!params) return bfail(b, TF_E_ARG, "params is NULL");
+  return bguarded(b, [&]() -> int {
+    if (!b->groups[b->where[m].first]->mlp_params(params))
+      return bfail(b, TF_E_STATE, "the batch was not opened with the learned warm start (warm_start 3)");
     return TF_OK;
   });
 }

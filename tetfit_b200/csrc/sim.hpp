@@ -20,6 +20,11 @@ struct RunOptions {
   // run the stability estimate even when the script pins the step (batches
   // turn it off: with a pinned step it only sets the possibly-unstable flag)
   bool estimate_pinned = true;
+  // learned warm start (warm_start 3)
+  int learn_steps = 500;      // steps whose solutions train the network
+  int learn_samples = 32768;  // sampled rows per training step
+  int learn_inner = 2;        // Adam steps per training step
+  float learn_rate = 1e-3f;
 };
 
 class Sim {
@@ -62,6 +67,16 @@ class Sim {
   // iterative solver statistics (gfdtd): iterations and final residual per step
   virtual size_t solver_stats(int32_t* iters, double* resid, size_t cap) const {
     (void)iters; (void)resid; (void)cap;
+    return 0;
+  }
+  // learned warm start: per step 1 when the network's guess was kept
+  virtual size_t guess_stats(int8_t* kept, size_t cap) const {
+    (void)kept; (void)cap;
+    return 0;
+  }
+  // learned warm start: training loss of every Adam step so far
+  virtual size_t training_loss(float* loss, size_t cap) const {
+    (void)loss; (void)cap;
     return 0;
   }
 };

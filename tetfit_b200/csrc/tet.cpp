@@ -1236,6 +1236,14 @@ size_t TetSim::solver_stats(int32_t* iters, double* resid, size_t cap) const {
   return step_;
 }
 
+size_t TetSim::guess_stats(int8_t* kept, size_t cap) const {
+  return group_ ? group_->guess_stats(0, kept, cap) : 0;
+}
+
+size_t TetSim::training_loss(float* loss, size_t cap) const {
+  return group_ ? group_->training_loss(loss, cap) : 0;
+}
+
 double TetSim::energy() {
   // 0.5 U.E U + 0.5 B.N B on the host in FP64 (gfdtd mass; dga returns the
   // magnetic part plus 0.5 U.(Einv^-1 restricted) is not formed: magnetic only)

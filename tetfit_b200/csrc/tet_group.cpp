@@ -307,10 +307,48 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
   d.p1 = zeros(d.nrow);
   d.q = zeros(d.nrow);
   d.rhs = zeros(d.nrow);
-  if (opt_.warm_start == 2) {
+  if (opt_.warm_start == 2 || opt_.warm_start == 3) {
     d.xh1 = zeros(d.nrow);
     d.xh2 = zeros(d.nrow);
     d.xh3 = zeros(d.nrow);
+  }
+  if (opt_.warm_start == 3) {
+    d.xe = zeros(d.nrow);
+    d.r_alt = zeros(d.nrow);
+    d.z_alt = zeros(d.nrow);
+    d.kept = (int8_t*)dalloc((size_t)stat);
+    CU(cudaMemset(d.kept, 0, (size_t)stat));
+    // sampled rows: every samp_stride-th free row, the first one rotating
+    // through the stride from step to step
+    samp_stride_ = std::max<int64_t>(1, d.nrow / std::max(1, opt_.learn_samples));
+    samp_n_ = (d.nrow + samp_stride_ - 1) / samp_stride_;
+    auto fz = [&](int64_t n) {
+      float* p = (float*)dalloc(sizeof(float) * (size_t)std::max<int64_t>(n, 1));
+      CU(cudaMemset(p, 0, sizeof(float) * (size_t)std::max<int64_t>(n, 1)));
+      return p;
+    };
+    d.samp_in = fz(6 * samp_n_);
+    d.samp_e = fz(samp_n_);
+    d.samp_s = fz(samp_n_);
+    d.samp_t = fz(samp_n_);
+    d.samp_w = fz(samp_n_);
+    d.samp_row = (int32_t*)dalloc(sizeof(int32_t) * (size_t)samp_n_);
+    CU(cudaMemset(d.samp_row, 0xff, sizeof(int32_t) * (size_t)samp_n_));
+    mlp_.max_blocks = (int)((samp_n_ + mlp_train_rows_per_block() - 1) / mlp_train_rows_per_block());
+    std::vector<float> p0(kNParam);
+    mlp_init_params(p0.data(), 0x5EEDF00Dull);
+    mlp_.params = (float*)upload(p0);
+    mlp_.adam_m = fz(kNParam);
+    mlp_.adam_v = fz(kNParam);
+    mlp_.image = (unsigned char*)dalloc(kImgBytes);
+    mlp_.grad_part = fz((int64_t)mlp_.max_blocks * kNParam);
+    mlp_.loss_part = fz(mlp_.max_blocks);
+    mlp_.grad = fz(kNParam);
+    mlp_.loss = fz(1);
+    CU(mlp_launch_pack(mlp_.params, mlp_.image, stream_));
+    d.mlp_img = mlp_.image;
+    loss_cap_ = (int64_t)std::max(1, opt_.learn_steps) * std::max(1, opt_.learn_inner);
+    loss_hist_ = fz(loss_cap_);
   }
   d.cg_maxiter = opt_.cg_maxiter > 0 ? opt_.cg_maxiter : 100;
   d.cg_criterion = opt_.cg_criterion;
@@ -413,15 +451,36 @@ void TetGroup::partition() {
   d.seg_s0 = (const int64_t*)upload(seg_s0);
   d.seg_s1 = (const int64_t*)upload(seg_s1);
   d.sim_seg = (const int*)upload(sim_seg);
-  d.part = (double*)dalloc(sizeof(double) * 3 * std::max<size_t>(seg_sim.size(), 1));
+  d.part = (double*)dalloc(sizeof(double) * kCgPart * std::max<size_t>(seg_sim.size(), 1));
 }
 
 void TetGroup::launch(int n, cudaEvent_t* ev) {
+  const bool f32 = opt_.precision == 1;
   for (int k = 0; k < n; k++) {
-    cudaError_t e = opt_.precision == 1
-                        ? group_launch_step<float>(dev_, cg_blocks_, cg_variant_, cg_smem_, stream_, ev)
+    const bool learned = opt_.warm_start == 3;
+    const bool training = learned && launched_ < opt_.learn_steps;
+    if (learned) {
+      dev_.mlp_on = training ? 0 : 1;
+      dev_.dual = training ? 0 : 1;
+      dev_.nsamp = training ? samp_n_ : 0;
+      dev_.samp_stride = samp_stride_;
+      dev_.samp_first = launched_ % samp_stride_;
+    }
+    cudaError_t e = f32 ? group_launch_step<float>(dev_, cg_blocks_, cg_variant_, cg_smem_, stream_, ev)
                         : group_launch_step<double>(dev_, cg_blocks_, cg_variant_, cg_smem_, stream_, ev);
     CU(e);
+    if (training) {
+      // the step's solutions are the training targets of its sampled rows
+      CU(f32 ? group_launch_targets<float>(dev_, stream_) : group_launch_targets<double>(dev_, stream_));
+      for (int q = 0; q < std::max(1, opt_.learn_inner); q++) {
+        CU(mlp_launch_train(mlp_, dev_.samp_in, dev_.samp_t, dev_.samp_w, (int)samp_n_, ++adam_step_,
+                            opt_.learn_rate, stream_));
+        if (adam_step_ - 1 < loss_cap_)
+          CU(cudaMemcpyAsync(loss_hist_ + adam_step_ - 1, mlp_.loss, sizeof(float), cudaMemcpyDeviceToDevice,
+                             stream_));
+      }
+    }
+    launched_++;
   }
 }
 
@@ -585,6 +644,28 @@ size_t TetGroup::solver_stats(int s, int32_t* iters, double* resid, size_t cap) 
   if (iters && n) CU(cudaMemcpy(iters, dev_.cg_iters + m.stat_off, n * 4, cudaMemcpyDeviceToHost));
   if (resid && n) CU(cudaMemcpy(resid, dev_.cg_resid + m.stat_off, n * 8, cudaMemcpyDeviceToHost));
   return m.step;
+}
+
+size_t TetGroup::guess_stats(int s, int8_t* kept, size_t cap) const {
+  const Meta& m = meta_[s];
+  if (!dev_.kept) return 0;
+  const size_t n = std::min<size_t>(m.step, cap);
+  if (kept && n) CU(cudaMemcpy(kept, dev_.kept + m.stat_off, n, cudaMemcpyDeviceToHost));
+  return m.step;
+}
+
+size_t TetGroup::training_loss(float* loss, size_t cap) const {
+  if (!loss_hist_) return 0;
+  const size_t have = (size_t)std::min<int64_t>(adam_step_, loss_cap_);
+  const size_t n = std::min(have, cap);
+  if (loss && n) CU(cudaMemcpy(loss, loss_hist_, n * sizeof(float), cudaMemcpyDeviceToHost));
+  return have;
+}
+
+bool TetGroup::mlp_params(float* out) const {
+  if (!mlp_.params) return false;
+  if (out) CU(cudaMemcpy(out, mlp_.params, sizeof(float) * kNParam, cudaMemcpyDeviceToHost));
+  return true;
 }
 
 void TetGroup::get_flux(int s, double* flux, size_t cap, size_t* n) const {

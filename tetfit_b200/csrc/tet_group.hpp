@@ -9,6 +9,7 @@
 
 #include "sim.hpp"
 #include "tet.hpp"
+#include "mlp.hpp"
 #include "tet_group_kernels.cuh"
 
 namespace tf {
@@ -44,6 +45,10 @@ class TetGroup {
   size_t n_samples(int s) const;
   void get_probes(int s, double* times, double* values, size_t cap) const;
   size_t solver_stats(int s, int32_t* iters, double* resid, size_t cap) const;
+  size_t guess_stats(int s, int8_t* kept, size_t cap) const;
+  size_t training_loss(float* loss, size_t cap) const;
+  // current network parameters (kNParam floats); false without warm_start 3
+  bool mlp_params(float* out) const;
   void get_flux(int s, double* flux, size_t cap, size_t* n) const;
   uint64_t device_bytes() const { return dev_bytes_; }
   int kernels_per_step() const { return 7 + (dev_.np ? 1 : 0); }
@@ -86,7 +91,14 @@ class TetGroup {
   double last_ms_ = 0;
   double* pinned_ = nullptr;
   size_t pinned_len_ = 0, io_src_ = 0, io_probe_ = 0;
-  std::vector<double> carrier_host_;  // per-simulation carrier tables (for step_io overrides)
+  std::vector<double> carrier_host_;
+  // learned warm start
+  MlpTrain mlp_{};
+  int64_t launched_ = 0;     // steps launched so far (group clock of the training schedule)
+  int adam_step_ = 0;
+  int64_t samp_n_ = 0, samp_stride_ = 1;
+  float* loss_hist_ = nullptr;
+  int64_t loss_cap_ = 0;  // per-simulation carrier tables (for step_io overrides)
 };
 
 }  // namespace tf

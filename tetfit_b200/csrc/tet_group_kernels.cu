@@ -27,6 +27,7 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include "mlp.cuh"
 #include "tet_group_kernels.cuh"
 
 namespace cg = cooperative_groups;
@@ -236,10 +237,140 @@ __global__ void __launch_bounds__(kGB) grp_rhs(GroupDev d) {
   }
 }
 
+// Learned warm start (warm_start 3), three kernels after grp_rhs.
+//   grp_extrap   e = quadratic extrapolation of the last three solutions -> xe
+//   grp_resid_e  r_e = b - A e -> r_alt, the right-hand side of the
+//                correction system A (x_n - e) = r_e
+//   grp_guess_mlp  per free row the network reads the last four solutions as
+//                the third difference D3 = x - 3 xh1 + 3 xh2 - xh3 and the
+//                compressed D2, D1 and level (asinh), and the Jacobi-scaled
+//                correction right-hand side pre r_e with its mean over the
+//                row's neighbours (A's pattern), all divided by the row scale
+//                sigma = rms(D3, pre r_e); its output y gives the guess
+//                e + sigma y in x.  Until the network is trained (mlp_on 0)
+//                x = e.  Sampled rows store their inputs, e and sigma for
+//                training.  A warp takes the 32 rows of one slice.
+template <typename T>
+__global__ void __launch_bounds__(kGB) grp_extrap(GroupDev d) {
+  const int64_t i = (int64_t)blockIdx.x * kGB + threadIdx.x;
+  if (i >= d.nrow) return;
+  const int s = d.slice_sim[i >> 5];
+  if (!running(d, s) || d.free_edge[i] < 0) return;
+  const T* x = (const T*)d.x;
+  const T a = x[i], b = ((const T*)d.xh1)[i], c = ((const T*)d.xh2)[i];
+  const int step = d.step[s];
+  ((T*)d.xe)[i] = step >= 3 ? (T)3 * a - (T)3 * b + c : (step >= 2 ? (T)2 * a - b : a);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kGB) grp_resid_e(GroupDev d) {
+  const int64_t i = (int64_t)blockIdx.x * kGB + threadIdx.x;
+  if (i >= d.nrow) return;
+  const int s = d.slice_sim[i >> 5];
+  if (!running(d, s)) return;
+  const T* xe = (const T*)d.xe;
+  ((T*)d.r_alt)[i] = ((const T*)d.rhs)[i] - sell_dot<T>(d.A, i, [&](int32_t c) { return xe[c]; });
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kGB) grp_guess_mlp(GroupDev d) {
+  __shared__ __align__(16) unsigned char img[kImgBytes];
+  if (d.mlp_on) mlp_load_image(img, d.mlp_img);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int64_t sl = ((int64_t)blockIdx.x * kGB + threadIdx.x) >> 5;
+  if (sl * 32 >= d.nrow) return;  // whole warp
+  const int64_t i = sl * 32 + lane;
+  const int s = d.slice_sim[sl];
+  if (!running(d, s)) return;  // whole warp: one simulation per slice
+  const bool real = d.free_edge[i] >= 0;
+  T* x = (T*)d.x;
+  T* h1 = (T*)d.xh1;
+  T* h2 = (T*)d.xh2;
+  T* h3 = (T*)d.xh3;
+  const T* re = (const T*)d.r_alt;
+  const T* pre = (const T*)d.pre;
+  const double a = x[i], b1 = h1[i], c = h2[i], dd = h3[i];
+  const double e = (double)((const T*)d.xe)[i];
+  // neighbour mean of r_e over the row's pattern (entries with a value, self excluded)
+  double sum = 0.0;
+  int cnt = 0;
+  {
+    const int64_t b0 = d.A.ptr[sl];
+    const int len = (int)((d.A.ptr[sl + 1] - b0) >> 5);
+    const int32_t* col = d.A.col + b0 + lane;
+    const T* val = (const T*)d.A.val + b0 + lane;
+    for (int j = 0; j < len; j++) {
+      const int32_t cc = __ldg(col + 32 * j);
+      if (__ldg(val + 32 * j) != (T)0 && cc != (int32_t)i) {
+        sum += (double)re[cc];
+        cnt++;
+      }
+    }
+  }
+  const double pr = (double)pre[i];
+  const double jr = pr * (double)re[i];
+  const double jm = cnt ? pr * sum / cnt : jr;
+  const double d3 = a - 3.0 * b1 + 3.0 * c - dd, d2 = a - 2.0 * b1 + c, d1 = a - b1;
+  const double sg = sqrt(0.5 * (d3 * d3 + jr * jr));
+  const bool ok = real && sg > 0.0 && isfinite(sg) && d.step[s] >= 4;
+  const double inv = ok ? 1.0 / sg : 0.0;
+  float f[6] = {(float)(d3 * inv), (float)asinh(d2 * inv), (float)asinh(d1 * inv), (float)asinh(a * inv),
+                (float)(jr * inv), (float)(jm * inv)};
+  double guess = e;
+  if (d.mlp_on) {
+    const MlpSmem w = mlp_view(img);
+    float yv = 0.0f;
+#pragma unroll
+    for (int qt = 0; qt < 2; qt++) {
+      uint32_t a1[4], a2[4][4], a3[4][4];
+      float z1[8][4], z2[8][4], y[4];
+      mlp_input_fragment(a1, f, 16 * qt, lane);
+      mlp_forward(w, a1, z1, z2, a2, a3, y, lane);
+      const float v = mlp_output_to_rows(y, lane);
+      if ((lane >> 4) == qt) yv = v;
+    }
+    if (ok) guess = e + sg * (double)yv;
+  }
+  if (!real) return;
+  h3[i] = (T)c;
+  h2[i] = (T)b1;
+  h1[i] = (T)a;
+  x[i] = (T)guess;
+  if (d.nsamp && i >= d.samp_first && (i - d.samp_first) % d.samp_stride == 0) {
+    const int64_t k = (i - d.samp_first) / d.samp_stride;
+    if (k < d.nsamp) {
+      for (int q = 0; q < 6; q++) d.samp_in[6 * k + q] = f[q];
+      d.samp_e[k] = (float)e;
+      d.samp_s[k] = (float)sg;
+      d.samp_row[k] = ok ? (int32_t)i : -1;
+    }
+  }
+}
+
+// Training targets of the sampled rows after the solve: (x_n - e) / sigma
+template <typename T>
+__global__ void grp_mlp_targets(GroupDev d) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.nsamp) return;
+  const int32_t i = d.samp_row[k];
+  if (i < 0) {
+    d.samp_t[k] = 0.0f;
+    d.samp_w[k] = 0.0f;
+    return;
+  }
+  // during training the CG starts from xe = e and leaves it untouched
+  const double t = ((double)((const T*)d.x)[i] - (double)((const T*)d.xe)[i]) / (double)d.samp_s[k];
+  d.samp_t[k] = (float)t;
+  d.samp_w[k] = isfinite(t) ? 1.0f : 0.0f;
+  if (!isfinite(t)) d.samp_t[k] = 0.0f;
+}
+
 struct SimCg {
   double rz, res0, bnorm, res, alpha, beta;
-  int it, active;
+  int it, active, sel, pad;
 };
+constexpr int kPart = kCgPart;
 
 // p_{j+1} at one row from z = pre r (stored by the residual phase), rounded
 // the same way wherever it is formed
@@ -263,13 +394,35 @@ __global__ void __launch_bounds__(kCgThreads, 2) grp_cg(GroupDev d) {
   const T* pre = (const T*)d.pre;
   T* z = (T*)d.z;
   auto pbuf = [&](int k) { return (k & 1) ? (T*)d.p1 : (T*)d.p0; };
+  // the buffers of a simulation's start (dual start: the extrapolation's)
+  auto xs_of = [&](const SimCg& c) { return c.sel ? (T*)d.xe : x; };
+  auto rs_of = [&](const SimCg& c) { return c.sel ? (T*)d.r_alt : r; };
+  auto zs_of = [&](const SimCg& c) { return c.sel ? (T*)d.z_alt : z; };
 
+  auto flush5 = [&](int g, double a0, double a1, double a2, double a3, double a4) {
+    a3 = warp_sum(a3);
+    a4 = warp_sum(a4);
+    if (lane == 0) {
+      double* w = wp + ((g - g0) * kCgWarps + warp) * kPart;
+      w[3] = a3;
+      w[4] = a4;
+    }
+    a0 = warp_sum(a0);
+    a1 = warp_sum(a1);
+    a2 = warp_sum(a2);
+    if (lane == 0) {
+      double* w = wp + ((g - g0) * kCgWarps + warp) * kPart;
+      w[0] = a0;
+      w[1] = a1;
+      w[2] = a2;
+    }
+  };
   auto flush = [&](int g, double a0, double a1, double a2) {
     a0 = warp_sum(a0);
     a1 = warp_sum(a1);
     a2 = warp_sum(a2);
     if (lane == 0) {
-      double* w = wp + ((g - g0) * kCgWarps + warp) * 3;
+      double* w = wp + ((g - g0) * kCgWarps + warp) * kPart;
       w[0] = a0;
       w[1] = a1;
       w[2] = a2;
@@ -280,8 +433,8 @@ __global__ void __launch_bounds__(kCgThreads, 2) grp_cg(GroupDev d) {
     for (int gl = threadIdx.x; gl < g1 - g0; gl += kCgThreads)
       for (int k = 0; k < nq; k++) {
         double a = 0.0;
-        for (int w = 0; w < kCgWarps; w++) a += wp[(gl * kCgWarps + w) * 3 + k];
-        d.part[3 * (int64_t)(g0 + gl) + k] = a;
+        for (int w = 0; w < kCgWarps; w++) a += wp[(gl * kCgWarps + w) * kPart + k];
+        d.part[kPart * (int64_t)(g0 + gl) + k] = a;
       }
   };
   // per-simulation totals of the published partials: one warp per
@@ -289,9 +442,9 @@ __global__ void __launch_bounds__(kCgThreads, 2) grp_cg(GroupDev d) {
   // runs on lane 0 with the nq totals t[]
   auto totals = [&](int nq, auto&& f) {
     for (int s = warp; s < d.S; s += kCgWarps) {
-      double t[3] = {0.0, 0.0, 0.0};
+      double t[kPart] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
       for (int g = d.sim_seg[s] + lane; g < d.sim_seg[s + 1]; g += 32)
-        for (int k = 0; k < nq; k++) t[k] += d.part[3 * (int64_t)g + k];
+        for (int k = 0; k < nq; k++) t[k] += d.part[kPart * (int64_t)g + k];
       for (int k = 0; k < nq; k++) t[k] = warp_sum(t[k]);
       if (lane == 0) f(s, t);
     }
@@ -302,10 +455,15 @@ __global__ void __launch_bounds__(kCgThreads, 2) grp_cg(GroupDev d) {
     return c.res > d.tol[s] * c.bnorm;
   };
 
-  // r = b - A x; rr = r.r, rz = r.(pre r), bb = b.b
+  // r = b - A x; rr = r.r, rz = r.(pre r), bb = b.b; in the dual start the
+  // same for the second guess xe (r_alt, z_alt)
+  T* xe = (T*)d.xe;
+  T* ra = (T*)d.r_alt;
+  T* za = (T*)d.z_alt;
+  const bool dual = d.dual != 0;
   for (int g = g0; g < g1; g++) {
     const int s = d.seg_sim[g];
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0;
     if (running(d, s))
       for (int64_t sl = d.seg_s0[g] + warp; sl < d.seg_s1[g]; sl += kCgWarps) {
         const int64_t i = sl * 32 + lane;
@@ -317,15 +475,25 @@ __global__ void __launch_bounds__(kCgThreads, 2) grp_cg(GroupDev d) {
         a0 += rd * rd;
         a1 += rd * (double)zi;
         a2 += (double)b[i] * (double)b[i];
+        if (dual) {
+          const T r2 = b[i] - sell_dot<T>(d.A, i, [&](int32_t c) { return xe[c]; });
+          ra[i] = r2;
+          const T z2 = mulT(pre[i], r2);
+          za[i] = z2;
+          a3 += (double)r2 * (double)r2;
+          a4 += (double)r2 * (double)z2;
+        }
       }
-    flush(g, a0, a1, a2);
+    flush5(g, a0, a1, a2, a3, a4);
   }
-  publish(3);
+  publish(dual ? 5 : 3);
   grid.sync();
-  totals(3, [&](int s, const double* t) {
+  totals(dual ? 5 : 3, [&](int s, const double* t) {
     SimCg c;
-    c.res0 = sqrt(t[0]);
-    c.rz = t[1];
+    c.sel = dual && t[3] < t[0] ? 1 : 0;
+    c.pad = 0;
+    c.res0 = sqrt(c.sel ? t[3] : t[0]);
+    c.rz = c.sel ? t[4] : t[1];
     c.bnorm = sqrt(t[2]);
     c.res = c.res0;
     c.alpha = c.beta = 0.0;
@@ -350,15 +518,17 @@ __global__ void __launch_bounds__(kCgThreads, 2) grp_cg(GroupDev d) {
         const T beta = (T)c.beta, alpha = (T)c.alpha;
         const T* pold = pbuf(c.it + 1);
         T* pn = pbuf(c.it);
+        T* xs = xs_of(c);
+        const T* zs = zs_of(c);
         for (int64_t sl = d.seg_s0[g] + warp; sl < d.seg_s1[g]; sl += kCgWarps) {
           const int64_t i = sl * 32 + lane;
           const T po = first ? (T)0 : pold[i];
-          const T pi = p_next<T>(z[i], po, beta, first);
-          if (!first) x[i] = fmaT(alpha, po, x[i]);
+          const T pi = p_next<T>(zs[i], po, beta, first);
+          if (!first) xs[i] = fmaT(alpha, po, xs[i]);
           pn[i] = pi;
           if (kFused) {
             const T qi = sell_dot<T>(d.A, i, [&](int32_t cc) {
-              return p_next<T>(z[cc], first ? (T)0 : pold[cc], beta, first);
+              return p_next<T>(zs[cc], first ? (T)0 : pold[cc], beta, first);
             });
             q[i] = qi;
             a0 += (double)pi * (double)qi;
@@ -397,12 +567,14 @@ __global__ void __launch_bounds__(kCgThreads, 2) grp_cg(GroupDev d) {
       double a0 = 0.0, a1 = 0.0;
       if (st[s].active) {
         const T alpha = (T)st[s].alpha;
+        T* rs = rs_of(st[s]);
+        T* zs = zs_of(st[s]);
         for (int64_t sl = d.seg_s0[g] + warp; sl < d.seg_s1[g]; sl += kCgWarps) {
           const int64_t i = sl * 32 + lane;
-          const T ri = r[i] - alpha * q[i];
-          r[i] = ri;
+          const T ri = rs[i] - alpha * q[i];
+          rs[i] = ri;
           const T zi = mulT(pre[i], ri);
-          z[i] = zi;
+          zs[i] = zi;
           const double rd = (double)ri;
           a0 += rd * rd;
           a1 += rd * (double)zi;
@@ -429,12 +601,15 @@ __global__ void __launch_bounds__(kCgThreads, 2) grp_cg(GroupDev d) {
   for (int g = g0; g < g1; g++) {
     const int s = d.seg_sim[g];
     const SimCg c = st[s];
-    if (!running(d, s) || c.it == 0) continue;
+    if (!running(d, s)) continue;
     const T alpha = (T)c.alpha;
     const T* pl = pbuf(c.it - 1);
+    T* xs = xs_of(c);
     for (int64_t sl = d.seg_s0[g] + warp; sl < d.seg_s1[g]; sl += kCgWarps) {
       const int64_t i = sl * 32 + lane;
-      x[i] = fmaT(alpha, pl[i], x[i]);
+      T v = xs[i];
+      if (c.it > 0) v = fmaT(alpha, pl[i], v);
+      if (c.it > 0 || c.sel) x[i] = v;  // the solution always ends in x
     }
   }
   if (blockIdx.x == 0)
@@ -446,6 +621,7 @@ __global__ void __launch_bounds__(kCgThreads, 2) grp_cg(GroupDev d) {
       d.cg_resid[k] = c.res / c.res0;
       const bool unmet = d.cg_criterion == 0 ? c.res / c.res0 > d.tol[s] : c.res > d.tol[s] * c.bnorm;
       d.cg_limit[k] = unmet ? 1 : 0;
+      if (d.kept) d.kept[k] = dual && !c.sel ? 1 : 0;
     }
 }
 
@@ -471,7 +647,7 @@ __global__ void grp_bump(GroupDev d) {
 // ------------------------------------------------------------------ launch
 static inline unsigned gblk(int64_t n) { return (unsigned)(n > 0 ? (n + kGB - 1) / kGB : 1); }
 
-static size_t cg_smem(int S) { return sizeof(SimCg) * (size_t)S + sizeof(double) * kMaxSeg * kCgWarps * 3; }
+static size_t cg_smem(int S) { return sizeof(SimCg) * (size_t)S + sizeof(double) * kMaxSeg * kCgWarps * kPart; }
 
 template <typename T>
 int group_cg_blocks(int device, int S, size_t* smem) {
@@ -499,6 +675,11 @@ cudaError_t group_launch_step(const GroupDev& d, int cg_blocks, int cg_variant, 
   if (ev) cudaEventRecord(ev[1], st);
   grp_sources<T><<<d.S, kGB, 0, st>>>(d);
   grp_rhs<T><<<gblk(d.nrow), kGB, 0, st>>>(d);
+  if (d.warm_start == 3) {
+    grp_extrap<T><<<gblk(d.nrow), kGB, 0, st>>>(d);
+    grp_resid_e<T><<<gblk(d.nrow), kGB, 0, st>>>(d);
+    grp_guess_mlp<T><<<gblk(d.nrow), kGB, 0, st>>>(d);
+  }
   if (ev) cudaEventRecord(ev[2], st);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cg_blocks);
@@ -520,6 +701,14 @@ cudaError_t group_launch_step(const GroupDev& d, int cg_blocks, int cg_variant, 
   if (ev) cudaEventRecord(ev[5], st);
   return cudaGetLastError();
 }
+
+template <typename T>
+cudaError_t group_launch_targets(const GroupDev& d, cudaStream_t st) {
+  if (d.nsamp) grp_mlp_targets<T><<<(unsigned)((d.nsamp + 255) / 256), 256, 0, st>>>(d);
+  return cudaGetLastError();
+}
+template cudaError_t group_launch_targets<double>(const GroupDev&, cudaStream_t);
+template cudaError_t group_launch_targets<float>(const GroupDev&, cudaStream_t);
 
 template cudaError_t group_launch_step<double>(const GroupDev&, int, int, size_t, cudaStream_t, cudaEvent_t*);
 template cudaError_t group_launch_step<float>(const GroupDev&, int, int, size_t, cudaStream_t, cudaEvent_t*);

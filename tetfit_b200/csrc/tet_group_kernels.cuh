@@ -32,6 +32,7 @@ constexpr int kCgThreads = 512;
 constexpr int kCgWarps = kCgThreads / 32;
 constexpr int kMaxSeg = 32;       // segments per CG block
 constexpr int kMaxGroup = 1024;   // simulations per group
+constexpr int kCgPart = 6;        // CG partial sums per segment
 
 struct SellDev {
   const int64_t* ptr = nullptr;  // [nslice + 1]
@@ -69,6 +70,18 @@ struct GroupDev {
   const int* sim_seg = nullptr;  // [S + 1]
   double* part = nullptr;        // [nseg][3]
   int cg_maxiter = 100, cg_criterion = 0, warm_start = 0;
+  // learned warm start (warm_start 3): the network's guess goes to x, the
+  // quadratic extrapolation to xe; with dual set, the CG starts from the one
+  // whose residual is smaller, per simulation (sel: extrapolation won), and
+  // kept[stat_off + step] records 1 when the network's guess was kept
+  void *xe = nullptr, *r_alt = nullptr, *z_alt = nullptr;
+  int mlp_on = 0, dual = 0;
+  int8_t* kept = nullptr;
+  const unsigned char* mlp_img = nullptr;
+  // training samples: rows i = samp_first + k * samp_stride, k < nsamp
+  float *samp_in = nullptr, *samp_e = nullptr, *samp_s = nullptr, *samp_t = nullptr, *samp_w = nullptr;
+  int32_t* samp_row = nullptr;
+  int64_t nsamp = 0, samp_stride = 1, samp_first = 0;
   int32_t* cg_iters = nullptr;
   double* cg_resid = nullptr;
   int32_t* cg_limit = nullptr;
@@ -104,5 +117,7 @@ cudaError_t group_launch_step(const GroupDev& d, int cg_blocks, int cg_variant, 
                               cudaEvent_t* ev);
 template <typename T>
 int group_cg_blocks(int device, int S, size_t* smem);
+template <typename T>
+cudaError_t group_launch_targets(const GroupDev& d, cudaStream_t st);
 
 }  // namespace tf
