@@ -57,7 +57,7 @@ WORKLOADS = {
     # ||r|| <= 1e-8 ||b||; the plain arm runs the same members one at a time in FP64 with the
     # reference's previous-solution guess
     "batch128": dict(kind="batch", members=128, n_lo=8, n_hi=48, steps=1000, seed=31337, prec="fp32",
-                     warm="extrapolate", crit="rhs", plain_steps=10),
+                     warm="learned", learn_steps=300, crit="rhs", plain_steps=10),
 }
 
 
@@ -297,16 +297,18 @@ def run_ours(args, rank, world, local_rank):
     return result
 
 
-def cg_bytes_per_launch(infos, its, es):
+def cg_bytes_per_launch(infos, its, es, dual=False):
     """Algorithmic bytes of one grp_cg launch: per member and iteration the
-    stored entries of A (int32 column + value) and 11 row-vector accesses
-    (p-update/SpMV phase: z, r, p_old, x read, x, p_new, q written; residual
-    phase: r, q, pre read, r written), plus the initial residual (A once and
-    b, x, pre, r) and the final x update (x, p read, x written)."""
+    entries of A (int32 column + value) and 11 row-vector accesses
+    (p-update/SpMV phase: z, p_old, x read, x, p_new, q written; residual
+    phase: r, q, pre read, r, z written), plus the initial residual (A once;
+    b, pre read, r, z written; twice with the learned warm start's dual
+    start) and the final x update (x, p read, x written)."""
     total = 0.0
     for info, it in zip(infos, its):
         nnz, n = info["nnz_system"], info["n_free"]
-        total += it * (nnz * (4 + es) + 11 * es * n) + nnz * (4 + es) + 4 * es * n + 3 * es * n
+        start = nnz * (4 + es) + 5 * es * n
+        total += it * (nnz * (4 + es) + 11 * es * n) + start * (2 if dual else 1) + 3 * es * n
     return total
 
 
@@ -346,20 +348,28 @@ def run_batch(args, rank, world, local_rank):
     write_s = time.time() - t0
     es = 4 if w["prec"] == "fp32" else 8
     t0 = time.time()
-    b = tb.Batch(members, precision=w["prec"], cg_criterion=w["crit"], warm_start=w["warm"], device=local_rank)
+    learn = w.get("learn_steps", 0) if w["warm"] == "learned" else 0
+    b = tb.Batch(members, precision=w["prec"], cg_criterion=w["crit"], warm_start=w["warm"], device=local_rank,
+                 learn_steps=learn)
     setup_s = time.time() - t0
     infos = [b.info(m) for m in range(b.size)]
     dofs = sum(i["n_edges"] + i["n_faces"] for i in infos)
     K, W = args.steps, args.warmup
     nph = min(K, 10)
     K2 = min(K, 20)
-    need = W + nph + K + K2
+    need = learn + W + nph + K + K2
     if need > w["steps"]:
         raise SystemExit(f"batch members have {w['steps']} steps, bench needs {need}")
-    b.step(W)
+    # the learned warm start trains on its first steps (untimed), then W warm-up steps
+    t0 = time.time()
+    if learn:
+        b.step(learn)
+    train_s = time.time() - t0
+    W = learn + W
+    b.step(W - learn)
     ms5, _ = b.phase_times(nph)
     its_ph = [b.solver_stats(m)[0][W:W + nph].mean() for m in range(b.size)]
-    cg_bytes = cg_bytes_per_launch(infos, its_ph, es)
+    cg_bytes = cg_bytes_per_launch(infos, its_ph, es, dual=bool(learn))
     cg_ms = ms5[2] / nph
     barrier()
     with ClockSampler(local_rank) as clk:
@@ -368,6 +378,14 @@ def run_batch(args, rank, world, local_rank):
     barrier()
     stats = [b.solver_stats(m)[0] for m in range(b.size)]
     it_timed = float(np.mean([s[W + nph:W + nph + K].mean() for s in stats]))
+    learned_info = None
+    if learn:
+        kept = np.concatenate([b.guess_stats(m)[W + nph:W + nph + K] for m in range(b.size)])
+        loss = b.training_loss()
+        learned_info = {"training_steps": learn, "training_s": round(train_s, 1), "adam_steps": int(len(loss)),
+                        "loss_first": float(loss[0]) if len(loss) else None,
+                        "loss_last": float(loss[-1]) if len(loss) else None,
+                        "network_guess_kept_frac": float(kept.mean())}
     # e2e: tf_batch_step_io, every member's carrier values H2D and probe samples D2H each step
     n_src = sum(i["n_sources"] for i in infos)
     n_probe_vals = 6 * sum(i["n_probes"] for i in infos)
@@ -421,13 +439,14 @@ def run_batch(args, rank, world, local_rank):
         ns = sorted(c.n for c in cases)
         result = {
             "metric": "dof-steps/s", "value": value, "unit": "dof-steps/s", "n_gpus": world, "steps": K,
-            "warmup": W, "ms_per_step": max_ms / K, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": max_ms / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if es == 4 else "f64", "data": "synthetic",
             "config": {"workload": f"{args.workload}: {w['members']} gfdtd members in one group, Kuhn meshes "
                                    f"n ~ U{{{w['n_lo']}..{w['n_hi']}}} (min {ns[0]}, median {ns[len(ns) // 2]}, "
                                    f"max {ns[-1]}) x 6 tets, eps_r ~ U[1,4] per x-half, f ~ U[1e8,4e8] Hz, "
                                    f"{w['prec']} fields, FP64 CG reductions, CG tol 1e-8 (||r|| <= tol ||b||), "
-                                   f"{w['warm']} warm start",
+                                   f"{w['warm']} warm start" + (f" (network trained on the first {learn} steps, "
+                                                                f"untimed)" if learn else ""),
                        "members": w["members"], "dofs": dofs, "parallelism": f"replicas x{world}",
                        "l2": f"CG working set {cg_bytes / max(it_timed, 1) / 1e6:.0f} MB per iteration > 126 MB L2 "
                              f"(no flush needed)",
@@ -444,6 +463,7 @@ def run_batch(args, rank, world, local_rank):
                            "mode": "members one at a time, FP64, previous-solution guess, same CG tolerance",
                            "speedup": value / plain_value},
             "probe_error_vs_fp64_oracle": {"members": len(perr), "max_rel_l2": max(perr) if perr else None},
+            "learned_warm_start": learned_info,
             "e2e": {"value": world * dofs * K2 / max_e2e, "unit": "dof-steps/s",
                     "h2d_bytes_per_step": 8 * n_src, "d2h_bytes_per_step": 8 * n_probe_vals,
                     "api": "tf_batch_step_io"},

@@ -75,10 +75,10 @@ __global__ void __launch_bounds__(256) mlp_eval_kernel(const unsigned char* imag
   float res = 0.0f;
 #pragma unroll
   for (int q = 0; q < 2; q++) {
-    uint32_t a1[4], a2[4][4], a3[4][4];
-    float z1[8][4], z2[8][4], y[4];
+    uint32_t a1[4];
+    float y[4];
     mlp_input_fragment(a1, f, 16 * q, lane);
-    mlp_forward(w, a1, z1, z2, a2, a3, y, lane);
+    mlp_infer(w, a1, y, lane);
     const float v = mlp_output_to_rows(y, lane);
     if ((lane >> 4) == q) res = v;
   }
@@ -153,8 +153,8 @@ __global__ void __launch_bounds__(32 * kTrainWarps) mlp_train_kernel(const unsig
 #pragma unroll
     for (int c = 0; c < 4; c++) {
       const int nn = nt * 8 + 2 * t + (c & 1), rr = warp * 16 + g + (c >= 2 ? 8 : 0);
-      h1T[nn * kLdR + rr] = __float2bfloat16_rn(mlp_silu(z1[nt][c]));
-      h2T[nn * kLdR + rr] = __float2bfloat16_rn(mlp_silu(z2[nt][c]));
+      h1T[nn * kLdR + rr] = __float2bfloat16_rn(mlp_silu_bf16(z1[nt][c]));
+      h2T[nn * kLdR + rr] = __float2bfloat16_rn(mlp_silu_bf16(z2[nt][c]));
     }
   // dL/dz2 = dL/dy W3 silu'(z2)
   float d2[8][4];

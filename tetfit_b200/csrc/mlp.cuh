@@ -60,11 +60,38 @@ __device__ __forceinline__ void mlp_lda(uint32_t a[4], const __nv_bfloat16* M, i
   a[3] = *reinterpret_cast<const uint32_t*>(p + 8 * ld + 8);
 }
 
-__device__ __forceinline__ float mlp_sigmoid(float z) { return 1.0f / (1.0f + __expf(-z)); }
+// sigmoid(z) = (1 + tanh(z / 2)) / 2 with the hardware tanh approximation
+// (one special-function op); training and inference share it.
+__device__ __forceinline__ float mlp_sigmoid(float z) {
+  float t;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(0.5f * z));
+  return 0.5f + 0.5f * t;
+}
 __device__ __forceinline__ float mlp_silu(float z) { return z * mlp_sigmoid(z); }
 __device__ __forceinline__ float mlp_dsilu(float z) {
   const float s = mlp_sigmoid(z);
   return s * (1.0f + z * (1.0f - s));
+}
+// silu of two values packed as the next layer's BF16 pair: both tanh(z / 2)
+// in one bf16x2 special-function op (the result is BF16 anyway)
+__device__ __forceinline__ uint32_t mlp_silu_pack(float z0, float z1) {
+  const uint32_t hz = mlp_pack(0.5f * z0, 0.5f * z1);
+  uint32_t th;
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(th) : "r"(hz));
+  const float t0 = __uint_as_float(th << 16), t1 = __uint_as_float(th & 0xffff0000u);
+  return mlp_pack(0.5f * z0 * (1.0f + t0), 0.5f * z1 * (1.0f + t1));
+}
+__device__ __forceinline__ float mlp_silu_bf16(float z) {
+  const uint32_t p = mlp_silu_pack(z, 0.0f);
+  return __uint_as_float(p << 16);
+}
+
+// asinh from its definition, sign(x) log(|x| + sqrt(x^2 + 1)); log(2|x|) for
+// large |x| where x^2 + 1 = x^2 in float
+__device__ __forceinline__ float mlp_asinh(float x) {
+  const float ax = fabsf(x);
+  const float r = ax > 1.0e4f ? __logf(2.0f * ax) : __logf(ax + sqrtf(ax * ax + 1.0f));
+  return copysignf(r, x);
 }
 
 // Shared-memory view of the weight image
@@ -116,10 +143,10 @@ __device__ __forceinline__ void mlp_forward(const MlpSmem& w, const uint32_t a1[
   }
 #pragma unroll
   for (int kt = 0; kt < 4; kt++) {
-    a2[kt][0] = mlp_pack(mlp_silu(z1[2 * kt][0]), mlp_silu(z1[2 * kt][1]));
-    a2[kt][1] = mlp_pack(mlp_silu(z1[2 * kt][2]), mlp_silu(z1[2 * kt][3]));
-    a2[kt][2] = mlp_pack(mlp_silu(z1[2 * kt + 1][0]), mlp_silu(z1[2 * kt + 1][1]));
-    a2[kt][3] = mlp_pack(mlp_silu(z1[2 * kt + 1][2]), mlp_silu(z1[2 * kt + 1][3]));
+    a2[kt][0] = mlp_silu_pack(z1[2 * kt][0], z1[2 * kt][1]);
+    a2[kt][1] = mlp_silu_pack(z1[2 * kt][2], z1[2 * kt][3]);
+    a2[kt][2] = mlp_silu_pack(z1[2 * kt + 1][0], z1[2 * kt + 1][1]);
+    a2[kt][3] = mlp_silu_pack(z1[2 * kt + 1][2], z1[2 * kt + 1][3]);
   }
 #pragma unroll
   for (int nt = 0; nt < 8; nt++) {
@@ -137,10 +164,10 @@ __device__ __forceinline__ void mlp_forward(const MlpSmem& w, const uint32_t a1[
   }
 #pragma unroll
   for (int kt = 0; kt < 4; kt++) {
-    a3[kt][0] = mlp_pack(mlp_silu(z2[2 * kt][0]), mlp_silu(z2[2 * kt][1]));
-    a3[kt][1] = mlp_pack(mlp_silu(z2[2 * kt][2]), mlp_silu(z2[2 * kt][3]));
-    a3[kt][2] = mlp_pack(mlp_silu(z2[2 * kt + 1][0]), mlp_silu(z2[2 * kt + 1][1]));
-    a3[kt][3] = mlp_pack(mlp_silu(z2[2 * kt + 1][2]), mlp_silu(z2[2 * kt + 1][3]));
+    a3[kt][0] = mlp_silu_pack(z2[2 * kt][0], z2[2 * kt][1]);
+    a3[kt][1] = mlp_silu_pack(z2[2 * kt][2], z2[2 * kt][3]);
+    a3[kt][2] = mlp_silu_pack(z2[2 * kt + 1][0], z2[2 * kt + 1][1]);
+    a3[kt][3] = mlp_silu_pack(z2[2 * kt + 1][2], z2[2 * kt + 1][3]);
   }
   const float bo = t == 0 ? w.b3[0] : 0.0f;
   y[0] = bo;
@@ -152,6 +179,65 @@ __device__ __forceinline__ void mlp_forward(const MlpSmem& w, const uint32_t a1[
     uint32_t b[2];
     mlp_ldb(b, w.w3, kLd2, kt, 0, lane);
     mlp_mma(y, a3[kt], b);
+  }
+}
+
+// Inference-only forward pass of one 16-row tile: layer by layer, nothing
+// kept for a backward pass (same arithmetic as mlp_forward).
+__device__ __forceinline__ void mlp_infer(const MlpSmem& w, const uint32_t a1[4], float y[4], int lane) {
+  const int t = lane & 3;
+  uint32_t a2[4][4];
+#pragma unroll
+  for (int kt = 0; kt < 4; kt++) {
+    float c[2][4];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int nt = 2 * kt + h;
+      const float b0 = w.b1[nt * 8 + 2 * t], b1v = w.b1[nt * 8 + 2 * t + 1];
+      c[h][0] = b0;
+      c[h][1] = b1v;
+      c[h][2] = b0;
+      c[h][3] = b1v;
+      uint32_t b[2];
+      mlp_ldb(b, w.w1, kLd1, 0, nt, lane);
+      mlp_mma(c[h], a1, b);
+    }
+    a2[kt][0] = mlp_silu_pack(c[0][0], c[0][1]);
+    a2[kt][1] = mlp_silu_pack(c[0][2], c[0][3]);
+    a2[kt][2] = mlp_silu_pack(c[1][0], c[1][1]);
+    a2[kt][3] = mlp_silu_pack(c[1][2], c[1][3]);
+  }
+  const float bo = t == 0 ? w.b3[0] : 0.0f;
+  y[0] = bo;
+  y[1] = 0.0f;
+  y[2] = bo;
+  y[3] = 0.0f;
+#pragma unroll
+  for (int k3 = 0; k3 < 4; k3++) {
+    float o[2][4];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int nt = 2 * k3 + h;
+      const float b0 = w.b2[nt * 8 + 2 * t], b1v = w.b2[nt * 8 + 2 * t + 1];
+      o[h][0] = b0;
+      o[h][1] = b1v;
+      o[h][2] = b0;
+      o[h][3] = b1v;
+#pragma unroll
+      for (int kt = 0; kt < 4; kt++) {
+        uint32_t b[2];
+        mlp_ldb(b, w.w2t, kLd2, kt, nt, lane);
+        mlp_mma(o[h], a2[kt], b);
+      }
+    }
+    uint32_t a3[4];
+    a3[0] = mlp_silu_pack(o[0][0], o[0][1]);
+    a3[1] = mlp_silu_pack(o[0][2], o[0][3]);
+    a3[2] = mlp_silu_pack(o[1][0], o[1][1]);
+    a3[3] = mlp_silu_pack(o[1][2], o[1][3]);
+    uint32_t b[2];
+    mlp_ldb(b, w.w3, kLd2, k3, 0, lane);
+    mlp_mma(y, a3, b);
   }
 }
 

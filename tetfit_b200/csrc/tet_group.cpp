@@ -347,6 +347,9 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
     mlp_.loss = fz(1);
     CU(mlp_launch_pack(mlp_.params, mlp_.image, stream_));
     d.mlp_img = mlp_.image;
+    int sms = 0;
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt_.device));
+    d.guess_blocks = 3 * sms;
     loss_cap_ = (int64_t)std::max(1, opt_.learn_steps) * std::max(1, opt_.learn_inner);
     loss_hist_ = fz(loss_cap_);
   }

@@ -273,77 +273,83 @@ __global__ void __launch_bounds__(kGB) grp_resid_e(GroupDev d) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kGB) grp_guess_mlp(GroupDev d) {
+__global__ void __launch_bounds__(kGB, 3) grp_guess_mlp(GroupDev d) {
   __shared__ __align__(16) unsigned char img[kImgBytes];
   if (d.mlp_on) mlp_load_image(img, d.mlp_img);
   __syncthreads();
+  const MlpSmem w = mlp_view(img);
   const int lane = threadIdx.x & 31;
-  const int64_t sl = ((int64_t)blockIdx.x * kGB + threadIdx.x) >> 5;
-  if (sl * 32 >= d.nrow) return;  // whole warp
-  const int64_t i = sl * 32 + lane;
-  const int s = d.slice_sim[sl];
-  if (!running(d, s)) return;  // whole warp: one simulation per slice
-  const bool real = d.free_edge[i] >= 0;
+  const int64_t nsl = d.nrow >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * kGB) >> 5;
   T* x = (T*)d.x;
   T* h1 = (T*)d.xh1;
   T* h2 = (T*)d.xh2;
   T* h3 = (T*)d.xh3;
   const T* re = (const T*)d.r_alt;
   const T* pre = (const T*)d.pre;
-  const double a = x[i], b1 = h1[i], c = h2[i], dd = h3[i];
-  const double e = (double)((const T*)d.xe)[i];
-  // neighbour mean of r_e over the row's pattern (entries with a value, self excluded)
-  double sum = 0.0;
-  int cnt = 0;
-  {
-    const int64_t b0 = d.A.ptr[sl];
-    const int len = (int)((d.A.ptr[sl + 1] - b0) >> 5);
-    const int32_t* col = d.A.col + b0 + lane;
-    const T* val = (const T*)d.A.val + b0 + lane;
-    for (int j = 0; j < len; j++) {
-      const int32_t cc = __ldg(col + 32 * j);
-      if (__ldg(val + 32 * j) != (T)0 && cc != (int32_t)i) {
-        sum += (double)re[cc];
-        cnt++;
+  // a warp takes whole slices (one simulation each), the grid strides over them
+  for (int64_t sl = ((int64_t)blockIdx.x * kGB + threadIdx.x) >> 5; sl < nsl; sl += nw) {
+    const int s = d.slice_sim[sl];
+    if (!running(d, s)) continue;
+    const int64_t i = sl * 32 + lane;
+    const bool real = d.free_edge[i] >= 0;
+    const double a = x[i], b1 = h1[i], c = h2[i], dd = h3[i];
+    const double e = (double)((const T*)d.xe)[i];
+    // neighbour mean of r_e over the row's pattern (padding entries point at
+    // the row itself and drop out with it)
+    float sum = 0.0f;
+    int cnt = 0;
+    {
+      const int64_t b0 = d.A.ptr[sl];
+      const int len = (int)((d.A.ptr[sl + 1] - b0) >> 5);
+      const int32_t* col = d.A.col + b0 + lane;
+      for (int j = 0; j < len; j++) {
+        const int32_t cc = __ldg(col + 32 * j);
+        if (cc != (int32_t)i) {
+          sum += (float)re[cc];
+          cnt++;
+        }
       }
     }
-  }
-  const double pr = (double)pre[i];
-  const double jr = pr * (double)re[i];
-  const double jm = cnt ? pr * sum / cnt : jr;
-  const double d3 = a - 3.0 * b1 + 3.0 * c - dd, d2 = a - 2.0 * b1 + c, d1 = a - b1;
-  const double sg = sqrt(0.5 * (d3 * d3 + jr * jr));
-  const bool ok = real && sg > 0.0 && isfinite(sg) && d.step[s] >= 4;
-  const double inv = ok ? 1.0 / sg : 0.0;
-  float f[6] = {(float)(d3 * inv), (float)asinh(d2 * inv), (float)asinh(d1 * inv), (float)asinh(a * inv),
-                (float)(jr * inv), (float)(jm * inv)};
-  double guess = e;
-  if (d.mlp_on) {
-    const MlpSmem w = mlp_view(img);
-    float yv = 0.0f;
-#pragma unroll
-    for (int qt = 0; qt < 2; qt++) {
-      uint32_t a1[4], a2[4][4], a3[4][4];
-      float z1[8][4], z2[8][4], y[4];
-      mlp_input_fragment(a1, f, 16 * qt, lane);
-      mlp_forward(w, a1, z1, z2, a2, a3, y, lane);
-      const float v = mlp_output_to_rows(y, lane);
-      if ((lane >> 4) == qt) yv = v;
+    // differences of the history in the state's precision (they cancel),
+    // everything after in FP32
+    const float pr = (float)pre[i];
+    const float jr = pr * (float)re[i];
+    const float jm = cnt ? pr * sum / (float)cnt : jr;
+    const float d3 = (float)(a - 3.0 * b1 + 3.0 * c - dd), d2 = (float)(a - 2.0 * b1 + c), d1 = (float)(a - b1);
+    const float sg = sqrtf(0.5f * (d3 * d3 + jr * jr));
+    const bool ok = real && sg > 0.0f && isfinite(sg) && d.step[s] >= 4;
+    const float inv = ok ? 1.0f / sg : 0.0f;
+    float f[6] = {d3 * inv, mlp_asinh(d2 * inv), mlp_asinh(d1 * inv), mlp_asinh((float)a * inv), jr * inv, jm * inv};
+    // history shift, the extrapolated guess and the training sample first,
+    // so that none of it stays live across the network
+    if (real) {
+      h3[i] = (T)c;
+      h2[i] = (T)b1;
+      h1[i] = (T)a;
+      x[i] = (T)e;
+      if (d.nsamp && i >= d.samp_first && (i - d.samp_first) % d.samp_stride == 0) {
+        const int64_t k = (i - d.samp_first) / d.samp_stride;
+        if (k < d.nsamp) {
+          for (int q = 0; q < 6; q++) d.samp_in[6 * k + q] = f[q];
+          d.samp_e[k] = (float)e;
+          d.samp_s[k] = sg;
+          d.samp_row[k] = ok ? (int32_t)i : -1;
+        }
+      }
     }
-    if (ok) guess = e + sg * (double)yv;
-  }
-  if (!real) return;
-  h3[i] = (T)c;
-  h2[i] = (T)b1;
-  h1[i] = (T)a;
-  x[i] = (T)guess;
-  if (d.nsamp && i >= d.samp_first && (i - d.samp_first) % d.samp_stride == 0) {
-    const int64_t k = (i - d.samp_first) / d.samp_stride;
-    if (k < d.nsamp) {
-      for (int q = 0; q < 6; q++) d.samp_in[6 * k + q] = f[q];
-      d.samp_e[k] = (float)e;
-      d.samp_s[k] = (float)sg;
-      d.samp_row[k] = ok ? (int32_t)i : -1;
+    if (d.mlp_on) {
+      float yv = 0.0f;
+#pragma unroll 1
+      for (int qt = 0; qt < 2; qt++) {
+        uint32_t a1[4];
+        float y[4];
+        mlp_input_fragment(a1, f, 16 * qt, lane);
+        mlp_infer(w, a1, y, lane);
+        const float v = mlp_output_to_rows(y, lane);
+        if ((lane >> 4) == qt) yv = v;
+      }
+      if (ok) x[i] = (T)((double)x[i] + (double)sg * (double)yv);
     }
   }
 }
@@ -678,7 +684,9 @@ cudaError_t group_launch_step(const GroupDev& d, int cg_blocks, int cg_variant, 
   if (d.warm_start == 3) {
     grp_extrap<T><<<gblk(d.nrow), kGB, 0, st>>>(d);
     grp_resid_e<T><<<gblk(d.nrow), kGB, 0, st>>>(d);
-    grp_guess_mlp<T><<<gblk(d.nrow), kGB, 0, st>>>(d);
+    const int64_t slices = d.nrow >> 5, per_block = kGB / 32;
+    const int64_t want = (slices + per_block - 1) / per_block;
+    grp_guess_mlp<T><<<(unsigned)(want < d.guess_blocks ? (want > 0 ? want : 1) : d.guess_blocks), kGB, 0, st>>>(d);
   }
   if (ev) cudaEventRecord(ev[2], st);
   cudaLaunchConfig_t cfg = {};

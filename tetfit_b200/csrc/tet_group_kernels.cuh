@@ -76,6 +76,7 @@ struct GroupDev {
   // kept[stat_off + step] records 1 when the network's guess was kept
   void *xe = nullptr, *r_alt = nullptr, *z_alt = nullptr;
   int mlp_on = 0, dual = 0;
+  int guess_blocks = 1;           // grid of the learned-guess kernel (a few blocks per SM)
   int8_t* kept = nullptr;
   const unsigned char* mlp_img = nullptr;
   // training samples: rows i = samp_first + k * samp_stride, k < nsamp
