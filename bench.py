@@ -302,13 +302,14 @@ def cg_bytes_per_launch(infos, its, es, dual=False):
     entries of A (int32 column + value) and 11 row-vector accesses
     (p-update/SpMV phase: z, p_old, x read, x, p_new, q written; residual
     phase: r, q, pre read, r, z written), plus the initial residual (A once;
-    b, pre read, r, z written; twice with the learned warm start's dual
-    start) and the final x update (x, p read, x written)."""
+    b, pre read, r, z written; with the learned warm start's dual start also
+    the second guess's residual read and its z written) and the final x
+    update (x, p read, x written)."""
     total = 0.0
     for info, it in zip(infos, its):
         nnz, n = info["nnz_system"], info["n_free"]
         start = nnz * (4 + es) + 5 * es * n
-        total += it * (nnz * (4 + es) + 11 * es * n) + start * (2 if dual else 1) + 3 * es * n
+        total += it * (nnz * (4 + es) + 11 * es * n) + start + (3 * es * n if dual else 0) + 3 * es * n
     return total
 
 

@@ -72,27 +72,27 @@ __device__ __forceinline__ float mlp_dsilu(float z) {
   const float s = mlp_sigmoid(z);
   return s * (1.0f + z * (1.0f - s));
 }
-// silu of two values packed as the next layer's BF16 pair: both tanh(z / 2)
-// in one bf16x2 special-function op (the result is BF16 anyway)
+// silu of two values packed as the next layer's BF16 pair, in BF16x2
+// arithmetic: z is converted once, tanh(z / 2) is one bf16x2 special-function
+// op, silu = z (1 + tanh(z / 2)) / 2 two bf16x2 FMA-pipe ops (the result is
+// BF16 anyway)
 __device__ __forceinline__ uint32_t mlp_silu_pack(float z0, float z1) {
-  const uint32_t hz = mlp_pack(0.5f * z0, 0.5f * z1);
-  uint32_t th;
+  const uint32_t zz = mlp_pack(z0, z1);
+  const uint32_t half = 0x3f003f00u;  // (0.5, 0.5) in BF16
+  uint32_t hz, th, u, h;
+  asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(hz) : "r"(zz), "r"(half));
   asm("tanh.approx.bf16x2 %0, %1;" : "=r"(th) : "r"(hz));
-  const float t0 = __uint_as_float(th << 16), t1 = __uint_as_float(th & 0xffff0000u);
-  return mlp_pack(0.5f * z0 * (1.0f + t0), 0.5f * z1 * (1.0f + t1));
+  asm("fma.rn.bf16x2 %0, %1, %2, %2;" : "=r"(u) : "r"(th), "r"(half));
+  asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(h) : "r"(zz), "r"(u));
+  return h;
 }
 __device__ __forceinline__ float mlp_silu_bf16(float z) {
   const uint32_t p = mlp_silu_pack(z, 0.0f);
   return __uint_as_float(p << 16);
 }
 
-// asinh from its definition, sign(x) log(|x| + sqrt(x^2 + 1)); log(2|x|) for
-// large |x| where x^2 + 1 = x^2 in float
-__device__ __forceinline__ float mlp_asinh(float x) {
-  const float ax = fabsf(x);
-  const float r = ax > 1.0e4f ? __logf(2.0f * ax) : __logf(ax + sqrtf(ax * ax + 1.0f));
-  return copysignf(r, x);
-}
+// sign(x) log2(1 + |x|): compresses large inputs, linear near 0
+__device__ __forceinline__ float mlp_compress(float x) { return copysignf(__log2f(1.0f + fabsf(x)), x); }
 
 // Shared-memory view of the weight image
 struct MlpSmem {
@@ -238,6 +238,81 @@ __device__ __forceinline__ void mlp_infer(const MlpSmem& w, const uint32_t a1[4]
     uint32_t b[2];
     mlp_ldb(b, w.w3, kLd2, k3, 0, lane);
     mlp_mma(y, a3, b);
+  }
+}
+
+// mlp_infer for the two 16-row tiles of a warp at once: every weight
+// fragment read from shared memory feeds both tiles' MMAs.
+__device__ __forceinline__ void mlp_infer2(const MlpSmem& w, const uint32_t a1[2][4], float y[2][4], int lane) {
+  const int t = lane & 3;
+  uint32_t a2[2][4][4];
+#pragma unroll
+  for (int kt = 0; kt < 4; kt++) {
+    float c[2][2][4];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int nt = 2 * kt + h;
+      const float b0 = w.b1[nt * 8 + 2 * t], b1v = w.b1[nt * 8 + 2 * t + 1];
+      uint32_t b[2];
+      mlp_ldb(b, w.w1, kLd1, 0, nt, lane);
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+        c[q][h][0] = b0;
+        c[q][h][1] = b1v;
+        c[q][h][2] = b0;
+        c[q][h][3] = b1v;
+        mlp_mma(c[q][h], a1[q], b);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      a2[q][kt][0] = mlp_silu_pack(c[q][0][0], c[q][0][1]);
+      a2[q][kt][1] = mlp_silu_pack(c[q][0][2], c[q][0][3]);
+      a2[q][kt][2] = mlp_silu_pack(c[q][1][0], c[q][1][1]);
+      a2[q][kt][3] = mlp_silu_pack(c[q][1][2], c[q][1][3]);
+    }
+  }
+  const float bo = t == 0 ? w.b3[0] : 0.0f;
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    y[q][0] = bo;
+    y[q][1] = 0.0f;
+    y[q][2] = bo;
+    y[q][3] = 0.0f;
+  }
+#pragma unroll
+  for (int k3 = 0; k3 < 4; k3++) {
+    float o[2][2][4];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int nt = 2 * k3 + h;
+      const float b0 = w.b2[nt * 8 + 2 * t], b1v = w.b2[nt * 8 + 2 * t + 1];
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+        o[q][h][0] = b0;
+        o[q][h][1] = b1v;
+        o[q][h][2] = b0;
+        o[q][h][3] = b1v;
+      }
+#pragma unroll
+      for (int kt = 0; kt < 4; kt++) {
+        uint32_t b[2];
+        mlp_ldb(b, w.w2t, kLd2, kt, nt, lane);
+        mlp_mma(o[0][h], a2[0][kt], b);
+        mlp_mma(o[1][h], a2[1][kt], b);
+      }
+    }
+    uint32_t b[2];
+    mlp_ldb(b, w.w3, kLd2, k3, 0, lane);
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      uint32_t a3[4];
+      a3[0] = mlp_silu_pack(o[q][0][0], o[q][0][1]);
+      a3[1] = mlp_silu_pack(o[q][0][2], o[q][0][3]);
+      a3[2] = mlp_silu_pack(o[q][1][0], o[q][1][1]);
+      a3[3] = mlp_silu_pack(o[q][1][2], o[q][1][3]);
+      mlp_mma(y[q], a3, b);
+    }
   }
 }
 

@@ -51,7 +51,7 @@ class TetGroup {
   bool mlp_params(float* out) const;
   void get_flux(int s, double* flux, size_t cap, size_t* n) const;
   uint64_t device_bytes() const { return dev_bytes_; }
-  int kernels_per_step() const { return 7 + (dev_.np ? 1 : 0) + (opt_.warm_start == 3 ? 3 : 0); }
+  int kernels_per_step() const { return 7 + (dev_.np ? 1 : 0) + (opt_.warm_start == 3 ? 2 : 0); }
   int cg_blocks() const { return cg_blocks_; }
   int cg_variant() const { return cg_variant_; }
   uint64_t total_dofs() const { return dofs_; }

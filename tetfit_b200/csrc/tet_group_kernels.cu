@@ -234,34 +234,27 @@ __global__ void __launch_bounds__(kGB) grp_rhs(GroupDev d) {
     h1[i] = a;
     if (step >= 3) x[i] = (T)3 * a - (T)3 * b + c;
     else if (step >= 2) x[i] = (T)2 * a - b;
+  } else if (d.warm_start == 3) {
+    // the learned warm start's base guess, the same extrapolation, to xe
+    const T a = x[i], b = ((const T*)d.xh1)[i], c = ((const T*)d.xh2)[i];
+    const int step = d.step[s];
+    ((T*)d.xe)[i] = step >= 3 ? (T)3 * a - (T)3 * b + c : (step >= 2 ? (T)2 * a - b : a);
   }
 }
 
-// Learned warm start (warm_start 3), three kernels after grp_rhs.
-//   grp_extrap   e = quadratic extrapolation of the last three solutions -> xe
+// Learned warm start (warm_start 3): grp_rhs puts the quadratic
+// extrapolation e of the last three solutions in xe, then
 //   grp_resid_e  r_e = b - A e -> r_alt, the right-hand side of the
 //                correction system A (x_n - e) = r_e
 //   grp_guess_mlp  per free row the network reads the last four solutions as
 //                the third difference D3 = x - 3 xh1 + 3 xh2 - xh3 and the
-//                compressed D2, D1 and level (asinh), and the Jacobi-scaled
+//                compressed D2, D1 and level (sign log2(1 + |.|)), the Jacobi-scaled
 //                correction right-hand side pre r_e with its mean over the
 //                row's neighbours (A's pattern), all divided by the row scale
 //                sigma = rms(D3, pre r_e); its output y gives the guess
 //                e + sigma y in x.  Until the network is trained (mlp_on 0)
 //                x = e.  Sampled rows store their inputs, e and sigma for
 //                training.  A warp takes the 32 rows of one slice.
-template <typename T>
-__global__ void __launch_bounds__(kGB) grp_extrap(GroupDev d) {
-  const int64_t i = (int64_t)blockIdx.x * kGB + threadIdx.x;
-  if (i >= d.nrow) return;
-  const int s = d.slice_sim[i >> 5];
-  if (!running(d, s) || d.free_edge[i] < 0) return;
-  const T* x = (const T*)d.x;
-  const T a = x[i], b = ((const T*)d.xh1)[i], c = ((const T*)d.xh2)[i];
-  const int step = d.step[s];
-  ((T*)d.xe)[i] = step >= 3 ? (T)3 * a - (T)3 * b + c : (step >= 2 ? (T)2 * a - b : a);
-}
-
 template <typename T>
 __global__ void __launch_bounds__(kGB) grp_resid_e(GroupDev d) {
   const int64_t i = (int64_t)blockIdx.x * kGB + threadIdx.x;
@@ -320,7 +313,7 @@ __global__ void __launch_bounds__(kGB, 3) grp_guess_mlp(GroupDev d) {
     const float sg = sqrtf(0.5f * (d3 * d3 + jr * jr));
     const bool ok = real && sg > 0.0f && isfinite(sg) && d.step[s] >= 4;
     const float inv = ok ? 1.0f / sg : 0.0f;
-    float f[6] = {d3 * inv, mlp_asinh(d2 * inv), mlp_asinh(d1 * inv), mlp_asinh((float)a * inv), jr * inv, jm * inv};
+    float f[6] = {d3 * inv, mlp_compress(d2 * inv), mlp_compress(d1 * inv), mlp_compress((float)a * inv), jr * inv, jm * inv};
     // history shift, the extrapolated guess and the training sample first,
     // so that none of it stays live across the network
     if (real) {
@@ -339,16 +332,13 @@ __global__ void __launch_bounds__(kGB, 3) grp_guess_mlp(GroupDev d) {
       }
     }
     if (d.mlp_on) {
-      float yv = 0.0f;
-#pragma unroll 1
-      for (int qt = 0; qt < 2; qt++) {
-        uint32_t a1[4];
-        float y[4];
-        mlp_input_fragment(a1, f, 16 * qt, lane);
-        mlp_infer(w, a1, y, lane);
-        const float v = mlp_output_to_rows(y, lane);
-        if ((lane >> 4) == qt) yv = v;
-      }
+      uint32_t a1[2][4];
+      float y[2][4];
+      mlp_input_fragment(a1[0], f, 0, lane);
+      mlp_input_fragment(a1[1], f, 16, lane);
+      mlp_infer2(w, a1, y, lane);
+      const float v0 = mlp_output_to_rows(y[0], lane), v1 = mlp_output_to_rows(y[1], lane);
+      const float yv = lane < 16 ? v0 : v1;
       if (ok) x[i] = (T)((double)x[i] + (double)sg * (double)yv);
     }
   }
@@ -462,8 +452,7 @@ __global__ void __launch_bounds__(kCgThreads, 2) grp_cg(GroupDev d) {
   };
 
   // r = b - A x; rr = r.r, rz = r.(pre r), bb = b.b; in the dual start the
-  // same for the second guess xe (r_alt, z_alt)
-  T* xe = (T*)d.xe;
+  // same for the second guess xe (its residual r_alt is already formed)
   T* ra = (T*)d.r_alt;
   T* za = (T*)d.z_alt;
   const bool dual = d.dual != 0;
@@ -482,8 +471,8 @@ __global__ void __launch_bounds__(kCgThreads, 2) grp_cg(GroupDev d) {
         a1 += rd * (double)zi;
         a2 += (double)b[i] * (double)b[i];
         if (dual) {
-          const T r2 = b[i] - sell_dot<T>(d.A, i, [&](int32_t c) { return xe[c]; });
-          ra[i] = r2;
+          // r_alt = b - A xe was formed by grp_resid_e from the same b and xe
+          const T r2 = ra[i];
           const T z2 = mulT(pre[i], r2);
           za[i] = z2;
           a3 += (double)r2 * (double)r2;
@@ -682,7 +671,6 @@ cudaError_t group_launch_step(const GroupDev& d, int cg_blocks, int cg_variant, 
   grp_sources<T><<<d.S, kGB, 0, st>>>(d);
   grp_rhs<T><<<gblk(d.nrow), kGB, 0, st>>>(d);
   if (d.warm_start == 3) {
-    grp_extrap<T><<<gblk(d.nrow), kGB, 0, st>>>(d);
     grp_resid_e<T><<<gblk(d.nrow), kGB, 0, st>>>(d);
     const int64_t slices = d.nrow >> 5, per_block = kGB / 32;
     const int64_t want = (slices + per_block - 1) / per_block;
