@@ -58,7 +58,29 @@ WORKLOADS = {
     # reference's previous-solution guess
     "batch128": dict(kind="batch", members=128, n_lo=8, n_hi=48, steps=1000, seed=31337, prec="fp32",
                      warm="learned", learn_steps=300, crit="rhs", plain_steps=10),
+    # the same scene at profiling size: 16 members n ~ U{8..32} (1.5 M CG rows, state > L2)
+    "batch16": dict(kind="batch", members=16, n_lo=8, n_hi=32, steps=1000, seed=31337, prec="fp32",
+                    warm="learned", learn_steps=40, crit="rhs", plain_steps=5),
+    # learned warm start at SURVEY cfg4 size: 96^3 Kuhn box, GRF eps_r, one member
+    "learned96": dict(kind="batch", members=1, n_lo=96, n_hi=96, steps=5000, seed=4242, prec="fp32",
+                      warm="learned", learn_steps=500, crit="rhs", plain_steps=5, grf=True),
 }
+
+
+def max_over_ranks(values, dist=None, device="cpu"):
+    """Element-wise maximum of per-rank timings over all ranks (the job's time
+    is its slowest rank's); identity without a process group."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t]
+
+
+def replica_seed(base: int, rank: int) -> int:
+    """Each rank of a multi-GPU run advances its own independent replica."""
+    return base + rank
 
 
 def hbm_peak():
@@ -256,13 +278,7 @@ def run_ours(args, rank, world, local_rank):
     e2e_s = time.perf_counter() - t0
     barrier()
     dofs = info["n_edges"] + info["n_faces"]
-    max_ms = dev_ms
-    max_e2e = e2e_s
-    if dist:
-        import torch
-        t = torch.tensor([dev_ms, e2e_s], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        max_ms, max_e2e = float(t[0]), float(t[1])
+    max_ms, max_e2e = max_over_ranks([dev_ms, e2e_s], dist, f"cuda:{local_rank}")
     kps = info["kernels_per_step"]
     result = None
     if rank == 0:
@@ -342,7 +358,13 @@ def run_batch(args, rank, world, local_rank):
             dist.barrier()
 
     # every rank runs its own batch of members (independent replicas)
-    cases = batch_cases(w["members"], w["n_lo"], w["n_hi"], steps=w["steps"], seed=w["seed"] + rank)
+    if w.get("grf"):
+        from tetfit_b200.cases import TetCase, grf_materials
+        mat, table, _ = grf_materials(seed=w["seed"])
+        cases = [TetCase(n=w["n_lo"], method="gfdtd", steps=w["steps"], mat_field=mat, eps=table,
+                         seed=replica_seed(0x7E7F17, rank))]
+    else:
+        cases = batch_cases(w["members"], w["n_lo"], w["n_hi"], steps=w["steps"], seed=replica_seed(w["seed"], rank))
     work = tempfile.mkdtemp(prefix=f"tfbatch{rank}_")
     t0 = time.time()
     members = write_batch(work, cases)
@@ -412,6 +434,15 @@ def run_batch(args, rank, world, local_rank):
             perr.append(float(np.linalg.norm(v_ - vo) / max(np.linalg.norm(vo), 1e-300)))
     kps = infos[0]["kernels_per_step"]
     b.close()
+    # CG iterations per step of the other warm starts over the same window
+    compare = None
+    if args.compare_warm:
+        compare = {"window": [W + nph, W + nph + K], "learned": it_timed}
+        for ws in ("zero", "previous", "extrapolate"):
+            c = tb.Batch(members, precision=w["prec"], cg_criterion=w["crit"], warm_start=ws, device=local_rank)
+            c.step(W + nph + K)
+            compare[ws] = float(np.mean([c.solver_stats(m)[0][W + nph:W + nph + K].mean() for m in range(c.size)]))
+            c.close()
     # plain arm: the same members one at a time in FP64, previous-solution guess
     t0 = time.time()
     p = tb.Batch(members, precision="fp64", batch_mode="serial", cg_criterion=w["crit"], warm_start="previous",
@@ -425,12 +456,7 @@ def run_batch(args, rank, world, local_rank):
     barrier()
     plain_it = float(np.mean([p.solver_stats(m)[0][3:3 + Kp].mean() for m in range(p.size)]))
     p.close()
-    max_ms, max_e2e, max_plain = dev_ms, e2e_s, plain_ms
-    if dist:
-        import torch
-        t = torch.tensor([dev_ms, e2e_s, plain_ms], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        max_ms, max_e2e, max_plain = (float(x) for x in t)
+    max_ms, max_e2e, max_plain = max_over_ranks([dev_ms, e2e_s, plain_ms], dist, f"cuda:{local_rank}")
     result = None
     if rank == 0:
         peak, peak_kind = hbm_peak()
@@ -438,16 +464,20 @@ def run_batch(args, rank, world, local_rank):
         value = world * dofs * K / (max_ms * 1e-3)
         plain_value = world * dofs * Kp / (max_plain * 1e-3)
         ns = sorted(c.n for c in cases)
+        if w.get("grf"):
+            scene = (f"{args.workload}: gfdtd on a {w['n_lo']}^3 x 6 jittered Kuhn box, eps_r from a seeded "
+                     f"Gaussian random field (corr. 0.1 m) mapped to [1,12] in 24 levels, PEC box, H-wave source")
+        else:
+            scene = (f"{args.workload}: {w['members']} gfdtd members in one group, Kuhn meshes "
+                     f"n ~ U{{{w['n_lo']}..{w['n_hi']}}} (min {ns[0]}, median {ns[len(ns) // 2]}, max {ns[-1]}) "
+                     f"x 6 tets, eps_r ~ U[1,4] per x-half, f ~ U[1e8,4e8] Hz")
+        desc = (scene + f", {w['prec']} fields, FP64 CG reductions, CG tol 1e-8 (||r|| <= tol ||b||), "
+                f"{w['warm']} warm start" + (f" (network trained on the first {learn} steps, untimed)" if learn else ""))
         result = {
             "metric": "dof-steps/s", "value": value, "unit": "dof-steps/s", "n_gpus": world, "steps": K,
             "warmup": args.warmup, "ms_per_step": max_ms / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if es == 4 else "f64", "data": "synthetic",
-            "config": {"workload": f"{args.workload}: {w['members']} gfdtd members in one group, Kuhn meshes "
-                                   f"n ~ U{{{w['n_lo']}..{w['n_hi']}}} (min {ns[0]}, median {ns[len(ns) // 2]}, "
-                                   f"max {ns[-1]}) x 6 tets, eps_r ~ U[1,4] per x-half, f ~ U[1e8,4e8] Hz, "
-                                   f"{w['prec']} fields, FP64 CG reductions, CG tol 1e-8 (||r|| <= tol ||b||), "
-                                   f"{w['warm']} warm start" + (f" (network trained on the first {learn} steps, "
-                                                                f"untimed)" if learn else ""),
+            "config": {"workload": desc,
                        "members": w["members"], "dofs": dofs, "parallelism": f"replicas x{world}",
                        "l2": f"CG working set {cg_bytes / max(it_timed, 1) / 1e6:.0f} MB per iteration > 126 MB L2 "
                              f"(no flush needed)",
@@ -465,6 +495,7 @@ def run_batch(args, rank, world, local_rank):
                            "speedup": value / plain_value},
             "probe_error_vs_fp64_oracle": {"members": len(perr), "max_rel_l2": max(perr) if perr else None},
             "learned_warm_start": learned_info,
+            "cg_iterations_by_warm_start": compare,
             "e2e": {"value": world * dofs * K2 / max_e2e, "unit": "dof-steps/s",
                     "h2d_bytes_per_step": 8 * n_src, "d2h_bytes_per_step": 8 * n_probe_vals,
                     "api": "tf_batch_step_io"},
@@ -645,6 +676,9 @@ def main():
     ap.add_argument("--workload", default="batch128", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--compare-warm", action="store_true",
+                    help="batch workloads: also run the zero, previous and extrapolation warm starts and report "
+                         "their CG iterations per step over the timed window")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))
