@@ -205,10 +205,18 @@ def roofline_kernel(d, info, es, ms5, nph):
     """(kernel name, algorithmic bytes per launch, launch ms, extra config)."""
     if info["method"] == "fdtd":
         e_bytes, h_bytes = fit_bytes(info, es)
+        # the per-dof coefficient variant streams M_h, M_q (E) and M_nu, M_mu (H)
+        ev, hv = info.get("cg_variant", 0) % 4, info.get("cg_variant", 0) // 4
+        if ev == 3:
+            e_bytes += 2 * es * info["n_edges"] - info["n_cells"]
+        if hv == 3:
+            h_bytes += 2 * es * info["n_faces"] - info["n_cells"]
         e_ms, h_ms = ms5[1] / nph, ms5[4] / nph
+        names = {0: "fit_{}_kernel", 1: "fit_{}_march", 2: "fit_{}_march", 3: "fit_{}_coef"}
+        extra = {"e_variant": ev, "h_variant": hv}
         if e_ms >= h_ms:
-            return "fit_e_kernel", e_bytes, e_ms, {}
-        return "fit_h_kernel", h_bytes, h_ms, {}
+            return names[ev].format("e"), e_bytes, e_ms, extra
+        return names[hv].format("h"), h_bytes, h_ms, extra
     if info["method"] == "dga":
         # tet_curl_f + tet_h_update: C^T F gather and the H SpMV
         # bytes: C^T F gather (int32 per entry, F once, cb, I, cf written),

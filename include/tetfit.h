@@ -59,7 +59,10 @@ typedef struct tf_opts {
   int32_t host_threads; /* tf_batch_open: host threads building members, 0 all  */
   int32_t learn_steps;  /* warm_start 3: steps whose solutions train the network
                            (0: 500); the extrapolation is used meanwhile         */
-  int32_t reserved[4];
+  int32_t fit_variant;  /* fdtd: 0 automatic (first steps time the variants on grids
+                           of 2 M cells or more), k > 0 forces variant k - 1 for
+                           both halves (all give bitwise identical results)     */
+  int32_t reserved[3];
 } tf_opts;
 
 typedef struct tf_info {
@@ -77,7 +80,10 @@ typedef struct tf_info {
   uint64_t n_free, nnz_system;         /* gfdtd: CG unknowns and nonzeros of A    */
   uint64_t nnz_operators;              /* nonzeros of H (dga) or of E (gfdtd)     */
   uint32_t cg_blocks;                  /* gfdtd: blocks of the persistent CG kernel */
-  int32_t cg_variant;                  /* gfdtd: CG variant the autotuner picked   */
+  int32_t cg_variant;                  /* gfdtd: CG variant the autotuner picked;
+                                          fdtd: E variant + 4 x H variant (0 one
+                                          thread per node, 1/2 z-march over 4/16
+                                          planes, 3 per-dof coefficient arrays) */
   uint64_t reserved[3];
 } tf_info;
 

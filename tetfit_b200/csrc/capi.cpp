@@ -167,6 +167,8 @@ int tf_prepare(tf_ctx* c, uint32_t label, const tf_opts* opts) {
     ro.cg_criterion = c->opts.cg_criterion;
     if (c->opts.cg_maxiter > 0) ro.cg_maxiter = c->opts.cg_maxiter;
     if (c->opts.learn_steps > 0) ro.learn_steps = c->opts.learn_steps;
+    ro.fit_variant = c->opts.fit_variant;
+    if (ro.fit_variant < 0 || ro.fit_variant > 4) return fail(c, TF_E_ARG, "fit_variant must be 0..4");
     if (meth == "fdtd") {
       c->fit.reset(new tf::FitSim(c->sc, label, ro));
     } else if (meth == "dga" || meth == "gfdtd") {
@@ -203,6 +205,7 @@ int tf_get_info(tf_ctx* c, tf_info* info) {
   info->n_free = f.n_free();
   info->nnz_system = f.nnz_system();
   info->nnz_operators = f.nnz_operators();
+  info->cg_variant = f.kernel_variant();
   return TF_OK;
 }
 

@@ -101,6 +101,7 @@ FitSim::FitSim(Script& sc, uint32_t label, const RunOptions& opt) : sc_(sc), opt
   }
   alloc_device();
   upload();
+  build_coefficients();
 }
 
 FitSim::~FitSim() {
@@ -750,6 +751,12 @@ void FitSim::fill_grid(FitGrid<T>& g, SpecialEdges<T>& s) {
   g.P = dP_; g.S = dS_; g.R = dR_; g.X = dX_;
   g.mh_pure = (const T*)dmh_; g.mq_pure = (const T*)dmq_; g.mnu_pure = (const T*)dmnu_; g.mmu_pure = (const T*)dmmu_;
   g.live = dlive_;
+  for (int a = 0; a < 3; a++) {
+    g.Ch[a] = (T*)dC_[a];
+    g.Cq[a] = (T*)dC_[3 + a];
+    g.Cn[a] = (T*)dC_[6 + a];
+    g.Cm[a] = (T*)dC_[9 + a];
+  }
   for (int a = 0; a < 3; a++) g.len[a] = L_[a];
   g.area[0] = L_[1] * L_[2]; g.area[1] = L_[0] * L_[2]; g.area[2] = L_[0] * L_[1];
   s.n = (int)special_.size();
@@ -792,6 +799,12 @@ void FitSim::alloc_device() {
   dmh_ = dalloc(nm3 * es); dmq_ = dalloc(nm3 * es); dmnu_ = dalloc(nm3 * es); dmmu_ = dalloc(nm3 * es);
   dlive_ = (uint8_t*)dalloc(mat_label_.size());
   dstep_ = (int*)dalloc(sizeof(int));
+  if (opt_.fit_variant == 4 || (opt_.fit_variant == 0 && n_cells() >= 2000000))
+    // the per-dof coefficient variant is forced or among the autotuner's candidates
+    for (int q = 0; q < 12; q++) {
+      dC_[q] = dalloc(nslot_ * es);
+      CU(cudaMemsetAsync(dC_[q], 0, nslot_ * es, stream_));
+    }
   dflux_ = (double*)dalloc(nsteps_ * 8);
   const size_t ns = special_.size();
   nflux_part_ = (int)((ns + 255) / 256);
@@ -1015,6 +1028,22 @@ void FitSim::upload() {
   CU(cudaStreamSynchronize(stream_));
 }
 
+// Per-dof coefficients for the coefficient-array kernel variant, from the
+// same tables and functions as the table-driven kernels (bit-identical).
+void FitSim::build_coefficients() {
+  if (!dC_[0]) return;
+  if (opt_.precision == 1) {
+    FitGrid<float> g; SpecialEdges<float> s;
+    fill_grid(g, s);
+    CU(fit_build_coefficients<float>(g, stream_));
+  } else {
+    FitGrid<double> g; SpecialEdges<double> s;
+    fill_grid(g, s);
+    CU(fit_build_coefficients<double>(g, stream_));
+  }
+  CU(cudaStreamSynchronize(stream_));
+}
+
 void FitSim::launch_steps(int n, cudaEvent_t* ev) {
   ProbeSet pr;
   pr.n = (int)probe_cell_.size();
@@ -1035,8 +1064,13 @@ void FitSim::launch_steps(int n, cudaEvent_t* ev) {
 // cycle through the E and H kernel variants (bit-identical results), timing
 // each with events, and keep the fastest of each for the rest of the run.
 void FitSim::autotune(uint64_t& n) {
+  if (opt_.fit_variant > 0) {
+    e_var_ = h_var_ = opt_.fit_variant - 1;
+    tuned_ = true;
+    return;
+  }
   if (tuned_ || n_cells() < 2000000) { tuned_ = true; return; }
-  const int kVariants = 3, kReps = 2;
+  const int kVariants = dC_[0] ? 4 : 3, kReps = 2;
   cudaEvent_t ev[6];
   for (auto& e : ev) CU(cudaEventCreate(&e));
   while (tune_pos_ < kVariants * kReps && n > 0) {

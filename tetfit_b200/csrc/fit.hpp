@@ -143,7 +143,14 @@ class FitSim : public Sim {
   int e_var_ = 2, h_var_ = 2; // kernel variants (see fit_launch_step)
   bool tuned_ = false;
   int tune_pos_ = 0;
-  double tune_e_[3] = {0, 0, 0}, tune_h_[3] = {0, 0, 0};
+  double tune_e_[4] = {0, 0, 0, 0}, tune_h_[4] = {0, 0, 0, 0};
+  void* dC_[12] = {};  // per-dof coefficients M_h, M_q, M_nu, M_mu x 3 axes (autotuned grids)
+  void build_coefficients();
+
+ public:
+  int kernel_variant() const override { return e_var_ + 4 * h_var_; }
+
+ private:
   // graphs
   cudaGraphExec_t graph_ = nullptr;
   int graph_len_ = 0;

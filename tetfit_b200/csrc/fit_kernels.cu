@@ -543,9 +543,150 @@ __global__ void fit_probe_kernel(FitGrid<T> g, ProbeSet pr, const int* step_coun
   }
 }
 
+// ---------------------------------------------------- per-dof coefficients
+// M_h, M_q of the interior stencil edges leaving node slot (i,j,k) and M_nu,
+// M_mu of the faces at that slot, with the same functions (and so the same
+// rounded values) the table-driven kernels use.
+template <typename T>
+__global__ void __launch_bounds__(256) fit_coef_kernel(FitGrid<T> g) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i > g.Nx || j > g.Ny) return;
+  const int64_t s = (int64_t)i + g.sx * j + g.sxy * k;
+  const bool xin = i > 0 && i < g.Nx, yin = j > 0 && j < g.Ny, zin = k > 0 && k < g.Nz;
+  uint8_t c[2][2][2];
+#pragma unroll
+  for (int dz = 0; dz < 2; dz++)
+#pragma unroll
+    for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+      for (int dx = 0; dx < 2; dx++) {
+        int ci = i - 1 + dx, cj = j - 1 + dy, ck = k - 1 + dz;
+        bool ok = ci >= 0 && ci < g.Nx && cj >= 0 && cj < g.Ny && ck >= 0 && ck < g.Nz;
+        c[dz][dy][dx] = ok ? g.mat[cell_index(ci, cj, ck, g.Nx, g.Ny)] : 0;
+      }
+  T mh = 0, mq = 0;
+  if (i < g.Nx && yin && zin) {
+    uint8_t m[4] = {c[0][0][1], c[0][1][1], c[1][0][1], c[1][1][1]};
+    edge_coef_t(g, 0, m, mh, mq);
+    g.Ch[0][s] = mh;
+    g.Cq[0][s] = mq;
+  }
+  if (j < g.Ny && xin && zin) {
+    uint8_t m[4] = {c[0][1][0], c[0][1][1], c[1][1][0], c[1][1][1]};
+    edge_coef_t(g, 1, m, mh, mq);
+    g.Ch[1][s] = mh;
+    g.Cq[1][s] = mq;
+  }
+  if (k < g.Nz && xin && yin) {
+    uint8_t m[4] = {c[1][0][0], c[1][0][1], c[1][1][0], c[1][1][1]};
+    edge_coef_t(g, 2, m, mh, mq);
+    g.Ch[2][s] = mh;
+    g.Cq[2][s] = mq;
+  }
+  const bool ci = i < g.Nx, cj = j < g.Ny, ck = k < g.Nz;
+  const uint8_t m0 = (ci && cj && ck) ? c[1][1][1] : 0;
+  T mnu, mmu;
+  if (cj && ck) {
+    const uint8_t ml = i > 0 ? c[1][1][0] : 0;
+    const bool live = face_coef_t(g, 0, i > 0, ci, ml, m0, mnu, mmu);
+    g.Cn[0][s] = live ? mnu : (T)-0.0;
+    g.Cm[0][s] = live ? mmu : (T)0;
+  }
+  if (ci && ck) {
+    const uint8_t ml = j > 0 ? c[1][0][1] : 0;
+    const bool live = face_coef_t(g, 1, j > 0, cj, ml, m0, mnu, mmu);
+    g.Cn[1][s] = live ? mnu : (T)-0.0;
+    g.Cm[1][s] = live ? mmu : (T)0;
+  }
+  if (ci && cj) {
+    const uint8_t ml = k > 0 ? c[0][1][1] : 0;
+    const bool live = face_coef_t(g, 2, k > 0, ck, ml, m0, mnu, mmu);
+    g.Cn[2][s] = live ? mnu : (T)-0.0;
+    g.Cm[2][s] = live ? mmu : (T)0;
+  }
+}
+
+template <typename T>
+cudaError_t fit_build_coefficients(const FitGrid<T>& g, cudaStream_t st) {
+  dim3 blk(32, 8, 1);
+  dim3 grd((unsigned)((g.Nx + 1 + 31) / 32), (unsigned)((g.Ny + 1 + 7) / 8), (unsigned)(g.Nz + 1));
+  fit_coef_kernel<T><<<grd, blk, 0, st>>>(g);
+  return cudaGetLastError();
+}
+template cudaError_t fit_build_coefficients<double>(const FitGrid<double>&, cudaStream_t);
+template cudaError_t fit_build_coefficients<float>(const FitGrid<float>&, cudaStream_t);
+
+// Interior E update from the per-dof coefficients (same arithmetic as
+// fit_e_kernel, coefficients streamed instead of rebuilt).
+template <typename T>
+__global__ void __launch_bounds__(256) fit_e_coef(FitGrid<T> g) {
+  using A = Ar<T>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i > g.Nx || j > g.Ny) return;
+  const int64_t s = (int64_t)i + g.sx * j + g.sxy * k;
+  const T dt = (T)g.dt;
+  const bool xin = i > 0 && i < g.Nx, yin = j > 0 && j < g.Ny, zin = k > 0 && k < g.Nz;
+  if (i < g.Nx && yin && zin) {
+    const T mh = __ldg(g.Ch[0] + s), mq = __ldg(g.Cq[0] + s);
+    T cf = A::sub(A::add(A::sub(g.Fy[s - g.sxy], g.Fz[s - g.sx]), g.Fz[s]), g.Fy[s]);
+    g.Ux[s] = A::mul(mh, A::add(A::mul(mq, g.Ux[s]), A::mul(dt, cf)));
+  }
+  if (j < g.Ny && xin && zin) {
+    const T mh = __ldg(g.Ch[1] + s), mq = __ldg(g.Cq[1] + s);
+    T cf = -A::sub(A::add(A::sub(g.Fx[s - g.sxy], g.Fz[s - 1]), g.Fz[s]), g.Fx[s]);
+    g.Uy[s] = A::mul(mh, A::add(A::mul(mq, g.Uy[s]), A::mul(dt, cf)));
+  }
+  if (k < g.Nz && xin && yin) {
+    const T mh = __ldg(g.Ch[2] + s), mq = __ldg(g.Cq[2] + s);
+    T cf = A::sub(A::add(A::sub(g.Fx[s - g.sx], g.Fy[s - 1]), g.Fy[s]), g.Fx[s]);
+    g.Uz[s] = A::mul(mh, A::add(A::mul(mq, g.Uz[s]), A::mul(dt, cf)));
+  }
+}
+
+// H update from the per-dof coefficients (same arithmetic as fit_h_kernel).
+template <typename T>
+__global__ void __launch_bounds__(256) fit_h_coef(FitGrid<T> g, int* step_counter) {
+  using A = Ar<T>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (step_counter && i == 0 && j == 0 && k == 0) atomicAdd(step_counter, 1);
+  if (i > g.Nx || j > g.Ny) return;
+  const int64_t s = (int64_t)i + g.sx * j + g.sxy * k;
+  const T dt = (T)g.dt;
+  const bool ci = i < g.Nx, cj = j < g.Ny, ck = k < g.Nz;
+  auto skip = [](T v) { return v == (T)0 && signbit(v); };
+  if (cj && ck) {
+    const T mnu = __ldg(g.Cn[0] + s);
+    if (!skip(mnu)) {
+      const T B = face_flux(__ldg(g.Cm[0] + s), g.Fx[s], dt, curl_x(g, s));
+      g.Fx[s] = A::mul(mnu, B);
+    }
+  }
+  if (ci && ck) {
+    const T mnu = __ldg(g.Cn[1] + s);
+    if (!skip(mnu)) {
+      const T B = face_flux(__ldg(g.Cm[1] + s), g.Fy[s], -dt, curl_y(g, s));
+      g.Fy[s] = A::mul(mnu, B);
+    }
+  }
+  if (ci && cj) {
+    const T mnu = __ldg(g.Cn[2] + s);
+    if (!skip(mnu)) {
+      const T B = face_flux(__ldg(g.Cm[2] + s), g.Fz[s], dt, curl_z(g, s));
+      g.Fz[s] = A::mul(mnu, B);
+    }
+  }
+}
+
 // ---------------------------------------------------------------- launchers
 // Kernel variants for the E and H halves (all compute bit-identical results):
-// 0 one thread per node slot, 1 z-march over 4 planes, 2 z-march over 16.
+// 0 one thread per node slot, 1 z-march over 4 planes, 2 z-march over 16,
+// 3 one thread per node slot with per-dof coefficient arrays.
 template <typename T>
 void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const ProbeSet& pr, int* step_counter,
                      double* flux, cudaStream_t st, cudaEvent_t* ev, int e_variant, int h_variant) {
@@ -560,6 +701,7 @@ void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const Probe
   if (sp.n > 0) fit_special_pre<T><<<nsb, 256, 0, st>>>(g, sp, step_counter);
   if (ev) cudaEventRecord(ev[1], st);
   if (e_variant == 0) fit_e_kernel<T><<<grd, blk, 0, st>>>(g);
+  else if (e_variant == 3) fit_e_coef<T><<<grd, blk, 0, st>>>(g);
   else {
     const int kc = e_variant == 1 ? 4 : 16;
     fit_e_march<T><<<mgrid(kc), blk, 0, st>>>(g, kc);
@@ -570,6 +712,7 @@ void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const Probe
   if (pr.n > 0) fit_probe_kernel<T><<<(pr.n + 127) / 128, 128, 0, st>>>(g, pr, step_counter);
   if (ev) cudaEventRecord(ev[4], st);
   if (h_variant == 0) fit_h_kernel<T><<<grd, blk, 0, st>>>(g, step_counter);
+  else if (h_variant == 3) fit_h_coef<T><<<grd, blk, 0, st>>>(g, step_counter);
   else {
     const int kc = h_variant == 1 ? 4 : 16;
     fit_h_march<T><<<mgrid(kc), blk, 0, st>>>(g, kc, step_counter);

@@ -15,6 +15,8 @@
 // as the reference's averaging (Discretization.hpp:5234-5330, 5485-5609), so
 // they are bit-identical to precomputed per-dof values.
 #pragma once
+#include <cuda_runtime.h>
+
 #include <cstdint>
 
 namespace tf {
@@ -37,6 +39,10 @@ struct FitGrid {
   const T* mmu_pure;   // M_mu "
   const uint8_t* live; // material label != 0 (the cell takes part in the H update)
   double len[3], area[3];
+  // optional per-dof coefficients (state-array shape, one array per axis),
+  // computed once from the tables above by fit_coef_kernel: M_h, M_q per
+  // edge, M_nu, M_mu per face (M_nu = -0.0 marks a face the H update skips)
+  T *Ch[3], *Cq[3], *Cn[3], *Cm[3];
 };
 
 // Edges whose update is not the 4-face interior stencil: boundary edges on
@@ -67,6 +73,9 @@ struct SpecialEdges {
   T* out;                  // [n] new value
   double* flux_part;       // [blocks] flux partial sums of this step
 };
+
+template <typename T>
+cudaError_t fit_build_coefficients(const FitGrid<T>& g, cudaStream_t st);
 
 struct ProbeSet {
   int n;

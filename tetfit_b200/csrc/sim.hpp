@@ -21,6 +21,7 @@ struct RunOptions {
   // turn it off: with a pinned step it only sets the possibly-unstable flag)
   bool estimate_pinned = true;
   // learned warm start (warm_start 3)
+  int fit_variant = 0;        // fdtd: 0 autotune, k > 0 force kernel variant k - 1
   int learn_steps = 500;      // steps whose solutions train the network
   int learn_samples = 32768;  // sampled rows per training step
   int learn_inner = 2;        // Adam steps per training step
@@ -64,6 +65,8 @@ class Sim {
   virtual uint64_t n_free() const { return 0; }
   virtual uint64_t nnz_system() const { return 0; }
   virtual uint64_t nnz_operators() const { return 0; }
+  // kernel variant in use (see tf_info.cg_variant)
+  virtual int kernel_variant() const { return 0; }
   // iterative solver statistics (gfdtd): iterations and final residual per step
   virtual size_t solver_stats(int32_t* iters, double* resid, size_t cap) const {
     (void)iters; (void)resid; (void)cap;

@@ -1236,6 +1236,8 @@ size_t TetSim::solver_stats(int32_t* iters, double* resid, size_t cap) const {
   return step_;
 }
 
+int TetSim::kernel_variant() const { return group_ ? group_->cg_variant() : 0; }
+
 size_t TetSim::guess_stats(int8_t* kept, size_t cap) const {
   return group_ ? group_->guess_stats(0, kept, cap) : 0;
 }

@@ -69,6 +69,7 @@ class TetSim : public Sim {
   size_t n_sources() const override { return src_labels_.size(); }
   size_t solver_stats(int32_t* iters, double* resid, size_t cap) const override;
   size_t guess_stats(int8_t* kept, size_t cap) const override;
+  int kernel_variant() const override;
   size_t training_loss(float* loss, size_t cap) const override;
   uint64_t n_free() const override { return free_edges_.size(); }
   uint64_t nnz_system() const override { return A_.val.size(); }
