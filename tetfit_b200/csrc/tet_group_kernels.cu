@@ -44,12 +44,12 @@ __device__ __forceinline__ double mulT(double a, double b) { return __dmul_rn(a,
 __device__ __forceinline__ bool running(const GroupDev& d, int s) { return d.step[s] < d.nsteps[s]; }
 
 // sum over the row's entries, in stored order, of val * g(col).  Entries
-// are taken 8 at a time: the index and value loads of a chunk are all issued
+// are taken 4 at a time: the index and value loads of a chunk are all issued
 // before its gathers, so a row costs about two memory latencies instead of
 // one per entry group.
 template <typename T, typename G>
 __device__ __forceinline__ T sell_dot(const SellDev& m, int64_t row, G g) {
-  constexpr int CH = 8;
+  constexpr int CH = 4;
   const int64_t sl = row >> 5;
   const int64_t b = m.ptr[sl];
   const int len = (int)((m.ptr[sl + 1] - b) >> 5);
@@ -375,8 +375,14 @@ __device__ __forceinline__ T p_next(T z, T pold, T beta, bool first) {
   return first ? z : fmaT(beta, pold, z);
 }
 
+// Co-resident CG blocks per SM the register budget is set for: more warps
+// in flight hide the SELL sweep's load latency better than longer load
+// chunks (measured: FP32 four blocks of 512, FP64 three, where four spill).
+template <typename T>
+constexpr int cg_min_blocks() { return sizeof(T) == 4 ? 4 : 3; }
+
 template <typename T, bool kFused>
-__global__ void __launch_bounds__(kCgThreads, 2) grp_cg(GroupDev d) {
+__global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDev d) {
   cg::grid_group grid = cg::this_grid();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SimCg* st = reinterpret_cast<SimCg*>(smem_raw);
