@@ -455,6 +455,21 @@ void TetGroup::partition() {
   d.seg_s1 = (const int64_t*)upload(seg_s1);
   d.sim_seg = (const int*)upload(sim_seg);
   d.part = (double*)dalloc(sizeof(double) * kCgPart * std::max<size_t>(seg_sim.size(), 1));
+  d.gbar = (unsigned int*)dalloc(2 * sizeof(unsigned int));
+  d.err = (int*)dalloc(sizeof(int));
+  CU(cudaMemset(d.gbar, 0, 2 * sizeof(unsigned int)));
+  CU(cudaMemset(d.err, 0, sizeof(int)));
+}
+
+// A grid-barrier timeout in the CG kernel leaves the step's results invalid:
+// report it (and reset the barrier so the group can be closed cleanly).
+void TetGroup::check_err() {
+  int e = 0;
+  CU(cudaMemcpy(&e, dev_.err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (!e) return;
+  CU(cudaMemset(dev_.err, 0, sizeof(int)));
+  CU(cudaMemset(dev_.gbar, 0, 2 * sizeof(unsigned int)));
+  throw CudaError("CG kernel: a grid barrier wait ran out of time; the step's results are not valid");
 }
 
 void TetGroup::launch(int n, cudaEvent_t* ev) {
@@ -526,6 +541,7 @@ uint64_t TetGroup::step(uint64_t n) {
   }
   last_ms_ = total;
   for (Meta& m : meta_) m.step = std::min(m.nsteps, m.step + n);
+  check_err();
   return n;
 }
 
@@ -547,6 +563,7 @@ uint64_t TetGroup::phase_times(uint64_t n, double* ms5) {
   }
   for (auto& e : ev) cudaEventDestroy(e);
   for (Meta& m : meta_) m.step = std::min(m.nsteps, m.step + n);
+  check_err();
   return n;
 }
 
@@ -586,6 +603,7 @@ uint64_t TetGroup::step_io(const double* car_in, double* probe_out) {
     o += meta_[s].np * 6;
   }
   for (Meta& m : meta_) m.step = std::min(m.nsteps, m.step + 1);
+  check_err();
   return 1;
 }
 

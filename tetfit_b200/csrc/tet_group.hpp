@@ -71,6 +71,7 @@ class TetGroup {
   template <typename T>
   void build(std::vector<TetSim*>& sims, bool release_host);
   void partition();
+  void check_err();
   void launch(int n, cudaEvent_t* ev);
   void* dalloc(size_t bytes);
   template <typename V>

@@ -362,11 +362,56 @@ __global__ void grp_mlp_targets(GroupDev d) {
   if (!isfinite(t)) d.samp_t[k] = 0.0f;
 }
 
+// Grid barrier of the persistent CG kernel: arrival counter bar[0] and
+// generation bar[1] in global memory (the cooperative launch keeps all blocks
+// resident).  The wait is bounded: after 2 s, or as soon as another block has
+// flagged an error, the block sets *err and goes on, so a fault in the
+// kernel's own logic ends the launch with an error the host reports instead
+// of a wait that never ends.
+__device__ __forceinline__ uint64_t grp_gtime() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void grid_barrier(unsigned int* bar, int* err, unsigned int nblocks) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int* gen = bar + 1;
+    const unsigned int g = *gen;
+    __threadfence();
+    if (atomicAdd(bar, 1u) == nblocks - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      const uint64_t t0 = grp_gtime();
+      while (*gen == g) {
+        if (*(volatile int*)err != 0 || grp_gtime() - t0 > 2000000000ull) {
+          atomicOr(err, 2);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
 struct SimCg {
   double rz, res0, bnorm, res, alpha, beta;
   int it, active, sel, pad;
 };
-constexpr int kPart = kCgPart;
+constexpr int kPart = 6;  // per-warp partials a segment flushes (shared memory)
+// Global partial slots of a segment: the initial residual's sums at 0..4, the
+// p.q sums at 5 and the residual update's at 6..7.  Disjoint groups matter:
+// no grid barrier separates a block's reads of one reduction's partials from
+// another block's writes of the next reduction, so consecutive reductions may
+// not share slots (the barrier after a reduction's writes does separate
+// reads of a group from its next writes).
+constexpr int kSlotStart = 0, kSlotPq = 5, kSlotRes = 6;
+static_assert(kCgPart >= 8, "global CG partial slots");
 
 // p_{j+1} at one row from z = pre r (stored by the residual phase), rounded
 // the same way wherever it is formed
@@ -383,9 +428,9 @@ constexpr int cg_min_blocks() { return sizeof(T) == 4 ? 4 : 3; }
 
 template <typename T, bool kFused>
 __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDev d) {
-  cg::grid_group grid = cg::this_grid();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SimCg* st = reinterpret_cast<SimCg*>(smem_raw);
+  auto grid_sync = [&]() { grid_barrier(d.gbar, d.err, gridDim.x); };
   double* wp = reinterpret_cast<double*>(smem_raw + sizeof(SimCg) * d.S);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g0 = d.blk_seg[blockIdx.x], g1 = d.blk_seg[blockIdx.x + 1];
@@ -430,23 +475,23 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
       w[2] = a2;
     }
   };
-  auto publish = [&](int nq) {
+  auto publish = [&](int nq, int slot) {
     __syncthreads();
     for (int gl = threadIdx.x; gl < g1 - g0; gl += kCgThreads)
       for (int k = 0; k < nq; k++) {
         double a = 0.0;
         for (int w = 0; w < kCgWarps; w++) a += wp[(gl * kCgWarps + w) * kPart + k];
-        d.part[kPart * (int64_t)(g0 + gl) + k] = a;
+        d.part[kCgPart * (int64_t)(g0 + gl) + slot + k] = a;
       }
   };
   // per-simulation totals of the published partials: one warp per
   // simulation, lanes over its segments, then a fixed shuffle tree; f(s, t)
   // runs on lane 0 with the nq totals t[]
-  auto totals = [&](int nq, auto&& f) {
+  auto totals = [&](int nq, int slot, auto&& f) {
     for (int s = warp; s < d.S; s += kCgWarps) {
       double t[kPart] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
       for (int g = d.sim_seg[s] + lane; g < d.sim_seg[s + 1]; g += 32)
-        for (int k = 0; k < nq; k++) t[k] += d.part[kPart * (int64_t)g + k];
+        for (int k = 0; k < nq; k++) t[k] += d.part[kCgPart * (int64_t)g + slot + k];
       for (int k = 0; k < nq; k++) t[k] = warp_sum(t[k]);
       if (lane == 0) f(s, t);
     }
@@ -487,9 +532,9 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
       }
     flush5(g, a0, a1, a2, a3, a4);
   }
-  publish(dual ? 5 : 3);
-  grid.sync();
-  totals(dual ? 5 : 3, [&](int s, const double* t) {
+  publish(dual ? 5 : 3, kSlotStart);
+  grid_sync();
+  totals(dual ? 5 : 3, kSlotStart, [&](int s, const double* t) {
     SimCg c;
     c.sel = dual && t[3] < t[0] ? 1 : 0;
     c.pad = 0;
@@ -539,7 +584,7 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
       if (kFused) flush(g, a0, 0.0, 0.0);
     }
     if (!kFused) {
-      grid.sync();
+      grid_sync();
       for (int g = g0; g < g1; g++) {
         const int s = d.seg_sim[g];
         const SimCg c = st[s];
@@ -556,9 +601,9 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
         flush(g, a0, 0.0, 0.0);
       }
     }
-    publish(1);
-    grid.sync();
-    totals(1, [&](int s, const double* t) {
+    publish(1, kSlotPq);
+    grid_sync();
+    totals(1, kSlotPq, [&](int s, const double* t) {
       if (st[s].active) st[s].alpha = st[s].rz / t[0];
     });
     __syncthreads();
@@ -583,9 +628,9 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
       }
       flush(g, a0, a1, 0.0);
     }
-    publish(2);
-    grid.sync();
-    totals(2, [&](int s, const double* t) {
+    publish(2, kSlotRes);
+    grid_sync();
+    totals(2, kSlotRes, [&](int s, const double* t) {
       SimCg c = st[s];
       if (!c.active) return;
       const double rz_prev = c.rz;

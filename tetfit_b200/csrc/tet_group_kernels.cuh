@@ -32,7 +32,7 @@ constexpr int kCgThreads = 512;
 constexpr int kCgWarps = kCgThreads / 32;
 constexpr int kMaxSeg = 32;       // segments per CG block
 constexpr int kMaxGroup = 1024;   // simulations per group
-constexpr int kCgPart = 6;        // CG partial sums per segment
+constexpr int kCgPart = 8;        // CG partial-sum slots per segment (three disjoint groups)
 
 struct SellDev {
   const int64_t* ptr = nullptr;  // [nslice + 1]
@@ -68,7 +68,9 @@ struct GroupDev {
   const int* seg_sim = nullptr;
   const int64_t *seg_s0 = nullptr, *seg_s1 = nullptr;  // slice range of a segment
   const int* sim_seg = nullptr;  // [S + 1]
-  double* part = nullptr;        // [nseg][3]
+  double* part = nullptr;        // [nseg][kCgPart]
+  unsigned int* gbar = nullptr;  // grid barrier: arrivals, generation
+  int* err = nullptr;            // set when a grid barrier wait ran out of time
   int cg_maxiter = 100, cg_criterion = 0, warm_start = 0;
   // learned warm start (warm_start 3): the network's guess goes to x, the
   // quadratic extrapolation to xe; with dual set, the CG starts from the one
