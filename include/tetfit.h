@@ -168,6 +168,19 @@ TF_API int tf_pcg_solve(const tf_pcg_args* args, int32_t* iters, double* rel_res
  * threads) race and must be serialised by the caller.  Same arguments, results
  * and status codes as tf_pcg_solve. */
 TF_API int tf_pcg_solve_noalloc(const tf_pcg_args* args, int32_t* iters, double* rel_resid);
+/* Self-check of the bounded grid barrier that the persistent CG kernels (the
+ * batch/gfdtd solve and tf_pcg_solve) use; no reference counterpart.  `blocks`
+ * co-resident blocks (one cooperative launch, blocks <= the SM count) pass
+ * `rounds` barriers that each wait for `expected` arrivals, every wait bounded
+ * by timeout_us.  With expected == blocks every barrier completes and *status
+ * is 0; with expected > blocks the first wait can never complete, it runs out,
+ * the launch still ends and *status is 2 -- the flag on which the CG kernels'
+ * callers return TF_E_CUDA.  *ms (optional) is the launch's duration.
+ * Arguments: 1 <= blocks, 1 <= expected <= 2 blocks, 1 <= rounds <= 100000,
+ * 1 <= timeout_us <= 1000000; otherwise TF_E_ARG (checked before the GPU is
+ * touched).  Errors through tf_last_error(NULL). */
+TF_API int tf_barrier_check(int32_t device, uint32_t blocks, uint32_t expected, uint32_t rounds,
+                            uint32_t timeout_us, int32_t* status, double* ms);
 /* ---- Batches: many gfdtd simulations advanced together ---------------------
  * The reference runs the simulations of a script one after another
  * (dga_main.cpp:52-62), each with its own mesh, materials, sources and time

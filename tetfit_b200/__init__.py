@@ -93,6 +93,9 @@ _SIGS = {
                                     ctypes.POINTER(ctypes.c_double)]),
     "tf_pcg_solve_noalloc": (ctypes.c_int, [ctypes.POINTER(PcgArgs), ctypes.POINTER(ctypes.c_int32),
                                             ctypes.POINTER(ctypes.c_double)]),
+    "tf_barrier_check": (ctypes.c_int, [ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                        ctypes.c_uint32, ctypes.POINTER(ctypes.c_int32),
+                                        ctypes.POINTER(ctypes.c_double)]),
     "tf_batch_open": (ctypes.c_int, [ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_uint32),
                                      ctypes.c_uint32, ctypes.POINTER(Opts), ctypes.POINTER(_P)]),
     "tf_batch_info": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(Info)]),
@@ -150,6 +153,19 @@ def pcg_solve(row_ptr, col, val, b, x, tol=1e-8, maxiter=0, criterion=0, device=
     rs = ctypes.c_double()
     rc = lib().tf_pcg_solve(ctypes.byref(a), ctypes.byref(it), ctypes.byref(rs))
     return rc, it.value, rs.value
+
+
+def barrier_check(blocks: int, expected: int, rounds: int = 1, timeout_us: int = 100000, device: int = 0):
+    """Self-check of the CG kernels' bounded grid barrier (tf_barrier_check):
+    (status, ms) of one launch of `blocks` blocks passing `rounds` barriers
+    that wait for `expected` arrivals.  status 0: every barrier completed;
+    2: a wait ran out of time (expected > blocks can never complete)."""
+    st = ctypes.c_int32()
+    ms = ctypes.c_double()
+    rc = lib().tf_barrier_check(device, blocks, expected, rounds, timeout_us, ctypes.byref(st), ctypes.byref(ms))
+    if rc != TF_OK:
+        raise TetfitError(rc, last_thread_error())
+    return st.value, ms.value
 
 
 def mlp_init(seed: int = 1) -> np.ndarray:

@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libtetfit_b200.so")
 SOURCES = ["script.cpp", "fit.cpp", "fit_kernels.cu", "tet.cpp", "tet_kernels.cu", "tet_group.cpp",
-           "tet_group_kernels.cu", "mlp.cu", "pcg.cu", "capi.cpp", "capi_batch.cpp"]
+           "tet_group_kernels.cu", "mlp.cu", "pcg.cu", "barrier_check.cu", "capi.cpp", "capi_batch.cpp"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared", "-Xcompiler", "-fvisibility=hidden"]
 

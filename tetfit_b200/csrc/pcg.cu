@@ -33,7 +33,8 @@ int check_args(const tf_pcg_args* a) {
 
 DevPtrs make_ptrs(const tf_pcg_args* a, double* work, int blocks) {
   // work layout: pre, r, p, q [n each], part_a [blocks], part_b [3 blocks],
-  // resid [1], then int32 iters, step counter and limit flag
+  // resid [1], then one 8-byte slot each for the int32 iters, step counter,
+  // limit flag, barrier error flag, and the grid barrier's two uint32 words
   const int64_t n = a->n;
   DevPtrs d;
   d.nfree = a->n;
@@ -52,23 +53,30 @@ DevPtrs make_ptrs(const tf_pcg_args* a, double* work, int blocks) {
   d.cg_iters = (int32_t*)(work + 4 * n + 4 * blocks + 1);
   d.step = (int*)(work + 4 * n + 4 * blocks + 2);
   d.cg_limit = (int32_t*)(work + 4 * n + 4 * blocks + 3);
+  d.err = (int*)(work + 4 * n + 4 * blocks + 4);
+  d.gbar = (unsigned int*)(work + 4 * n + 4 * blocks + 5);
   d.tol = a->tol;
   d.cg_maxiter = a->maxiter > 0 ? a->maxiter : 100;
   d.cg_criterion = a->criterion;
   return d;
 }
 
-size_t work_doubles(int64_t n, int blocks) { return (size_t)(4 * n + 4 * blocks + 4); }
+size_t work_doubles(int64_t n, int blocks) { return (size_t)(4 * n + 4 * blocks + 6); }
 
 int finish(cudaStream_t st, const DevPtrs& d, int32_t* iters, double* resid) {
-  int32_t it = 0, lim = 0;
+  int32_t it = 0, lim = 0, berr = 0;
   double rs = 0;
   cudaError_t e = cudaMemcpyAsync(&it, d.cg_iters, sizeof(it), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&rs, d.cg_resid, sizeof(rs), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&lim, d.cg_limit, sizeof(lim), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&berr, d.err, sizeof(berr), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     tf::set_thread_error(std::string("tf_pcg_solve: ") + cudaGetErrorString(e));
+    return TF_E_CUDA;
+  }
+  if (berr) {
+    tf::set_thread_error("tf_pcg_solve: a grid barrier wait of the CG kernel ran out of time; no valid result");
     return TF_E_CUDA;
   }
   if (iters) *iters = it;
@@ -124,7 +132,7 @@ namespace {
 constexpr int kNoAllocMaxN = 1 << 18;   // 262,144 unknowns
 constexpr int kNoAllocMaxBlocks = 1024; // reduction slots for the cooperative grid
 
-__device__ __align__(256) double g_pcg_scratch[4 * (size_t)kNoAllocMaxN + 4 * kNoAllocMaxBlocks + 4];
+__device__ __align__(256) double g_pcg_scratch[4 * (size_t)kNoAllocMaxN + 4 * kNoAllocMaxBlocks + 6];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
@@ -182,7 +190,8 @@ extern "C" int tf_pcg_solve_noalloc(const tf_pcg_args* a, int32_t* iters, double
   // the layout places the n-sized vectors first; the reduction slots and
   // counters sit after 4 * n, inside the array for any n <= kNoAllocMaxN.
   // Every value the kernel reads is written earlier in the same call (the
-  // step counter is cleared by pcg_launch_solve).
+  // step counter, barrier words and error flag are cleared by
+  // pcg_launch_solve).
   DevPtrs d = make_ptrs(a, work, blocks);
   e = tf::pcg_launch_solve(d, blocks, st);
   if (e != cudaSuccess) {

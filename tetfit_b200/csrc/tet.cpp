@@ -28,9 +28,7 @@
 namespace tf {
 
 template <typename T>
-cudaError_t tet_launch_step(const DevPtrs& d, int method, int cg_blocks, cudaStream_t st, cudaEvent_t* ev);
-template <typename T>
-int tet_cg_blocks(int device);
+cudaError_t tet_launch_step(const DevPtrs& d, cudaStream_t st, cudaEvent_t* ev);
 template <typename T>
 void tet_launch_initial_probes(const DevPtrs& d, cudaStream_t st);
 
@@ -988,7 +986,7 @@ void TetSim::alloc_and_upload() {
   d.nF = (int)NF;
   d.dt = dt_;
   d.U = zeros(NE); d.F = zeros(NF); d.B = zeros(NF); d.cu = zeros(NF); d.cf = zeros(NE);
-  d.I = zeros(NE); d.cb = zeros(NE); d.src = zeros(NE);
+  d.I = zeros(NE); d.cb = zeros(NE);
   d.fte = (const int32_t*)up(fte_.data(), NF * 3 * 4);
   {
     std::vector<int32_t> cc(Ct_.col.size());
@@ -1002,30 +1000,7 @@ void TetSim::alloc_and_upload() {
     val = upT(m.val);
   };
   upcsr(N_, d.n_ptr, d.n_col, d.n_val);
-  if (method_ == 1) {
-    upcsr(H_, d.h_ptr, d.h_col, d.h_val);
-  } else {
-    upcsr(E_, d.e_ptr, d.e_col, d.e_val);
-    upcsr(A_, d.a_ptr, d.a_col, d.a_val);
-    upcsr(R_, d.r_ptr, d.r_col, d.r_val);
-    d.jac = upT(jacobi_);
-    d.nfree = (int)free_edges_.size();
-    d.ndir = (int)dir_edges_.size();
-    d.free_edges = (const int32_t*)up(free_edges_.data(), free_edges_.size() * 4);
-    d.dir_edges = (const int32_t*)up(dir_edges_.data(), dir_edges_.size() * 4);
-    d.x = zeros(d.nfree); d.r = zeros(d.nfree); d.p = zeros(d.nfree); d.q = zeros(d.nfree);
-    d.rhs = zeros(d.nfree); d.xh1 = zeros(d.nfree); d.xh2 = zeros(d.nfree); d.xh3 = zeros(d.nfree);
-    cg_blocks_ = f32 ? tet_cg_blocks<float>(opt_.device) : tet_cg_blocks<double>(opt_.device);
-    if (cg_blocks_ < 1) throw CudaError("no co-resident blocks for the cooperative CG kernel");
-    d.part_a = (double*)dalloc((size_t)cg_blocks_ * 8);
-    d.part_b = (double*)dalloc((size_t)cg_blocks_ * 3 * 8);
-    d.cg_iters = (int32_t*)dalloc((nsteps_ + 1) * 4);
-    d.cg_resid = (double*)dalloc((nsteps_ + 1) * 8);
-    d.cg_maxiter = opt_.cg_maxiter;
-    d.cg_criterion = opt_.cg_criterion;
-    d.warm_start = opt_.warm_start;
-    d.tol = sim_.tol;
-  }
+  upcsr(H_, d.h_ptr, d.h_col, d.h_val);
   const size_t nsrc = src_labels_.size();
   d.nse = (int)src_edge_.size();
   d.nsrc = (int)nsrc;
@@ -1041,7 +1016,7 @@ void TetSim::alloc_and_upload() {
   d.carrier = (const double*)up(carrier_.data(), carrier_.size() * 8);
   d.flux = (double*)dalloc((nsteps_ + 1) * 8);
   CU(cudaMemsetAsync(d.flux, 0, (nsteps_ + 1) * 8, stream_));
-  d.nflux_part = method_ == 1 ? (int)((NE + 255) / 256) : (int)((src_edge_.size() + 255) / 256);
+  d.nflux_part = (int)((NE + 255) / 256);
   if (d.nflux_part < 1) d.nflux_part = 1;
   d.flux_part = (double*)dalloc((size_t)d.nflux_part * 8);
   CU(cudaMemsetAsync(d.flux_part, 0, (size_t)d.nflux_part * 8, stream_));
@@ -1063,7 +1038,7 @@ void TetSim::alloc_and_upload() {
   d.step = (int*)dalloc(sizeof(int));
   CU(cudaMemsetAsync(d.step, 0, sizeof(int), stream_));
   CU(cudaHostAlloc((void**)&pinned_, (nsrc + 6 * np + 1) * sizeof(double), cudaHostAllocDefault));
-  // initial state (t = 0 sources, dga :671-791, gfdtd :1425-1445)
+  // initial state (t = 0 sources, Discretization.hpp:671-791)
   auto put_state = [&](void* dst, const std::vector<double>& v) {
     if (!f32) CU(cudaMemcpyAsync(dst, v.data(), v.size() * 8, cudaMemcpyHostToDevice, stream_));
     else {
@@ -1074,19 +1049,16 @@ void TetSim::alloc_and_upload() {
   };
   put_state(d.U, init_U_);
   put_state(d.I, init_I_);
-  put_state(d.src, init_src_);
-  if (method_ == 1) {
-    if (f32) tet_launch_initial_probes<float>(d, stream_);
-    else tet_launch_initial_probes<double>(d, stream_);
-  }
+  if (f32) tet_launch_initial_probes<float>(d, stream_);
+  else tet_launch_initial_probes<double>(d, stream_);
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(stream_));
 }
 
 void TetSim::launch_steps(int n, cudaEvent_t* ev) {
   for (int q = 0; q < n; q++) {
-    cudaError_t e = opt_.precision == 1 ? tet_launch_step<float>(dp_, method_, cg_blocks_, stream_, ev)
-                                        : tet_launch_step<double>(dp_, method_, cg_blocks_, stream_, ev);
+    cudaError_t e = opt_.precision == 1 ? tet_launch_step<float>(dp_, stream_, ev)
+                                        : tet_launch_step<double>(dp_, stream_, ev);
     CU(e);
   }
 }

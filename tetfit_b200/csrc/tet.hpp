@@ -88,8 +88,6 @@ class TetSim : public Sim {
   void alloc_and_upload();
   friend class TetGroup;
   void launch_steps(int n, cudaEvent_t* ev);
-  template <typename T>
-  void fill(TetDev<T>& d) const;
   std::array<int32_t, 6> vol_edges(uint32_t v) const;
 
   Script& sc_;
@@ -151,7 +149,6 @@ class TetSim : public Sim {
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   std::vector<void*> allocs_;
   DevPtrs dp_{};
-  int cg_blocks_ = 0;
   double* pinned_ = nullptr;
   // gfdtd runs on the group engine (a group of one simulation)
   std::unique_ptr<TetGroup> group_;

@@ -24,13 +24,12 @@
 // owner uses, so p_{j+1} needs no barrier before the SpMV: two grid barriers
 // per iteration instead of three.
 // Both variants give bitwise identical iterates.
-#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include "grid_barrier.cuh"
 #include "mlp.cuh"
 #include "tet_group_kernels.cuh"
 
-namespace cg = cooperative_groups;
 
 namespace tf {
 
@@ -360,43 +359,6 @@ __global__ void grp_mlp_targets(GroupDev d) {
   d.samp_t[k] = (float)t;
   d.samp_w[k] = isfinite(t) ? 1.0f : 0.0f;
   if (!isfinite(t)) d.samp_t[k] = 0.0f;
-}
-
-// Grid barrier of the persistent CG kernel: arrival counter bar[0] and
-// generation bar[1] in global memory (the cooperative launch keeps all blocks
-// resident).  The wait is bounded: after 2 s, or as soon as another block has
-// flagged an error, the block sets *err and goes on, so a fault in the
-// kernel's own logic ends the launch with an error the host reports instead
-// of a wait that never ends.
-__device__ __forceinline__ uint64_t grp_gtime() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ void grid_barrier(unsigned int* bar, int* err, unsigned int nblocks) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    volatile unsigned int* gen = bar + 1;
-    const unsigned int g = *gen;
-    __threadfence();
-    if (atomicAdd(bar, 1u) == nblocks - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      const uint64_t t0 = grp_gtime();
-      while (*gen == g) {
-        if (*(volatile int*)err != 0 || grp_gtime() - t0 > 2000000000ull) {
-          atomicOr(err, 2);
-          break;
-        }
-        __nanosleep(32);
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
 }
 
 struct SimCg {

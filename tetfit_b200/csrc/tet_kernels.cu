@@ -1,26 +1,24 @@
-// Tetrahedral DGA kernels for sm_100a.
+// Kernels of the explicit tetrahedral DGA method (dga) for sm_100a, and the
+// standalone CG solve of the C ABI.  (gfdtd simulations run on the group
+// engine, tet_group_kernels.cu, also when a simulation is alone.)
 //
 //   tet_curl_u        cu = C U (3 signed edges per face), B -= dt cu
-//                     (Discretization.hpp:902-916, 1466-1467)
-//   tet_nmul          F -= dt N cu (dga, :917) or F = N B (gfdtd, :1468)
-//   tet_curl_f        cf = C^T F + Ctb Fb - I (dga, :878-879)
-//   tet_h_update      U += dt H cf on interior edges, boundary flux (dga, :889-894)
+//                     (Discretization.hpp:902-916)
+//   tet_nmul          F -= dt N cu (:917)
+//   tet_curl_f        cf = C^T F + Ctb Fb - I (:878-879)
+//   tet_h_update      U += dt H cf on interior edges, boundary flux (:889-894)
 //   tet_sources       source edges from the carrier table: E values, boundary
-//                     dual-edge H sources, currents (:821-868, :1478-1504)
-//   tet_rhs           Psi = E U_old - R Src - dt I + dt C^T F + dt Ctb Fb on
-//                     the free edges (gfdtd, :1516-1523)
-//   tet_cg            persistent cooperative Jacobi-PCG on the free edges
+//                     dual-edge H sources, currents (:821-868)
+//   tet_probes        Whitney E and face-flux H at probe points (:3768-3897)
+//   tet_cg            persistent cooperative Jacobi-PCG on a CSR system
 //                     (ConjugateGradientSolver.hpp:52-103): SpMV, dots and
 //                     axpys fused, FP64 reductions in a fixed order, a hard
-//                     iteration limit and three grid barriers per iteration
-//   tet_scatter       U[free] = x, U[Dirichlet] = source values (:1540-1541)
-//   tet_probes        Whitney E and face-flux H at probe points (:3768-3897)
-#include <cooperative_groups.h>
+//                     iteration limit and three bounded grid barriers per
+//                     iteration
 #include <cuda_runtime.h>
 
+#include "grid_barrier.cuh"
 #include "tet_kernels.cuh"
-
-namespace cg = cooperative_groups;
 
 namespace tf {
 
@@ -49,30 +47,27 @@ __device__ double block_sum(double v, double* sh) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kBlock) tet_curl_u(DevPtrs d, int update_B) {
+__global__ void __launch_bounds__(kBlock) tet_curl_u(DevPtrs d) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= d.nF) return;
   const T* U = (const T*)d.U;
   const int32_t* e = d.fte + 3 * (int64_t)f;
   T c = U[e[0]] - U[e[1]] + U[e[2]];
   ((T*)d.cu)[f] = c;
-  if (update_B) {
-    T* B = (T*)d.B;
-    B[f] = B[f] - (T)d.dt * c;
-  }
+  T* B = (T*)d.B;
+  B[f] = B[f] - (T)d.dt * c;
 }
 
-// mode 0: F -= dt N cu (dga); mode 1: F = N B (gfdtd)
+// F -= dt N cu
 template <typename T>
-__global__ void __launch_bounds__(kBlock) tet_nmul(DevPtrs d, int mode) {
+__global__ void __launch_bounds__(kBlock) tet_nmul(DevPtrs d) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= d.nF) return;
-  const T* x = (const T*)(mode == 0 ? d.cu : d.B);
+  const T* x = (const T*)d.cu;
   T s = 0;
   for (int64_t k = d.n_ptr[f]; k < d.n_ptr[f + 1]; k++) s += ld<T>(d.n_val, k) * x[d.n_col[k]];
   T* F = (T*)d.F;
-  if (mode == 0) F[f] = F[f] - (T)d.dt * s;
-  else F[f] = s;
+  F[f] = F[f] - (T)d.dt * s;
 }
 
 template <typename T>
@@ -114,15 +109,12 @@ __global__ void __launch_bounds__(kBlock) tet_h_update(DevPtrs d) {
   if (threadIdx.x == 0) d.flux_part[blockIdx.x] = fl;
 }
 
-// Source edges.  method 1 (dga): E sources write U, H sources write cb (reset
-// each step), currents write I.  method 2 (gfdtd): E sources write the
-// Dirichlet value array, flux partials use U (the previous solution).
+// Source edges: E sources write U, H sources write cb (reset each step),
+// currents write I.
 template <typename T>
-__global__ void __launch_bounds__(kBlock) tet_sources(DevPtrs d, int method) {
-  __shared__ double sh[33];
+__global__ void __launch_bounds__(kBlock) tet_sources(DevPtrs d) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   const int step = *d.step;
-  double fl = 0.0;
   if (s < d.nse) {
     auto value = [&](int row) {
       double v[3] = {0.0, 0.0, 0.0};
@@ -141,22 +133,9 @@ __global__ void __launch_bounds__(kBlock) tet_sources(DevPtrs d, int method) {
     const int e = d.se_edge[s];
     const int kind = d.se_kind[s];
     const double val = value(step);
-    if (kind == 1) {
-      if (method == 1) ((T*)d.U)[e] = (T)val;
-      else ((T*)d.src)[e] = (T)val;
-    } else if (kind == 2) {
-      ((T*)d.cb)[e] = (T)val;
-      if (method == 2) {
-        const double prev = step > 0 ? value(step - 1) : 0.0;
-        fl = (double)((const T*)d.U)[e] * (0.5 * (val + prev));
-      }
-    } else if (kind == 3) {
-      ((T*)d.I)[e] = (T)val;
-    }
-  }
-  if (method == 2) {
-    fl = block_sum(fl, sh);
-    if (threadIdx.x == 0) d.flux_part[blockIdx.x] = fl;
+    if (kind == 1) ((T*)d.U)[e] = (T)val;
+    else if (kind == 2) ((T*)d.cb)[e] = (T)val;
+    else if (kind == 3) ((T*)d.I)[e] = (T)val;
   }
 }
 
@@ -166,44 +145,6 @@ __global__ void flux_reduce(DevPtrs d, double scale) {
   for (int b = threadIdx.x; b < d.nflux_part; b += blockDim.x) a += d.flux_part[b];
   a = block_sum(a, sh);
   if (threadIdx.x == 0) d.flux[*d.step] = scale * a;
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kBlock) tet_rhs(DevPtrs d) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= d.nfree) return;
-  const int e = d.free_edges[k];
-  const T* U = (const T*)d.U;
-  const T* S = (const T*)d.src;
-  T eu = 0, rs = 0;
-  for (int64_t q = d.e_ptr[e]; q < d.e_ptr[e + 1]; q++) eu += ld<T>(d.e_val, q) * U[d.e_col[q]];
-  for (int64_t q = d.r_ptr[k]; q < d.r_ptr[k + 1]; q++) rs += ld<T>(d.r_val, q) * S[d.r_col[q]];
-  const T dt = (T)d.dt;
-  ((T*)d.rhs)[k] = eu - rs - dt * ((const T*)d.I)[e] + dt * ctf<T>(d, e) + dt * ((const T*)d.cb)[e];
-}
-
-// Initial guess: 0 previous solution (x kept), 1 zero, 2 quadratic
-// extrapolation from the last three solutions; history shifts here.
-template <typename T>
-__global__ void __launch_bounds__(kBlock) tet_guess(DevPtrs d) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= d.nfree) return;
-  T* x = (T*)d.x;
-  T* h1 = (T*)d.xh1;
-  T* h2 = (T*)d.xh2;
-  T* h3 = (T*)d.xh3;
-  const int step = *d.step;
-  if (d.warm_start == 1) {
-    x[k] = 0;
-  } else if (d.warm_start == 2) {
-    // x_{n-1} = x (last solution); keep three levels
-    const T a = x[k], b = h1[k], c = h2[k];
-    h3[k] = c;
-    h2[k] = b;
-    h1[k] = a;
-    if (step >= 3) x[k] = (T)3 * a - (T)3 * b + c;
-    else if (step >= 2) x[k] = (T)2 * a - b;
-  }
 }
 
 template <typename T>
@@ -226,7 +167,6 @@ __device__ double sum_parts(const double* part, int nb, int stride, int off, dou
 // product and norm accumulated in FP64.
 template <typename T>
 __global__ void __launch_bounds__(kBlock) tet_cg(DevPtrs d) {
-  cg::grid_group grid = cg::this_grid();
   __shared__ double sh[33];
   const int n = d.nfree;
   const int nb = gridDim.x;
@@ -256,7 +196,7 @@ __global__ void __launch_bounds__(kBlock) tet_cg(DevPtrs d) {
     d.part_b[3 * blockIdx.x + 1] = rz;
     d.part_b[3 * blockIdx.x + 2] = bb;
   }
-  grid.sync();
+  grid_barrier(d.gbar, d.err, nb);
   rr = sum_parts(d.part_b, nb, 3, 0, sh);
   rz = sum_parts(d.part_b, nb, 3, 1, sh);
   bb = sum_parts(d.part_b, nb, 3, 2, sh);
@@ -276,7 +216,7 @@ __global__ void __launch_bounds__(kBlock) tet_cg(DevPtrs d) {
       const T z = pre[i] * r[i];
       p[i] = it == 0 ? z : z + beta * p[i];
     }
-    grid.sync();
+    grid_barrier(d.gbar, d.err, nb);
     double pq = 0;
     for (int64_t i = tid; i < n; i += nth) {
       const T qi = spmv_row<T>(d.a_ptr, d.a_col, d.a_val, p, (int)i);
@@ -285,7 +225,7 @@ __global__ void __launch_bounds__(kBlock) tet_cg(DevPtrs d) {
     }
     pq = block_sum(pq, sh);
     if (threadIdx.x == 0) d.part_a[blockIdx.x] = pq;
-    grid.sync();
+    grid_barrier(d.gbar, d.err, nb);
     pq = sum_parts(d.part_a, nb, 1, 0, sh);
     const T alpha = (T)(rz / pq);
     double rr2 = 0, rz2 = 0;
@@ -303,7 +243,7 @@ __global__ void __launch_bounds__(kBlock) tet_cg(DevPtrs d) {
       d.part_b[3 * blockIdx.x + 0] = rr2;
       d.part_b[3 * blockIdx.x + 1] = rz2;
     }
-    grid.sync();
+    grid_barrier(d.gbar, d.err, nb);
     rr = sum_parts(d.part_b, nb, 3, 0, sh);
     rz_prev = rz;
     rz = sum_parts(d.part_b, nb, 3, 1, sh);
@@ -321,20 +261,8 @@ __global__ void __launch_bounds__(kBlock) tet_cg(DevPtrs d) {
   }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kBlock) tet_scatter(DevPtrs d) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  T* U = (T*)d.U;
-  if (k < d.nfree) U[d.free_edges[k]] = ((const T*)d.x)[k];
-  if (k < d.ndir) {
-    const int e = d.dir_edges[k];
-    U[e] = ((const T*)d.src)[e];
-  }
-}
-
-// Probe export.  The print schedule is indexed by step counter + offset
-// (dga exports after the step, time (s+1) dt: offset 1; gfdtd exports U^{s}
-// before the solve, time s dt: offset 0).
+// Probe export.  The print schedule is indexed by step counter + offset:
+// after a step, time (s+1) dt, offset 1; before the first step, offset 0.
 template <typename T>
 __global__ void tet_probes(DevPtrs d, int offset) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -374,47 +302,25 @@ int tet_cg_blocks(int device) {
   return per_sm * sms;
 }
 
-// One leapfrog step.  ev (optional, 6 events) brackets: sources, E half,
-// scatter/flux, probes, H half.
+// One leapfrog step of the dga method (Discretization.hpp:810-931).  ev
+// (optional, 6 events) brackets: sources, H half, flux, E half, probes.
 template <typename T>
-cudaError_t tet_launch_step(const DevPtrs& d, int method, int cg_blocks, cudaStream_t st, cudaEvent_t* ev) {
-  if (method == 1) {  // dga (Discretization.hpp:810-931)
-    if (ev) cudaEventRecord(ev[0], st);
-    cudaMemsetAsync(d.cb, 0, sizeof(T) * (size_t)d.nE, st);
-    if (d.nse) tet_sources<T><<<nblk(d.nse), kBlock, 0, st>>>(d, 1);
-    if (ev) cudaEventRecord(ev[1], st);
-    tet_curl_f<T><<<nblk(d.nE), kBlock, 0, st>>>(d);
-    tet_h_update<T><<<nblk(d.nE), kBlock, 0, st>>>(d);
-    if (ev) cudaEventRecord(ev[2], st);
-    flux_reduce<<<1, kBlock, 0, st>>>(d, 0.5);
-    if (ev) cudaEventRecord(ev[3], st);
-    tet_curl_u<T><<<nblk(d.nF), kBlock, 0, st>>>(d, 1);
-    tet_nmul<T><<<nblk(d.nF), kBlock, 0, st>>>(d, 0);
-    if (ev) cudaEventRecord(ev[4], st);
-    if (d.np) tet_probes<T><<<nblk(d.np), kBlock, 0, st>>>(d, 1);
-    bump_step<<<1, 1, 0, st>>>(d.step);
-    if (ev) cudaEventRecord(ev[5], st);
-  } else {  // gfdtd (Discretization.hpp:1459-1565)
-    if (ev) cudaEventRecord(ev[0], st);
-    tet_curl_u<T><<<nblk(d.nF), kBlock, 0, st>>>(d, 1);
-    tet_nmul<T><<<nblk(d.nF), kBlock, 0, st>>>(d, 1);
-    if (d.np) tet_probes<T><<<nblk(d.np), kBlock, 0, st>>>(d, 0);
-    if (ev) cudaEventRecord(ev[1], st);
-    tet_sources<T><<<nblk(d.nse), kBlock, 0, st>>>(d, 2);
-    flux_reduce<<<1, kBlock, 0, st>>>(d, 1.0);
-    tet_rhs<T><<<nblk(d.nfree), kBlock, 0, st>>>(d);
-    tet_guess<T><<<nblk(d.nfree), kBlock, 0, st>>>(d);
-    if (ev) cudaEventRecord(ev[2], st);
-    DevPtrs dd = d;
-    void* args[] = {(void*)&dd};
-    cudaError_t err = cudaLaunchCooperativeKernel((void*)tet_cg<T>, dim3(cg_blocks), dim3(kBlock), args, 0, st);
-    if (err != cudaSuccess) return err;
-    if (ev) cudaEventRecord(ev[3], st);
-    tet_scatter<T><<<nblk(d.nfree > d.ndir ? d.nfree : d.ndir), kBlock, 0, st>>>(d);
-    if (ev) cudaEventRecord(ev[4], st);
-    bump_step<<<1, 1, 0, st>>>(d.step);
-    if (ev) cudaEventRecord(ev[5], st);
-  }
+cudaError_t tet_launch_step(const DevPtrs& d, cudaStream_t st, cudaEvent_t* ev) {
+  if (ev) cudaEventRecord(ev[0], st);
+  cudaMemsetAsync(d.cb, 0, sizeof(T) * (size_t)d.nE, st);
+  if (d.nse) tet_sources<T><<<nblk(d.nse), kBlock, 0, st>>>(d);
+  if (ev) cudaEventRecord(ev[1], st);
+  tet_curl_f<T><<<nblk(d.nE), kBlock, 0, st>>>(d);
+  tet_h_update<T><<<nblk(d.nE), kBlock, 0, st>>>(d);
+  if (ev) cudaEventRecord(ev[2], st);
+  flux_reduce<<<1, kBlock, 0, st>>>(d, 0.5);
+  if (ev) cudaEventRecord(ev[3], st);
+  tet_curl_u<T><<<nblk(d.nF), kBlock, 0, st>>>(d);
+  tet_nmul<T><<<nblk(d.nF), kBlock, 0, st>>>(d);
+  if (ev) cudaEventRecord(ev[4], st);
+  if (d.np) tet_probes<T><<<nblk(d.np), kBlock, 0, st>>>(d, 1);
+  bump_step<<<1, 1, 0, st>>>(d.step);
+  if (ev) cudaEventRecord(ev[5], st);
   return cudaGetLastError();
 }
 
@@ -434,6 +340,8 @@ cudaError_t pcg_launch_solve(DevPtrs d, int blocks, cudaStream_t st) {
   jacobi_from_csr<<<nblk(d.nfree), kBlock, 0, st>>>(d.a_ptr, d.a_col, (const double*)d.a_val, (double*)d.jac,
                                                     d.nfree);
   cudaMemsetAsync(d.step, 0, sizeof(int), st);
+  cudaMemsetAsync(d.gbar, 0, 2 * sizeof(unsigned int), st);
+  cudaMemsetAsync(d.err, 0, sizeof(int), st);
   void* args[] = {(void*)&d};
   cudaError_t err = cudaLaunchCooperativeKernel((void*)tet_cg<double>, dim3(blocks), dim3(kBlock), args, 0, st);
   if (err != cudaSuccess) return err;
@@ -446,10 +354,9 @@ void tet_launch_initial_probes(const DevPtrs& d, cudaStream_t st) {
   if (d.np) tet_probes<T><<<nblk(d.np), kBlock, 0, st>>>(d, 0);
 }
 
-template cudaError_t tet_launch_step<double>(const DevPtrs&, int, int, cudaStream_t, cudaEvent_t*);
-template cudaError_t tet_launch_step<float>(const DevPtrs&, int, int, cudaStream_t, cudaEvent_t*);
+template cudaError_t tet_launch_step<double>(const DevPtrs&, cudaStream_t, cudaEvent_t*);
+template cudaError_t tet_launch_step<float>(const DevPtrs&, cudaStream_t, cudaEvent_t*);
 template int tet_cg_blocks<double>(int);
-template int tet_cg_blocks<float>(int);
 template void tet_launch_initial_probes<double>(const DevPtrs&, cudaStream_t);
 template void tet_launch_initial_probes<float>(const DevPtrs&, cudaStream_t);
 

@@ -1,41 +1,43 @@
-// Device layout of the tetrahedral DGA paths.
+// Device layout of the explicit tetrahedral DGA method (dga) and of the
+// standalone CG solve.
 //
 // Complex: faces carry their three edges (p0p1, p0p2, p1p2 with signs +, -, +,
 // the reference's fte order, Discretization.hpp:6327-6352); C^T is a CSR over
 // edges whose int32 entries hold the face index with the sign in bit 31.  The
 // material operators are CSR with int32 columns: N (faces x faces, per-tet
-// inverse blocks summed), H (dga: masked node-star inverses), E / A / R
-// (gfdtd eps-mass, its free-free block and its free-Dirichlet block).
+// inverse blocks summed) and H (masked node-star inverses); the CG solve takes
+// the caller's CSR system A.
 #pragma once
 #include <cstdint>
 
 namespace tf {
 
-// Type-erased device pointers (T = float or double arrays are void*).
+// Type-erased device pointers (T = float or double arrays are void*).  The
+// dga step uses the complex, N, H, the state and the sources; the standalone
+// CG solve (tf_pcg_solve) uses the system A, jac and the CG work.
 struct DevPtrs {
-  int nE = 0, nF = 0, nfree = 0, ndir = 0;
+  int nE = 0, nF = 0, nfree = 0;
   double dt = 0;
   // state (T)
-  void *U = nullptr, *F = nullptr, *B = nullptr, *cu = nullptr, *cf = nullptr, *I = nullptr, *cb = nullptr,
-       *src = nullptr;
+  void *U = nullptr, *F = nullptr, *B = nullptr, *cu = nullptr, *cf = nullptr, *I = nullptr, *cb = nullptr;
   // complex
   const int32_t* fte = nullptr;
   const int64_t* ct_ptr = nullptr;
   const int32_t* ct_col = nullptr;
   // operators (values T)
-  const int64_t *n_ptr = nullptr, *h_ptr = nullptr, *e_ptr = nullptr, *a_ptr = nullptr, *r_ptr = nullptr;
-  const int32_t *n_col = nullptr, *h_col = nullptr, *e_col = nullptr, *a_col = nullptr, *r_col = nullptr;
-  const void *n_val = nullptr, *h_val = nullptr, *e_val = nullptr, *a_val = nullptr, *r_val = nullptr;
+  const int64_t *n_ptr = nullptr, *h_ptr = nullptr, *a_ptr = nullptr;
+  const int32_t *n_col = nullptr, *h_col = nullptr, *a_col = nullptr;
+  const void *n_val = nullptr, *h_val = nullptr, *a_val = nullptr;
   const void* jac = nullptr;
-  const int32_t *free_edges = nullptr, *dir_edges = nullptr;
-  // CG work (T) and statistics
-  void *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *rhs = nullptr, *xh1 = nullptr, *xh2 = nullptr,
-       *xh3 = nullptr;
+  // CG work (T), reductions, grid barrier and statistics
+  void *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *rhs = nullptr;
   double *part_a = nullptr, *part_b = nullptr;
+  unsigned int* gbar = nullptr;  // grid barrier: arrivals, generation
+  int* err = nullptr;            // raised when a grid barrier wait ran out of time
   int32_t* cg_iters = nullptr;
   double* cg_resid = nullptr;
   int32_t* cg_limit = nullptr;  // optional: 1 when the iteration limit stopped the solve
-  int cg_maxiter = 100, cg_criterion = 0, warm_start = 0;
+  int cg_maxiter = 100, cg_criterion = 0;
   double tol = 1e-8;
   // sources
   int nse = 0, nsrc = 0;
@@ -56,12 +58,6 @@ struct DevPtrs {
   double* samples = nullptr;
   const int* slot_of_step = nullptr;
   int* step = nullptr;
-};
-
-template <typename T>
-struct TetDev {
-  DevPtrs d;
-  __host__ __device__ T* U() const { return (T*)d.U; }
 };
 
 }  // namespace tf
