@@ -42,6 +42,27 @@ __device__ __forceinline__ double mulT(double a, double b) { return __dmul_rn(a,
 
 __device__ __forceinline__ bool running(const GroupDev& d, int s) { return d.step[s] < d.nsteps[s]; }
 
+// Loads of a matrix's index and value streams: each entry is read once per
+// sweep, so they bypass L1 (read-only path, no L1 allocation) and leave it to
+// the gathered vector entries, which neighbouring rows reuse.  Measured on a
+// 64-member batch (11.3 M rows): 7 % (FP32) and 10 % (FP64) less time per CG
+// iteration than plain read-only loads.
+__device__ __forceinline__ int32_t ld_stream(const int32_t* p) {
+  int32_t v;
+  asm("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float ld_stream(const float* p) {
+  float v;
+  asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double ld_stream(const double* p) {
+  double v;
+  asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+
 // sum over the row's entries, in stored order, of val * g(col).  Entries
 // are taken 4 at a time: the index and value loads of a chunk are all issued
 // before its gathers, so a row costs about two memory latencies instead of
@@ -61,8 +82,8 @@ __device__ __forceinline__ T sell_dot(const SellDev& m, int64_t row, G g) {
 #pragma unroll
     for (int k = 0; k < CH; k++)
       if (j0 + k < len) {
-        c[k] = __ldg(col + 32 * (j0 + k));
-        v[k] = __ldg(val + 32 * (j0 + k));
+        c[k] = ld_stream(col + 32 * (j0 + k));
+        v[k] = ld_stream(val + 32 * (j0 + k));
       }
 #pragma unroll
     for (int k = 0; k < CH; k++)
@@ -211,7 +232,7 @@ __global__ void __launch_bounds__(kGB) grp_rhs(GroupDev d) {
     const int len = (int)((d.Ct.ptr[sl + 1] - b) >> 5);
     const int32_t* col = d.Ct.col + b + (i & 31);
     for (int j = 0; j < len; j++) {
-      const int32_t c = __ldg(col + 32 * j);
+      const int32_t c = ld_stream(col + 32 * j);
       if (c == kPadCol) break;
       const T v = F[c & 0x7fffffff];
       cf = c < 0 ? cf - v : cf + v;
@@ -296,7 +317,7 @@ __global__ void __launch_bounds__(kGB, 3) grp_guess_mlp(GroupDev d) {
       const int len = (int)((d.A.ptr[sl + 1] - b0) >> 5);
       const int32_t* col = d.A.col + b0 + lane;
       for (int j = 0; j < len; j++) {
-        const int32_t cc = __ldg(col + 32 * j);
+        const int32_t cc = ld_stream(col + 32 * j);
         if (cc != (int32_t)i) {
           sum += (float)re[cc];
           cnt++;
