@@ -225,17 +225,26 @@ __global__ void __launch_bounds__(kGB) grp_rhs(GroupDev d) {
   const T* S = (const T*)d.src;
   const T* F = (const T*)d.F;
   const T eu = sell_dot<T>(d.Ef, i, [&](int32_t c) { return U[c] - S[c]; });
+  // C^T F over the edge's faces in stored order; the face indices of 4
+  // entries are loaded before their gathers (padding entries hold kPadCol
+  // and add nothing)
   T cf = 0;
   {
+    constexpr int CH = 4;
     const int64_t sl = i >> 5;
     const int64_t b = d.Ct.ptr[sl];
     const int len = (int)((d.Ct.ptr[sl + 1] - b) >> 5);
     const int32_t* col = d.Ct.col + b + (i & 31);
-    for (int j = 0; j < len; j++) {
-      const int32_t c = ld_stream(col + 32 * j);
-      if (c == kPadCol) break;
-      const T v = F[c & 0x7fffffff];
-      cf = c < 0 ? cf - v : cf + v;
+    for (int j0 = 0; j0 < len; j0 += CH) {
+      int32_t c[CH];
+#pragma unroll
+      for (int k = 0; k < CH; k++) c[k] = j0 + k < len ? ld_stream(col + 32 * (j0 + k)) : kPadCol;
+#pragma unroll
+      for (int k = 0; k < CH; k++)
+        if (c[k] != kPadCol) {
+          const T v = F[c[k] & 0x7fffffff];
+          cf = c[k] < 0 ? cf - v : cf + v;
+        }
     }
   }
   const T dt = (T)d.dt[s];
