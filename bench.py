@@ -44,16 +44,16 @@ MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
 WORKLOADS = {
-    # Cartesian FIT cavities (SURVEY cfg0 / cfg2)
+    # Cartesian FIT cavities: 64^3 FP64 vacuum cavity, 512^3 FP32 with 200 random spheres
     "fit512": dict(kind="fit", n=512, spheres=200, prec="fp32", steps=5000),
     "fit64": dict(kind="fit", n=64, spheres=0, prec="fp64", steps=2000),
     "fit256": dict(kind="fit", n=256, spheres=200, prec="fp32", steps=2000),  # profiling size, state > L2
-    # tetrahedral box, jittered Kuhn mesh (SURVEY cfg1 at 24^3, cfg4 size at 96^3)
+    # tetrahedral 1 m box, jittered Kuhn mesh of 24^3 or 96^3 cubes (96^3: GRF eps_r)
     "gfdtd24": dict(kind="tet", method="gfdtd", n=24, prec="fp64", steps=1200, cpu_n=24),
     "dga24": dict(kind="tet", method="dga", n=24, prec="fp64", steps=1200, cpu_n=24),
     "gfdtd96": dict(kind="tet", method="gfdtd", n=96, prec="fp32", steps=5000, grf=True, cpu_n=24),
     "gfdtd96_fp64": dict(kind="tet", method="gfdtd", n=96, prec="fp64", steps=5000, grf=True, cpu_n=24),
-    # batched gfdtd (SURVEY cfg3): 128 members, n ~ U{8..48}, FP32 fields, FP64 CG reductions, CG to
+    # batched gfdtd: 128 members, n ~ U{8..48}, FP32 fields, FP64 CG reductions, CG to
     # ||r|| <= 1e-8 ||b||; the plain arm runs the same members one at a time in FP64 with the
     # reference's previous-solution guess
     "batch128": dict(kind="batch", members=128, n_lo=8, n_hi=48, steps=1000, seed=31337, prec="fp32",
@@ -61,7 +61,7 @@ WORKLOADS = {
     # the same scene at profiling size: 16 members n ~ U{8..32} (1.5 M CG rows, state > L2)
     "batch16": dict(kind="batch", members=16, n_lo=8, n_hi=32, steps=1000, seed=31337, prec="fp32",
                     warm="learned", learn_steps=40, crit="rhs", plain_steps=5),
-    # learned warm start at SURVEY cfg4 size: 96^3 Kuhn box, GRF eps_r, one member
+    # learned warm start on one 96^3 Kuhn box (5.3 M tets), GRF eps_r
     "learned96": dict(kind="batch", members=1, n_lo=96, n_hi=96, steps=5000, seed=4242, prec="fp32",
                       warm="learned", learn_steps=500, crit="rhs", plain_steps=5, grf=True),
 }
@@ -165,7 +165,7 @@ def make_case(workdir: str, workload: str, n_override: int | None = None):
 
 
 def fit_bytes(info: dict, es: int):
-    """Algorithmic bytes of one E and one H launch (see DESIGN.md, FIT byte model):
+    """Algorithmic bytes of one E and one H launch (FIT byte model):
     E reads U and F and writes U; H reads F and U and writes F; plus 1 B of
     material index per cell each."""
     nE, nF, nc = info["n_edges"], info["n_faces"], info["n_cells"]

@@ -1,5 +1,5 @@
 """Discrete leapfrog energy of a lossless cavity after the source has
-switched off (SURVEY §7): a Gaussian carrier exp(-(t-d)^2/w^2) underflows to
+switched off: a Gaussian carrier exp(-(t-d)^2/w^2) underflows to
 exactly 0 some 27 widths after its delay; from then on the H-source surface is
 a natural (zero tangential H) boundary and every other face is PEC, so
 
