@@ -89,6 +89,8 @@ int tf_batch_open(const char* const* scripts, const uint32_t* labels, uint32_t n
     std::atomic<uint32_t> next{0};
     unsigned nt = o.host_threads > 0 ? (unsigned)o.host_threads : std::max(1u, std::thread::hardware_concurrency());
     nt = std::min<unsigned>(nt, n);
+    // members are built nt at a time; each takes its share of the host threads
+    ro.setup_threads = (int)std::max(1u, std::max(1u, std::thread::hardware_concurrency()) / nt);
     // host build of every member (mesh, operators, probes, source tables)
     auto work = [&]() {
       for (uint32_t i = next++; i < n; i = next++) {

@@ -26,6 +26,7 @@ struct RunOptions {
   int learn_samples = 32768;  // sampled rows per training step
   int learn_inner = 2;        // Adam steps per training step
   float learn_rate = 1e-3f;
+  int setup_threads = 0;      // host threads of one simulation's set-up (0: all)
 };
 
 class Sim {

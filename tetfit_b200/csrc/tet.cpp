@@ -23,6 +23,7 @@
 #include <stdexcept>
 
 #include "cuda_util.hpp"
+#include "host_parallel.hpp"
 #include "tet_group.hpp"
 
 namespace tf {
@@ -104,22 +105,68 @@ double tridiag_max(const std::vector<double>& a, const std::vector<double>& bf) 
 }
 }  // namespace
 
-HostCsr HostCsr::build(uint32_t nr, uint32_t nc, std::vector<Trip>& t) {
+// Triplets to CSR with duplicates summed.  Entries are bucketed by row in
+// their given order (a counting sort), then each row is sorted by column with
+// a stable sort: the same order as one stable sort by (row, column), so
+// duplicates are summed in the order they were given, for any thread count.
+HostCsr HostCsr::build(uint32_t nr, uint32_t nc, std::vector<Trip>& t, int threads) {
   HostCsr m;
   m.nrows = nr;
   m.ncols = nc;
-  std::stable_sort(t.begin(), t.end(), [](const Trip& a, const Trip& b) { return a.r != b.r ? a.r < b.r : a.c < b.c; });
-  m.ptr.assign(nr + 1, 0);
-  for (size_t k = 0; k < t.size(); k++) {
-    if (k > 0 && t[k].r == t[k - 1].r && t[k].c == t[k - 1].c) {
-      m.val.back() += t[k].v;
-      continue;
+  struct CV {
+    int32_t c;
+    double v;
+  };
+  // each thread owns a row range: it counts, then places, the entries of its
+  // rows (scanning all triplets in order keeps every row's order)
+  std::vector<int64_t> start(nr + 1, 0);
+  parallel_for(nr, threads, [&](int64_t r0, int64_t r1) {
+    for (const Trip& x : t)
+      if (x.r >= r0 && x.r < r1) start[x.r + 1]++;
+  });
+  for (uint32_t r = 0; r < nr; r++) start[r + 1] += start[r];
+  std::vector<CV> b(t.size());
+  parallel_for(nr, threads, [&](int64_t r0, int64_t r1) {
+    std::vector<int64_t> pos(start.begin() + r0, start.begin() + r1);
+    for (const Trip& x : t)
+      if (x.r >= r0 && x.r < r1) b[pos[x.r - r0]++] = {(int32_t)x.c, x.v};
+  });
+  std::vector<int64_t> cnt(nr + 1, 0);
+  parallel_for(nr, threads, [&](int64_t r0, int64_t r1) {
+    for (int64_t r = r0; r < r1; r++) {
+      const int64_t lo = start[r], hi = start[r + 1];
+      if (hi - lo <= 32) {
+        for (int64_t k = lo + 1; k < hi; k++) {  // insertion sort: stable
+          const CV e = b[k];
+          int64_t j = k;
+          while (j > lo && b[j - 1].c > e.c) {
+            b[j] = b[j - 1];
+            j--;
+          }
+          b[j] = e;
+        }
+      } else {
+        std::stable_sort(b.begin() + lo, b.begin() + hi, [](const CV& x, const CV& y) { return x.c < y.c; });
+      }
+      int64_t w = lo;
+      for (int64_t k = lo; k < hi; k++) {
+        if (w > lo && b[w - 1].c == b[k].c) b[w - 1].v += b[k].v;
+        else b[w++] = b[k];
+      }
+      cnt[r + 1] = w - lo;
     }
-    m.col.push_back((int32_t)t[k].c);
-    m.val.push_back(t[k].v);
-    m.ptr[t[k].r + 1]++;
-  }
-  for (uint32_t r = 0; r < nr; r++) m.ptr[r + 1] += m.ptr[r];
+  });
+  m.ptr.assign(nr + 1, 0);
+  for (uint32_t r = 0; r < nr; r++) m.ptr[r + 1] = m.ptr[r] + cnt[r + 1];
+  m.col.resize(m.ptr[nr]);
+  m.val.resize(m.ptr[nr]);
+  parallel_for(nr, threads, [&](int64_t r0, int64_t r1) {
+    for (int64_t r = r0; r < r1; r++)
+      for (int64_t k = 0; k < cnt[r + 1]; k++) {
+        m.col[m.ptr[r] + k] = b[start[r] + k].c;
+        m.val[m.ptr[r] + k] = b[start[r] + k].v;
+      }
+  });
   return m;
 }
 
@@ -346,7 +393,7 @@ void TetSim::read_mesh() {
       t.push_back({(uint32_t)fte_[f][1], f, -1.0});
       t.push_back({(uint32_t)fte_[f][2], f, 1.0});
     }
-    Ct_ = HostCsr::build(NE, NF, t);
+    Ct_ = HostCsr::build(NE, NF, t, opt_.setup_threads);
   }
   // boundary faces and their dual edges (Discretization.hpp:6380-6489)
   bnd_edge_.assign(NE, -1);
@@ -466,42 +513,51 @@ void TetSim::build_ops() {
     const auto &a = pts_[faces_[f][0]], &b = pts_[faces_[f][1]], &c = pts_[faces_[f][2]];
     return V3{(a[0] + b[0] + c[0]) / 3.0, (a[1] + b[1] + c[1]) / 3.0, (a[2] + b[2] + c[2]) / 3.0};
   };
-  // N = sum of per-tet inverse magnetic blocks (Discretization.hpp:8754-8807, 9158-9255)
+  const int nth = opt_.setup_threads;
+  // N = sum of per-tet inverse magnetic blocks (Discretization.hpp:8754-8807, 9158-9255);
+  // the blocks are formed in parallel, then listed in tet order
   {
+    std::vector<double> blk(16 * (size_t)L);
+    parallel_for(L, nth, [&](int64_t v0, int64_t v1) {
+      for (uint32_t v = (uint32_t)v0; v < (uint32_t)v1; v++) {
+        auto es = vol_edges(v);
+        V3 eb[6], fb[4];
+        for (int i = 0; i < 6; i++) eb[i] = ebar(es[i]);
+        for (int i = 0; i < 4; i++) fb[i] = fbar(vtf_[v][i]);
+        V3 vb{0, 0, 0};
+        for (int q = 0; q < 4; q++)
+          for (int a = 0; a < 3; a++) vb[a] += pts_[vols_[v][q]][a];
+        vb = {vb[0] / 4.0, vb[1] / 4.0, vb[2] / 4.0};
+        const double sgn = cell_vol_[v] < 0 ? -0.5 : 0.5;
+        const V3 fv[6] = {scale(cross(sub(vb, eb[0]), sub(fb[2], fb[3])), sgn),
+                          scale(cross(sub(vb, eb[1]), sub(fb[0], fb[3])), sgn),
+                          scale(cross(sub(vb, eb[2]), sub(fb[3], fb[1])), sgn),
+                          scale(cross(sub(vb, eb[3]), sub(fb[1], fb[2])), sgn),
+                          scale(cross(sub(vb, eb[4]), sub(fb[2], fb[0])), sgn),
+                          scale(cross(sub(vb, eb[5]), sub(fb[0], fb[1])), sgn)};
+        const Mat3& mu = sc_.materials.at(vol_mat_[v]).mu;
+        auto d = [&](int a, int b) { return dot(fv[a], mv(mu, fv[b])); };
+        const double c = 36.0 / std::fabs(cell_vol_[v]);
+        std::vector<double> M = {(d(0, 0) + d(2, 2) + d(3, 3)) * c, (-d(1, 2) - d(3, 4)) * c,
+                                 (-d(0, 1) + d(3, 5)) * c,          (d(0, 4) + d(2, 5)) * c,
+                                 0, (d(0, 0) + d(1, 1) + d(4, 4)) * c, (-d(0, 2) - d(4, 5)) * c, (d(0, 3) - d(1, 5)) * c,
+                                 0, 0, (d(1, 1) + d(2, 2) + d(5, 5)) * c, (-d(2, 3) - d(1, 4)) * c,
+                                 0, 0, 0, (d(3, 3) + d(4, 4) + d(5, 5)) * c};
+        for (int i = 0; i < 4; i++)
+          for (int j = 0; j < i; j++) M[4 * i + j] = M[4 * j + i];
+        spd_inv(M, 4);
+        std::copy(M.begin(), M.end(), blk.begin() + 16 * (size_t)v);
+      }
+    });
     std::vector<HostCsr::Trip> t;
     t.reserve(16 * (size_t)L);
-    for (uint32_t v = 0; v < L; v++) {
-      auto es = vol_edges(v);
-      V3 eb[6], fb[4];
-      for (int i = 0; i < 6; i++) eb[i] = ebar(es[i]);
-      for (int i = 0; i < 4; i++) fb[i] = fbar(vtf_[v][i]);
-      V3 vb{0, 0, 0};
-      for (int q = 0; q < 4; q++)
-        for (int a = 0; a < 3; a++) vb[a] += pts_[vols_[v][q]][a];
-      vb = {vb[0] / 4.0, vb[1] / 4.0, vb[2] / 4.0};
-      const double sgn = cell_vol_[v] < 0 ? -0.5 : 0.5;
-      const V3 fv[6] = {scale(cross(sub(vb, eb[0]), sub(fb[2], fb[3])), sgn),
-                        scale(cross(sub(vb, eb[1]), sub(fb[0], fb[3])), sgn),
-                        scale(cross(sub(vb, eb[2]), sub(fb[3], fb[1])), sgn),
-                        scale(cross(sub(vb, eb[3]), sub(fb[1], fb[2])), sgn),
-                        scale(cross(sub(vb, eb[4]), sub(fb[2], fb[0])), sgn),
-                        scale(cross(sub(vb, eb[5]), sub(fb[0], fb[1])), sgn)};
-      const Mat3& mu = sc_.materials.at(vol_mat_[v]).mu;
-      auto d = [&](int a, int b) { return dot(fv[a], mv(mu, fv[b])); };
-      const double c = 36.0 / std::fabs(cell_vol_[v]);
-      std::vector<double> M = {(d(0, 0) + d(2, 2) + d(3, 3)) * c, (-d(1, 2) - d(3, 4)) * c,
-                               (-d(0, 1) + d(3, 5)) * c,          (d(0, 4) + d(2, 5)) * c,
-                               0, (d(0, 0) + d(1, 1) + d(4, 4)) * c, (-d(0, 2) - d(4, 5)) * c, (d(0, 3) - d(1, 5)) * c,
-                               0, 0, (d(1, 1) + d(2, 2) + d(5, 5)) * c, (-d(2, 3) - d(1, 4)) * c,
-                               0, 0, 0, (d(3, 3) + d(4, 4) + d(5, 5)) * c};
-      for (int i = 0; i < 4; i++)
-        for (int j = 0; j < i; j++) M[4 * i + j] = M[4 * j + i];
-      spd_inv(M, 4);
+    for (uint32_t v = 0; v < L; v++)
       for (int j = 0; j < 4; j++)
-        for (int k = 0; k < 4; k++)
-          if (M[4 * j + k] != 0) t.push_back({(uint32_t)vtf_[v][j], (uint32_t)vtf_[v][k], M[4 * j + k]});
-    }
-    N_ = HostCsr::build(NF, NF, t);
+        for (int k = 0; k < 4; k++) {
+          const double x = blk[16 * (size_t)v + 4 * j + k];
+          if (x != 0) t.push_back({(uint32_t)vtf_[v][j], (uint32_t)vtf_[v][k], x});
+        }
+    N_ = HostCsr::build(NF, NF, t, nth);
   }
   auto primal_area = [&](uint32_t v) {
     const auto& n = vols_[v];
@@ -517,93 +573,112 @@ void TetSim::build_ops() {
     static const int kFv[4][3] = {{1, 2, 3}, {0, 2, 3}, {1, 0, 3}, {0, 1, 2}};
     static const double kSg[4][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {1, 1, 1}};
     static const int kVtfSign[4] = {1, -1, 1, -1};  // vtf signs (Discretization.hpp:6239-6267)
+    // node stars in parallel, each into its own lists, then concatenated in
+    // node order (the order a sequential pass would list them)
+    const size_t NP = pts_.size();
+    std::vector<std::vector<HostCsr::Trip>> ein_n(NP), h_n(NP);
+    parallel_for((int64_t)NP, nth, [&](int64_t n0, int64_t n1) {
+      for (uint32_t nid = (uint32_t)n0; nid < (uint32_t)n1; nid++) {
+        std::vector<HostCsr::Trip>& einv_t = ein_n[nid];
+        std::vector<HostCsr::Trip>& h_t = h_n[nid];
+        const int64_t b0 = star_ptr_[nid];
+        const int n = (int)(star_ptr_[nid + 1] - b0);
+        std::vector<double> E(n * n, 0.0);
+        for (int64_t q = nvol_ptr_[nid]; q < nvol_ptr_[nid + 1]; q++) {
+          const int32_t vv = nvol_[q];
+          auto el = vol_edges(vv);
+          auto fv = primal_area(vv);
+          const double V = std::fabs(cell_vol_[vv]);
+          const Mat3& eps = sc_.materials.at(vol_mat_[vv]).eps;
+          int k = 0;
+          while (vols_[vv][k] != (int32_t)nid) k++;
+          int li[3];
+          V3 w[3];
+          for (int a = 0; a < 3; a++) {
+            li[a] = (int)(std::lower_bound(star_edge_.begin() + b0, star_edge_.begin() + b0 + n, el[kEd[k][a]]) -
+                          (star_edge_.begin() + b0));
+            w[a] = scale(fv[kFv[k][a]], kSg[k][a] * 2.0 / 3.0 / V * kVtfSign[kFv[k][a]]);
+          }
+          for (int a = 0; a < 3; a++)
+            for (int b = a; b < 3; b++) {
+              double val = dot(w[a], mv(eps, w[b])) * V / 4;
+              E[li[a] * n + li[b]] += val;
+              if (a != b) E[li[b] * n + li[a]] = E[li[a] * n + li[b]];
+            }
+        }
+        std::vector<double> Hl = E;
+        spd_inv(Hl, n);
+        for (int j = 0; j < n; j++)
+          for (int k = j; k < n; k++)
+            if (Hl[j * n + k] != 0) {
+              einv_t.push_back({(uint32_t)star_edge_[b0 + j], (uint32_t)star_edge_[b0 + k], Hl[j * n + k]});
+              if (j != k) einv_t.push_back({(uint32_t)star_edge_[b0 + k], (uint32_t)star_edge_[b0 + j], Hl[j * n + k]});
+            }
+        // masked inverse (Discretization.hpp:9263-9333)
+        for (int j = 0; j < n; j++)
+          if (cls_[star_edge_[b0 + j]] == 4) {
+            for (int k = 0; k < n; k++) E[j * n + k] = E[k * n + j] = 0;
+            E[j * n + j] = 1;
+          }
+        spd_inv(E, n);
+        for (int j = 0; j < n; j++) {
+          const int32_t ej = star_edge_[b0 + j];
+          if (cls_[ej] != 1) continue;
+          for (int k = j; k < n; k++) {
+            const int32_t ek = star_edge_[b0 + k];
+            if (cls_[ek] == 4 || E[j * n + k] == 0) continue;
+            h_t.push_back({(uint32_t)ej, (uint32_t)ek, E[j * n + k]});
+            if (j != k) h_t.push_back({(uint32_t)ek, (uint32_t)ej, E[j * n + k]});
+          }
+        }
+      }
+    });
     std::vector<HostCsr::Trip> einv_t, h_t;
-    for (uint32_t nid = 0; nid < pts_.size(); nid++) {
-      const int64_t b0 = star_ptr_[nid];
-      const int n = (int)(star_ptr_[nid + 1] - b0);
-      std::vector<double> E(n * n, 0.0);
-      for (int64_t q = nvol_ptr_[nid]; q < nvol_ptr_[nid + 1]; q++) {
-        const int32_t vv = nvol_[q];
-        auto el = vol_edges(vv);
-        auto fv = primal_area(vv);
-        const double V = std::fabs(cell_vol_[vv]);
-        const Mat3& eps = sc_.materials.at(vol_mat_[vv]).eps;
-        int k = 0;
-        while (vols_[vv][k] != (int32_t)nid) k++;
-        int li[3];
-        V3 w[3];
-        for (int a = 0; a < 3; a++) {
-          li[a] = (int)(std::lower_bound(star_edge_.begin() + b0, star_edge_.begin() + b0 + n, el[kEd[k][a]]) -
-                        (star_edge_.begin() + b0));
-          w[a] = scale(fv[kFv[k][a]], kSg[k][a] * 2.0 / 3.0 / V * kVtfSign[kFv[k][a]]);
-        }
-        for (int a = 0; a < 3; a++)
-          for (int b = a; b < 3; b++) {
-            double val = dot(w[a], mv(eps, w[b])) * V / 4;
-            E[li[a] * n + li[b]] += val;
-            if (a != b) E[li[b] * n + li[a]] = E[li[a] * n + li[b]];
-          }
-      }
-      std::vector<double> Hl = E;
-      spd_inv(Hl, n);
-      for (int j = 0; j < n; j++)
-        for (int k = j; k < n; k++)
-          if (Hl[j * n + k] != 0) {
-            einv_t.push_back({(uint32_t)star_edge_[b0 + j], (uint32_t)star_edge_[b0 + k], Hl[j * n + k]});
-            if (j != k) einv_t.push_back({(uint32_t)star_edge_[b0 + k], (uint32_t)star_edge_[b0 + j], Hl[j * n + k]});
-          }
-      // masked inverse (Discretization.hpp:9263-9333)
-      for (int j = 0; j < n; j++)
-        if (cls_[star_edge_[b0 + j]] == 4) {
-          for (int k = 0; k < n; k++) E[j * n + k] = E[k * n + j] = 0;
-          E[j * n + j] = 1;
-        }
-      spd_inv(E, n);
-      for (int j = 0; j < n; j++) {
-        const int32_t ej = star_edge_[b0 + j];
-        if (cls_[ej] != 1) continue;
-        for (int k = j; k < n; k++) {
-          const int32_t ek = star_edge_[b0 + k];
-          if (cls_[ek] == 4 || E[j * n + k] == 0) continue;
-          h_t.push_back({(uint32_t)ej, (uint32_t)ek, E[j * n + k]});
-          if (j != k) h_t.push_back({(uint32_t)ek, (uint32_t)ej, E[j * n + k]});
-        }
-      }
+    for (size_t nid = 0; nid < NP; nid++) {
+      einv_t.insert(einv_t.end(), ein_n[nid].begin(), ein_n[nid].end());
+      h_t.insert(h_t.end(), h_n[nid].begin(), h_n[nid].end());
+      std::vector<HostCsr::Trip>().swap(ein_n[nid]);
+      std::vector<HostCsr::Trip>().swap(h_n[nid]);
     }
-    HostCsr Einv = HostCsr::build(NE, NE, einv_t);
-    H_ = HostCsr::build(NE, NE, h_t);
+    HostCsr Einv = HostCsr::build(NE, NE, einv_t, nth);
+    H_ = HostCsr::build(NE, NE, h_t, nth);
     dt_est_ = sim_.courant * estimate_dt(Einv, false);
   } else {
-    // gfdtd eps-mass from the node dual bases (Discretization.hpp:8357-8621)
-    std::vector<HostCsr::Trip> t;
-    for (uint32_t nid = 0; nid < pts_.size(); nid++)
-      for (int64_t q = nvol_ptr_[nid]; q < nvol_ptr_[nid + 1]; q++) {
-        const int32_t vv = nvol_[q];
-        auto el = vol_edges(vv);
-        const double om = std::fabs(cell_vol_[vv]) / 4.0;
-        const Mat3& eps = sc_.materials.at(vol_mat_[vv]).eps;
-        int k = 0;
-        while (vols_[vv][k] != (int32_t)nid) k++;
-        int32_t e[3] = {el[kEd[k][0]], el[kEd[k][1]], el[kEd[k][2]]};
-        V3 a1 = sub(ebar(e[0]), pts_[nid]), a2 = sub(ebar(e[1]), pts_[nid]), a3 = sub(ebar(e[2]), pts_[nid]);
-        const double nc = std::pow(dot(a1, cross(a2, a3)), -1);
-        const V3 f[3] = {scale(cross(a2, a3), nc), scale(cross(a3, a1), nc), scale(cross(a1, a2), nc)};
-        Mat3 oe;
-        for (int i = 0; i < 3; i++)
-          for (int j = 0; j < 3; j++) oe.m[i][j] = om * eps.m[i][j];
-        // reference form: half-edge duals, no 1/4, no orientation signs;
-        // consistent form: both applied
-        double sg[3] = {1, 1, 1}, quarter = 1;
-        if (opt_.consistent_mass) {
-          for (int a = 0; a < 3; a++) sg[a] = edges_[e[a]][1] == (int32_t)nid ? -1.0 : 1.0;
-          quarter = 0.25;
+    // gfdtd eps-mass from the node dual bases (Discretization.hpp:8357-8621):
+    // nine entries per (node, tet) pair at fixed positions, formed in parallel
+    std::vector<HostCsr::Trip> t(9 * nvol_.size());
+    parallel_for((int64_t)pts_.size(), nth, [&](int64_t n0, int64_t n1) {
+      for (uint32_t nid = (uint32_t)n0; nid < (uint32_t)n1; nid++)
+        for (int64_t q = nvol_ptr_[nid]; q < nvol_ptr_[nid + 1]; q++) {
+          const int32_t vv = nvol_[q];
+          auto el = vol_edges(vv);
+          const double om = std::fabs(cell_vol_[vv]) / 4.0;
+          const Mat3& eps = sc_.materials.at(vol_mat_[vv]).eps;
+          int k = 0;
+          while (vols_[vv][k] != (int32_t)nid) k++;
+          int32_t e[3] = {el[kEd[k][0]], el[kEd[k][1]], el[kEd[k][2]]};
+          V3 a1 = sub(ebar(e[0]), pts_[nid]), a2 = sub(ebar(e[1]), pts_[nid]), a3 = sub(ebar(e[2]), pts_[nid]);
+          const double nc = std::pow(dot(a1, cross(a2, a3)), -1);
+          const V3 f[3] = {scale(cross(a2, a3), nc), scale(cross(a3, a1), nc), scale(cross(a1, a2), nc)};
+          Mat3 oe;
+          for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) oe.m[i][j] = om * eps.m[i][j];
+          // reference form: half-edge duals, no 1/4, no orientation signs;
+          // consistent form: both applied
+          double sg[3] = {1, 1, 1}, quarter = 1;
+          if (opt_.consistent_mass) {
+            for (int a = 0; a < 3; a++) sg[a] = edges_[e[a]][1] == (int32_t)nid ? -1.0 : 1.0;
+            quarter = 0.25;
+          }
+          static const int kPair[9][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {1, 0}, {0, 2}, {2, 0}, {1, 2}, {2, 1}};
+          for (int k2 = 0; k2 < 9; k2++) {
+            const int* pq = kPair[k2];
+            t[9 * q + k2] = {(uint32_t)e[pq[0]], (uint32_t)e[pq[1]],
+                             quarter * sg[pq[0]] * sg[pq[1]] * dot(f[pq[0]], mv(oe, f[pq[1]]))};
+          }
         }
-        static const int kPair[9][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {1, 0}, {0, 2}, {2, 0}, {1, 2}, {2, 1}};
-        for (auto& pq : kPair)
-          t.push_back({(uint32_t)e[pq[0]], (uint32_t)e[pq[1]],
-                       quarter * sg[pq[0]] * sg[pq[1]] * dot(f[pq[0]], mv(oe, f[pq[1]]))});
-      }
-    E_ = HostCsr::build(NE, NE, t);
+    });
+    E_ = HostCsr::build(NE, NE, t, nth);
     std::vector<int32_t> fidx(NE, -1);
     for (uint32_t e = 0; e < NE; e++) {
       if (cls_[e] != 4) {
@@ -623,8 +698,8 @@ void TetSim::build_ops() {
       }
     }
     const uint32_t nf = (uint32_t)free_edges_.size();
-    A_ = HostCsr::build(nf, nf, at);
-    R_ = HostCsr::build(nf, NE, rt);
+    A_ = HostCsr::build(nf, nf, at, nth);
+    R_ = HostCsr::build(nf, NE, rt, nth);
     jacobi_.resize(nf);
     for (uint32_t i = 0; i < nf; i++) {
       double dg = 0;
@@ -742,7 +817,25 @@ void TetSim::locate_probes() {
   std::vector<uint8_t> colour(L, 0);
   std::vector<uint32_t> touched;
   uint32_t root = 0;
+  // A point outside the mesh's bounding box by more than 1e-3 of its largest
+  // extent lies in no tet: the containment test below fails there (the
+  // sub-tet volumes are far beyond its 1e-12 tolerance), so the walk, which
+  // would visit every tet before giving up, is skipped.  Nearer points take
+  // the walk as before.
+  V3 lo{1e300, 1e300, 1e300}, hi{-1e300, -1e300, -1e300};
+  for (const auto& q : pts_)
+    for (int a = 0; a < 3; a++) {
+      lo[a] = std::min(lo[a], q[a]);
+      hi[a] = std::max(hi[a], q[a]);
+    }
+  const double margin = 1e-3 * std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], 0.0});
+  auto outside = [&](const std::array<double, 3>& pv) {
+    for (int a = 0; a < 3; a++)
+      if (pv[a] < lo[a] - margin || pv[a] > hi[a] + margin) return true;
+    return false;
+  };
   auto find = [&](const std::array<double, 3>& pv) -> int64_t {
+    if (L == 0 || outside(pv)) return -1;
     for (uint32_t t : touched) colour[t] = 0;
     touched.clear();
     std::vector<uint32_t> q{root};

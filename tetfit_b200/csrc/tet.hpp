@@ -29,7 +29,8 @@ struct HostCsr {
     uint32_t r, c;
     double v;
   };
-  static HostCsr build(uint32_t nr, uint32_t nc, std::vector<Trip>& t);
+  // threads: host threads for the per-row work (<= 0: all)
+  static HostCsr build(uint32_t nr, uint32_t nc, std::vector<Trip>& t, int threads = 1);
   void mul(const double* x, double* y) const;
 };
 
