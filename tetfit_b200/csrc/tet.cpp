@@ -282,7 +282,8 @@ void TetSim::read_mesh() {
     std::sort(q.begin(), q.end());
     if (m != 7) tt.push_back({q[0], q[1], q[2], q[3], m});
   }
-  std::stable_sort(tt.begin(), tt.end(), [](const auto& a, const auto& b) {
+  const int nth = opt_.setup_threads;
+  parallel_stable_sort(tt.begin(), tt.end(), nth, [](const auto& a, const auto& b) {
     return std::lexicographical_compare(a.begin(), a.begin() + 4, b.begin(), b.begin() + 4);
   });
   const uint32_t L = (uint32_t)tt.size();
@@ -316,9 +317,11 @@ void TetSim::read_mesh() {
       if (!packed) ftup[slot] = {tri[q][0], tri[q][1], tri[q][2]};
     }
   }
-  if (packed) std::sort(fk.begin(), fk.end());
+  // (key, slot) pairs are distinct: any sort gives this order
+  if (packed) parallel_stable_sort(fk.begin(), fk.end(), nth, std::less<std::pair<uint64_t, uint32_t>>());
   else
-    std::stable_sort(fk.begin(), fk.end(), [&](const auto& a, const auto& b) { return ftup[a.first] < ftup[b.first]; });
+    parallel_stable_sort(fk.begin(), fk.end(), nth,
+                         [&](const auto& a, const auto& b) { return ftup[a.first] < ftup[b.first]; });
   std::vector<int32_t> flab(4 * (size_t)L);
   auto face_tuple = [&](size_t slot) -> std::array<int32_t, 3> {
     uint32_t k = (uint32_t)(slot % L);
@@ -354,13 +357,15 @@ void TetSim::read_mesh() {
     ek[f + 2 * (size_t)NF] = ((uint64_t)s[1] << 32) | (uint32_t)s[2];
   }
   std::vector<uint64_t> eu(ek);
-  std::sort(eu.begin(), eu.end());
+  parallel_stable_sort(eu.begin(), eu.end(), nth, std::less<uint64_t>());
   eu.erase(std::unique(eu.begin(), eu.end()), eu.end());
   edges_.resize(eu.size());
   for (size_t e = 0; e < eu.size(); e++) edges_[e] = {(int32_t)(eu[e] >> 32), (int32_t)(eu[e] & 0xffffffffu)};
   auto eid = [&](uint64_t key) { return (int32_t)(std::lower_bound(eu.begin(), eu.end(), key) - eu.begin()); };
   fte_.resize(NF);
-  for (uint32_t f = 0; f < NF; f++) fte_[f] = {eid(ek[f]), eid(ek[f + NF]), eid(ek[f + 2 * (size_t)NF])};
+  parallel_for(NF, nth, [&](int64_t f0, int64_t f1) {
+    for (int64_t f = f0; f < f1; f++) fte_[f] = {eid(ek[f]), eid(ek[f + NF]), eid(ek[f + 2 * (size_t)NF])};
+  });
   const uint32_t NE = (uint32_t)edges_.size();
   // node stars (edges ascending) and node -> tets (ascending)
   star_ptr_.assign(np + 1, 0);
@@ -393,7 +398,7 @@ void TetSim::read_mesh() {
       t.push_back({(uint32_t)fte_[f][1], f, -1.0});
       t.push_back({(uint32_t)fte_[f][2], f, 1.0});
     }
-    Ct_ = HostCsr::build(NE, NF, t, opt_.setup_threads);
+    Ct_ = HostCsr::build(NE, NF, t, nth);
   }
   // boundary faces and their dual edges (Discretization.hpp:6380-6489)
   bnd_edge_.assign(NE, -1);
@@ -549,14 +554,24 @@ void TetSim::build_ops() {
         std::copy(M.begin(), M.end(), blk.begin() + 16 * (size_t)v);
       }
     });
-    std::vector<HostCsr::Trip> t;
-    t.reserve(16 * (size_t)L);
-    for (uint32_t v = 0; v < L; v++)
-      for (int j = 0; j < 4; j++)
-        for (int k = 0; k < 4; k++) {
-          const double x = blk[16 * (size_t)v + 4 * j + k];
-          if (x != 0) t.push_back({(uint32_t)vtf_[v][j], (uint32_t)vtf_[v][k], x});
-        }
+    // nonzero entries in tet order, at positions from a prefix of the counts
+    std::vector<int64_t> off(L + 1, 0);
+    parallel_for(L, nth, [&](int64_t v0, int64_t v1) {
+      for (int64_t v = v0; v < v1; v++)
+        for (int k = 0; k < 16; k++) off[v + 1] += blk[16 * v + k] != 0;
+    });
+    for (uint32_t v = 0; v < L; v++) off[v + 1] += off[v];
+    std::vector<HostCsr::Trip> t(off[L]);
+    parallel_for(L, nth, [&](int64_t v0, int64_t v1) {
+      for (int64_t v = v0; v < v1; v++) {
+        int64_t w = off[v];
+        for (int j = 0; j < 4; j++)
+          for (int k = 0; k < 4; k++) {
+            const double x = blk[16 * v + 4 * j + k];
+            if (x != 0) t[w++] = {(uint32_t)vtf_[v][j], (uint32_t)vtf_[v][k], x};
+          }
+      }
+    });
     N_ = HostCsr::build(NF, NF, t, nth);
   }
   auto primal_area = [&](uint32_t v) {
@@ -688,18 +703,45 @@ void TetSim::build_ops() {
         dir_edges_.push_back((int32_t)e);
       }
     }
-    std::vector<HostCsr::Trip> at, rt;
-    for (uint32_t r = 0; r < NE; r++) {
-      if (fidx[r] < 0) continue;
-      for (int64_t k = E_.ptr[r]; k < E_.ptr[r + 1]; k++) {
-        const int32_t c = E_.col[k];
-        if (fidx[c] < 0) rt.push_back({(uint32_t)fidx[r], (uint32_t)c, E_.val[k]});
-        else at.push_back({(uint32_t)fidx[r], (uint32_t)fidx[c], E_.val[k]});
-      }
-    }
+    // A (free x free) and R (free x Dirichlet) split the rows of E.  The free
+    // numbering fidx is increasing in the edge index, so each split row keeps
+    // E's sorted, merged column order: the rows are copied, not re-sorted.
     const uint32_t nf = (uint32_t)free_edges_.size();
-    A_ = HostCsr::build(nf, nf, at, nth);
-    R_ = HostCsr::build(nf, NE, rt, nth);
+    A_.nrows = A_.ncols = nf;
+    R_.nrows = nf;
+    R_.ncols = NE;
+    A_.ptr.assign(nf + 1, 0);
+    R_.ptr.assign(nf + 1, 0);
+    parallel_for(nf, nth, [&](int64_t i0, int64_t i1) {
+      for (int64_t i = i0; i < i1; i++) {
+        const int32_t r = free_edges_[i];
+        for (int64_t k = E_.ptr[r]; k < E_.ptr[r + 1]; k++) (fidx[E_.col[k]] < 0 ? R_.ptr[i + 1] : A_.ptr[i + 1])++;
+      }
+    });
+    for (uint32_t i = 0; i < nf; i++) {
+      A_.ptr[i + 1] += A_.ptr[i];
+      R_.ptr[i + 1] += R_.ptr[i];
+    }
+    A_.col.resize(A_.ptr[nf]);
+    A_.val.resize(A_.ptr[nf]);
+    R_.col.resize(R_.ptr[nf]);
+    R_.val.resize(R_.ptr[nf]);
+    parallel_for(nf, nth, [&](int64_t i0, int64_t i1) {
+      for (int64_t i = i0; i < i1; i++) {
+        const int32_t r = free_edges_[i];
+        int64_t wa = A_.ptr[i], wr = R_.ptr[i];
+        for (int64_t k = E_.ptr[r]; k < E_.ptr[r + 1]; k++) {
+          const int32_t c = E_.col[k];
+          if (fidx[c] < 0) {
+            R_.col[wr] = c;
+            R_.val[wr++] = E_.val[k];
+          } else {
+            A_.col[wa] = fidx[c];
+            A_.val[wa++] = E_.val[k];
+          }
+        }
+      }
+    });
     jacobi_.resize(nf);
     for (uint32_t i = 0; i < nf; i++) {
       double dg = 0;
@@ -817,40 +859,70 @@ void TetSim::locate_probes() {
   std::vector<uint8_t> colour(L, 0);
   std::vector<uint32_t> touched;
   uint32_t root = 0;
-  // A point outside the mesh's bounding box by more than 1e-3 of its largest
-  // extent lies in no tet: the containment test below fails there (the
-  // sub-tet volumes are far beyond its 1e-12 tolerance), so the walk, which
-  // would visit every tet before giving up, is skipped.  Nearer points take
-  // the walk as before.
-  V3 lo{1e300, 1e300, 1e300}, hi{-1e300, -1e300, -1e300};
-  for (const auto& q : pts_)
-    for (int a = 0; a < 3; a++) {
-      lo[a] = std::min(lo[a], q[a]);
-      hi[a] = std::max(hi[a], q[a]);
+  const double tol = 1e-12;
+  // Exact pre-test.  The walk below accepts tet v when every barycentric
+  // coordinate d1_r / d0 of the point is >= -tol / |d0|.  A point beyond the
+  // tet's bounding box by delta along an axis of extent `ext` has negative
+  // coordinates summing to at most -delta / ext, so one of them (at most three
+  // are negative) is <= -delta / (3 ext): it cannot pass once delta exceeds
+  // 3 ext tol / |d0|.  Each tet's box is widened by 4 ext (2 tol) / |d0|
+  // (twice the tolerance covers the rounding of the determinants) and stored
+  // rounded outwards; a point outside it skips the determinants, with the same
+  // outcome, and a point outside every box skips the walk.  Near-degenerate
+  // tets (|d0| <= tol) get an unbounded box.
+  std::vector<float> box(6 * (size_t)L);
+  parallel_for(L, opt_.setup_threads, [&](int64_t v0, int64_t v1) {
+    for (int64_t v = v0; v < v1; v++) {
+      double rows[4][4], lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+      for (int r = 0; r < 4; r++) {
+        for (int a = 0; a < 3; a++) {
+          rows[r][a] = pts_[vols_[v][r]][a];
+          lo[a] = std::min(lo[a], rows[r][a]);
+          hi[a] = std::max(hi[a], rows[r][a]);
+        }
+        rows[r][3] = 1;
+      }
+      const double d0 = std::fabs(det4(rows));
+      const double ext = std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]});
+      const bool open = !(d0 > tol) || !std::isfinite(d0);
+      const double m = open ? 0.0 : 4.0 * ext * (2.0 * tol) / d0;
+      for (int a = 0; a < 3; a++) {
+        float l = open ? -INFINITY : (float)(lo[a] - m), h = open ? INFINITY : (float)(hi[a] + m);
+        if (!open && (double)l > lo[a] - m) l = std::nextafter(l, -INFINITY);
+        if (!open && (double)h < hi[a] + m) h = std::nextafter(h, INFINITY);
+        box[6 * v + a] = l;
+        box[6 * v + 3 + a] = h;
+      }
     }
-  const double margin = 1e-3 * std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], 0.0});
-  auto outside = [&](const std::array<double, 3>& pv) {
+  });
+  float glo[3] = {INFINITY, INFINITY, INFINITY}, ghi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (size_t v = 0; v < L; v++)
+    for (int a = 0; a < 3; a++) {
+      glo[a] = std::min(glo[a], box[6 * v + a]);
+      ghi[a] = std::max(ghi[a], box[6 * v + 3 + a]);
+    }
+  auto in_box = [](const float* bx, const std::array<double, 3>& pv) {
     for (int a = 0; a < 3; a++)
-      if (pv[a] < lo[a] - margin || pv[a] > hi[a] + margin) return true;
-    return false;
+      if (pv[a] < (double)bx[a] || pv[a] > (double)bx[3 + a]) return false;
+    return true;
   };
+  const float gbox[6] = {glo[0], glo[1], glo[2], ghi[0], ghi[1], ghi[2]};
   auto find = [&](const std::array<double, 3>& pv) -> int64_t {
-    if (L == 0 || outside(pv)) return -1;
+    if (L == 0 || !in_box(gbox, pv)) return -1;
     for (uint32_t t : touched) colour[t] = 0;
     touched.clear();
     std::vector<uint32_t> q{root};
     colour[0] = 1;
     touched.push_back(0);
-    const double tol = 1e-12;
     for (size_t h = 0; h < q.size(); h++) {
       const uint32_t v = q[h];
+      bool ok = in_box(&box[6 * (size_t)v], pv);
       double rows[4][4];
       for (int r = 0; r < 4; r++) {
         for (int a = 0; a < 3; a++) rows[r][a] = pts_[vols_[v][r]][a];
         rows[r][3] = 1;
       }
-      const double d0 = det4(rows);
-      bool ok = true;
+      const double d0 = ok ? det4(rows) : 0.0;
       for (int r = 0; r < 4 && ok; r++) {
         double m[4][4];
         std::memcpy(m, rows, sizeof(m));
