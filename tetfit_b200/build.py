@@ -1,4 +1,5 @@
-"""Build recipe for libtetfit_b200.so (sm_100a, in-tree).
+"""Build recipe for libtetfit_b200.so (sm_100a, in-tree) and the `tetfit`
+command-line driver linked against it.
 
     python -m tetfit_b200.build
 """
@@ -11,6 +12,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libtetfit_b200.so")
+CLI = os.path.join(HERE, "tetfit")
+CLI_SOURCE = os.path.join(CSRC, "tetfit_main.cpp")
 SOURCES = ["script.cpp", "fit.cpp", "fit_kernels.cu", "tet.cpp", "tet_kernels.cu", "tet_group.cpp",
            "tet_group_kernels.cu", "mlp.cu", "pcg.cu", "barrier_check.cu", "capi.cpp", "capi_batch.cpp"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
@@ -30,15 +33,29 @@ def needs_build() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not needs_build():
-        return OUT
-    nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc] + NVCC_FLAGS + sources() + ["-o", OUT + ".tmp"]
+def build_cli(verbose: bool = False) -> str:
+    """`tetfit` driver: links libtetfit_b200.so from its own folder."""
+    cxx = os.environ.get("CXX", "g++")
+    cmd = [cxx, "-O2", "-std=c++17", CLI_SOURCE, "-o", CLI + ".tmp", "-L" + HERE, "-l:libtetfit_b200.so",
+           "-Wl,-rpath,$ORIGIN"]
     if verbose:
         print(" ".join(cmd))
-    subprocess.run(cmd, check=True, cwd=CSRC)
-    os.replace(OUT + ".tmp", OUT)
+    subprocess.run(cmd, check=True, cwd=HERE)
+    os.replace(CLI + ".tmp", CLI)
+    return CLI
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if force or needs_build():
+        nvcc = os.environ.get("NVCC", "nvcc")
+        cmd = [nvcc] + NVCC_FLAGS + sources() + ["-o", OUT + ".tmp"]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True, cwd=CSRC)
+        os.replace(OUT + ".tmp", OUT)
+    if force or not os.path.exists(CLI) or os.path.getmtime(CLI) < max(os.path.getmtime(OUT),
+                                                                        os.path.getmtime(CLI_SOURCE)):
+        build_cli(verbose)
     return OUT
 
 
