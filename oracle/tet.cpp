@@ -1,6 +1,7 @@
 // ORACLE — test infrastructure only.
 // FP64 CPU restatement of TetFIT's tetrahedral paths:
 //   netgen reader + numbering   src/DGA/Discretization.hpp:5868-6926, unique :10173-10299
+//   gmsh conversion             Discretization.hpp:5692-5866, Utilities.hpp:159-223
 //   geometry helpers            Discretization.hpp:10301-10545
 //   dga operators               ConstructCodecasaMaterialMatrices :8694-9513
 //   gfdtd operators             ConstructGFDTDMaterialMatrices   :8132-8692
@@ -171,14 +172,70 @@ std::array<double, 3> TetOracle::vol_bar(uint32_t v) const {
   return {r[0] / 4.0, r[1] / 4.0, r[2] / 4.0};
 }
 
+// ConvertFromGMSH (Discretization.hpp:5692-5866) with the element parser of
+// Utilities.hpp:159-223, restated: skip 4 lines, node count, "id x y z" per
+// node, skip 2 lines, element count, then per element "id type ntags t1 t2
+// nodes" (two tags taken as given).  Tetrahedra (type 4) keep the first tag as
+// material and their sorted nodes, triangles (type 2) the first tag as
+// boundary id.  The result is the netgen text the reference writes to a
+// temporary file: coordinates through a default ostream (6 significant
+// digits), tetrahedra sorted, triangles in file order.
+static std::string gmsh_as_netgen(std::istream& in) {
+  std::string ln;
+  for (int k = 0; k < 4; k++) std::getline(in, ln);
+  std::getline(in, ln);
+  const uint32_t np = (uint32_t)std::stoul(ln);
+  std::ostringstream os;
+  os << np << "\n";
+  for (uint32_t i = 0; i < np; i++) {
+    std::getline(in, ln);
+    std::istringstream ls(ln);
+    double id, x, y, z;
+    ls >> id >> x >> y >> z;
+    os << x << " " << y << " " << z << "\n";
+  }
+  std::getline(in, ln);
+  std::getline(in, ln);
+  std::getline(in, ln);
+  const uint32_t ne = (uint32_t)std::stoul(ln);
+  std::vector<std::pair<std::array<uint32_t, 4>, uint32_t>> tet;
+  std::vector<std::array<uint32_t, 4>> tri;
+  for (uint32_t i = 0; i < ne; i++) {
+    std::getline(in, ln);
+    std::istringstream ls(ln);
+    uint32_t id, type, ntag, t1, t2;
+    ls >> id >> type;
+    if (type != 4 && type != 2) continue;
+    ls >> ntag >> t1 >> t2;
+    std::array<uint32_t, 4> n{0, 0, 0, 0};
+    for (uint32_t j = 0; j < (type == 4 ? 4u : 3u); j++) ls >> n[j];
+    if (type == 4) {
+      std::sort(n.begin(), n.end());
+      tet.push_back({n, t1});
+    } else {
+      tri.push_back({t1, n[0], n[1], n[2]});
+    }
+  }
+  std::stable_sort(tet.begin(), tet.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+  os << tet.size() << "\n";
+  for (auto& t : tet) os << t.second << " " << t.first[0] << " " << t.first[1] << " " << t.first[2] << " " << t.first[3] << "\n";
+  os << tri.size() << "\n";
+  for (auto& t : tri) os << t[0] << " " << t[1] << " " << t[2] << " " << t[3] << "\n";
+  return os.str();
+}
+
 void TetOracle::read_mesh() {
   const Mesh& msh = sc.meshes[sim.mesh];
-  if (msh.mesher == "gmsh") throw std::runtime_error("gmsh meshes are outside the supported path");
   std::ifstream f(msh.file.c_str(), std::ios::binary);
   if (!f.is_open()) throw ScriptError("Invalid mesh file name");
-  std::stringstream ss;
-  ss << f.rdbuf();
-  const std::string buf = ss.str();
+  std::string buf;
+  if (msh.mesher == "gmsh") {
+    buf = gmsh_as_netgen(f);
+  } else {
+    std::stringstream ss;
+    ss << f.rdbuf();
+    buf = ss.str();
+  }
   const char* p = buf.c_str();
   if (*p < '0' || *p > '9') my_throw(0, "Undefined mesh type! Available: tetrahedral, cartesian");
   char* end;

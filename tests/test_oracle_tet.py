@@ -103,3 +103,24 @@ def test_gfdtd_cg_criterion_reference(tmp_path):
     it, err = o.cg()
     assert it.max() <= 100 and it.min() > 0
     assert np.nanmax(err) <= 1e-8
+
+
+@pytest.mark.parametrize("method", ["gfdtd", "dga"])
+def test_gmsh_input_is_the_rounded_netgen_mesh(tmp_path, method):
+    """A gmsh mesh goes through the reference's conversion to netgen text,
+    which prints coordinates with 6 significant digits
+    (Discretization.hpp:5692-5866): it runs exactly as the netgen file of the
+    same mesh written with %g coordinates, and not as the full-precision one."""
+    kw = dict(n=4, method=method, steps=12, split_x=True, eps=(1.5, 3.0), seed=11)
+    runs = []
+    for sub, extra in (("g", dict(mesh_format="gmsh")), ("r", dict(coord_fmt="%g")), ("f", {})):
+        s = write_tet_case(str(tmp_path / sub), TetCase(**kw, **extra))
+        o = oracle.TetOracle(s)
+        o.run()
+        _, v, _, _ = o.probes()
+        U, B, F = o.state()
+        o.close()
+        runs.append((v, U, B, F))
+    for a, b in zip(runs[0], runs[1]):
+        assert np.array_equal(a, b)
+    assert not np.array_equal(runs[0][1], runs[2][1])

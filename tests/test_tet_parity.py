@@ -49,6 +49,20 @@ def test_dga_fp64_matches_oracle(tmp_path, product_lib, oracle_lib, n, steps):
     assert np.abs(o["v"]).max() > 0
 
 
+@pytest.mark.parametrize("method", ["dga", "gfdtd"])
+def test_gmsh_mesh_matches_oracle(tmp_path, product_lib, oracle_lib, method):
+    """gmsh input (the reference's conversion to netgen text) on the GPU path
+    against the oracle reading the same file."""
+    s = write_tet_case(str(tmp_path), TetCase(n=4, method=method, steps=40, mesh_format="gmsh",
+                                              split_x=True, eps=(1.5, 3.0)))
+    g, o = run_pair(s)
+    assert np.array_equal(g["t"], o["t"]) and np.array_equal(g["xyz"], o["xyz"])
+    tol = TOL_FP64 if method == "dga" else 1e-8
+    for k in ("v", "U", "F"):
+        assert rel(g[k], o[k]) <= tol, k
+    assert np.abs(o["v"]).max() > 0
+
+
 @pytest.mark.parametrize("n,steps", [(4, 60), (8, 120)])
 def test_gfdtd_fp64_matches_oracle(tmp_path, product_lib, oracle_lib, n, steps):
     s = write_tet_case(str(tmp_path), TetCase(n=n, method="gfdtd", steps=steps))

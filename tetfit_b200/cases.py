@@ -169,17 +169,37 @@ def kuhn_mesh(n: int, jitter: float = 0.15, seed: int = 0x7E7F17, material=None)
     return pts, tets, mats, np.concatenate(tris), np.concatenate(labels)
 
 
-def write_netgen(path: str, pts, tets, mats, tris, labels) -> str:
+def write_netgen(path: str, pts, tets, mats, tris, labels, coord_fmt: str = "%.17g") -> str:
     """Netgen neutral format as TetFIT reads it (Discretization.hpp:5924-6101,
     6612-6654): point count + coordinates, tetrahedron count + `mat p1..p4`,
     triangle count + `label p1 p2 p3`, all node indices 1-based."""
     with open(path, "w") as f:
         f.write(f"{len(pts)}\n")
-        np.savetxt(f, pts, fmt="%.17g")
+        np.savetxt(f, pts, fmt=coord_fmt)
         f.write(f"{len(tets)}\n")
         np.savetxt(f, np.column_stack([mats, tets + 1]), fmt="%d")
         f.write(f"{len(tris)}\n")
         np.savetxt(f, np.column_stack([labels, tris + 1]), fmt="%d")
+    return path
+
+
+def write_gmsh(path: str, pts, tets, mats, tris, labels) -> str:
+    """ASCII gmsh 2.2 mesh, the layout TetFIT's gmsh conversion reads
+    (Discretization.hpp:5692-5866): nodes at full precision, then triangles
+    (type 2) and tetrahedra (type 4), each with two tags (physical =
+    elementary = the boundary id or material), node indices 1-based."""
+    with open(path, "w") as f:
+        f.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n")
+        f.write(f"{len(pts)}\n")
+        np.savetxt(f, np.column_stack([np.arange(1, len(pts) + 1), pts]), fmt=["%d", "%.17g", "%.17g", "%.17g"])
+        f.write("$EndNodes\n$Elements\n")
+        f.write(f"{len(tris) + len(tets)}\n")
+        ids = np.arange(1, len(tris) + len(tets) + 1)
+        nt = len(tris)
+        np.savetxt(f, np.column_stack([ids[:nt], np.full(nt, 2), np.full(nt, 2), labels, labels, tris + 1]), fmt="%d")
+        nv = len(tets)
+        np.savetxt(f, np.column_stack([ids[nt:], np.full(nv, 4), np.full(nv, 2), mats, mats, tets + 1]), fmt="%d")
+        f.write("$EndElements\n")
     return path
 
 
@@ -204,6 +224,8 @@ class TetCase:
     mat_field: object = None         # optional callable centroids -> labels
     width: float | None = None       # gaussian carrier width (s)
     delay: float | None = None       # carrier delay (s)
+    mesh_format: str = "netgen"      # "netgen" or "gmsh"
+    coord_fmt: str = "%.17g"         # netgen coordinates ("%g": the 6 digits a gmsh conversion keeps)
 
     def dt(self) -> float:
         if self.step is not None:
@@ -220,11 +242,14 @@ def write_tet_case(directory: str, case: TetCase, name: str = "box") -> str:
         material = lambda c: np.where(c[:, 0] < 0.5, 1, 2)
     else:
         material = None
-    mesh = write_netgen(os.path.join(directory, f"{name}.mesh"),
-                        *kuhn_mesh(case.n, case.jitter, case.seed, material))
+    geo = kuhn_mesh(case.n, case.jitter, case.seed, material)
+    if case.mesh_format == "gmsh":
+        mesh = write_gmsh(os.path.join(directory, f"{name}.msh"), *geo)
+    else:
+        mesh = write_netgen(os.path.join(directory, f"{name}.mesh"), *geo, coord_fmt=case.coord_fmt)
     dt = float(case.dt())
     duration = float((case.steps - 1) * dt if case.method == "dga" else case.steps * dt)
-    lines = ["DEFINE mesh 1", "   SET type tetrahedral", "   SET mesher netgen",
+    lines = ["DEFINE mesh 1", "   SET type tetrahedral", f"   SET mesher {case.mesh_format}",
              f"   SET file {os.path.basename(mesh)}", "   SET name box", "   SET scalefactor 1", "END mesh 1"]
     eps_items = case.eps.items() if isinstance(case.eps, dict) else enumerate(case.eps, start=1)
     for m, e in eps_items:

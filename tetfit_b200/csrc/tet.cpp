@@ -46,6 +46,73 @@ V3 mv(const Mat3& m, const V3& v) {
   for (int i = 0; i < 3; i++) r[i] = m.m[i][0] * v[0] + m.m[i][1] * v[1] + m.m[i][2] * v[2];
   return r;
 }
+// ConvertFromGMSH (Discretization.hpp:5692-5866, element parser
+// Utilities.hpp:159-223): an ASCII gmsh 2.x mesh becomes the netgen text the
+// reader takes, as the reference writes it to a temporary .mesh file.  Layout
+// read: four header lines, the node count, one "id x y z" line per node, two
+// lines, the element count, one "id type ntags tag1 tag2 nodes..." line per
+// element (two tags assumed, as the reference does).  Written: the node
+// count and coordinates with 6 significant digits (the reference prints
+// them through a default ostream, so they are rounded), the tetrahedra (type
+// 4, material = first tag) with sorted 1-based nodes in sorted order, then
+// the triangles (type 2, boundary id = first tag) in file order.
+std::string gmsh_to_netgen(const std::string& text) {
+  std::vector<const char*> line;
+  line.push_back(text.c_str());
+  for (size_t i = 0; i < text.size(); i++)
+    if (text[i] == '\n' && i + 1 < text.size()) line.push_back(text.c_str() + i + 1);
+  auto at = [&](size_t k) -> const char* {
+    if (k >= line.size()) throw ScriptError("gmsh mesh file ends early");
+    return line[k];
+  };
+  char* end;
+  size_t k = 4;
+  const uint32_t np = (uint32_t)std::strtoul(at(k), &end, 10);
+  std::string out = std::to_string(np) + "\n";
+  char num[64];
+  for (uint32_t i = 0; i < np; i++) {
+    const char* q = at(k + 1 + i);
+    std::strtod(q, &end);  // node id
+    for (int a = 0; a < 3; a++) {
+      std::snprintf(num, sizeof(num), a < 2 ? "%g " : "%g\n", std::strtod(end, &end));
+      out += num;
+    }
+  }
+  k += 1 + np + 2;
+  const uint32_t ne = (uint32_t)std::strtoul(at(k), &end, 10);
+  std::vector<std::array<uint32_t, 5>> tets;  // sorted nodes (0-based), material
+  std::vector<std::array<uint32_t, 4>> tris;  // boundary id, nodes (0-based)
+  for (uint32_t i = 0; i < ne; i++) {
+    const char* q = at(k + 1 + i);
+    std::strtoul(q, &end, 10);  // element id
+    const uint32_t type = (uint32_t)std::strtoul(end, &end, 10);
+    if (type != 4 && type != 2) continue;
+    std::strtoul(end, &end, 10);  // number of tags
+    const uint32_t tag = (uint32_t)std::strtoul(end, &end, 10);
+    std::strtoul(end, &end, 10);  // second tag
+    uint32_t n[4] = {0, 0, 0, 0};
+    for (uint32_t j = 0; j < (type == 4 ? 4u : 3u); j++) n[j] = (uint32_t)std::strtoul(end, &end, 10) - 1;
+    if (type == 4) {
+      std::sort(n, n + 4);
+      tets.push_back({n[0], n[1], n[2], n[3], tag});
+    } else {
+      tris.push_back({tag, n[0], n[1], n[2]});
+    }
+  }
+  std::stable_sort(tets.begin(), tets.end(), [](const auto& a, const auto& b) {
+    return std::lexicographical_compare(a.begin(), a.begin() + 4, b.begin(), b.begin() + 4);
+  });
+  out += std::to_string(tets.size()) + "\n";
+  for (const auto& t : tets)
+    out += std::to_string(t[4]) + " " + std::to_string(t[0] + 1) + " " + std::to_string(t[1] + 1) + " " +
+           std::to_string(t[2] + 1) + " " + std::to_string(t[3] + 1) + "\n";
+  out += std::to_string(tris.size()) + "\n";
+  for (const auto& t : tris)
+    out += std::to_string(t[0]) + " " + std::to_string(t[1] + 1) + " " + std::to_string(t[2] + 1) + " " +
+           std::to_string(t[3] + 1) + "\n";
+  return out;
+}
+
 bool is_zero(const Mat3& m) {
   for (auto& r : m.m)
     for (double x : r)
@@ -255,14 +322,14 @@ TetSim::~TetSim() {
 }
 
 void TetSim::read_mesh() {
-  // netgen neutral reader (Discretization.hpp:5924-6101)
+  // netgen neutral reader (Discretization.hpp:5924-6101); gmsh files are
+  // converted to the same text first (Discretization.hpp:5890-5895)
   const Mesh& msh = sc_.meshes[sim_.mesh];
-  if (msh.mesher == "gmsh") throw UnsupportedError("gmsh meshes are outside the supported path (use netgen)");
   std::ifstream fin(msh.file.c_str(), std::ios::binary);
   if (!fin.is_open()) throw ScriptError("Invalid mesh file name");
   std::stringstream ss;
   ss << fin.rdbuf();
-  const std::string buf = ss.str();
+  const std::string buf = msh.mesher == "gmsh" ? gmsh_to_netgen(ss.str()) : ss.str();
   const char* p = buf.c_str();
   if (*p < '0' || *p > '9') my_throw(0, "Undefined mesh type! Available: tetrahedral, cartesian");
   char* end;
