@@ -347,6 +347,22 @@ def member_carriers(infos, cases, steps_done):
     return np.asarray(out if out else [0.0])
 
 
+def batch_description(workload, cases):
+    """The `config.workload` text of a batch workload (both bench arms)."""
+    w = WORKLOADS[workload]
+    learn = w.get("learn_steps", 0) if w["warm"] == "learned" else 0
+    ns = sorted(c.n for c in cases)
+    if w.get("grf"):
+        scene = (f"{workload}: gfdtd on a {w['n_lo']}^3 x 6 jittered Kuhn box, eps_r from a seeded "
+                 f"Gaussian random field (corr. 0.1 m) mapped to [1,12] in 24 levels, PEC box, H-wave source")
+    else:
+        scene = (f"{workload}: {w['members']} gfdtd members in one group, Kuhn meshes "
+                 f"n ~ U{{{w['n_lo']}..{w['n_hi']}}} (min {ns[0]}, median {ns[len(ns) // 2]}, max {ns[-1]}) "
+                 f"x 6 tets, eps_r ~ U[1,4] per x-half, f ~ U[1e8,4e8] Hz")
+    return (scene + f", {w['prec']} fields, FP64 CG reductions, CG tol 1e-8 (||r|| <= tol ||b||), "
+            f"{w['warm']} warm start" + (f" (network trained on the first {learn} steps, untimed)" if learn else ""))
+
+
 def run_batch(args, rank, world, local_rank):
     import tetfit_b200 as tb
     from tetfit_b200.cases import batch_cases, write_batch
@@ -471,16 +487,7 @@ def run_batch(args, rank, world, local_rank):
         achieved = cg_bytes / (cg_ms * 1e-3) / 1e9
         value = world * dofs * K / (max_ms * 1e-3)
         plain_value = world * dofs * Kp / (max_plain * 1e-3)
-        ns = sorted(c.n for c in cases)
-        if w.get("grf"):
-            scene = (f"{args.workload}: gfdtd on a {w['n_lo']}^3 x 6 jittered Kuhn box, eps_r from a seeded "
-                     f"Gaussian random field (corr. 0.1 m) mapped to [1,12] in 24 levels, PEC box, H-wave source")
-        else:
-            scene = (f"{args.workload}: {w['members']} gfdtd members in one group, Kuhn meshes "
-                     f"n ~ U{{{w['n_lo']}..{w['n_hi']}}} (min {ns[0]}, median {ns[len(ns) // 2]}, max {ns[-1]}) "
-                     f"x 6 tets, eps_r ~ U[1,4] per x-half, f ~ U[1e8,4e8] Hz")
-        desc = (scene + f", {w['prec']} fields, FP64 CG reductions, CG tol 1e-8 (||r|| <= tol ||b||), "
-                f"{w['warm']} warm start" + (f" (network trained on the first {learn} steps, untimed)" if learn else ""))
+        desc = batch_description(args.workload, cases)
         result = {
             "metric": "dof-steps/s", "value": value, "unit": "dof-steps/s", "n_gpus": world, "steps": K,
             "warmup": args.warmup, "ms_per_step": max_ms / K, "higher_is_better": True, "scaling": "weak",
@@ -669,7 +676,9 @@ def run_batch_reference(args, rank):
     return {"impl": "reference", "metric": "dof-steps/s", "value": v, "unit": "dof-steps/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": f"{args.workload} (bounded CPU sample)"},
+            "data": "synthetic", "config": {"workload": batch_description(args.workload, cases),
+                                            "members": w["members"], "parallelism": "host threads",
+                                            "cpu_sample": f"{len(members)} members"},
             "cpu_baseline": {"value": v, "unit": "dof-steps/s", "cores": len(members), "kind": "port",
                              "sample": sample, "cpu": _cpu_model()},
             "e2e": {"value": v, "unit": "dof-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
