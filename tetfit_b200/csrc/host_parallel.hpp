@@ -2,8 +2,15 @@
 // index ranges, one per thread, and every caller writes only its own
 // positions, so results are the same for any thread count.
 #pragma once
+#include <unistd.h>
+
 #include <algorithm>
+#include <atomic>
+#include <condition_variable>
 #include <cstdint>
+#include <functional>
+#include <memory>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -16,14 +23,101 @@ inline int host_threads(int threads) {
   return h ? (int)h : 1;
 }
 
-// f(begin, end) over [0, n) in up to `threads` contiguous ranges
+// Persistent workers for the set-up loops, so that the many short parallel
+// regions of an iterative set-up step (the stability estimate) do not pay a
+// thread start each.  One job at a time: a caller that finds the pool busy
+// (another host thread's set-up) starts its own threads instead.  The pool
+// belongs to the process that created it (worker threads do not survive a
+// fork) and is never destroyed, so no destructor runs while workers wait.
+class HostPool {
+ public:
+  static HostPool* get() {
+    static HostPool* p = new HostPool(std::max(1u, std::thread::hardware_concurrency()) - 1);
+    return p->pid_ == getpid() ? p : nullptr;
+  }
+  int workers() const { return (int)workers_.size(); }
+  // runs f(k) for k in [0, nt) on the caller and the workers; false if busy
+  bool run(int nt, const std::function<void(int)>& f) {
+    std::unique_lock<std::mutex> busy(busy_, std::try_to_lock);
+    if (!busy.owns_lock()) return false;
+    auto job = std::make_shared<Job>(&f, nt);
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      cur_ = job;
+      gen_++;
+    }
+    cv_.notify_all();
+    execute(*job);
+    {
+      std::unique_lock<std::mutex> lk(job->m);
+      job->cv.wait(lk, [&] { return job->done; });
+    }
+    std::lock_guard<std::mutex> lk(m_);
+    cur_.reset();
+    return true;
+  }
+
+ private:
+  // One job's own counters: a worker that wakes late still holds the job it
+  // woke for, finds its tasks all claimed and leaves, so it can never claim
+  // or count a task of a later job.
+  struct Job {
+    Job(const std::function<void(int)>* fn, int n) : f(fn), n(n), left(n) {}
+    const std::function<void(int)>* f;
+    const int n;
+    std::atomic<int> next{0}, left;
+    std::mutex m;
+    std::condition_variable cv;
+    bool done = false;
+  };
+  static void execute(Job& j) {
+    for (int k = j.next.fetch_add(1); k < j.n; k = j.next.fetch_add(1)) {
+      (*j.f)(k);
+      if (j.left.fetch_sub(1) == 1) {
+        std::lock_guard<std::mutex> lk(j.m);
+        j.done = true;
+        j.cv.notify_all();
+      }
+    }
+  }
+  explicit HostPool(unsigned nw) : pid_(getpid()) {
+    for (unsigned k = 0; k < nw; k++)
+      workers_.emplace_back([this] {
+        uint64_t seen = 0;
+        for (;;) {
+          std::shared_ptr<Job> job;
+          {
+            std::unique_lock<std::mutex> lk(m_);
+            cv_.wait(lk, [&] { return gen_ != seen; });
+            seen = gen_;
+            job = cur_;
+          }
+          if (job) execute(*job);
+        }
+      });
+    for (auto& t : workers_) t.detach();
+  }
+  const pid_t pid_;
+  std::mutex busy_, m_;
+  std::condition_variable cv_;
+  std::vector<std::thread> workers_;
+  std::shared_ptr<Job> cur_;
+  uint64_t gen_ = 0;
+};
+
+// f(begin, end) over [0, n) in up to `threads` contiguous ranges of at
+// least `grain` indices; loops below one grain run inline
 template <typename F>
-void parallel_for(int64_t n, int threads, F&& f) {
-  const int64_t nt = std::max<int64_t>(1, std::min<int64_t>(host_threads(threads), n / 4096 + 1));
+void parallel_for(int64_t n, int threads, F&& f, int64_t grain = 4096) {
+  const int64_t nt = std::max<int64_t>(1, std::min<int64_t>(host_threads(threads), n / grain));
   if (nt <= 1) {
     if (n > 0) f((int64_t)0, n);
     return;
   }
+  HostPool* hp = HostPool::get();
+  if (hp && nt <= hp->workers() + 1 &&
+      hp->run((int)nt, [&](int k) { f(n * k / nt, n * (k + 1) / nt); }))
+    return;
   std::vector<std::thread> pool;
   pool.reserve(nt - 1);
   for (int64_t k = 1; k < nt; k++) pool.emplace_back([&, k] { f(n * k / nt, n * (k + 1) / nt); });

@@ -237,12 +237,14 @@ HostCsr HostCsr::build(uint32_t nr, uint32_t nc, std::vector<Trip>& t, int threa
   return m;
 }
 
-void HostCsr::mul(const double* x, double* y) const {
-  for (uint32_t r = 0; r < nrows; r++) {
-    double s = 0;
-    for (int64_t k = ptr[r]; k < ptr[r + 1]; k++) s += val[k] * x[col[k]];
-    y[r] = s;
-  }
+void HostCsr::mul(const double* x, double* y, int threads) const {
+  parallel_for(nrows, threads, [&](int64_t r0, int64_t r1) {
+    for (int64_t r = r0; r < r1; r++) {
+      double s = 0;
+      for (int64_t k = ptr[r]; k < ptr[r + 1]; k++) s += val[k] * x[col[k]];
+      y[r] = s;
+    }
+  });
 }
 
 // ------------------------------------------------------------------ set-up
@@ -837,41 +839,72 @@ void TetSim::build_ops() {
 double TetSim::estimate_dt(const HostCsr& M, bool generalized) {
   const size_t n = edges_.size(), nf = faces_.size();
   if (sim_.step != 0 && (n > 3000000 || !opt_.estimate_pinned)) return sim_.step / sim_.courant;
+  // Loops run on the set-up threads: matrix products and updates row by row,
+  // inner products as sums of fixed 4096-row chunks added in chunk order, so
+  // the estimate does not depend on the thread count.
+  const int nth = opt_.setup_threads;
+  auto par = [&](size_t m, auto&& f) {
+    parallel_for((int64_t)m, nth, [&](int64_t i0, int64_t i1) {
+      for (int64_t i = i0; i < i1; i++) f((size_t)i);
+    });
+  };
+  std::vector<double> part((n + 4095) / 4096);
+  auto dot = [&](const double* a, const double* b) {
+    parallel_for((int64_t)part.size(), nth, [&](int64_t c0, int64_t c1) {
+      for (int64_t c = c0; c < c1; c++) {
+        double t = 0;
+        for (size_t i = (size_t)c * 4096; i < std::min(n, (size_t)(c + 1) * 4096); i++) t += a[i] * b[i];
+        part[c] = t;
+      }
+    }, 4);
+    double t = 0;
+    for (double x : part) t += x;
+    return t;
+  };
   std::vector<double> cu(nf), ncu(nf);
   auto K = [&](const double* x, double* y) {
-    for (size_t f = 0; f < nf; f++) cu[f] = x[fte_[f][0]] - x[fte_[f][1]] + x[fte_[f][2]];
-    N_.mul(cu.data(), ncu.data());
-    for (size_t e = 0; e < n; e++) {
-      double s = 0;
-      for (int64_t k = Ct_.ptr[e]; k < Ct_.ptr[e + 1]; k++) s += Ct_.val[k] * ncu[Ct_.col[k]];
-      y[e] = s;
-    }
+    par(nf, [&](size_t f) { cu[f] = x[fte_[f][0]] - x[fte_[f][1]] + x[fte_[f][2]]; });
+    N_.mul(cu.data(), ncu.data(), nth);
+    par(n, [&](size_t e) {
+      double t = 0;
+      for (int64_t k = Ct_.ptr[e]; k < Ct_.ptr[e + 1]; k++) t += Ct_.val[k] * ncu[Ct_.col[k]];
+      y[e] = t;
+    });
   };
   std::vector<double> pre(n), r(n), z(n), p(n), q(n);
   if (generalized)
-    for (size_t i = 0; i < n; i++) {
+    par(n, [&](size_t i) {
       double dg = 0;
       for (int64_t k = M.ptr[i]; k < M.ptr[i + 1]; k++)
         if (M.col[k] == (int32_t)i) dg = M.val[k];
       pre[i] = dg != 0 ? 1.0 / dg : 1.0;
-    }
+    });
   auto Minv = [&](const double* x, double* y) {
     if (!generalized) {
-      M.mul(x, y);
+      M.mul(x, y, nth);
       return;
     }
     // y = E^-1 x by Jacobi-PCG from zero
-    std::fill(y, y + n, 0.0);
-    double rr0 = 0, rz = 0;
-    for (size_t i = 0; i < n; i++) { r[i] = x[i]; rr0 += r[i] * r[i]; z[i] = pre[i] * r[i]; rz += r[i] * z[i]; p[i] = z[i]; }
+    par(n, [&](size_t i) {
+      y[i] = 0.0;
+      r[i] = x[i];
+      z[i] = pre[i] * r[i];
+      p[i] = z[i];
+    });
+    const double rr0 = dot(r.data(), r.data());
+    double rz = dot(r.data(), z.data());
     for (int it = 0; it < 1000 && rr0 > 0; it++) {
-      M.mul(p.data(), q.data());
-      double pq = 0;
-      for (size_t i = 0; i < n; i++) pq += p[i] * q[i];
-      double a = rz / pq, rr = 0, rz2 = 0;
-      for (size_t i = 0; i < n; i++) { y[i] += a * p[i]; r[i] -= a * q[i]; rr += r[i] * r[i]; z[i] = pre[i] * r[i]; rz2 += r[i] * z[i]; }
+      M.mul(p.data(), q.data(), nth);
+      const double a = rz / dot(p.data(), q.data());
+      par(n, [&](size_t i) {
+        y[i] += a * p[i];
+        r[i] -= a * q[i];
+        z[i] = pre[i] * r[i];
+      });
+      const double rr = dot(r.data(), r.data()), rz2 = dot(r.data(), z.data());
       if (std::sqrt(rr / rr0) < 1e-12) break;
-      for (size_t i = 0; i < n; i++) p[i] = z[i] + rz2 / rz * p[i];
+      const double bt = rz2 / rz;
+      par(n, [&](size_t i) { p[i] = z[i] + bt * p[i]; });
       rz = rz2;
     }
   };
@@ -884,21 +917,17 @@ double TetSim::estimate_dt(const HostCsr& M, bool generalized) {
   K(x.data(), Kv.data());
   Minv(Kv.data(), v.data());
   K(v.data(), Kv.data());
-  double nrm = 0;
-  for (size_t i = 0; i < n; i++) nrm += v[i] * Kv[i];
-  nrm = std::sqrt(nrm);
-  for (size_t i = 0; i < n; i++) { v[i] /= nrm; Kv[i] /= nrm; }
+  const double nrm = std::sqrt(dot(v.data(), Kv.data()));
+  par(n, [&](size_t i) { v[i] /= nrm; Kv[i] /= nrm; });
   std::vector<double> al, be;
   double beta = 0, last = 0, lam = 0;
   for (int it = 0; it < 400; it++) {
     Minv(Kv.data(), w.data());
-    double alpha = 0;
-    for (size_t i = 0; i < n; i++) alpha += w[i] * Kv[i];
-    for (size_t i = 0; i < n; i++) w[i] -= alpha * v[i] + beta * vp[i];
+    const double alpha = dot(w.data(), Kv.data());
+    par(n, [&](size_t i) { w[i] -= alpha * v[i] + beta * vp[i]; });
     al.push_back(alpha);
     K(w.data(), Kw.data());
-    double nb = 0;
-    for (size_t i = 0; i < n; i++) nb += w[i] * Kw[i];
+    double nb = dot(w.data(), Kw.data());
     nb = nb > 0 ? std::sqrt(nb) : 0;
     if (it % 10 == 9 || nb == 0 || it == 399) {
       lam = tridiag_max(al, be);
@@ -908,7 +937,7 @@ double TetSim::estimate_dt(const HostCsr& M, bool generalized) {
     be.push_back(nb);
     beta = nb;
     vp.swap(v);
-    for (size_t i = 0; i < n; i++) { v[i] = w[i] / nb; Kv[i] = Kw[i] / nb; }
+    par(n, [&](size_t i) { v[i] = w[i] / nb; Kv[i] = Kw[i] / nb; });
   }
   return 2.0 / std::sqrt(lam);
 }

@@ -31,7 +31,7 @@ struct HostCsr {
   };
   // threads: host threads for the per-row work (<= 0: all)
   static HostCsr build(uint32_t nr, uint32_t nc, std::vector<Trip>& t, int threads = 1);
-  void mul(const double* x, double* y) const;
+  void mul(const double* x, double* y, int threads = 1) const;
 };
 
 class TetSim : public Sim {
