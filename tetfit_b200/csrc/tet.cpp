@@ -184,20 +184,71 @@ HostCsr HostCsr::build(uint32_t nr, uint32_t nc, std::vector<Trip>& t, int threa
     int32_t c;
     double v;
   };
-  // each thread owns a row range: it counts, then places, the entries of its
-  // rows (scanning all triplets in order keeps every row's order)
+  // Stable bucketing in two levels: contiguous chunks of the triplets are
+  // counted into row ranges and placed range by range in chunk order, then
+  // each row range is bucketed by row; every row keeps the order its entries
+  // were given in.
+  const int64_t nt_ = (int64_t)t.size();
+  const int64_t P = std::max<int64_t>(1, std::min<int64_t>(host_threads(threads), nt_ / 65536));
+  const int64_t R = P;  // row ranges
+  auto range_of = [&](uint32_t r) { return (int64_t)r * R / std::max<int64_t>(nr, 1); };
+  std::vector<int64_t> rcut(R + 1);
+  for (int64_t q = 0; q <= R; q++) {  // first row of each range
+    int64_t lo = 0, hi = nr;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) / 2;
+      if (range_of((uint32_t)mid) >= q) hi = mid;
+      else lo = mid + 1;
+    }
+    rcut[q] = lo;
+  }
+  std::vector<int64_t> cc((size_t)P * R, 0);  // [chunk][range] counts, then offsets
+  parallel_for(P, (int)P, [&](int64_t c0, int64_t c1) {
+    for (int64_t c = c0; c < c1; c++)
+      for (int64_t k = nt_ * c / P; k < nt_ * (c + 1) / P; k++) cc[c * R + range_of(t[k].r)]++;
+  }, 1);
+  std::vector<int64_t> rbeg(R + 1, 0);
+  {
+    int64_t o = 0;
+    for (int64_t q = 0; q < R; q++) {
+      rbeg[q] = o;
+      for (int64_t c = 0; c < P; c++) {
+        const int64_t x = cc[c * R + q];
+        cc[c * R + q] = o;
+        o += x;
+      }
+    }
+    rbeg[R] = o;
+  }
+  std::vector<Trip> tmp(t.size());
+  parallel_for(P, (int)P, [&](int64_t c0, int64_t c1) {
+    for (int64_t c = c0; c < c1; c++) {
+      int64_t* pos = &cc[c * R];
+      for (int64_t k = nt_ * c / P; k < nt_ * (c + 1) / P; k++) tmp[pos[range_of(t[k].r)]++] = t[k];
+    }
+  }, 1);
+  std::vector<Trip>().swap(t);
   std::vector<int64_t> start(nr + 1, 0);
-  parallel_for(nr, threads, [&](int64_t r0, int64_t r1) {
-    for (const Trip& x : t)
-      if (x.r >= r0 && x.r < r1) start[x.r + 1]++;
-  });
-  for (uint32_t r = 0; r < nr; r++) start[r + 1] += start[r];
-  std::vector<CV> b(t.size());
-  parallel_for(nr, threads, [&](int64_t r0, int64_t r1) {
-    std::vector<int64_t> pos(start.begin() + r0, start.begin() + r1);
-    for (const Trip& x : t)
-      if (x.r >= r0 && x.r < r1) b[pos[x.r - r0]++] = {(int32_t)x.c, x.v};
-  });
+  std::vector<CV> b(tmp.size());
+  parallel_for(R, (int)R, [&](int64_t q0, int64_t q1) {
+    for (int64_t q = q0; q < q1; q++) {
+      const int64_t r0 = rcut[q], r1 = rcut[q + 1];
+      std::vector<int64_t> pos(r1 - r0, 0);
+      for (int64_t k = rbeg[q]; k < rbeg[q + 1]; k++) pos[tmp[k].r - r0]++;
+      int64_t o = rbeg[q];
+      for (int64_t r = r0; r < r1; r++) {  // each range writes the starts of its own rows only
+        const int64_t x = pos[r - r0];
+        start[r] = pos[r - r0] = o;
+        o += x;
+      }
+      for (int64_t k = rbeg[q]; k < rbeg[q + 1]; k++) {
+        const Trip& x = tmp[k];
+        b[pos[x.r - r0]++] = {(int32_t)x.c, x.v};
+      }
+    }
+  }, 1);
+  start[nr] = (int64_t)b.size();
+  std::vector<Trip>().swap(tmp);
   std::vector<int64_t> cnt(nr + 1, 0);
   parallel_for(nr, threads, [&](int64_t r0, int64_t r1) {
     for (int64_t r = r0; r < r1; r++) {
