@@ -119,14 +119,17 @@ int tf_batch_open(const char* const* scripts, const uint32_t* labels, uint32_t n
     for (auto& t : pool) t.join();
     for (uint32_t i = 0; i < n; i++)
       if (codes[i] != TF_OK) return bfail(b, codes[i], "batch member " + std::to_string(i) + ": " + errs[i]);
+    // the device image is laid out by this thread alone: all host threads
+    tf::RunOptions rg = ro;
+    rg.setup_threads = 0;
     if (b->mode == 0) {
       std::vector<tf::TetSim*> v;
       for (auto& s : b->sims) v.push_back(s.get());
-      b->groups.emplace_back(new tf::TetGroup(v, ro, true));
+      b->groups.emplace_back(new tf::TetGroup(v, rg, true));
       for (uint32_t i = 0; i < n; i++) b->where.push_back({0, (int)i});
     } else {
       for (uint32_t i = 0; i < n; i++) {
-        b->groups.emplace_back(new tf::TetGroup({b->sims[i].get()}, ro, true));
+        b->groups.emplace_back(new tf::TetGroup({b->sims[i].get()}, rg, true));
         b->where.push_back({(int)i, 0});
       }
     }

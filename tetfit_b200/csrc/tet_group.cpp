@@ -10,6 +10,7 @@
 #include <string>
 
 #include "cuda_util.hpp"
+#include "host_parallel.hpp"
 
 namespace tf {
 
@@ -28,28 +29,39 @@ struct SellHost {
   // padding.  len(p): entries of row p; ent(p, j, c, v): entry j; pad(p):
   // column of a padding entry.
   template <typename L, typename E, typename P>
-  void append(int64_t nrows, int64_t nreal, L len, E ent, P pad, bool values) {
-    for (int64_t s0 = 0; s0 < nrows; s0 += 32) {
-      int ml = 0;
-      for (int l = 0; l < 32; l++)
-        if (s0 + l < nreal) ml = std::max(ml, (int)len(s0 + l));
-      const size_t base = col.size();
-      col.resize(base + 32 * (size_t)ml);
-      if (values) val.resize(base + 32 * (size_t)ml);
-      for (int l = 0; l < 32; l++) {
-        const int64_t p = s0 + l;
-        const int n = p < nreal ? (int)len(p) : 0;
-        for (int j = 0; j < ml; j++) {
-          int32_t c = 0;
-          double v = 0.0;
-          if (j < n) ent(p, j, c, v);
-          else c = pad(p);
-          col[base + 32 * (size_t)j + l] = c;
-          if (values) val[base + 32 * (size_t)j + l] = (T)v;
+  void append(int64_t nrows, int64_t nreal, L len, E ent, P pad, bool values, int threads = 1) {
+    // slice widths and offsets, then every slice filled at its own place
+    const int64_t ns = nrows / 32, s_base = (int64_t)ptr.size() - 1;
+    ptr.resize(ptr.size() + ns);
+    parallel_for(ns, threads, [&](int64_t q0, int64_t q1) {
+      for (int64_t q = q0; q < q1; q++) {
+        int ml = 0;
+        for (int l = 0; l < 32; l++)
+          if (32 * q + l < nreal) ml = std::max(ml, (int)len(32 * q + l));
+        ptr[s_base + q + 1] = 32 * (int64_t)ml;
+      }
+    });
+    for (int64_t q = 0; q < ns; q++) ptr[s_base + q + 1] += ptr[s_base + q];
+    col.resize(ptr.back());
+    if (values) val.resize(ptr.back());
+    parallel_for(ns, threads, [&](int64_t q0, int64_t q1) {
+      for (int64_t q = q0; q < q1; q++) {
+        const size_t base = (size_t)ptr[s_base + q];
+        const int ml = (int)((ptr[s_base + q + 1] - ptr[s_base + q]) / 32);
+        for (int l = 0; l < 32; l++) {
+          const int64_t p = 32 * q + l;
+          const int n = p < nreal ? (int)len(p) : 0;
+          for (int j = 0; j < ml; j++) {
+            int32_t c = 0;
+            double v = 0.0;
+            if (j < n) ent(p, j, c, v);
+            else c = pad(p);
+            col[base + 32 * (size_t)j + l] = c;
+            if (values) val[base + 32 * (size_t)j + l] = (T)v;
+          }
         }
       }
-      ptr.push_back((int64_t)col.size());
-    }
+    });
   }
 };
 
@@ -155,7 +167,7 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
           c = (int32_t)(roff + pos[t.A_.col[q]]);
           v = t.A_.val[q];
         },
-        [&](int64_t p) { return (int32_t)(roff + p); }, true);
+        [&](int64_t p) { return (int32_t)(roff + p); }, true, opt_.setup_threads);
     auto erow = [&](int64_t p) { return (int64_t)t.free_edges_[old_of_new[p]]; };
     Ef.append(
         nfp, nf, [&](int64_t p) { return t.E_.ptr[erow(p) + 1] - t.E_.ptr[erow(p)]; },
@@ -164,7 +176,7 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
           c = (int32_t)(eoff + t.E_.col[q]);
           v = t.E_.val[q];
         },
-        [&](int64_t) { return (int32_t)eoff; }, true);
+        [&](int64_t) { return (int32_t)eoff; }, true, opt_.setup_threads);
     Ct.append(
         nfp, nf, [&](int64_t p) { return t.Ct_.ptr[erow(p) + 1] - t.Ct_.ptr[erow(p)]; },
         [&](int64_t p, int j, int32_t& c, double& v) {
@@ -173,7 +185,7 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
           if (t.Ct_.val[q] < 0) c = (int32_t)((uint32_t)c | 0x80000000u);
           v = 0.0;
         },
-        [&](int64_t) { return kPadCol; }, false);
+        [&](int64_t) { return kPadCol; }, false, opt_.setup_threads);
     N.append(
         NFp, NF, [&](int64_t f) { return t.N_.ptr[f + 1] - t.N_.ptr[f]; },
         [&](int64_t f, int j, int32_t& c, double& v) {
@@ -181,7 +193,7 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
           c = (int32_t)(foff + t.N_.col[q]);
           v = t.N_.val[q];
         },
-        [&](int64_t f) { return (int32_t)(foff + f); }, true);
+        [&](int64_t f) { return (int32_t)(foff + f); }, true, opt_.setup_threads);
     for (int64_t f = 0; f < NFp; f++)
       for (int k = 0; k < 3; k++) fte.push_back(f < NF ? (int32_t)(eoff + t.fte_[f][k]) : -1);
     for (int64_t p = 0; p < nfp; p++) {
