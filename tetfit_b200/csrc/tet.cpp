@@ -1054,8 +1054,33 @@ void TetSim::locate_probes() {
     return true;
   };
   const float gbox[6] = {glo[0], glo[1], glo[2], ghi[0], ghi[1], ghi[2]};
-  auto find = [&](const std::array<double, 3>& pv) -> int64_t {
-    if (L == 0 || !in_box(gbox, pv)) return -1;
+  // the walk's containment test, behind the exact box pre-test
+  auto passes = [&](uint32_t v, const std::array<double, 3>& pv) {
+    if (!in_box(&box[6 * (size_t)v], pv)) return false;
+    double rows[4][4];
+    for (int r = 0; r < 4; r++) {
+      for (int a = 0; a < 3; a++) rows[r][a] = pts_[vols_[v][r]][a];
+      rows[r][3] = 1;
+    }
+    const double d0 = det4(rows);
+    bool ok = true;
+    for (int r = 0; r < 4 && ok; r++) {
+      double m[4][4];
+      std::memcpy(m, rows, sizeof(m));
+      for (int a = 0; a < 3; a++) m[r][a] = pv[a];
+      const double d1 = det4(m);
+      ok = (d0 >= -tol && d1 >= -tol) || (d0 <= tol && d1 <= tol);
+    }
+    return ok;
+  };
+  auto neighbour = [&](uint32_t v, int32_t f) {
+    int32_t n = ftv_[f][0];
+    if (n == (int32_t)v) n = ftv_[f][1] >= 0 ? ftv_[f][1] : n;
+    return n;
+  };
+  // FindProbe's walk: breadth first from the last hit, tet 0 marked visited
+  // from the start, the first tet that passes wins
+  auto walk = [&](const std::array<double, 3>& pv) -> int64_t {
     for (uint32_t t : touched) colour[t] = 0;
     touched.clear();
     std::vector<uint32_t> q{root};
@@ -1063,27 +1088,12 @@ void TetSim::locate_probes() {
     touched.push_back(0);
     for (size_t h = 0; h < q.size(); h++) {
       const uint32_t v = q[h];
-      bool ok = in_box(&box[6 * (size_t)v], pv);
-      double rows[4][4];
-      for (int r = 0; r < 4; r++) {
-        for (int a = 0; a < 3; a++) rows[r][a] = pts_[vols_[v][r]][a];
-        rows[r][3] = 1;
-      }
-      const double d0 = ok ? det4(rows) : 0.0;
-      for (int r = 0; r < 4 && ok; r++) {
-        double m[4][4];
-        std::memcpy(m, rows, sizeof(m));
-        for (int a = 0; a < 3; a++) m[r][a] = pv[a];
-        const double d1 = det4(m);
-        ok = (d0 >= -tol && d1 >= -tol) || (d0 <= tol && d1 <= tol);
-      }
-      if (ok) {
+      if (passes(v, pv)) {
         root = v;
         return v;
       }
       for (int32_t f : vtf_[v]) {
-        int32_t n = ftv_[f][0];
-        if (n == (int32_t)v) n = ftv_[f][1] >= 0 ? ftv_[f][1] : n;
+        const int32_t n = neighbour(v, f);
         if (!colour[n]) {
           colour[n] = 1;
           touched.push_back(n);
@@ -1093,6 +1103,109 @@ void TetSim::locate_probes() {
       if (!colour[v]) { colour[v] = 1; touched.push_back(v); }
     }
     return -1;
+  };
+  // The walk's answer without the walk.  Its first passing tet is its only
+  // passing tet when exactly one tet it can reach passes, and it finds none
+  // when none does; only real ties (two or more) need the walk's order.
+  // Candidates come from a uniform grid over the widened tet boxes (every tet
+  // whose box holds the point is listed in the point's cell; unbounded boxes
+  // are kept aside and tried for every point).  What the walk reaches: the
+  // components of the face graph without tet 0 (it starts with tet 0
+  // marked), the root's own component, or from root 0 tet 0 and the
+  // components next to it.
+  std::vector<int32_t> comp(L, -1);
+  {
+    int32_t nc = 0;
+    std::vector<uint32_t> stack;
+    for (uint32_t s0 = 1; s0 < L; s0++) {
+      if (comp[s0] >= 0) continue;
+      comp[s0] = nc;
+      stack.assign(1, s0);
+      while (!stack.empty()) {
+        const uint32_t v = stack.back();
+        stack.pop_back();
+        for (int32_t f : vtf_[v]) {
+          const int32_t n = neighbour(v, f);
+          if (n != 0 && comp[n] < 0) {
+            comp[n] = nc;
+            stack.push_back((uint32_t)n);
+          }
+        }
+      }
+      nc++;
+    }
+  }
+  std::vector<int32_t> next_to_0;
+  if (L > 0)
+    for (int32_t f : vtf_[0]) {
+      const int32_t n = neighbour(0, f);
+      if (n != 0) next_to_0.push_back(comp[n]);
+    }
+  auto reached = [&](uint32_t t) {
+    if (root != 0) return t != 0 && comp[t] == comp[root];
+    return t == 0 || std::find(next_to_0.begin(), next_to_0.end(), comp[t]) != next_to_0.end();
+  };
+  std::vector<uint32_t> unbounded;
+  double flo[3] = {1e300, 1e300, 1e300}, fhi[3] = {-1e300, -1e300, -1e300};
+  for (size_t v = 0; v < L; v++) {
+    if (!std::isfinite(box[6 * v]) || !std::isfinite(box[6 * v + 3]) || !std::isfinite(box[6 * v + 1]) ||
+        !std::isfinite(box[6 * v + 4]) || !std::isfinite(box[6 * v + 2]) || !std::isfinite(box[6 * v + 5])) {
+      unbounded.push_back((uint32_t)v);
+      continue;
+    }
+    for (int a = 0; a < 3; a++) {
+      flo[a] = std::min(flo[a], (double)box[6 * v + a]);
+      fhi[a] = std::max(fhi[a], (double)box[6 * v + 3 + a]);
+    }
+  }
+  const int64_t G = std::max<int64_t>(1, std::min<int64_t>(256, (int64_t)std::cbrt((double)L / 8.0)));
+  double cw[3];
+  for (int a = 0; a < 3; a++) cw[a] = fhi[a] > flo[a] ? (fhi[a] - flo[a]) / (double)G : 1.0;
+  auto cell_of = [&](int a, double x) {
+    const double c = std::floor((x - flo[a]) / cw[a]);
+    return c < 0 ? (int64_t)0 : (c > (double)(G - 1) ? G - 1 : (int64_t)c);
+  };
+  std::vector<int64_t> cstart(G * G * G + 1, 0);
+  std::vector<uint32_t> cidx;
+  {
+    auto each_cell = [&](size_t v, auto&& f) {
+      int64_t c0[3], c1[3];
+      for (int a = 0; a < 3; a++) {
+        c0[a] = cell_of(a, (double)box[6 * v + a]);
+        c1[a] = cell_of(a, (double)box[6 * v + 3 + a]);
+      }
+      for (int64_t k = c0[2]; k <= c1[2]; k++)
+        for (int64_t j = c0[1]; j <= c1[1]; j++)
+          for (int64_t i = c0[0]; i <= c1[0]; i++) f((k * G + j) * G + i);
+    };
+    std::vector<uint8_t> is_unb(L, 0);
+    for (uint32_t v : unbounded) is_unb[v] = 1;
+    for (size_t v = 0; v < L; v++)
+      if (!is_unb[v]) each_cell(v, [&](int64_t c) { cstart[c + 1]++; });
+    for (int64_t c = 0; c < G * G * G; c++) cstart[c + 1] += cstart[c];
+    cidx.resize(cstart[G * G * G]);
+    std::vector<int64_t> pos(cstart.begin(), cstart.end() - 1);
+    for (size_t v = 0; v < L; v++)
+      if (!is_unb[v]) each_cell(v, [&](int64_t c) { cidx[pos[c]++] = (uint32_t)v; });
+  }
+  auto find = [&](const std::array<double, 3>& pv) -> int64_t {
+    if (L == 0 || !in_box(gbox, pv)) return -1;
+    std::vector<uint32_t> hits;
+    bool inside = true;
+    for (int a = 0; a < 3; a++) inside = inside && pv[a] >= flo[a] && pv[a] <= fhi[a];
+    if (inside) {
+      const int64_t c = (cell_of(2, pv[2]) * G + cell_of(1, pv[1])) * G + cell_of(0, pv[0]);
+      for (int64_t k = cstart[c]; k < cstart[c + 1]; k++)
+        if (passes(cidx[k], pv) && reached(cidx[k])) hits.push_back(cidx[k]);
+    }
+    for (uint32_t v : unbounded)
+      if (passes(v, pv) && reached(v)) hits.push_back(v);
+    if (hits.empty()) return -1;
+    if (hits.size() == 1) {
+      root = hits[0];
+      return hits[0];
+    }
+    return walk(pv);
   };
   if (out_.mode == "probepoint") {
     for (auto& pv : out_.probes) {
