@@ -12,9 +12,31 @@
 #include <memory>
 #include <mutex>
 #include <thread>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 namespace tf {
+
+// Allocator whose vectors default-initialise their elements: large scratch
+// arrays that are filled completely are not zeroed first (on one thread)
+// and are first touched by the parallel loops that fill them.
+template <typename T, typename A = std::allocator<T>>
+struct default_init_allocator : A {
+  using A::A;
+  template <typename U>
+  struct rebind {
+    using other = default_init_allocator<U, typename std::allocator_traits<A>::template rebind_alloc<U>>;
+  };
+  template <typename U>
+  void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <typename U, typename... Args>
+  void construct(U* p, Args&&... args) {
+    std::allocator_traits<A>::construct(static_cast<A&>(*this), p, std::forward<Args>(args)...);
+  }
+};
 
 // threads <= 0: all hardware threads
 inline int host_threads(int threads) {

@@ -176,7 +176,7 @@ double tridiag_max(const std::vector<double>& a, const std::vector<double>& bf) 
 // their given order (a counting sort), then each row is sorted by column with
 // a stable sort: the same order as one stable sort by (row, column), so
 // duplicates are summed in the order they were given, for any thread count.
-HostCsr HostCsr::build(uint32_t nr, uint32_t nc, std::vector<Trip>& t, int threads) {
+HostCsr HostCsr::build(uint32_t nr, uint32_t nc, Trips& t, int threads) {
   HostCsr m;
   m.nrows = nr;
   m.ncols = nc;
@@ -220,16 +220,16 @@ HostCsr HostCsr::build(uint32_t nr, uint32_t nc, std::vector<Trip>& t, int threa
     }
     rbeg[R] = o;
   }
-  std::vector<Trip> tmp(t.size());
+  Trips tmp(t.size());
   parallel_for(P, (int)P, [&](int64_t c0, int64_t c1) {
     for (int64_t c = c0; c < c1; c++) {
       int64_t* pos = &cc[c * R];
       for (int64_t k = nt_ * c / P; k < nt_ * (c + 1) / P; k++) tmp[pos[range_of(t[k].r)]++] = t[k];
     }
   }, 1);
-  std::vector<Trip>().swap(t);
+  Trips().swap(t);
   std::vector<int64_t> start(nr + 1, 0);
-  std::vector<CV> b(tmp.size());
+  std::vector<CV, default_init_allocator<CV>> b(tmp.size());
   parallel_for(R, (int)R, [&](int64_t q0, int64_t q1) {
     for (int64_t q = q0; q < q1; q++) {
       const int64_t r0 = rcut[q], r1 = rcut[q + 1];
@@ -248,7 +248,7 @@ HostCsr HostCsr::build(uint32_t nr, uint32_t nc, std::vector<Trip>& t, int threa
     }
   }, 1);
   start[nr] = (int64_t)b.size();
-  std::vector<Trip>().swap(tmp);
+  Trips().swap(tmp);
   std::vector<int64_t> cnt(nr + 1, 0);
   parallel_for(nr, threads, [&](int64_t r0, int64_t r1) {
     for (int64_t r = r0; r < r1; r++) {
@@ -511,7 +511,7 @@ void TetSim::read_mesh() {
   }
   // C^T: edge -> faces ascending, sign in bit 31
   {
-    std::vector<HostCsr::Trip> t;
+    HostCsr::Trips t;
     t.reserve(3 * (size_t)NF);
     for (uint32_t f = 0; f < NF; f++) {
       t.push_back({(uint32_t)fte_[f][0], f, 1.0});
@@ -681,7 +681,7 @@ void TetSim::build_ops() {
         for (int k = 0; k < 16; k++) off[v + 1] += blk[16 * v + k] != 0;
     });
     for (uint32_t v = 0; v < L; v++) off[v + 1] += off[v];
-    std::vector<HostCsr::Trip> t(off[L]);
+    HostCsr::Trips t(off[L]);
     parallel_for(L, nth, [&](int64_t v0, int64_t v1) {
       for (int64_t v = v0; v < v1; v++) {
         int64_t w = off[v];
@@ -711,11 +711,11 @@ void TetSim::build_ops() {
     // node stars in parallel, each into its own lists, then concatenated in
     // node order (the order a sequential pass would list them)
     const size_t NP = pts_.size();
-    std::vector<std::vector<HostCsr::Trip>> ein_n(NP), h_n(NP);
+    std::vector<HostCsr::Trips> ein_n(NP), h_n(NP);
     parallel_for((int64_t)NP, nth, [&](int64_t n0, int64_t n1) {
       for (uint32_t nid = (uint32_t)n0; nid < (uint32_t)n1; nid++) {
-        std::vector<HostCsr::Trip>& einv_t = ein_n[nid];
-        std::vector<HostCsr::Trip>& h_t = h_n[nid];
+        HostCsr::Trips& einv_t = ein_n[nid];
+        HostCsr::Trips& h_t = h_n[nid];
         const int64_t b0 = star_ptr_[nid];
         const int n = (int)(star_ptr_[nid + 1] - b0);
         std::vector<double> E(n * n, 0.0);
@@ -768,12 +768,12 @@ void TetSim::build_ops() {
         }
       }
     });
-    std::vector<HostCsr::Trip> einv_t, h_t;
+    HostCsr::Trips einv_t, h_t;
     for (size_t nid = 0; nid < NP; nid++) {
       einv_t.insert(einv_t.end(), ein_n[nid].begin(), ein_n[nid].end());
       h_t.insert(h_t.end(), h_n[nid].begin(), h_n[nid].end());
-      std::vector<HostCsr::Trip>().swap(ein_n[nid]);
-      std::vector<HostCsr::Trip>().swap(h_n[nid]);
+      HostCsr::Trips().swap(ein_n[nid]);
+      HostCsr::Trips().swap(h_n[nid]);
     }
     HostCsr Einv = HostCsr::build(NE, NE, einv_t, nth);
     H_ = HostCsr::build(NE, NE, h_t, nth);
@@ -781,7 +781,7 @@ void TetSim::build_ops() {
   } else {
     // gfdtd eps-mass from the node dual bases (Discretization.hpp:8357-8621):
     // nine entries per (node, tet) pair at fixed positions, formed in parallel
-    std::vector<HostCsr::Trip> t(9 * nvol_.size());
+    HostCsr::Trips t(9 * nvol_.size());
     parallel_for((int64_t)pts_.size(), nth, [&](int64_t n0, int64_t n1) {
       for (uint32_t nid = (uint32_t)n0; nid < (uint32_t)n1; nid++)
         for (int64_t q = nvol_ptr_[nid]; q < nvol_ptr_[nid + 1]; q++) {

@@ -10,6 +10,7 @@
 #include <string>
 #include <vector>
 
+#include "host_parallel.hpp"
 #include "script.hpp"
 #include "sim.hpp"
 #include "tet_kernels.cuh"
@@ -29,8 +30,9 @@ struct HostCsr {
     uint32_t r, c;
     double v;
   };
-  // threads: host threads for the per-row work (<= 0: all)
-  static HostCsr build(uint32_t nr, uint32_t nc, std::vector<Trip>& t, int threads = 1);
+  using Trips = std::vector<Trip, default_init_allocator<Trip>>;
+  // threads: host threads for the per-row work (<= 0: all); t is consumed
+  static HostCsr build(uint32_t nr, uint32_t nc, Trips& t, int threads = 1);
   void mul(const double* x, double* y, int threads = 1) const;
 };
 
