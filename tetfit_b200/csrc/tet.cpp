@@ -428,15 +428,17 @@ void TetSim::read_mesh() {
   std::vector<std::pair<uint64_t, uint32_t>> fk(4 * (size_t)L);
   std::vector<std::array<int32_t, 3>> ftup;
   if (!packed) ftup.resize(4 * (size_t)L);
-  for (uint32_t k = 0; k < L; k++) {
-    const auto& t = vols_[k];
-    const int32_t tri[4][3] = {{t[0], t[1], t[2]}, {t[0], t[1], t[3]}, {t[0], t[2], t[3]}, {t[1], t[2], t[3]}};
-    for (int q = 0; q < 4; q++) {
-      size_t slot = k + (size_t)q * L;
-      fk[slot] = {packed ? fkey(tri[q][0], tri[q][1], tri[q][2]) : slot, (uint32_t)slot};
-      if (!packed) ftup[slot] = {tri[q][0], tri[q][1], tri[q][2]};
+  parallel_for(L, nth, [&](int64_t k0, int64_t k1) {
+    for (int64_t k = k0; k < k1; k++) {
+      const auto& t = vols_[k];
+      const int32_t tri[4][3] = {{t[0], t[1], t[2]}, {t[0], t[1], t[3]}, {t[0], t[2], t[3]}, {t[1], t[2], t[3]}};
+      for (int q = 0; q < 4; q++) {
+        size_t slot = k + (size_t)q * L;
+        fk[slot] = {packed ? fkey(tri[q][0], tri[q][1], tri[q][2]) : slot, (uint32_t)slot};
+        if (!packed) ftup[slot] = {tri[q][0], tri[q][1], tri[q][2]};
+      }
     }
-  }
+  });
   // (key, slot) pairs are distinct: any sort gives this order
   if (packed) parallel_stable_sort(fk.begin(), fk.end(), nth, std::less<std::pair<uint64_t, uint32_t>>());
   else
@@ -469,14 +471,16 @@ void TetSim::read_mesh() {
     vtf_[k] = {f3, f2, f1, f0};  // opposite nodes 0..3 (Discretization.hpp:6239-6267)
   }
   // edges
-  std::vector<uint64_t> ek(3 * (size_t)NF);
-  for (uint32_t f = 0; f < NF; f++) {
-    const auto& s = faces_[f];
-    ek[f] = ((uint64_t)s[0] << 32) | (uint32_t)s[1];
-    ek[f + NF] = ((uint64_t)s[0] << 32) | (uint32_t)s[2];
-    ek[f + 2 * (size_t)NF] = ((uint64_t)s[1] << 32) | (uint32_t)s[2];
-  }
-  std::vector<uint64_t> eu(ek);
+  std::vector<uint64_t, default_init_allocator<uint64_t>> ek(3 * (size_t)NF);
+  parallel_for(NF, nth, [&](int64_t f0, int64_t f1) {
+    for (int64_t f = f0; f < f1; f++) {
+      const auto& s = faces_[f];
+      ek[f] = ((uint64_t)s[0] << 32) | (uint32_t)s[1];
+      ek[f + NF] = ((uint64_t)s[0] << 32) | (uint32_t)s[2];
+      ek[f + 2 * (size_t)NF] = ((uint64_t)s[1] << 32) | (uint32_t)s[2];
+    }
+  });
+  std::vector<uint64_t> eu(ek.begin(), ek.end());
   parallel_stable_sort(eu.begin(), eu.end(), nth, std::less<uint64_t>());
   eu.erase(std::unique(eu.begin(), eu.end()), eu.end());
   edges_.resize(eu.size());
@@ -511,13 +515,14 @@ void TetSim::read_mesh() {
   }
   // C^T: edge -> faces ascending, sign in bit 31
   {
-    HostCsr::Trips t;
-    t.reserve(3 * (size_t)NF);
-    for (uint32_t f = 0; f < NF; f++) {
-      t.push_back({(uint32_t)fte_[f][0], f, 1.0});
-      t.push_back({(uint32_t)fte_[f][1], f, -1.0});
-      t.push_back({(uint32_t)fte_[f][2], f, 1.0});
-    }
+    HostCsr::Trips t(3 * (size_t)NF);
+    parallel_for(NF, nth, [&](int64_t f0, int64_t f1) {
+      for (int64_t f = f0; f < f1; f++) {
+        t[3 * f] = {(uint32_t)fte_[f][0], (uint32_t)f, 1.0};
+        t[3 * f + 1] = {(uint32_t)fte_[f][1], (uint32_t)f, -1.0};
+        t[3 * f + 2] = {(uint32_t)fte_[f][2], (uint32_t)f, 1.0};
+      }
+    });
     Ct_ = HostCsr::build(NE, NF, t, nth);
   }
   // boundary faces and their dual edges (Discretization.hpp:6380-6489)
