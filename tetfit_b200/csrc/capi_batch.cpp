@@ -87,10 +87,11 @@ int tf_batch_open(const char* const* scripts, const uint32_t* labels, uint32_t n
     std::vector<std::string> errs(n);
     std::vector<int> codes(n, TF_OK);
     std::atomic<uint32_t> next{0};
-    unsigned nt = o.host_threads > 0 ? (unsigned)o.host_threads : std::max(1u, std::thread::hardware_concurrency());
-    nt = std::min<unsigned>(nt, n);
+    const unsigned limit =
+        o.host_threads > 0 ? (unsigned)o.host_threads : std::max(1u, std::thread::hardware_concurrency());
+    const unsigned nt = std::min<unsigned>(limit, n);
     // members are built nt at a time; each takes its share of the host threads
-    ro.setup_threads = (int)std::max(1u, std::max(1u, std::thread::hardware_concurrency()) / nt);
+    ro.setup_threads = (int)std::max(1u, limit / nt);
     // host build of every member (mesh, operators, probes, source tables)
     auto work = [&]() {
       for (uint32_t i = next++; i < n; i = next++) {
@@ -121,7 +122,7 @@ int tf_batch_open(const char* const* scripts, const uint32_t* labels, uint32_t n
       if (codes[i] != TF_OK) return bfail(b, codes[i], "batch member " + std::to_string(i) + ": " + errs[i]);
     // the device image is laid out by this thread alone: all host threads
     tf::RunOptions rg = ro;
-    rg.setup_threads = 0;
+    rg.setup_threads = (int)limit;
     if (b->mode == 0) {
       std::vector<tf::TetSim*> v;
       for (auto& s : b->sims) v.push_back(s.get());
