@@ -56,7 +56,7 @@ typedef struct tf_opts {
   int32_t cg_maxiter;   /* 0: 100, the reference's limit                             */
   int32_t batch_mode;   /* tf_batch_open: 0 all members advance together in one
                            group, 1 each member alone (one after another)       */
-  int32_t host_threads; /* tf_batch_open: host threads of the set-up, 0 all    */
+  int32_t host_threads; /* host threads of the set-up (tf_prepare, tf_batch_open), 0 all */
   int32_t learn_steps;  /* warm_start 3: steps whose solutions train the network
                            (0: 500); the extrapolation is used meanwhile         */
   int32_t fit_variant;  /* fdtd: 0 automatic (first steps time the variants on grids
