@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <functional>
@@ -620,14 +621,14 @@ void FitSim::locate_probes_and_dipoles() {
   std::vector<uint8_t> colour(ncell, 0);
   std::vector<size_t> touched;
   size_t root = 0;
-  auto find = [&](const std::array<double, 3>& pv) -> int64_t {
+  const double tol = 1e-12;
+  auto walk = [&](const std::array<double, 3>& pv) -> int64_t {
     for (size_t t : touched) colour[t] = 0;
     touched.clear();
     std::vector<size_t> q;
     q.push_back(root);
     colour[0] = 1;
     touched.push_back(0);
-    const double tol = 1e-12;
     for (size_t h = 0; h < q.size(); h++) {
       size_t v = q[h];
       int i = (int)(v % Nx_), j = (int)((v / Nx_) % Ny_), k = (int)(v / ((size_t)Nx_ * Ny_));
@@ -651,6 +652,58 @@ void FitSim::locate_probes_and_dipoles() {
       if (!colour[v]) { colour[v] = 1; touched.push_back(v); }
     }
     return -1;
+  };
+  // The walk's answer without the walk.  The test is one interval per axis,
+  // so the cubes that pass are the products of the (one or two) indices that
+  // pass on each axis.  The walk reaches every cube but cube 0 (marked from
+  // the start; a box grid without a corner cube stays connected) and cube 0
+  // itself only from root 0.  No cube that passes: the walk finds none; one,
+  // or a single nearest one: it is the walk's answer; two or more at the same
+  // distance: the walk decides, in its own order.
+  const int N[3] = {Nx_, Ny_, Nz_};
+  auto find = [&](const std::array<double, 3>& pv) -> int64_t {
+    std::vector<int> ax[3];
+    for (int a = 0; a < 3; a++) {
+      const int g = (int)(std::upper_bound(xs_[a].begin(), xs_[a].begin() + N[a], pv[a]) - xs_[a].begin()) - 1;
+      for (int i = std::max(0, g - 1); i <= std::min(N[a] - 1, g + 1); i++) {
+        const double d = pv[a] - xs_[a][i];
+        if (d >= -tol && d < L_[a] + tol) ax[a].push_back(i);
+      }
+    }
+    std::vector<size_t> hits;
+    for (int k : ax[2])
+      for (int j : ax[1])
+        for (int i : ax[0]) {
+          const size_t v = (size_t)i + (size_t)Nx_ * ((size_t)j + (size_t)Ny_ * k);
+          if (root == 0 || v != 0) hits.push_back(v);
+        }
+    if (hits.empty()) return -1;
+    // The walk visits cubes in order of their index distance from the root
+    // (|di| + |dj| + |dk|: cube 0 lengthens no shortest path to another
+    // cube, a monotone path can always pass around a corner), so among cubes
+    // that pass, a single nearest one is the walk's answer.
+    auto dist = [&](size_t v) {
+      const int64_t i = (int64_t)(v % Nx_), j = (int64_t)((v / Nx_) % Ny_), k = (int64_t)(v / ((size_t)Nx_ * Ny_));
+      const int64_t i0 = (int64_t)(root % Nx_), j0 = (int64_t)((root / Nx_) % Ny_),
+                    k0 = (int64_t)(root / ((size_t)Nx_ * Ny_));
+      return std::llabs(i - i0) + std::llabs(j - j0) + std::llabs(k - k0);
+    };
+    size_t best = hits[0];
+    int nbest = 1;
+    for (size_t q = 1; q < hits.size(); q++) {
+      const int64_t dq = dist(hits[q]), db = dist(best);
+      if (dq < db) {
+        best = hits[q];
+        nbest = 1;
+      } else if (dq == db) {
+        nbest++;
+      }
+    }
+    if (nbest == 1) {
+      root = best;
+      return (int64_t)best;
+    }
+    return walk(pv);
   };
   if (out_.mode == "probepoint") {
     for (auto& pv : out_.probes) {
