@@ -62,7 +62,9 @@ typedef struct tf_opts {
   int32_t fit_variant;  /* fdtd: 0 automatic (first steps time the variants on grids
                            of 2 M cells or more), k > 0 forces variant k - 1 for
                            both halves (all give bitwise identical results)     */
-  int32_t reserved[3];
+  int32_t file_digits;  /* tf_run: significant digits of the probe files (0: 6, the
+                           reference's default stream precision; 17 round-trips) */
+  int32_t reserved[2];
 } tf_opts;
 
 typedef struct tf_info {

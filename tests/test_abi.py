@@ -66,3 +66,12 @@ def test_unknown_label_and_order_errors(tmp_path, product_lib):
         d.prepare(7)
     assert ei.value.code == tb.TF_E_ARG
     d.close()
+
+
+def test_file_digits_out_of_range_is_rejected(tmp_path, product_lib):
+    script = write_fit_cavity(str(tmp_path), FitCase(n=8, steps=5))
+    d = tb.Discretization(script)
+    with pytest.raises(tb.TetfitError) as ei:
+        d.prepare(1, file_digits=18)
+    assert ei.value.code == tb.TF_E_ARG and "file_digits" in ei.value.message
+    d.close()

@@ -103,3 +103,22 @@ def test_cli_writes_reference_files(cli, tmp_path, kind):
     assert P.shape == (len(flux), 3)
     assert close(P[:, 1], flux)
     assert info is not None
+
+
+@pytest.mark.gpu
+def test_cli_digits_round_trip(cli, tmp_path):
+    """--digits 17: the probe files carry the values exactly."""
+    src = tmp_path / "case"
+    src.mkdir()
+    script = write_fit_cavity(str(src), FitCase(n=8, steps=10))
+    work = tmp_path / "run"
+    work.mkdir()
+    r = run(cli, ["--digits", "17", script], work)
+    assert r.returncode == 0, r.stdout + r.stderr
+    E = read_columns(glob.glob(str(work / "*00001_probe_E.dat"))[0])
+    with tb.Discretization(script) as d:
+        d.prepare(1, precision="fp64", device=0)
+        d.step(10 ** 9)
+        t, v = d.probes()
+    assert np.array_equal(E[:, 3], np.repeat(t, v.shape[1]))
+    assert np.array_equal(E[:, 4:], v[:, :, :3].reshape(-1, 3))

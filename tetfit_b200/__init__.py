@@ -35,7 +35,8 @@ class Opts(ctypes.Structure):
                 ("verbose", ctypes.c_int32), ("graph_steps", ctypes.c_int32), ("mass_model", ctypes.c_int32),
                 ("warm_start", ctypes.c_int32), ("cg_criterion", ctypes.c_int32), ("cg_maxiter", ctypes.c_int32),
                 ("batch_mode", ctypes.c_int32), ("host_threads", ctypes.c_int32), ("learn_steps", ctypes.c_int32),
-                ("fit_variant", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
+                ("fit_variant", ctypes.c_int32), ("file_digits", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 2)]
 
 
 class Info(ctypes.Structure):
@@ -245,7 +246,7 @@ class Discretization:
     @staticmethod
     def _opts(precision="fp64", device=0, write_files=False, verbose=False, graph_steps=0, mass="reference",
               warm_start="previous", cg_criterion="reference", cg_maxiter=0, batch_mode=0, host_threads=0,
-              learn_steps=0, fit_variant=0) -> Opts:
+              learn_steps=0, fit_variant=0, file_digits=0) -> Opts:
         o = Opts()
         lib().tf_default_opts(ctypes.byref(o))
         o.precision = {"fp64": FP64, "fp32": FP32}[precision] if isinstance(precision, str) else int(precision)
@@ -258,6 +259,7 @@ class Discretization:
         o.host_threads = host_threads
         o.learn_steps = learn_steps
         o.fit_variant = fit_variant
+        o.file_digits = file_digits
         return o
 
     def prepare(self, label: int, **opts) -> dict:

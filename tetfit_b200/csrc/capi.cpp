@@ -69,6 +69,10 @@ void write_outputs(tf_ctx* c) {
     se << o.name << std::setw(5) << std::setfill('0') << c->label << "_probe_E.dat";
     sh << o.name << std::setw(5) << std::setfill('0') << c->label << "_probe_H.dat";
     std::ofstream os(se.str()), osh(sh.str());
+    if (c->opts.file_digits > 0) {  // more digits than the reference's default 6 (an extension)
+      os.precision(c->opts.file_digits);
+      osh.precision(c->opts.file_digits);
+    }
     for (size_t k = 0; k < ns; k++)
       for (size_t p = 0; p < np; p++) {
         const double* s = &v[(k * np + p) * 6];
@@ -170,6 +174,7 @@ int tf_prepare(tf_ctx* c, uint32_t label, const tf_opts* opts) {
     ro.fit_variant = c->opts.fit_variant;
     ro.setup_threads = c->opts.host_threads > 0 ? c->opts.host_threads : 0;
     if (ro.fit_variant < 0 || ro.fit_variant > 4) return fail(c, TF_E_ARG, "fit_variant must be 0..4");
+    if (c->opts.file_digits < 0 || c->opts.file_digits > 17) return fail(c, TF_E_ARG, "file_digits must be 0..17");
     if (meth == "fdtd") {
       c->fit.reset(new tf::FitSim(c->sc, label, ro));
     } else if (meth == "dga" || meth == "gfdtd") {

@@ -4,7 +4,10 @@
 // (<name><label>_probe_E.dat / _probe_H.dat) and poynting.dat into the
 // working directory.
 //
-//   tetfit [--fp32] [--device N] input_file
+//   tetfit [--fp32] [--device N] [--digits D] input_file
+//
+// --digits D writes the probe files with D significant digits (the reference
+// writes 6).
 //
 // With no input file it prints the reference's "Input file missing!" text.
 // Script errors print the reference's "Input file error at line N: ..." text.
@@ -38,6 +41,8 @@ int main(int argc, char** argv) {
       o.precision = TF_FP32;
     } else if (std::strcmp(argv[k], "--device") == 0 && k + 1 < argc) {
       o.device = std::atoi(argv[++k]);
+    } else if (std::strcmp(argv[k], "--digits") == 0 && k + 1 < argc) {
+      o.file_digits = std::atoi(argv[++k]);
     } else if (argv[k][0] == '-' && argv[k][1] == '-') {
       std::printf("unknown option %s\n", argv[k]);
       return 1;
