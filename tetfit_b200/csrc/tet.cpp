@@ -452,11 +452,23 @@ void TetSim::read_mesh() {
     const int32_t tri[4][3] = {{t[0], t[1], t[2]}, {t[0], t[1], t[3]}, {t[0], t[2], t[3]}, {t[1], t[2], t[3]}};
     return {tri[q][0], tri[q][1], tri[q][2]};
   };
-  for (size_t q = 0; q < fk.size(); q++) {
-    auto tup = face_tuple(fk[q].second);
-    if (faces_.empty() || faces_.back() != tup) faces_.push_back(tup);
-    flab[fk[q].second] = (int32_t)faces_.size() - 1;
-  }
+  // a new face starts wherever the sorted tuple changes: mark, number by a
+  // prefix, then place (the numbering of one sequential pass)
+  const int64_t nk = (int64_t)fk.size();
+  std::vector<int32_t> fid(nk);
+  parallel_for(nk, nth, [&](int64_t q0, int64_t q1) {
+    for (int64_t q = q0; q < q1; q++)
+      fid[q] = q == 0 || face_tuple(fk[q].second) != face_tuple(fk[q - 1].second) ? 1 : 0;
+  });
+  for (int64_t q = 1; q < nk; q++) fid[q] += fid[q - 1];  // 1-based face number
+  faces_.resize(nk ? (size_t)fid[nk - 1] : 0);
+  parallel_for(nk, nth, [&](int64_t q0, int64_t q1) {
+    for (int64_t q = q0; q < q1; q++) {
+      const int32_t f = fid[q] - 1;
+      if (q == 0 || fid[q] != fid[q - 1]) faces_[f] = face_tuple(fk[q].second);
+      flab[fk[q].second] = f;
+    }
+  });
   fk.clear();
   fk.shrink_to_fit();
   const uint32_t NF = (uint32_t)faces_.size();
