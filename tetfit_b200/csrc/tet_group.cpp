@@ -23,8 +23,8 @@ int64_t up32(int64_t n) { return (n + 31) & ~int64_t(31); }
 template <typename T>
 struct SellHost {
   std::vector<int64_t> ptr{0};
-  std::vector<int32_t> col;
-  std::vector<T> val;
+  std::vector<int32_t, default_init_allocator<int32_t>> col;  // every slot is written
+  std::vector<T, default_init_allocator<T>> val;
   // rows [0, nrows) of one simulation, nrows % 32 == 0; rows p >= nreal are
   // padding.  len(p): entries of row p; ent(p, j, c, v): entry j; pad(p):
   // column of a padding entry.
@@ -40,7 +40,7 @@ struct SellHost {
           if (32 * q + l < nreal) ml = std::max(ml, (int)len(32 * q + l));
         ptr[s_base + q + 1] = 32 * (int64_t)ml;
       }
-    });
+    }, 64);
     for (int64_t q = 0; q < ns; q++) ptr[s_base + q + 1] += ptr[s_base + q];
     col.resize(ptr.back());
     if (values) val.resize(ptr.back());
@@ -61,7 +61,7 @@ struct SellHost {
           }
         }
       }
-    });
+    }, 64);
   }
 };
 
@@ -75,8 +75,8 @@ void* TetGroup::dalloc(size_t bytes) {
   return p;
 }
 
-template <typename V>
-void* TetGroup::upload(const std::vector<V>& v) {
+template <typename V, typename A>
+void* TetGroup::upload(const std::vector<V, A>& v) {
   void* p = dalloc(v.size() * sizeof(V));
   if (!v.empty()) CU(cudaMemcpy(p, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice));
   return p;
@@ -111,8 +111,28 @@ template <typename T>
 void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
   const int S = (int)sims.size();
   SellHost<T> A, Ef, N, Ct;
-  std::vector<int32_t> fte, free_edge, dir_edge;
-  std::vector<T> pre, U0, I0, Src0;
+  std::vector<int32_t, default_init_allocator<int32_t>> fte, free_edge;  // filled completely
+  std::vector<int32_t> dir_edge;
+  std::vector<T, default_init_allocator<T>> pre, U0, I0, Src0;
+  {
+    // capacity for the stored entries (plus slice padding, which the class
+    // grouping keeps small), so the members' appends rarely reallocate
+    size_t na = 0, ne = 0, nc = 0, nn = 0;
+    for (TetSim* t : sims) {
+      na += t->A_.val.size();
+      ne += t->E_.val.size();
+      nc += t->Ct_.col.size();
+      nn += t->N_.val.size();
+    }
+    auto room = [](size_t x) { return x + x / 8 + 4096; };
+    A.col.reserve(room(na));
+    A.val.reserve(room(na));
+    Ef.col.reserve(room(ne));
+    Ef.val.reserve(room(ne));
+    Ct.col.reserve(room(nc));
+    N.col.reserve(room(nn));
+    N.val.reserve(room(nn));
+  }
   std::vector<uint16_t> slice_sim, fslice_sim;
   std::vector<double> dt(S), tol(S);
   std::vector<int> nsteps(S);
@@ -154,11 +174,12 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
       for (int64_t k = 0; k < nf; k++) {
         key.clear();
         for (int64_t q = t.A_.ptr[k]; q < t.A_.ptr[k + 1]; q++) key.push_back((int32_t)(t.A_.col[q] - k));
-        cls[k] = classes.emplace(key, (int32_t)classes.size()).first->second;
+        cls[k] = classes.try_emplace(key, (int32_t)classes.size()).first->second;  // no node for known keys
       }
     }
     std::iota(old_of_new.begin(), old_of_new.end(), 0);
-    std::stable_sort(old_of_new.begin(), old_of_new.end(), [&](int32_t a, int32_t b) { return cls[a] < cls[b]; });
+    parallel_stable_sort(old_of_new.begin(), old_of_new.end(), opt_.setup_threads,
+                         [&](int32_t a, int32_t b) { return cls[a] < cls[b]; });
     for (int64_t p = 0; p < nf; p++) pos[old_of_new[p]] = (int32_t)p;
     A.append(
         nfp, nf, [&](int64_t p) { return alen_old(old_of_new[p]); },
@@ -194,20 +215,34 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
           v = t.N_.val[q];
         },
         [&](int64_t f) { return (int32_t)(foff + f); }, true, opt_.setup_threads);
-    for (int64_t f = 0; f < NFp; f++)
-      for (int k = 0; k < 3; k++) fte.push_back(f < NF ? (int32_t)(eoff + t.fte_[f][k]) : -1);
-    for (int64_t p = 0; p < nfp; p++) {
-      pre.push_back(p < nf ? (T)t.jacobi_[old_of_new[p]] : (T)0);
-      free_edge.push_back(p < nf ? (int32_t)(eoff + t.free_edges_[old_of_new[p]]) : -1);
-    }
+    const int nth = opt_.setup_threads;
+    const size_t f0 = fte.size(), r0 = pre.size(), e0 = U0.size();
+    fte.resize(f0 + 3 * (size_t)NFp);
+    pre.resize(r0 + nfp);
+    free_edge.resize(r0 + nfp);
+    U0.resize(e0 + NE);
+    I0.resize(e0 + NE);
+    Src0.resize(e0 + NE);
+    parallel_for(NFp, nth, [&](int64_t a0, int64_t a1) {
+      for (int64_t f = a0; f < a1; f++)
+        for (int k = 0; k < 3; k++) fte[f0 + 3 * f + k] = f < NF ? (int32_t)(eoff + t.fte_[f][k]) : -1;
+    });
+    parallel_for(nfp, nth, [&](int64_t a0, int64_t a1) {
+      for (int64_t p = a0; p < a1; p++) {
+        pre[r0 + p] = p < nf ? (T)t.jacobi_[old_of_new[p]] : (T)0;
+        free_edge[r0 + p] = p < nf ? (int32_t)(eoff + t.free_edges_[old_of_new[p]]) : -1;
+      }
+    });
+    parallel_for(NE, nth, [&](int64_t a0, int64_t a1) {
+      for (int64_t e = a0; e < a1; e++) {
+        U0[e0 + e] = (T)t.init_U_[e];
+        I0[e0 + e] = (T)t.init_I_[e];
+        Src0[e0 + e] = (T)t.init_src_[e];
+      }
+    });
     for (int32_t e : t.dir_edges_) dir_edge.push_back((int32_t)(eoff + e));
     slice_sim.insert(slice_sim.end(), nfp / 32, (uint16_t)s);
     fslice_sim.insert(fslice_sim.end(), NFp / 32, (uint16_t)s);
-    for (int64_t e = 0; e < NE; e++) {
-      U0.push_back((T)t.init_U_[e]);
-      I0.push_back((T)t.init_I_[e]);
-      Src0.push_back((T)t.init_src_[e]);
-    }
     dt[s] = t.dt_;
     tol[s] = t.sim_.tol;
     nsteps[s] = (int)t.nsteps_;
@@ -301,9 +336,9 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
     o.ptr = (const int64_t*)upload(m.ptr);
     o.col = (const int32_t*)upload(m.col);
     o.val = values ? upload(m.val) : nullptr;
-    std::vector<int64_t>().swap(m.ptr);
-    std::vector<int32_t>().swap(m.col);
-    std::vector<T>().swap(m.val);
+    decltype(m.ptr)().swap(m.ptr);
+    decltype(m.col)().swap(m.col);
+    decltype(m.val)().swap(m.val);
   };
   put(N, d.N, true);
   put(Ef, d.Ef, true);

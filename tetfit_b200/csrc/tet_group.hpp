@@ -74,8 +74,8 @@ class TetGroup {
   void check_err();
   void launch(int n, cudaEvent_t* ev);
   void* dalloc(size_t bytes);
-  template <typename V>
-  void* upload(const std::vector<V>& v);
+  template <typename V, typename A>
+  void* upload(const std::vector<V, A>& v);
 
   RunOptions opt_;
   std::vector<Meta> meta_;
