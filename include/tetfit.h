@@ -167,8 +167,10 @@ TF_API int tf_pcg_solve(const tf_pcg_args* args, int32_t* iters, double* rel_res
  * call on a device looks up the array's device address (once per device, that
  * device current); make that first call before any stream capture.  All calls
  * share the one array: calls that overlap on the GPU (other streams, other host
- * threads) race and must be serialised by the caller.  Same arguments, results
- * and status codes as tf_pcg_solve. */
+ * threads) race and must be serialised by the caller.  The address lookup is
+ * kept for the life of the process, so cudaDeviceReset (which reloads the
+ * module) is not supported while the library is loaded.  Same arguments,
+ * results and status codes as tf_pcg_solve. */
 TF_API int tf_pcg_solve_noalloc(const tf_pcg_args* args, int32_t* iters, double* rel_resid);
 /* Self-check of the bounded grid barrier that the persistent CG kernels (the
  * batch/gfdtd solve and tf_pcg_solve) use; no reference counterpart.  `blocks`

@@ -8,6 +8,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -17,7 +18,8 @@ CLI_SOURCE = os.path.join(CSRC, "tetfit_main.cpp")
 SOURCES = ["script.cpp", "fit.cpp", "fit_kernels.cu", "tet.cpp", "tet_kernels.cu", "tet_group.cpp",
            "tet_group_kernels.cu", "mlp.cu", "pcg.cu", "barrier_check.cu", "capi.cpp", "capi_batch.cpp"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
-              "-Xcompiler", "-fPIC", "-shared", "-Xcompiler", "-fvisibility=hidden"]
+              "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
+OBJ_DIR = os.path.join(HERE, "_build")
 
 
 def sources():
@@ -48,7 +50,19 @@ def build_cli(verbose: bool = False) -> str:
 def build(force: bool = False, verbose: bool = False) -> str:
     if force or needs_build():
         nvcc = os.environ.get("NVCC", "nvcc")
-        cmd = [nvcc] + NVCC_FLAGS + sources() + ["-o", OUT + ".tmp"]
+        os.makedirs(OBJ_DIR, exist_ok=True)
+        objs = [os.path.join(OBJ_DIR, os.path.splitext(s)[0] + ".o") for s in SOURCES]
+
+        def compile_one(src_obj):
+            cmd = [nvcc] + NVCC_FLAGS + ["-c", src_obj[0], "-o", src_obj[1]]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True, cwd=CSRC)
+
+        # one nvcc per source file, in parallel, then one link
+        with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as ex:
+            list(ex.map(compile_one, zip(sources(), objs)))
+        cmd = [nvcc] + NVCC_FLAGS + ["-shared"] + objs + ["-o", OUT + ".tmp"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True, cwd=CSRC)

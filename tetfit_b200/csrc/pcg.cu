@@ -141,6 +141,9 @@ int g_scratch_blocks[kMaxDevices] = {0};
 
 // Device address of the array on `device` (which must be current), looked
 // up once per device: in host code the symbol name is only a host-side handle.
+// The address is kept for the life of the process; cudaDeviceReset reloads
+// the module and may move the array, so it is not supported while this
+// library is loaded.
 int scratch_for(int device, double** addr, int* blocks) {
   if (device < 0 || device >= kMaxDevices) {
     tf::set_thread_error("tf_pcg_solve_noalloc: device ordinal out of range");
