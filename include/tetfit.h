@@ -91,6 +91,13 @@ typedef struct tf_info {
 
 /* Parse a .fdtd script (Discretization(std::string), Discretization.hpp:45-211). */
 TF_API int tf_open(const char* fdtd_path, tf_ctx** out);
+/* The parsed script as canonical JSON (no reference counterpart: the parsed
+ * primitives of Discretization.hpp:45-211 made visible): materials, bcs,
+ * meshes, sources, simulations and outputs by ascending label with doubles to
+ * 17 significant digits, the 100-slot surface-to-bc table, and the solids of
+ * each cartesian mesh file.  *len receives the size needed including the
+ * terminating 0; a smaller non-zero cap returns TF_E_ARG with the text cut. */
+TF_API int tf_script_dump(tf_ctx* ctx, char* buf, size_t cap, size_t* len);
 /* Simulation labels in ascending order (the order dga_main.cpp:52-62 runs them). */
 TF_API int tf_simulations(tf_ctx* ctx, uint32_t* labels, uint32_t cap, uint32_t* n);
 /* Build mesh, operators and device state for one simulation
@@ -111,6 +118,13 @@ TF_API int tf_get_state(tf_ctx* ctx, double* U, size_t nU, double* B, size_t nB,
 TF_API int tf_set_state(tf_ctx* ctx, const double* U, size_t nU, const double* F, size_t nF);
 /* Per-step boundary flux 0.5 (U_old + U) . curl_fb (Discretization.hpp:1901). */
 TF_API int tf_get_flux(tf_ctx* ctx, double* flux, size_t cap, size_t* n);
+/* Per-step Joule loss, the third column of poynting.dat: 0.25 (U_old + U)^T
+ * Si (U_old + U) (fdtd, Discretization.hpp:1902; dga :895; gfdtd :1519).  As
+ * in the reference, the fdtd conductance vector Si is filled only for l2norm
+ * outputs (:5368, :5594-5597), so the loss is zero for other outputs; the
+ * tetrahedral paths accept lossless materials only, so theirs is zero.  FP64
+ * accumulation on the GPU. */
+TF_API int tf_get_losses(tf_ctx* ctx, double* losses, size_t cap, size_t* n);
 /* Discrete leapfrog energy 0.5 U.Me U + 0.5 B_prev.Mnu B (FP64 accumulation). */
 TF_API int tf_energy(tf_ctx* ctx, double* energy);
 /* One step driven from host memory: carrier_in[n_sources] replaces the script

@@ -41,6 +41,7 @@ def lib(omp: bool = False):
         L.orc_fit_probes.argtypes = [P, P, P, P, P]
         L.orc_fit_state.argtypes = [P, P, P, P]
         L.orc_fit_flux.argtypes = [P, P]
+        L.orc_fit_losses.argtypes = [P, P]
         L.orc_fit_topology.argtypes = [P, P, P, P, P]
         L.orc_fit_coeffs.argtypes = [P, P, P, P, P]
         _libs[path] = L
@@ -49,6 +50,21 @@ def lib(omp: bool = False):
 
 def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def script_dump(path: str) -> dict:
+    """The oracle front end's parse of a script, as a dict (raises
+    RuntimeError with the parser's message on a script error)."""
+    import json
+    L = lib()
+    L.orc_script_dump.restype = ctypes.c_long
+    L.orc_script_dump.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_long]
+    n = L.orc_script_dump(os.fsencode(path), None, 0)
+    buf = ctypes.create_string_buffer(max(n, 4096))
+    n = L.orc_script_dump(os.fsencode(path), buf, len(buf))
+    if n < 0:
+        raise RuntimeError(buf.value.decode())
+    return json.loads(buf.value.decode())
 
 
 class FitOracle:
@@ -94,6 +110,12 @@ class FitOracle:
     def flux(self):
         f = np.zeros(self.steps_done)
         self.L.orc_fit_flux(self.h, _p(f))
+        return f
+
+    def losses(self):
+        """Joule loss of every step taken (Discretization.hpp:1902)."""
+        f = np.zeros(self.steps_done)
+        self.L.orc_fit_losses(self.h, _p(f))
         return f
 
     def coeffs(self):

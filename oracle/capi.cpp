@@ -1,7 +1,11 @@
 // ORACLE — test infrastructure only.  extern "C" surface of the CPU oracle,
 // loaded with ctypes by tests/ and by bench.py's cpu_baseline leg.
+#include <array>
+#include <cstdio>
 #include <cstring>
 #include <exception>
+#include <iomanip>
+#include <sstream>
 #include <string>
 
 #include "fit.hpp"
@@ -16,7 +20,201 @@ static void put_err(char* err, int len, const char* m) {
   }
 }
 
+
+// ---------------------------------------------------------------- script dump
+// Canonical JSON of a parsed script: every primitive by ascending label, with
+// doubles printed to 17 significant digits (exact round trip).  The solids of
+// each cartesian mesh are read from its file.
+namespace {
+
+void js_str(std::ostringstream& o, const std::string& s) {
+  o << '"';
+  for (char ch : s) {
+    if (ch == '"' || ch == '\\') o << '\\' << ch;
+    else if ((unsigned char)ch < 0x20) o << "\\u" << std::hex << std::setw(4) << std::setfill('0') << (int)ch
+                                          << std::dec << std::setfill(' ');
+    else o << ch;
+  }
+  o << '"';
+}
+void js_num(std::ostringstream& o, double v) {
+  char b[40];
+  std::snprintf(b, sizeof b, "%.17g", v);
+  o << b;
+}
+template <class V>
+void js_vec(std::ostringstream& o, const V& v) {
+  o << '[';
+  bool first = true;
+  for (const auto& x : v) {
+    if (!first) o << ", ";
+    first = false;
+    js_num(o, (double)x);
+  }
+  o << ']';
+}
+void js_strs(std::ostringstream& o, const std::array<std::string, 3>& v) {
+  o << '[';
+  for (int k = 0; k < 3; k++) {
+    if (k) o << ", ";
+    js_str(o, v[k]);
+  }
+  o << ']';
+}
+void js_mat(std::ostringstream& o, const orc::Mat3& m) {
+  o << '[';
+  for (int r = 0; r < 3; r++) {
+    if (r) o << ", ";
+    o << '[';
+    for (int c = 0; c < 3; c++) {
+      if (c) o << ", ";
+      js_num(o, m.m[r][c]);
+    }
+    o << ']';
+  }
+  o << ']';
+}
+struct Obj {  // comma bookkeeping for one JSON object
+  std::ostringstream& o;
+  bool first = true;
+  explicit Obj(std::ostringstream& os) : o(os) { o << '{'; }
+  std::ostringstream& key(const char* k) {
+    if (!first) o << ", ";
+    first = false;
+    js_str(o, k);
+    o << ": ";
+    return o;
+  }
+  void num(const char* k, double v) { key(k); js_num(o, v); }
+  void str(const char* k, const std::string& v) { key(k); js_str(o, v); }
+  void end() { o << '}'; }
+};
+template <class MapT, class F>
+void js_map(Obj& top, const char* name, const MapT& m, F&& each) {
+  std::ostringstream& o = top.key(name);
+  Obj inner(o);
+  for (const auto& kv : m) {
+    inner.key(std::to_string(kv.first).c_str());
+    each(kv.second);
+  }
+  inner.end();
+}
+
+std::string script_json(const orc::Script& sc) {
+  std::ostringstream o;
+  Obj top(o);
+  js_map(top, "materials", sc.materials, [&](const orc::Material& m) {
+    Obj x(o);
+    x.key("eps"); js_mat(o, m.eps);
+    x.key("mu"); js_mat(o, m.mu);
+    x.key("sigma"); js_mat(o, m.sigma);
+    x.key("chi"); js_mat(o, m.chi);
+    x.end();
+  });
+  js_map(top, "bcs", sc.bcs, [&](const orc::BoundaryCondition& b) {
+    Obj x(o);
+    x.str("type", b.type); x.str("dir", b.dir); x.num("width", b.width); x.num("val", b.val);
+    x.key("surfs"); js_vec(o, b.surfs);
+    x.end();
+  });
+  js_map(top, "meshes", sc.meshes, [&](const orc::Mesh& m) {
+    Obj x(o);
+    x.str("file", m.file); x.str("name", m.name); x.str("type", m.type); x.str("mesher", m.mesher);
+    x.num("scale", m.scale);
+    x.num("xmin", m.xmin); x.num("xstep", m.xstep); x.num("xmax", m.xmax);
+    x.num("ymin", m.ymin); x.num("ystep", m.ystep); x.num("ymax", m.ymax);
+    x.num("zmin", m.zmin); x.num("zstep", m.zstep); x.num("zmax", m.zmax);
+    x.end();
+  });
+  js_map(top, "sources", sc.sources, [&](const orc::Source& s) {
+    Obj x(o);
+    x.str("st", s.st); x.str("prof", s.prof); x.str("carrier", s.carrier); x.str("dir", s.dir);
+    x.num("amp", s.amp); x.num("freq", s.freq); x.num("radius", s.radius); x.num("decay", s.decay);
+    x.num("width", s.width); x.num("delay", s.delay); x.num("impedance", s.impedance);
+    x.key("kvec"); js_vec(o, s.kvec);
+    x.key("center"); js_vec(o, s.center);
+    x.key("location"); js_vec(o, s.location);
+    x.key("bfuncs"); js_strs(o, s.bfuncs);
+    x.key("surfaces"); js_vec(o, s.surfaces);
+    x.end();
+  });
+  js_map(top, "simulations", sc.simulations, [&](const orc::Simulation& s) {
+    Obj x(o);
+    x.num("duration", s.duration); x.num("courant", s.courant); x.num("step", s.step); x.num("tol", s.tol);
+    x.str("method", s.method); x.str("solver", s.solver); x.str("analytic", s.analytic);
+    x.key("debug") << (s.debug ? "true" : "false");
+    x.key("sources"); js_vec(o, s.sources);
+    x.num("mesh", s.mesh); x.num("output", s.output);
+    x.end();
+  });
+  js_map(top, "outputs", sc.outputs, [&](const orc::Output& p) {
+    Obj x(o);
+    x.str("mode", p.mode); x.str("name", p.name); x.num("period", p.period); x.num("nextprint", p.nextprint);
+    x.num("delay", p.delay); x.num("ref_sys", p.ref_sys);
+    x.num("xstart", p.xstart); x.num("xstep", p.xstep); x.num("xstop", p.xstop);
+    x.num("ystart", p.ystart); x.num("ystep", p.ystep); x.num("ystop", p.ystop);
+    x.num("zstart", p.zstart); x.num("zstep", p.zstep); x.num("zstop", p.zstop);
+    x.key("probes");
+    o << '[';
+    for (size_t q = 0; q < p.probes.size(); q++) {
+      if (q) o << ", ";
+      js_vec(o, p.probes[q]);
+    }
+    o << ']';
+    x.end();
+  });
+  top.key("bnd_to_bc"); js_vec(o, sc.bnd_to_bc);
+  // solids of the cartesian meshes (solids-file reader)
+  {
+    std::ostringstream& os = top.key("solids");
+    Obj meshes(os);
+    for (const auto& kv : sc.meshes) {
+      if (kv.second.type != "cartesian" || kv.second.file == "none") continue;
+      meshes.key(std::to_string(kv.first).c_str());
+      Obj sol(o);
+      for (const auto& s : orc::read_solids(kv.second.file)) {
+        sol.key(std::to_string(s.first).c_str());
+        Obj x(o);
+        x.str("type", s.second.type); x.num("material", s.second.material); x.num("sqr", s.second.sqr);
+        x.key("center"); js_vec(o, s.second.center);
+        x.key("corner"); js_vec(o, s.second.corner);
+        x.key("size"); js_vec(o, s.second.size);
+        x.end();
+      }
+      sol.end();
+    }
+    meshes.end();
+  }
+  top.end();
+  return o.str();
+}
+
+}  // namespace
+
 extern "C" {
+
+// Parses a script with the oracle's front end and writes its canonical JSON
+// into buf (cap bytes); returns the length needed including the terminator,
+// or -1 with the error text in buf.
+long orc_script_dump(const char* script, char* buf, long cap) {
+  std::string out;
+  long rc;
+  try {
+    orc::Script sc;
+    sc.parse(script);
+    out = script_json(sc);
+    rc = (long)out.size() + 1;
+  } catch (const std::exception& e) {
+    out = e.what();
+    rc = -1;
+  }
+  if (buf && cap > 0) {
+    const size_t m = out.size() < (size_t)cap - 1 ? out.size() : (size_t)cap - 1;
+    std::memcpy(buf, out.data(), m);
+    buf[m] = 0;
+  }
+  return rc;
+}
 
 void* orc_fit_open(const char* script, unsigned label, char* err, int errlen) {
   auto* o = new FitOracle();
@@ -73,6 +271,12 @@ int orc_fit_flux(void* h, double* flux) {
   auto* o = static_cast<FitOracle*>(h);
   std::memcpy(flux, o->flux.data(), o->flux.size() * sizeof(double));
   return 0;
+}
+
+int orc_fit_losses(void* h, double* loss) {
+  auto* o = static_cast<FitOracle*>(h);
+  std::memcpy(loss, o->losses.data(), o->losses.size() * sizeof(double));
+  return (int)o->losses.size();
 }
 
 // Material coefficients in the reference numbering: M_h, M_q (edges), M_nu, M_mu (faces).

@@ -299,6 +299,7 @@ void FitOracle::build_mesh() {
       }
       edge_src[i] = keep;
     }
+    Si.push_back((out.mode == "l2norm" && avg_eps[i] != 0) ? avg_sigma[i] / edge_len[i] : 0.0);
     if (avg_eps[i] != 0) {
       if (ele_lossy[i]) {
         M_h.push_back(edge_len[i] / (avg_eps[i] + 0.5 * dt * avg_sigma[i]));
@@ -443,7 +444,7 @@ void FitOracle::prepare(uint32_t label) {
       edge_src[best].push_back(sl);
     }
   }
-  times.clear(); samples.clear(); flux.clear();
+  times.clear(); samples.clear(); flux.clear(); losses.clear();
   step_index = 0;
   nsteps_total = 0;
   while ((double)nsteps_total * dt <= sim.duration) nsteps_total++;
@@ -574,6 +575,13 @@ uint64_t FitOracle::step(uint64_t n) {
     double fl = 0;
     for (uint32_t e = 0; e < nE; e++) fl += (U_old[e] + U[e]) * curl_fb[e];
     flux.push_back(0.5 * fl);
+    // 0.25 (U_old + U)^T (Si .* (U_old + U)), Discretization.hpp:1902
+    double lo = 0;
+    for (uint32_t e = 0; e < nE; e++) {
+      const double w = U_old[e] + U[e];
+      lo += w * (Si[e] * w);
+    }
+    losses.push_back(0.25 * lo);
 #pragma omp parallel for schedule(static)
     for (size_t q = 0; q < tbc.size(); q++) {
       const uint32_t j = tbc[q];

@@ -38,6 +38,10 @@ struct FitOracle {
   std::vector<uint32_t> bc_edges, src_edges, uncommon_edges, common_edges;
   std::vector<std::vector<uint32_t>> edge_src;
   std::vector<double> M_nu, M_mu, M_h, M_q;
+  // Si_vec (Discretization.hpp:5374, :5594-5597): sigma-bar / length of each
+  // edge, filled only when the output mode is l2norm (store_E, :5368); zero
+  // otherwise, so the loss column is zero for every other output mode
+  std::vector<double> Si;
   std::vector<std::array<double, 3>> bnd_dual;
   double dt = 0, dt_estimate = 0;
   bool possibly_unstable = false;
@@ -47,6 +51,7 @@ struct FitOracle {
   std::vector<uint32_t> probe_elem;
   std::vector<std::array<double, 3>> probe_pts;
   std::vector<double> times, samples, flux;  // samples: [time][probe][Ex Ey Ez Hx Hy Hz]
+  std::vector<double> losses;               // Joule loss per step (Discretization.hpp:1902)
   uint64_t step_index = 0, nsteps_total = 0;
 
   void prepare(uint32_t label);

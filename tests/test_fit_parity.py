@@ -120,3 +120,28 @@ def test_every_kernel_variant_is_bitwise_identical(tmp_path, product_lib, oracle
         U, _, F = d.state()
         assert d.info()["cg_variant"] == (variant - 1) * 5
     assert np.array_equal(U, Uo) and np.array_equal(F, Fo)
+
+
+@pytest.mark.parametrize("mode", ["l2norm", "probepoint"])
+def test_joule_losses_match_oracle(tmp_path, product_lib, oracle_lib, mode):
+    """poynting.dat's third column, 0.25 (U_old + U)^T Si (U_old + U)
+    (Discretization.hpp:1902).  The reference fills Si (sigma-bar / length)
+    only for l2norm outputs (:5368, :5594-5597): with lossy spheres the loss
+    is non-zero there and exactly zero for probe outputs."""
+    case = FitCase(n=20, steps=120, spheres=random_spheres(12, seed=7), output_mode=mode)
+    script = write_fit_cavity(str(tmp_path), case)
+    o = oracle.FitOracle(script)
+    o.run()
+    lo = o.losses()
+    for prec, tol in (("fp64", TOL_FP64), ("fp32", TOL_FP32)):
+        with tb.Discretization(script) as d:
+            info = d.prepare(1, precision=prec)
+            d.step(info["n_steps"])
+            lg = d.losses()
+            U, _, _ = d.state()
+        assert lg.shape == lo.shape == (120,)
+        if mode == "probepoint":
+            assert not lg.any() and not lo.any()
+        else:
+            assert lo.max() > 0
+            assert rel(lg, lo) <= tol, prec

@@ -79,6 +79,8 @@ _SIGS = {
     "tf_get_state": (ctypes.c_int, [_P, _P, ctypes.c_size_t, _P, ctypes.c_size_t, _P, ctypes.c_size_t]),
     "tf_set_state": (ctypes.c_int, [_P, _P, ctypes.c_size_t, _P, ctypes.c_size_t]),
     "tf_get_flux": (ctypes.c_int, [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "tf_get_losses": (ctypes.c_int, [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "tf_script_dump": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "tf_energy": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double)]),
     "tf_step_io": (ctypes.c_int, [_P, _P, _P, ctypes.POINTER(ctypes.c_uint64)]),
     "tf_phase_times": (ctypes.c_int, [_P, ctypes.c_uint64, _P, ctypes.POINTER(ctypes.c_uint64)]),
@@ -241,6 +243,15 @@ class Discretization:
         self._check(lib().tf_simulations(self._h, arr, n.value, ctypes.byref(n)))
         return list(arr)[: n.value]
 
+    def script(self) -> dict:
+        """The parsed script (tf_script_dump) as a dict."""
+        import json
+        n = ctypes.c_size_t()
+        self._check(lib().tf_script_dump(self._h, None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        self._check(lib().tf_script_dump(self._h, buf, n.value, ctypes.byref(n)))
+        return json.loads(buf.value.decode())
+
     WARM_STARTS = {"previous": 0, "zero": 1, "extrapolate": 2, "learned": 3}
 
     @staticmethod
@@ -359,6 +370,14 @@ class Discretization:
         self._check(lib().tf_get_flux(self._h, None, 0, ctypes.byref(n)))
         f = np.zeros(n.value)
         self._check(lib().tf_get_flux(self._h, _ptr(f), n.value, ctypes.byref(n)))
+        return f
+
+    def losses(self):
+        """Joule loss of every step taken (the third column of poynting.dat)."""
+        n = ctypes.c_size_t()
+        self._check(lib().tf_get_losses(self._h, None, 0, ctypes.byref(n)))
+        f = np.zeros(n.value)
+        self._check(lib().tf_get_losses(self._h, _ptr(f), n.value, ctypes.byref(n)))
         return f
 
     def energy(self) -> float:

@@ -45,6 +45,7 @@ class FitCase:
     spheres: list = field(default_factory=list)
     probes: bool = True
     output_name: str = "zsections"
+    output_mode: str = "probepoint"  # "l2norm" turns on the reference's FIT Joule-loss column
     source_type: str = "h"
     source_surface: int = 1
     pec_surfaces: tuple = (2, 3, 4, 5, 6)
@@ -97,7 +98,7 @@ def write_fit_cavity(directory: str, case: FitCase, name: str = "cavity") -> str
         lines += [f"   SET delay {float(case.delay)!r}"]
     lines += ["END source 1"]
     if case.probes:
-        lines += ["DEFINE output 1", f"   SET name {case.output_name}", "   SET mode probepoint",
+        lines += ["DEFINE output 1", f"   SET name {case.output_name}", f"   SET mode {case.output_mode}",
                   "   SET xgrid { 0.1, 0.1,0.6}", "   SET ygrid { 0.5, 1, 0.5}", "   SET zgrid { 0, 0.04, 1.05}",
                   "   SET grid on", "   SET period 0", "END output 1"]
     lines += ["DEFINE simulation 1", "   SET method fdtd", "   SET mesh 1", "   SET source 1",

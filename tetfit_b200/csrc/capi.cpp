@@ -1,5 +1,7 @@
 // extern "C" boundary (include/tetfit.h).  Maps C++ exceptions to status
 // codes; nothing throws across the ABI.
+#include <array>
+#include <cstdio>
 #include <cstring>
 #include <fstream>
 #include <iomanip>
@@ -86,13 +88,14 @@ void write_outputs(tf_ctx* c) {
   }
   size_t n = 0;
   f.get_flux(nullptr, 0, &n);
-  std::vector<double> fl(n);
+  std::vector<double> fl(n), lo(n);
   f.get_flux(fl.data(), n, &n);
+  f.get_losses(lo.data(), n, nullptr);
   // poynting.dat: times (k + 1/2) dt for fdtd/dga (:1936-1941, :945-950),
   // (k + 1) dt for gfdtd (:1570-1574)
   std::ofstream pf("poynting.dat");
   const double off = f.method() == 2 ? 1.0 : 0.5;
-  for (size_t k = 0; k < n; k++) pf << double(k + off) * f.dt() << "\t" << fl[k] << "\t" << 0.0 << std::endl;
+  for (size_t k = 0; k < n; k++) pf << double(k + off) * f.dt() << "\t" << fl[k] << "\t" << lo[k] << std::endl;
 }
 
 void banner(tf_ctx* c) {
@@ -111,6 +114,177 @@ void banner(tf_ctx* c) {
     std::cout << "WARNING: the time step size chosen by the user is possibly unstable! (Upper stable limit will "
                  "be used instead...)"
               << std::endl;
+}
+
+}  // namespace
+
+
+// ---------------------------------------------------------------- script dump
+// Canonical JSON of a parsed script: every primitive by ascending label, with
+// doubles printed to 17 significant digits (exact round trip).  The solids of
+// each cartesian mesh are read from its file.
+namespace {
+
+void js_str(std::ostringstream& o, const std::string& s) {
+  o << '"';
+  for (char ch : s) {
+    if (ch == '"' || ch == '\\') o << '\\' << ch;
+    else if ((unsigned char)ch < 0x20) o << "\\u" << std::hex << std::setw(4) << std::setfill('0') << (int)ch
+                                          << std::dec << std::setfill(' ');
+    else o << ch;
+  }
+  o << '"';
+}
+void js_num(std::ostringstream& o, double v) {
+  char b[40];
+  std::snprintf(b, sizeof b, "%.17g", v);
+  o << b;
+}
+template <class V>
+void js_vec(std::ostringstream& o, const V& v) {
+  o << '[';
+  bool first = true;
+  for (const auto& x : v) {
+    if (!first) o << ", ";
+    first = false;
+    js_num(o, (double)x);
+  }
+  o << ']';
+}
+void js_strs(std::ostringstream& o, const std::array<std::string, 3>& v) {
+  o << '[';
+  for (int k = 0; k < 3; k++) {
+    if (k) o << ", ";
+    js_str(o, v[k]);
+  }
+  o << ']';
+}
+void js_mat(std::ostringstream& o, const tf::Mat3& m) {
+  o << '[';
+  for (int r = 0; r < 3; r++) {
+    if (r) o << ", ";
+    o << '[';
+    for (int c = 0; c < 3; c++) {
+      if (c) o << ", ";
+      js_num(o, m.m[r][c]);
+    }
+    o << ']';
+  }
+  o << ']';
+}
+struct Obj {  // comma bookkeeping for one JSON object
+  std::ostringstream& o;
+  bool first = true;
+  explicit Obj(std::ostringstream& os) : o(os) { o << '{'; }
+  std::ostringstream& key(const char* k) {
+    if (!first) o << ", ";
+    first = false;
+    js_str(o, k);
+    o << ": ";
+    return o;
+  }
+  void num(const char* k, double v) { key(k); js_num(o, v); }
+  void str(const char* k, const std::string& v) { key(k); js_str(o, v); }
+  void end() { o << '}'; }
+};
+template <class MapT, class F>
+void js_map(Obj& top, const char* name, const MapT& m, F&& each) {
+  std::ostringstream& o = top.key(name);
+  Obj inner(o);
+  for (const auto& kv : m) {
+    inner.key(std::to_string(kv.first).c_str());
+    each(kv.second);
+  }
+  inner.end();
+}
+
+std::string script_json(const tf::Script& sc) {
+  std::ostringstream o;
+  Obj top(o);
+  js_map(top, "materials", sc.materials, [&](const tf::Material& m) {
+    Obj x(o);
+    x.key("eps"); js_mat(o, m.eps);
+    x.key("mu"); js_mat(o, m.mu);
+    x.key("sigma"); js_mat(o, m.sigma);
+    x.key("chi"); js_mat(o, m.chi);
+    x.end();
+  });
+  js_map(top, "bcs", sc.bcs, [&](const tf::BoundaryCondition& b) {
+    Obj x(o);
+    x.str("type", b.type); x.str("dir", b.dir); x.num("width", b.width); x.num("val", b.val);
+    x.key("surfs"); js_vec(o, b.surfs);
+    x.end();
+  });
+  js_map(top, "meshes", sc.meshes, [&](const tf::Mesh& m) {
+    Obj x(o);
+    x.str("file", m.file); x.str("name", m.name); x.str("type", m.type); x.str("mesher", m.mesher);
+    x.num("scale", m.scale);
+    x.num("xmin", m.xmin); x.num("xstep", m.xstep); x.num("xmax", m.xmax);
+    x.num("ymin", m.ymin); x.num("ystep", m.ystep); x.num("ymax", m.ymax);
+    x.num("zmin", m.zmin); x.num("zstep", m.zstep); x.num("zmax", m.zmax);
+    x.end();
+  });
+  js_map(top, "sources", sc.sources, [&](const tf::Source& s) {
+    Obj x(o);
+    x.str("st", s.st); x.str("prof", s.prof); x.str("carrier", s.carrier); x.str("dir", s.dir);
+    x.num("amp", s.amp); x.num("freq", s.freq); x.num("radius", s.radius); x.num("decay", s.decay);
+    x.num("width", s.width); x.num("delay", s.delay); x.num("impedance", s.impedance);
+    x.key("kvec"); js_vec(o, s.kvec);
+    x.key("center"); js_vec(o, s.center);
+    x.key("location"); js_vec(o, s.location);
+    x.key("bfuncs"); js_strs(o, s.bfuncs);
+    x.key("surfaces"); js_vec(o, s.surfaces);
+    x.end();
+  });
+  js_map(top, "simulations", sc.simulations, [&](const tf::Simulation& s) {
+    Obj x(o);
+    x.num("duration", s.duration); x.num("courant", s.courant); x.num("step", s.step); x.num("tol", s.tol);
+    x.str("method", s.method); x.str("solver", s.solver); x.str("analytic", s.analytic);
+    x.key("debug") << (s.debug ? "true" : "false");
+    x.key("sources"); js_vec(o, s.sources);
+    x.num("mesh", s.mesh); x.num("output", s.output);
+    x.end();
+  });
+  js_map(top, "outputs", sc.outputs, [&](const tf::Output& p) {
+    Obj x(o);
+    x.str("mode", p.mode); x.str("name", p.name); x.num("period", p.period); x.num("nextprint", p.nextprint);
+    x.num("delay", p.delay); x.num("ref_sys", p.ref_sys);
+    x.num("xstart", p.xstart); x.num("xstep", p.xstep); x.num("xstop", p.xstop);
+    x.num("ystart", p.ystart); x.num("ystep", p.ystep); x.num("ystop", p.ystop);
+    x.num("zstart", p.zstart); x.num("zstep", p.zstep); x.num("zstop", p.zstop);
+    x.key("probes");
+    o << '[';
+    for (size_t q = 0; q < p.probes.size(); q++) {
+      if (q) o << ", ";
+      js_vec(o, p.probes[q]);
+    }
+    o << ']';
+    x.end();
+  });
+  top.key("bnd_to_bc"); js_vec(o, sc.bnd_to_bc);
+  // solids of the cartesian meshes (solids-file reader)
+  {
+    std::ostringstream& os = top.key("solids");
+    Obj meshes(os);
+    for (const auto& kv : sc.meshes) {
+      if (kv.second.type != "cartesian" || kv.second.file == "none") continue;
+      meshes.key(std::to_string(kv.first).c_str());
+      Obj sol(o);
+      for (const auto& s : tf::read_solids(kv.second.file)) {
+        sol.key(std::to_string(s.first).c_str());
+        Obj x(o);
+        x.str("type", s.second.type); x.num("material", s.second.material); x.num("sqr", s.second.sqr);
+        x.key("center"); js_vec(o, s.second.center);
+        x.key("corner"); js_vec(o, s.second.corner);
+        x.key("size"); js_vec(o, s.second.size);
+        x.end();
+      }
+      sol.end();
+    }
+    meshes.end();
+  }
+  top.end();
+  return o.str();
 }
 
 }  // namespace
@@ -135,6 +309,21 @@ int tf_open(const char* path, tf_ctx** out) {
   });
   *out = c;  // the context carries the error message even on failure
   return rc;
+}
+
+int tf_script_dump(tf_ctx* c, char* buf, size_t cap, size_t* len) {
+  if (!c) return TF_E_ARG;
+  return guarded(c, [&]() -> int {
+    const std::string js = script_json(c->sc);
+    if (len) *len = js.size() + 1;
+    if (buf && cap) {
+      const size_t m = js.size() < cap - 1 ? js.size() : cap - 1;
+      std::memcpy(buf, js.data(), m);
+      buf[m] = 0;
+      if (m < js.size()) return fail(c, TF_E_ARG, "tf_script_dump: buffer too small");
+    }
+    return TF_OK;
+  });
 }
 
 int tf_simulations(tf_ctx* c, uint32_t* labels, uint32_t cap, uint32_t* n) {
@@ -290,6 +479,15 @@ int tf_get_flux(tf_ctx* c, double* flux, size_t cap, size_t* n) {
   if (!c->fit) return fail(c, TF_E_STATE, "tf_get_flux before tf_prepare");
   return guarded(c, [&]() -> int {
     c->fit->get_flux(flux, cap, n);
+    return TF_OK;
+  });
+}
+
+int tf_get_losses(tf_ctx* c, double* loss, size_t cap, size_t* n) {
+  if (!c) return TF_E_ARG;
+  if (!c->fit) return fail(c, TF_E_STATE, "tf_get_losses before tf_prepare");
+  return guarded(c, [&]() -> int {
+    c->fit->get_losses(loss, cap, n);
     return TF_OK;
   });
 }

@@ -24,8 +24,10 @@ namespace tf {
 
 template <typename T>
 void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const ProbeSet& pr, int* step_counter,
-                     double* flux, cudaStream_t st, cudaEvent_t* ev, int e_variant, int h_variant);
-int fit_kernels_per_step(int n_special, int n_probes);
+                     double* flux, cudaStream_t st, cudaEvent_t* ev, int e_variant, int h_variant,
+                     const FitLoss<T>* loss);
+int fit_kernels_per_step(int n_special, int n_probes, bool losses);
+size_t fit_loss_parts(int Nx, int Ny, int Nz);
 template <typename T>
 size_t fit_launch_energy(const FitGrid<T>& g, double* part, cudaStream_t st);
 
@@ -859,6 +861,21 @@ void FitSim::alloc_device() {
       CU(cudaMemsetAsync(dC_[q], 0, nslot_ * es, stream_));
     }
   dflux_ = (double*)dalloc(nsteps_ * 8);
+  // Joule losses (Discretization.hpp:1902): the reference's Si is non-zero
+  // only for l2norm outputs (:5368, :5594-5597) and conducting materials
+  losses_on_ = false;
+  if (out_.mode == "l2norm")
+    for (double v : S_) losses_on_ = losses_on_ || v != 0.0;
+  if (losses_on_) {
+    for (int a = 0; a < 3; a++) {
+      dUold_[a] = dalloc(nslot_ * es);
+      CU(cudaMemsetAsync(dUold_[a], 0, nslot_ * es, stream_));
+    }
+    nloss_part_ = (int)fit_loss_parts(Nx_, Ny_, Nz_);
+    dloss_part_ = (double*)dalloc((size_t)nloss_part_ * 8);
+    dloss_ = (double*)dalloc(nsteps_ * 8);
+    CU(cudaMemsetAsync(dloss_, 0, nsteps_ * 8, stream_));
+  }
   const size_t ns = special_.size();
   nflux_part_ = (int)((ns + 255) / 256);
   dflux_part_ = (double*)dalloc((nflux_part_ + 1) * 8);
@@ -1105,11 +1122,16 @@ void FitSim::launch_steps(int n, cudaEvent_t* ev) {
   if (opt_.precision == 1) {
     FitGrid<float> g; SpecialEdges<float> s;
     fill_grid(g, s);
-    for (int q = 0; q < n; q++) fit_launch_step<float>(g, s, pr, dstep_, dflux_, stream_, ev, e_var_, h_var_);
+    FitLoss<float> lb{(float*)dUold_[0], (float*)dUold_[1], (float*)dUold_[2], dloss_part_, dloss_, nloss_part_};
+    for (int q = 0; q < n; q++)
+      fit_launch_step<float>(g, s, pr, dstep_, dflux_, stream_, ev, e_var_, h_var_, losses_on_ ? &lb : nullptr);
   } else {
     FitGrid<double> g; SpecialEdges<double> s;
     fill_grid(g, s);
-    for (int q = 0; q < n; q++) fit_launch_step<double>(g, s, pr, dstep_, dflux_, stream_, ev, e_var_, h_var_);
+    FitLoss<double> lb{(double*)dUold_[0], (double*)dUold_[1], (double*)dUold_[2], dloss_part_, dloss_,
+                       nloss_part_};
+    for (int q = 0; q < n; q++)
+      fit_launch_step<double>(g, s, pr, dstep_, dflux_, stream_, ev, e_var_, h_var_, losses_on_ ? &lb : nullptr);
   }
 }
 
@@ -1196,7 +1218,7 @@ uint64_t FitSim::step(uint64_t n) {
 }
 
 int FitSim::kernels_per_step() const {
-  return fit_kernels_per_step((int)special_.size(), (int)probe_cell_.size());
+  return fit_kernels_per_step((int)special_.size(), (int)probe_cell_.size(), losses_on_);
 }
 
 // Per-phase device time over n steps (sources/BC, E, scatter+flux, probes, H),
@@ -1274,6 +1296,15 @@ void FitSim::probe_points(double* xyz, uint64_t* cells, size_t cap) const {
 void FitSim::get_flux(double* flux, size_t cap, size_t* n) const {
   size_t m = step_ < cap ? step_ : cap;
   if (flux && m) CU(cudaMemcpy(flux, dflux_, m * 8, cudaMemcpyDeviceToHost));
+  if (n) *n = step_;
+}
+
+void FitSim::get_losses(double* loss, size_t cap, size_t* n) const {
+  size_t m = step_ < cap ? step_ : cap;
+  if (loss && m) {
+    if (losses_on_) CU(cudaMemcpy(loss, dloss_, m * 8, cudaMemcpyDeviceToHost));
+    else std::fill(loss, loss + m, 0.0);
+  }
   if (n) *n = step_;
 }
 

@@ -59,6 +59,7 @@ class FitSim : public Sim {
   void get_state(double* U, double* B, double* F) override;
   void set_state(const double* U, const double* F) override;
   void get_flux(double* flux, size_t cap, size_t* n) const override;
+  void get_losses(double* loss, size_t cap, size_t* n) const override;
   double energy() override;
   uint64_t phase_times(uint64_t n, double* ms5) override;
   uint64_t step_io(const double* carrier_in, double* probe_out) override;
@@ -125,6 +126,12 @@ class FitSim : public Sim {
   double* dflux_ = nullptr;
   double* dflux_part_ = nullptr;
   int nflux_part_ = 0;
+  // Joule losses (l2norm outputs with conducting materials only)
+  bool losses_on_ = false;
+  void* dUold_[3] = {nullptr, nullptr, nullptr};
+  double* dloss_ = nullptr;
+  double* dloss_part_ = nullptr;
+  int nloss_part_ = 0;
   // special edges (device SoA)
   int64_t* dsp_slot_ = nullptr;
   int8_t *dsp_comp_ = nullptr, *dsp_op_ = nullptr, *dsp_nface_ = nullptr, *dsp_fcomp_ = nullptr, *dsp_fsign_ = nullptr;

@@ -683,14 +683,79 @@ __global__ void __launch_bounds__(256) fit_h_coef(FitGrid<T> g, int* step_counte
   }
 }
 
+// Joule loss partials: one thread per node slot sums Si_e (U_old + U)_e^2 over
+// the x, y and z edges leaving the node, Si_e = (sum of da_a sigma over the
+// edge's cells) / L_a (Discretization.hpp:5294-5330, :5597); FP64 throughout.
+template <typename T>
+__global__ void __launch_bounds__(256) fit_loss_kernel(FitGrid<T> g, FitLoss<T> lb) {
+  __shared__ double red[256];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  double acc = 0.0;
+  if (i <= g.Nx && j <= g.Ny) {
+    const int64_t s = (int64_t)i + g.sx * j + g.sxy * k;
+    const T* Us[3] = {g.Ux, g.Uy, g.Uz};
+    const T* Os[3] = {lb.Ox, lb.Oy, lb.Oz};
+    const bool valid[3] = {i < g.Nx, j < g.Ny, k < g.Nz};
+    for (int a = 0; a < 3; a++) {
+      if (!valid[a]) continue;
+      // the edge's cells: offsets -1/0 on the two axes other than a
+      double sig = 0.0, eps = 0.0;
+      for (int q = 0; q < 4; q++) {
+        int ci = i, cj = j, ck = k;
+        const int d0 = (q & 1) - 1, d1 = ((q >> 1) & 1) - 1;
+        if (a == 0) { cj += d0; ck += d1; }
+        else if (a == 1) { ci += d0; ck += d1; }
+        else { ci += d0; cj += d1; }
+        if (ci >= 0 && ci < g.Nx && cj >= 0 && cj < g.Ny && ck >= 0 && ck < g.Nz) {
+          const int m = g.mat[cell_index(ci, cj, ck, g.Nx, g.Ny)];
+          sig += g.S[3 * m + a];
+          eps += g.P[3 * m + a];
+        }
+      }
+      if (sig != 0.0 && eps != 0.0) {  // Si is set only where avg_eps != 0 (:5579)
+        const double w = (double)Os[a][s] + (double)Us[a][s];
+        acc += w * ((sig / g.len[a]) * w);
+      }
+    }
+  }
+  red[tid] = acc;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (tid < w) red[tid] += red[tid + w];
+    __syncthreads();
+  }
+  if (tid == 0) lb.part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * (uint64_t)blockIdx.z)] = red[0];
+}
+
+// Fixed-order sum of the partials into loss[step] (before the H half step
+// advances the step counter).
+__global__ void __launch_bounds__(256) fit_loss_finish(const double* part, int nparts, double* loss,
+                                                      const int* step_counter) {
+  __shared__ double red[256];
+  double acc = 0.0;
+  for (int b = threadIdx.x; b < nparts; b += blockDim.x) acc += part[b];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) loss[*step_counter] = 0.25 * red[0];
+}
+
 // ---------------------------------------------------------------- launchers
 // Kernel variants for the E and H halves (all compute bit-identical results):
 // 0 one thread per node slot, 1 z-march over 4 planes, 2 z-march over 16,
 // 3 one thread per node slot with per-dof coefficient arrays.
 template <typename T>
 void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const ProbeSet& pr, int* step_counter,
-                     double* flux, cudaStream_t st, cudaEvent_t* ev, int e_variant, int h_variant) {
-  // ev (optional): 6 events recorded around the 5 phases, for per-phase timing
+                     double* flux, cudaStream_t st, cudaEvent_t* ev, int e_variant, int h_variant,
+                     const FitLoss<T>* loss) {
+  // ev (optional): 6 events recorded around the 5 phases, for per-phase timing;
+  // loss (optional): Joule loss of the E half step
   dim3 blk(32, 8, 1);
   dim3 grd((unsigned)((g.Nx + 1 + 31) / 32), (unsigned)((g.Ny + 1 + 7) / 8), (unsigned)(g.Nz + 1));
   auto mgrid = [&](int kc) {
@@ -698,6 +763,12 @@ void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const Probe
   };
   const int nsb = (sp.n + 255) / 256;
   if (ev) cudaEventRecord(ev[0], st);
+  if (loss) {
+    const size_t bytes = (size_t)(g.sxy * (g.Nz + 1)) * sizeof(T);
+    cudaMemcpyAsync(loss->Ox, g.Ux, bytes, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(loss->Oy, g.Uy, bytes, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(loss->Oz, g.Uz, bytes, cudaMemcpyDeviceToDevice, st);
+  }
   if (sp.n > 0) fit_special_pre<T><<<nsb, 256, 0, st>>>(g, sp, step_counter);
   if (ev) cudaEventRecord(ev[1], st);
   if (e_variant == 0) fit_e_kernel<T><<<grd, blk, 0, st>>>(g);
@@ -708,6 +779,10 @@ void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const Probe
   }
   if (ev) cudaEventRecord(ev[2], st);
   fit_special_post<T><<<nsb > 0 ? nsb : 1, 256, 0, st>>>(g, sp, step_counter, flux, nsb);
+  if (loss) {
+    fit_loss_kernel<T><<<grd, blk, 0, st>>>(g, *loss);
+    fit_loss_finish<<<1, 256, 0, st>>>(loss->part, loss->nparts, loss->loss, step_counter);
+  }
   if (ev) cudaEventRecord(ev[3], st);
   if (pr.n > 0) fit_probe_kernel<T><<<(pr.n + 127) / 128, 128, 0, st>>>(g, pr, step_counter);
   if (ev) cudaEventRecord(ev[4], st);
@@ -720,12 +795,19 @@ void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const Probe
   if (ev) cudaEventRecord(ev[5], st);
 }
 
-int fit_kernels_per_step(int n_special, int n_probes) { return 3 + (n_special > 0) + (n_probes > 0); }
+int fit_kernels_per_step(int n_special, int n_probes, bool losses) {
+  return 3 + (n_special > 0) + (n_probes > 0) + (losses ? 2 : 0);
+}
+
+// Number of partial sums fit_loss_kernel writes.
+size_t fit_loss_parts(int Nx, int Ny, int Nz) {
+  return (size_t)((Nx + 1 + 31) / 32) * ((Ny + 1 + 7) / 8) * (Nz + 1);
+}
 
 template void fit_launch_step<double>(const FitGrid<double>&, const SpecialEdges<double>&, const ProbeSet&, int*,
-                                      double*, cudaStream_t, cudaEvent_t*, int, int);
+                                      double*, cudaStream_t, cudaEvent_t*, int, int, const FitLoss<double>*);
 template void fit_launch_step<float>(const FitGrid<float>&, const SpecialEdges<float>&, const ProbeSet&, int*,
-                                     double*, cudaStream_t, cudaEvent_t*, int, int);
+                                     double*, cudaStream_t, cudaEvent_t*, int, int, const FitLoss<float>*);
 
 // Discrete leapfrog energy: 0.5 sum M_e U^2 + 0.5 sum M_mu F_old F_new, with
 // F_new recomputed (not stored) from the current U.  FP64 accumulation, one

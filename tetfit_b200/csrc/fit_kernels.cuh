@@ -74,6 +74,18 @@ struct SpecialEdges {
   double* flux_part;       // [blocks] flux partial sums of this step
 };
 
+// Joule loss of each E half step, 0.25 (U_old + U)^T Si (U_old + U)
+// (Discretization.hpp:1902), with Si = sigma-bar / length per edge.  The
+// reference fills Si only for l2norm outputs (:5368, :5594-5597); the loss
+// kernels run only then, and only when some material conducts.
+template <typename T>
+struct FitLoss {
+  T *Ox, *Oy, *Oz;   // U before the E half step (state-array shape)
+  double* part;      // [nparts] per-block partial sums
+  double* loss;      // [nsteps] loss per step
+  int nparts;
+};
+
 template <typename T>
 cudaError_t fit_build_coefficients(const FitGrid<T>& g, cudaStream_t st);
 

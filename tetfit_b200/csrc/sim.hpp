@@ -58,6 +58,17 @@ class Sim {
   virtual void get_state(double* U, double* B, double* F) = 0;
   virtual void set_state(const double* U, const double* F) = 0;
   virtual void get_flux(double* flux, size_t cap, size_t* n) const = 0;
+  // Joule loss per step (Discretization.hpp:895, :1519, :1902).  Zero unless
+  // the simulation conducts: the tetrahedral paths accept lossless materials
+  // only, and the FIT path's conductance vector is non-zero only for l2norm
+  // outputs, as in the reference.
+  virtual void get_losses(double* loss, size_t cap, size_t* n) const {
+    const uint64_t s = step_index();
+    const size_t m = s < cap ? (size_t)s : cap;
+    if (loss)
+      for (size_t q = 0; q < m; q++) loss[q] = 0.0;
+    if (n) *n = (size_t)s;
+  }
   virtual double energy() = 0;
   virtual uint64_t phase_times(uint64_t n, double* ms5) = 0;
   virtual uint64_t step_io(const double* carrier_in, double* probe_out) = 0;
