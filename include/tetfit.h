@@ -72,7 +72,7 @@ typedef struct tf_info {
   uint64_t n_probes, n_steps;          /* probes inside the mesh; loop length     */
   uint64_t step_index;                 /* steps already taken                     */
   uint32_t nx, ny, nz;                 /* Cartesian cells per axis (0 for tets)   */
-  int32_t method;                      /* 0 fdtd, 1 dga, 2 gfdtd                  */
+  int32_t method;                      /* 0 fdtd, 1 dga, 2 gfdtd, 3 fem           */
   double dt, dt_estimate;              /* step used; courant x stability estimate */
   int32_t possibly_unstable;           /* SET step exceeded the estimate          */
   int32_t precision;
@@ -125,7 +125,12 @@ TF_API int tf_get_flux(tf_ctx* ctx, double* flux, size_t cap, size_t* n);
  * tetrahedral paths accept lossless materials only, so theirs is zero.  FP64
  * accumulation on the GPU. */
 TF_API int tf_get_losses(tf_ctx* ctx, double* losses, size_t cap, size_t* n);
-/* Discrete leapfrog energy 0.5 U.Me U + 0.5 B_prev.Mnu B (FP64 accumulation). */
+/* Discrete leapfrog energy of the current state (U^n, F^{n+1/2}) in FP64
+ * accumulation: fdtd 0.5 U^n.Me.U^n + 0.5 F^{n+1/2}.Mmu.F^{n-1/2} (F^{n-1/2}
+ * recomputed from U^n); gfdtd 0.5 U^n.E.U^n + 0.5 B^{n-1/2}.N.B^{n+1/2} over the
+ * free edges (B^{n+1/2} recomputed).  Both are invariants of the lossless
+ * leapfrog once the sources are off.  dga returns TF_E_UNSUPPORTED (its
+ * electric mass is the inverse of the assembled H). */
 TF_API int tf_energy(tf_ctx* ctx, double* energy);
 /* One step driven from host memory: carrier_in[n_sources] replaces the script
  * waveform's value for this step (NULL keeps it); probe_out[n_probes*6]
@@ -229,6 +234,8 @@ TF_API int tf_batch_get_probe_points(tf_batch* b, uint32_t member, double* xyz, 
 TF_API int tf_batch_get_state(tf_batch* b, uint32_t member, double* U, size_t nU, double* B, size_t nB, double* F,
                               size_t nF);
 TF_API int tf_batch_get_flux(tf_batch* b, uint32_t member, double* flux, size_t cap, size_t* n);
+/* tf_energy of one member (gfdtd: 0.5 U^n.E.U^n + 0.5 B^{n-1/2}.N.B^{n+1/2}, GPU FP64 reduction). */
+TF_API int tf_batch_energy(tf_batch* b, uint32_t member, double* energy);
 TF_API int tf_batch_solver_stats(tf_batch* b, uint32_t member, int32_t* iters, double* resid, size_t cap,
                                  size_t* n);
 TF_API int tf_batch_guess_stats(tf_batch* b, uint32_t member, int8_t* kept, size_t cap, size_t* n);

@@ -676,7 +676,13 @@ void TetOracle::build_gfdtd() {
     }
   }
   E = Csr::build(NE, NE, et);
+  estimate_dt_pencil();
+  split_system(1.0);
+}
+
+void TetOracle::estimate_dt_pencil() {
   // dt (ComputeFEMTimeStep, :6928-7034): generalized problem K x = lambda E x
+  const uint32_t NE = (uint32_t)edges.size();
   const char* skip = std::getenv("TF_ORACLE_SKIP_DT");
   if (skip && skip[0] == '1' && sim.step != 0) {
     dt_estimate = sim.step;
@@ -699,14 +705,21 @@ void TetOracle::build_gfdtd() {
     if (sim.step > dt) possibly_unstable = true;
     else dt = sim.step;
   }
-  // A = E on free rows/cols, RHSmat1 = E on free rows x Dirichlet cols (:8644-8670)
+}
+
+void TetOracle::split_system(double scale) {
+  // SysMat = scale * E; A = SysMat on free rows/cols, RHSmat1 = SysMat on free
+  // rows x Dirichlet cols (gfdtd :8644-8670 with scale 1; fem :8086-8120 with
+  // scale 1 / dt^2, applied as E * (1 / (dt dt)))
+  const uint32_t NE = (uint32_t)edges.size();
   std::vector<Csr::Trip> at, rt;
   for (uint32_t r = 0; r < NE; r++) {
     if (free_index[r] < 0) continue;
     for (uint64_t k = E.ptr[r]; k < E.ptr[r + 1]; k++) {
       uint32_t c = E.col[k];
-      if (free_index[c] < 0) rt.push_back({r, c, E.val[k]});
-      else at.push_back({(uint32_t)free_index[r], (uint32_t)free_index[c], E.val[k]});
+      const double v = scale == 1.0 ? E.val[k] : E.val[k] * scale;
+      if (free_index[c] < 0) rt.push_back({r, c, v});
+      else at.push_back({(uint32_t)free_index[r], (uint32_t)free_index[c], v});
     }
   }
   A = Csr::build((uint32_t)free_edges.size(), (uint32_t)free_edges.size(), at);
@@ -716,6 +729,83 @@ void TetOracle::build_gfdtd() {
     double d = A.diag(i);
     jacobi[i] = d != 0 ? 1.0 / d : 1.0;
   }
+}
+
+void TetOracle::build_fem() {
+  // ConstructFEMaterialMatrices (Discretization.hpp:7687-8130), lossless:
+  // N as for dga/gfdtd; E the Whitney edge mass by the quadrature with weight
+  // 1/40 at the tet's nodes and 9/40 at its face barycentres (:7985-8060)
+  const uint32_t NE = (uint32_t)edges.size();
+  free_index.assign(NE, -1);
+  free_edges.clear();
+  for (uint32_t e = 0; e < NE; e++)
+    if (cls[e] != 4) {
+      free_index[e] = (int64_t)free_edges.size();
+      free_edges.push_back(e);
+    }
+  N = assemble_N();
+  std::vector<Csr::Trip> et;
+  static const int kEdge[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
+  for (uint32_t vv = 0; vv < vols.size(); vv++) {
+    const Mat3& eps = sc.materials.at(vol_mat[vv]).eps;
+    auto el = vol_edges(vv);
+    // barycentric coordinates: [x y z 1] wn = (l0 l1 l2 l3), wn the inverse
+    // of the matrix whose rows are [x_i y_i z_i 1] (:7960-7977), by cofactors
+    double P[4][4], wn[4][4];
+    for (int i = 0; i < 4; i++) {
+      for (int a = 0; a < 3; a++) P[i][a] = pts[vols[vv][i]][a];
+      P[i][3] = 1.0;
+    }
+    auto minor3 = [&](int r, int c) {
+      double m[3][3];
+      for (int i = 0, ii = 0; i < 4; i++) {
+        if (i == r) continue;
+        for (int j = 0, jj = 0; j < 4; j++) {
+          if (j == c) continue;
+          m[ii][jj++] = P[i][j];
+        }
+        ii++;
+      }
+      return m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) - m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
+             m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+    };
+    double det = 0.0;
+    for (int c = 0; c < 4; c++) det += ((c & 1) ? -1.0 : 1.0) * P[0][c] * minor3(0, c);
+    for (int r = 0; r < 4; r++)
+      for (int c = 0; c < 4; c++) wn[c][r] = (((r + c) & 1) ? -1.0 : 1.0) * minor3(r, c) / det;
+    // Whitney edge functions at a point: w_ab = l_a grad l_b - l_b grad l_a
+    auto whitney = [&](const V3& p, V3 w[6]) {
+      double l[4];
+      for (int i = 0; i < 4; i++) l[i] = p[0] * wn[0][i] + p[1] * wn[1][i] + p[2] * wn[2][i] + wn[3][i];
+      for (int k = 0; k < 6; k++) {
+        const int a = kEdge[k][0], b = kEdge[k][1];
+        for (int x = 0; x < 3; x++) w[k][x] = l[a] * wn[x][b] - l[b] * wn[x][a];
+      }
+    };
+    double sumn[6][6] = {}, sumf[6][6] = {};
+    for (int h = 0; h < 4; h++) {
+      V3 w1[6], w2[6];
+      whitney(pts[vols[vv][h]], w1);
+      whitney(face_bar(vtf[vv][h].first), w2);
+      for (int j = 0; j < 6; j++)
+        for (int k = j; k < 6; k++) {
+          sumn[j][k] += dot(w1[k], matvec(eps, w1[j]));
+          sumf[j][k] += dot(w2[k], matvec(eps, w2[j]));
+        }
+    }
+    const double vol = std::fabs(cell_vol[vv]);
+    for (int j = 0; j < 6; j++)
+      for (int k = j; k < 6; k++) {
+        const double val = vol * (sumn[j][k] + sumf[j][k] * 9.0) / 40.0;
+        if (val != 0) {
+          et.push_back({el[j], el[k], val});
+          if (k != j) et.push_back({el[k], el[j], val});
+        }
+      }
+  }
+  E = Csr::build(NE, NE, et);
+  estimate_dt_pencil();
+  split_system(1.0 / (dt * dt));
 }
 
 int TetOracle::cg_solve(const Csr& M, const std::vector<double>& pre, const double* b, double* x, double tol,
@@ -911,13 +1001,15 @@ void TetOracle::prepare(uint32_t label) {
   if (msh.type != "tetrahedral") throw std::runtime_error("tet oracle needs a tetrahedral mesh");
   if (sim.method == "dga") method = 1;
   else if (sim.method == "gfdtd") method = 2;
-  else throw std::runtime_error("tet oracle supports methods dga and gfdtd");
+  else if (sim.method == "fem") method = 3;
+  else throw std::runtime_error("tet oracle supports methods dga, gfdtd and fem");
   out = sc.outputs[sim.output];
   out.initialize();
   root = 0;
   read_mesh();
   if (method == 1) build_dga();
-  else build_gfdtd();
+  else if (method == 2) build_gfdtd();
+  else build_fem();
   const size_t NE = edges.size(), NF = faces.size();
   U.assign(NE, 0); I.assign(NE, 0); F.assign(NF, 0); B.assign(NF, 0);
   Fb.assign(bnd_dual.size(), 0); Fb_old = Fb; SrcFld.assign(NE, 0);
@@ -971,6 +1063,7 @@ void TetOracle::prepare(uint32_t label) {
     }
   }
   U_old = U;
+  U_older = U;
   if (method == 1 && out.mode == "probepoint" && out.allow_print(0.0)) export_probes(0.0);
 }
 
@@ -1057,13 +1150,66 @@ void TetOracle::gfdtd_step(double t, double t_prev) {
   U_old = U;
 }
 
+void TetOracle::fem_step(double t, double t_prev) {
+  // Discretization.hpp:1676-1776: central differences of the second-order
+  // wave equation, E (U^{n+1} - 2 U^n + U^{n-1}) / dt^2 + C^T N C U^n = ...
+  const size_t NE = edges.size(), NF = faces.size();
+  std::vector<double> cu(NF);
+  C.mul(U.data(), cu.data());
+  for (size_t f = 0; f < NF; f++) B[f] -= dt * cu[f];
+  if (out.mode == "probepoint" && out.allow_print(t_prev)) export_probes(t_prev);
+  Fb_old = Fb;
+  for (uint32_t e = 0; e < NE; e++) {
+    if (edge_bcs[e] != 0 && sc.bcs[edge_bcs[e]].type != "none") {
+      U[e] = 0;
+      SrcFld[e] = U[e];
+    } else if (!edge_src[e].empty()) {
+      const std::string& ty = sc.sources[edge_src[e][0]].st;
+      if (ty == "h" && bnd_edges[e] >= 0) Fb[bnd_edges[e]] = hfield_source(e, t - 0.5 * dt);
+      else if (ty != "h") {
+        if (ty == "j") I[e] = current_source(e, t);
+        else U[e] = efield_source(e, t);
+        SrcFld[e] = U[e];
+      }
+    }
+  }
+  // Psi = 2 (E U_old) / dt^2 - C^T N C U_old + (1/dt) Ctb (Fb - Fb_old)
+  //       - (E U_older) / dt^2 - RHSmat1 SrcFld - (1/dt) I   (:1713-1716)
+  std::vector<double> cuo(NF), ncu(NF), cc(NE), eu(NE), euo(NE), rs(NE), psi(NE);
+  C.mul(U_old.data(), cuo.data());
+  N.mul(cuo.data(), ncu.data());
+  C.mul_t(ncu.data(), cc.data());
+  E.mul(U_old.data(), eu.data());
+  E.mul(U_older.data(), euo.data());
+  RHS1.mul(SrcFld.data(), rs.data());
+  const double idt2 = 1.0 / (dt * dt), idt = 1.0 / dt;
+  double fl = 0;
+  for (uint32_t e = 0; e < NE; e++) {
+    const double fb = bnd_edges[e] >= 0 ? Fb[bnd_edges[e]] : 0.0;
+    const double fbo = bnd_edges[e] >= 0 ? Fb_old[bnd_edges[e]] : 0.0;
+    psi[e] = 2.0 * eu[e] * idt2 - cc[e] + idt * (fb - fbo) - euo[e] * idt2 - rs[e] - idt * I[e];
+    fl += U_old[e] * (0.5 * (fb + fbo));
+  }
+  flux.push_back(fl);
+  std::vector<double> rhs(free_edges.size());
+  for (size_t k = 0; k < free_edges.size(); k++) rhs[k] = psi[free_edges[k]];
+  double err = 0;
+  int it = cg_solve(A, jacobi, rhs.data(), solution.data(), sim.tol, cg_maxiter, &err);
+  cg_iters.push_back(it);
+  cg_err.push_back(err);
+  for (size_t k = 0; k < free_edges.size(); k++) U[free_edges[k]] = solution[k];
+  U_older = U_old;
+  U_old = U;
+}
+
 uint64_t TetOracle::step(uint64_t n) {
   uint64_t done = 0;
   for (; done < n && step_index < nsteps_total; done++, step_index++) {
     const uint64_t i = step_index + 1;
     const double t = (double)i * dt;
     if (method == 1) dga_step(t);
-    else gfdtd_step(t, t - dt);
+    else if (method == 2) gfdtd_step(t, t - dt);
+    else fem_step(t, t - dt);
   }
   return done;
 }

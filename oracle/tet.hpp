@@ -34,7 +34,7 @@ struct TetOracle {
   Simulation sim;
   Output out;
   uint32_t sim_label = 0;
-  int method = 1;  // 1 dga, 2 gfdtd
+  int method = 1;  // 1 dga, 2 gfdtd, 3 fem
   // mesh and complex (reference numbering: sorted unique faces/edges)
   std::vector<std::array<double, 3>> pts;
   std::vector<std::array<uint32_t, 4>> vols;
@@ -57,7 +57,7 @@ struct TetOracle {
   // operators
   Csr N;                               // F x F
   Csr H;                               // E x E, rows of class-1 edges (dga)
-  Csr E;                               // E x E eps mass (gfdtd)
+  Csr E;                               // E x E eps mass (gfdtd: node-star dual basis; fem: Whitney)
   Csr A, RHS1;                         // free x free system; E(free rows, Dirichlet cols)
   std::vector<int64_t> free_index;     // edge -> compressed free index or -1
   std::vector<uint32_t> free_edges;
@@ -65,7 +65,7 @@ struct TetOracle {
   double dt = 0, dt_estimate = 0;
   bool possibly_unstable = false;
   // state
-  std::vector<double> U, I, F, B, Fb, Fb_old, U_old, SrcFld, solution;
+  std::vector<double> U, I, F, B, Fb, Fb_old, U_old, U_older, SrcFld, solution;
   uint32_t root = 0;
   std::vector<uint32_t> probe_elem;
   std::vector<std::array<double, 3>> probe_pts;
@@ -87,6 +87,8 @@ struct TetOracle {
   void read_mesh();
   void build_dga();
   void build_gfdtd();
+  void build_fem();
+  void split_system(double scale);
   std::array<uint32_t, 6> vol_edges(uint32_t v) const;
   std::array<std::array<double, 3>, 6> dual_area_vectors(uint32_t v) const;
   std::array<std::array<double, 3>, 4> primal_area_vectors(uint32_t v) const;
@@ -102,6 +104,8 @@ struct TetOracle {
   void export_probes(double t);
   void dga_step(double t);
   void gfdtd_step(double t, double t_prev);
+  void fem_step(double t, double t_prev);
+  void estimate_dt_pencil();
   std::vector<std::array<double, 16>> whitney_;
 };
 

@@ -50,13 +50,46 @@ def test_fit_cavity_energy_drift(tmp_path, product_lib, oracle_lib):
     assert abs(w1 - w0) / w0 <= 1e-12, f"relative drift {abs(w1 - w0) / w0:.3e}"
 
 
+def test_fit_gpu_energy_kernel(tmp_path, product_lib, oracle_lib):
+    """tf_energy (fit_energy_kernel, FP64 block reduction on the GPU) of the
+    state after a step, (U^n, F^{n+1/2}): W^n = 1/2 U^n . Me . U^n +
+    1/2 F^{n+1/2} . Mmu . F^{n-1/2} with F^{n-1/2} recomputed from U^n.  It
+    matches the same sum formed in numpy from the states read back before and
+    after the step, and it is invariant once the source is off.  FP64 and
+    FP32 state (FP64 accumulation in both)."""
+    n = 16
+    dt = FitCase(n=n).dt()
+    w = 8 * dt
+    case = FitCase(n=n, steps=1700, carrier="gaussian", width=w, delay=4 * w, step=dt,
+                   spheres=[])
+    s = write_fit_cavity(str(tmp_path), case)
+    o = oracle.FitOracle(s)
+    mh, _, _, mmu = o.coeffs()
+    me = np.where(mh != 0, 1.0 / np.where(mh != 0, mh, 1), 0.0)
+    off = int(4 * w / dt + 30 * w / dt) + 2
+    for prec, tol_np, tol_drift in (("fp64", 1e-12, 1e-12), ("fp32", 1e-6, 1e-5)):
+        with tb.Discretization(s) as d:
+            d.prepare(1, precision=prec)
+            d.step(off)
+            _, _, Fprev = d.state()
+            d.step(1)
+            U0, _, F0 = d.state()
+            w_gpu = d.energy()
+            w_np = 0.5 * np.dot(U0 * me, U0) + 0.5 * np.dot(F0 * mmu, Fprev)
+            assert w_np > 0
+            assert abs(w_gpu - w_np) / w_np <= tol_np, (prec, w_gpu, w_np)
+            d.step(999)
+            w_end = d.energy()
+        assert abs(w_end - w_gpu) / w_gpu <= tol_drift, f"{prec}: relative drift {abs(w_end - w_gpu) / w_gpu:.3e}"
+
+
 @pytest.mark.parametrize("method", ["dga", "gfdtd"])
 def test_tet_cavity_energy_drift(tmp_path, product_lib, oracle_lib, method):
     import scipy.sparse.linalg as spla
     n = 5
     dt = TetCase(n=n).dt()
     w = 8 * dt
-    case = TetCase(n=n, method=method, steps=1700, carrier="gaussian", width=w, delay=4 * w, step=dt,
+    case = TetCase(n=n, method=method, steps=2800, carrier="gaussian", width=w, delay=4 * w, step=dt,
                    tolerance=1e-14)
     s = write_tet_case(str(tmp_path), case)
     o = oracle.TetOracle(s)
@@ -86,6 +119,18 @@ def test_tet_cavity_energy_drift(tmp_path, product_lib, oracle_lib, method):
         w0 = energy()
         d.step(999)
         w1 = energy()
+        if method == "gfdtd":
+            # the GPU reduction of W^n = 1/2 U^n.E.U^n + 1/2 B^{n-1/2}.N.B^{n+1/2}
+            # (tf_energy): against numpy on the same states, and its drift
+            g0 = d.energy()
+            U0, B0, _ = d.state()
+            d.step(1)
+            _, B1, _ = d.state()
+            w_np = 0.5 * me_dot(U0, U0) + 0.5 * np.dot(B0, N @ B1)
+            assert abs(g0 - w_np) / w_np <= 1e-12, (g0, w_np)
+            d.step(998)
+            g1 = d.energy()
+            assert abs(g1 - g0) / g0 <= 1e-10, f"GPU energy drift {abs(g1 - g0) / g0:.3e}"
     assert w0 > 0
     tol = 1e-12 if method == "dga" else 1e-10
     assert abs(w1 - w0) / w0 <= tol, f"{method}: relative drift {abs(w1 - w0) / w0:.3e}"

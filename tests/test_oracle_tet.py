@@ -124,3 +124,27 @@ def test_gmsh_input_is_the_rounded_netgen_mesh(tmp_path, method):
     for a, b in zip(runs[0], runs[1]):
         assert np.array_equal(a, b)
     assert not np.array_equal(runs[0][1], runs[2][1])
+
+
+@pytest.mark.parametrize("jitter", [0.0, 0.15])
+def test_fem_whitney_mass_constant_field(tmp_path, jitter):
+    """fem's edge mass (Discretization.hpp:7902-8060: Whitney functions
+    l_a grad l_b - l_b grad l_a on the local edge order ab, bc, ac, ad, bd,
+    cd, quadrature 1/40 at the nodes and 9/40 at the face barycentres)
+    reproduces a constant field exactly, so for the edge voltages of a
+    uniform E0, u.E.u = eps |E0|^2 times the box volume (1 m^3)."""
+    n, eps_r = 4, 2.5
+    case = TetCase(n=n, method="fem", steps=3, eps=(eps_r,), jitter=jitter)
+    s = write_tet_case(str(tmp_path), case)
+    o = oracle.TetOracle(s)
+    assert o.method == 3
+    pts = kuhn_mesh(n, jitter, case.seed)[0]
+    e, _, _, _ = o.topology()
+    E = csr_dense(*o.matrix("E"), o.nE)
+    assert np.allclose(E, E.T, rtol=0, atol=1e-14 * np.abs(E).max())
+    for E0 in ([1.0, 0.0, 0.0], [0.3, -1.2, 0.7]):
+        u = (pts[e[:, 1]] - pts[e[:, 0]]) @ np.asarray(E0)
+        want = 8.854187817e-12 * eps_r * float(np.dot(E0, E0))
+        assert u @ E @ u == pytest.approx(want, rel=1e-12)
+    # positive definite
+    assert np.linalg.eigvalsh(E).min() > 0

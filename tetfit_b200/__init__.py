@@ -20,7 +20,7 @@ LIB_PATH = os.path.join(_HERE, "libtetfit_b200.so")
 
 TF_OK, TF_E_SCRIPT, TF_E_ARG, TF_E_CUDA, TF_E_UNSUPPORTED, TF_E_STATE, TF_E_SOLVER = 0, -1, -2, -3, -4, -5, -6
 FP64, FP32 = 0, 1
-METHODS = {0: "fdtd", 1: "dga", 2: "gfdtd"}
+METHODS = {0: "fdtd", 1: "dga", 2: "gfdtd", 3: "fem"}
 
 
 class TetfitError(RuntimeError):
@@ -111,6 +111,7 @@ _SIGS = {
     "tf_batch_get_state": (ctypes.c_int, [_P, ctypes.c_uint32, _P, ctypes.c_size_t, _P, ctypes.c_size_t, _P,
                                           ctypes.c_size_t]),
     "tf_batch_get_flux": (ctypes.c_int, [_P, ctypes.c_uint32, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "tf_batch_energy": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]),
     "tf_batch_solver_stats": (ctypes.c_int, [_P, ctypes.c_uint32, _P, _P, ctypes.c_size_t,
                                              ctypes.POINTER(ctypes.c_size_t)]),
     "tf_batch_last_step_ms": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double)]),
@@ -505,6 +506,11 @@ class Batch:
         p = np.zeros(lib().tf_mlp_param_count(), dtype=np.float32)
         self._check(lib().tf_batch_mlp_params(self._h, m, _ptr(p)))
         return p
+
+    def energy(self, m: int) -> float:
+        e = ctypes.c_double()
+        self._check(lib().tf_batch_energy(self._h, m, ctypes.byref(e)))
+        return e.value
 
     def solver_stats(self, m: int):
         n = ctypes.c_size_t()

@@ -52,12 +52,37 @@ class FitCase:
     carrier: str = "sin"
     width: float | None = None       # gaussian carrier width (s)
     delay: float | None = None       # carrier delay (s)
+    profile: str = "wave"            # spatial profile: wave (mode/wavevector) or gaussian (center, radius)
+    amplitude: float = 1.0
+    center: tuple = (0.0, 0.0, 0.0)
+    radius: float | None = None      # gaussian profile radius (m)
+    decay: float | None = None       # radial decay exponent about the centre
+    direction: str = "x"
 
     def dt(self) -> float:
         if self.step is not None:
             return float(self.step)
         h = 1.0 / self.n
         return 0.95 * self.courant * h / (C0 * math.sqrt(3.0))
+
+
+def source_lines(case) -> list:
+    """The `source 1` block of a generated script (Source.hpp:60-300)."""
+    c = tuple(float(x) for x in case.center)
+    lines = ["DEFINE source 1", f"   SET surface {case.source_surface}", f"   SET type {case.source_type}",
+             f"   SET profile {case.profile}", "   SET mode { sin , cos , cos }",
+             "   SET center {%r, %r, %r}" % c, f"   SET direction {case.direction}",
+             f"   SET amplitude {float(case.amplitude)!r}", f"   SET frequency {case.frequency!r}",
+             f"   SET carrier {case.carrier}", "   SET wavevector { 0.5, 0, 0 }"]
+    if case.width is not None:
+        lines += [f"   SET width {float(case.width)!r}"]
+    if case.delay is not None:
+        lines += [f"   SET delay {float(case.delay)!r}"]
+    if case.radius is not None:
+        lines += [f"   SET radius {float(case.radius)!r}"]
+    if case.decay is not None:
+        lines += [f"   SET decay {float(case.decay)!r}"]
+    return lines + ["END source 1"]
 
 
 def write_fit_cavity(directory: str, case: FitCase, name: str = "cavity") -> str:
@@ -88,15 +113,7 @@ def write_fit_cavity(directory: str, case: FitCase, name: str = "cavity") -> str
     lines += [f"DEFINE material {nmat}", "   SET epsilon 1", "   SET mu 1", "   SET sigma 0",
               f"END material {nmat}"]
     lines += ["DEFINE bc 1"] + [f"   SET surface {s}" for s in case.pec_surfaces] + ["   SET type pec", "END bc 1"]
-    lines += ["DEFINE source 1", f"   SET surface {case.source_surface}", f"   SET type {case.source_type}",
-              "   SET profile wave", "   SET mode { sin , cos , cos }", "   SET center {0, 0, 0}",
-              "   SET direction x", "   SET amplitude 1", f"   SET frequency {case.frequency!r}",
-              f"   SET carrier {case.carrier}", "   SET wavevector { 0.5, 0, 0 }"]
-    if case.width is not None:
-        lines += [f"   SET width {float(case.width)!r}"]
-    if case.delay is not None:
-        lines += [f"   SET delay {float(case.delay)!r}"]
-    lines += ["END source 1"]
+    lines += source_lines(case)
     if case.probes:
         lines += ["DEFINE output 1", f"   SET name {case.output_name}", f"   SET mode {case.output_mode}",
                   "   SET xgrid { 0.1, 0.1,0.6}", "   SET ygrid { 0.5, 1, 0.5}", "   SET zgrid { 0, 0.04, 1.05}",
@@ -207,7 +224,7 @@ def write_gmsh(path: str, pts, tets, mats, tris, labels) -> str:
 @dataclass
 class TetCase:
     n: int = 24
-    method: str = "gfdtd"            # "dga" (explicit) or "gfdtd" (PCG)
+    method: str = "gfdtd"            # "dga" (explicit), "gfdtd" or "fem" (PCG each step)
     steps: int = 200
     courant: float = 0.98
     step: float | None = None        # pinned time step; default from the Kuhn-mesh bound below
@@ -225,6 +242,12 @@ class TetCase:
     mat_field: object = None         # optional callable centroids -> labels
     width: float | None = None       # gaussian carrier width (s)
     delay: float | None = None       # carrier delay (s)
+    profile: str = "wave"            # spatial profile: wave or gaussian
+    amplitude: float = 1.0
+    center: tuple = (0.0, 0.0, 0.0)
+    radius: float | None = None
+    decay: float | None = None
+    direction: str = "x"
     mesh_format: str = "netgen"      # "netgen" or "gmsh"
     coord_fmt: str = "%.17g"         # netgen coordinates ("%g": the 6 digits a gmsh conversion keeps)
 
@@ -232,7 +255,8 @@ class TetCase:
         if self.step is not None:
             return float(self.step)
         # 0.25 h / c0: below the stability limit of the jittered Kuhn meshes
-        return 0.25 * (1.0 / self.n) / C0
+        # for dga and gfdtd; fem (Whitney mass) is stable to about 0.21 h / c0
+        return (0.15 if self.method == "fem" else 0.25) * (1.0 / self.n) / C0
 
 
 def write_tet_case(directory: str, case: TetCase, name: str = "box") -> str:
@@ -257,15 +281,7 @@ def write_tet_case(directory: str, case: TetCase, name: str = "box") -> str:
         lines += [f"DEFINE material {m}", f"   SET epsilon {float(e)!r}", "   SET mu 1", "   SET sigma 0",
                   "   SET chi 0", f"END material {m}"]
     lines += ["DEFINE bc 1"] + [f"   SET surface {s}" for s in case.pec_surfaces] + ["   SET type pec", "END bc 1"]
-    lines += ["DEFINE source 1", f"   SET surface {case.source_surface}", f"   SET type {case.source_type}",
-              "   SET profile wave", "   SET mode { sin , cos , cos }", "   SET center {0, 0, 0}",
-              "   SET direction x", "   SET amplitude 1", f"   SET frequency {case.frequency!r}",
-              f"   SET carrier {case.carrier}", "   SET wavevector { 0.5, 0, 0 }"]
-    if case.width is not None:
-        lines += [f"   SET width {float(case.width)!r}"]
-    if case.delay is not None:
-        lines += [f"   SET delay {float(case.delay)!r}"]
-    lines += ["END source 1"]
+    lines += source_lines(case)
     if case.probes:
         lines += ["DEFINE output 1", "   SET name zsections", "   SET mode probepoint",
                   "   SET xgrid { 0.1, 0.1,0.6}", "   SET ygrid { 0.5, 1, 0.5}", "   SET zgrid { 0, 0.04, 1.05}",

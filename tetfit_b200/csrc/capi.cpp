@@ -94,13 +94,13 @@ void write_outputs(tf_ctx* c) {
   // poynting.dat: times (k + 1/2) dt for fdtd/dga (:1936-1941, :945-950),
   // (k + 1) dt for gfdtd (:1570-1574)
   std::ofstream pf("poynting.dat");
-  const double off = f.method() == 2 ? 1.0 : 0.5;
+  const double off = f.method() >= 2 ? 1.0 : 0.5;
   for (size_t k = 0; k < n; k++) pf << double(k + off) * f.dt() << "\t" << fl[k] << "\t" << lo[k] << std::endl;
 }
 
 void banner(tf_ctx* c) {
   tf::Sim& f = *c->fit;
-  static const char* kNames[3] = {"fdtd", "dga", "gfdtd"};
+  static const char* kNames[4] = {"fdtd", "dga", "gfdtd", "fem"};
   std::cout << std::endl << "Simulation parameters:" << std::endl;
   std::cout << std::setw(20) << "Method: " << std::setw(20) << kNames[f.method()] << std::endl;
   std::cout << std::setw(20) << "Simulation time: " << std::setw(20) << f.simulation().duration << " sec"
@@ -366,10 +366,10 @@ int tf_prepare(tf_ctx* c, uint32_t label, const tf_opts* opts) {
     if (c->opts.file_digits < 0 || c->opts.file_digits > 17) return fail(c, TF_E_ARG, "file_digits must be 0..17");
     if (meth == "fdtd") {
       c->fit.reset(new tf::FitSim(c->sc, label, ro));
-    } else if (meth == "dga" || meth == "gfdtd") {
+    } else if (meth == "dga" || meth == "gfdtd" || meth == "fem") {
       c->fit.reset(new tf::TetSim(c->sc, label, ro));
     } else {
-      return fail(c, TF_E_UNSUPPORTED, "method " + meth + " is outside the time-stepping path (fdtd, dga, gfdtd)");
+      return fail(c, TF_E_UNSUPPORTED, "method " + meth + " is outside the time-stepping path (fdtd, dga, gfdtd, fem)");
     }
     c->label = label;
     if (ro.verbose) banner(c);

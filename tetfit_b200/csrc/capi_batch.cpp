@@ -101,8 +101,9 @@ int tf_batch_open(const char* const* scripts, const uint32_t* labels, uint32_t n
           auto it = sc->simulations.find(labels[i]);
           if (it == sc->simulations.end()) throw std::invalid_argument("unknown simulation label " +
                                                                        std::to_string(labels[i]));
-          if (it->second.method != "gfdtd" || sc->meshes[it->second.mesh].type != "tetrahedral")
-            throw std::invalid_argument("batches run tetrahedral method gfdtd simulations");
+          if ((it->second.method != "gfdtd" && it->second.method != "fem") ||
+              sc->meshes[it->second.mesh].type != "tetrahedral")
+            throw std::invalid_argument("batches run tetrahedral method gfdtd or fem simulations");
           b->sims[i].reset(new tf::TetSim(*sc, labels[i], ro, false));
           b->scripts[i] = std::move(sc);
         } catch (const tf::ScriptError& e) {
@@ -246,6 +247,16 @@ int tf_batch_get_flux(tf_batch* b, uint32_t m, double* flux, size_t cap, size_t*
   return bguarded(b, [&]() -> int {
     const auto [g, k] = b->where[m];
     b->groups[g]->get_flux(k, flux, cap, n);
+    return TF_OK;
+  });
+}
+
+int tf_batch_energy(tf_batch* b, uint32_t m, double* energy) {
+  if (int rc = member_ok(b, m)) return rc;
+  if (!energy) return bfail(b, TF_E_ARG, "tf_batch_energy: null output");
+  return bguarded(b, [&]() -> int {
+    const auto [g, k] = b->where[m];
+    *energy = b->groups[g]->energy(k);
     return TF_OK;
   });
 }

@@ -16,6 +16,13 @@
 
 #include "fit_kernels.cuh"
 
+// z-march loop unrolling (planes whose loads the compiler may overlap)
+#ifndef TF_FIT_UNROLL
+#define TF_FIT_UNROLL 1
+#endif
+#define TF_PRAGMA(x) _Pragma(#x)
+#define TF_UNROLL(n) TF_PRAGMA(unroll n)
+
 namespace tf {
 
 template <typename T>
@@ -215,6 +222,7 @@ __global__ void __launch_bounds__(256) fit_e_march(FitGrid<T> g, int kchunk) {
   }
   T fy_lo = (k0 > 0 && xe) ? __ldg(Fy + s - g.sxy) : (T)0;
   T fx_lo = (k0 > 0 && ye) ? __ldg(Fx + s - g.sxy) : (T)0;
+TF_UNROLL(TF_FIT_UNROLL)
   for (int k = k0; k < k1; k++, s += g.sxy) {
     const bool zin = k > 0 && k < g.Nz;
     uint8_t hi[2][2] = {{0, 0}, {0, 0}};
@@ -380,6 +388,7 @@ __global__ void __launch_bounds__(256) fit_h_march(FitGrid<T> g, int kchunk, int
   const int64_t cc = (int64_t)i + (int64_t)g.Nx * j;
   T ux = (ci) ? __ldg(Ux + s) : (T)0, uy = (cj) ? __ldg(Uy + s) : (T)0;
   uint8_t m_lo = (ci && cj && k0 > 0) ? __ldg(mat + cc + cplane * (k0 - 1)) : 0;
+TF_UNROLL(TF_FIT_UNROLL)
   for (int k = k0; k < k1; k++, s += g.sxy) {
     const bool ck = k < g.Nz;
     const uint8_t m0 = (ci && cj && ck) ? __ldg(mat + cc + cplane * k) : 0;
@@ -809,9 +818,12 @@ template void fit_launch_step<double>(const FitGrid<double>&, const SpecialEdges
 template void fit_launch_step<float>(const FitGrid<float>&, const SpecialEdges<float>&, const ProbeSet&, int*,
                                      double*, cudaStream_t, cudaEvent_t*, int, int, const FitLoss<float>*);
 
-// Discrete leapfrog energy: 0.5 sum M_e U^2 + 0.5 sum M_mu F_old F_new, with
-// F_new recomputed (not stored) from the current U.  FP64 accumulation, one
-// partial per block.
+// Discrete leapfrog energy of the state after a step, (U^n, F^{n+1/2}):
+// W^n = 0.5 sum M_e (U^n)^2 + 0.5 sum M_mu F^{n+1/2} F^{n-1/2}, an invariant of
+// the lossless leapfrog.  F^{n-1/2} is recomputed (not stored): the H update
+// gave M_mu F^{n+1/2} = M_mu F^{n-1/2} - dt curl U^n, so its B is
+// 2 M_mu F^{n+1/2} - B(F^{n+1/2}, U^n).  FP64 accumulation, one partial per
+// block.
 template <typename T>
 __global__ void __launch_bounds__(256) fit_energy_kernel(FitGrid<T> g, double* part) {
   __shared__ double red[256];
@@ -857,8 +869,9 @@ __global__ void __launch_bounds__(256) fit_energy_kernel(FitGrid<T> g, double* p
         double Fold = (double)Fs[s];
         T mmu;
         if (face_B(g, a, i, j, k, B, nu, &mmu)) {
-          double Fnew = (double)nu * (double)B;
-          acc += 0.5 * ((double)mmu * Fold) * Fnew;
+          const double Bprev = 2.0 * (double)mmu * Fold - (double)B;
+          const double Fprev = (double)nu * Bprev;
+          acc += 0.5 * ((double)mmu * Fold) * Fprev;
         }
       }
     }

@@ -304,7 +304,7 @@ TetSim::TetSim(Script& sc, uint32_t label, const RunOptions& opt, bool device)
   sim_ = sc_.simulations.at(label);
   out_ = sc_.outputs[sim_.output];
   out_.initialize();
-  method_ = sim_.method == "dga" ? 1 : 2;
+  method_ = sim_.method == "dga" ? 1 : (sim_.method == "fem" ? 3 : 2);
   src_labels_ = sim_.sources;
   auto t0 = std::chrono::steady_clock::now();
   auto lap = [&](const char* what) {
@@ -341,7 +341,7 @@ TetSim::TetSim(Script& sc, uint32_t label, const RunOptions& opt, bool device)
   }
   build_sources();
   if (!device) return;
-  if (method_ == 2) group_.reset(new TetGroup({this}, opt_, false));
+  if (method_ >= 2) group_.reset(new TetGroup({this}, opt_, false));
   else alloc_and_upload();
 }
 
@@ -795,6 +795,87 @@ void TetSim::build_ops() {
     HostCsr Einv = HostCsr::build(NE, NE, einv_t, nth);
     H_ = HostCsr::build(NE, NE, h_t, nth);
     dt_est_ = sim_.courant * estimate_dt(Einv, false);
+  } else if (method_ == 3) {
+    // fem: Whitney edge mass (Discretization.hpp:7902-8060).  Per tet, the
+    // barycentric coordinates l_1..l_3 = J^-1 (p - x_0), l_0 = 1 - l_1 - l_2 - l_3
+    // (J the edge matrix [x_1-x_0, x_2-x_0, x_3-x_0]), the edge functions
+    // w_ab = l_a grad l_b - l_b grad l_a on the local edges ab, bc, ac, ad,
+    // bd, cd, and the quadrature |V| (sum over the 4 nodes + 9 x sum over
+    // the 4 face barycentres) / 40 of w_k . eps w_j.  Entries j <= k, then
+    // their mirror, zero values skipped, listed in tet order.
+    static const int kWe[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
+    std::vector<double> blk(36 * (size_t)L);
+    parallel_for(L, nth, [&](int64_t v0, int64_t v1) {
+      for (uint32_t v = (uint32_t)v0; v < (uint32_t)v1; v++) {
+        const V3& x0 = pts_[vols_[v][0]];
+        V3 c1 = sub(pts_[vols_[v][1]], x0), c2 = sub(pts_[vols_[v][2]], x0), c3 = sub(pts_[vols_[v][3]], x0);
+        // rows of J^-1 = (c2 x c3, c3 x c1, c1 x c2) / det J: grad l_1..l_3
+        const double det = dot(c1, cross(c2, c3));
+        V3 g[4];
+        g[1] = scale(cross(c2, c3), 1.0 / det);
+        g[2] = scale(cross(c3, c1), 1.0 / det);
+        g[3] = scale(cross(c1, c2), 1.0 / det);
+        for (int a = 0; a < 3; a++) g[0][a] = -(g[1][a] + g[2][a] + g[3][a]);
+        const Mat3& eps = sc_.materials.at(vol_mat_[v]).eps;
+        double acc[2][6][6] = {};
+        auto add_point = [&](const V3& p, int which) {
+          const V3 d = sub(p, x0);
+          double l[4];
+          l[1] = dot(g[1], d);
+          l[2] = dot(g[2], d);
+          l[3] = dot(g[3], d);
+          l[0] = 1.0 - l[1] - l[2] - l[3];
+          V3 w[6], ew[6];
+          for (int k = 0; k < 6; k++) {
+            const int a = kWe[k][0], b = kWe[k][1];
+            w[k] = sub(scale(g[b], l[a]), scale(g[a], l[b]));
+            ew[k] = mv(eps, w[k]);
+          }
+          for (int j = 0; j < 6; j++)
+            for (int k = j; k < 6; k++) acc[which][j][k] += dot(w[k], ew[j]);
+        };
+        for (int h = 0; h < 4; h++) {
+          add_point(pts_[vols_[v][h]], 0);
+          add_point(fbar(vtf_[v][h]), 1);
+        }
+        const double V = std::fabs(cell_vol_[v]);
+        for (int j = 0; j < 6; j++)
+          for (int k = 0; k < 6; k++)
+            blk[36 * (size_t)v + 6 * j + k] =
+                k >= j ? V * (acc[0][j][k] + acc[1][j][k] * 9.0) / 40.0 : 0.0;
+      }
+    });
+    std::vector<int64_t> off(L + 1, 0);
+    parallel_for(L, nth, [&](int64_t v0, int64_t v1) {
+      for (int64_t v = v0; v < v1; v++)
+        for (int j = 0; j < 6; j++)
+          for (int k = j; k < 6; k++)
+            if (blk[36 * v + 6 * j + k] != 0) off[v + 1] += k == j ? 1 : 2;
+    });
+    for (uint32_t v = 0; v < L; v++) off[v + 1] += off[v];
+    HostCsr::Trips t(off[L]);
+    parallel_for(L, nth, [&](int64_t v0, int64_t v1) {
+      for (int64_t v = v0; v < v1; v++) {
+        auto el = vol_edges((uint32_t)v);
+        int64_t w = off[v];
+        for (int j = 0; j < 6; j++)
+          for (int k = j; k < 6; k++) {
+            const double x = blk[36 * v + 6 * j + k];
+            if (x == 0) continue;
+            t[w++] = {(uint32_t)el[j], (uint32_t)el[k], x};
+            if (k != j) t[w++] = {(uint32_t)el[k], (uint32_t)el[j], x};
+          }
+      }
+    });
+    E_ = HostCsr::build(NE, NE, t, nth);
+    dt_est_ = sim_.courant * estimate_dt(E_, true);
+    dt_ = dt_est_;
+    if (sim_.step != 0) {  // Discretization.hpp:8029-8036
+      if (sim_.step > dt_) unstable_ = true;
+      else dt_ = sim_.step;
+    }
+    // SysMat = E * (1 / (dt dt)) (:8086-8093)
+    split_system(1.0 / (dt_ * dt_));
   } else {
     // gfdtd eps-mass from the node dual bases (Discretization.hpp:8357-8621):
     // nine entries per (node, tet) pair at fixed positions, formed in parallel
@@ -831,6 +912,28 @@ void TetSim::build_ops() {
         }
     });
     E_ = HostCsr::build(NE, NE, t, nth);
+    split_system(1.0);
+    auto te = std::chrono::steady_clock::now();
+    dt_est_ = sim_.courant * estimate_dt(E_, true);
+    if (opt_.verbose)
+      std::printf("  set-up %-14s %8.3f s\n", "(dt estimate)",
+                  std::chrono::duration<double>(std::chrono::steady_clock::now() - te).count());
+  }
+  if (method_ != 3) dt_ = dt_est_;
+  if (method_ != 3 && sim_.step != 0) {  // Discretization.hpp:9146-9153, 8634-8641
+    if (sim_.step > dt_) unstable_ = true;
+    else dt_ = sim_.step;
+  }
+}
+
+// A (free x free) and R (free x Dirichlet) split the rows of scale * E: the
+// system of gfdtd (scale 1) and of fem (scale 1 / dt^2).  The free numbering
+// fidx is increasing in the edge index, so each split row keeps E's sorted,
+// merged column order: the rows are copied, not re-sorted.
+void TetSim::split_system(double scale) {
+  const uint32_t NE = (uint32_t)edges_.size();
+  const int nth = opt_.setup_threads;
+  {
     std::vector<int32_t> fidx(NE, -1);
     for (uint32_t e = 0; e < NE; e++) {
       if (cls_[e] != 4) {
@@ -840,9 +943,6 @@ void TetSim::build_ops() {
         dir_edges_.push_back((int32_t)e);
       }
     }
-    // A (free x free) and R (free x Dirichlet) split the rows of E.  The free
-    // numbering fidx is increasing in the edge index, so each split row keeps
-    // E's sorted, merged column order: the rows are copied, not re-sorted.
     const uint32_t nf = (uint32_t)free_edges_.size();
     A_.nrows = A_.ncols = nf;
     R_.nrows = nf;
@@ -869,12 +969,13 @@ void TetSim::build_ops() {
         int64_t wa = A_.ptr[i], wr = R_.ptr[i];
         for (int64_t k = E_.ptr[r]; k < E_.ptr[r + 1]; k++) {
           const int32_t c = E_.col[k];
+          const double v = scale == 1.0 ? E_.val[k] : E_.val[k] * scale;
           if (fidx[c] < 0) {
             R_.col[wr] = c;
-            R_.val[wr++] = E_.val[k];
+            R_.val[wr++] = v;
           } else {
             A_.col[wa] = fidx[c];
-            A_.val[wa++] = E_.val[k];
+            A_.val[wa++] = v;
           }
         }
       }
@@ -886,16 +987,6 @@ void TetSim::build_ops() {
         if (A_.col[k] == (int32_t)i) dg = A_.val[k];
       jacobi_[i] = dg != 0 ? 1.0 / dg : 1.0;  // ConjugateGradientSolver.hpp:119-127
     }
-    auto te = std::chrono::steady_clock::now();
-    dt_est_ = sim_.courant * estimate_dt(E_, true);
-    if (opt_.verbose)
-      std::printf("  set-up %-14s %8.3f s\n", "(dt estimate)",
-                  std::chrono::duration<double>(std::chrono::steady_clock::now() - te).count());
-  }
-  dt_ = dt_est_;
-  if (sim_.step != 0) {  // Discretization.hpp:9146-9153, 8634-8641
-    if (sim_.step > dt_) unstable_ = true;
-    else dt_ = sim_.step;
   }
 }
 
@@ -1362,7 +1453,7 @@ void TetSim::build_sources() {
     }
     const double val0 = post * ((v0[0] * vec[0] + v0[1] * vec[1]) + v0[2] * vec[2]);
     if (kind == 1) { init_U_[e] = val0; init_src_[e] = val0; }
-    else if (kind == 3 && method_ == 2) init_I_[e] = val0;
+    else if (kind == 3 && method_ >= 2) init_I_[e] = val0;
   }
   src_begin_.push_back((int)pair_src_.size());
   src_amp_.resize(nsrc);
@@ -1643,7 +1734,7 @@ void TetSim::get_flux(double* flux, size_t cap, size_t* n) const {
 
 size_t TetSim::solver_stats(int32_t* iters, double* resid, size_t cap) const {
   if (group_) return group_->solver_stats(0, iters, resid, cap);
-  if (method_ != 2) return 0;
+  if (method_ < 2) return 0;
   size_t m = step_ < cap ? step_ : cap;
   if (iters && m) CU(cudaMemcpy(iters, dp_.cg_iters, m * 4, cudaMemcpyDeviceToHost));
   if (resid && m) CU(cudaMemcpy(resid, dp_.cg_resid, m * 8, cudaMemcpyDeviceToHost));
@@ -1661,20 +1752,10 @@ size_t TetSim::training_loss(float* loss, size_t cap) const {
 }
 
 double TetSim::energy() {
-  // 0.5 U.E U + 0.5 B.N B on the host in FP64 (gfdtd mass; dga returns the
-  // magnetic part plus 0.5 U.(Einv^-1 restricted) is not formed: magnetic only)
-  std::vector<double> U(edges_.size()), B(faces_.size()), F(faces_.size()), t;
-  get_state(U.data(), B.data(), F.data());
-  double w = 0;
-  t.resize(faces_.size());
-  N_.mul(B.data(), t.data());
-  for (size_t f = 0; f < B.size(); f++) w += 0.5 * B[f] * t[f];
-  if (method_ == 2) {
-    t.resize(edges_.size());
-    E_.mul(U.data(), t.data());
-    for (size_t e = 0; e < U.size(); e++) w += 0.5 * U[e] * t[e];
-  }
-  return w;
+  // gfdtd: the group engine's GPU reduction; dga's electric energy needs the
+  // inverse of the assembled H, which is not formed
+  if (method_ != 2 || !group_) throw UnsupportedError("tf_energy: dga's electric mass is the inverse of H");
+  return group_->energy(0);
 }
 
 }  // namespace tf

@@ -59,7 +59,7 @@ class TetSim : public Sim {
   const Output& output() const override { return out_; }
   const Simulation& simulation() const override { return sim_; }
   size_t n_samples() const override;
-  double sample_time_shift() const override { return method_ == 2 ? 0.5 * dt_ : -0.5 * dt_; }
+  double sample_time_shift() const override { return method_ >= 2 ? 0.5 * dt_ : -0.5 * dt_; }
   void get_probes(double* times, double* values, size_t cap) const override;
   void probe_points(double* xyz, uint64_t* cells, size_t cap) const override;
   void get_state(double* U, double* B, double* F) override;
@@ -85,6 +85,7 @@ class TetSim : public Sim {
   void read_mesh();
   void classify();
   void build_ops();
+  void split_system(double scale);
   double estimate_dt(const HostCsr& Minv_or_E, bool generalized);
   void locate_probes();
   void build_sources();

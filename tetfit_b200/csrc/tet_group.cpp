@@ -87,7 +87,7 @@ TetGroup::TetGroup(std::vector<TetSim*> sims, const RunOptions& opt, bool releas
   if (sims.size() > (size_t)kMaxGroup)
     throw std::invalid_argument("a group holds at most " + std::to_string(kMaxGroup) + " simulations");
   for (TetSim* t : sims)
-    if (t->method() != 2) throw std::invalid_argument("simulation groups run method gfdtd only");
+    if (t->method() < 2) throw std::invalid_argument("simulation groups run methods gfdtd and fem only");
   CU(cudaSetDevice(opt_.device));
   int major = 0;
   CU(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, opt_.device));
@@ -135,6 +135,7 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
   }
   std::vector<uint16_t> slice_sim, fslice_sim;
   std::vector<double> dt(S), tol(S);
+  std::vector<uint8_t> fem(S, 0);
   std::vector<int> nsteps(S);
   std::vector<int64_t> stat_off(S), samp_off(S), sched_off(S), car_off(S);
   std::vector<int> nsrc(S), src_off(S), sim_se(S + 1), sim_probe(S + 1);
@@ -157,6 +158,8 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
     m.eoff = eoff;
     m.foff = foff;
     m.roff = roff;
+    m.nrow_pad = nfp;
+    m.nface_pad = NFp;
     dofs_ += (uint64_t)(NE + NF);
     nnz_a_real_ += t.A_.val.size();
     m.nnz_a = t.A_.val.size();
@@ -244,6 +247,7 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
     slice_sim.insert(slice_sim.end(), nfp / 32, (uint16_t)s);
     fslice_sim.insert(fslice_sim.end(), NFp / 32, (uint16_t)s);
     dt[s] = t.dt_;
+    fem[s] = t.method_ == 3 ? 1 : 0;
     tol[s] = t.sim_.tol;
     nsteps[s] = (int)t.nsteps_;
     // sources
@@ -331,6 +335,11 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
   d.F = zeros(d.nF);
   d.B = zeros(d.nF);
   d.cb = zeros(d.nE);
+  if (std::find(fem.begin(), fem.end(), 1) != fem.end()) {
+    d.fem = (const uint8_t*)upload(fem);
+    d.cu = zeros(d.nF);
+    d.Uo = upload(U0);  // U_older = U_old = U at t = 0 (Discretization.hpp:1664-1665)
+  }
   d.fte = (const int32_t*)upload(fte);
   auto put = [&](SellHost<T>& m, SellDev& o, bool values) {
     o.ptr = (const int64_t*)upload(m.ptr);
@@ -720,6 +729,24 @@ size_t TetGroup::guess_stats(int s, int8_t* kept, size_t cap) const {
   const size_t n = std::min<size_t>(m.step, cap);
   if (kept && n) CU(cudaMemcpy(kept, dev_.kept + m.stat_off, n, cudaMemcpyDeviceToHost));
   return m.step;
+}
+
+double TetGroup::energy(int s) {
+  constexpr int kBlocks = 592;  // 4 x 148 SMs
+  if (!energy_part_) energy_part_ = (double*)dalloc(kBlocks * sizeof(double));
+  const Meta& m = meta_[s];
+  cudaError_t e = opt_.precision == 1
+                      ? group_launch_energy<float>(dev_, s, m.roff, m.nrow_pad, m.foff, m.nface_pad, energy_part_,
+                                                   kBlocks, stream_)
+                      : group_launch_energy<double>(dev_, s, m.roff, m.nrow_pad, m.foff, m.nface_pad, energy_part_,
+                                                    kBlocks, stream_);
+  CU(e);
+  std::vector<double> h(kBlocks);
+  CU(cudaMemcpyAsync(h.data(), energy_part_, kBlocks * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  CU(cudaStreamSynchronize(stream_));
+  double w = 0.0;
+  for (double x : h) w += x;
+  return w;
 }
 
 size_t TetGroup::training_loss(float* loss, size_t cap) const {

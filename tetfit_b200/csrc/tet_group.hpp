@@ -50,6 +50,8 @@ class TetGroup {
   // current network parameters (kNParam floats); false without warm_start 3
   bool mlp_params(float* out) const;
   void get_flux(int s, double* flux, size_t cap, size_t* n) const;
+  // leapfrog energy of member s on the GPU (see grp_energy)
+  double energy(int s);
   uint64_t device_bytes() const { return dev_bytes_; }
   int kernels_per_step() const { return 7 + (dev_.np ? 1 : 0) + (opt_.warm_start == 3 ? 2 : 0); }
   int cg_blocks() const { return cg_blocks_; }
@@ -64,6 +66,7 @@ class TetGroup {
   struct Meta {
     uint64_t nE = 0, nF = 0, nsteps = 0, step = 0, np = 0, nsrc = 0, nnz_a = 0;
     int64_t eoff = 0, foff = 0, roff = 0, stat_off = 0, samp_off = 0, car_off = 0;
+    int64_t nrow_pad = 0, nface_pad = 0;  // the member's free rows and faces, padded to 32
     int nslots = 0;
     std::vector<int> slot_of_step;
     std::vector<double> sample_times;
@@ -99,6 +102,7 @@ class TetGroup {
   int adam_step_ = 0;
   int64_t samp_n_ = 0, samp_stride_ = 1;
   float* loss_hist_ = nullptr;
+  double* energy_part_ = nullptr;  // partial sums of grp_energy (allocated on first use)
   int64_t loss_cap_ = 0;  // per-simulation carrier tables (for step_io overrides)
 };
 

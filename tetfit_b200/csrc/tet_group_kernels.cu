@@ -92,6 +92,77 @@ __device__ __forceinline__ T sell_dot(const SellDev& m, int64_t row, G g) {
   return s;
 }
 
+#ifndef TF_CG_PIPE
+#define TF_CG_PIPE 0
+#endif
+// The CG kernel's sweep over A.  TF_CG_PIPE 0: sell_dot.  1: software
+// pipelined -- the index and value loads of chunk k + 1 are issued before the
+// gathers of chunk k, so the matrix stream stays in flight while the gathers
+// wait.  2: the whole row's index and value loads first (rows of up to 16
+// entries), then its gathers.  Same entry order and arithmetic in all forms.
+template <typename T, typename G>
+__device__ __forceinline__ T sell_dot_cg(const SellDev& m, int64_t row, G g) {
+#if TF_CG_PIPE == 0
+  return sell_dot<T>(m, row, g);
+#elif TF_CG_PIPE == 1
+  constexpr int CH = 4;
+  const int64_t sl = row >> 5;
+  const int64_t b = m.ptr[sl];
+  const int len = (int)((m.ptr[sl + 1] - b) >> 5);
+  const int32_t* col = m.col + b + (row & 31);
+  const T* val = (const T*)m.val + b + (row & 31);
+  T s = 0;
+  int32_t c[CH];
+  T v[CH];
+#pragma unroll
+  for (int k = 0; k < CH; k++)
+    if (k < len) {
+      c[k] = ld_stream(col + 32 * k);
+      v[k] = ld_stream(val + 32 * k);
+    }
+  for (int j0 = 0; j0 < len; j0 += CH) {
+    int32_t cn[CH];
+    T vn[CH];
+#pragma unroll
+    for (int k = 0; k < CH; k++)
+      if (j0 + CH + k < len) {
+        cn[k] = ld_stream(col + 32 * (j0 + CH + k));
+        vn[k] = ld_stream(val + 32 * (j0 + CH + k));
+      }
+#pragma unroll
+    for (int k = 0; k < CH; k++)
+      if (j0 + k < len) s += v[k] * g(c[k]);
+#pragma unroll
+    for (int k = 0; k < CH; k++) {
+      c[k] = cn[k];
+      v[k] = vn[k];
+    }
+  }
+  return s;
+#else
+  constexpr int LM = 16;
+  const int64_t sl = row >> 5;
+  const int64_t b = m.ptr[sl];
+  const int len = (int)((m.ptr[sl + 1] - b) >> 5);
+  if (len > LM) return sell_dot<T>(m, row, g);
+  const int32_t* col = m.col + b + (row & 31);
+  const T* val = (const T*)m.val + b + (row & 31);
+  int32_t c[LM];
+  T v[LM];
+#pragma unroll
+  for (int k = 0; k < LM; k++)
+    if (k < len) {
+      c[k] = ld_stream(col + 32 * k);
+      v[k] = ld_stream(val + 32 * k);
+    }
+  T s = 0;
+#pragma unroll
+  for (int k = 0; k < LM; k++)
+    if (k < len) s += v[k] * g(c[k]);
+  return s;
+#endif
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   return v;
@@ -126,14 +197,17 @@ __global__ void __launch_bounds__(kGB) grp_curl_u(GroupDev d) {
   const T c = U[e0] - U[e[1]] + U[e[2]];
   T* B = (T*)d.B;
   B[f] = B[f] - (T)d.dt[s] * c;
+  if (d.fem && d.fem[s]) ((T*)d.cu)[f] = c;  // fem: C U_old for C^T N C U_old
 }
 
 template <typename T>
 __global__ void __launch_bounds__(kGB) grp_nmul(GroupDev d) {
   const int64_t f = (int64_t)blockIdx.x * kGB + threadIdx.x;
   if (f >= d.nF) return;
-  if (!running(d, d.fslice_sim[f >> 5])) return;
-  const T* B = (const T*)d.B;
+  const int s = d.fslice_sim[f >> 5];
+  if (!running(d, s)) return;
+  // gfdtd: F = N B; fem: F = N C U_old (Discretization.hpp:1709-1711)
+  const T* B = (const T*)(d.fem && d.fem[s] ? d.cu : d.B);
   ((T*)d.F)[f] = sell_dot<T>(d.N, f, [&](int32_t c) { return B[c]; });
 }
 
@@ -199,8 +273,9 @@ __global__ void __launch_bounds__(kGB) grp_sources(GroupDev d) {
     if (kind == 1) {
       ((T*)d.src)[e] = (T)val;
     } else if (kind == 2) {
-      ((T*)d.cb)[e] = (T)val;
       const double prev = step > 0 ? value(step - 1) : 0.0;
+      // gfdtd: Ctb Fb; fem: Ctb (Fb - Fb_old) (Discretization.hpp:1713)
+      ((T*)d.cb)[e] = (T)(d.fem && d.fem[s] ? val - prev : val);
       fl += (double)((const T*)d.U)[e] * (0.5 * (val + prev));
     } else if (kind == 3) {
       ((T*)d.I)[e] = (T)val;
@@ -224,7 +299,12 @@ __global__ void __launch_bounds__(kGB) grp_rhs(GroupDev d) {
   const T* U = (const T*)d.U;
   const T* S = (const T*)d.src;
   const T* F = (const T*)d.F;
-  const T eu = sell_dot<T>(d.Ef, i, [&](int32_t c) { return U[c] - S[c]; });
+  const bool fem = d.fem && d.fem[s];
+  const T* Uo = (const T*)d.Uo;
+  // gfdtd: E U_old - RHSmat1 SrcFld; fem: E (2 U_old - U_older) - E_dir SrcFld
+  // (the source values live on the Dirichlet columns only)
+  const T eu = fem ? sell_dot<T>(d.Ef, i, [&](int32_t c) { return (T)2 * U[c] - Uo[c] - S[c]; })
+                   : sell_dot<T>(d.Ef, i, [&](int32_t c) { return U[c] - S[c]; });
   // C^T F over the edge's faces in stored order; the face indices of 4
   // entries are loaded before their gathers (padding entries hold kPadCol
   // and add nothing)
@@ -248,7 +328,14 @@ __global__ void __launch_bounds__(kGB) grp_rhs(GroupDev d) {
     }
   }
   const T dt = (T)d.dt[s];
-  ((T*)d.rhs)[i] = eu - dt * ((const T*)d.I)[e] + dt * cf + dt * ((const T*)d.cb)[e];
+  if (fem) {
+    // Psi = (2 E U_old - E U_older - E_dir SrcFld) / dt^2 - C^T N C U_old
+    //       + (Fb - Fb_old) / dt - I / dt   (Discretization.hpp:1713-1716)
+    const double idt = 1.0 / d.dt[s];
+    ((T*)d.rhs)[i] = eu * (T)(idt * idt) - cf + (T)idt * ((const T*)d.cb)[e] - (T)idt * ((const T*)d.I)[e];
+  } else {
+    ((T*)d.rhs)[i] = eu - dt * ((const T*)d.I)[e] + dt * cf + dt * ((const T*)d.cb)[e];
+  }
   T* x = (T*)d.x;
   if (d.warm_start == 1) {
     x[i] = 0;
@@ -415,8 +502,14 @@ __device__ __forceinline__ T p_next(T z, T pold, T beta, bool first) {
 // Co-resident CG blocks per SM the register budget is set for: more warps
 // in flight hide the SELL sweep's load latency better than longer load
 // chunks (measured: FP32 four blocks of 512, FP64 three, where four spill).
+#ifndef TF_CG_MINB32
+#define TF_CG_MINB32 4
+#endif
+#ifndef TF_CG_MINB64
+#define TF_CG_MINB64 3
+#endif
 template <typename T>
-constexpr int cg_min_blocks() { return sizeof(T) == 4 ? 4 : 3; }
+constexpr int cg_min_blocks() { return sizeof(T) == 4 ? TF_CG_MINB32 : TF_CG_MINB64; }
 
 template <typename T, bool kFused>
 __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDev d) {
@@ -505,7 +598,7 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
     if (running(d, s))
       for (int64_t sl = d.seg_s0[g] + warp; sl < d.seg_s1[g]; sl += kCgWarps) {
         const int64_t i = sl * 32 + lane;
-        const T ri = b[i] - sell_dot<T>(d.A, i, [&](int32_t c) { return x[c]; });
+        const T ri = b[i] - sell_dot_cg<T>(d.A, i, [&](int32_t c) { return x[c]; });
         r[i] = ri;
         const T zi = mulT(pre[i], ri);
         z[i] = zi;
@@ -565,7 +658,7 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
           if (!first) xs[i] = fmaT(alpha, po, xs[i]);
           pn[i] = pi;
           if (kFused) {
-            const T qi = sell_dot<T>(d.A, i, [&](int32_t cc) {
+            const T qi = sell_dot_cg<T>(d.A, i, [&](int32_t cc) {
               return p_next<T>(zs[cc], first ? (T)0 : pold[cc], beta, first);
             });
             q[i] = qi;
@@ -585,7 +678,7 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
           const T* pn = pbuf(c.it);
           for (int64_t sl = d.seg_s0[g] + warp; sl < d.seg_s1[g]; sl += kCgWarps) {
             const int64_t i = sl * 32 + lane;
-            const T qi = sell_dot<T>(d.A, i, [&](int32_t cc) { return pn[cc]; });
+            const T qi = sell_dot_cg<T>(d.A, i, [&](int32_t cc) { return pn[cc]; });
             q[i] = qi;
             a0 += (double)pn[i] * (double)qi;
           }
@@ -663,16 +756,80 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
     }
 }
 
+// Leapfrog energy of member s in the state after a step, (U^n, B^{n-1/2}):
+// W^n = 0.5 U^n.E.U^n + 0.5 B^{n-1/2}.N.B^{n+1/2}, with B^{n+1/2} =
+// B^{n-1/2} - dt C U^n recomputed per gathered face (what the next step's
+// grp_curl_u forms).  The electric sum runs over the member's free rows (E's
+// rows of the free edges; the Dirichlet edges hold 0 once the sources are
+// off).  FP64 products and sums; one partial per block, in a fixed order.
+template <typename T>
+__global__ void __launch_bounds__(kGB) grp_energy(GroupDev d, int s, int64_t r0, int64_t nr, int64_t f0,
+                                                  int64_t nf, double* part) {
+  __shared__ double sh[33];
+  const T* U = (const T*)d.U;
+  const T* B = (const T*)d.B;
+  const double dt = d.dt[s];
+  auto row_dot = [&](const SellDev& m, int64_t row, auto&& g) {
+    const int64_t sl = row >> 5;
+    const int64_t b = m.ptr[sl];
+    const int len = (int)((m.ptr[sl + 1] - b) >> 5);
+    double acc = 0.0;
+    for (int j = 0; j < len; j++) {
+      const int64_t q = b + 32 * j + (row & 31);
+      acc += (double)((const T*)m.val)[q] * g(m.col[q]);
+    }
+    return acc;
+  };
+  double acc = 0.0;
+  for (int64_t k = (int64_t)blockIdx.x * kGB + threadIdx.x; k < nr + nf; k += (int64_t)gridDim.x * kGB) {
+    if (k < nr) {
+      const int64_t i = r0 + k;
+      const int32_t e = d.free_edge[i];
+      if (e < 0) continue;
+      const double eu = row_dot(d.Ef, i, [&](int32_t c) { return (double)U[c]; });
+      acc += 0.5 * (double)U[e] * eu;
+    } else {
+      const int64_t f = f0 + (k - nr);
+      if (d.fte[3 * f] < 0) continue;
+      const double nb = row_dot(d.N, f, [&](int32_t c) {
+        const int32_t* e = d.fte + 3 * (int64_t)c;
+        if (e[0] < 0) return 0.0;
+        const double cu = ((double)U[e[0]] - (double)U[e[1]]) + (double)U[e[2]];
+        return (double)B[c] - dt * cu;
+      });
+      acc += 0.5 * (double)B[f] * nb;
+    }
+  }
+  acc = grp_block_sum(acc, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+template <typename T>
+cudaError_t group_launch_energy(const GroupDev& d, int s, int64_t r0, int64_t nr, int64_t f0, int64_t nf,
+                                double* part, int blocks, cudaStream_t st) {
+  grp_energy<T><<<blocks, kGB, 0, st>>>(d, s, r0, nr, f0, nf, part);
+  return cudaGetLastError();
+}
+template cudaError_t group_launch_energy<float>(const GroupDev&, int, int64_t, int64_t, int64_t, int64_t, double*,
+                                                int, cudaStream_t);
+template cudaError_t group_launch_energy<double>(const GroupDev&, int, int64_t, int64_t, int64_t, int64_t, double*,
+                                                 int, cudaStream_t);
+
 template <typename T>
 __global__ void __launch_bounds__(kGB) grp_scatter(GroupDev d) {
   const int64_t k = (int64_t)blockIdx.x * kGB + threadIdx.x;
   T* U = (T*)d.U;
+  T* Uo = (T*)d.Uo;  // fem groups: U_older = U_old before U takes the new values
   if (k < d.nrow) {
     const int32_t e = d.free_edge[k];
-    if (e >= 0) U[e] = ((const T*)d.x)[k];
+    if (e >= 0) {
+      if (Uo) Uo[e] = U[e];
+      U[e] = ((const T*)d.x)[k];
+    }
   }
   if (k < d.ndir) {
     const int32_t e = d.dir_edge[k];
+    if (Uo) Uo[e] = U[e];
     U[e] = ((const T*)d.src)[e];
   }
 }

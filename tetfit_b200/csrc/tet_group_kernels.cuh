@@ -52,6 +52,10 @@ struct GroupDev {
   const uint16_t* slice_sim = nullptr;
   // state (T)
   void *U = nullptr, *F = nullptr, *B = nullptr, *I = nullptr, *cb = nullptr, *src = nullptr;
+  // method fem (central differences of the second-order equation): per
+  // simulation flag, C U_old on the faces and U one step further back
+  const uint8_t* fem = nullptr;
+  void *cu = nullptr, *Uo = nullptr;
   // complex and operators
   const int32_t* fte = nullptr;  // [nF][3] global edges (signs +, -, +), -1 on padding faces
   SellDev N;                     // faces x faces
@@ -122,5 +126,10 @@ template <typename T>
 int group_cg_blocks(int device, int S, size_t* smem);
 template <typename T>
 cudaError_t group_launch_targets(const GroupDev& d, cudaStream_t st);
+// Energy partials of member s (free rows [r0, r0 + nr), faces [f0, f0 + nf))
+// into part[0 .. blocks).
+template <typename T>
+cudaError_t group_launch_energy(const GroupDev& d, int s, int64_t r0, int64_t nr, int64_t f0, int64_t nf,
+                                double* part, int blocks, cudaStream_t st);
 
 }  // namespace tf
