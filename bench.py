@@ -61,6 +61,9 @@ WORKLOADS = {
     # the same scene at profiling size: 16 members n ~ U{8..32} (1.5 M CG rows, state > L2)
     "batch16": dict(kind="batch", members=16, n_lo=8, n_hi=32, steps=1000, seed=31337, prec="fp32",
                     warm="learned", learn_steps=40, crit="rhs", plain_steps=5),
+    # DRAM-traffic capture size: 32 members n ~ U{8..48} (A about 0.7 GB, far above L2; about 2 GB held)
+    "batch32": dict(kind="batch", members=32, n_lo=8, n_hi=48, steps=1000, seed=31337, prec="fp32",
+                    warm="learned", learn_steps=40, crit="rhs", plain_steps=5),
     # learned warm start on one 96^3 Kuhn box (5.3 M tets), GRF eps_r
     "learned96": dict(kind="batch", members=1, n_lo=96, n_hi=96, steps=5000, seed=4242, prec="fp32",
                       warm="learned", learn_steps=500, crit="rhs", plain_steps=5, grf=True),
@@ -497,10 +500,17 @@ def run_batch(args, rank, world, local_rank):
         arms[name] = {"ms_per_step": ms, "cg_iterations_mean": it, "setup_s": round(su, 1), **{
             k: v for k, v in kw.items() if k in ("precision", "warm_start", "batch_mode")}}
 
-    run_arm("batched_fp64_previous", precision="fp64", warm_start="previous")
-    run_arm("batched_fp32_previous", precision="fp32", warm_start="previous")
-    run_arm("batched_fp32_extrapolate", precision="fp32", warm_start="extrapolate")
-    run_arm("plain_fp64", precision="fp64", warm_start="previous", batch_mode="serial")
+    if args.no_arms:
+        # profiling runs: the headline arm only (the other arms' lines read null)
+        arms = {k: {"ms_per_step": float("nan"), "cg_iterations_mean": float("nan")}
+                for k in ("batched_fp64_previous", "batched_fp32_previous", "batched_fp32_extrapolate",
+                          "plain_fp64")}
+        fp64_probes = fp32_probes
+    else:
+        run_arm("batched_fp64_previous", precision="fp64", warm_start="previous")
+        run_arm("batched_fp32_previous", precision="fp32", warm_start="previous")
+        run_arm("batched_fp32_extrapolate", precision="fp32", warm_start="extrapolate")
+        run_arm("plain_fp64", precision="fp64", warm_start="previous", batch_mode="serial")
     arm_names = list(arms)
     arm_ms = max_over_ranks([arms[k]["ms_per_step"] for k in arm_names], dist, f"cuda:{local_rank}")
     for k, v in zip(arm_names, arm_ms):
@@ -526,7 +536,7 @@ def run_batch(args, rank, world, local_rank):
             k = min(len(t32), len(t64))
             perr[m] = _rel(v32[:k], v64[:k])
         import oracle
-        for m in sorted(range(len(cases)), key=lambda q: (cases[q].n, q))[:2]:
+        for m in ([] if args.no_arms else sorted(range(len(cases)), key=lambda q: (cases[q].n, q))[:2]):
             if m not in fp32_probes:
                 continue
             t32, v32 = fp32_probes[m]
@@ -820,6 +830,8 @@ def main():
     ap.add_argument("--workload", default="batch128", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-arms", action="store_true",
+                    help="batch workloads: skip the speed-up decomposition arms and the probe checks (profiling)")
     ap.add_argument("--compare-warm", action="store_true",
                     help="batch workloads: also run the zero, previous and extrapolation warm starts and report "
                          "their CG iterations per step over the timed window")

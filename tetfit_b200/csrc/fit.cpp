@@ -25,7 +25,9 @@ namespace tf {
 template <typename T>
 void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const ProbeSet& pr, int* step_counter,
                      double* flux, cudaStream_t st, cudaEvent_t* ev, int e_variant, int h_variant,
-                     const FitLoss<T>* loss);
+                     const FitLoss<T>* loss, const FitTmaMaps* tma);
+bool fit_make_tma_maps(void* const U[3], void* const F[3], int es, int Nx, int Ny, int Nz, int64_t sx,
+                       FitTmaMaps* out);
 int fit_kernels_per_step(int n_special, int n_probes, bool losses);
 size_t fit_loss_parts(int Nx, int Ny, int Nz);
 template <typename T>
@@ -896,6 +898,11 @@ void FitSim::alloc_device() {
   dinvmu_ = (double*)dalloc(3 * np * 8);
   dslot_ = (int*)dalloc(nsteps_ * 4);
   dsamples_ = (double*)dalloc((size_t)nslots_ * np * 6 * 8);
+  // tensor maps of the TMA z-march (variant 4) and its wait-timeout flag
+  dtma_err_ = (int*)dalloc(sizeof(int));
+  CU(cudaMemsetAsync(dtma_err_, 0, sizeof(int), stream_));
+  tma_.err = dtma_err_;
+  tma_ok_ = fit_make_tma_maps(dU_, dF_, (int)es, Nx_, Ny_, Nz_, sx_, &tma_);
   // pinned staging for tf_step_io, allocated here so the stepping path
   // allocates nothing
   CU(cudaHostAlloc((void**)&pinned_, (src_labels_.size() + 6 * np + 1) * sizeof(double), cudaHostAllocDefault));
@@ -1124,14 +1131,16 @@ void FitSim::launch_steps(int n, cudaEvent_t* ev) {
     fill_grid(g, s);
     FitLoss<float> lb{(float*)dUold_[0], (float*)dUold_[1], (float*)dUold_[2], dloss_part_, dloss_, nloss_part_};
     for (int q = 0; q < n; q++)
-      fit_launch_step<float>(g, s, pr, dstep_, dflux_, stream_, ev, e_var_, h_var_, losses_on_ ? &lb : nullptr);
+      fit_launch_step<float>(g, s, pr, dstep_, dflux_, stream_, ev, e_var_, h_var_, losses_on_ ? &lb : nullptr,
+                             tma_ok_ ? &tma_ : nullptr);
   } else {
     FitGrid<double> g; SpecialEdges<double> s;
     fill_grid(g, s);
     FitLoss<double> lb{(double*)dUold_[0], (double*)dUold_[1], (double*)dUold_[2], dloss_part_, dloss_,
                        nloss_part_};
     for (int q = 0; q < n; q++)
-      fit_launch_step<double>(g, s, pr, dstep_, dflux_, stream_, ev, e_var_, h_var_, losses_on_ ? &lb : nullptr);
+      fit_launch_step<double>(g, s, pr, dstep_, dflux_, stream_, ev, e_var_, h_var_, losses_on_ ? &lb : nullptr,
+                              tma_ok_ ? &tma_ : nullptr);
   }
 }
 
@@ -1145,11 +1154,16 @@ void FitSim::autotune(uint64_t& n) {
     return;
   }
   if (tuned_ || n_cells() < 2000000) { tuned_ = true; return; }
-  const int kVariants = dC_[0] ? 4 : 3, kReps = 2;
+  // candidates: node slot, 4- and 16-plane z-march, per-dof coefficients
+  // (when allocated), TMA z-march (when the tensor maps exist)
+  int cand[5], kVariants = 0;
+  for (int v = 0; v < 5; v++)
+    if ((v != 3 || dC_[0]) && (v != 4 || tma_ok_)) cand[kVariants++] = v;
+  const int kReps = 2;
   cudaEvent_t ev[6];
   for (auto& e : ev) CU(cudaEventCreate(&e));
   while (tune_pos_ < kVariants * kReps && n > 0) {
-    const int v = tune_pos_ / kReps;
+    const int v = cand[tune_pos_ / kReps];
     e_var_ = h_var_ = v;
     launch_steps(1, ev);
     CU(cudaEventSynchronize(ev[5]));
@@ -1164,8 +1178,9 @@ void FitSim::autotune(uint64_t& n) {
   }
   for (auto& e : ev) cudaEventDestroy(e);
   if (tune_pos_ < kVariants * kReps) return;  // continue on the next call
-  int be = 0, bh = 0;
-  for (int v = 1; v < kVariants; v++) {
+  int be = cand[0], bh = cand[0];
+  for (int c = 1; c < kVariants; c++) {
+    const int v = cand[c];
     if (tune_e_[v] < tune_e_[be]) be = v;
     if (tune_h_[v] < tune_h_[bh]) bh = v;
   }
@@ -1214,7 +1229,18 @@ uint64_t FitSim::step(uint64_t n) {
   CU(cudaEventElapsedTime(&ms, ev0_, ev1_));
   last_ms_ = ms;
   step_ += n;
+  check_tma();
   return n;
+}
+
+// A TMA march whose mbarrier wait gave up leaves the step's results invalid.
+void FitSim::check_tma() {
+  if (!tma_ok_) return;
+  int e = 0;
+  CU(cudaMemcpy(&e, dtma_err_, sizeof(int), cudaMemcpyDeviceToHost));
+  if (!e) return;
+  CU(cudaMemset(dtma_err_, 0, sizeof(int)));
+  throw CudaError("FIT TMA march: a shared-memory stage never arrived; the step's results are not valid");
 }
 
 int FitSim::kernels_per_step() const {

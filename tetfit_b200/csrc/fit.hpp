@@ -80,6 +80,7 @@ class FitSim : public Sim {
   void build_ref_maps();
   void launch_steps(int n, cudaEvent_t* ev = nullptr);
   void autotune(uint64_t& n);
+  void check_tma();
   template <typename T>
   void fill_grid(FitGrid<T>& g, SpecialEdges<T>& s);
 
@@ -150,12 +151,15 @@ class FitSim : public Sim {
   int e_var_ = 2, h_var_ = 2; // kernel variants (see fit_launch_step)
   bool tuned_ = false;
   int tune_pos_ = 0;
-  double tune_e_[4] = {0, 0, 0, 0}, tune_h_[4] = {0, 0, 0, 0};
+  double tune_e_[5] = {0, 0, 0, 0, 0}, tune_h_[5] = {0, 0, 0, 0, 0};
+  FitTmaMaps tma_{};
+  bool tma_ok_ = false;
+  int* dtma_err_ = nullptr;
   void* dC_[12] = {};  // per-dof coefficients M_h, M_q, M_nu, M_mu x 3 axes (autotuned grids)
   void build_coefficients();
 
  public:
-  int kernel_variant() const override { return e_var_ + 4 * h_var_; }
+  int kernel_variant() const override { return e_var_ + 5 * h_var_; }
 
  private:
   // graphs

@@ -12,13 +12,17 @@
 // FMA) in the reference's operation order, so the FP64 path reproduces the
 // CPU reference arithmetic exactly; the FP32 path runs the same code on
 // float state with coefficients rounded from their double values.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "fit_kernels.cuh"
 
-// z-march loop unrolling (planes whose loads the compiler may overlap)
+// z-march loop unrolling: with two planes per iteration the compiler issues
+// the next plane's loads before the current plane's stores (measured at 512^3
+// FP32: E 2.46 -> 2.07 ms, H 2.71 -> 2.26 ms, results bitwise unchanged; four
+// planes spill registers and lose)
 #ifndef TF_FIT_UNROLL
-#define TF_FIT_UNROLL 1
+#define TF_FIT_UNROLL 2
 #endif
 #define TF_PRAGMA(x) _Pragma(#x)
 #define TF_UNROLL(n) TF_PRAGMA(unroll n)
@@ -421,6 +425,322 @@ TF_UNROLL(TF_FIT_UNROLL)
   }
 }
 
+// ---------------------------------------------------------------- TMA z-march
+// The same E and H updates with the face (E) or edge (H) planes a tile of
+// 32 x 8 node columns needs staged in shared memory by the tensor memory
+// accelerator: one elected thread keeps kTmaStages planes in flight
+// (cp.async.bulk.tensor into a ring of buffers, an mbarrier per buffer with
+// the expected byte count), the other threads compute from shared memory.
+// A box covers the tile plus its one-node halo (E: the x-1 / y-1 side, H:
+// the x+1 / y+1 side), its x extent rounded to 16 bytes; the E box starts
+// 16 bytes left of the tile so that every x coordinate stays 16-byte aligned.
+// Coordinates beyond the arrays (the halo at the domain's faces, plane -1 or
+// Nz+1) read as zero and are never used unguarded.  One-GPU code: the tensor
+// maps cover this GPU's arrays only, no multicast.
+constexpr int kTmaTX = 32, kTmaTY = 8;
+// planes in flight: four (FP32) or three (FP64), within 48 KB of static shared memory
+template <typename T>
+__host__ __device__ constexpr int tma_stages() { return sizeof(T) == 4 ? 4 : 3; }
+constexpr long kTmaWaitLimit = 1L << 22;  // mbarrier polls before a wait gives up
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Shared state of one TMA march: ring buffers for three arrays per plane.
+template <typename T, int BX, int BY, int kTmaStages = tma_stages<T>()>
+struct TmaRing {
+  static constexpr int kPlane = BX * BY;                    // elements per array and plane
+  static constexpr uint32_t kBytes = 6u * kPlane * sizeof(T);  // bytes a plane's six boxes bring
+  alignas(128) T buf[kTmaStages][6][kPlane + (128 / sizeof(T) - kPlane % (128 / sizeof(T))) % (128 / sizeof(T))];
+  alignas(8) uint64_t bar[kTmaStages];
+};
+
+// Ring control, run by every thread of the block: issue(q) loads plane q of
+// the march (global plane base + q) into buffer q % kTmaStages; wait(q)
+// blocks until it has arrived.  A wait that runs out of polls raises *err
+// and reports failure; the caller then stops computing, drains the copies
+// still in flight (bounded again) and returns.
+template <typename T, int BX, int BY, int kTmaStages = tma_stages<T>()>
+struct TmaMarch {
+  TmaRing<T, BX, BY>& r;
+  const CUtensorMap* m[6];  // the three staged-neighbour arrays, then the three updated ones
+  int x, y, zbase, nplanes;
+  int* err;
+  __device__ void issue(int q) const {
+    const int st = q % kTmaStages;
+    mbar_expect_tx(&r.bar[st], TmaRing<T, BX, BY>::kBytes);
+#pragma unroll
+    for (int a = 0; a < 6; a++) tma_load_3d(r.buf[st][a], m[a], &r.bar[st], x, y, zbase + q);
+  }
+  __device__ bool wait(int q) const {
+    const uint32_t parity = (uint32_t)((q / kTmaStages) & 1);
+    for (long it = 0; !mbar_try_wait(&r.bar[q % kTmaStages], parity); it++)
+      if (it > kTmaWaitLimit) {
+        atomicExch(err, 1);
+        return false;
+      }
+    return true;
+  }
+  // wait (bounded) for the planes [from, issued) still in flight
+  __device__ void drain(int from, int issued) const {
+    for (int q = from; q < issued; q++) {
+      const uint32_t parity = (uint32_t)((q / kTmaStages) & 1);
+      for (long it = 0; it <= kTmaWaitLimit && !mbar_try_wait(&r.bar[q % kTmaStages], parity); it++) {
+      }
+    }
+  }
+};
+
+template <typename T, int BX, int BY>
+__device__ __forceinline__ void tma_ring_init(TmaRing<T, BX, BY>& r) {
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    for (int q = 0; q < tma_stages<T>(); q++) mbar_init(&r.bar[q], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+}
+
+// H update, TMA form of fit_h_march: the boxes of plane q hold (i0 .. i0+BX-1)
+// x (j0 .. j0+kTmaTY) of Ux, Uy, Uz and of the updated Fx, Fy, Fz; plane k
+// uses the U of planes k and k+1 and the F of plane k.
+template <typename T>
+__global__ void __launch_bounds__(kTmaTX * kTmaTY) fit_h_tma(FitGrid<T> g, int kchunk, int* step_counter,
+                                                            const __grid_constant__ CUtensorMap mUx,
+                                                            const __grid_constant__ CUtensorMap mUy,
+                                                            const __grid_constant__ CUtensorMap mUz,
+                                                            const __grid_constant__ CUtensorMap mFx,
+                                                            const __grid_constant__ CUtensorMap mFy,
+                                                            const __grid_constant__ CUtensorMap mFz, int* err) {
+  using A = Ar<T>;
+  constexpr int BX = kTmaTX + 16 / (int)sizeof(T), BY = kTmaTY + 1;
+  constexpr int kTmaStages = tma_stages<T>();
+  __shared__ TmaRing<T, BX, BY> ring;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = blockIdx.x * kTmaTX, j0 = blockIdx.y * kTmaTY, k0 = blockIdx.z * kchunk;
+  const int i = i0 + tx, j = j0 + ty;
+  if (step_counter && i == 0 && j == 0 && k0 == 0) atomicAdd(step_counter, 1);
+  const int k1 = min(k0 + kchunk, g.Nz + 1);
+  const int nplanes = k1 - k0 + 1;  // planes k0 .. k1
+  tma_ring_init(ring);
+  const TmaMarch<T, BX, BY> mr{ring, {&mUx, &mUy, &mUz, &mFx, &mFy, &mFz}, i0, j0, k0, nplanes, err};
+  const bool lead = tx == 0 && ty == 0;
+  if (lead)
+    for (int q = 0; q < min(kTmaStages, nplanes); q++) mr.issue(q);
+  const bool valid = i <= g.Nx && j <= g.Ny;
+  const T dt = (T)g.dt;
+  const bool ci = i < g.Nx, cj = j < g.Ny;
+  T* __restrict__ Fx = g.Fx;
+  T* __restrict__ Fy = g.Fy;
+  T* __restrict__ Fz = g.Fz;
+  const uint8_t* __restrict__ mat = g.mat;
+  int64_t s = (int64_t)i + g.sx * j + g.sxy * k0;
+  const int64_t cplane = (int64_t)g.Nx * g.Ny;
+  const int64_t cc = (int64_t)i + (int64_t)g.Nx * j;
+  uint8_t m_lo = (valid && ci && cj && k0 > 0) ? __ldg(mat + cc + cplane * (k0 - 1)) : 0;
+  const int o = ty * BX + tx;  // this node in a box
+  int issued = min(kTmaStages, nplanes), failed = -1;
+  bool ok = __syncthreads_and(mr.wait(0));
+  if (!ok) failed = 0;
+  for (int k = k0; ok && k < k1; k++, s += g.sxy) {
+    const int q = k - k0;
+    ok = __syncthreads_and(mr.wait(q + 1));  // every thread leaves together
+    if (!ok) {
+      failed = q + 1;
+      break;
+    }
+    const T* Ux = ring.buf[q % kTmaStages][0];
+    const T* Uy = ring.buf[q % kTmaStages][1];
+    const T* Uz = ring.buf[q % kTmaStages][2];
+    const T* Ux1 = ring.buf[(q + 1) % kTmaStages][0];
+    const T* Uy1 = ring.buf[(q + 1) % kTmaStages][1];
+    const T* Fxs = ring.buf[q % kTmaStages][3];
+    const T* Fys = ring.buf[q % kTmaStages][4];
+    const T* Fzs = ring.buf[q % kTmaStages][5];
+    if (valid) {
+      const bool ck = k < g.Nz;
+      const uint8_t m0 = (ci && cj && ck) ? __ldg(mat + cc + cplane * k) : 0;
+      const T ux = ci ? Ux[o] : (T)0, uy = cj ? Uy[o] : (T)0;
+      const T ux1 = (ci && ck) ? Ux1[o] : (T)0, uy1 = (cj && ck) ? Uy1[o] : (T)0;
+      T mnu, mmu;
+      if (cj && ck) {  // Fx(i,j,k): cells (i-1,j,k), (i,j,k)
+        const uint8_t ml = i > 0 ? __ldg(mat + cc - 1 + cplane * k) : 0;
+        if (face_coef_t(g, 0, i > 0, ci, ml, m0, mnu, mmu)) {
+          const T cs = A::sub(A::add(A::sub(uy, Uz[o]), Uz[o + BX]), uy1);
+          Fx[s] = A::mul(mnu, face_flux(mmu, Fxs[o], dt, cs));
+        }
+      }
+      if (ci && ck) {  // Fy(i,j,k): cells (i,j-1,k), (i,j,k); curl -1
+        const uint8_t ml = j > 0 ? __ldg(mat + cc - g.Nx + cplane * k) : 0;
+        if (face_coef_t(g, 1, j > 0, cj, ml, m0, mnu, mmu)) {
+          const T cs = A::sub(A::add(A::sub(ux, Uz[o]), Uz[o + 1]), ux1);
+          Fy[s] = A::mul(mnu, face_flux(mmu, Fys[o], -dt, cs));
+        }
+      }
+      if (ci && cj) {  // Fz(i,j,k): cells (i,j,k-1), (i,j,k)
+        if (face_coef_t(g, 2, k > 0, ck, m_lo, m0, mnu, mmu)) {
+          const T cs = A::sub(A::add(A::sub(ux, uy), Uy[o + 1]), Ux[o + BX]);
+          Fz[s] = A::mul(mnu, face_flux(mmu, Fzs[o], dt, cs));
+        }
+      }
+      m_lo = m0;
+    }
+    __syncthreads();  // plane q's buffer is free again
+    if (q + kTmaStages < nplanes) {
+      if (lead) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mr.issue(q + kTmaStages);
+      }
+      issued = q + kTmaStages + 1;
+    }
+  }
+  if (!ok && lead) mr.drain(failed, issued);
+}
+
+// E update, TMA form of fit_e_march: the boxes of plane q hold
+// (i0-H .. i0+kTmaTX-1) x (j0-1 .. j0+kTmaTY-1) of Fx, Fy, Fz and of the
+// updated Ux, Uy, Uz, H = 16 bytes of elements; plane k uses the F of planes
+// k-1 and k and the U of plane k.
+template <typename T>
+__global__ void __launch_bounds__(kTmaTX * kTmaTY) fit_e_tma(FitGrid<T> g, int kchunk,
+                                                            const __grid_constant__ CUtensorMap mFx,
+                                                            const __grid_constant__ CUtensorMap mFy,
+                                                            const __grid_constant__ CUtensorMap mFz,
+                                                            const __grid_constant__ CUtensorMap mUx,
+                                                            const __grid_constant__ CUtensorMap mUy,
+                                                            const __grid_constant__ CUtensorMap mUz, int* err) {
+  using A = Ar<T>;
+  constexpr int H = 16 / (int)sizeof(T);
+  constexpr int BX = kTmaTX + H, BY = kTmaTY + 1;
+  constexpr int kTmaStages = tma_stages<T>();
+  __shared__ TmaRing<T, BX, BY> ring;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i0 = blockIdx.x * kTmaTX, j0 = blockIdx.y * kTmaTY, k0 = blockIdx.z * kchunk;
+  const int i = i0 + tx, j = j0 + ty;
+  const int k1 = min(k0 + kchunk, g.Nz + 1);
+  const int nplanes = k1 - k0 + 1;  // planes k0-1 .. k1-1
+  tma_ring_init(ring);
+  const TmaMarch<T, BX, BY> mr{ring, {&mFx, &mFy, &mFz, &mUx, &mUy, &mUz}, i0 - H, j0 - 1, k0 - 1, nplanes, err};
+  const bool lead = tx == 0 && ty == 0;
+  if (lead)
+    for (int q = 0; q < min(kTmaStages, nplanes); q++) mr.issue(q);
+  const bool valid = i <= g.Nx && j <= g.Ny;
+  const T dt = (T)g.dt;
+  T* __restrict__ Ux = g.Ux;
+  T* __restrict__ Uy = g.Uy;
+  T* __restrict__ Uz = g.Uz;
+  const uint8_t* __restrict__ mat = g.mat;
+  const bool xin = i > 0 && i < g.Nx, yin = j > 0 && j < g.Ny;
+  const bool xe = i < g.Nx && yin, ye = j < g.Ny && xin, ze = xin && yin;
+  const bool ci0 = i > 0, ci1 = i < g.Nx, cj0 = j > 0, cj1 = j < g.Ny;
+  int64_t s = (int64_t)i + g.sx * j + g.sxy * k0;
+  const int64_t cb = (int64_t)(i - 1) + (int64_t)g.Nx * (j - 1);
+  const int64_t cplane = (int64_t)g.Nx * g.Ny;
+  uint8_t lo[2][2] = {{0, 0}, {0, 0}};
+  if (valid && k0 > 0) {
+    const uint8_t* m = mat + cb + cplane * (k0 - 1);
+    lo[0][0] = (ci0 && cj0) ? __ldg(m) : 0;
+    lo[0][1] = (ci1 && cj0) ? __ldg(m + 1) : 0;
+    lo[1][0] = (ci0 && cj1) ? __ldg(m + g.Nx) : 0;
+    lo[1][1] = (ci1 && cj1) ? __ldg(m + g.Nx + 1) : 0;
+  }
+  const int o = (ty + 1) * BX + tx + H;  // this node in a box
+  int issued = min(kTmaStages, nplanes), failed = -1;
+  bool ok = __syncthreads_and(mr.wait(0));
+  if (!ok) failed = 0;
+  for (int k = k0; ok && k < k1; k++, s += g.sxy) {
+    const int q = k - k0;  // plane k-1 is ring plane q, plane k is q + 1
+    ok = __syncthreads_and(mr.wait(q + 1));
+    if (!ok) {
+      failed = q + 1;
+      break;
+    }
+    const T* Fxl = ring.buf[q % kTmaStages][0];
+    const T* Fyl = ring.buf[q % kTmaStages][1];
+    const T* Fx = ring.buf[(q + 1) % kTmaStages][0];
+    const T* Fy = ring.buf[(q + 1) % kTmaStages][1];
+    const T* Fz = ring.buf[(q + 1) % kTmaStages][2];
+    const T* Uxs = ring.buf[(q + 1) % kTmaStages][3];
+    const T* Uys = ring.buf[(q + 1) % kTmaStages][4];
+    const T* Uzs = ring.buf[(q + 1) % kTmaStages][5];
+    if (valid) {
+      const bool zin = k > 0 && k < g.Nz;
+      uint8_t hi[2][2] = {{0, 0}, {0, 0}};
+      if (k < g.Nz) {
+        const uint8_t* m = mat + cb + cplane * k;
+        hi[0][0] = (ci0 && cj0) ? __ldg(m) : 0;
+        hi[0][1] = (ci1 && cj0) ? __ldg(m + 1) : 0;
+        hi[1][0] = (ci0 && cj1) ? __ldg(m + g.Nx) : 0;
+        hi[1][1] = (ci1 && cj1) ? __ldg(m + g.Nx + 1) : 0;
+      }
+      const T fx = (j < g.Ny && k < g.Nz) ? Fx[o] : (T)0;
+      const T fy = (i < g.Nx && k < g.Nz) ? Fy[o] : (T)0;
+      if (zin) {
+        const T fz = Fz[o];
+        const bool same = lo[0][0] == lo[0][1] && lo[0][0] == lo[1][0] && lo[0][0] == lo[1][1] &&
+                          lo[0][0] == hi[0][0] && lo[0][0] == hi[0][1] && lo[0][0] == hi[1][0] &&
+                          lo[0][0] == hi[1][1];
+        if (xe) {  // x-edge: faces Fy(k-1), Fz(j-1), Fz, Fy
+          T mh, mq;
+          if (same) { mh = g.mh_pure[3 * lo[0][0]]; mq = g.mq_pure[3 * lo[0][0]]; }
+          else { uint8_t m[4] = {lo[0][1], lo[1][1], hi[0][1], hi[1][1]}; edge_coef_t(g, 0, m, mh, mq); }
+          const T cf = A::sub(A::add(A::sub(Fyl[o], Fz[o - BX]), fz), fy);
+          Ux[s] = A::mul(mh, A::add(A::mul(mq, Uxs[o]), A::mul(dt, cf)));
+        }
+        if (ye) {  // y-edge: faces Fx(k-1), Fz(i-1), Fz, Fx; dual curl -1
+          T mh, mq;
+          if (same) { mh = g.mh_pure[3 * lo[0][0] + 1]; mq = g.mq_pure[3 * lo[0][0] + 1]; }
+          else { uint8_t m[4] = {lo[1][0], lo[1][1], hi[1][0], hi[1][1]}; edge_coef_t(g, 1, m, mh, mq); }
+          const T cf = -A::sub(A::add(A::sub(Fxl[o], Fz[o - 1]), fz), fx);
+          Uy[s] = A::mul(mh, A::add(A::mul(mq, Uys[o]), A::mul(dt, cf)));
+        }
+      }
+      if (ze && k < g.Nz) {  // z-edge: faces Fx(j-1), Fy(i-1), Fy, Fx
+        T mh, mq;
+        if (hi[0][0] == hi[0][1] && hi[0][0] == hi[1][0] && hi[0][0] == hi[1][1]) {
+          mh = g.mh_pure[3 * hi[0][0] + 2];
+          mq = g.mq_pure[3 * hi[0][0] + 2];
+        } else {
+          uint8_t m[4] = {hi[0][0], hi[0][1], hi[1][0], hi[1][1]};
+          edge_coef_t(g, 2, m, mh, mq);
+        }
+        const T cf = A::sub(A::add(A::sub(Fx[o - BX], Fy[o - 1]), fy), fx);
+        Uz[s] = A::mul(mh, A::add(A::mul(mq, Uzs[o]), A::mul(dt, cf)));
+      }
+      lo[0][0] = hi[0][0]; lo[0][1] = hi[0][1]; lo[1][0] = hi[1][0]; lo[1][1] = hi[1][1];
+    }
+    __syncthreads();
+    if (q + kTmaStages < nplanes) {
+      if (lead) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mr.issue(q + kTmaStages);
+      }
+      issued = q + kTmaStages + 1;
+    }
+  }
+  if (!ok && lead) mr.drain(failed, issued);
+}
+
 template <typename T>
 __device__ __forceinline__ T* comp_ptr(T* x, T* y, T* z, int c) {
   return c == 0 ? x : (c == 1 ? y : z);
@@ -762,7 +1082,7 @@ __global__ void __launch_bounds__(256) fit_loss_finish(const double* part, int n
 template <typename T>
 void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const ProbeSet& pr, int* step_counter,
                      double* flux, cudaStream_t st, cudaEvent_t* ev, int e_variant, int h_variant,
-                     const FitLoss<T>* loss) {
+                     const FitLoss<T>* loss, const FitTmaMaps* tma) {
   // ev (optional): 6 events recorded around the 5 phases, for per-phase timing;
   // loss (optional): Joule loss of the E half step
   dim3 blk(32, 8, 1);
@@ -782,8 +1102,11 @@ void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const Probe
   if (ev) cudaEventRecord(ev[1], st);
   if (e_variant == 0) fit_e_kernel<T><<<grd, blk, 0, st>>>(g);
   else if (e_variant == 3) fit_e_coef<T><<<grd, blk, 0, st>>>(g);
+  else if (e_variant == 4 && tma)
+    fit_e_tma<T><<<mgrid(16), blk, 0, st>>>(g, 16, tma->F[0], tma->F[1], tma->F[2], tma->U[0], tma->U[1], tma->U[2],
+                                             tma->err);
   else {
-    const int kc = e_variant == 1 ? 4 : 16;
+    const int kc = e_variant == 1 ? 4 : 16;  // variants 1, 2 (and 4 without tensor maps)
     fit_e_march<T><<<mgrid(kc), blk, 0, st>>>(g, kc);
   }
   if (ev) cudaEventRecord(ev[2], st);
@@ -797,6 +1120,9 @@ void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const Probe
   if (ev) cudaEventRecord(ev[4], st);
   if (h_variant == 0) fit_h_kernel<T><<<grd, blk, 0, st>>>(g, step_counter);
   else if (h_variant == 3) fit_h_coef<T><<<grd, blk, 0, st>>>(g, step_counter);
+  else if (h_variant == 4 && tma)
+    fit_h_tma<T><<<mgrid(16), blk, 0, st>>>(g, 16, step_counter, tma->U[0], tma->U[1], tma->U[2], tma->F[0],
+                                             tma->F[1], tma->F[2], tma->err);
   else {
     const int kc = h_variant == 1 ? 4 : 16;
     fit_h_march<T><<<mgrid(kc), blk, 0, st>>>(g, kc, step_counter);
@@ -814,9 +1140,46 @@ size_t fit_loss_parts(int Nx, int Ny, int Nz) {
 }
 
 template void fit_launch_step<double>(const FitGrid<double>&, const SpecialEdges<double>&, const ProbeSet&, int*,
-                                      double*, cudaStream_t, cudaEvent_t*, int, int, const FitLoss<double>*);
+                                      double*, cudaStream_t, cudaEvent_t*, int, int, const FitLoss<double>*,
+                                      const FitTmaMaps*);
 template void fit_launch_step<float>(const FitGrid<float>&, const SpecialEdges<float>&, const ProbeSet&, int*,
-                                     double*, cudaStream_t, cudaEvent_t*, int, int, const FitLoss<float>*);
+                                     double*, cudaStream_t, cudaEvent_t*, int, int, const FitLoss<float>*,
+                                     const FitTmaMaps*);
+
+// Tensor maps for the TMA z-march; false when the driver offers no encoder
+// or refuses the layout (the variant is then not offered).
+bool fit_make_tma_maps(void* const U[3], void* const F[3], int es, int Nx, int Ny, int Nz, int64_t sx,
+                       FitTmaMaps* out) {
+  typedef CUresult (*Encode)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                             const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                             CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn ||
+      q != cudaDriverEntryPointSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  Encode enc = (Encode)fn;
+  const cuuint64_t dims[3] = {(cuuint64_t)sx, (cuuint64_t)Ny + 1, (cuuint64_t)Nz + 1};
+  const cuuint64_t strides[2] = {(cuuint64_t)(sx * es), (cuuint64_t)(sx * es * (Ny + 1))};
+  const cuuint32_t box[3] = {(cuuint32_t)(kTmaTX + 16 / es), (cuuint32_t)(kTmaTY + 1), 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUtensorMapDataType dtype = es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  if ((sx * es) % 16 != 0) return false;
+  for (int a = 0; a < 3; a++) {
+    if (enc(&out->U[a], dtype, 3, U[a], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+    if (enc(&out->F[a], dtype, 3, F[a], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+  }
+  (void)Nx;
+  return true;
+}
 
 // Discrete leapfrog energy of the state after a step, (U^n, F^{n+1/2}):
 // W^n = 0.5 sum M_e (U^n)^2 + 0.5 sum M_mu F^{n+1/2} F^{n-1/2}, an invariant of

@@ -15,6 +15,7 @@
 // as the reference's averaging (Discretization.hpp:5234-5330, 5485-5609), so
 // they are bit-identical to precomputed per-dof values.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -84,6 +85,14 @@ struct FitLoss {
   double* part;      // [nparts] per-block partial sums
   double* loss;      // [nsteps] loss per step
   int nparts;
+};
+
+// Tensor maps of the TMA z-march (kernel variant 4): Ux, Uy, Uz and Fx, Fy,
+// Fz over their [Nz+1][Ny+1][sx] arrays, box (32 + 16 bytes) x 9 x 1; err
+// receives 1 when an mbarrier wait gave up.
+struct FitTmaMaps {
+  CUtensorMap U[3], F[3];
+  int* err;
 };
 
 template <typename T>

@@ -13,6 +13,7 @@
 
 #include "../../include/tetfit.h"
 #include "mlp.cuh"
+#include "mlp_tc.cuh"
 
 namespace tf {
 void set_thread_error(const std::string& m);
@@ -266,9 +267,41 @@ cudaError_t mlp_launch_train(const MlpTrain& m, const float* inputs, const float
   return cudaGetLastError();
 }
 
+// Inference on the 5th-generation tensor cores (mlp_tc.cuh): 128 rows per
+// tile, a grid-stride loop of tiles per CTA.  err receives 4 when an MMA
+// completion wait gave up.
+__global__ void __launch_bounds__(kTcRows) mlp_eval_tc_kernel(const unsigned char* image, const float* in, int64_t n,
+                                                              float* out, int* err) {
+  extern __shared__ __align__(128) unsigned char tc_raw[];
+  MlpTcSmem& sm = *reinterpret_cast<MlpTcSmem*>(tc_raw);
+  mlp_tc_setup(sm, image);
+  uint32_t phase = 0;
+  const int64_t tiles = (n + kTcRows - 1) / kTcRows;
+  for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const int64_t row = t * kTcRows + threadIdx.x;
+    float f[6];
+    for (int k = 0; k < 6; k++) f[k] = row < n ? in[row * 6 + k] : 0.0f;
+    float y = 0.0f;
+    if (!mlp_tc_forward(sm, phase, f, y, err)) break;
+    if (row < n) out[row] = y;
+  }
+  mlp_tc_teardown(sm);
+}
+
 cudaError_t mlp_launch_eval(const unsigned char* image, const float* in, int64_t n, float* out, cudaStream_t st) {
   const int64_t warps = (n + 31) / 32;
   mlp_eval_kernel<<<(unsigned)((warps + 7) / 8), 256, 0, st>>>(image, in, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t mlp_launch_eval_tc(const unsigned char* image, const float* in, int64_t n, float* out, int* err,
+                               cudaStream_t st) {
+  const int64_t tiles = (n + kTcRows - 1) / kTcRows;
+  int sms = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t grid = tiles < 4 * (int64_t)sms ? tiles : 4 * (int64_t)sms;
+  mlp_eval_tc_kernel<<<(unsigned)(grid > 0 ? grid : 1), kTcRows, sizeof(MlpTcSmem), st>>>(image, in, n, out, err);
   return cudaGetLastError();
 }
 
@@ -339,8 +372,14 @@ TF_API int tf_mlp_forward(const float* params, int64_t n, const float* inputs, f
   int rc;
   if ((rc = mlp_cuda(cudaMemcpy(p, params, sizeof(float) * tf::kNParam, cudaMemcpyHostToDevice), "copy"))) return rc;
   if ((rc = mlp_cuda(cudaMemcpy(in, inputs, sizeof(float) * 6 * n, cudaMemcpyHostToDevice), "copy"))) return rc;
+  int* err = b.get<int>(1);
+  if (!err) return mlp_fail(TF_E_CUDA, "tf_mlp_forward: device allocation failed");
+  if ((rc = mlp_cuda(cudaMemset(err, 0, sizeof(int)), "memset"))) return rc;
   if ((rc = mlp_cuda(tf::mlp_launch_pack(p, img, 0), "pack"))) return rc;
-  if ((rc = mlp_cuda(tf::mlp_launch_eval(img, in, n, out, 0), "eval"))) return rc;
+  if ((rc = mlp_cuda(tf::mlp_launch_eval_tc(img, in, n, out, err, 0), "eval"))) return rc;
+  int e = 0;
+  if ((rc = mlp_cuda(cudaMemcpy(&e, err, sizeof(int), cudaMemcpyDeviceToHost), "copy"))) return rc;
+  if (e) return mlp_fail(TF_E_CUDA, "tf_mlp_forward: a tensor-core completion wait ran out of time");
   return mlp_cuda(cudaMemcpy(outputs, out, sizeof(float) * n, cudaMemcpyDeviceToHost), "copy");
 }
 

@@ -100,6 +100,7 @@ TetGroup::TetGroup(std::vector<TetSim*> sims, const RunOptions& opt, bool releas
 }
 
 TetGroup::~TetGroup() {
+  if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
   if (pinned_) cudaFreeHost(pinned_);
   for (void* p : allocs_) cudaFree(p);
   if (ev0_) cudaEventDestroy(ev0_);
@@ -588,7 +589,26 @@ uint64_t TetGroup::step(uint64_t n) {
   }
   if (done < n) {
     CU(cudaEventRecord(ev0_, stream_));
-    launch((int)(n - done), nullptr);
+    uint64_t rest = n - done;
+    // Once the CG variant is chosen and the network (if any) has finished
+    // training, every step launches the same kernels with the same
+    // arguments (per-step state lives in device memory), so runs of
+    // graph_len_ steps replay one captured CUDA graph.
+    const int glen = opt_.graph_steps > 0 ? opt_.graph_steps : 16;
+    while (rest > 0) {
+      const bool training = opt_.warm_start == 3 && launched_ < opt_.learn_steps;
+      if (glen > 1 && rest >= (uint64_t)glen && !training && !graph_failed_) {
+        if (!graph_exec_) capture_graph(glen);
+        if (graph_exec_) {
+          CU(cudaGraphLaunch(graph_exec_, stream_));
+          launched_ += glen;
+          rest -= glen;
+          continue;
+        }
+      }
+      launch(1, nullptr);
+      rest--;
+    }
     CU(cudaEventRecord(ev1_, stream_));
     CU(cudaEventSynchronize(ev1_));
     float ms = 0;
@@ -599,6 +619,37 @@ uint64_t TetGroup::step(uint64_t n) {
   for (Meta& m : meta_) m.step = std::min(m.nsteps, m.step + n);
   check_err();
   return n;
+}
+
+// Captures `len` steps of kernel launches into graph_exec_.  A capture that
+// the runtime refuses leaves graph_exec_ null and graph_failed_ set; the
+// steps are then launched one by one (same kernels, same results).
+void TetGroup::capture_graph(int len) {
+  cudaGraph_t g = nullptr;
+  if (cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    graph_failed_ = true;
+    return;
+  }
+  const int64_t before = launched_;
+  bool ok = true;
+  try {
+    launch(len, nullptr);
+  } catch (const CudaError&) {
+    ok = false;  // a launch the capture refused; end the capture below
+  }
+  launched_ = before;  // captured, not run
+  cudaError_t e = cudaStreamEndCapture(stream_, &g);
+  if (!ok && e == cudaSuccess) e = cudaErrorStreamCaptureInvalidated;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&graph_exec_, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    graph_exec_ = nullptr;
+    graph_failed_ = true;
+    return;
+  }
+  graph_len_ = len;
 }
 
 uint64_t TetGroup::phase_times(uint64_t n, double* ms5) {

@@ -76,6 +76,7 @@ class TetGroup {
   void partition();
   void check_err();
   void launch(int n, cudaEvent_t* ev);
+  void capture_graph(int len);
   void* dalloc(size_t bytes);
   template <typename V, typename A>
   void* upload(const std::vector<V, A>& v);
@@ -103,6 +104,13 @@ class TetGroup {
   int64_t samp_n_ = 0, samp_stride_ = 1;
   float* loss_hist_ = nullptr;
   double* energy_part_ = nullptr;  // partial sums of grp_energy (allocated on first use)
+  // captured step loop (see step())
+  cudaGraphExec_t graph_exec_ = nullptr;
+  int graph_len_ = 0;
+  bool graph_failed_ = false;
+ public:
+  bool graph_active() const { return graph_exec_ != nullptr; }
+ private:
   int64_t loss_cap_ = 0;  // per-simulation carrier tables (for step_io overrides)
 };
 

@@ -28,6 +28,7 @@
 
 #include "grid_barrier.cuh"
 #include "mlp.cuh"
+#include "mlp_tc.cuh"
 #include "tet_group_kernels.cuh"
 
 
@@ -67,6 +68,33 @@ __device__ __forceinline__ double ld_stream(const double* p) {
 // are taken 4 at a time: the index and value loads of a chunk are all issued
 // before its gathers, so a row costs about two memory latencies instead of
 // one per entry group.
+// The same sweep with the sum in A (values of type T read from the matrix):
+// sell_dot<double>(m, row, g, (const float*)nullptr) sums FP32 entries in FP64.
+template <typename A, typename G, typename T>
+__device__ __forceinline__ A sell_dot(const SellDev& m, int64_t row, G g, const T*) {
+  constexpr int CH = 4;
+  const int64_t sl = row >> 5;
+  const int64_t b = m.ptr[sl];
+  const int len = (int)((m.ptr[sl + 1] - b) >> 5);
+  const int32_t* col = m.col + b + (row & 31);
+  const T* val = (const T*)m.val + b + (row & 31);
+  A s = 0;
+  for (int j0 = 0; j0 < len; j0 += CH) {
+    int32_t c[CH];
+    T v[CH];
+#pragma unroll
+    for (int k = 0; k < CH; k++)
+      if (j0 + k < len) {
+        c[k] = ld_stream(col + 32 * (j0 + k));
+        v[k] = ld_stream(val + 32 * (j0 + k));
+      }
+#pragma unroll
+    for (int k = 0; k < CH; k++)
+      if (j0 + k < len) s += (A)v[k] * g(c[k]);
+  }
+  return s;
+}
+
 template <typename T, typename G>
 __device__ __forceinline__ T sell_dot(const SellDev& m, int64_t row, G g) {
   constexpr int CH = 4;
@@ -302,9 +330,15 @@ __global__ void __launch_bounds__(kGB) grp_rhs(GroupDev d) {
   const bool fem = d.fem && d.fem[s];
   const T* Uo = (const T*)d.Uo;
   // gfdtd: E U_old - RHSmat1 SrcFld; fem: E (2 U_old - U_older) - E_dir SrcFld
-  // (the source values live on the Dirichlet columns only)
-  const T eu = fem ? sell_dot<T>(d.Ef, i, [&](int32_t c) { return (T)2 * U[c] - Uo[c] - S[c]; })
-                   : sell_dot<T>(d.Ef, i, [&](int32_t c) { return U[c] - S[c]; });
+  // (the source values live on the Dirichlet columns only).  fem sums in
+  // FP64: its right-hand side is dominated by E U / dt^2 terms whose
+  // difference carries the update, so FP32 sums would lose it.
+  double eu_fem = 0.0;
+  if (fem)
+    eu_fem = sell_dot<double>(d.Ef, i, [&](int32_t c) {
+      return 2.0 * (double)U[c] - (double)Uo[c] - (double)S[c];
+    }, (const T*)nullptr);
+  const T eu = fem ? (T)0 : sell_dot<T>(d.Ef, i, [&](int32_t c) { return U[c] - S[c]; });
   // C^T F over the edge's faces in stored order; the face indices of 4
   // entries are loaded before their gathers (padding entries hold kPadCol
   // and add nothing)
@@ -332,7 +366,8 @@ __global__ void __launch_bounds__(kGB) grp_rhs(GroupDev d) {
     // Psi = (2 E U_old - E U_older - E_dir SrcFld) / dt^2 - C^T N C U_old
     //       + (Fb - Fb_old) / dt - I / dt   (Discretization.hpp:1713-1716)
     const double idt = 1.0 / d.dt[s];
-    ((T*)d.rhs)[i] = eu * (T)(idt * idt) - cf + (T)idt * ((const T*)d.cb)[e] - (T)idt * ((const T*)d.I)[e];
+    ((T*)d.rhs)[i] = (T)(eu_fem * (idt * idt) - (double)cf + idt * (double)((const T*)d.cb)[e] -
+                         idt * (double)((const T*)d.I)[e]);
   } else {
     ((T*)d.rhs)[i] = eu - dt * ((const T*)d.I)[e] + dt * cf + dt * ((const T*)d.cb)[e];
   }
@@ -381,6 +416,92 @@ __global__ void __launch_bounds__(kGB) grp_resid_e(GroupDev d) {
   ((T*)d.r_alt)[i] = ((const T*)d.rhs)[i] - sell_dot<T>(d.A, i, [&](int32_t c) { return xe[c]; });
 }
 
+// Inputs of one row of the learned guess (see above), with the history
+// shift, the extrapolated guess in x and the training sample written here:
+// f[6] the network's inputs, sg the row scale, ok whether the guess applies.
+template <typename T>
+__device__ __forceinline__ void guess_row(const GroupDev& d, int64_t sl, int64_t i, int s, float f[6], float& sg,
+                                          bool& ok) {
+  T* x = (T*)d.x;
+  T* h1 = (T*)d.xh1;
+  T* h2 = (T*)d.xh2;
+  T* h3 = (T*)d.xh3;
+  const T* re = (const T*)d.r_alt;
+  const T* pre = (const T*)d.pre;
+  const bool real = d.free_edge[i] >= 0;
+  const double a = x[i], b1 = h1[i], c = h2[i], dd = h3[i];
+  const double e = (double)((const T*)d.xe)[i];
+  float sum = 0.0f;
+  int cnt = 0;
+  {
+    const int64_t b0 = d.A.ptr[sl];
+    const int len = (int)((d.A.ptr[sl + 1] - b0) >> 5);
+    const int32_t* col = d.A.col + b0 + (i & 31);
+    for (int j = 0; j < len; j++) {
+      const int32_t cc = ld_stream(col + 32 * j);
+      if (cc != (int32_t)i) {
+        sum += (float)re[cc];
+        cnt++;
+      }
+    }
+  }
+  const float pr = (float)pre[i];
+  const float jr = pr * (float)re[i];
+  const float jm = cnt ? pr * sum / (float)cnt : jr;
+  const float d3 = (float)(a - 3.0 * b1 + 3.0 * c - dd), d2 = (float)(a - 2.0 * b1 + c), d1 = (float)(a - b1);
+  sg = sqrtf(0.5f * (d3 * d3 + jr * jr));
+  ok = real && sg > 0.0f && isfinite(sg) && d.step[s] >= 4;
+  const float inv = ok ? 1.0f / sg : 0.0f;
+  f[0] = d3 * inv;
+  f[1] = mlp_compress(d2 * inv);
+  f[2] = mlp_compress(d1 * inv);
+  f[3] = mlp_compress((float)a * inv);
+  f[4] = jr * inv;
+  f[5] = jm * inv;
+  if (real) {
+    h3[i] = (T)c;
+    h2[i] = (T)b1;
+    h1[i] = (T)a;
+    x[i] = (T)e;
+    if (d.nsamp && i >= d.samp_first && (i - d.samp_first) % d.samp_stride == 0) {
+      const int64_t k = (i - d.samp_first) / d.samp_stride;
+      if (k < d.nsamp) {
+        for (int q = 0; q < 6; q++) d.samp_in[6 * k + q] = f[q];
+        d.samp_e[k] = (float)e;
+        d.samp_s[k] = sg;
+        d.samp_row[k] = ok ? (int32_t)i : -1;
+      }
+    }
+  }
+}
+
+// The trained network's guess on the 5th-generation tensor cores
+// (mlp_tc.cuh): a CTA of four warps takes four slices (128 rows) per tile,
+// warp w the slice whose rows are TMEM lanes 32w..32w+31.  Same inputs and
+// outputs as grp_guess_mlp with mlp_on set.
+template <typename T>
+__global__ void __launch_bounds__(kTcRows) grp_guess_tc(GroupDev d) {
+  extern __shared__ __align__(128) unsigned char tc_raw[];
+  MlpTcSmem& sm = *reinterpret_cast<MlpTcSmem*>(tc_raw);
+  mlp_tc_setup(sm, d.mlp_img);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t nsl = d.nrow >> 5, tiles = (nsl + 3) / 4;
+  T* x = (T*)d.x;
+  uint32_t phase = 0;
+  for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const int64_t sl = 4 * t + warp;
+    const int64_t i = sl * 32 + lane;
+    const int s = sl < nsl ? d.slice_sim[sl] : 0;
+    const bool act = sl < nsl && running(d, s);
+    float f[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, sg = 0.0f, y = 0.0f;
+    bool ok = false;
+    if (act) guess_row<T>(d, sl, i, s, f, sg, ok);
+    if (!mlp_tc_forward(sm, phase, f, y, d.err)) break;
+    if (act && ok) x[i] = (T)((double)x[i] + (double)sg * (double)y);
+  }
+  mlp_tc_teardown(sm);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kGB, 3) grp_guess_mlp(GroupDev d) {
   __shared__ __align__(16) unsigned char img[kImgBytes];
@@ -391,62 +512,14 @@ __global__ void __launch_bounds__(kGB, 3) grp_guess_mlp(GroupDev d) {
   const int64_t nsl = d.nrow >> 5;
   const int64_t nw = ((int64_t)gridDim.x * kGB) >> 5;
   T* x = (T*)d.x;
-  T* h1 = (T*)d.xh1;
-  T* h2 = (T*)d.xh2;
-  T* h3 = (T*)d.xh3;
-  const T* re = (const T*)d.r_alt;
-  const T* pre = (const T*)d.pre;
   // a warp takes whole slices (one simulation each), the grid strides over them
   for (int64_t sl = ((int64_t)blockIdx.x * kGB + threadIdx.x) >> 5; sl < nsl; sl += nw) {
     const int s = d.slice_sim[sl];
     if (!running(d, s)) continue;
     const int64_t i = sl * 32 + lane;
-    const bool real = d.free_edge[i] >= 0;
-    const double a = x[i], b1 = h1[i], c = h2[i], dd = h3[i];
-    const double e = (double)((const T*)d.xe)[i];
-    // neighbour mean of r_e over the row's pattern (padding entries point at
-    // the row itself and drop out with it)
-    float sum = 0.0f;
-    int cnt = 0;
-    {
-      const int64_t b0 = d.A.ptr[sl];
-      const int len = (int)((d.A.ptr[sl + 1] - b0) >> 5);
-      const int32_t* col = d.A.col + b0 + lane;
-      for (int j = 0; j < len; j++) {
-        const int32_t cc = ld_stream(col + 32 * j);
-        if (cc != (int32_t)i) {
-          sum += (float)re[cc];
-          cnt++;
-        }
-      }
-    }
-    // differences of the history in the state's precision (they cancel),
-    // everything after in FP32
-    const float pr = (float)pre[i];
-    const float jr = pr * (float)re[i];
-    const float jm = cnt ? pr * sum / (float)cnt : jr;
-    const float d3 = (float)(a - 3.0 * b1 + 3.0 * c - dd), d2 = (float)(a - 2.0 * b1 + c), d1 = (float)(a - b1);
-    const float sg = sqrtf(0.5f * (d3 * d3 + jr * jr));
-    const bool ok = real && sg > 0.0f && isfinite(sg) && d.step[s] >= 4;
-    const float inv = ok ? 1.0f / sg : 0.0f;
-    float f[6] = {d3 * inv, mlp_compress(d2 * inv), mlp_compress(d1 * inv), mlp_compress((float)a * inv), jr * inv, jm * inv};
-    // history shift, the extrapolated guess and the training sample first,
-    // so that none of it stays live across the network
-    if (real) {
-      h3[i] = (T)c;
-      h2[i] = (T)b1;
-      h1[i] = (T)a;
-      x[i] = (T)e;
-      if (d.nsamp && i >= d.samp_first && (i - d.samp_first) % d.samp_stride == 0) {
-        const int64_t k = (i - d.samp_first) / d.samp_stride;
-        if (k < d.nsamp) {
-          for (int q = 0; q < 6; q++) d.samp_in[6 * k + q] = f[q];
-          d.samp_e[k] = (float)e;
-          d.samp_s[k] = sg;
-          d.samp_row[k] = ok ? (int32_t)i : -1;
-        }
-      }
-    }
+    float f[6], sg;
+    bool ok;
+    guess_row<T>(d, sl, i, s, f, sg, ok);
     if (d.mlp_on) {
       uint32_t a1[2][4];
       float y[2][4];
@@ -874,7 +947,14 @@ cudaError_t group_launch_step(const GroupDev& d, int cg_blocks, int cg_variant, 
     grp_resid_e<T><<<gblk(d.nrow), kGB, 0, st>>>(d);
     const int64_t slices = d.nrow >> 5, per_block = kGB / 32;
     const int64_t want = (slices + per_block - 1) / per_block;
-    grp_guess_mlp<T><<<(unsigned)(want < d.guess_blocks ? (want > 0 ? want : 1) : d.guess_blocks), kGB, 0, st>>>(d);
+    if (d.mlp_on) {
+      // trained network: the tensor-core form, 128 rows per tile
+      const int64_t tiles = (slices + 3) / 4;
+      const int64_t g = tiles < 2 * (int64_t)d.guess_blocks ? tiles : 2 * (int64_t)d.guess_blocks;
+      grp_guess_tc<T><<<(unsigned)(g > 0 ? g : 1), kTcRows, sizeof(MlpTcSmem), st>>>(d);
+    } else {
+      grp_guess_mlp<T><<<(unsigned)(want < d.guess_blocks ? (want > 0 ? want : 1) : d.guess_blocks), kGB, 0, st>>>(d);
+    }
   }
   if (ev) cudaEventRecord(ev[2], st);
   cudaLaunchConfig_t cfg = {};
