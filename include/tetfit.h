@@ -83,10 +83,11 @@ typedef struct tf_info {
   uint64_t nnz_operators;              /* nonzeros of H (dga) or of E (gfdtd)     */
   uint32_t cg_blocks;                  /* gfdtd: blocks of the persistent CG kernel */
   int32_t cg_variant;                  /* gfdtd: CG variant the autotuner picked;
-                                          fdtd: E variant + 5 x H variant (0 one
+                                          fdtd: E variant + 8 x H variant (0 one
                                           thread per node, 1/2 z-march over 4/16
                                           planes, 3 per-dof coefficient arrays,
-                                          4 z-march with TMA-staged planes)     */
+                                          4 z-march with TMA-staged planes,
+                                          5 coefficient classes)               */
   uint64_t reserved[3];
 } tf_info;
 

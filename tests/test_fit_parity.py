@@ -104,12 +104,12 @@ def test_chunked_stepping_matches_single_call(tmp_path, product_lib):
     assert np.array_equal(U1, U2) and np.array_equal(F1, F2)
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6])
 def test_every_kernel_variant_is_bitwise_identical(tmp_path, product_lib, oracle_lib, variant):
     """The E/H kernel variants the autotuner chooses between (one thread per
     node, z-march over 4 or 16 planes, per-dof coefficient arrays, z-march
-    with TMA-staged planes) give the same FP64 state bit for bit, on a lossy
-    multi-material scene."""
+    with TMA-staged planes, coefficient classes) give the same FP64 state bit
+    for bit, on a lossy multi-material scene."""
     case = FitCase(n=14, steps=50, spheres=random_spheres(5, seed=9))
     script = write_fit_cavity(str(tmp_path), case)
     o = oracle.FitOracle(script)
@@ -119,7 +119,7 @@ def test_every_kernel_variant_is_bitwise_identical(tmp_path, product_lib, oracle
         info = d.prepare(1, precision="fp64", fit_variant=variant)
         d.step(50)
         U, _, F = d.state()
-        assert d.info()["cg_variant"] == (variant - 1) * 6
+        assert d.info()["cg_variant"] == (variant - 1) * 9
     assert np.array_equal(U, Uo) and np.array_equal(F, Fo)
 
 

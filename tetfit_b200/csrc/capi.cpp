@@ -362,7 +362,7 @@ int tf_prepare(tf_ctx* c, uint32_t label, const tf_opts* opts) {
     if (c->opts.learn_steps > 0) ro.learn_steps = c->opts.learn_steps;
     ro.fit_variant = c->opts.fit_variant;
     ro.setup_threads = c->opts.host_threads > 0 ? c->opts.host_threads : 0;
-    if (ro.fit_variant < 0 || ro.fit_variant > 5) return fail(c, TF_E_ARG, "fit_variant must be 0..5");
+    if (ro.fit_variant < 0 || ro.fit_variant > 6) return fail(c, TF_E_ARG, "fit_variant must be 0..6");
     if (c->opts.file_digits < 0 || c->opts.file_digits > 17) return fail(c, TF_E_ARG, "file_digits must be 0..17");
     if (meth == "fdtd") {
       c->fit.reset(new tf::FitSim(c->sc, label, ro));

@@ -813,7 +813,11 @@ void FitSim::fill_grid(FitGrid<T>& g, SpecialEdges<T>& s) {
     g.Cq[a] = (T*)dC_[3 + a];
     g.Cn[a] = (T*)dC_[6 + a];
     g.Cm[a] = (T*)dC_[9 + a];
+    g.Ke[a] = dK_[a];
+    g.Kf[a] = dK_[3 + a];
   }
+  g.lut_e = cls_ok_ ? (T*)dlut_[0] : nullptr;
+  g.lut_f = cls_ok_ ? (T*)dlut_[1] : nullptr;
   for (int a = 0; a < 3; a++) g.len[a] = L_[a];
   g.area[0] = L_[1] * L_[2]; g.area[1] = L_[0] * L_[2]; g.area[2] = L_[0] * L_[1];
   s.n = (int)special_.size();
@@ -862,6 +866,14 @@ void FitSim::alloc_device() {
       dC_[q] = dalloc(nslot_ * es);
       CU(cudaMemsetAsync(dC_[q], 0, nslot_ * es, stream_));
     }
+  if (opt_.fit_variant == 6 || (opt_.fit_variant == 0 && n_cells() >= 2000000)) {
+    // the coefficient-class variant is forced or among the autotuner's candidates
+    for (int q = 0; q < 6; q++) {
+      dK_[q] = (uint16_t*)dalloc(nslot_ * sizeof(uint16_t));
+      CU(cudaMemsetAsync(dK_[q], 0, nslot_ * sizeof(uint16_t), stream_));
+    }
+    for (int q = 0; q < 2; q++) dlut_[q] = dalloc((size_t)2 * kMaxClasses * es);
+  }
   dflux_ = (double*)dalloc(nsteps_ * 8);
   // Joule losses (Discretization.hpp:1902): the reference's Si is non-zero
   // only for l2norm outputs (:5368, :5594-5597) and conducting materials
@@ -1105,20 +1117,50 @@ void FitSim::upload() {
   CU(cudaStreamSynchronize(stream_));
 }
 
-// Per-dof coefficients for the coefficient-array kernel variant, from the
-// same tables and functions as the table-driven kernels (bit-identical).
+// Per-dof coefficients for the coefficient-array kernel variant, and the
+// coefficient classes of the class variant, from the same tables and
+// functions as the table-driven kernels (bit-identical).
 void FitSim::build_coefficients() {
-  if (!dC_[0]) return;
+  if (dC_[0]) {
+    if (opt_.precision == 1) {
+      FitGrid<float> g; SpecialEdges<float> s;
+      fill_grid(g, s);
+      CU(fit_build_coefficients<float>(g, stream_));
+    } else {
+      FitGrid<double> g; SpecialEdges<double> s;
+      fill_grid(g, s);
+      CU(fit_build_coefficients<double>(g, stream_));
+    }
+    CU(cudaStreamSynchronize(stream_));
+  }
+  if (!dK_[0]) return;
+  // hash tables of the build: set-up only, released before stepping
+  FitClassWork w{};
+  void* work = nullptr;
+  const size_t kb = sizeof(unsigned long long) * kClassTable, ib = sizeof(int) * kClassTable;
+  CU(cudaMalloc(&work, 2 * (kb + ib) + 4 * sizeof(int)));
+  char* p = (char*)work;
+  w.keys[0] = (unsigned long long*)p; w.keys[1] = (unsigned long long*)(p + kb);
+  w.ids[0] = (int*)(p + 2 * kb); w.ids[1] = (int*)(p + 2 * kb + ib);
+  w.count = (int*)(p + 2 * (kb + ib));
+  int ncls[2] = {-1, -1};
+  cudaError_t e;
+  cls_ok_ = true;  // fill_grid hands the tables to the build
   if (opt_.precision == 1) {
     FitGrid<float> g; SpecialEdges<float> s;
     fill_grid(g, s);
-    CU(fit_build_coefficients<float>(g, stream_));
+    e = fit_build_classes<float>(g, w, ncls, stream_);
   } else {
     FitGrid<double> g; SpecialEdges<double> s;
     fill_grid(g, s);
-    CU(fit_build_coefficients<double>(g, stream_));
+    e = fit_build_classes<double>(g, w, ncls, stream_);
   }
-  CU(cudaStreamSynchronize(stream_));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  cudaFree(work);
+  CU(e);
+  cls_ok_ = ncls[0] >= 0 && ncls[1] >= 0;
+  ncls_[0] = ncls[0];
+  ncls_[1] = ncls[1];
 }
 
 void FitSim::launch_steps(int n, cudaEvent_t* ev) {
@@ -1150,15 +1192,19 @@ void FitSim::launch_steps(int n, cudaEvent_t* ev) {
 void FitSim::autotune(uint64_t& n) {
   if (opt_.fit_variant > 0) {
     e_var_ = h_var_ = opt_.fit_variant - 1;
+    // a forced variant whose tensor maps or class tables could not be made
+    // runs as the 16-plane z-march, and says so
+    if ((e_var_ == 4 && !tma_ok_) || (e_var_ == 5 && !cls_ok_)) e_var_ = h_var_ = 2;
     tuned_ = true;
     return;
   }
   if (tuned_ || n_cells() < 2000000) { tuned_ = true; return; }
   // candidates: node slot, 4- and 16-plane z-march, per-dof coefficients
-  // (when allocated), TMA z-march (when the tensor maps exist)
-  int cand[5], kVariants = 0;
-  for (int v = 0; v < 5; v++)
-    if ((v != 3 || dC_[0]) && (v != 4 || tma_ok_)) cand[kVariants++] = v;
+  // (when allocated), TMA z-march (when the tensor maps exist), coefficient
+  // classes (when the tables were built)
+  int cand[6], kVariants = 0;
+  for (int v = 0; v < 6; v++)
+    if ((v != 3 || dC_[0]) && (v != 4 || tma_ok_) && (v != 5 || cls_ok_)) cand[kVariants++] = v;
   const int kReps = 2;
   cudaEvent_t ev[6];
   for (auto& e : ev) CU(cudaEventCreate(&e));

@@ -151,15 +151,19 @@ class FitSim : public Sim {
   int e_var_ = 2, h_var_ = 2; // kernel variants (see fit_launch_step)
   bool tuned_ = false;
   int tune_pos_ = 0;
-  double tune_e_[5] = {0, 0, 0, 0, 0}, tune_h_[5] = {0, 0, 0, 0, 0};
+  double tune_e_[6] = {0, 0, 0, 0, 0, 0}, tune_h_[6] = {0, 0, 0, 0, 0, 0};
   FitTmaMaps tma_{};
   bool tma_ok_ = false;
   int* dtma_err_ = nullptr;
   void* dC_[12] = {};  // per-dof coefficients M_h, M_q, M_nu, M_mu x 3 axes (autotuned grids)
+  uint16_t* dK_[6] = {};  // coefficient classes of the x, y, z edges, then faces
+  void* dlut_[2] = {};    // class tables (edges, faces)
+  bool cls_ok_ = false;
+  int ncls_[2] = {0, 0};  // edge and face classes (-1: more than the tables hold)
   void build_coefficients();
 
  public:
-  int kernel_variant() const override { return e_var_ + 5 * h_var_; }
+  int kernel_variant() const override { return e_var_ + 8 * h_var_; }
 
  private:
   // graphs

@@ -428,9 +428,11 @@ TF_UNROLL(TF_FIT_UNROLL)
 // ---------------------------------------------------------------- TMA z-march
 // The same E and H updates with the face (E) or edge (H) planes a tile of
 // 32 x 8 node columns needs staged in shared memory by the tensor memory
-// accelerator: one elected thread keeps kTmaStages planes in flight
-// (cp.async.bulk.tensor into a ring of buffers, an mbarrier per buffer with
-// the expected byte count), the other threads compute from shared memory.
+// accelerator: the elected thread of a ninth (producer) warp keeps
+// kTmaStages planes in flight (cp.async.bulk.tensor into a ring of buffers,
+// a "full" mbarrier per buffer with the expected byte count, an "empty"
+// mbarrier the eight consumer warps release it on), the consumer warps
+// compute from shared memory.
 // A box covers the tile plus its one-node halo (E: the x-1 / y-1 side, H:
 // the x+1 / y+1 side), its x extent rounded to 16 bytes; the E box starts
 // 16 bytes left of the tile so that every x coordinate stays 16-byte aligned.
@@ -438,6 +440,10 @@ TF_UNROLL(TF_FIT_UNROLL)
 // Nz+1) read as zero and are never used unguarded.  One-GPU code: the tensor
 // maps cover this GPU's arrays only, no multicast.
 constexpr int kTmaTX = 32, kTmaTY = 8;
+// resident blocks per SM the TMA kernels are compiled for (4: no register cap)
+#ifndef TF_TMA_MINB
+#define TF_TMA_MINB 4
+#endif
 // planes in flight: four (FP32) or three (FP64), within 48 KB of static shared memory
 template <typename T>
 __host__ __device__ constexpr int tma_stages() { return sizeof(T) == 4 ? 4 : 3; }
@@ -473,59 +479,78 @@ struct TmaRing {
   static constexpr int kPlane = BX * BY;                    // elements per array and plane
   static constexpr uint32_t kBytes = 6u * kPlane * sizeof(T);  // bytes a plane's six boxes bring
   alignas(128) T buf[kTmaStages][6][kPlane + (128 / sizeof(T) - kPlane % (128 / sizeof(T))) % (128 / sizeof(T))];
-  alignas(8) uint64_t bar[kTmaStages];
+  alignas(8) uint64_t full[kTmaStages];   // plane arrived: the producer's expect_tx and the copies' bytes
+  alignas(8) uint64_t empty[kTmaStages];  // plane consumed: one arrival per consumer warp
 };
 
-// Ring control, run by every thread of the block: issue(q) loads plane q of
-// the march (global plane base + q) into buffer q % kTmaStages; wait(q)
-// blocks until it has arrived.  A wait that runs out of polls raises *err
-// and reports failure; the caller then stops computing, drains the copies
-// still in flight (bounded again) and returns.
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// bounded wait for the completion of the phase with this parity
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (long it = 0; !mbar_try_wait(bar, parity); it++)
+    if (it > kTmaWaitLimit) return false;
+  return true;
+}
+
+// Ring control with a producer warp and kTmaTY consumer warps, no block-wide
+// barrier per plane.  The producer's elected thread runs produce(): plane q
+// of the march (global plane zbase + q) goes into buffer q % kTmaStages as
+// soon as every consumer warp has released the plane that buffer held.  A
+// consumer warp wait()s for a plane and release()s it when it no longer
+// reads it, so consumer warps drift apart by up to kTmaStages planes.  Every
+// wait is bounded: one that runs out raises *err; the consumers then return,
+// the producer stops issuing and waits (bounded) for the copies it still has
+// in flight, so no copy lands in the shared memory of an exited block.
 template <typename T, int BX, int BY, int kTmaStages = tma_stages<T>()>
 struct TmaMarch {
   TmaRing<T, BX, BY>& r;
   const CUtensorMap* m[6];  // the three staged-neighbour arrays, then the three updated ones
   int x, y, zbase, nplanes;
   int* err;
-  __device__ void issue(int q) const {
-    const int st = q % kTmaStages;
-    mbar_expect_tx(&r.bar[st], TmaRing<T, BX, BY>::kBytes);
-#pragma unroll
-    for (int a = 0; a < 6; a++) tma_load_3d(r.buf[st][a], m[a], &r.bar[st], x, y, zbase + q);
-  }
-  __device__ bool wait(int q) const {
-    const uint32_t parity = (uint32_t)((q / kTmaStages) & 1);
-    for (long it = 0; !mbar_try_wait(&r.bar[q % kTmaStages], parity); it++)
-      if (it > kTmaWaitLimit) {
-        atomicExch(err, 1);
-        return false;
-      }
-    return true;
-  }
-  // wait (bounded) for the planes [from, issued) still in flight
-  __device__ void drain(int from, int issued) const {
-    for (int q = from; q < issued; q++) {
-      const uint32_t parity = (uint32_t)((q / kTmaStages) & 1);
-      for (long it = 0; it <= kTmaWaitLimit && !mbar_try_wait(&r.bar[q % kTmaStages], parity); it++) {
-      }
+  // one thread, followed by a __syncthreads of the block
+  __device__ void init(int consumers) const {
+    for (int q = 0; q < kTmaStages; q++) {
+      mbar_init(&r.full[q], 1);
+      mbar_init(&r.empty[q], consumers);
     }
-  }
-};
-
-template <typename T, int BX, int BY>
-__device__ __forceinline__ void tma_ring_init(TmaRing<T, BX, BY>& r) {
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
-    for (int q = 0; q < tma_stages<T>(); q++) mbar_init(&r.bar[q], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  __syncthreads();
-}
+  __device__ void produce() const {
+    int issued = 0;
+    for (int q = 0; q < nplanes; q++) {
+      const int st = q % kTmaStages;
+      if (q >= kTmaStages && !mbar_wait(&r.empty[st], (uint32_t)((q / kTmaStages - 1) & 1))) {
+        atomicExch(err, 1);
+        break;
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_expect_tx(&r.full[st], TmaRing<T, BX, BY>::kBytes);
+#pragma unroll
+      for (int a = 0; a < 6; a++) tma_load_3d(r.buf[st][a], m[a], &r.full[st], x, y, zbase + q);
+      issued = q + 1;
+    }
+    // the last kTmaStages planes issued are the only ones that can still be
+    // in flight (each earlier one was released, so it had arrived)
+    for (int q = issued > kTmaStages ? issued - kTmaStages : 0; q < issued; q++)
+      mbar_wait(&r.full[q % kTmaStages], (uint32_t)((q / kTmaStages) & 1));
+  }
+  __device__ bool wait(int q) const {
+    if (mbar_wait(&r.full[q % kTmaStages], (uint32_t)((q / kTmaStages) & 1))) return true;
+    atomicExch(err, 1);
+    return false;
+  }
+  __device__ void release(int q) const {
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) mbar_arrive(&r.empty[q % kTmaStages]);
+  }
+};
 
 // H update, TMA form of fit_h_march: the boxes of plane q hold (i0 .. i0+BX-1)
 // x (j0 .. j0+kTmaTY) of Ux, Uy, Uz and of the updated Fx, Fy, Fz; plane k
 // uses the U of planes k and k+1 and the F of plane k.
 template <typename T>
-__global__ void __launch_bounds__(kTmaTX * kTmaTY) fit_h_tma(FitGrid<T> g, int kchunk, int* step_counter,
+__global__ void __launch_bounds__(kTmaTX * (kTmaTY + 1), TF_TMA_MINB) fit_h_tma(FitGrid<T> g, int kchunk, int* step_counter,
                                                             const __grid_constant__ CUtensorMap mUx,
                                                             const __grid_constant__ CUtensorMap mUy,
                                                             const __grid_constant__ CUtensorMap mUz,
@@ -542,11 +567,13 @@ __global__ void __launch_bounds__(kTmaTX * kTmaTY) fit_h_tma(FitGrid<T> g, int k
   if (step_counter && i == 0 && j == 0 && k0 == 0) atomicAdd(step_counter, 1);
   const int k1 = min(k0 + kchunk, g.Nz + 1);
   const int nplanes = k1 - k0 + 1;  // planes k0 .. k1
-  tma_ring_init(ring);
   const TmaMarch<T, BX, BY> mr{ring, {&mUx, &mUy, &mUz, &mFx, &mFy, &mFz}, i0, j0, k0, nplanes, err};
-  const bool lead = tx == 0 && ty == 0;
-  if (lead)
-    for (int q = 0; q < min(kTmaStages, nplanes); q++) mr.issue(q);
+  if (tx == 0 && ty == 0) mr.init(kTmaTY);
+  __syncthreads();
+  if (ty == kTmaTY) {  // the producer warp
+    if (tx == 0) mr.produce();
+    return;
+  }
   const bool valid = i <= g.Nx && j <= g.Ny;
   const T dt = (T)g.dt;
   const bool ci = i < g.Nx, cj = j < g.Ny;
@@ -559,16 +586,10 @@ __global__ void __launch_bounds__(kTmaTX * kTmaTY) fit_h_tma(FitGrid<T> g, int k
   const int64_t cc = (int64_t)i + (int64_t)g.Nx * j;
   uint8_t m_lo = (valid && ci && cj && k0 > 0) ? __ldg(mat + cc + cplane * (k0 - 1)) : 0;
   const int o = ty * BX + tx;  // this node in a box
-  int issued = min(kTmaStages, nplanes), failed = -1;
-  bool ok = __syncthreads_and(mr.wait(0));
-  if (!ok) failed = 0;
-  for (int k = k0; ok && k < k1; k++, s += g.sxy) {
+  if (!mr.wait(0)) return;
+  for (int k = k0; k < k1; k++, s += g.sxy) {
     const int q = k - k0;
-    ok = __syncthreads_and(mr.wait(q + 1));  // every thread leaves together
-    if (!ok) {
-      failed = q + 1;
-      break;
-    }
+    if (!mr.wait(q + 1)) return;
     const T* Ux = ring.buf[q % kTmaStages][0];
     const T* Uy = ring.buf[q % kTmaStages][1];
     const T* Uz = ring.buf[q % kTmaStages][2];
@@ -605,16 +626,8 @@ __global__ void __launch_bounds__(kTmaTX * kTmaTY) fit_h_tma(FitGrid<T> g, int k
       }
       m_lo = m0;
     }
-    __syncthreads();  // plane q's buffer is free again
-    if (q + kTmaStages < nplanes) {
-      if (lead) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mr.issue(q + kTmaStages);
-      }
-      issued = q + kTmaStages + 1;
-    }
+    mr.release(q);  // plane q is not read again
   }
-  if (!ok && lead) mr.drain(failed, issued);
 }
 
 // E update, TMA form of fit_e_march: the boxes of plane q hold
@@ -622,7 +635,7 @@ __global__ void __launch_bounds__(kTmaTX * kTmaTY) fit_h_tma(FitGrid<T> g, int k
 // updated Ux, Uy, Uz, H = 16 bytes of elements; plane k uses the F of planes
 // k-1 and k and the U of plane k.
 template <typename T>
-__global__ void __launch_bounds__(kTmaTX * kTmaTY) fit_e_tma(FitGrid<T> g, int kchunk,
+__global__ void __launch_bounds__(kTmaTX * (kTmaTY + 1), TF_TMA_MINB) fit_e_tma(FitGrid<T> g, int kchunk,
                                                             const __grid_constant__ CUtensorMap mFx,
                                                             const __grid_constant__ CUtensorMap mFy,
                                                             const __grid_constant__ CUtensorMap mFz,
@@ -639,11 +652,13 @@ __global__ void __launch_bounds__(kTmaTX * kTmaTY) fit_e_tma(FitGrid<T> g, int k
   const int i = i0 + tx, j = j0 + ty;
   const int k1 = min(k0 + kchunk, g.Nz + 1);
   const int nplanes = k1 - k0 + 1;  // planes k0-1 .. k1-1
-  tma_ring_init(ring);
   const TmaMarch<T, BX, BY> mr{ring, {&mFx, &mFy, &mFz, &mUx, &mUy, &mUz}, i0 - H, j0 - 1, k0 - 1, nplanes, err};
-  const bool lead = tx == 0 && ty == 0;
-  if (lead)
-    for (int q = 0; q < min(kTmaStages, nplanes); q++) mr.issue(q);
+  if (tx == 0 && ty == 0) mr.init(kTmaTY);
+  __syncthreads();
+  if (ty == kTmaTY) {  // the producer warp
+    if (tx == 0) mr.produce();
+    return;
+  }
   const bool valid = i <= g.Nx && j <= g.Ny;
   const T dt = (T)g.dt;
   T* __restrict__ Ux = g.Ux;
@@ -665,16 +680,10 @@ __global__ void __launch_bounds__(kTmaTX * kTmaTY) fit_e_tma(FitGrid<T> g, int k
     lo[1][1] = (ci1 && cj1) ? __ldg(m + g.Nx + 1) : 0;
   }
   const int o = (ty + 1) * BX + tx + H;  // this node in a box
-  int issued = min(kTmaStages, nplanes), failed = -1;
-  bool ok = __syncthreads_and(mr.wait(0));
-  if (!ok) failed = 0;
-  for (int k = k0; ok && k < k1; k++, s += g.sxy) {
+  if (!mr.wait(0)) return;
+  for (int k = k0; k < k1; k++, s += g.sxy) {
     const int q = k - k0;  // plane k-1 is ring plane q, plane k is q + 1
-    ok = __syncthreads_and(mr.wait(q + 1));
-    if (!ok) {
-      failed = q + 1;
-      break;
-    }
+    if (!mr.wait(q + 1)) return;
     const T* Fxl = ring.buf[q % kTmaStages][0];
     const T* Fyl = ring.buf[q % kTmaStages][1];
     const T* Fx = ring.buf[(q + 1) % kTmaStages][0];
@@ -729,16 +738,8 @@ __global__ void __launch_bounds__(kTmaTX * kTmaTY) fit_e_tma(FitGrid<T> g, int k
       }
       lo[0][0] = hi[0][0]; lo[0][1] = hi[0][1]; lo[1][0] = hi[1][0]; lo[1][1] = hi[1][1];
     }
-    __syncthreads();
-    if (q + kTmaStages < nplanes) {
-      if (lead) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mr.issue(q + kTmaStages);
-      }
-      issued = q + kTmaStages + 1;
-    }
+    mr.release(q);
   }
-  if (!ok && lead) mr.drain(failed, issued);
 }
 
 template <typename T>
@@ -947,6 +948,168 @@ cudaError_t fit_build_coefficients(const FitGrid<T>& g, cudaStream_t st) {
 template cudaError_t fit_build_coefficients<double>(const FitGrid<double>&, cudaStream_t);
 template cudaError_t fit_build_coefficients<float>(const FitGrid<float>&, cudaStream_t);
 
+// ------------------------------------------------------------ coefficient classes
+// An edge's coefficients are a function of its axis and the materials of its
+// four cells (cells outside the grid read as material 0, as above), a face's
+// of its axis, which of its two cells exist, and their materials.  The build
+// packs each updated dof's tuple into a 64-bit key, inserts the keys into an
+// open-addressing hash table (linear probing; MurmurHash3's 64-bit finalizer
+// as the hash), numbers the occupied slots, computes one coefficient pair per
+// class with edge_coef_t / face_coef_t, and writes each dof's class.  Class
+// numbers depend on insertion order; the coefficients a dof reads do not.
+constexpr unsigned long long kNoKey = ~0ull;
+
+__device__ __forceinline__ uint32_t class_hash(unsigned long long k) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdull;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ull;
+  k ^= k >> 33;
+  return (uint32_t)k & (kClassTable - 1);
+}
+
+__device__ __forceinline__ int class_insert(unsigned long long* keys, unsigned long long k) {
+  uint32_t h = class_hash(k);
+  for (int p = 0; p < kClassTable; p++, h = (h + 1) & (kClassTable - 1)) {
+    const unsigned long long cur = *(volatile unsigned long long*)&keys[h];
+    if (cur == k) return (int)h;
+    if (cur == kNoKey) {
+      const unsigned long long prev = atomicCAS(&keys[h], kNoKey, k);
+      if (prev == kNoKey || prev == k) return (int)h;
+    }
+  }
+  return -1;
+}
+
+__device__ __forceinline__ int class_find(const unsigned long long* keys, unsigned long long k) {
+  uint32_t h = class_hash(k);
+  for (int p = 0; p < kClassTable; p++, h = (h + 1) & (kClassTable - 1)) {
+    const unsigned long long cur = keys[h];
+    if (cur == k) return (int)h;
+    if (cur == kNoKey) return -1;
+  }
+  return -1;
+}
+
+__device__ __forceinline__ unsigned long long edge_key(int a, const uint8_t m[4]) {
+  return ((unsigned long long)a << 32) | (uint32_t)m[0] | ((uint32_t)m[1] << 8) | ((uint32_t)m[2] << 16) |
+         ((uint32_t)m[3] << 24);
+}
+__device__ __forceinline__ unsigned long long face_key(int a, bool has_lo, bool has_hi, uint8_t mlo, uint8_t mhi) {
+  return ((unsigned long long)a << 32) | (uint32_t)has_lo | ((uint32_t)has_hi << 1) | ((uint32_t)mlo << 8) |
+         ((uint32_t)mhi << 16);
+}
+
+// The tuples of the dofs at node slot (i, j, k), in the order and under the
+// conditions fit_coef_kernel uses; f(kind, axis, key, slot) per updated dof,
+// kind 0 edge, 1 face.
+template <typename T, typename F>
+__device__ __forceinline__ void for_each_dof_key(const FitGrid<T>& g, int i, int j, int k, F f) {
+  const int64_t s = (int64_t)i + g.sx * j + g.sxy * k;
+  const bool xin = i > 0 && i < g.Nx, yin = j > 0 && j < g.Ny, zin = k > 0 && k < g.Nz;
+  uint8_t c[2][2][2];
+#pragma unroll
+  for (int dz = 0; dz < 2; dz++)
+#pragma unroll
+    for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+      for (int dx = 0; dx < 2; dx++) {
+        const int ci = i - 1 + dx, cj = j - 1 + dy, ck = k - 1 + dz;
+        const bool ok = ci >= 0 && ci < g.Nx && cj >= 0 && cj < g.Ny && ck >= 0 && ck < g.Nz;
+        c[dz][dy][dx] = ok ? g.mat[cell_index(ci, cj, ck, g.Nx, g.Ny)] : 0;
+      }
+  if (i < g.Nx && yin && zin) {
+    const uint8_t m[4] = {c[0][0][1], c[0][1][1], c[1][0][1], c[1][1][1]};
+    f(0, 0, edge_key(0, m), s);
+  }
+  if (j < g.Ny && xin && zin) {
+    const uint8_t m[4] = {c[0][1][0], c[0][1][1], c[1][1][0], c[1][1][1]};
+    f(0, 1, edge_key(1, m), s);
+  }
+  if (k < g.Nz && xin && yin) {
+    const uint8_t m[4] = {c[1][0][0], c[1][0][1], c[1][1][0], c[1][1][1]};
+    f(0, 2, edge_key(2, m), s);
+  }
+  const bool ci = i < g.Nx, cj = j < g.Ny, ck = k < g.Nz;
+  const uint8_t m0 = (ci && cj && ck) ? c[1][1][1] : 0;
+  if (cj && ck) f(1, 0, face_key(0, i > 0, ci, i > 0 ? c[1][1][0] : 0, m0), s);
+  if (ci && ck) f(1, 1, face_key(1, j > 0, cj, j > 0 ? c[1][0][1] : 0, m0), s);
+  if (ci && cj) f(1, 2, face_key(2, k > 0, ck, k > 0 ? c[0][1][1] : 0, m0), s);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) fit_class_insert(FitGrid<T> g, FitClassWork w) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i > g.Nx || j > g.Ny) return;
+  for_each_dof_key(g, i, j, k, [&](int kind, int, unsigned long long key, int64_t) {
+    if (class_insert(w.keys[kind], key) < 0) atomicExch(&w.count[2], 1);
+  });
+}
+
+// One thread per table slot: number the occupied slots and fill the tables.
+template <typename T>
+__global__ void __launch_bounds__(256) fit_class_number(FitGrid<T> g, FitClassWork w, int kind) {
+  const int h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= kClassTable) return;
+  const unsigned long long key = w.keys[kind][h];
+  if (key == kNoKey) return;
+  const int id = atomicAdd(&w.count[kind], 1);
+  w.ids[kind][h] = id;
+  if (id >= kMaxClasses) return;
+  const int a = (int)(key >> 32);
+  if (kind == 0) {
+    const uint8_t m[4] = {(uint8_t)key, (uint8_t)(key >> 8), (uint8_t)(key >> 16), (uint8_t)(key >> 24)};
+    T mh, mq;
+    edge_coef_t(g, a, m, mh, mq);
+    g.lut_e[2 * id] = mh;
+    g.lut_e[2 * id + 1] = mq;
+  } else {
+    T mnu, mmu;
+    const bool live = face_coef_t(g, a, (key & 1) != 0, (key & 2) != 0, (uint8_t)(key >> 8), (uint8_t)(key >> 16),
+                                  mnu, mmu);
+    g.lut_f[2 * id] = live ? mnu : (T)-0.0;
+    g.lut_f[2 * id + 1] = live ? mmu : (T)0;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) fit_class_assign(FitGrid<T> g, FitClassWork w) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i > g.Nx || j > g.Ny) return;
+  for_each_dof_key(g, i, j, k, [&](int kind, int a, unsigned long long key, int64_t s) {
+    const int h = class_find(w.keys[kind], key);
+    const uint16_t c = (uint16_t)(h >= 0 ? w.ids[kind][h] : 0);
+    if (kind == 0) g.Ke[a][s] = c;
+    else g.Kf[a][s] = c;
+  });
+}
+
+template <typename T>
+cudaError_t fit_build_classes(const FitGrid<T>& g, const FitClassWork& w, int ncls[2], cudaStream_t st) {
+  for (int q = 0; q < 2; q++)
+    if (cudaMemsetAsync(w.keys[q], 0xff, sizeof(unsigned long long) * kClassTable, st) != cudaSuccess)
+      return cudaGetLastError();
+  if (cudaMemsetAsync(w.count, 0, 3 * sizeof(int), st) != cudaSuccess) return cudaGetLastError();
+  dim3 blk(32, 8, 1);
+  dim3 grd((unsigned)((g.Nx + 1 + 31) / 32), (unsigned)((g.Ny + 1 + 7) / 8), (unsigned)(g.Nz + 1));
+  fit_class_insert<T><<<grd, blk, 0, st>>>(g, w);
+  for (int q = 0; q < 2; q++) fit_class_number<T><<<kClassTable / 256, 256, 0, st>>>(g, w, q);
+  int c[3] = {0, 0, 0};
+  cudaMemcpyAsync(c, w.count, sizeof(c), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return e;
+  for (int q = 0; q < 2; q++) ncls[q] = (c[2] || c[q] > kMaxClasses) ? -1 : c[q];
+  if (ncls[0] < 0 || ncls[1] < 0) return cudaSuccess;
+  fit_class_assign<T><<<grd, blk, 0, st>>>(g, w);
+  return cudaGetLastError();
+}
+template cudaError_t fit_build_classes<double>(const FitGrid<double>&, const FitClassWork&, int*, cudaStream_t);
+template cudaError_t fit_build_classes<float>(const FitGrid<float>&, const FitClassWork&, int*, cudaStream_t);
+
 // Interior E update from the per-dof coefficients (same arithmetic as
 // fit_e_kernel, coefficients streamed instead of rebuilt).
 template <typename T>
@@ -1007,6 +1170,79 @@ __global__ void __launch_bounds__(256) fit_h_coef(FitGrid<T> g, int* step_counte
     const T mnu = __ldg(g.Cn[2] + s);
     if (!skip(mnu)) {
       const T B = face_flux(__ldg(g.Cm[2] + s), g.Fz[s], dt, curl_z(g, s));
+      g.Fz[s] = A::mul(mnu, B);
+    }
+  }
+}
+
+// E and H updates with the coefficients looked up by class (same arithmetic
+// as fit_e_kernel / fit_h_kernel): per dof a 2-byte class instead of the
+// coefficient rebuild or two streamed coefficients.
+template <typename T>
+__global__ void __launch_bounds__(256) fit_e_class(FitGrid<T> g) {
+  using A = Ar<T>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i > g.Nx || j > g.Ny) return;
+  const int64_t s = (int64_t)i + g.sx * j + g.sxy * k;
+  const T dt = (T)g.dt;
+  const T* __restrict__ lut = g.lut_e;
+  const bool xin = i > 0 && i < g.Nx, yin = j > 0 && j < g.Ny, zin = k > 0 && k < g.Nz;
+  if (i < g.Nx && yin && zin) {
+    const int c = __ldg(g.Ke[0] + s);
+    const T mh = __ldg(lut + 2 * c), mq = __ldg(lut + 2 * c + 1);
+    T cf = A::sub(A::add(A::sub(g.Fy[s - g.sxy], g.Fz[s - g.sx]), g.Fz[s]), g.Fy[s]);
+    g.Ux[s] = A::mul(mh, A::add(A::mul(mq, g.Ux[s]), A::mul(dt, cf)));
+  }
+  if (j < g.Ny && xin && zin) {
+    const int c = __ldg(g.Ke[1] + s);
+    const T mh = __ldg(lut + 2 * c), mq = __ldg(lut + 2 * c + 1);
+    T cf = -A::sub(A::add(A::sub(g.Fx[s - g.sxy], g.Fz[s - 1]), g.Fz[s]), g.Fx[s]);
+    g.Uy[s] = A::mul(mh, A::add(A::mul(mq, g.Uy[s]), A::mul(dt, cf)));
+  }
+  if (k < g.Nz && xin && yin) {
+    const int c = __ldg(g.Ke[2] + s);
+    const T mh = __ldg(lut + 2 * c), mq = __ldg(lut + 2 * c + 1);
+    T cf = A::sub(A::add(A::sub(g.Fx[s - g.sx], g.Fy[s - 1]), g.Fy[s]), g.Fx[s]);
+    g.Uz[s] = A::mul(mh, A::add(A::mul(mq, g.Uz[s]), A::mul(dt, cf)));
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) fit_h_class(FitGrid<T> g, int* step_counter) {
+  using A = Ar<T>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (step_counter && i == 0 && j == 0 && k == 0) atomicAdd(step_counter, 1);
+  if (i > g.Nx || j > g.Ny) return;
+  const int64_t s = (int64_t)i + g.sx * j + g.sxy * k;
+  const T dt = (T)g.dt;
+  const T* __restrict__ lut = g.lut_f;
+  const bool ci = i < g.Nx, cj = j < g.Ny, ck = k < g.Nz;
+  auto skip = [](T v) { return v == (T)0 && signbit(v); };
+  if (cj && ck) {
+    const int c = __ldg(g.Kf[0] + s);
+    const T mnu = __ldg(lut + 2 * c);
+    if (!skip(mnu)) {
+      const T B = face_flux(__ldg(lut + 2 * c + 1), g.Fx[s], dt, curl_x(g, s));
+      g.Fx[s] = A::mul(mnu, B);
+    }
+  }
+  if (ci && ck) {
+    const int c = __ldg(g.Kf[1] + s);
+    const T mnu = __ldg(lut + 2 * c);
+    if (!skip(mnu)) {
+      const T B = face_flux(__ldg(lut + 2 * c + 1), g.Fy[s], -dt, curl_y(g, s));
+      g.Fy[s] = A::mul(mnu, B);
+    }
+  }
+  if (ci && cj) {
+    const int c = __ldg(g.Kf[2] + s);
+    const T mnu = __ldg(lut + 2 * c);
+    if (!skip(mnu)) {
+      const T B = face_flux(__ldg(lut + 2 * c + 1), g.Fz[s], dt, curl_z(g, s));
       g.Fz[s] = A::mul(mnu, B);
     }
   }
@@ -1102,11 +1338,12 @@ void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const Probe
   if (ev) cudaEventRecord(ev[1], st);
   if (e_variant == 0) fit_e_kernel<T><<<grd, blk, 0, st>>>(g);
   else if (e_variant == 3) fit_e_coef<T><<<grd, blk, 0, st>>>(g);
+  else if (e_variant == 5 && g.lut_e) fit_e_class<T><<<grd, blk, 0, st>>>(g);
   else if (e_variant == 4 && tma)
-    fit_e_tma<T><<<mgrid(16), blk, 0, st>>>(g, 16, tma->F[0], tma->F[1], tma->F[2], tma->U[0], tma->U[1], tma->U[2],
+    fit_e_tma<T><<<mgrid(16), dim3(kTmaTX, kTmaTY + 1), 0, st>>>(g, 16, tma->F[0], tma->F[1], tma->F[2], tma->U[0], tma->U[1], tma->U[2],
                                              tma->err);
   else {
-    const int kc = e_variant == 1 ? 4 : 16;  // variants 1, 2 (and 4 without tensor maps)
+    const int kc = e_variant == 1 ? 4 : 16;  // variants 1, 2 (and 4, 5 without their tensor maps or tables)
     fit_e_march<T><<<mgrid(kc), blk, 0, st>>>(g, kc);
   }
   if (ev) cudaEventRecord(ev[2], st);
@@ -1120,8 +1357,9 @@ void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const Probe
   if (ev) cudaEventRecord(ev[4], st);
   if (h_variant == 0) fit_h_kernel<T><<<grd, blk, 0, st>>>(g, step_counter);
   else if (h_variant == 3) fit_h_coef<T><<<grd, blk, 0, st>>>(g, step_counter);
+  else if (h_variant == 5 && g.lut_f) fit_h_class<T><<<grd, blk, 0, st>>>(g, step_counter);
   else if (h_variant == 4 && tma)
-    fit_h_tma<T><<<mgrid(16), blk, 0, st>>>(g, 16, step_counter, tma->U[0], tma->U[1], tma->U[2], tma->F[0],
+    fit_h_tma<T><<<mgrid(16), dim3(kTmaTX, kTmaTY + 1), 0, st>>>(g, 16, step_counter, tma->U[0], tma->U[1], tma->U[2], tma->F[0],
                                              tma->F[1], tma->F[2], tma->err);
   else {
     const int kc = h_variant == 1 ? 4 : 16;

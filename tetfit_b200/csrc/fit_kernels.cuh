@@ -44,6 +44,23 @@ struct FitGrid {
   // computed once from the tables above by fit_coef_kernel: M_h, M_q per
   // edge, M_nu, M_mu per face (M_nu = -0.0 marks a face the H update skips)
   T *Ch[3], *Cq[3], *Cn[3], *Cm[3];
+  // optional coefficient classes: a uint16 class per updated edge and face
+  // (state-array shape, one array per axis) into tables of coefficient
+  // pairs, lut_e[2c] = M_h, lut_e[2c+1] = M_q and lut_f[2c] = M_nu,
+  // lut_f[2c+1] = M_mu (M_nu = -0.0 marks a face the H update skips).  A
+  // class is a distinct tuple (axis, materials of the dof's cells), and its
+  // pair is computed from the tuple by the same functions as above.
+  uint16_t *Ke[3], *Kf[3];
+  T *lut_e, *lut_f;
+};
+
+// Hash tables of the class build (device memory, kClassTable slots each).
+constexpr int kClassTable = 1 << 20;
+constexpr int kMaxClasses = 65535;
+struct FitClassWork {
+  unsigned long long* keys[2];  // edge and face tuples, ~0 empty
+  int* ids[2];                  // dense class of an occupied slot
+  int* count;                   // [2] classes found; [2] overflow flag
 };
 
 // Edges whose update is not the 4-face interior stencil: boundary edges on
@@ -97,6 +114,10 @@ struct FitTmaMaps {
 
 template <typename T>
 cudaError_t fit_build_coefficients(const FitGrid<T>& g, cudaStream_t st);
+// Fills g.Ke, g.Kf and the class tables; ncls[0..1] receive the edge and
+// face class counts, -1 when there are more than kMaxClasses.
+template <typename T>
+cudaError_t fit_build_classes(const FitGrid<T>& g, const FitClassWork& w, int ncls[2], cudaStream_t st);
 
 struct ProbeSet {
   int n;

@@ -33,11 +33,13 @@ constexpr long kTcWaitLimit = 1L << 22;    // mbarrier polls before a wait gives
 struct MlpTcSmem {
   alignas(128) __nv_bfloat16 w1[64 * 16];   // layer-1 B: 8 n-groups x 2 k-groups of core matrices
   alignas(128) __nv_bfloat16 w2[64 * 64];   // layer-2 B: 8 x 8
-  alignas(128) __nv_bfloat16 a1[128 * 16];  // layer-1 A: 16 row groups x 2
-  alignas(128) __nv_bfloat16 a2[128 * 64];  // layer-2 A: 16 x 8
+  // layer-2 A (16 row groups x 8 k-groups); its first 4 KB also hold layer-1
+  // A (16 x 2), which the first MMA has finished reading before A2 is written
+  alignas(128) __nv_bfloat16 a2[128 * 64];
   float b1[64], b2[64], w3[64], b3;
   alignas(8) uint64_t bar;
   uint32_t tmem;
+  __device__ __nv_bfloat16* a1() { return a2; }
 };
 
 // element (r, k) of a K-major operand with `kg` 8-element k-groups
@@ -156,14 +158,14 @@ __device__ __forceinline__ bool mlp_tc_forward(MlpTcSmem& sm, uint32_t& phase, c
 #pragma unroll
   for (int k = 0; k < 16; k += 2) {
     const float lo = k < 6 ? f[k] : 0.0f, hi = k + 1 < 6 ? f[k + 1] : 0.0f;
-    *reinterpret_cast<uint32_t*>(&sm.a1[tc_off(tid, k, 2)]) = mlp_pack(lo, hi);
+    *reinterpret_cast<uint32_t*>(&sm.a1()[tc_off(tid, k, 2)]) = mlp_pack(lo, hi);
   }
   tc_proxy_fence();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   if (tid == 0) {
-    tc_mma(tmem, tc_desc(sm.a1, 128, 256), tc_desc(sm.w1, 128, 256), kId, 0);
+    tc_mma(tmem, tc_desc(sm.a1(), 128, 256), tc_desc(sm.w1, 128, 256), kId, 0);
     tc_commit(&sm.bar);
   }
   bool ok = tc_wait(&sm.bar, phase & 1);

@@ -407,6 +407,8 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
     int sms = 0;
     CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt_.device));
     d.guess_blocks = 3 * sms;
+    d.tc_blocks = opt_.precision == 1 ? group_guess_tc_blocks<float>(opt_.device)
+                                      : group_guess_tc_blocks<double>(opt_.device);
     loss_cap_ = (int64_t)std::max(1, opt_.learn_steps) * std::max(1, opt_.learn_inner);
     loss_hist_ = fz(loss_cap_);
   }

@@ -434,15 +434,25 @@ __device__ __forceinline__ void guess_row(const GroupDev& d, int64_t sl, int64_t
   float sum = 0.0f;
   int cnt = 0;
   {
+    // the row's columns are fetched CH at a time and their r_e gathered
+    // together (independent loads in flight); the sum keeps column order
+    constexpr int CH = 8;
     const int64_t b0 = d.A.ptr[sl];
     const int len = (int)((d.A.ptr[sl + 1] - b0) >> 5);
     const int32_t* col = d.A.col + b0 + (i & 31);
-    for (int j = 0; j < len; j++) {
-      const int32_t cc = ld_stream(col + 32 * j);
-      if (cc != (int32_t)i) {
-        sum += (float)re[cc];
-        cnt++;
-      }
+    for (int j0 = 0; j0 < len; j0 += CH) {
+      int32_t cc[CH];
+      float rv[CH];
+#pragma unroll
+      for (int k = 0; k < CH; k++) cc[k] = j0 + k < len ? ld_stream(col + 32 * (j0 + k)) : (int32_t)i;
+#pragma unroll
+      for (int k = 0; k < CH; k++) rv[k] = cc[k] != (int32_t)i ? (float)re[cc[k]] : 0.0f;
+#pragma unroll
+      for (int k = 0; k < CH; k++)
+        if (cc[k] != (int32_t)i) {
+          sum += rv[k];
+          cnt++;
+        }
     }
   }
   const float pr = (float)pre[i];
@@ -931,6 +941,39 @@ int group_cg_blocks(int device, int S, size_t* smem) {
   return (a < b ? a : b) * sms;
 }
 
+// Resident CTAs of the tensor-core guess kernel over the whole GPU, from its
+// registers and shared memory against the SM's limits, capped at the 8 CTAs
+// whose 64 TMEM columns each fill the SM's 512 (the runtime's occupancy
+// query reported 1 for this kernel, a fraction of what ncu measured).
+template <typename T>
+int group_guess_tc_blocks(int device) {
+  int sms = 0, regs_sm = 0, smem_sm = 0, thr_sm = 0, blk_sm = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, device);
+  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
+  cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, device);
+  cudaDeviceGetAttribute(&blk_sm, cudaDevAttrMaxBlocksPerMultiprocessor, device);
+  cudaFuncSetAttribute(grp_guess_tc<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       (int)cudaSharedmemCarveoutMaxShared);
+  cudaFuncAttributes fa{};
+  int a = 6;  // what the shared operands allow at any carveout of 192 KB or more
+  if (cudaFuncGetAttributes(&fa, grp_guess_tc<T>) == cudaSuccess && fa.numRegs > 0) {
+    const int warps = kTcRows / 32;
+    const int regs_warp = (fa.numRegs * 32 + 255) / 256 * 256;  // 256-register allocation unit
+    const int by_regs = regs_sm / (regs_warp * warps);
+    const int by_smem = smem_sm / (int)(sizeof(MlpTcSmem) + fa.sharedSizeBytes + 1024);  // 1 KB reserved per CTA
+    const int by_thr = thr_sm / kTcRows;
+    a = by_regs < by_smem ? by_regs : by_smem;
+    if (by_thr < a) a = by_thr;
+    if (blk_sm > 0 && blk_sm < a) a = blk_sm;
+    if (a < 1) a = 1;
+  } else {
+    cudaGetLastError();
+  }
+  const int tmem_cap = 512 / kTcCols;
+  return (a < tmem_cap ? a : tmem_cap) * sms;
+}
+
 // One step of every running simulation.  ev (optional, 6 events) brackets:
 // H update + probes, sources + rhs, CG, scatter, step end.
 template <typename T>
@@ -950,7 +993,7 @@ cudaError_t group_launch_step(const GroupDev& d, int cg_blocks, int cg_variant, 
     if (d.mlp_on) {
       // trained network: the tensor-core form, 128 rows per tile
       const int64_t tiles = (slices + 3) / 4;
-      const int64_t g = tiles < 2 * (int64_t)d.guess_blocks ? tiles : 2 * (int64_t)d.guess_blocks;
+      const int64_t g = tiles < (int64_t)d.tc_blocks ? tiles : (int64_t)d.tc_blocks;
       grp_guess_tc<T><<<(unsigned)(g > 0 ? g : 1), kTcRows, sizeof(MlpTcSmem), st>>>(d);
     } else {
       grp_guess_mlp<T><<<(unsigned)(want < d.guess_blocks ? (want > 0 ? want : 1) : d.guess_blocks), kGB, 0, st>>>(d);
@@ -990,5 +1033,7 @@ template cudaError_t group_launch_step<double>(const GroupDev&, int, int, size_t
 template cudaError_t group_launch_step<float>(const GroupDev&, int, int, size_t, cudaStream_t, cudaEvent_t*);
 template int group_cg_blocks<double>(int, int, size_t*);
 template int group_cg_blocks<float>(int, int, size_t*);
+template int group_guess_tc_blocks<double>(int);
+template int group_guess_tc_blocks<float>(int);
 
 }  // namespace tf

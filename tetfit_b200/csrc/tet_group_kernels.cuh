@@ -83,6 +83,7 @@ struct GroupDev {
   void *xe = nullptr, *r_alt = nullptr, *z_alt = nullptr;
   int mlp_on = 0, dual = 0;
   int guess_blocks = 1;           // grid of the learned-guess kernel (a few blocks per SM)
+  int tc_blocks = 1;              // grid of the tensor-core guess kernel (resident CTAs x SMs)
   int8_t* kept = nullptr;
   const unsigned char* mlp_img = nullptr;
   // training samples: rows i = samp_first + k * samp_stride, k < nsamp
@@ -124,6 +125,8 @@ cudaError_t group_launch_step(const GroupDev& d, int cg_blocks, int cg_variant, 
                               cudaEvent_t* ev);
 template <typename T>
 int group_cg_blocks(int device, int S, size_t* smem);
+template <typename T>
+int group_guess_tc_blocks(int device);
 template <typename T>
 cudaError_t group_launch_targets(const GroupDev& d, cudaStream_t st);
 // Energy partials of member s (free rows [r0, r0 + nr), faces [f0, f0 + nf))
