@@ -511,7 +511,8 @@ def run_batch(args, rank, world, local_rank):
         b.step_io(member_carriers(infos, cases, [d_ + k for d_ in done]), probes)
     e2e_s = time.perf_counter() - t0
     barrier()
-    check = _sample_members(cases) if rank == 0 else []
+    smallest = sorted(range(len(cases)), key=lambda q: (cases[q].n, q))[:3]
+    check = sorted(set(_sample_members(cases)) | set(smallest)) if rank == 0 else []
     fp32_probes = {m: b.probes(m) for m in check}
     kps = infos[0]["kernels_per_step"]
     b.close()
@@ -567,7 +568,7 @@ def run_batch(args, rank, world, local_rank):
         c.close()
     # probe error of the FP32 learned run: against the batched FP64 run of the
     # same members (stratified sample incl. the largest mesh) over the steps
-    # both took, and against the FP64 CPU oracle for the two smallest members
+    # both took, and against the FP64 CPU oracle for the three smallest members
     perr, perr_oracle = {}, {}
     if rank == 0:
         for m in check:
@@ -576,7 +577,7 @@ def run_batch(args, rank, world, local_rank):
             k = min(len(t32), len(t64))
             perr[m] = _rel(v32[:k], v64[:k])
         import oracle
-        for m in ([] if args.no_arms else sorted(range(len(cases)), key=lambda q: (cases[q].n, q))[:2]):
+        for m in ([] if args.no_arms else smallest):
             if m not in fp32_probes:
                 continue
             t32, v32 = fp32_probes[m]

@@ -36,7 +36,7 @@ enum {
   TF_E_SCRIPT = -1,      /* script / mesh / solids file error (MyThrow text)        */
   TF_E_ARG = -2,         /* bad argument, unknown simulation label, buffer too small */
   TF_E_CUDA = -3,        /* CUDA runtime error or no usable sm_100 device           */
-  TF_E_UNSUPPORTED = -4, /* feature outside the time-stepping path (e.g. PML, silo)  */
+  TF_E_UNSUPPORTED = -4, /* feature outside the time-stepping path (e.g. PML)         */
   TF_E_STATE = -5,       /* call out of order (e.g. tf_step before tf_prepare)       */
   TF_E_SOLVER = -6       /* iterative solve hit its iteration limit                 */
 };
@@ -46,7 +46,9 @@ enum { TF_FP64 = 0, TF_FP32 = 1 };
 typedef struct tf_opts {
   int32_t precision;    /* TF_FP64 (default) or TF_FP32 field state                     */
   int32_t device;       /* CUDA device ordinal                                          */
-  int32_t write_files;  /* tf_run: write <name><label>_probe_E/H.dat and poynting.dat   */
+  int32_t write_files;  /* tf_run: write <name><label>_probe_E/H.dat (probepoint) or one
+                           <name><label>_<dump>.tfd per print time (silo, tets), and
+                           poynting.dat                                            */
   int32_t verbose;      /* print the reference's parameter banner and stats            */
   int32_t graph_steps;  /* steps per captured CUDA graph (0: automatic)                */
   int32_t mass_model;   /* gfdtd eps-mass: 0 as the reference builds it, 1 consistent  */
@@ -109,7 +111,9 @@ TF_API int tf_get_info(tf_ctx* ctx, tf_info* info);
 /* Advance up to nsteps leapfrog steps (Discretization.hpp:1840-1933). */
 TF_API int tf_step(tf_ctx* ctx, uint64_t nsteps, uint64_t* done);
 /* Probe series so far: times[n], values[n][n_probes][6] = Ex Ey Ez Hx Hy Hz
- * (ExportFitFields, Discretization.hpp:3096-3158).  *n_samples is always set. */
+ * (ExportFitFields, Discretization.hpp:3096-3158).  *n_samples is always set.
+ * In silo mode on tets every tet is a probe, at its barycentre, in tet order
+ * (the per-tet E and H of the reference's Silo export, :2601-2677). */
 TF_API int tf_get_probes(tf_ctx* ctx, double* times, double* values, size_t cap_samples, size_t* n_samples);
 /* Probe coordinates [n_probes][3] and containing cell index (reference numbering). */
 TF_API int tf_get_probe_points(tf_ctx* ctx, double* xyz, uint64_t* cells, size_t cap);

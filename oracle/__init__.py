@@ -164,6 +164,7 @@ class TetOracle:
             L.orc_tet_probes.argtypes = [P, P, P, P, P]
             L.orc_tet_state.argtypes = [P, P, P, P]
             L.orc_tet_flux.argtypes = [P, P]
+            L.orc_tet_losses.argtypes = [P, P]
             L.orc_tet_cg.argtypes = [P, P, P]
             L.orc_tet_topology.argtypes = [P, P, P, P, P]
             L.orc_tet_matrix.restype = ctypes.c_longlong
@@ -209,6 +210,12 @@ class TetOracle:
         self.L.orc_tet_flux(self.h, _p(f))
         return f
 
+    def losses(self):
+        """poynting.dat's third column (one entry per step taken)."""
+        f = np.zeros(self.steps_done)
+        self.L.orc_tet_losses(self.h, _p(f))
+        return f
+
     def cg(self):
         it = np.zeros(self.steps_done, dtype=np.int32)
         er = np.zeros(self.steps_done)
@@ -224,10 +231,11 @@ class TetOracle:
         return e, f, c, b
 
     def matrix(self, which: str):
-        """CSR (ptr, col, val) of one operator: C, N, H (dga), E or A (gfdtd)."""
-        w = {"C": 0, "N": 1, "H": 2, "E": 3, "A": 4}[which]
+        """CSR (ptr, col, val) of one operator: C, N, H (dga), E, Sig (the
+        conductivity mass) or A (gfdtd, fem)."""
+        w = {"C": 0, "N": 1, "H": 2, "E": 3, "A": 4, "Sig": 5}[which]
         nnz = int(self.L.orc_tet_matrix(self.h, w, None, None, None))
-        nrows = {0: self.nF, 1: self.nF, 2: self.nE, 3: self.nE, 4: self.n_free}[w]
+        nrows = {0: self.nF, 1: self.nF, 2: self.nE, 3: self.nE, 4: self.n_free, 5: self.nE}[w]
         ptr = np.zeros(nrows + 1, dtype=np.uint64)
         col = np.zeros(nnz, dtype=np.uint32)
         val = np.zeros(nnz)

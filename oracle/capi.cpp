@@ -365,6 +365,15 @@ int orc_tet_flux(void* h, double* flux) {
   return (int)o->flux.size();
 }
 
+// poynting.dat's third column: the first n entries of the losses list, one
+// per step taken (gfdtd, fem; dga returns zeros)
+int orc_tet_losses(void* h, double* loss) {
+  auto* o = static_cast<orc::TetOracle*>(h);
+  const size_t n = o->flux.size();
+  for (size_t k = 0; k < n; k++) loss[k] = k < o->losses.size() ? o->losses[k] : 0.0;
+  return (int)n;
+}
+
 int orc_tet_cg(void* h, int* iters, double* errs) {
   auto* o = static_cast<orc::TetOracle*>(h);
   for (size_t k = 0; k < o->cg_iters.size(); k++) {
@@ -391,7 +400,8 @@ int orc_tet_topology(void* h, unsigned* edges, unsigned* faces, unsigned char* c
 // CSR export of an operator: which 0 C, 1 N, 2 H, 3 E, 4 A; returns nnz
 long long orc_tet_matrix(void* h, int which, unsigned long long* ptr, unsigned* col, double* val) {
   auto* o = static_cast<orc::TetOracle*>(h);
-  const orc::Csr* m = which == 0 ? &o->C : which == 1 ? &o->N : which == 2 ? &o->H : which == 3 ? &o->E : &o->A;
+  const orc::Csr* m = which == 0 ? &o->C : which == 1 ? &o->N : which == 2 ? &o->H : which == 3 ? &o->E
+                     : which == 5 ? &o->Sig : &o->A;
   if (ptr) for (size_t i = 0; i < m->ptr.size(); i++) ptr[i] = m->ptr[i];
   if (col) std::memcpy(col, m->col.data(), m->col.size() * sizeof(unsigned));
   if (val) std::memcpy(val, m->val.data(), m->val.size() * sizeof(double));

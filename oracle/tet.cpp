@@ -61,6 +61,14 @@ static V3 matvec(const Mat3& m, const V3& v) {
   for (int i = 0; i < 3; i++) r[i] = m.m[i][0] * v[0] + m.m[i][1] * v[1] + m.m[i][2] * v[2];
   return r;
 }
+// 3x3 determinant by cofactor expansion along the first row (the zero test
+// the reference applies to sigma, Discretization.hpp:8604, 8041)
+static double mat_det(const Mat3& a) {
+  const auto& m = a.m;
+  return m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) - m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
+         m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+}
+
 static bool mat_zero(const Mat3& m) {
   for (int i = 0; i < 3; i++)
     for (int j = 0; j < 3; j++)
@@ -271,8 +279,10 @@ void TetOracle::read_mesh() {
     V3 v1 = sub(pts[t[1]], pts[t[0]]), v2 = sub(pts[t[2]], pts[t[0]]), v3 = sub(pts[t[3]], pts[t[0]]);
     cell_vol.push_back(dot(v1, cross(v2, v3)) / 6.0);
     const Material& mt = sc.materials[tt[k].second];
-    if (!mat_zero(mt.sigma) || !mat_zero(mt.chi))
-      throw std::runtime_error("lossy materials (sigma or chi) on tetrahedra are outside the supported path");
+    // conductivity enters gfdtd and fem through SigMat; dga's lossy
+    // ("fractured") edge classes and magnetic losses are not restated
+    if (!mat_zero(mt.chi) || (method == 1 && !mat_zero(mt.sigma)))
+      throw std::runtime_error("lossy materials (chi on tetrahedra, or sigma with dga) are outside the supported path");
   }
   // unique faces (Discretization.hpp:10173-10219)
   std::sort(tri.begin(), tri.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
@@ -645,7 +655,7 @@ void TetOracle::build_gfdtd() {
       free_edges.push_back(e);
     }
   N = assemble_N();
-  std::vector<Csr::Trip> et;
+  std::vector<Csr::Trip> et, st;
   for (uint32_t nid = 0; nid < pts.size(); nid++) {
     for (uint32_t vv : node_vols[nid]) {
       auto el = vol_edges(vv);
@@ -673,11 +683,24 @@ void TetOracle::build_gfdtd() {
       }
       for (auto& pq : kPair)
         et.push_back({e[pq[0]], e[pq[1]], quarter * sg[pq[0]] * sg[pq[1]] * dot(f[pq[0]], matvec(oe, f[pq[1]]))});
+      // SigMat: the same dual basis with sigma, for tets whose sigma has a
+      // non-zero determinant (:8604-8616)
+      const Mat3& sig = sc.materials.at(vol_mat[vv]).sigma;
+      if (mat_det(sig) != 0) {
+        Mat3 os;
+        for (int i = 0; i < 3; i++)
+          for (int j = 0; j < 3; j++) os.m[i][j] = om * sig.m[i][j];
+        for (auto& pq : kPair)
+          st.push_back({e[pq[0]], e[pq[1]], quarter * sg[pq[0]] * sg[pq[1]] * dot(f[pq[0]], matvec(os, f[pq[1]]))});
+      }
     }
   }
   E = Csr::build(NE, NE, et);
+  Sig = Csr::build(NE, NE, st);
+  lossy = !st.empty();
   estimate_dt_pencil();
-  split_system(1.0);
+  // SysMat = E + (0.5 dt) SigMat (:8644)
+  split_system(1.0, 0.5 * dt);
 }
 
 void TetOracle::estimate_dt_pencil() {
@@ -707,17 +730,36 @@ void TetOracle::estimate_dt_pencil() {
   }
 }
 
-void TetOracle::split_system(double scale) {
-  // SysMat = scale * E; A = SysMat on free rows/cols, RHSmat1 = SysMat on free
-  // rows x Dirichlet cols (gfdtd :8644-8670 with scale 1; fem :8086-8120 with
-  // scale 1 / dt^2, applied as E * (1 / (dt dt)))
+void TetOracle::split_system(double scale, double sig_coef) {
+  // SysMat = scale * E + sig_coef * SigMat; A = SysMat on free rows/cols,
+  // RHSmat1 = SysMat on free rows x Dirichlet cols (gfdtd :8644-8670 with
+  // scale 1 and sig_coef dt / 2; fem :8086-8120 with scale 1 / dt^2, applied
+  // as E * (1 / (dt dt)), and sig_coef 0.5 / dt).  The rows of E and SigMat
+  // are merged by column: E_rc scale + coef S_rc where both hold an entry,
+  // the one present otherwise.
   const uint32_t NE = (uint32_t)edges.size();
   std::vector<Csr::Trip> at, rt;
   for (uint32_t r = 0; r < NE; r++) {
     if (free_index[r] < 0) continue;
-    for (uint64_t k = E.ptr[r]; k < E.ptr[r + 1]; k++) {
-      uint32_t c = E.col[k];
-      const double v = scale == 1.0 ? E.val[k] : E.val[k] * scale;
+    uint64_t k = E.ptr[r], ks = lossy ? Sig.ptr[r] : 0;
+    const uint64_t ke = E.ptr[r + 1], kse = lossy ? Sig.ptr[r + 1] : 0;
+    while (k < ke || ks < kse) {
+      uint32_t c;
+      double v;
+      if (ks >= kse || (k < ke && E.col[k] < Sig.col[ks])) {
+        c = E.col[k];
+        v = scale == 1.0 ? E.val[k] : E.val[k] * scale;
+        k++;
+      } else if (k >= ke || Sig.col[ks] < E.col[k]) {
+        c = Sig.col[ks];
+        v = sig_coef * Sig.val[ks];
+        ks++;
+      } else {
+        c = E.col[k];
+        v = (scale == 1.0 ? E.val[k] : E.val[k] * scale) + sig_coef * Sig.val[ks];
+        k++;
+        ks++;
+      }
       if (free_index[c] < 0) rt.push_back({r, c, v});
       else at.push_back({(uint32_t)free_index[r], (uint32_t)free_index[c], v});
     }
@@ -744,7 +786,7 @@ void TetOracle::build_fem() {
       free_edges.push_back(e);
     }
   N = assemble_N();
-  std::vector<Csr::Trip> et;
+  std::vector<Csr::Trip> et, st;
   static const int kEdge[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
   for (uint32_t vv = 0; vv < vols.size(); vv++) {
     const Mat3& eps = sc.materials.at(vol_mat[vv]).eps;
@@ -782,7 +824,9 @@ void TetOracle::build_fem() {
         for (int x = 0; x < 3; x++) w[k][x] = l[a] * wn[x][b] - l[b] * wn[x][a];
       }
     };
-    double sumn[6][6] = {}, sumf[6][6] = {};
+    const Mat3& sig = sc.materials.at(vol_mat[vv]).sigma;
+    const bool lossy_vol = mat_det(sig) != 0;
+    double sumn[6][6] = {}, sumf[6][6] = {}, sumn_s[6][6] = {}, sumf_s[6][6] = {};
     for (int h = 0; h < 4; h++) {
       V3 w1[6], w2[6];
       whitney(pts[vols[vv][h]], w1);
@@ -791,6 +835,10 @@ void TetOracle::build_fem() {
         for (int k = j; k < 6; k++) {
           sumn[j][k] += dot(w1[k], matvec(eps, w1[j]));
           sumf[j][k] += dot(w2[k], matvec(eps, w2[j]));
+          if (lossy_vol) {  // (:8020-8021)
+            sumn_s[j][k] += dot(w1[k], matvec(sig, w1[j]));
+            sumf_s[j][k] += dot(w2[k], matvec(sig, w2[j]));
+          }
         }
     }
     const double vol = std::fabs(cell_vol[vv]);
@@ -801,11 +849,21 @@ void TetOracle::build_fem() {
           et.push_back({el[j], el[k], val});
           if (k != j) et.push_back({el[k], el[j], val});
         }
+        if (lossy_vol) {  // SigMat (:8041-8051)
+          const double sv = vol * (sumn_s[j][k] + sumf_s[j][k] * 9.0) / 40.0;
+          if (sv != 0) {
+            st.push_back({el[j], el[k], sv});
+            if (k != j) st.push_back({el[k], el[j], sv});
+          }
+        }
       }
   }
   E = Csr::build(NE, NE, et);
+  Sig = Csr::build(NE, NE, st);
+  lossy = !st.empty();
   estimate_dt_pencil();
-  split_system(1.0 / (dt * dt));
+  // SysMat = E (1 / dt^2) + (0.5 / dt) SigMat (:8092-8093)
+  split_system(1.0 / (dt * dt), 0.5 / dt);
 }
 
 int TetOracle::cg_solve(const Csr& M, const std::vector<double>& pre, const double* b, double* x, double tol,
@@ -1014,14 +1072,29 @@ void TetOracle::prepare(uint32_t label) {
   U.assign(NE, 0); I.assign(NE, 0); F.assign(NF, 0); B.assign(NF, 0);
   Fb.assign(bnd_dual.size(), 0); Fb_old = Fb; SrcFld.assign(NE, 0);
   solution.assign(free_edges.size(), 0);
-  if (out.mode == "probepoint") {
-    for (auto& pv : out.probes) {
-      uint32_t v = find_probe(pv);
-      if (v < vols.size()) {
-        probe_elem.push_back(v);
-        probe_pts.push_back(pv);
-      }
+  if (out.mode == "silo") {
+    // ExportFields "silo" (:2601-2677): E (Whitney) at the barycentre
+    // (p0+p1+p2+p3)/4 (:10479-10484) and H of every tet at each print time,
+    // sampled here like probes
+    for (uint32_t v = 0; v < vols.size(); v++) {
+      std::array<double, 3> b;
+      for (int a = 0; a < 3; a++)
+        b[a] = (pts[vols[v][0]][a] + pts[vols[v][1]][a] + pts[vols[v][2]][a] + pts[vols[v][3]][a]) / 4.0;
+      probe_elem.push_back(v);
+      probe_pts.push_back(b);
     }
+  }
+  // probes and point dipoles are located in the probepoint and maxerror
+  // output modes only (:378-464)
+  if (out.mode == "probepoint" || out.mode == "maxerror") {
+    if (out.mode == "probepoint")
+      for (auto& pv : out.probes) {
+        uint32_t v = find_probe(pv);
+        if (v < vols.size()) {
+          probe_elem.push_back(v);
+          probe_pts.push_back(pv);
+        }
+      }
     // point dipoles: nearest edge of the star of the tet's first node (:436-464)
     for (uint32_t sl : sim.sources) {
       Source& s = sc.sources[sl];
@@ -1064,7 +1137,7 @@ void TetOracle::prepare(uint32_t label) {
   }
   U_old = U;
   U_older = U;
-  if (method == 1 && out.mode == "probepoint" && out.allow_print(0.0)) export_probes(0.0);
+  if (method == 1 && (out.mode == "probepoint" || out.mode == "silo") && out.allow_print(0.0)) export_probes(0.0);
 }
 
 void TetOracle::dga_step(double t) {
@@ -1101,7 +1174,7 @@ void TetOracle::dga_step(double t) {
     B[f] = B[f] - dt * cu[f];
     F[f] = F[f] - dt * ncu[f];
   }
-  if (out.mode == "probepoint" && out.allow_print(t)) export_probes(t);
+  if ((out.mode == "probepoint" || out.mode == "silo") && out.allow_print(t)) export_probes(t);
 }
 
 void TetOracle::gfdtd_step(double t, double t_prev) {
@@ -1111,7 +1184,7 @@ void TetOracle::gfdtd_step(double t, double t_prev) {
   C.mul(U.data(), cu.data());
   for (size_t f = 0; f < NF; f++) B[f] -= dt * cu[f];
   N.mul(B.data(), F.data());
-  if (out.mode == "probepoint" && out.allow_print(t_prev)) export_probes(t_prev);
+  if ((out.mode == "probepoint" || out.mode == "silo") && out.allow_print(t_prev)) export_probes(t_prev);
   Fb_old = Fb;
   for (uint32_t e = 0; e < NE; e++) {
     if (edge_bcs[e] != 0 && sc.bcs[edge_bcs[e]].type != "none") {
@@ -1127,15 +1200,18 @@ void TetOracle::gfdtd_step(double t, double t_prev) {
       }
     }
   }
-  // Psi = E U_old - RHSmat1 SrcFld - dt I + dt C^T F + dt Ctb Fb
-  std::vector<double> eu(NE), rs(NE), ctf(NE), psi(NE);
+  // Psi = E U_old - (dt/2) SigMat U_old - RHSmat1 SrcFld - dt I + dt C^T F
+  //       + dt Ctb Fb   (:1516-1519)
+  std::vector<double> eu(NE), rs(NE), ctf(NE), psi(NE), su(NE, 0.0);
   E.mul(U_old.data(), eu.data());
+  if (lossy) Sig.mul(U_old.data(), su.data());
   RHS1.mul(SrcFld.data(), rs.data());
   C.mul_t(F.data(), ctf.data());
+  push_loss_pre(su);
   double fl = 0;
   for (uint32_t e = 0; e < NE; e++) {
     double cb = bnd_edges[e] >= 0 ? Fb[bnd_edges[e]] : 0.0;
-    psi[e] = eu[e] - rs[e] - dt * I[e] + dt * ctf[e] + dt * cb;
+    psi[e] = eu[e] - (0.5 * dt) * su[e] - rs[e] - dt * I[e] + dt * ctf[e] + dt * cb;
     double cbh = bnd_edges[e] >= 0 ? 0.5 * (Fb[bnd_edges[e]] + Fb_old[bnd_edges[e]]) : 0.0;
     fl += U_old[e] * cbh;
   }
@@ -1147,7 +1223,29 @@ void TetOracle::gfdtd_step(double t, double t_prev) {
   cg_iters.push_back(it);
   cg_err.push_back(err);
   for (size_t k = 0; k < free_edges.size(); k++) U[free_edges[k]] = solution[k];
+  push_loss_post();
   U_old = U;
+}
+
+// poynting.dat's third column for gfdtd and fem: each step pushes
+// 0.5 U_old^T SigMat U_old before the solve and, from the second step on,
+// U^T SigMat U after it (:1518-1546, :1733-1757), and the file prints the
+// first n entries of that list (one row per step)
+void TetOracle::push_loss_pre(const std::vector<double>& su) {
+  double a = 0;
+  if (lossy)
+    for (size_t e = 0; e < su.size(); e++) a += U_old[e] * su[e];
+  losses.push_back(0.5 * a);
+}
+void TetOracle::push_loss_post() {
+  if (step_index + 1 <= 1) return;  // `if (i > 1)`
+  double a = 0;
+  if (lossy) {
+    std::vector<double> su(U.size());
+    Sig.mul(U.data(), su.data());
+    for (size_t e = 0; e < su.size(); e++) a += U[e] * su[e];
+  }
+  losses.push_back(a);
 }
 
 void TetOracle::fem_step(double t, double t_prev) {
@@ -1157,7 +1255,7 @@ void TetOracle::fem_step(double t, double t_prev) {
   std::vector<double> cu(NF);
   C.mul(U.data(), cu.data());
   for (size_t f = 0; f < NF; f++) B[f] -= dt * cu[f];
-  if (out.mode == "probepoint" && out.allow_print(t_prev)) export_probes(t_prev);
+  if ((out.mode == "probepoint" || out.mode == "silo") && out.allow_print(t_prev)) export_probes(t_prev);
   Fb_old = Fb;
   for (uint32_t e = 0; e < NE; e++) {
     if (edge_bcs[e] != 0 && sc.bcs[edge_bcs[e]].type != "none") {
@@ -1175,19 +1273,26 @@ void TetOracle::fem_step(double t, double t_prev) {
   }
   // Psi = 2 (E U_old) / dt^2 - C^T N C U_old + (1/dt) Ctb (Fb - Fb_old)
   //       - (E U_older) / dt^2 - RHSmat1 SrcFld - (1/dt) I   (:1713-1716)
-  std::vector<double> cuo(NF), ncu(NF), cc(NE), eu(NE), euo(NE), rs(NE), psi(NE);
+  //       + (0.5/dt) SigMat U_older (lossy materials)
+  std::vector<double> cuo(NF), ncu(NF), cc(NE), eu(NE), euo(NE), rs(NE), psi(NE), suo(NE, 0.0), su(NE, 0.0);
   C.mul(U_old.data(), cuo.data());
   N.mul(cuo.data(), ncu.data());
   C.mul_t(ncu.data(), cc.data());
   E.mul(U_old.data(), eu.data());
   E.mul(U_older.data(), euo.data());
+  if (lossy) {
+    Sig.mul(U_older.data(), suo.data());
+    Sig.mul(U_old.data(), su.data());
+  }
   RHS1.mul(SrcFld.data(), rs.data());
+  push_loss_pre(su);
   const double idt2 = 1.0 / (dt * dt), idt = 1.0 / dt;
   double fl = 0;
   for (uint32_t e = 0; e < NE; e++) {
     const double fb = bnd_edges[e] >= 0 ? Fb[bnd_edges[e]] : 0.0;
     const double fbo = bnd_edges[e] >= 0 ? Fb_old[bnd_edges[e]] : 0.0;
-    psi[e] = 2.0 * eu[e] * idt2 - cc[e] + idt * (fb - fbo) - euo[e] * idt2 - rs[e] - idt * I[e];
+    psi[e] = 2.0 * eu[e] * idt2 - cc[e] + idt * (fb - fbo) - euo[e] * idt2 + (0.5 / dt) * suo[e] - rs[e] -
+             idt * I[e];
     fl += U_old[e] * (0.5 * (fb + fbo));
   }
   flux.push_back(fl);
@@ -1198,6 +1303,7 @@ void TetOracle::fem_step(double t, double t_prev) {
   cg_iters.push_back(it);
   cg_err.push_back(err);
   for (size_t k = 0; k < free_edges.size(); k++) U[free_edges[k]] = solution[k];
+  push_loss_post();
   U_older = U_old;
   U_old = U;
 }

@@ -58,6 +58,9 @@ struct TetOracle {
   Csr N;                               // F x F
   Csr H;                               // E x E, rows of class-1 edges (dga)
   Csr E;                               // E x E eps mass (gfdtd: node-star dual basis; fem: Whitney)
+  Csr Sig;                             // E x E conductivity mass (SigMat), same construction with sigma
+  bool lossy = false;                  // some tet conducts (sigma with non-zero determinant)
+  std::vector<double> losses;          // poynting.dat third column entries (gfdtd, fem)
   Csr A, RHS1;                         // free x free system; E(free rows, Dirichlet cols)
   std::vector<int64_t> free_index;     // edge -> compressed free index or -1
   std::vector<uint32_t> free_edges;
@@ -88,7 +91,9 @@ struct TetOracle {
   void build_dga();
   void build_gfdtd();
   void build_fem();
-  void split_system(double scale);
+  void split_system(double scale, double sig_coef = 0.0);
+  void push_loss_pre(const std::vector<double>& su);
+  void push_loss_post();
   std::array<uint32_t, 6> vol_edges(uint32_t v) const;
   std::array<std::array<double, 3>, 6> dual_area_vectors(uint32_t v) const;
   std::array<std::array<double, 3>, 4> primal_area_vectors(uint32_t v) const;

@@ -1,0 +1,141 @@
+"""Conducting materials on tetrahedra (gfdtd and fem): the conductivity mass
+SigMat (Discretization.hpp:8604-8616 for gfdtd, the same dual basis as the
+eps-mass; :8020-8051 for fem, the same Whitney quadrature), the system
+SysMat = E + (dt/2) SigMat (gfdtd, :8644) or E / dt^2 + (0.5/dt) SigMat (fem,
+:8092-8093), the right-hand-side terms (:1516-1519, :1729-1731) and the
+Joule-loss column of poynting.dat (:1518-1546, :1733-1757).  dga's lossy
+("fractured") classes and magnetic losses stay outside the supported path."""
+import numpy as np
+import pytest
+
+import oracle
+import tetfit_b200 as tb
+from tetfit_b200.cases import TetCase, write_tet_case
+
+EPS0_SCRIPT = 8.854187817e-12  # the reference's vacuum permittivity
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def csr(m, n):
+    import scipy.sparse as sp
+    ptr, col, val = m
+    return sp.csr_matrix((val, col.astype(np.int64), ptr.astype(np.int64)), shape=(n, n))
+
+
+def lossy_case(method, **kw):
+    base = dict(n=4, method=method, steps=60, split_x=True, eps=(1.5, 3.0), sigma=(0.0, 0.02),
+                carrier="gaussian", width=2e-9, delay=4e-9)
+    base.update(kw)
+    return TetCase(**base)
+
+
+@pytest.mark.parametrize("method", ["gfdtd", "fem"])
+def test_uniform_conductivity_mass_is_the_scaled_eps_mass(tmp_path, oracle_lib, method):
+    """With one material, SigMat is built exactly like E with sigma for eps, so
+    SigMat = sigma / (eps_r eps0) E (CPU, oracle)."""
+    s = write_tet_case(str(tmp_path), TetCase(n=3, method=method, steps=4, eps=(2.0,), sigma=(0.01,)))
+    o = oracle.TetOracle(s)
+    E, S = csr(o.matrix("E"), o.nE), csr(o.matrix("Sig"), o.nE)
+    o.close()
+    assert S.nnz > 0
+    d = S - (0.01 / (2.0 * EPS0_SCRIPT)) * E
+    assert abs(d).max() <= 1e-12 * abs(S).max()
+
+
+@pytest.mark.parametrize("method", ["gfdtd", "fem"])
+def test_losses_column_follows_the_reference_list(tmp_path, oracle_lib, method):
+    """The reference pushes 0.5 a_{i-1} before and (from step 2) a_i after each
+    solve into one list and prints its first n entries, so from the third row
+    on every odd row is half the even row before it (CPU, oracle)."""
+    s = write_tet_case(str(tmp_path), lossy_case(method, steps=40))
+    o = oracle.TetOracle(s)
+    o.run()
+    L = o.losses()
+    o.close()
+    assert L[0] == 0.0 and np.all(L >= 0) and L.max() > 0
+    assert np.array_equal(L[3::2], 0.5 * L[2:-1:2][:len(L[3::2])])
+
+
+@pytest.mark.parametrize("method", ["gfdtd", "fem"])
+def test_conductivity_damps_the_field(tmp_path, oracle_lib, method):
+    """A gaussian pulse in a PEC box: with a conducting half the field left
+    after the pulse is smaller than without (CPU, oracle)."""
+    norms = {}
+    for sig in ((0.0, 0.0), (0.0, 0.02)):
+        s = write_tet_case(str(tmp_path / str(sig[1])), lossy_case(method, steps=80, sigma=sig))
+        o = oracle.TetOracle(s)
+        o.run()
+        norms[sig[1]] = np.linalg.norm(o.state()[0])
+        o.close()
+    assert norms[0.02] < 0.5 * norms[0.0]
+
+
+def test_oracle_rejects_conductivity_with_dga(tmp_path, oracle_lib):
+    s = write_tet_case(str(tmp_path), TetCase(n=3, method="dga", steps=4, sigma=(0.01,)))
+    with pytest.raises(Exception):
+        oracle.TetOracle(s)
+
+
+def pair(script, precision="fp64"):
+    o = oracle.TetOracle(script)
+    o.run()
+    to, vo, _, _ = o.probes()
+    ref = dict(t=to, v=vo, U=o.state()[0], flux=o.flux(), loss=o.losses(), it=o.cg()[0])
+    o.close()
+    with tb.Discretization(script) as d:
+        d.prepare(1, precision=precision)
+        d.step(10 ** 6)
+        t, v = d.probes()
+        got = dict(t=t, v=v, U=d.state()[0], flux=d.flux(), loss=d.losses(), it=d.solver_stats()[0])
+    return got, ref
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", ["gfdtd", "fem"])
+def test_conducting_members_match_oracle(tmp_path, product_lib, oracle_lib, method):
+    s = write_tet_case(str(tmp_path), lossy_case(method, tolerance=1e-13))
+    g, o = pair(s)
+    assert np.array_equal(g["t"], o["t"])
+    assert np.abs(o["loss"]).max() > 0
+    for k in ("v", "U", "flux", "loss"):
+        assert rel(g[k], o[k]) <= 1e-10, k
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", ["gfdtd", "fem"])
+def test_conducting_members_at_reference_tolerance(tmp_path, product_lib, oracle_lib, method):
+    """CG to 1e-8 as the configurations run it: iteration counts within one of
+    the oracle's step by step; FP32 state within 2e-5 of the FP64 oracle."""
+    s = write_tet_case(str(tmp_path), lossy_case(method, n=5))
+    g, o = pair(s)
+    assert np.abs(g["it"] - o["it"]).max() <= 1 and rel(g["v"], o["v"]) <= 1e-8
+    g32, _ = pair(s, precision="fp32")
+    assert rel(g32["v"], o["v"]) <= 2e-5 and rel(g32["loss"], o["loss"]) <= 2e-5
+
+
+@pytest.mark.gpu
+def test_conducting_and_lossless_members_in_one_batch(tmp_path, product_lib, oracle_lib):
+    cases = [lossy_case("gfdtd", steps=40), TetCase(n=4, method="gfdtd", steps=50, seed=5),
+             lossy_case("fem", steps=50, n=5, sigma=(0.01, 0.0))]
+    scripts = [write_tet_case(str(tmp_path / f"m{i}"), c) for i, c in enumerate(cases)]
+    with tb.Batch([(s, 1) for s in scripts], precision="fp64") as b:
+        b.step(10 ** 6)
+        res = [(b.probes(m), b.state(m)[0]) for m in range(len(scripts))]
+    for s, ((t, v), U) in zip(scripts, res):
+        o = oracle.TetOracle(s)
+        o.run()
+        assert np.array_equal(t, o.probes()[0])
+        assert rel(v, o.probes()[1]) <= 1e-8 and rel(U, o.state()[0]) <= 1e-8
+        o.close()
+
+
+@pytest.mark.gpu
+def test_dga_rejects_conductivity(tmp_path, product_lib):
+    s = write_tet_case(str(tmp_path), TetCase(n=3, method="dga", steps=4, sigma=(0.01,)))
+    with tb.Discretization(s) as d:
+        with pytest.raises(tb.TetfitError) as e:
+            d.prepare(1)
+    assert e.value.code == tb.TF_E_UNSUPPORTED

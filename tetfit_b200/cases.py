@@ -233,6 +233,7 @@ class TetCase:
     jitter: float = 0.15
     seed: int = 0x7E7F17
     eps: object = (1.0,)             # eps_r per material label 1, 2, ... (tuple) or {label: eps_r}
+    sigma: object = None             # conductivity (S/m) per material label, like eps (None: lossless)
     split_x: bool = False            # material 1 for x < 0.5, 2 for x >= 0.5
     pec_surfaces: tuple = (2, 3, 4, 5, 6)
     source_surface: int = 1
@@ -250,6 +251,8 @@ class TetCase:
     direction: str = "x"
     mesh_format: str = "netgen"      # "netgen" or "gmsh"
     coord_fmt: str = "%.17g"         # netgen coordinates ("%g": the 6 digits a gmsh conversion keeps)
+    output_mode: str = "probepoint"  # "silo": per-tet field dumps at every print time
+    output_period: float = 0.0       # SET period of the output (0: every step)
 
     def dt(self) -> float:
         if self.step is not None:
@@ -277,15 +280,16 @@ def write_tet_case(directory: str, case: TetCase, name: str = "box") -> str:
     lines = ["DEFINE mesh 1", "   SET type tetrahedral", f"   SET mesher {case.mesh_format}",
              f"   SET file {os.path.basename(mesh)}", "   SET name box", "   SET scalefactor 1", "END mesh 1"]
     eps_items = case.eps.items() if isinstance(case.eps, dict) else enumerate(case.eps, start=1)
+    sig = dict(case.sigma.items() if isinstance(case.sigma, dict) else enumerate(case.sigma or (), start=1))
     for m, e in eps_items:
-        lines += [f"DEFINE material {m}", f"   SET epsilon {float(e)!r}", "   SET mu 1", "   SET sigma 0",
-                  "   SET chi 0", f"END material {m}"]
+        lines += [f"DEFINE material {m}", f"   SET epsilon {float(e)!r}", "   SET mu 1",
+                  f"   SET sigma {float(sig.get(m, 0.0))!r}", "   SET chi 0", f"END material {m}"]
     lines += ["DEFINE bc 1"] + [f"   SET surface {s}" for s in case.pec_surfaces] + ["   SET type pec", "END bc 1"]
     lines += source_lines(case)
     if case.probes:
-        lines += ["DEFINE output 1", "   SET name zsections", "   SET mode probepoint",
+        lines += ["DEFINE output 1", "   SET name zsections", f"   SET mode {case.output_mode}",
                   "   SET xgrid { 0.1, 0.1,0.6}", "   SET ygrid { 0.5, 1, 0.5}", "   SET zgrid { 0, 0.04, 1.05}",
-                  "   SET grid on", "   SET period 0", "END output 1"]
+                  "   SET grid on", f"   SET period {case.output_period!r}", "END output 1"]
     lines += ["DEFINE simulation 1", f"   SET method {case.method}", "   SET solver cg",
               f"   SET tolerance {case.tolerance!r}", "   SET mesh 1", "   SET source 1",
               f"   SET duration {duration!r}", f"   SET step {dt!r}", f"   SET courant {case.courant!r}"]

@@ -86,6 +86,42 @@ void write_outputs(tf_ctx* c) {
             << " " << std::setw(15) << s[4] << " " << std::setw(15) << s[5] << std::endl;
       }
   }
+  if (o.mode == "silo") {
+    // In place of the Silo files (Discretization.hpp:2601-2677): one binary
+    // dump per print time, <output name><simulation, 5 digits>_<dump, 5
+    // digits>.tfd, little endian:
+    //   char[8] "TFDUMP1", int32 n_nodes, n_tets, simulation, dump; double t;
+    //   double xyz[n_nodes][3]; int32 tet[n_tets][4] (0-based, ExportMesh's
+    //   orientation); double E[n_tets][3] (Whitney, barycentre); double H[n_tets][3]
+    std::vector<double> xyz;
+    std::vector<int32_t> tets;
+    if (f.mesh_arrays(&xyz, &tets)) {
+      const size_t ns = f.n_samples(), np = f.n_probes();
+      std::vector<double> t(ns), v(ns * np * 6), e(np * 3), h(np * 3);
+      f.get_probes(t.data(), v.data(), ns);
+      for (size_t k = 0; k < ns; k++) {
+        std::stringstream sn;
+        sn << o.name << std::setw(5) << std::setfill('0') << c->label << "_" << std::setw(5) << std::setfill('0')
+           << k << ".tfd";
+        std::ofstream os(sn.str(), std::ios::binary);
+        const char magic[8] = {'T', 'F', 'D', 'U', 'M', 'P', '1', 0};
+        const int32_t head[4] = {(int32_t)(xyz.size() / 3), (int32_t)(tets.size() / 4), (int32_t)c->label,
+                                 (int32_t)k};
+        for (size_t p = 0; p < np; p++)
+          for (int a = 0; a < 3; a++) {
+            e[3 * p + a] = v[(k * np + p) * 6 + a];
+            h[3 * p + a] = v[(k * np + p) * 6 + 3 + a];
+          }
+        os.write(magic, 8);
+        os.write(reinterpret_cast<const char*>(head), sizeof head);
+        os.write(reinterpret_cast<const char*>(&t[k]), sizeof(double));
+        os.write(reinterpret_cast<const char*>(xyz.data()), (std::streamsize)(xyz.size() * sizeof(double)));
+        os.write(reinterpret_cast<const char*>(tets.data()), (std::streamsize)(tets.size() * sizeof(int32_t)));
+        os.write(reinterpret_cast<const char*>(e.data()), (std::streamsize)(e.size() * sizeof(double)));
+        os.write(reinterpret_cast<const char*>(h.data()), (std::streamsize)(h.size() * sizeof(double)));
+      }
+    }
+  }
   size_t n = 0;
   f.get_flux(nullptr, 0, &n);
   std::vector<double> fl(n), lo(n);

@@ -13,8 +13,9 @@
 // row groups follow each other (stride-dimension byte offset = 128 x K / 8).
 // The FP32 accumulator (128 lanes x 64 columns) lives in tensor memory,
 // allocated once per CTA; one thread issues tcgen05.mma and tcgen05.commit,
-// whose completion arrives on an mbarrier that every thread waits on
-// (bounded), and each warp reads its 32 lanes back with tcgen05.ld.
+// whose completion arrives on an mbarrier that thread polls (bounded) while
+// the others wait in a barrier, and each warp reads its 32 lanes back with
+// tcgen05.ld after tcgen05.fence::after_thread_sync.
 // Numerics: BF16 products and FP32 accumulation as on the mma.sync path; the
 // activation works on z' = z / 2 = fma(acc, 1/2, b / 2) in FP32, packed to a
 // BF16 pair by integer adds on the bit patterns (magnitude rounded half up,
@@ -186,12 +187,17 @@ __device__ __forceinline__ bool mlp_tc_forward(MlpTcSmem& sm, uint32_t& phase, c
     tc_mma(tmem, tc_desc(sm.a1(), 128, 256), tc_desc(sm.w1, 128, 256), kId, 0);
     tc_commit(&sm.bar);
   }
-  bool ok = tc_wait(&sm.bar, phase & 1);
+  // thread 0 polls the completion; the others wait in the barrier (no
+  // issue slots spent polling) and order their TMEM reads after it
+  bool ok = tid == 0 ? tc_wait(&sm.bar, phase & 1) : true;
   phase++;
   if (!__syncthreads_and(ok)) {
     // give the MMA one more bounded wait before the caller frees its TMEM
-    if (tid == 0) atomicExch(err, 4);
-    tc_wait(&sm.bar, (phase - 1) & 1);
+    if (tid == 0) {
+      atomicExch(err, 4);
+      tc_wait(&sm.bar, (phase - 1) & 1);
+    }
+    __syncthreads();
     return false;
   }
   tc_fence_after();
@@ -218,11 +224,14 @@ __device__ __forceinline__ bool mlp_tc_forward(MlpTcSmem& sm, uint32_t& phase, c
       tc_mma(tmem, tc_desc(sm.a2 + 128 * s, 128, 1024), tc_desc(sm.w2 + 128 * s, 128, 1024), kId, s > 0 ? 1u : 0u);
     tc_commit(&sm.bar);
   }
-  ok = tc_wait(&sm.bar, phase & 1);
+  ok = tid == 0 ? tc_wait(&sm.bar, phase & 1) : true;
   phase++;
   if (!__syncthreads_and(ok)) {
-    if (tid == 0) atomicExch(err, 4);
-    tc_wait(&sm.bar, (phase - 1) & 1);
+    if (tid == 0) {
+      atomicExch(err, 4);
+      tc_wait(&sm.bar, (phase - 1) & 1);
+    }
+    __syncthreads();
     return false;
   }
   tc_fence_after();

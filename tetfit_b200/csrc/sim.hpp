@@ -59,9 +59,9 @@ class Sim {
   virtual void set_state(const double* U, const double* F) = 0;
   virtual void get_flux(double* flux, size_t cap, size_t* n) const = 0;
   // Joule loss per step (Discretization.hpp:895, :1519, :1902).  Zero unless
-  // the simulation conducts: the tetrahedral paths accept lossless materials
-  // only, and the FIT path's conductance vector is non-zero only for l2norm
-  // outputs, as in the reference.
+  // the simulation conducts: dga accepts lossless materials only, gfdtd and
+  // fem form it from SigMat, and the FIT path's conductance vector is
+  // non-zero only for l2norm outputs, as in the reference.
   virtual void get_losses(double* loss, size_t cap, size_t* n) const {
     const uint64_t s = step_index();
     const size_t m = s < cap ? (size_t)s : cap;
@@ -93,6 +93,13 @@ class Sim {
   virtual size_t training_loss(float* loss, size_t cap) const {
     (void)loss; (void)cap;
     return 0;
+  }
+  // Tetrahedral mesh of the silo-mode field dumps: node coordinates and the
+  // tets' node ids (0-based), each tet ordered as the reference's ExportMesh
+  // writes it (Discretization.hpp:2354-2376).  False without a tet mesh.
+  virtual bool mesh_arrays(std::vector<double>* xyz, std::vector<int32_t>* tets) const {
+    (void)xyz; (void)tets;
+    return false;
   }
 };
 

@@ -327,7 +327,7 @@ TetSim::TetSim(Script& sc, uint32_t label, const RunOptions& opt, bool device)
   // gfdtd exports U^{i-1} inside step i (index i-1 <-> (i-1) dt)
   const uint64_t nsched = method_ == 1 ? nsteps_ + 1 : nsteps_;
   slot_of_step_.assign(nsched + 1, -1);
-  if (out_.mode == "probepoint") {
+  if (out_.mode == "probepoint" || out_.mode == "silo") {
     Output o = out_;
     for (uint64_t i = 0; i < nsched; i++) {
       // gfdtd stamps the export of loop step i+1 as current_time - t_step
@@ -355,7 +355,7 @@ int TetSim::kernels_per_step() const {
 
 void TetSim::release_host() {
   auto drop = [](auto& v) { std::remove_reference_t<decltype(v)>().swap(v); };
-  for (HostCsr* m : {&Ct_, &N_, &H_, &E_, &A_, &R_}) {
+  for (HostCsr* m : {&Ct_, &N_, &H_, &E_, &A_, &R_, &Sig_}) {
     drop(m->ptr);
     drop(m->col);
     drop(m->val);
@@ -417,8 +417,10 @@ void TetSim::read_mesh() {
     V3 v1 = sub(pts_[t[1]], pts_[t[0]]), v2 = sub(pts_[t[2]], pts_[t[0]]), v3 = sub(pts_[t[3]], pts_[t[0]]);
     cell_vol_[k] = dot(v1, cross(v2, v3)) / 6.0;
     const Material& mt = sc_.materials[vol_mat_[k]];
-    if (!is_zero(mt.sigma) || !is_zero(mt.chi))
-      throw UnsupportedError("lossy materials (sigma or chi) on tetrahedra are outside the supported path");
+    // conductivity enters gfdtd and fem through SigMat; dga's lossy
+    // ("fractured") edge classes and magnetic losses (chi) are not built
+    if (!is_zero(mt.chi) || (method_ == 1 && !is_zero(mt.sigma)))
+      throw UnsupportedError("lossy materials (chi on tetrahedra, or sigma with dga) are outside the supported path");
   }
   // faces: packed keys when node ids fit in 21 bits, else tuple order
   const bool packed = np < (1u << 21);
@@ -656,6 +658,19 @@ void TetSim::build_ops() {
     return V3{(a[0] + b[0] + c[0]) / 3.0, (a[1] + b[1] + c[1]) / 3.0, (a[2] + b[2] + c[2]) / 3.0};
   };
   const int nth = opt_.setup_threads;
+  // conducting tets (gfdtd, fem): sigma with a non-zero determinant, the
+  // reference's test (Discretization.hpp:8604, 8041), by cofactor expansion
+  // along the first row
+  std::vector<uint8_t> sig_tet(L, 0);
+  lossy_ = false;
+  if (method_ >= 2)
+    for (uint32_t v = 0; v < L; v++) {
+      const auto& m = sc_.materials.at(vol_mat_[v]).sigma.m;
+      const double det = m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) -
+                         m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
+                         m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+      if (det != 0) sig_tet[v] = 1, lossy_ = true;
+    }
   // N = sum of per-tet inverse magnetic blocks (Discretization.hpp:8754-8807, 9158-9255);
   // the blocks are formed in parallel, then listed in tet order
   {
@@ -804,7 +819,7 @@ void TetSim::build_ops() {
     // the 4 face barycentres) / 40 of w_k . eps w_j.  Entries j <= k, then
     // their mirror, zero values skipped, listed in tet order.
     static const int kWe[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
-    std::vector<double> blk(36 * (size_t)L);
+    std::vector<double> blk(36 * (size_t)L), sblk(lossy_ ? 36 * (size_t)L : 0, 0.0);
     parallel_for(L, nth, [&](int64_t v0, int64_t v1) {
       for (uint32_t v = (uint32_t)v0; v < (uint32_t)v1; v++) {
         const V3& x0 = pts_[vols_[v][0]];
@@ -817,7 +832,9 @@ void TetSim::build_ops() {
         g[3] = scale(cross(c1, c2), 1.0 / det);
         for (int a = 0; a < 3; a++) g[0][a] = -(g[1][a] + g[2][a] + g[3][a]);
         const Mat3& eps = sc_.materials.at(vol_mat_[v]).eps;
-        double acc[2][6][6] = {};
+        const Mat3& sig = sc_.materials.at(vol_mat_[v]).sigma;
+        const bool cond = sig_tet[v] != 0;
+        double acc[2][6][6] = {}, accs[2][6][6] = {};
         auto add_point = [&](const V3& p, int which) {
           const V3 d = sub(p, x0);
           double l[4];
@@ -833,6 +850,11 @@ void TetSim::build_ops() {
           }
           for (int j = 0; j < 6; j++)
             for (int k = j; k < 6; k++) acc[which][j][k] += dot(w[k], ew[j]);
+          if (cond) {  // SigMat by the same quadrature (:8020-8021)
+            for (int k = 0; k < 6; k++) ew[k] = mv(sig, w[k]);
+            for (int j = 0; j < 6; j++)
+              for (int k = j; k < 6; k++) accs[which][j][k] += dot(w[k], ew[j]);
+          }
         };
         for (int h = 0; h < 4; h++) {
           add_point(pts_[vols_[v][h]], 0);
@@ -843,6 +865,10 @@ void TetSim::build_ops() {
           for (int k = 0; k < 6; k++)
             blk[36 * (size_t)v + 6 * j + k] =
                 k >= j ? V * (acc[0][j][k] + acc[1][j][k] * 9.0) / 40.0 : 0.0;
+        if (cond)
+          for (int j = 0; j < 6; j++)
+            for (int k = 0; k < 6; k++)
+              sblk[36 * (size_t)v + 6 * j + k] = k >= j ? V * (accs[0][j][k] + accs[1][j][k] * 9.0) / 40.0 : 0.0;
       }
     });
     std::vector<int64_t> off(L + 1, 0);
@@ -868,18 +894,33 @@ void TetSim::build_ops() {
       }
     });
     E_ = HostCsr::build(NE, NE, t, nth);
+    if (lossy_) {  // SigMat entries, zero values skipped, tet order (:8041-8051)
+      HostCsr::Trips ts;
+      for (uint32_t v = 0; v < L; v++) {
+        if (!sig_tet[v]) continue;
+        auto el = vol_edges(v);
+        for (int j = 0; j < 6; j++)
+          for (int k = j; k < 6; k++) {
+            const double x = sblk[36 * (size_t)v + 6 * j + k];
+            if (x == 0) continue;
+            ts.push_back({(uint32_t)el[j], (uint32_t)el[k], x});
+            if (k != j) ts.push_back({(uint32_t)el[k], (uint32_t)el[j], x});
+          }
+      }
+      Sig_ = HostCsr::build(NE, NE, ts, nth);
+    }
     dt_est_ = sim_.courant * estimate_dt(E_, true);
     dt_ = dt_est_;
     if (sim_.step != 0) {  // Discretization.hpp:8029-8036
       if (sim_.step > dt_) unstable_ = true;
       else dt_ = sim_.step;
     }
-    // SysMat = E * (1 / (dt dt)) (:8086-8093)
-    split_system(1.0 / (dt_ * dt_));
+    // SysMat = E * (1 / (dt dt)) + (0.5 / dt) SigMat (:8086-8093)
+    split_system(1.0 / (dt_ * dt_), 0.5 / dt_);
   } else {
     // gfdtd eps-mass from the node dual bases (Discretization.hpp:8357-8621):
     // nine entries per (node, tet) pair at fixed positions, formed in parallel
-    HostCsr::Trips t(9 * nvol_.size());
+    HostCsr::Trips t(9 * nvol_.size()), ts(lossy_ ? 9 * nvol_.size() : 0);
     parallel_for((int64_t)pts_.size(), nth, [&](int64_t n0, int64_t n1) {
       for (uint32_t nid = (uint32_t)n0; nid < (uint32_t)n1; nid++)
         for (int64_t q = nvol_ptr_[nid]; q < nvol_ptr_[nid + 1]; q++) {
@@ -909,15 +950,34 @@ void TetSim::build_ops() {
             t[9 * q + k2] = {(uint32_t)e[pq[0]], (uint32_t)e[pq[1]],
                              quarter * sg[pq[0]] * sg[pq[1]] * dot(f[pq[0]], mv(oe, f[pq[1]]))};
           }
+          if (lossy_) {  // SigMat: the same basis with sigma on conducting tets (:8604-8616)
+            const Mat3& sig = sc_.materials.at(vol_mat_[vv]).sigma;
+            Mat3 os;
+            for (int i = 0; i < 3; i++)
+              for (int j = 0; j < 3; j++) os.m[i][j] = om * sig.m[i][j];
+            for (int k2 = 0; k2 < 9; k2++) {
+              const int* pq = kPair[k2];
+              ts[9 * q + k2] = {(uint32_t)e[pq[0]], (uint32_t)e[pq[1]],
+                                sig_tet[vv] ? quarter * sg[pq[0]] * sg[pq[1]] * dot(f[pq[0]], mv(os, f[pq[1]]))
+                                            : 0.0};
+            }
+          }
         }
     });
     E_ = HostCsr::build(NE, NE, t, nth);
-    split_system(1.0);
+    if (lossy_) Sig_ = HostCsr::build(NE, NE, ts, nth);
     auto te = std::chrono::steady_clock::now();
     dt_est_ = sim_.courant * estimate_dt(E_, true);
     if (opt_.verbose)
       std::printf("  set-up %-14s %8.3f s\n", "(dt estimate)",
                   std::chrono::duration<double>(std::chrono::steady_clock::now() - te).count());
+    dt_ = dt_est_;
+    if (sim_.step != 0) {  // Discretization.hpp:8634-8641
+      if (sim_.step > dt_) unstable_ = true;
+      else dt_ = sim_.step;
+    }
+    // SysMat = E + (0.5 dt) SigMat (:8644)
+    split_system(1.0, 0.5 * dt_);
   }
   if (method_ != 3) dt_ = dt_est_;
   if (method_ != 3 && sim_.step != 0) {  // Discretization.hpp:9146-9153, 8634-8641
@@ -926,11 +986,13 @@ void TetSim::build_ops() {
   }
 }
 
-// A (free x free) and R (free x Dirichlet) split the rows of scale * E: the
-// system of gfdtd (scale 1) and of fem (scale 1 / dt^2).  The free numbering
-// fidx is increasing in the edge index, so each split row keeps E's sorted,
-// merged column order: the rows are copied, not re-sorted.
-void TetSim::split_system(double scale) {
+// A (free x free) and R (free x Dirichlet) split the rows of SysMat =
+// scale * E + sig_coef * SigMat: the system of gfdtd (scale 1, sig_coef dt/2)
+// and of fem (scale 1 / dt^2, sig_coef 0.5 / dt); SigMat only with conducting
+// tets.  The free numbering fidx is increasing in the edge index, so each
+// split row keeps the sorted, merged column order: the rows are merged, not
+// re-sorted.
+void TetSim::split_system(double scale, double sig_coef) {
   const uint32_t NE = (uint32_t)edges_.size();
   const int nth = opt_.setup_threads;
   {
@@ -949,11 +1011,29 @@ void TetSim::split_system(double scale) {
     R_.ncols = NE;
     A_.ptr.assign(nf + 1, 0);
     R_.ptr.assign(nf + 1, 0);
-    parallel_for(nf, nth, [&](int64_t i0, int64_t i1) {
-      for (int64_t i = i0; i < i1; i++) {
-        const int32_t r = free_edges_[i];
-        for (int64_t k = E_.ptr[r]; k < E_.ptr[r + 1]; k++) (fidx[E_.col[k]] < 0 ? R_.ptr[i + 1] : A_.ptr[i + 1])++;
+    // row r of SysMat: E's and SigMat's entries merged by column,
+    // E_rc scale + coef S_rc where both hold one (the sum the reference forms)
+    const bool sg = lossy_;
+    auto row = [&](int32_t r, auto&& f) {
+      int64_t k = E_.ptr[r], ks = sg ? Sig_.ptr[r] : 0;
+      const int64_t ke = E_.ptr[r + 1], kse = sg ? Sig_.ptr[r + 1] : 0;
+      while (k < ke || ks < kse) {
+        if (ks >= kse || (k < ke && E_.col[k] < Sig_.col[ks])) {
+          f(E_.col[k], scale == 1.0 ? E_.val[k] : E_.val[k] * scale);
+          k++;
+        } else if (k >= ke || Sig_.col[ks] < E_.col[k]) {
+          f(Sig_.col[ks], sig_coef * Sig_.val[ks]);
+          ks++;
+        } else {
+          f(E_.col[k], (scale == 1.0 ? E_.val[k] : E_.val[k] * scale) + sig_coef * Sig_.val[ks]);
+          k++;
+          ks++;
+        }
       }
+    };
+    parallel_for(nf, nth, [&](int64_t i0, int64_t i1) {
+      for (int64_t i = i0; i < i1; i++)
+        row(free_edges_[i], [&](int32_t c, double) { (fidx[c] < 0 ? R_.ptr[i + 1] : A_.ptr[i + 1])++; });
     });
     for (uint32_t i = 0; i < nf; i++) {
       A_.ptr[i + 1] += A_.ptr[i];
@@ -965,11 +1045,8 @@ void TetSim::split_system(double scale) {
     R_.val.resize(R_.ptr[nf]);
     parallel_for(nf, nth, [&](int64_t i0, int64_t i1) {
       for (int64_t i = i0; i < i1; i++) {
-        const int32_t r = free_edges_[i];
         int64_t wa = A_.ptr[i], wr = R_.ptr[i];
-        for (int64_t k = E_.ptr[r]; k < E_.ptr[r + 1]; k++) {
-          const int32_t c = E_.col[k];
-          const double v = scale == 1.0 ? E_.val[k] : E_.val[k] * scale;
+        row(free_edges_[i], [&](int32_t c, double v) {
           if (fidx[c] < 0) {
             R_.col[wr] = c;
             R_.val[wr++] = v;
@@ -977,7 +1054,7 @@ void TetSim::split_system(double scale) {
             A_.col[wa] = fidx[c];
             A_.val[wa++] = v;
           }
-        }
+        });
       }
     });
     jacobi_.resize(nf);
@@ -1315,9 +1392,25 @@ void TetSim::locate_probes() {
     }
     return walk(pv);
   };
-  if (out_.mode == "probepoint") {
-    for (auto& pv : out_.probes) {
-      int64_t v = find(pv);
+  // silo mode: the reference writes E (Whitney, at the barycentre) and H of
+  // every tet at each print time (ExportFields, Discretization.hpp:2601-2677);
+  // here every tet is a sample point at its barycentre, (p0+p1+p2+p3)/4
+  // (vol_barycenter, :10479-10484), through the same weights as a probe
+  const bool silo = out_.mode == "silo";
+  std::vector<std::pair<int64_t, V3>> where;
+  if (out_.mode == "probepoint")
+    for (auto& pv : out_.probes) where.push_back({find(pv), pv});
+  if (silo) {
+    where.reserve(L);
+    for (uint32_t v = 0; v < L; v++) {
+      const auto& n = vols_[v];
+      V3 b;
+      for (int a = 0; a < 3; a++) b[a] = (pts_[n[0]][a] + pts_[n[1]][a] + pts_[n[2]][a] + pts_[n[3]][a]) / 4.0;
+      where.push_back({(int64_t)v, b});
+    }
+  }
+  for (auto& [v, pv] : where) {
+    {
       if (v < 0) continue;
       probe_tet_.push_back((int32_t)v);
       probe_pts_.push_back(pv);
@@ -1367,8 +1460,11 @@ void TetSim::locate_probes() {
       for (int q = 0; q < 4; q++)
         for (int a = 0; a < 3; a++) probe_hf_.push_back(0.25 * (1.0 / mu.m[a][a]) * hq[q][a] / vv);
     }
-    // current dipoles: nearest edge of the star of the tet's first node
-    // (Discretization.hpp:436-464)
+  }
+  // current dipoles: nearest edge of the star of the tet's first node
+  // (Discretization.hpp:431-464); the reference locates them only in the
+  // probepoint and maxerror output modes (:378), and so does this
+  if (out_.mode == "probepoint" || out_.mode == "maxerror") {
     for (uint32_t sl : src_labels_) {
       Source& s = sc_.sources[sl];
       if (s.st != "j") continue;
@@ -1388,6 +1484,28 @@ void TetSim::locate_probes() {
       edge_src_[best].push_back(sl);
     }
   }
+}
+
+bool TetSim::mesh_arrays(std::vector<double>* xyz, std::vector<int32_t>* tets) const {
+  if (xyz) {
+    xyz->resize(3 * pts_.size());
+    for (size_t n = 0; n < pts_.size(); n++)
+      for (int a = 0; a < 3; a++) (*xyz)[3 * n + a] = pts_[n][a];
+  }
+  if (tets) {
+    // positive volume: nodes 0 1 2 3, else 0 2 1 3 (ExportMesh, :2358-2373)
+    tets->resize(4 * vols_.size());
+    for (size_t v = 0; v < vols_.size(); v++) {
+      const auto& n = vols_[v];
+      const bool pos = cell_vol_[v] > 0;
+      int32_t* o = &(*tets)[4 * v];
+      o[0] = n[0];
+      o[1] = pos ? n[1] : n[2];
+      o[2] = pos ? n[2] : n[1];
+      o[3] = n[3];
+    }
+  }
+  return true;
 }
 
 // ------------------------------------------------------------------ device
@@ -1730,6 +1848,11 @@ void TetSim::get_flux(double* flux, size_t cap, size_t* n) const {
   size_t m = step_ < cap ? step_ : cap;
   if (flux && m) CU(cudaMemcpy(flux, dp_.flux, m * 8, cudaMemcpyDeviceToHost));
   if (n) *n = step_;
+}
+
+void TetSim::get_losses(double* loss, size_t cap, size_t* n) const {
+  if (group_) return group_->get_losses(0, loss, cap, n);
+  Sim::get_losses(loss, cap, n);  // dga: lossless here
 }
 
 size_t TetSim::solver_stats(int32_t* iters, double* resid, size_t cap) const {

@@ -74,6 +74,8 @@ class TetSim : public Sim {
   size_t guess_stats(int8_t* kept, size_t cap) const override;
   int kernel_variant() const override;
   size_t training_loss(float* loss, size_t cap) const override;
+  bool mesh_arrays(std::vector<double>* xyz, std::vector<int32_t>* tets) const override;
+  void get_losses(double* loss, size_t cap, size_t* n) const override;
   uint64_t n_free() const override { return free_edges_.size(); }
   uint64_t nnz_system() const override { return A_.val.size(); }
   // nonzeros of the step's main operator: H (dga) or E (gfdtd)
@@ -85,7 +87,7 @@ class TetSim : public Sim {
   void read_mesh();
   void classify();
   void build_ops();
-  void split_system(double scale);
+  void split_system(double scale, double sig_coef = 0.0);
   double estimate_dt(const HostCsr& Minv_or_E, bool generalized);
   void locate_probes();
   void build_sources();
@@ -121,7 +123,9 @@ class TetSim : public Sim {
   std::vector<std::vector<uint32_t>> edge_src_;
   // operators
   HostCsr Ct_;                                     // E x F, +-1 (C transposed)
-  HostCsr N_, H_, E_, A_, R_;                      // R_: eps-mass, free rows x Dirichlet cols
+  HostCsr N_, H_, E_, A_, R_;                      // R_: SysMat, free rows x Dirichlet cols
+  HostCsr Sig_;                                    // conductivity mass SigMat (gfdtd, fem; lossy_ only)
+  bool lossy_ = false;                             // some tet conducts
   std::vector<int32_t> free_edges_, dir_edges_;
   std::vector<double> jacobi_;
   // sources

@@ -111,7 +111,10 @@ TetGroup::~TetGroup() {
 template <typename T>
 void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
   const int S = (int)sims.size();
-  SellHost<T> A, Ef, N, Ct;
+  SellHost<T> A, Ef, N, Ct, Sg, Sa;
+  std::vector<int32_t> sa_edge;
+  std::vector<uint16_t> sa_slice_sim;
+  std::vector<uint8_t> lossy(S, 0);
   std::vector<int32_t, default_init_allocator<int32_t>> fte, free_edge;  // filled completely
   std::vector<int32_t> dir_edge;
   std::vector<T, default_init_allocator<T>> pre, U0, I0, Src0;
@@ -202,6 +205,32 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
           v = t.E_.val[q];
         },
         [&](int64_t) { return (int32_t)eoff; }, true, opt_.setup_threads);
+    // SigMat rows of the free edges (empty for a member without conducting
+    // tets), in the rows' order, for the right-hand side
+    const bool sig = t.lossy_;
+    lossy[s] = sig ? 1 : 0;
+    Sg.append(
+        nfp, nf, [&](int64_t p) { return sig ? t.Sig_.ptr[erow(p) + 1] - t.Sig_.ptr[erow(p)] : (int64_t)0; },
+        [&](int64_t p, int j, int32_t& c, double& v) {
+          const int64_t q = t.Sig_.ptr[erow(p)] + j;
+          c = (int32_t)(eoff + t.Sig_.col[q]);
+          v = t.Sig_.val[q];
+        },
+        [&](int64_t) { return (int32_t)eoff; }, true, opt_.setup_threads);
+    if (sig) {
+      // every edge's SigMat row, in edge order, for the Joule losses
+      const int64_t NEp = up32(NE);
+      Sa.append(
+          NEp, NE, [&](int64_t e) { return t.Sig_.ptr[e + 1] - t.Sig_.ptr[e]; },
+          [&](int64_t e, int j, int32_t& c, double& v) {
+            const int64_t q = t.Sig_.ptr[e] + j;
+            c = (int32_t)(eoff + t.Sig_.col[q]);
+            v = t.Sig_.val[q];
+          },
+          [&](int64_t) { return (int32_t)eoff; }, true, opt_.setup_threads);
+      for (int64_t e = 0; e < NEp; e++) sa_edge.push_back(e < NE ? (int32_t)(eoff + e) : -1);
+      sa_slice_sim.insert(sa_slice_sim.end(), NEp / 32, (uint16_t)s);
+    }
     Ct.append(
         nfp, nf, [&](int64_t p) { return t.Ct_.ptr[erow(p) + 1] - t.Ct_.ptr[erow(p)]; },
         [&](int64_t p, int j, int32_t& c, double& v) {
@@ -352,6 +381,22 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
   };
   put(N, d.N, true);
   put(Ef, d.Ef, true);
+  lossy_host_.assign(lossy.begin(), lossy.end());
+  if (std::find(lossy.begin(), lossy.end(), 1) != lossy.end()) {
+    // conducting members: SigMat terms of the right-hand side, and the
+    // Joule-loss reduction over every edge's row
+    put(Sg, d.Sg, true);
+    put(Sa, d.Sa, true);
+    d.lossy = (const uint8_t*)upload(lossy);
+    d.nsa = (int64_t)sa_edge.size();
+    d.sa_edge = (const int32_t*)upload(sa_edge);
+    d.sa_slice_sim = (const uint16_t*)upload(sa_slice_sim);
+    d.loss_part = (double*)dalloc(sizeof(double) * (size_t)(d.nsa / 32));
+    std::vector<int> sim_sa(S + 1, 0);
+    for (uint16_t q : sa_slice_sim) sim_sa[q + 1]++;
+    for (int q = 0; q < S; q++) sim_sa[q + 1] += sim_sa[q];
+    d.sim_sa = (const int*)upload(sim_sa);
+  }
   put(Ct, d.Ct, false);
   put(A, d.A, true);
   d.pre = upload(pre);
@@ -423,6 +468,10 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
   CU(cudaMemset(d.cg_resid, 0, sizeof(double) * stat));
   CU(cudaMemset(d.cg_limit, 0, sizeof(int32_t) * stat));
   CU(cudaMemset(d.flux, 0, sizeof(double) * stat));
+  if (d.lossy) {
+    d.loss_a = (double*)dalloc(sizeof(double) * stat);
+    CU(cudaMemset(d.loss_a, 0, sizeof(double) * stat));
+  }
   d.stat_off = (const int64_t*)upload(stat_off);
   d.sim_se = (const int*)upload(sim_se);
   d.se_edge = (const int32_t*)upload(se_edge);
@@ -819,6 +868,29 @@ bool TetGroup::mlp_params(float* out) const {
   if (!mlp_.params) return false;
   if (out) CU(cudaMemcpy(out, mlp_.params, sizeof(float) * kNParam, cudaMemcpyDeviceToHost));
   return true;
+}
+
+// poynting.dat's third column for gfdtd and fem (Discretization.hpp
+// :1518-1546, :1733-1757): the reference pushes 0.5 a_{i-1} before the solve
+// of step i and, from step 2 on, a_i after it, with a_j = U_j^T SigMat U_j,
+// and prints the first n entries: 0.5 a_0, then 0.5 a_{(k+1)/2} for odd k and
+// a_{k/2+1} for even k.  a_{j} is formed at the start of step j + 1.
+void TetGroup::get_losses(int s, double* loss, size_t cap, size_t* n) const {
+  const Meta& m = meta_[s];
+  const size_t k = (size_t)m.step;
+  if (n) *n = k;
+  if (!loss) return;
+  const size_t w = std::min(k, cap);
+  if (!dev_.loss_a || !dev_.lossy || !lossy_host_[s]) {
+    std::fill(loss, loss + w, 0.0);
+    return;
+  }
+  std::vector<double> a(k);
+  if (k) CU(cudaMemcpy(a.data(), dev_.loss_a + m.stat_off, k * 8, cudaMemcpyDeviceToHost));
+  for (size_t q = 0; q < w; q++) {
+    const size_t j = q == 0 ? 0 : (q % 2 ? (q + 1) / 2 : q / 2 + 1);
+    loss[q] = (q == 0 || q % 2) ? 0.5 * a[j] : a[j];
+  }
 }
 
 void TetGroup::get_flux(int s, double* flux, size_t cap, size_t* n) const {

@@ -50,10 +50,13 @@ class TetGroup {
   // current network parameters (kNParam floats); false without warm_start 3
   bool mlp_params(float* out) const;
   void get_flux(int s, double* flux, size_t cap, size_t* n) const;
+  void get_losses(int s, double* loss, size_t cap, size_t* n) const;
   // leapfrog energy of member s on the GPU (see grp_energy)
   double energy(int s);
   uint64_t device_bytes() const { return dev_bytes_; }
-  int kernels_per_step() const { return 7 + (dev_.np ? 1 : 0) + (opt_.warm_start == 3 ? 2 : 0); }
+  int kernels_per_step() const {
+    return 7 + (dev_.np ? 1 : 0) + (opt_.warm_start == 3 ? 2 : 0) + (dev_.nsa ? 2 : 0);
+  }
   int cg_blocks() const { return cg_blocks_; }
   int cg_variant() const { return cg_variant_; }
   uint64_t total_dofs() const { return dofs_; }
@@ -97,6 +100,7 @@ class TetGroup {
   double* pinned_ = nullptr;
   size_t pinned_len_ = 0, io_src_ = 0, io_probe_ = 0;
   std::vector<double> carrier_host_;
+  std::vector<uint8_t> lossy_host_;  // member has conducting tets
   // learned warm start
   MlpTrain mlp_{};
   int64_t launched_ = 0;     // steps launched so far (group clock of the training schedule)

@@ -333,12 +333,21 @@ __global__ void __launch_bounds__(kGB) grp_rhs(GroupDev d) {
   // (the source values live on the Dirichlet columns only).  fem sums in
   // FP64: its right-hand side is dominated by E U / dt^2 terms whose
   // difference carries the update, so FP32 sums would lose it.
-  double eu_fem = 0.0;
+  double eu_fem = 0.0, su_fem = 0.0;
   if (fem)
     eu_fem = sell_dot<double>(d.Ef, i, [&](int32_t c) {
       return 2.0 * (double)U[c] - (double)Uo[c] - (double)S[c];
     }, (const T*)nullptr);
-  const T eu = fem ? (T)0 : sell_dot<T>(d.Ef, i, [&](int32_t c) { return U[c] - S[c]; });
+  T eu = fem ? (T)0 : sell_dot<T>(d.Ef, i, [&](int32_t c) { return U[c] - S[c]; });
+  // conducting members: SysMat = scale E + coef SigMat, so the SigMat rows add
+  // gfdtd  - (dt/2) SigMat U_old - (dt/2) SigMat_dir SrcFld   (:1516-1519)
+  // fem    + (0.5/dt) SigMat U_older - (0.5/dt) SigMat_dir SrcFld   (:1729-1731)
+  if (d.lossy && d.lossy[s]) {
+    if (fem)
+      su_fem = sell_dot<double>(d.Sg, i, [&](int32_t c) { return (double)Uo[c] - (double)S[c]; }, (const T*)nullptr);
+    else
+      eu -= (T)(0.5 * d.dt[s]) * sell_dot<T>(d.Sg, i, [&](int32_t c) { return U[c] + S[c]; });
+  }
   // C^T F over the edge's faces in stored order; the face indices of 4
   // entries are loaded before their gathers (padding entries hold kPadCol
   // and add nothing)
@@ -366,8 +375,8 @@ __global__ void __launch_bounds__(kGB) grp_rhs(GroupDev d) {
     // Psi = (2 E U_old - E U_older - E_dir SrcFld) / dt^2 - C^T N C U_old
     //       + (Fb - Fb_old) / dt - I / dt   (Discretization.hpp:1713-1716)
     const double idt = 1.0 / d.dt[s];
-    ((T*)d.rhs)[i] = (T)(eu_fem * (idt * idt) - (double)cf + idt * (double)((const T*)d.cb)[e] -
-                         idt * (double)((const T*)d.I)[e]);
+    ((T*)d.rhs)[i] = (T)(eu_fem * (idt * idt) + (0.5 * idt) * su_fem - (double)cf +
+                         idt * (double)((const T*)d.cb)[e] - idt * (double)((const T*)d.I)[e]);
   } else {
     ((T*)d.rhs)[i] = eu - dt * ((const T*)d.I)[e] + dt * cf + dt * ((const T*)d.cb)[e];
   }
@@ -917,6 +926,35 @@ __global__ void __launch_bounds__(kGB) grp_scatter(GroupDev d) {
   }
 }
 
+// Joule-loss term of conducting members at the start of a step, with U the
+// previous step's state: one warp per 32-row slice of Sa writes the slice's
+// sum of U_e (SigMat U)_e in FP64 (fixed shuffle tree)...
+template <typename T>
+__global__ void __launch_bounds__(kGB) grp_loss_rows(GroupDev d) {
+  const int64_t i = (int64_t)blockIdx.x * kGB + threadIdx.x;
+  if (i >= d.nsa) return;
+  const int s = d.sa_slice_sim[i >> 5];
+  const T* U = (const T*)d.U;
+  double a = 0.0;
+  const int32_t e = d.sa_edge[i];
+  if (running(d, s) && e >= 0)
+    a = (double)U[e] * sell_dot<double>(d.Sa, i, [&](int32_t c) { return (double)U[c]; }, (const T*)nullptr);
+  a = warp_sum(a);
+  if ((threadIdx.x & 31) == 0) d.loss_part[i >> 5] = a;
+}
+
+// ... and one warp per member adds its slices' sums in slice order into
+// loss_a[stat_off + step]
+__global__ void grp_loss_sum(GroupDev d) {
+  const int s = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (s >= d.S || !d.lossy[s] || !running(d, s)) return;
+  double a = 0.0;
+  for (int g = d.sim_sa[s] + lane; g < d.sim_sa[s + 1]; g += 32) a += d.loss_part[g];
+  a = warp_sum(a);
+  if (lane == 0) d.loss_a[d.stat_off[s] + d.step[s]] = a;
+}
+
 __global__ void grp_bump(GroupDev d) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < d.S && d.step[s] < d.nsteps[s]) d.step[s] += 1;
@@ -980,6 +1018,10 @@ template <typename T>
 cudaError_t group_launch_step(const GroupDev& d, int cg_blocks, int cg_variant, size_t smem, cudaStream_t st,
                               cudaEvent_t* ev) {
   if (ev) cudaEventRecord(ev[0], st);
+  if (d.nsa > 0) {  // Joule losses of the conducting members, before U changes
+    grp_loss_rows<T><<<gblk(d.nsa), kGB, 0, st>>>(d);
+    grp_loss_sum<<<(unsigned)((d.S * 32 + 255) / 256), 256, 0, st>>>(d);
+  }
   grp_curl_u<T><<<gblk(d.nF), kGB, 0, st>>>(d);
   grp_nmul<T><<<gblk(d.nF), kGB, 0, st>>>(d);
   if (d.np) grp_probes<T><<<(unsigned)((d.np + 127) / 128), 128, 0, st>>>(d);

@@ -62,6 +62,19 @@ struct GroupDev {
   SellDev Ef;                    // free rows x edges: eps-mass rows of the free edges
   SellDev Ct;                    // free rows x faces, +-1
   SellDev A;                     // free rows x free rows
+  // conducting members (SigMat, gfdtd and fem): Sg the SigMat rows of the
+  // free edges (empty rows for the other members) for the right-hand side;
+  // Sa every edge's SigMat row of the conducting members, member by member
+  // (32-row slices of one member, sa_edge the row's edge or -1), for the
+  // per-step Joule-loss term a = U^T SigMat U into loss_a[stat_off + step]
+  SellDev Sg, Sa;
+  const uint8_t* lossy = nullptr;
+  int64_t nsa = 0;
+  const int32_t* sa_edge = nullptr;
+  const uint16_t* sa_slice_sim = nullptr;
+  const int* sim_sa = nullptr;   // [S + 1] first Sa slice of each member
+  double* loss_part = nullptr;   // [nsa / 32] slice partials
+  double* loss_a = nullptr;      // [stat]
   const void* pre = nullptr;     // Jacobi 1/diag (0 on padding rows)
   const int32_t* free_edge = nullptr;
   const int32_t* dir_edge = nullptr;
