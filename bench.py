@@ -511,7 +511,8 @@ def run_batch(args, rank, world, local_rank):
         b.step_io(member_carriers(infos, cases, [d_ + k for d_ in done]), probes)
     e2e_s = time.perf_counter() - t0
     barrier()
-    smallest = sorted(range(len(cases)), key=lambda q: (cases[q].n, q))[:3]
+    # the CPU oracle steps members of up to 24^3 cubes within the bench's time
+    smallest = [q for q in sorted(range(len(cases)), key=lambda q: (cases[q].n, q))[:3] if cases[q].n <= 24]
     check = sorted(set(_sample_members(cases)) | set(smallest)) if rank == 0 else []
     fp32_probes = {m: b.probes(m) for m in check}
     kps = infos[0]["kernels_per_step"]
