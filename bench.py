@@ -318,7 +318,9 @@ def run_ours(args, rank, world, local_rank):
                        "dofs": dofs, "cells": info["n_cells"], "parallelism": f"replicas x{world}",
                        "l2": l2_note(info, es), "setup_s": round(setup_s, 2), "autotune_steps": tune, **extra},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": fit_traffic_estimate(dom, es, dom_bytes),
+                         "traffic_note": FIT_TRAFFIC_NOTE if fit_traffic_estimate(dom, es, dom_bytes) else None,
                          "algorithmic_bytes": dom_bytes, "launch_ms": dom_ms},
             "phases_ms_per_step": {k: v / nph for k, v in zip(phase_names(info), ms5)},
             "e2e": {"value": world * dofs * K2 / max_e2e, "unit": "dof-steps/s",
@@ -363,6 +365,20 @@ def precision_report(script, device, steps=400, every=100):
         "energy": [{"step": every * (q + 1), "fp64": a, "fp32": b, "rel_diff": abs(b - a) / max(abs(a), 1e-300)}
                    for q, (a, b) in enumerate(zip(e64, e32))],
     }
+
+
+# DRAM traffic of the FIT class kernels measured by ncu (one launch each of
+# the 256^3 scene, state 607 MB > L2): fit_e_class 691.8 MB against 709.4 MB
+# algorithmic, fit_h_class 697.6 MB against 708.2 MB.  The ratio is per byte
+# (one plane per block, the same re-use at every size), reported for the
+# dominant kernel as ratio x its algorithmic bytes.
+FIT_DRAM_OVER_ALGORITHMIC = {("fit_e_class", 4): 0.975, ("fit_h_class", 4): 0.985}
+FIT_TRAFFIC_NOTE = "ncu DRAM bytes / algorithmic bytes of the kernel at 256^3, times this launch's algorithmic bytes"
+
+
+def fit_traffic_estimate(kernel, es, nbytes):
+    r = FIT_DRAM_OVER_ALGORITHMIC.get((kernel, es))
+    return None if r is None else r * nbytes
 
 
 def cg_bytes_per_launch(infos, its, es, dual=False):

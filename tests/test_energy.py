@@ -106,7 +106,9 @@ def test_tet_cavity_energy_drift(tmp_path, product_lib, oracle_lib, method):
         me_dot = lambda a, b: np.dot(a, E @ b)
     off = int(4 * w / dt + 30 * w / dt) + 2
     with tb.Discretization(s) as d:
-        d.prepare(1, precision="fp64", cg_criterion="rhs", cg_maxiter=1000)
+        # the reference's stopping test, ||r|| <= 1e-14 ||r_0||, r_0 from the
+        # previous solution: the oracle drifts 7e-16 over these steps with it
+        d.prepare(1, precision="fp64", cg_maxiter=1000)
         d.step(off)
 
         def energy():
@@ -131,7 +133,6 @@ def test_tet_cavity_energy_drift(tmp_path, product_lib, oracle_lib, method):
             assert abs(g0 - w_np) / w_np <= 1e-12, (g0, w_np)
             d.step(998)
             g1 = d.energy()
-            assert abs(g1 - g0) / g0 <= 1e-10, f"GPU energy drift {abs(g1 - g0) / g0:.3e}"
+            assert abs(g1 - g0) / g0 <= 1e-12, f"GPU energy drift {abs(g1 - g0) / g0:.3e}"
     assert w0 > 0
-    tol = 1e-12 if method == "dga" else 1e-10
-    assert abs(w1 - w0) / w0 <= tol, f"{method}: relative drift {abs(w1 - w0) / w0:.3e}"
+    assert abs(w1 - w0) / w0 <= 1e-12, f"{method}: relative drift {abs(w1 - w0) / w0:.3e}"
