@@ -130,3 +130,38 @@ def test_batch_step_io_host_buffers(tmp_path, product_lib):
         zero = np.zeros(sum(nsrc))
         b.step_io(zero, out)
         assert b.info(0)["step_index"] == 6
+
+
+@pytest.mark.gpu
+def test_batch_step_io_routes_each_members_carriers(tmp_path, product_lib):
+    """tf_batch_step_io moves every member's carrier values for the step in
+    one host-to-device copy and scatters them to the members: a batch driven
+    with per-member values matches each member driven alone through
+    tf_step_io with its own values (CG to 1e-13, so the two reduction orders
+    agree far below the bound), and the probe samples it returns are the
+    ones the members record."""
+    ms = members(tmp_path, SPECS, steps=30, tolerance=1e-13)
+    rng = np.random.default_rng(7)
+    steps = 20
+    with tb.Batch(ms, precision="fp64") as b:
+        nsrc = [b.info(m)["n_sources"] for m in range(b.size)]
+        npr = [b.info(m)["n_probes"] for m in range(b.size)]
+        car = rng.uniform(-1.0, 1.0, (steps, sum(nsrc)))
+        out = np.zeros(6 * sum(npr))
+        for k in range(steps):
+            b.step_io(car[k], out)
+        got = [(b.state(m)[0], b.probes(m)[1]) for m in range(b.size)]
+        last = out.copy()
+    offs = np.cumsum([0] + nsrc)
+    poffs = np.cumsum([0] + [6 * p for p in npr])
+    for m, (script, _) in enumerate(ms):
+        with tb.Discretization(script) as d:
+            d.prepare(1, precision="fp64")
+            po = np.zeros(6 * npr[m])
+            for k in range(steps):
+                d.step_io(car[k, offs[m]:offs[m + 1]], po)
+            U = d.state()[0]
+            v = d.probes()[1]
+        assert np.abs(U).max() > 0
+        assert rel(got[m][0], U) <= 1e-11 and rel(got[m][1], v) <= 1e-11
+        assert np.array_equal(last[poffs[m]:poffs[m + 1]], got[m][1][-1].ravel())

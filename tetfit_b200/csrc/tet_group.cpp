@@ -501,10 +501,24 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
                                    : group_cg_blocks<double>(opt_.device, S, &cg_smem_);
   if (cg_blocks_ < 1) throw CudaError("no co-resident blocks for the cooperative CG kernel");
   partition();
-  for (const Meta& m : meta_) {
-    io_src_ += m.nsrc;
-    io_probe_ += 6 * m.np;
+  // step_io staging: every member's carrier values of a step in one
+  // contiguous H2D buffer, every member's exported sample in one D2H buffer
+  std::vector<int> io_src_sim, io_in_off(S + 1, 0);
+  std::vector<int64_t> io_out_off(S + 1, 0);
+  for (int q = 0; q < S; q++) {
+    const Meta& m = meta_[q];
+    io_in_off[q + 1] = io_in_off[q] + (int)m.nsrc;
+    io_out_off[q + 1] = io_out_off[q] + 6 * (int64_t)m.np;
+    io_src_sim.insert(io_src_sim.end(), m.nsrc, q);
   }
+  io_src_ = (size_t)io_in_off[S];
+  io_probe_ = (size_t)io_out_off[S];
+  d.n_io_in = (int64_t)io_src_;
+  d.io_src_sim = (const int*)upload(io_src_sim);
+  d.io_in_off = (const int*)upload(io_in_off);
+  d.io_out_off = (const int64_t*)upload(io_out_off);
+  dio_in_ = (double*)dalloc(sizeof(double) * std::max<size_t>(io_src_, 1));
+  dio_out_ = (double*)dalloc(sizeof(double) * std::max<size_t>(io_probe_, 1));
   const size_t mp = io_src_ + io_probe_ + 1;
   pinned_len_ = mp;
   CU(cudaHostAlloc((void**)&pinned_, mp * sizeof(double), cudaHostAllocDefault));
@@ -736,31 +750,28 @@ uint64_t TetGroup::step_io(const double* car_in, double* probe_out) {
   if (left == 0) return 0;
   double* hin = pinned_;
   double* hout = pinned_ + io_src_;
+  // one copy each way: the carriers land in a staging buffer that a kernel
+  // writes into each running member's carrier row of this step, and the
+  // probe kernel writes this step's samples to a contiguous staging buffer
   if (car_in && io_src_) {
     std::memcpy(hin, car_in, io_src_ * sizeof(double));
-    size_t o = 0;
-    for (const Meta& m : meta_) {
-      if (m.nsrc && m.step < m.nsteps)
-        CU(cudaMemcpyAsync((double*)dev_.carrier + m.car_off + m.step * m.nsrc, hin + o, m.nsrc * sizeof(double),
-                           cudaMemcpyHostToDevice, stream_));
-      o += m.nsrc;
-    }
+    CU(cudaMemcpyAsync(dio_in_, hin, io_src_ * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    CU(group_launch_io_carriers(dev_, dio_in_, stream_));
   }
-  launch(1, nullptr);
-  size_t o = 0;
   std::vector<char> got(meta_.size(), 0);
+  bool any = false;
   for (size_t s = 0; s < meta_.size(); s++) {
     const Meta& m = meta_[s];
     const int slot = m.step < m.nsteps ? m.slot_of_step[m.step] : -1;
-    if (probe_out && slot >= 0 && m.np) {
-      CU(cudaMemcpyAsync(hout + o, dev_.samples + m.samp_off + (size_t)slot * m.np * 6, m.np * 6 * sizeof(double),
-                         cudaMemcpyDeviceToHost, stream_));
-      got[s] = 1;
-    }
-    o += m.np * 6;
+    got[s] = probe_out && slot >= 0 && m.np ? 1 : 0;
+    any = any || got[s];
   }
+  dev_.io_out = any ? dio_out_ : nullptr;
+  launch(1, nullptr);
+  dev_.io_out = nullptr;
+  if (any) CU(cudaMemcpyAsync(hout, dio_out_, io_probe_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
   CU(cudaStreamSynchronize(stream_));
-  o = 0;
+  size_t o = 0;
   for (size_t s = 0; s < meta_.size(); s++) {
     if (got[s]) std::memcpy(probe_out + o, hout + o, meta_[s].np * 6 * sizeof(double));
     o += meta_[s].np * 6;

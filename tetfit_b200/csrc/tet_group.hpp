@@ -98,6 +98,7 @@ class TetGroup {
   double tune_ms_[2] = {0, 0};
   double last_ms_ = 0;
   double* pinned_ = nullptr;
+  double *dio_in_ = nullptr, *dio_out_ = nullptr;  // step_io staging on the device
   size_t pinned_len_ = 0, io_src_ = 0, io_probe_ = 0;
   std::vector<double> carrier_host_;
   std::vector<uint8_t> lossy_host_;  // member has conducting tets

@@ -265,6 +265,27 @@ __global__ void grp_probes(GroupDev d) {
     out[a] = E[a];
     out[3 + a] = H[a];
   }
+  if (d.io_out) {  // step_io: the same sample, contiguous per member
+    double* o2 = d.io_out + d.io_out_off[s] + (p - d.sim_probe[s]) * 6;
+    for (int a = 0; a < 3; a++) {
+      o2[a] = E[a];
+      o2[3 + a] = H[a];
+    }
+  }
+}
+
+__global__ void grp_io_carriers(GroupDev d, const double* in) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.n_io_in) return;
+  const int s = d.io_src_sim[k];
+  if (d.step[s] >= d.nsteps[s]) return;
+  const_cast<double*>(d.carrier)[d.car_off[s] + (int64_t)d.step[s] * d.nsrc[s] + (k - d.io_in_off[s])] = in[k];
+}
+
+cudaError_t group_launch_io_carriers(const GroupDev& d, const double* in, cudaStream_t st) {
+  if (d.n_io_in == 0) return cudaSuccess;
+  grp_io_carriers<<<(unsigned)((d.n_io_in + 255) / 256), 256, 0, st>>>(d, in);
+  return cudaGetLastError();
 }
 
 // One block per simulation.  E sources write the Dirichlet values, H sources

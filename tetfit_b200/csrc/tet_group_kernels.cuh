@@ -75,6 +75,14 @@ struct GroupDev {
   const int* sim_sa = nullptr;   // [S + 1] first Sa slice of each member
   double* loss_part = nullptr;   // [nsa / 32] slice partials
   double* loss_a = nullptr;      // [stat]
+  // step_io staging: io_out (when set) receives each member's sample of this
+  // step at io_out_off[s]; the carriers of a step arrive contiguous, member
+  // s's at io_in_off[s], io_src_sim[k] the member of entry k
+  double* io_out = nullptr;
+  const int64_t* io_out_off = nullptr;
+  const int* io_in_off = nullptr;
+  const int* io_src_sim = nullptr;
+  int64_t n_io_in = 0;
   const void* pre = nullptr;     // Jacobi 1/diag (0 on padding rows)
   const int32_t* free_edge = nullptr;
   const int32_t* dir_edge = nullptr;
@@ -138,6 +146,9 @@ cudaError_t group_launch_step(const GroupDev& d, int cg_blocks, int cg_variant, 
                               cudaEvent_t* ev);
 template <typename T>
 int group_cg_blocks(int device, int S, size_t* smem);
+// step_io: this step's carrier values (staging, contiguous) into each
+// running member's carrier row
+cudaError_t group_launch_io_carriers(const GroupDev& d, const double* in, cudaStream_t st);
 template <typename T>
 int group_guess_tc_blocks(int device);
 template <typename T>
