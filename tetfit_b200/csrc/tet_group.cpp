@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <queue>
 #include <numeric>
 #include <string>
 
@@ -525,10 +526,20 @@ void TetGroup::build(std::vector<TetSim*>& sims, bool release_host) {
   CU(cudaDeviceSynchronize());
 }
 
-// Contiguous slice ranges of about equal work (stored entries of A plus the
-// vector passes) for the CG blocks, cut at simulation boundaries into
-// segments.  The block count follows the problem size (at most one slice per
-// warp and pass) so that small systems keep their grid barriers cheap.
+#ifndef TF_CG_MIX
+#define TF_CG_MIX 1
+#endif
+#ifndef TF_CG_CHUNKS
+#define TF_CG_CHUNKS 12
+#endif
+
+// The CG blocks' rows.  A group of several members: chunks of each member's
+// slices dealt to the blocks by work (below).  A single simulation:
+// contiguous slice ranges of about equal work (stored entries of A plus the
+// vector passes).  Either way a block's rows form segments of one member
+// each, the unit of the partial sums.  The block count follows the problem
+// size (at most one slice per warp and pass) so that small systems keep
+// their grid barriers cheap.
 void TetGroup::partition() {
   GroupDev& d = dev_;
   const int64_t nslice = d.nrow / 32;
@@ -547,23 +558,81 @@ void TetGroup::partition() {
     cut[b] = std::lower_bound(cum.begin(), cum.end(), target) - cum.begin();
     cut[b] = std::max(cut[b], cut[b - 1]);
   }
-  std::vector<int> blk_seg(G + 1, 0), seg_sim, sim_seg(d.S + 1, 0);
+  std::vector<int> blk_seg(G + 1, 0), seg_sim, sim_seg(d.S + 1, 0), seg_of;
   std::vector<int64_t> seg_s0, seg_s1;
-  for (int b = 0; b < G; b++) {
-    blk_seg[b] = (int)seg_sim.size();
-    int64_t s = cut[b];
-    while (s < cut[b + 1]) {
-      int64_t e = s;
-      while (e < cut[b + 1] && ssim[e] == ssim[s]) e++;
-      seg_sim.push_back(ssim[s]);
-      seg_s0.push_back(s);
-      seg_s1.push_back(e);
-      s = e;
+  bool mixed = false;
+#if TF_CG_MIX
+  if (d.S > 1 && G > 1) {
+    // Members converge after different numbers of iterations, and a block
+    // whose rows all belong to converged members waits at the barriers.  So
+    // every member's slices are cut into chunks of about K slices (segments,
+    // numbered member by member) and the chunks are dealt to the blocks
+    // largest first, each to the least loaded block: a block then holds
+    // chunks of about a dozen members, and as members converge every block
+    // loses a similar share of its work.
+    const int64_t per = TF_CG_CHUNKS;  // chunks per block aimed at
+    for (int64_t K = std::max<int64_t>(16, (nslice + per * G - 1) / (per * G));; K *= 2) {
+      seg_sim.clear(); seg_s0.clear(); seg_s1.clear();
+      for (int64_t a = 0; a < nslice;) {
+        int64_t e = a;
+        while (e < nslice && ssim[e] == ssim[a]) e++;
+        const int64_t pieces = (e - a + K - 1) / K;
+        for (int64_t q = 0; q < pieces; q++) {
+          seg_sim.push_back(ssim[a]);
+          seg_s0.push_back(a + (e - a) * q / pieces);
+          seg_s1.push_back(a + (e - a) * (q + 1) / pieces);
+        }
+        a = e;
+      }
+      const int C = (int)seg_sim.size();
+      std::vector<int> order(C);
+      std::iota(order.begin(), order.end(), 0);
+      auto work = [&](int c) { return cum[seg_s1[c]] - cum[seg_s0[c]]; };
+      std::stable_sort(order.begin(), order.end(), [&](int a2, int b2) { return work(a2) > work(b2); });
+      using Load = std::pair<double, int>;
+      std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+      for (int b = 0; b < G; b++) heap.push({0.0, b});
+      std::vector<std::vector<int>> mine(G);
+      for (int c : order) {
+        Load l = heap.top();
+        heap.pop();
+        mine[l.second].push_back(c);
+        heap.push({l.first + work(c), l.second});
+      }
+      size_t most = 0;
+      for (auto& v : mine) most = std::max(most, v.size());
+      if ((int)most > kMaxSeg) continue;  // too many chunks for a block's partial slots: coarser chunks
+      seg_of.clear();
+      for (int b = 0; b < G; b++) {
+        std::sort(mine[b].begin(), mine[b].end());
+        blk_seg[b] = (int)seg_of.size();
+        seg_of.insert(seg_of.end(), mine[b].begin(), mine[b].end());
+      }
+      mixed = true;
+      break;
     }
-    if ((int)seg_sim.size() - blk_seg[b] > kMaxSeg)
-      throw std::invalid_argument("CG block spans more than " + std::to_string(kMaxSeg) + " simulations");
   }
-  blk_seg[G] = (int)seg_sim.size();
+#endif
+  if (!mixed) {
+    seg_sim.clear(); seg_s0.clear(); seg_s1.clear();
+    for (int b = 0; b < G; b++) {
+      blk_seg[b] = (int)seg_sim.size();
+      int64_t s = cut[b];
+      while (s < cut[b + 1]) {
+        int64_t e = s;
+        while (e < cut[b + 1] && ssim[e] == ssim[s]) e++;
+        seg_sim.push_back(ssim[s]);
+        seg_s0.push_back(s);
+        seg_s1.push_back(e);
+        s = e;
+      }
+      if ((int)seg_sim.size() - blk_seg[b] > kMaxSeg)
+        throw std::invalid_argument("CG block spans more than " + std::to_string(kMaxSeg) + " simulations");
+    }
+    seg_of.resize(seg_sim.size());
+    std::iota(seg_of.begin(), seg_of.end(), 0);
+  }
+  blk_seg[G] = (int)seg_of.size();
   // segments of a simulation are consecutive
   for (size_t g = 0; g < seg_sim.size(); g++) sim_seg[seg_sim[g] + 1]++;
   for (int s = 0; s < d.S; s++) sim_seg[s + 1] += sim_seg[s];
@@ -572,6 +641,7 @@ void TetGroup::partition() {
   cg_blocks_ = G;
   blk_seg_.assign(blk_seg.begin(), blk_seg.end());
   d.blk_seg = (const int*)upload(blk_seg);
+  d.seg_of = (const int*)upload(seg_of);
   d.seg_sim = (const int*)upload(seg_sim);
   d.seg_s0 = (const int64_t*)upload(seg_s0);
   d.seg_s1 = (const int64_t*)upload(seg_s1);

@@ -679,7 +679,7 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
       for (int k = 0; k < nq; k++) {
         double a = 0.0;
         for (int w = 0; w < kCgWarps; w++) a += wp[(gl * kCgWarps + w) * kPart + k];
-        d.part[kCgPart * (int64_t)(g0 + gl) + slot + k] = a;
+        d.part[kCgPart * (int64_t)d.seg_of[g0 + gl] + slot + k] = a;
       }
   };
   // per-simulation totals of the published partials: one warp per
@@ -706,10 +706,10 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
   T* za = (T*)d.z_alt;
   const bool dual = d.dual != 0;
   for (int g = g0; g < g1; g++) {
-    const int s = d.seg_sim[g];
+    const int s = d.seg_sim[d.seg_of[g]];
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0;
     if (running(d, s))
-      for (int64_t sl = d.seg_s0[g] + warp; sl < d.seg_s1[g]; sl += kCgWarps) {
+      for (int64_t sl = d.seg_s0[d.seg_of[g]] + warp; sl < d.seg_s1[d.seg_of[g]]; sl += kCgWarps) {
         const int64_t i = sl * 32 + lane;
         const T ri = b[i] - sell_dot_cg<T>(d.A, i, [&](int32_t c) { return x[c]; });
         r[i] = ri;
@@ -754,7 +754,7 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
     // p_{j+1} = z + beta p_j, x += alpha_j p_j (lazy), and in the fused
     // variant q = A p_{j+1} with p.q partials
     for (int g = g0; g < g1; g++) {
-      const int s = d.seg_sim[g];
+      const int s = d.seg_sim[d.seg_of[g]];
       const SimCg c = st[s];
       double a0 = 0.0;
       if (c.active) {
@@ -764,7 +764,7 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
         T* pn = pbuf(c.it);
         T* xs = xs_of(c);
         const T* zs = zs_of(c);
-        for (int64_t sl = d.seg_s0[g] + warp; sl < d.seg_s1[g]; sl += kCgWarps) {
+        for (int64_t sl = d.seg_s0[d.seg_of[g]] + warp; sl < d.seg_s1[d.seg_of[g]]; sl += kCgWarps) {
           const int64_t i = sl * 32 + lane;
           const T po = first ? (T)0 : pold[i];
           const T pi = p_next<T>(zs[i], po, beta, first);
@@ -784,12 +784,12 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
     if (!kFused) {
       grid_sync();
       for (int g = g0; g < g1; g++) {
-        const int s = d.seg_sim[g];
+        const int s = d.seg_sim[d.seg_of[g]];
         const SimCg c = st[s];
         double a0 = 0.0;
         if (c.active) {
           const T* pn = pbuf(c.it);
-          for (int64_t sl = d.seg_s0[g] + warp; sl < d.seg_s1[g]; sl += kCgWarps) {
+          for (int64_t sl = d.seg_s0[d.seg_of[g]] + warp; sl < d.seg_s1[d.seg_of[g]]; sl += kCgWarps) {
             const int64_t i = sl * 32 + lane;
             const T qi = sell_dot_cg<T>(d.A, i, [&](int32_t cc) { return pn[cc]; });
             q[i] = qi;
@@ -807,13 +807,13 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
     __syncthreads();
     // r -= alpha q; rr, rz partials
     for (int g = g0; g < g1; g++) {
-      const int s = d.seg_sim[g];
+      const int s = d.seg_sim[d.seg_of[g]];
       double a0 = 0.0, a1 = 0.0;
       if (st[s].active) {
         const T alpha = (T)st[s].alpha;
         T* rs = rs_of(st[s]);
         T* zs = zs_of(st[s]);
-        for (int64_t sl = d.seg_s0[g] + warp; sl < d.seg_s1[g]; sl += kCgWarps) {
+        for (int64_t sl = d.seg_s0[d.seg_of[g]] + warp; sl < d.seg_s1[d.seg_of[g]]; sl += kCgWarps) {
           const int64_t i = sl * 32 + lane;
           const T ri = rs[i] - alpha * q[i];
           rs[i] = ri;
@@ -843,13 +843,13 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
   }
   // the last x update, x += alpha_{J-1} p_{J-1}
   for (int g = g0; g < g1; g++) {
-    const int s = d.seg_sim[g];
+    const int s = d.seg_sim[d.seg_of[g]];
     const SimCg c = st[s];
     if (!running(d, s)) continue;
     const T alpha = (T)c.alpha;
     const T* pl = pbuf(c.it - 1);
     T* xs = xs_of(c);
-    for (int64_t sl = d.seg_s0[g] + warp; sl < d.seg_s1[g]; sl += kCgWarps) {
+    for (int64_t sl = d.seg_s0[d.seg_of[g]] + warp; sl < d.seg_s1[d.seg_of[g]]; sl += kCgWarps) {
       const int64_t i = sl * 32 + lane;
       T v = xs[i];
       if (c.it > 0) v = fmaT(alpha, pl[i], v);

@@ -89,7 +89,8 @@ struct GroupDev {
   // CG
   void *x = nullptr, *r = nullptr, *z = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr, *rhs = nullptr;
   void *xh1 = nullptr, *xh2 = nullptr, *xh3 = nullptr;
-  const int* blk_seg = nullptr;  // [G + 1]
+  const int* blk_seg = nullptr;  // [G + 1] block b's positions blk_seg[b] .. blk_seg[b+1] in seg_of
+  const int* seg_of = nullptr;   // position -> segment (segments numbered member by member)
   const int* seg_sim = nullptr;
   const int64_t *seg_s0 = nullptr, *seg_s1 = nullptr;  // slice range of a segment
   const int* sim_seg = nullptr;  // [S + 1]
