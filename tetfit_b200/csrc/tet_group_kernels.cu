@@ -70,9 +70,11 @@ __device__ __forceinline__ double ld_stream(const double* p) {
 // one per entry group.
 // The same sweep with the sum in A (values of type T read from the matrix):
 // sell_dot<double>(m, row, g, (const float*)nullptr) sums FP32 entries in FP64.
-template <typename A, typename G, typename T>
+#ifndef TF_SPMV_CH
+#define TF_SPMV_CH 4
+#endif
+template <typename A, typename G, typename T, int CH = TF_SPMV_CH>
 __device__ __forceinline__ A sell_dot(const SellDev& m, int64_t row, G g, const T*) {
-  constexpr int CH = 4;
   const int64_t sl = row >> 5;
   const int64_t b = m.ptr[sl];
   const int len = (int)((m.ptr[sl + 1] - b) >> 5);
@@ -95,9 +97,8 @@ __device__ __forceinline__ A sell_dot(const SellDev& m, int64_t row, G g, const 
   return s;
 }
 
-template <typename T, typename G>
+template <typename T, typename G, int CH = TF_SPMV_CH>
 __device__ __forceinline__ T sell_dot(const SellDev& m, int64_t row, G g) {
-  constexpr int CH = 4;
   const int64_t sl = row >> 5;
   const int64_t b = m.ptr[sl];
   const int len = (int)((m.ptr[sl + 1] - b) >> 5);
@@ -131,7 +132,7 @@ __device__ __forceinline__ T sell_dot(const SellDev& m, int64_t row, G g) {
 template <typename T, typename G>
 __device__ __forceinline__ T sell_dot_cg(const SellDev& m, int64_t row, G g) {
 #if TF_CG_PIPE == 0
-  return sell_dot<T>(m, row, g);
+  return sell_dot<T, G, 4>(m, row, g);  // 4-entry chunks: the CG's register budget
 #elif TF_CG_PIPE == 1
   constexpr int CH = 4;
   const int64_t sl = row >> 5;
@@ -374,7 +375,7 @@ __global__ void __launch_bounds__(kGB) grp_rhs(GroupDev d) {
   // and add nothing)
   T cf = 0;
   {
-    constexpr int CH = 4;
+    constexpr int CH = TF_SPMV_CH;
     const int64_t sl = i >> 5;
     const int64_t b = d.Ct.ptr[sl];
     const int len = (int)((d.Ct.ptr[sl + 1] - b) >> 5);
