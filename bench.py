@@ -106,18 +106,35 @@ class ClockSampler:
         self.proc = None
         self.path = tempfile.mktemp(suffix=".csv")
 
+    def _lines(self):
+        try:
+            with open(self.path) as f:
+                return sum(1 for _ in f)
+        except OSError:
+            return 0
+
     def __enter__(self):
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
+            # the timed region opens once the sampler is live (its start-up
+            # would otherwise swallow a short region)
+            t0 = time.time()
+            while self._lines() == 0 and time.time() - t0 < 3.0 and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.n0 = self._lines()
         except Exception:
             self.proc = None
         return self
 
     def __exit__(self, *a):
         if self.proc:
+            # one more sample at the end of a region shorter than the period
+            t0 = time.time()
+            while self._lines() <= self.n0 and time.time() - t0 < 0.5 and self.proc.poll() is None:
+                time.sleep(0.01)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
