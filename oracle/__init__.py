@@ -169,6 +169,7 @@ class TetOracle:
             L.orc_tet_topology.argtypes = [P, P, P, P, P]
             L.orc_tet_matrix.restype = ctypes.c_longlong
             L.orc_tet_matrix.argtypes = [P, ctypes.c_int, P, P, P]
+            L.orc_tet_dga_p.argtypes = [P, P]
             L._tet_sigs = True
         err = ctypes.create_string_buffer(1024)
         self.h = L.orc_tet_open(os.fsencode(script), label, int(consistent_mass), err, 1024)
@@ -229,6 +230,13 @@ class TetOracle:
         b = np.zeros(self.nE, dtype=np.int32)
         self.L.orc_tet_topology(self.h, _p(e), _p(f), _p(c), _p(b))
         return e, f, c, b
+
+    def dga_p(self):
+        """dga: (P per edge: 1 on class-1, P_p on class-2 edges, 0 elsewhere;
+        number of node-star fractions U_c)."""
+        P = np.zeros(self.nE)
+        nq = int(self.L.orc_tet_dga_p(self.h, _p(P)))
+        return P, nq
 
     def matrix(self, which: str):
         """CSR (ptr, col, val) of one operator: C, N, H (dga), E, Sig (the

@@ -397,6 +397,14 @@ int orc_tet_topology(void* h, unsigned* edges, unsigned* faces, unsigned char* c
   return 0;
 }
 
+// dga: P per edge (1 on class-1 edges, P_p on class-2 edges, 0 elsewhere)
+int orc_tet_dga_p(void* h, double* P) {
+  auto* o = static_cast<orc::TetOracle*>(h);
+  for (size_t e = 0; e < o->edges.size(); e++)
+    P[e] = o->cls[e] == 1 ? 1.0 : o->cls[e] == 2 ? o->P_p[o->p_index[e]] : 0.0;
+  return (int)o->Q_size;
+}
+
 // CSR export of an operator: which 0 C, 1 N, 2 H, 3 E, 4 A; returns nnz
 long long orc_tet_matrix(void* h, int which, unsigned long long* ptr, unsigned* col, double* val) {
   auto* o = static_cast<orc::TetOracle*>(h);

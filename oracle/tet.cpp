@@ -16,8 +16,9 @@
 // the reference's order.
 //
 // Scope and documented divergences:
-//  * lossless materials only (sigma = chi = 0): the lossy / "fractured" edge and
-//    face classes (:6776-6905, :6501-6542) are rejected;
+//  * conductivity (sigma) enters gfdtd and fem through SigMat and dga through
+//    its edge classes (:6776-6905, :9262-9475); magnetic losses (chi, the face
+//    classes :6501-6542) are rejected;
 //  * tets with material label 7 are dropped (:6091); the reference also keeps 4
 //    zero-initialised face slots per dropped tet (:6130-6152) that create a
 //    spurious face (0,0,0); here they are not created;
@@ -279,10 +280,9 @@ void TetOracle::read_mesh() {
     V3 v1 = sub(pts[t[1]], pts[t[0]]), v2 = sub(pts[t[2]], pts[t[0]]), v3 = sub(pts[t[3]], pts[t[0]]);
     cell_vol.push_back(dot(v1, cross(v2, v3)) / 6.0);
     const Material& mt = sc.materials[tt[k].second];
-    // conductivity enters gfdtd and fem through SigMat; dga's lossy
-    // ("fractured") edge classes and magnetic losses are not restated
-    if (!mat_zero(mt.chi) || (method == 1 && !mat_zero(mt.sigma)))
-      throw std::runtime_error("lossy materials (chi on tetrahedra, or sigma with dga) are outside the supported path");
+    // conductivity enters gfdtd and fem through SigMat and dga through its
+    // edge classes; magnetic losses (chi, the face classes) are not restated
+    if (!mat_zero(mt.chi)) throw std::runtime_error("magnetic losses (chi) on tetrahedra are outside the supported path");
   }
   // unique faces (Discretization.hpp:10173-10219)
   std::sort(tri.begin(), tri.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
@@ -416,6 +416,7 @@ void TetOracle::read_mesh() {
       if (sc.sources[s].st == "e") dir = true;
     if (dir) cls[e] = 4;
   }
+  if (method == 1) classify_dga();
 }
 
 std::array<uint32_t, 6> TetOracle::vol_edges(uint32_t v) const {
@@ -555,21 +556,21 @@ static double lanczos_K(size_t n, const std::function<void(const double*, double
 }
 
 void TetOracle::build_dga() {
-  // ConstructCodecasaMaterialMatrices (Discretization.hpp:8694-9513), lossless
+  // ConstructCodecasaMaterialMatrices (Discretization.hpp:8694-9513)
   N = assemble_N();
   const uint32_t NE = (uint32_t)edges.size();
-  std::vector<Csr::Trip> einv_t, h_t;
-  std::vector<std::vector<double>> star_E(pts.size());
-  for (uint32_t nid = 0; nid < pts.size(); nid++) {
-    std::vector<uint32_t> gi;
-    for (auto& se : nte[nid]) gi.push_back(se.first);
+  // node-star matrix of eps (or of sigma, from the tets whose sigma has a
+  // non-zero determinant, :8897): the dual basis of the star's edges
+  // (:8900-9080), entries j <= k accumulated, then mirrored
+  auto star_mass = [&](uint32_t nid, const std::vector<uint32_t>& gi, bool sigma) {
     const int n = (int)gi.size();
     std::vector<double> E(n * n, 0.0);
     for (uint32_t vv : node_vols[nid]) {
+      const Mat3& mat = sigma ? sc.materials.at(vol_mat[vv]).sigma : sc.materials.at(vol_mat[vv]).eps;
+      if (sigma && mat_det(mat) == 0) continue;
       auto el = vol_edges(vv);
       auto fv = primal_area_vectors(vv);
       const double V = std::fabs(cell_vol[vv]);
-      const Mat3& eps = sc.materials.at(vol_mat[vv]).eps;
       int k = 0;
       while (vols[vv][k] != nid) k++;
       // (local edges, face vector index, sign of the 2/3V factor) per node position
@@ -585,13 +586,23 @@ void TetOracle::build_dga() {
       }
       for (int a = 0; a < 3; a++)
         for (int b = a; b < 3; b++) {
-          double val = dot(w[a], matvec(eps, w[b])) * V / 4;
+          double val = dot(w[a], matvec(mat, w[b])) * V / 4;
           E[ei[a] * n + ei[b]] += val;
           if (a != b) E[ei[b] * n + ei[a]] = E[ei[a] * n + ei[b]];
         }
     }
-    star_E[nid] = E;
-    std::vector<double> Hl = E;
+    return E;
+  };
+  auto star_edges = [&](uint32_t nid) {
+    std::vector<uint32_t> gi;
+    for (auto& se : nte[nid]) gi.push_back(se.first);
+    return gi;
+  };
+  std::vector<Csr::Trip> einv_t;
+  for (uint32_t nid = 0; nid < pts.size(); nid++) {
+    auto gi = star_edges(nid);
+    const int n = (int)gi.size();
+    std::vector<double> Hl = star_mass(nid, gi, false);
     spd_inverse(Hl, n);
     for (int j = 0; j < n; j++)
       for (int k = j; k < n; k++)
@@ -601,7 +612,7 @@ void TetOracle::build_dga() {
         }
   }
   Csr Einv = Csr::build(NE, NE, einv_t);
-  // dt (ComputeDGATimeStep, :7121-7174)
+  // dt (ComputeDGATimeStep, :7121-7174), from the unmasked eps inverses
   const char* skip = std::getenv("TF_ORACLE_SKIP_DT");
   if (skip && skip[0] == '1' && sim.step != 0) {
     dt_estimate = sim.step;
@@ -617,31 +628,158 @@ void TetOracle::build_dga() {
     if (sim.step > dt) possibly_unstable = true;
     else dt = sim.step;
   }
-  // masked node-star inverses -> H (:9263-9450)
+  // masked node-star inverses (:9262-9475).  A star with a conducting tet
+  // (sigma_node, :8897) gets H = (E + dt/2 S)^-1 and PQ = H (E - dt/2 S),
+  // else H = E^-1 and PQ = I; Dirichlet rows and columns are masked.
+  // Class-1 rows go to Ha, class-2 rows to Mp with the diagonal of PQ in
+  // P_p (the star of the higher node writes it last), and a fractured
+  // star's rows to Q and Mq.  Ha and Mp are filled from the upper triangle
+  // and its mirror, whose row is h_index / p_index of the column's edge: 0
+  // for an edge of another class, as the reference's zero-filled index
+  // vectors give (:6546-6547).
+  std::vector<Csr::Trip> h_t, mp_t, q_t, mq_t;
+  P_p.assign(P_size, 0.0);
   for (uint32_t nid = 0; nid < pts.size(); nid++) {
-    std::vector<uint32_t> gi;
-    for (auto& se : nte[nid]) gi.push_back(se.first);
+    auto gi = star_edges(nid);
     const int n = (int)gi.size();
-    std::vector<double> E = star_E[nid];
+    bool sig_node = false;
+    for (uint32_t vv : node_vols[nid])
+      if (mat_det(sc.materials.at(vol_mat[vv]).sigma) != 0) sig_node = true;
+    std::vector<double> E = star_mass(nid, gi, false);
+    std::vector<double> S = sig_node ? star_mass(nid, gi, true) : std::vector<double>(n * n, 0.0);
     for (int j = 0; j < n; j++)
       if (cls[gi[j]] == 4) {
         for (int k = 0; k < n; k++) E[j * n + k] = E[k * n + j] = 0;
         E[j * n + j] = 1;
+        if (sig_node)
+          for (int k = 0; k < n; k++) S[j * n + k] = S[k * n + j] = 0;
       }
-    spd_inverse(E, n);
+    std::vector<double> Hl(n * n), PQ(n * n, 0.0);
+    if (sig_node) {
+      for (int q = 0; q < n * n; q++) Hl[q] = E[q] + 0.5 * dt * S[q];
+      spd_inverse(Hl, n);
+      for (int j = 0; j < n; j++)
+        for (int k = 0; k < n; k++) {
+          double acc = 0;
+          for (int m = 0; m < n; m++) acc += Hl[j * n + m] * (E[m * n + k] - 0.5 * dt * S[m * n + k]);
+          PQ[j * n + k] = acc;
+        }
+    } else {
+      Hl = E;
+      spd_inverse(Hl, n);
+      for (int j = 0; j < n; j++) PQ[j * n + j] = 1;
+    }
     for (int j = 0; j < n; j++)
-      if (cls[gi[j]] == 4)
-        for (int k = 0; k < n; k++) E[j * n + k] = E[k * n + j] = 0;
+      if (cls[gi[j]] == 4) {
+        for (int k = 0; k < n; k++) Hl[j * n + k] = Hl[k * n + j] = PQ[j * n + k] = PQ[k * n + j] = 0;
+        PQ[j * n + j] = 1;
+      }
+    const bool frac = dual_frac[nid] > 0;
+    const uint32_t off = frac ? dual_frac[nid] - 1 : 0;
     for (int j = 0; j < n; j++) {
-      if (cls[gi[j]] != 1) continue;
-      for (int k = j; k < n; k++)
-        if (cls[gi[k]] != 4 && E[j * n + k] != 0) {
-          h_t.push_back({gi[j], gi[k], E[j * n + k]});
-          if (j != k) h_t.push_back({gi[k], gi[j], E[j * n + k]});
+      const uint32_t ej = gi[j];
+      if (cls[ej] == 1 || cls[ej] == 2) {
+        const bool c1 = cls[ej] == 1;
+        const std::vector<uint32_t>& idx = c1 ? h_index : p_index;
+        std::vector<Csr::Trip>& t = c1 ? h_t : mp_t;
+        if (!c1) P_p[p_index[ej]] = PQ[j * n + j];
+        for (int k = j; k < n; k++)
+          if (cls[gi[k]] != 4 && Hl[j * n + k] != 0) {
+            t.push_back({idx[ej], gi[k], Hl[j * n + k]});
+            if (j != k) t.push_back({idx[gi[k]], ej, Hl[j * n + k]});
+          }
+      }
+      if (frac && cls[ej] != 4)
+        for (int k = 0; k < n; k++) {
+          if (cls[gi[k]] == 4) continue;
+          if (PQ[j * n + k] != 0) q_t.push_back({off + (uint32_t)j, off + (uint32_t)k, PQ[j * n + k]});
+          if (Hl[j * n + k] != 0) mq_t.push_back({off + (uint32_t)j, gi[k], Hl[j * n + k]});
         }
     }
   }
-  H = Csr::build(NE, NE, h_t);
+  Ha = Csr::build(H_size, NE, h_t);
+  Mp = Csr::build(P_size, NE, mp_t);
+  Q = Csr::build(Q_size, Q_size, q_t);
+  Mq = Csr::build(Q_size, NE, mq_t);
+  // edge-indexed view for the operator export: the Ha row of each class-1
+  // edge and the Mp row of each class-2 edge
+  std::vector<Csr::Trip> hv;
+  for (uint32_t e = 0; e < NE; e++) {
+    const Csr* m = cls[e] == 1 ? &Ha : cls[e] == 2 ? &Mp : nullptr;
+    if (!m) continue;
+    const uint32_t r = cls[e] == 1 ? h_index[e] : p_index[e];
+    for (uint64_t q = m->ptr[r]; q < m->ptr[r + 1]; q++) hv.push_back({e, m->col[q], m->val[q]});
+  }
+  H = Csr::build(NE, NE, hv);
+}
+
+// dga edge classes (Discretization.hpp:6186-6215, 6776-6903).  Each node
+// keeps the eps and sigma of the first tet that lists it; bit 0 of its class
+// says that sigma is non-zero, bit 1 that a later tet has another eps, bit 2
+// another sigma.  A free edge is fractured (3) when an end has class > 2,
+// the ends' classes sum to 1 or 3, or their first sigmas differ; else
+// lossless (1) when an end has class 0 or 2; else uniformly conducting (2).
+// A fractured edge's ends get a block of U_c as long as their star, in the
+// order the edges first reach them.
+void TetOracle::classify_dga() {
+  const uint32_t NE = (uint32_t)edges.size(), NP = (uint32_t)pts.size();
+  std::vector<uint8_t> ncls(NP, 0);
+  std::vector<Mat3> first_eps(NP), first_sig(NP);
+  auto same = [](const Mat3& a, const Mat3& b) {
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++)
+        if (a.m[i][j] != b.m[i][j]) return false;
+    return true;
+  };
+  for (uint32_t v = 0; v < vols.size(); v++) {
+    const Material& mt = sc.materials.at(vol_mat[v]);
+    for (int q = 0; q < 4; q++) {
+      const uint32_t p = vols[v][q];
+      if (!mat_zero(first_eps[p])) {
+        if (!same(mt.sigma, first_sig[p])) ncls[p] |= 4;
+        if (!same(mt.eps, first_eps[p])) ncls[p] |= 2;
+        if (!mat_zero(first_sig[p])) ncls[p] |= 1;
+      } else {
+        first_eps[p] = mt.eps;
+        first_sig[p] = mt.sigma;
+        if (!mat_zero(mt.sigma)) ncls[p] |= 1;
+      }
+    }
+  }
+  h_index.assign(NE, 0);
+  p_index.assign(NE, 0);
+  dual_frac.assign(NP, 0);
+  H_size = P_size = Q_size = 0;
+  for (uint32_t e = 0; e < NE; e++) {
+    if (cls[e] == 4) continue;
+    const uint32_t p0 = edges[e][0], p1 = edges[e][1];
+    const int r0 = ncls[p0], r1 = ncls[p1];
+    if (r0 > 2 || r1 > 2 || r0 + r1 == 1 || r0 + r1 == 3 || !same(first_sig[p0], first_sig[p1])) {
+      cls[e] = 3;
+      for (uint32_t p : {p0, p1})
+        if (dual_frac[p] == 0) {
+          dual_frac[p] = Q_size + 1;
+          Q_size += (uint32_t)nte[p].size();
+        }
+    } else if (r0 == 2 || r1 == 2 || r0 == 0 || r1 == 0) {
+      cls[e] = 1;
+      h_index[e] = H_size++;
+    } else {
+      cls[e] = 2;
+      p_index[e] = P_size++;
+    }
+  }
+  // U of a fractured edge is the sum of its entries in its two ends' blocks
+  frac_cols.assign(NE, {0, 0});
+  for (uint32_t e = 0; e < NE; e++) {
+    if (cls[e] != 3) continue;
+    for (int a = 0; a < 2; a++) {
+      const uint32_t p = edges[e][a];
+      uint32_t pos = 0;
+      while (nte[p][pos].first != e) pos++;
+      frac_cols[e][a] = dual_frac[p] - 1 + pos;
+    }
+  }
 }
 
 void TetOracle::build_gfdtd() {
@@ -1070,6 +1208,7 @@ void TetOracle::prepare(uint32_t label) {
   else build_fem();
   const size_t NE = edges.size(), NF = faces.size();
   U.assign(NE, 0); I.assign(NE, 0); F.assign(NF, 0); B.assign(NF, 0);
+  U_a.assign(H_size, 0); U_b.assign(P_size, 0); U_c.assign(Q_size, 0); U_c_old = U_c;
   Fb.assign(bnd_dual.size(), 0); Fb_old = Fb; SrcFld.assign(NE, 0);
   solution.assign(free_edges.size(), 0);
   if (out.mode == "silo") {
@@ -1146,6 +1285,7 @@ void TetOracle::dga_step(double t) {
   Fb_old = Fb;
   std::fill(Fb.begin(), Fb.end(), 0.0);
   U_old = U;
+  U_c_old = U_c;
   for (uint32_t e = 0; e < NE; e++) {
     if (edge_bcs[e] != 0 && sc.bcs[edge_bcs[e]].type != "none") {
       U[e] = 0;
@@ -1156,14 +1296,26 @@ void TetOracle::dga_step(double t) {
       else U[e] = efield_source(e, t);
     }
   }
-  std::vector<double> curl_b(NE, 0.0), curl_f(NE), hc(NE);
+  std::vector<double> curl_b(NE, 0.0), curl_f(NE);
   for (uint32_t e = 0; e < NE; e++)
     if (bnd_edges[e] >= 0) curl_b[e] = Fb[bnd_edges[e]];
   C.mul_t(F.data(), curl_f.data());
   for (uint32_t e = 0; e < NE; e++) curl_f[e] = curl_f[e] + curl_b[e] - I[e];
-  H.mul(curl_f.data(), hc.data());
-  for (uint32_t e = 0; e < NE; e++)
-    if (cls[e] == 1) U[e] = U[e] + dt * hc[e];
+  // U_a += dt Ha cf, U_b = P_p .* U_b + dt Mp cf, U_c = Q U_c_old + dt Mq cf,
+  // U = M U_frac (:887-891)
+  std::vector<double> ha(H_size), mp(P_size), qo(Q_size), mq(Q_size);
+  Ha.mul(curl_f.data(), ha.data());
+  Mp.mul(curl_f.data(), mp.data());
+  Q.mul(U_c_old.data(), qo.data());
+  Mq.mul(curl_f.data(), mq.data());
+  for (uint32_t r = 0; r < H_size; r++) U_a[r] = U_a[r] + dt * ha[r];
+  for (uint32_t r = 0; r < P_size; r++) U_b[r] = P_p[r] * U_b[r] + dt * mp[r];
+  for (uint32_t r = 0; r < Q_size; r++) U_c[r] = qo[r] + dt * mq[r];
+  for (uint32_t e = 0; e < NE; e++) {
+    if (cls[e] == 1) U[e] = U_a[h_index[e]];
+    else if (cls[e] == 2) U[e] = U_b[p_index[e]];
+    else if (cls[e] == 3) U[e] = U_c[frac_cols[e][0]] + U_c[frac_cols[e][1]];
+  }
   double fl = 0;
   for (uint32_t e = 0; e < NE; e++) fl += (U_old[e] + U[e]) * curl_b[e];
   flux.push_back(0.5 * fl);

@@ -52,11 +52,20 @@ struct TetOracle {
   std::vector<std::array<double, 3>> bnd_dual;
   std::vector<uint32_t> edge_bcs;
   std::vector<std::vector<uint32_t>> edge_src;
-  std::vector<uint8_t> is_pec, cls;  // cls: 1 interior dof, 4 Dirichlet (PEC or e-source)
+  std::vector<uint8_t> is_pec, cls;  // cls: 1 interior dof, 4 Dirichlet (PEC or e-source); dga
+                                     // also 2 (uniformly conducting) and 3 (fractured)
   Csr C;                               // F x E, +-1
   // operators
   Csr N;                               // F x F
-  Csr H;                               // E x E, rows of class-1 edges (dga)
+  Csr H;                               // E x E, rows of class-1 and class-2 edges (dga; view of Ha, Mp)
+  // dga with conductivity (Discretization.hpp:6776-6903, 9262-9475): U is M
+  // times U_frac = [U_a (class 1), U_b (class 2), U_c (node-star fractions)]
+  std::vector<uint32_t> h_index, p_index;  // edge -> row of Ha / Mp (0 when not of that class)
+  std::vector<uint32_t> dual_frac;         // node -> U_c offset + 1 (0: not fractured)
+  std::vector<std::array<uint32_t, 2>> frac_cols;  // class-3 edge -> its two U_c entries
+  uint32_t H_size = 0, P_size = 0, Q_size = 0;
+  Csr Ha, Mp, Q, Mq;                   // H_size x E, P_size x E, Q_size x Q_size, Q_size x E
+  std::vector<double> P_p, U_a, U_b, U_c, U_c_old;
   Csr E;                               // E x E eps mass (gfdtd: node-star dual basis; fem: Whitney)
   Csr Sig;                             // E x E conductivity mass (SigMat), same construction with sigma
   bool lossy = false;                  // some tet conducts (sigma with non-zero determinant)
@@ -89,6 +98,7 @@ struct TetOracle {
  private:
   void read_mesh();
   void build_dga();
+  void classify_dga();
   void build_gfdtd();
   void build_fem();
   void split_system(double scale, double sig_coef = 0.0);

@@ -120,6 +120,14 @@ bool is_zero(const Mat3& m) {
   return true;
 }
 
+// 3x3 determinant by cofactor expansion along the first row: the reference's
+// zero test on sigma (Discretization.hpp:8604, 8041, 8897)
+double mat_det(const Mat3& a) {
+  const auto& m = a.m;
+  return m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) - m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
+         m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+}
+
 // inverse of a small SPD matrix by Cholesky
 void spd_inv(std::vector<double>& a, int n) {
   std::vector<double> L(n * n, 0.0), inv(n * n), y(n);
@@ -350,12 +358,12 @@ double TetSim::last_step_ms() const { return group_ ? group_->last_step_ms() : l
 int TetSim::kernels_per_step() const {
   if (group_) return group_->kernels_per_step();
   const int np = probe_tet_.empty() ? 0 : 1;
-  return 6 + np + (src_edge_.empty() ? 0 : 1);
+  return 6 + np + (src_edge_.empty() ? 0 : 1) + (dp_.nq > 0 ? 1 : 0) + (dp_.nfe > 0 ? 1 : 0);
 }
 
 void TetSim::release_host() {
   auto drop = [](auto& v) { std::remove_reference_t<decltype(v)>().swap(v); };
-  for (HostCsr* m : {&Ct_, &N_, &H_, &E_, &A_, &R_, &Sig_}) {
+  for (HostCsr* m : {&Ct_, &N_, &H_, &E_, &A_, &R_, &Sig_, &Q_, &Mq_}) {
     drop(m->ptr);
     drop(m->col);
     drop(m->val);
@@ -363,6 +371,7 @@ void TetSim::release_host() {
   drop(vtf_); drop(ftv_); drop(fte_); drop(star_ptr_); drop(star_edge_); drop(nvol_ptr_); drop(nvol_);
   drop(bnd_edge_); drop(bnd_dual_); drop(edge_src_); drop(carrier_); drop(init_U_); drop(init_I_);
   drop(init_src_); drop(jacobi_); drop(cls_); drop(pec_);
+  drop(hp_); drop(frac_off_); drop(fe_edge_); drop(fe_a_); drop(fe_b_);
 }
 
 TetSim::~TetSim() {
@@ -417,10 +426,9 @@ void TetSim::read_mesh() {
     V3 v1 = sub(pts_[t[1]], pts_[t[0]]), v2 = sub(pts_[t[2]], pts_[t[0]]), v3 = sub(pts_[t[3]], pts_[t[0]]);
     cell_vol_[k] = dot(v1, cross(v2, v3)) / 6.0;
     const Material& mt = sc_.materials[vol_mat_[k]];
-    // conductivity enters gfdtd and fem through SigMat; dga's lossy
-    // ("fractured") edge classes and magnetic losses (chi) are not built
-    if (!is_zero(mt.chi) || (method_ == 1 && !is_zero(mt.sigma)))
-      throw UnsupportedError("lossy materials (chi on tetrahedra, or sigma with dga) are outside the supported path");
+    // conductivity enters gfdtd and fem through SigMat and dga through its
+    // edge classes; magnetic losses (chi, dga's face classes) are not built
+    if (!is_zero(mt.chi)) throw UnsupportedError("magnetic losses (chi) on tetrahedra are outside the supported path");
   }
   // faces: packed keys when node ids fit in 21 bits, else tuple order
   const bool packed = np < (1u << 21);
@@ -628,6 +636,73 @@ void TetSim::classify() {
       if (sc_.sources[s].st == "e") dir = true;
     if (dir) cls_[e] = 4;
   }
+  if (method_ != 1) return;
+  // dga with conducting tets (Discretization.hpp:6186-6215, 6776-6903).  A
+  // node holds the eps and sigma of its first tet; its class bits: 1 that
+  // sigma is non-zero, 2 that a later tet differs in eps, 4 in sigma.
+  const uint32_t NP = (uint32_t)pts_.size();
+  std::vector<uint8_t> nb(NP, 0);
+  std::vector<int32_t> first(NP, -1);  // material of the node's first tet
+  auto same = [](const Mat3& a, const Mat3& b) {  // element-wise ==, as Eigen compares
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++)
+        if (a.m[i][j] != b.m[i][j]) return false;
+    return true;
+  };
+  for (size_t v = 0; v < vols_.size(); v++) {
+    const Material& mt = sc_.materials.at(vol_mat_[v]);
+    for (int32_t p : vols_[v]) {
+      // a node counts as seen once it holds a non-zero eps (the reference's test)
+      if (first[p] >= 0 && !is_zero(sc_.materials.at(first[p]).eps)) {
+        const Material& f = sc_.materials.at(first[p]);
+        if (!same(mt.sigma, f.sigma)) nb[p] |= 4;
+        if (!same(mt.eps, f.eps)) nb[p] |= 2;
+        if (!is_zero(f.sigma)) nb[p] |= 1;
+      } else {
+        first[p] = (int32_t)vol_mat_[v];
+        if (!is_zero(mt.sigma)) nb[p] |= 1;
+      }
+    }
+  }
+  // free edges: fractured (3) if an end's class exceeds 2, the classes sum to
+  // 1 or 3, or the ends' first sigmas differ; lossless (1) if an end has
+  // class 0 or 2; else uniformly conducting (2).  A fractured edge's ends get
+  // a block of U_c as long as their star.
+  frac_off_.assign(NP, -1);
+  q_size_ = 0;
+  dga_frac_ = false;
+  for (uint32_t e = 0; e < NE; e++) {
+    if (cls_[e] == 4) continue;
+    const int32_t p0 = edges_[e][0], p1 = edges_[e][1];
+    const int r0 = nb[p0], r1 = nb[p1];
+    const bool sig_eq = same(sc_.materials.at(first[p0]).sigma, sc_.materials.at(first[p1]).sigma);
+    if (r0 > 2 || r1 > 2 || r0 + r1 == 1 || r0 + r1 == 3 || !sig_eq) {
+      cls_[e] = 3;
+      for (int32_t p : {p0, p1})
+        if (frac_off_[p] < 0) {
+          frac_off_[p] = q_size_;
+          q_size_ += (uint32_t)(star_ptr_[p + 1] - star_ptr_[p]);
+        }
+    } else if (!(r0 == 2 || r1 == 2 || r0 == 0 || r1 == 0)) {
+      cls_[e] = 2;
+    }
+    dga_frac_ = dga_frac_ || cls_[e] != 1;
+  }
+  fe_edge_.clear(); fe_a_.clear(); fe_b_.clear();
+  for (uint32_t e = 0; e < NE; e++) {
+    if (cls_[e] != 3) continue;
+    int32_t at[2];
+    for (int a = 0; a < 2; a++) {
+      const int32_t p = edges_[e][a];
+      const int64_t b0 = star_ptr_[p];
+      const int64_t pos = std::lower_bound(star_edge_.begin() + b0, star_edge_.begin() + star_ptr_[p + 1], (int32_t)e) -
+                          (star_edge_.begin() + b0);
+      at[a] = (int32_t)(frac_off_[p] + pos);
+    }
+    fe_edge_.push_back((int32_t)e);
+    fe_a_.push_back(at[0]);
+    fe_b_.push_back(at[1]);
+  }
 }
 
 std::array<int32_t, 6> TetSim::vol_edges(uint32_t v) const {
@@ -664,13 +739,8 @@ void TetSim::build_ops() {
   std::vector<uint8_t> sig_tet(L, 0);
   lossy_ = false;
   if (method_ >= 2)
-    for (uint32_t v = 0; v < L; v++) {
-      const auto& m = sc_.materials.at(vol_mat_[v]).sigma.m;
-      const double det = m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) -
-                         m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
-                         m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
-      if (det != 0) sig_tet[v] = 1, lossy_ = true;
-    }
+    for (uint32_t v = 0; v < L; v++)
+      if (mat_det(sc_.materials.at(vol_mat_[v]).sigma) != 0) sig_tet[v] = 1, lossy_ = true;
   // N = sum of per-tet inverse magnetic blocks (Discretization.hpp:8754-8807, 9158-9255);
   // the blocks are formed in parallel, then listed in tet order
   {
@@ -740,39 +810,51 @@ void TetSim::build_ops() {
     static const int kFv[4][3] = {{1, 2, 3}, {0, 2, 3}, {1, 0, 3}, {0, 1, 2}};
     static const double kSg[4][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {1, 1, 1}};
     static const int kVtfSign[4] = {1, -1, 1, -1};  // vtf signs (Discretization.hpp:6239-6267)
+    // star matrix of eps, or of sigma over the star's tets whose sigma has a
+    // non-zero determinant (:8897); returns whether such a tet exists
+    auto star_mass = [&](uint32_t nid, bool sigma, std::vector<double>& E) {
+      const int64_t b0 = star_ptr_[nid];
+      const int n = (int)(star_ptr_[nid + 1] - b0);
+      E.assign((size_t)n * n, 0.0);
+      bool any = false;
+      for (int64_t q = nvol_ptr_[nid]; q < nvol_ptr_[nid + 1]; q++) {
+        const int32_t vv = nvol_[q];
+        const Mat3& mat = sigma ? sc_.materials.at(vol_mat_[vv]).sigma : sc_.materials.at(vol_mat_[vv]).eps;
+        if (sigma && mat_det(mat) == 0) continue;
+        any = true;
+        auto el = vol_edges(vv);
+        auto fv = primal_area(vv);
+        const double V = std::fabs(cell_vol_[vv]);
+        int k = 0;
+        while (vols_[vv][k] != (int32_t)nid) k++;
+        int li[3];
+        V3 w[3];
+        for (int a = 0; a < 3; a++) {
+          li[a] = (int)(std::lower_bound(star_edge_.begin() + b0, star_edge_.begin() + b0 + n, el[kEd[k][a]]) -
+                        (star_edge_.begin() + b0));
+          w[a] = scale(fv[kFv[k][a]], kSg[k][a] * 2.0 / 3.0 / V * kVtfSign[kFv[k][a]]);
+        }
+        for (int a = 0; a < 3; a++)
+          for (int b = a; b < 3; b++) {
+            double val = dot(w[a], mv(mat, w[b])) * V / 4;
+            E[li[a] * n + li[b]] += val;
+            if (a != b) E[li[b] * n + li[a]] = E[li[a] * n + li[b]];
+          }
+      }
+      return any;
+    };
     // node stars in parallel, each into its own lists, then concatenated in
     // node order (the order a sequential pass would list them)
     const size_t NP = pts_.size();
     std::vector<HostCsr::Trips> ein_n(NP), h_n(NP);
     parallel_for((int64_t)NP, nth, [&](int64_t n0, int64_t n1) {
+      std::vector<double> E;
       for (uint32_t nid = (uint32_t)n0; nid < (uint32_t)n1; nid++) {
         HostCsr::Trips& einv_t = ein_n[nid];
         HostCsr::Trips& h_t = h_n[nid];
         const int64_t b0 = star_ptr_[nid];
         const int n = (int)(star_ptr_[nid + 1] - b0);
-        std::vector<double> E(n * n, 0.0);
-        for (int64_t q = nvol_ptr_[nid]; q < nvol_ptr_[nid + 1]; q++) {
-          const int32_t vv = nvol_[q];
-          auto el = vol_edges(vv);
-          auto fv = primal_area(vv);
-          const double V = std::fabs(cell_vol_[vv]);
-          const Mat3& eps = sc_.materials.at(vol_mat_[vv]).eps;
-          int k = 0;
-          while (vols_[vv][k] != (int32_t)nid) k++;
-          int li[3];
-          V3 w[3];
-          for (int a = 0; a < 3; a++) {
-            li[a] = (int)(std::lower_bound(star_edge_.begin() + b0, star_edge_.begin() + b0 + n, el[kEd[k][a]]) -
-                          (star_edge_.begin() + b0));
-            w[a] = scale(fv[kFv[k][a]], kSg[k][a] * 2.0 / 3.0 / V * kVtfSign[kFv[k][a]]);
-          }
-          for (int a = 0; a < 3; a++)
-            for (int b = a; b < 3; b++) {
-              double val = dot(w[a], mv(eps, w[b])) * V / 4;
-              E[li[a] * n + li[b]] += val;
-              if (a != b) E[li[b] * n + li[a]] = E[li[a] * n + li[b]];
-            }
-        }
+        star_mass(nid, false, E);
         std::vector<double> Hl = E;
         spd_inv(Hl, n);
         for (int j = 0; j < n; j++)
@@ -781,6 +863,7 @@ void TetSim::build_ops() {
               einv_t.push_back({(uint32_t)star_edge_[b0 + j], (uint32_t)star_edge_[b0 + k], Hl[j * n + k]});
               if (j != k) einv_t.push_back({(uint32_t)star_edge_[b0 + k], (uint32_t)star_edge_[b0 + j], Hl[j * n + k]});
             }
+        if (dga_frac_) continue;  // the masked inverses need dt (below)
         // masked inverse (Discretization.hpp:9263-9333)
         for (int j = 0; j < n; j++)
           if (cls_[star_edge_[b0 + j]] == 4) {
@@ -800,16 +883,97 @@ void TetSim::build_ops() {
         }
       }
     });
-    HostCsr::Trips einv_t, h_t;
+    HostCsr::Trips einv_t;
     for (size_t nid = 0; nid < NP; nid++) {
       einv_t.insert(einv_t.end(), ein_n[nid].begin(), ein_n[nid].end());
-      h_t.insert(h_t.end(), h_n[nid].begin(), h_n[nid].end());
       HostCsr::Trips().swap(ein_n[nid]);
-      HostCsr::Trips().swap(h_n[nid]);
     }
     HostCsr Einv = HostCsr::build(NE, NE, einv_t, nth);
-    H_ = HostCsr::build(NE, NE, h_t, nth);
     dt_est_ = sim_.courant * estimate_dt(Einv, false);
+    if (dga_frac_) {
+      // conducting tets (Discretization.hpp:9262-9475) with the run's dt: a
+      // star with a conducting tet gets H = (E + dt/2 S)^-1 and PQ =
+      // H (E - dt/2 S), else H = E^-1 and PQ = I, Dirichlet rows and
+      // columns masked.  Class-1 and class-2 rows (never in one star) are
+      // filled from the upper triangle and its mirror; the mirror's row is
+      // the column edge's own when it has the row's class, else that of the
+      // class's first edge (the reference indexes the mirror through
+      // zero-filled h_index / p_index vectors, :6546-6547).  P of a class-2
+      // edge is the diagonal of PQ in the star of its higher node (the star
+      // the reference writes last).  A fractured star's rows go to Q and Mq.
+      double dt = dt_est_;
+      if (sim_.step != 0 && !(sim_.step > dt)) dt = sim_.step;
+      int32_t first_of[5] = {-1, -1, -1, -1, -1};
+      for (uint32_t e = 0; e < NE; e++)
+        if (first_of[cls_[e]] < 0) first_of[cls_[e]] = (int32_t)e;
+      hp_.assign(NE, 1.0);
+      std::vector<HostCsr::Trips> q_n(NP), mq_n(NP);
+      parallel_for((int64_t)NP, nth, [&](int64_t n0, int64_t n1) {
+        std::vector<double> E, S;
+        for (uint32_t nid = (uint32_t)n0; nid < (uint32_t)n1; nid++) {
+          const int64_t b0 = star_ptr_[nid];
+          const int n = (int)(star_ptr_[nid + 1] - b0);
+          const int32_t* gi = star_edge_.data() + b0;
+          star_mass(nid, false, E);
+          const bool sig_node = star_mass(nid, true, S);
+          for (int j = 0; j < n; j++)
+            if (cls_[gi[j]] == 4) {
+              for (int k = 0; k < n; k++) E[j * n + k] = E[k * n + j] = S[j * n + k] = S[k * n + j] = 0;
+              E[j * n + j] = 1;
+            }
+          std::vector<double> Hl(E), PQ((size_t)n * n, 0.0);
+          if (sig_node) {
+            for (size_t q = 0; q < Hl.size(); q++) Hl[q] += 0.5 * dt * S[q];
+            spd_inv(Hl, n);
+            for (int j = 0; j < n; j++)
+              for (int k = 0; k < n; k++) {
+                double acc = 0;
+                for (int m = 0; m < n; m++) acc += Hl[j * n + m] * (E[m * n + k] - 0.5 * dt * S[m * n + k]);
+                PQ[j * n + k] = acc;
+              }
+          } else {
+            spd_inv(Hl, n);
+            for (int j = 0; j < n; j++) PQ[j * n + j] = 1;
+          }
+          HostCsr::Trips& h_t = h_n[nid];
+          const int64_t off = frac_off_[nid];
+          for (int j = 0; j < n; j++) {
+            const int32_t ej = gi[j];
+            const int c = cls_[ej];
+            if (c == 4) continue;
+            if (c == 1 || c == 2) {
+              if (c == 2 && (int32_t)nid == std::max(edges_[ej][0], edges_[ej][1])) hp_[ej] = PQ[j * n + j];
+              for (int k = j; k < n; k++) {
+                const int32_t ek = gi[k];
+                if (cls_[ek] == 4 || Hl[j * n + k] == 0) continue;
+                h_t.push_back({(uint32_t)ej, (uint32_t)ek, Hl[j * n + k]});
+                if (j != k) h_t.push_back({(uint32_t)(cls_[ek] == c ? ek : first_of[c]), (uint32_t)ej, Hl[j * n + k]});
+              }
+            }
+            if (off >= 0)
+              for (int k = 0; k < n; k++) {
+                if (cls_[gi[k]] == 4) continue;
+                const uint32_t r = (uint32_t)(off + j);
+                if (PQ[j * n + k] != 0) q_n[nid].push_back({r, (uint32_t)(off + k), PQ[j * n + k]});
+                if (Hl[j * n + k] != 0) mq_n[nid].push_back({r, (uint32_t)gi[k], Hl[j * n + k]});
+              }
+          }
+        }
+      });
+      HostCsr::Trips q_t, mq_t;
+      for (size_t nid = 0; nid < NP; nid++) {
+        q_t.insert(q_t.end(), q_n[nid].begin(), q_n[nid].end());
+        mq_t.insert(mq_t.end(), mq_n[nid].begin(), mq_n[nid].end());
+      }
+      Q_ = HostCsr::build(q_size_, q_size_, q_t, nth);
+      Mq_ = HostCsr::build(q_size_, NE, mq_t, nth);
+    }
+    HostCsr::Trips h_t;
+    for (size_t nid = 0; nid < NP; nid++) {
+      h_t.insert(h_t.end(), h_n[nid].begin(), h_n[nid].end());
+      HostCsr::Trips().swap(h_n[nid]);
+    }
+    H_ = HostCsr::build(NE, NE, h_t, nth);
   } else if (method_ == 3) {
     // fem: Whitney edge mass (Discretization.hpp:7902-8060).  Per tet, the
     // barycentric coordinates l_1..l_3 = J^-1 (p - x_0), l_0 = 1 - l_1 - l_2 - l_3
@@ -1652,6 +1816,22 @@ void TetSim::alloc_and_upload() {
   };
   upcsr(N_, d.n_ptr, d.n_col, d.n_val);
   upcsr(H_, d.h_ptr, d.h_col, d.h_val);
+  if (dga_frac_) {
+    d.h_p = upT(hp_);
+    d.nq = (int)q_size_;
+    d.nfe = (int)fe_edge_.size();
+    if (d.nq > 0) {
+      upcsr(Q_, d.q_ptr, d.q_col, d.q_val);
+      upcsr(Mq_, d.mq_ptr, d.mq_col, d.mq_val);
+      d.Uc = zeros(q_size_);
+      d.Uc_old = zeros(q_size_);
+    }
+    if (d.nfe > 0) {
+      d.fe_edge = (const int32_t*)up(fe_edge_.data(), fe_edge_.size() * 4);
+      d.fe_a = (const int32_t*)up(fe_a_.data(), fe_a_.size() * 4);
+      d.fe_b = (const int32_t*)up(fe_b_.data(), fe_b_.size() * 4);
+    }
+  }
   const size_t nsrc = src_labels_.size();
   d.nse = (int)src_edge_.size();
   d.nsrc = (int)nsrc;
@@ -1667,8 +1847,10 @@ void TetSim::alloc_and_upload() {
   d.carrier = (const double*)up(carrier_.data(), carrier_.size() * 8);
   d.flux = (double*)dalloc((nsteps_ + 1) * 8);
   CU(cudaMemsetAsync(d.flux, 0, (nsteps_ + 1) * 8, stream_));
+  // tet_h_update's block partials, then tet_frac_gather's
   d.nflux_part = (int)((NE + 255) / 256);
   if (d.nflux_part < 1) d.nflux_part = 1;
+  if (d.nfe > 0) d.nflux_part += (d.nfe + 255) / 256;
   d.flux_part = (double*)dalloc((size_t)d.nflux_part * 8);
   CU(cudaMemsetAsync(d.flux_part, 0, (size_t)d.nflux_part * 8, stream_));
   // probes
@@ -1830,6 +2012,8 @@ void TetSim::get_state(double* U, double* B, double* F) {
 
 void TetSim::set_state(const double* U, const double* F) {
   if (group_) return group_->set_state(0, U, F);
+  if (U && q_size_ > 0)
+    throw UnsupportedError("tf_set_state: a dga run with fractured edges keeps node-star fractions that U does not fix");
   const bool f32 = opt_.precision == 1;
   auto put = [&](void* dst, const double* src, size_t n) {
     if (!src) return;

@@ -118,7 +118,18 @@ class TetSim : public Sim {
   std::vector<int32_t> nvol_;
   std::vector<int32_t> bnd_edge_;                  // edge -> boundary dual index or -1
   std::vector<std::array<double, 3>> bnd_dual_;
-  std::vector<uint8_t> cls_;                       // 1 interior dof, 4 Dirichlet
+  std::vector<uint8_t> cls_;                       // 1 interior dof, 4 Dirichlet; dga with
+                                                   // conducting tets: 2 uniformly conducting,
+                                                   // 3 fractured
+  // dga with conducting tets: class-1 and class-2 rows share H_ (U = P U +
+  // dt H cf, P = 1 on class 1); fractured edges sum two node-star fractions
+  // U_c, which step as U_c = Q U_c_old + dt Mq cf
+  bool dga_frac_ = false;                          // some edge of class 2 or 3
+  std::vector<double> hp_;                         // P per edge (dga_frac_ only)
+  HostCsr Q_, Mq_;                                 // U_c rows
+  std::vector<int64_t> frac_off_;                  // node -> U_c offset, -1 if not fractured
+  uint32_t q_size_ = 0;
+  std::vector<int32_t> fe_edge_, fe_a_, fe_b_;     // fractured edges and their two U_c entries
   std::vector<uint8_t> pec_;
   std::vector<std::vector<uint32_t>> edge_src_;
   // operators

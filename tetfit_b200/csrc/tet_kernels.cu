@@ -6,7 +6,11 @@
 //                     (Discretization.hpp:902-916)
 //   tet_nmul          F -= dt N cu (:917)
 //   tet_curl_f        cf = C^T F + Ctb Fb - I (:878-879)
-//   tet_h_update      U += dt H cf on interior edges, boundary flux (:889-894)
+//   tet_h_update      U = P U + dt H cf on interior edges (P = 1 when
+//                     lossless), boundary flux (:887-894)
+//   tet_frac_update   U_c = Q U_c_old + dt Mq cf: node-star fractions of the
+//                     fractured edges (:891)
+//   tet_frac_gather   U = sum of a fractured edge's two fractions (:892), flux
 //   tet_sources       source edges from the carrier table: E values, boundary
 //                     dual-edge H sources, currents (:821-868)
 //   tet_probes        Whitney E and face-flux H at probe points (:3768-3897)
@@ -100,13 +104,45 @@ __global__ void __launch_bounds__(kBlock) tet_h_update(DevPtrs d) {
     for (int64_t k = d.h_ptr[e]; k < d.h_ptr[e + 1]; k++) s += ld<T>(d.h_val, k) * cf[d.h_col[k]];
     T* U = (T*)d.U;
     const T uo = U[e];
-    const T un = uo + (T)d.dt * s;
+    const T un = d.h_p ? ((const T*)d.h_p)[e] * uo + (T)d.dt * s : uo + (T)d.dt * s;
     U[e] = un;
     const T cb = ((const T*)d.cb)[e];
     if (cb != (T)0) fl = ((double)uo + (double)un) * (double)cb;
   }
   fl = block_sum(fl, sh);
   if (threadIdx.x == 0) d.flux_part[blockIdx.x] = fl;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock) tet_frac_update(DevPtrs d) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= d.nq) return;
+  const T* uo = (const T*)d.Uc_old;
+  const T* cf = (const T*)d.cf;
+  T a = 0, b = 0;
+  for (int64_t k = d.q_ptr[r]; k < d.q_ptr[r + 1]; k++) a += ld<T>(d.q_val, k) * uo[d.q_col[k]];
+  for (int64_t k = d.mq_ptr[r]; k < d.mq_ptr[r + 1]; k++) b += ld<T>(d.mq_val, k) * cf[d.mq_col[k]];
+  ((T*)d.Uc)[r] = a + (T)d.dt * b;
+}
+
+// flux partials after tet_h_update's, at flux_part[nblk(nE) + block]
+template <typename T>
+__global__ void __launch_bounds__(kBlock) tet_frac_gather(DevPtrs d, int part0) {
+  __shared__ double sh[33];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double fl = 0.0;
+  if (i < d.nfe) {
+    const T* uc = (const T*)d.Uc;
+    const int e = d.fe_edge[i];
+    T* U = (T*)d.U;
+    const T uo = U[e];
+    const T un = uc[d.fe_a[i]] + uc[d.fe_b[i]];
+    U[e] = un;
+    const T cb = ((const T*)d.cb)[e];
+    if (cb != (T)0) fl = ((double)uo + (double)un) * (double)cb;
+  }
+  fl = block_sum(fl, sh);
+  if (threadIdx.x == 0) d.flux_part[part0 + blockIdx.x] = fl;
 }
 
 // Source edges: E sources write U, H sources write cb (reset each step),
@@ -312,6 +348,11 @@ cudaError_t tet_launch_step(const DevPtrs& d, cudaStream_t st, cudaEvent_t* ev) 
   if (ev) cudaEventRecord(ev[1], st);
   tet_curl_f<T><<<nblk(d.nE), kBlock, 0, st>>>(d);
   tet_h_update<T><<<nblk(d.nE), kBlock, 0, st>>>(d);
+  if (d.nq > 0) {
+    cudaMemcpyAsync(d.Uc_old, d.Uc, sizeof(T) * (size_t)d.nq, cudaMemcpyDeviceToDevice, st);
+    tet_frac_update<T><<<nblk(d.nq), kBlock, 0, st>>>(d);
+  }
+  if (d.nfe > 0) tet_frac_gather<T><<<nblk(d.nfe), kBlock, 0, st>>>(d, (int)nblk(d.nE));
   if (ev) cudaEventRecord(ev[2], st);
   flux_reduce<<<1, kBlock, 0, st>>>(d, 0.5);
   if (ev) cudaEventRecord(ev[3], st);

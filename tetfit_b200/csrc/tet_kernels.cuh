@@ -29,6 +29,17 @@ struct DevPtrs {
   const int32_t *n_col = nullptr, *h_col = nullptr, *a_col = nullptr;
   const void *n_val = nullptr, *h_val = nullptr, *a_val = nullptr;
   const void* jac = nullptr;
+  // dga with conducting tets: P per edge (null when lossless), the node-star
+  // fractions U_c (and their copy from the step before) with their operators
+  // Q (U_c x U_c) and Mq (U_c x edges), and the fractured edges with their
+  // two U_c entries
+  const void* h_p = nullptr;
+  int nq = 0, nfe = 0;
+  const int64_t *q_ptr = nullptr, *mq_ptr = nullptr;
+  const int32_t *q_col = nullptr, *mq_col = nullptr;
+  const void *q_val = nullptr, *mq_val = nullptr;
+  void *Uc = nullptr, *Uc_old = nullptr;
+  const int32_t *fe_edge = nullptr, *fe_a = nullptr, *fe_b = nullptr;
   // CG work (T), reductions, grid barrier and statistics
   void *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *rhs = nullptr;
   double *part_a = nullptr, *part_b = nullptr;
