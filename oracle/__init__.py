@@ -170,6 +170,7 @@ class TetOracle:
             L.orc_tet_matrix.restype = ctypes.c_longlong
             L.orc_tet_matrix.argtypes = [P, ctypes.c_int, P, P, P]
             L.orc_tet_dga_p.argtypes = [P, P]
+            L.orc_tet_dga_r.argtypes = [P, P]
             L._tet_sigs = True
         err = ctypes.create_string_buffer(1024)
         self.h = L.orc_tet_open(os.fsencode(script), label, int(consistent_mass), err, 1024)
@@ -238,12 +239,20 @@ class TetOracle:
         nq = int(self.L.orc_tet_dga_p(self.h, _p(P)))
         return P, nq
 
+    def dga_r(self):
+        """dga: (R per face: 1 on class-1, R_r on class-2 faces; number of
+        class-2 faces)."""
+        R = np.zeros(self.nF)
+        nr = int(self.L.orc_tet_dga_r(self.h, _p(R)))
+        return R, nr
+
     def matrix(self, which: str):
         """CSR (ptr, col, val) of one operator: C, N, H (dga), E, Sig (the
-        conductivity mass) or A (gfdtd, fem)."""
-        w = {"C": 0, "N": 1, "H": 2, "E": 3, "A": 4, "Sig": 5}[which]
+        conductivity mass), A (gfdtd, fem) or Nmag (dga: the N or Tr row of
+        each face, the operator of the F update)."""
+        w = {"C": 0, "N": 1, "H": 2, "E": 3, "A": 4, "Sig": 5, "Nmag": 6}[which]
         nnz = int(self.L.orc_tet_matrix(self.h, w, None, None, None))
-        nrows = {0: self.nF, 1: self.nF, 2: self.nE, 3: self.nE, 4: self.n_free, 5: self.nE}[w]
+        nrows = {0: self.nF, 1: self.nF, 2: self.nE, 3: self.nE, 4: self.n_free, 5: self.nE, 6: self.nF}[w]
         ptr = np.zeros(nrows + 1, dtype=np.uint64)
         col = np.zeros(nnz, dtype=np.uint32)
         val = np.zeros(nnz)

@@ -405,11 +405,19 @@ int orc_tet_dga_p(void* h, double* P) {
   return (int)o->Q_size;
 }
 
-// CSR export of an operator: which 0 C, 1 N, 2 H, 3 E, 4 A; returns nnz
+// dga: R per face (1 on class-1 faces, R_r on class-2 faces)
+int orc_tet_dga_r(void* h, double* R) {
+  auto* o = static_cast<orc::TetOracle*>(h);
+  for (size_t f = 0; f < o->faces.size(); f++) R[f] = o->fcls[f] == 1 ? 1.0 : o->R_r[o->r_index[f]];
+  return (int)o->R_size;
+}
+
+// CSR export of an operator: which 0 C, 1 N, 2 H, 3 E, 4 A, 5 Sig, 6 the dga F-update
+// operator (Na / Tr rows by face); returns nnz
 long long orc_tet_matrix(void* h, int which, unsigned long long* ptr, unsigned* col, double* val) {
   auto* o = static_cast<orc::TetOracle*>(h);
   const orc::Csr* m = which == 0 ? &o->C : which == 1 ? &o->N : which == 2 ? &o->H : which == 3 ? &o->E
-                     : which == 5 ? &o->Sig : &o->A;
+                     : which == 5 ? &o->Sig : which == 6 ? &o->Nv : &o->A;
   if (ptr) for (size_t i = 0; i < m->ptr.size(); i++) ptr[i] = m->ptr[i];
   if (col) std::memcpy(col, m->col.data(), m->col.size() * sizeof(unsigned));
   if (val) std::memcpy(val, m->val.data(), m->val.size() * sizeof(double));

@@ -281,8 +281,9 @@ void TetOracle::read_mesh() {
     cell_vol.push_back(dot(v1, cross(v2, v3)) / 6.0);
     const Material& mt = sc.materials[tt[k].second];
     // conductivity enters gfdtd and fem through SigMat and dga through its
-    // edge classes; magnetic losses (chi, the face classes) are not restated
-    if (!mat_zero(mt.chi)) throw std::runtime_error("magnetic losses (chi) on tetrahedra are outside the supported path");
+    // edge classes; magnetic losses (chi) enter dga through its face classes
+    if (!mat_zero(mt.chi) && method != 1)
+      throw std::runtime_error("magnetic losses (chi) on tetrahedra are supported with method dga only");
   }
   // unique faces (Discretization.hpp:10173-10219)
   std::sort(tri.begin(), tri.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
@@ -462,10 +463,11 @@ std::array<std::array<double, 3>, 4> TetOracle::primal_area_vectors(uint32_t v) 
   return r;
 }
 
-void TetOracle::local_M(uint32_t v, double M[4][4]) const {
-  // per-tet magnetic mass from dual area vectors (Discretization.hpp:8754-8776)
+void TetOracle::local_M(uint32_t v, double M[4][4], const Mat3* mat) const {
+  // per-tet magnetic mass from dual area vectors (Discretization.hpp:8754-8776);
+  // with chi in place of mu it is the magnetic-loss matrix Z (:8778-8802)
   auto fv = dual_area_vectors(v);
-  const Mat3& mu = sc.materials.at(vol_mat[v]).mu;
+  const Mat3& mu = mat ? *mat : sc.materials.at(vol_mat[v]).mu;
   auto d = [&](int a, int b) { return dot(fv[a], matvec(mu, fv[b])); };
   const double c = 36.0 / std::fabs(cell_vol[v]);
   M[0][0] = (d(0, 0) + d(2, 2) + d(3, 3)) * c;
@@ -627,6 +629,87 @@ void TetOracle::build_dga() {
   if (sim.step != 0) {
     if (sim.step > dt) possibly_unstable = true;
     else dt = sim.step;
+  }
+  // face classes (:6357-6542): a face is class 1 when its first tet has
+  // chi = 0, else 2, unless its tets differ in chi (or, with chi, in mu): the
+  // reference then makes it fractured (3), whose old values it maps onto the
+  // electric state vector (Old_F_c, :586), which is refused here.  Per tet
+  // (:9128-9205): N = (M + dt/2 Z)^-1 and RS = N (M - dt/2 Z) when chi has a
+  // non-zero determinant, else N = M^-1 and RS = I; class-1 rows of N go to
+  // Na, class-2 rows to Tr with R_r the diagonal of RS (the face's last tet
+  // writes it).
+  {
+    const uint32_t NF = (uint32_t)faces.size();
+    auto same = [](const Mat3& a, const Mat3& b) {
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++)
+          if (a.m[i][j] != b.m[i][j]) return false;
+      return true;
+    };
+    fcls.assign(NF, 1);
+    n_index.assign(NF, 0);
+    r_index.assign(NF, 0);
+    N_size = R_size = 0;
+    for (uint32_t f = 0; f < NF; f++) {
+      const Material& m0 = sc.materials.at(vol_mat[ftv[f][0].first]);
+      if (ftv[f].size() == 2) {
+        const Material& m1 = sc.materials.at(vol_mat[ftv[f][1].first]);
+        if ((!mat_zero(m0.chi) || !mat_zero(m1.chi)) && (!same(m0.chi, m1.chi) || !same(m0.mu, m1.mu)))
+          throw std::runtime_error("fractured magnetic-loss faces (chi or mu changing across a face with chi) are "
+                                   "outside the supported path: the reference reads their old values from the "
+                                   "electric state");
+      }
+      if (mat_zero(m0.chi)) {
+        fcls[f] = 1;
+        n_index[f] = N_size++;
+      } else {
+        fcls[f] = 2;
+        r_index[f] = R_size++;
+      }
+    }
+    std::vector<Csr::Trip> na_t, tr_t;
+    R_r.assign(R_size, 0.0);
+    for (uint32_t v = 0; v < vols.size(); v++) {
+      const Mat3& chi = sc.materials.at(vol_mat[v]).chi;
+      double M[4][4], Z[4][4];
+      local_M(v, M);
+      std::vector<double> Nl(16), RS(16, 0.0);
+      if (mat_det(chi) != 0) {
+        local_M(v, Z, &chi);
+        for (int i = 0; i < 4; i++)
+          for (int j = 0; j < 4; j++) Nl[4 * i + j] = M[i][j] + 0.5 * dt * Z[i][j];
+        spd_inverse(Nl, 4);
+        for (int i = 0; i < 4; i++)
+          for (int j = 0; j < 4; j++) {
+            double acc = 0;
+            for (int m = 0; m < 4; m++) acc += Nl[4 * i + m] * (M[m][j] - 0.5 * dt * Z[m][j]);
+            RS[4 * i + j] = acc;
+          }
+      } else {
+        for (int i = 0; i < 4; i++)
+          for (int j = 0; j < 4; j++) Nl[4 * i + j] = M[i][j];
+        spd_inverse(Nl, 4);
+        for (int i = 0; i < 4; i++) RS[5 * i] = 1;
+      }
+      for (int j = 0; j < 4; j++) {
+        const uint32_t f = vtf[v][j].first;
+        if (fcls[f] == 2) R_r[r_index[f]] = RS[5 * j];
+        for (int k = 0; k < 4; k++)
+          if (Nl[4 * j + k] != 0) {
+            if (fcls[f] == 1) na_t.push_back({n_index[f], vtf[v][k].first, Nl[4 * j + k]});
+            else tr_t.push_back({r_index[f], vtf[v][k].first, Nl[4 * j + k]});
+          }
+      }
+    }
+    Na = Csr::build(N_size, NF, na_t);
+    Tr = Csr::build(R_size, NF, tr_t);
+    std::vector<Csr::Trip> nv;
+    for (uint32_t f = 0; f < NF; f++) {
+      const Csr& m = fcls[f] == 1 ? Na : Tr;
+      const uint32_t r = fcls[f] == 1 ? n_index[f] : r_index[f];
+      for (uint64_t q = m.ptr[r]; q < m.ptr[r + 1]; q++) nv.push_back({f, m.col[q], m.val[q]});
+    }
+    Nv = Csr::build(NF, NF, nv);
   }
   // masked node-star inverses (:9262-9475).  A star with a conducting tet
   // (sigma_node, :8897) gets H = (E + dt/2 S)^-1 and PQ = H (E - dt/2 S),
@@ -1209,6 +1292,7 @@ void TetOracle::prepare(uint32_t label) {
   const size_t NE = edges.size(), NF = faces.size();
   U.assign(NE, 0); I.assign(NE, 0); F.assign(NF, 0); B.assign(NF, 0);
   U_a.assign(H_size, 0); U_b.assign(P_size, 0); U_c.assign(Q_size, 0); U_c_old = U_c;
+  F_a.assign(N_size, 0); F_b.assign(R_size, 0);
   Fb.assign(bnd_dual.size(), 0); Fb_old = Fb; SrcFld.assign(NE, 0);
   solution.assign(free_edges.size(), 0);
   if (out.mode == "silo") {
@@ -1319,13 +1403,16 @@ void TetOracle::dga_step(double t) {
   double fl = 0;
   for (uint32_t e = 0; e < NE; e++) fl += (U_old[e] + U[e]) * curl_b[e];
   flux.push_back(0.5 * fl);
-  std::vector<double> cu(faces.size()), ncu(faces.size());
+  // B -= dt cu, F_a -= dt Na cu, F_b = R_r .* F_b - dt Tr cu, F = T F_frac
+  // (:912-918)
+  std::vector<double> cu(faces.size()), na(N_size), tr(R_size);
   C.mul(U.data(), cu.data());
-  N.mul(cu.data(), ncu.data());
-  for (size_t f = 0; f < faces.size(); f++) {
-    B[f] = B[f] - dt * cu[f];
-    F[f] = F[f] - dt * ncu[f];
-  }
+  Na.mul(cu.data(), na.data());
+  Tr.mul(cu.data(), tr.data());
+  for (size_t f = 0; f < faces.size(); f++) B[f] = B[f] - dt * cu[f];
+  for (uint32_t r = 0; r < N_size; r++) F_a[r] = F_a[r] - dt * na[r];
+  for (uint32_t r = 0; r < R_size; r++) F_b[r] = R_r[r] * F_b[r] - dt * tr[r];
+  for (size_t f = 0; f < faces.size(); f++) F[f] = fcls[f] == 1 ? F_a[n_index[f]] : F_b[r_index[f]];
   if ((out.mode == "probepoint" || out.mode == "silo") && out.allow_print(t)) export_probes(t);
 }
 

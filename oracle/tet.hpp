@@ -66,6 +66,14 @@ struct TetOracle {
   uint32_t H_size = 0, P_size = 0, Q_size = 0;
   Csr Ha, Mp, Q, Mq;                   // H_size x E, P_size x E, Q_size x Q_size, Q_size x E
   std::vector<double> P_p, U_a, U_b, U_c, U_c_old;
+  // dga with magnetic losses (face classes, :6357-6542, 9128-9205): F is T
+  // times F_frac = [F_a (class-1 faces, rows of Na), F_b (class-2, rows of Tr)]
+  std::vector<uint8_t> fcls;               // face -> 1 (chi = 0) or 2 (chi, uniform across it)
+  std::vector<uint32_t> n_index, r_index;  // face -> row of Na / Tr
+  uint32_t N_size = 0, R_size = 0;
+  Csr Na, Tr;                              // N_size x F, R_size x F
+  Csr Nv;                                  // F x F view: the Na or Tr row of each face
+  std::vector<double> R_r, F_a, F_b;
   Csr E;                               // E x E eps mass (gfdtd: node-star dual basis; fem: Whitney)
   Csr Sig;                             // E x E conductivity mass (SigMat), same construction with sigma
   bool lossy = false;                  // some tet conducts (sigma with non-zero determinant)
@@ -107,7 +115,7 @@ struct TetOracle {
   std::array<uint32_t, 6> vol_edges(uint32_t v) const;
   std::array<std::array<double, 3>, 6> dual_area_vectors(uint32_t v) const;
   std::array<std::array<double, 3>, 4> primal_area_vectors(uint32_t v) const;
-  void local_M(uint32_t v, double M[4][4]) const;
+  void local_M(uint32_t v, double M[4][4], const Mat3* mat = nullptr) const;  // mat: mu by default
   Csr assemble_N() const;
   uint32_t find_probe(const std::array<double, 3>& pv);
   double efield_source(uint32_t e, double t);

@@ -6,7 +6,11 @@ SysMat = E + (dt/2) SigMat (gfdtd, :8644) or E / dt^2 + (0.5/dt) SigMat (fem,
 Joule-loss column of poynting.dat (:1518-1546, :1733-1757).  dga: the edge
 classes (:6186-6215, :6776-6903) and the node-star operators H, P, Q, Mq of
 :9262-9475 stepped as :887-892; dga never fills its SigMat, so its loss
-column stays zero.  Magnetic losses (chi) stay outside the supported path."""
+column stays zero.  Magnetic losses (chi) on dga: the face classes
+(:6357-6542) and per-tet operators (:9128-9205) stepped as :912-918, for
+faces whose tets share chi; fractured faces, whose old values the reference
+reads from the electric state (:586), are refused, and so is chi on gfdtd
+and fem."""
 import numpy as np
 import pytest
 
@@ -223,4 +227,91 @@ def test_conducting_dga_state_cannot_be_set(tmp_path, product_lib):
         U, _, F = d.state()
         with pytest.raises(tb.TetfitError) as e:
             d.set_state(U, F)
+    assert e.value.code == tb.TF_E_UNSUPPORTED
+
+
+MU0_SCRIPT = 4e-7 * np.pi  # the reference's vacuum permeability
+
+
+def test_uniform_magnetic_loss_dga_operators(tmp_path, oracle_lib):
+    """One material with chi: every face is class 2, the per-tet loss matrix
+    is chi / (mu_r mu0) times the magnetic mass, so the F-update operator is
+    the lossless N / (1 + b) and R = (1 - b) / (1 + b), b = dt chi / (2 mu_r
+    mu0) (CPU, oracle)."""
+    ops = {}
+    for chi in (0.0, 400.0):
+        s = write_tet_case(str(tmp_path / str(chi)), lossy_case("dga", eps=(2.0,), mu=(1.5,), chi=(chi,),
+                                                                split_x=False))
+        o = oracle.TetOracle(s)
+        ops[chi] = (csr(o.matrix("Nmag"), o.nF), o.dga_r(), o.dt)
+        o.close()
+    N0, (R0, nr0), dt = ops[0.0]
+    N1, (R1, nr1), dt1 = ops[400.0]
+    assert dt == dt1 and nr0 == 0 and np.all(R0 == 1) and nr1 == len(R1)
+    b = dt * 400.0 / (2 * 1.5 * MU0_SCRIPT)
+    assert 0.01 < b < 1
+    assert np.abs(R1 - (1 - b) / (1 + b)).max() <= 1e-12
+    d = N1 - N0 / (1 + b)
+    assert abs(d).max() <= 1e-12 * abs(N1).max()
+
+
+def test_magnetic_loss_damps_the_field(tmp_path, oracle_lib):
+    """A pulse in a PEC box filled with one magnetically lossy material ends
+    with less field than without (CPU, oracle)."""
+    norms = {}
+    for chi in (0.0, 400.0):
+        s = write_tet_case(str(tmp_path / str(chi)), lossy_case("dga", steps=80, eps=(2.0,), chi=(chi,), split_x=False,
+                                                                sigma=(0.0,)))
+        o = oracle.TetOracle(s)
+        o.run()
+        norms[chi] = np.linalg.norm(o.state()[2])
+        o.close()
+    assert norms[400.0] < 0.5 * norms[0.0]
+
+
+@pytest.mark.parametrize("method,kw", [("dga", dict(chi=(0.0, 400.0))), ("dga", dict(chi=(400.0, 400.0), mu=(1.0, 2.0))),
+                                       ("gfdtd", dict(chi=(400.0, 400.0)))])
+def test_oracle_refuses_unsupported_magnetic_losses(tmp_path, oracle_lib, method, kw):
+    """dga faces whose tets differ in chi (or in mu, with chi) are fractured in
+    the reference, which reads their old values from the electric state
+    (:586); gfdtd and fem have no magnetic-loss path that the oracle follows."""
+    s = write_tet_case(str(tmp_path), lossy_case(method, **kw))
+    with pytest.raises(Exception):
+        oracle.TetOracle(s)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kw", [dict(eps=(2.0,), mu=(1.5,), chi=(400.0,), sigma=(0.0,), split_x=False),
+                                dict(eps=(1.5, 3.0), chi=(250.0, 250.0), sigma=(0.0, 0.02))])
+def test_magnetic_loss_dga_matches_oracle(tmp_path, product_lib, oracle_lib, kw):
+    """Class-2 faces (and, in the second scene, conducting and fractured
+    edges as well) on the GPU against the oracle's F_frac restatement: FP64
+    within 1e-10 on probes, U, F and flux; FP32 within 2e-5 on the probes and
+    U, 1e-4 on the decayed F and the flux history."""
+    s = write_tet_case(str(tmp_path), lossy_case("dga", steps=80, **kw))
+    o = oracle.TetOracle(s)
+    o.run()
+    to, vo, _, _ = o.probes()
+    Uo, _, Fo = o.state()
+    fo = o.flux()
+    o.close()
+    for prec, tol, tol_f in (("fp64", 1e-10, 1e-10), ("fp32", 2e-5, 1e-4)):
+        with tb.Discretization(s) as d:
+            d.prepare(1, precision=prec)
+            d.step(10 ** 6)
+            t, v = d.probes()
+            U, _, F = d.state()
+            fl = d.flux()
+        assert np.array_equal(t, to) and np.abs(vo).max() > 0
+        for name, g, r, t_ in (("v", v, vo, tol), ("U", U, Uo, tol), ("F", F, Fo, tol_f), ("flux", fl, fo, tol_f)):
+            assert rel(g, r) <= t_, (prec, name, rel(g, r))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method,kw", [("dga", dict(chi=(0.0, 400.0))), ("gfdtd", dict(chi=(400.0, 400.0)))])
+def test_unsupported_magnetic_losses_are_refused(tmp_path, product_lib, method, kw):
+    s = write_tet_case(str(tmp_path), lossy_case(method, **kw))
+    with tb.Discretization(s) as d:
+        with pytest.raises(tb.TetfitError) as e:
+            d.prepare(1)
     assert e.value.code == tb.TF_E_UNSUPPORTED

@@ -234,6 +234,8 @@ class TetCase:
     seed: int = 0x7E7F17
     eps: object = (1.0,)             # eps_r per material label 1, 2, ... (tuple) or {label: eps_r}
     sigma: object = None             # conductivity (S/m) per material label, like eps (None: lossless)
+    chi: object = None               # magnetic conductivity per material label, like eps (None: 0)
+    mu: object = None                # mu_r per material label, like eps (None: 1)
     split_x: bool = False            # material 1 for x < 0.5, 2 for x >= 0.5
     pec_surfaces: tuple = (2, 3, 4, 5, 6)
     source_surface: int = 1
@@ -280,10 +282,12 @@ def write_tet_case(directory: str, case: TetCase, name: str = "box") -> str:
     lines = ["DEFINE mesh 1", "   SET type tetrahedral", f"   SET mesher {case.mesh_format}",
              f"   SET file {os.path.basename(mesh)}", "   SET name box", "   SET scalefactor 1", "END mesh 1"]
     eps_items = case.eps.items() if isinstance(case.eps, dict) else enumerate(case.eps, start=1)
-    sig = dict(case.sigma.items() if isinstance(case.sigma, dict) else enumerate(case.sigma or (), start=1))
+    per_label = lambda v: dict(v.items() if isinstance(v, dict) else enumerate(v or (), start=1))
+    sig, chi, mu = per_label(case.sigma), per_label(case.chi), per_label(case.mu)
     for m, e in eps_items:
-        lines += [f"DEFINE material {m}", f"   SET epsilon {float(e)!r}", "   SET mu 1",
-                  f"   SET sigma {float(sig.get(m, 0.0))!r}", "   SET chi 0", f"END material {m}"]
+        lines += [f"DEFINE material {m}", f"   SET epsilon {float(e)!r}", f"   SET mu {float(mu.get(m, 1.0))!r}",
+                  f"   SET sigma {float(sig.get(m, 0.0))!r}", f"   SET chi {float(chi.get(m, 0.0))!r}",
+                  f"END material {m}"]
     lines += ["DEFINE bc 1"] + [f"   SET surface {s}" for s in case.pec_surfaces] + ["   SET type pec", "END bc 1"]
     lines += source_lines(case)
     if case.probes:

@@ -371,7 +371,7 @@ void TetSim::release_host() {
   drop(vtf_); drop(ftv_); drop(fte_); drop(star_ptr_); drop(star_edge_); drop(nvol_ptr_); drop(nvol_);
   drop(bnd_edge_); drop(bnd_dual_); drop(edge_src_); drop(carrier_); drop(init_U_); drop(init_I_);
   drop(init_src_); drop(jacobi_); drop(cls_); drop(pec_);
-  drop(hp_); drop(frac_off_); drop(fe_edge_); drop(fe_a_); drop(fe_b_);
+  drop(hp_); drop(nr_); drop(frac_off_); drop(fe_edge_); drop(fe_a_); drop(fe_b_);
 }
 
 TetSim::~TetSim() {
@@ -427,8 +427,9 @@ void TetSim::read_mesh() {
     cell_vol_[k] = dot(v1, cross(v2, v3)) / 6.0;
     const Material& mt = sc_.materials[vol_mat_[k]];
     // conductivity enters gfdtd and fem through SigMat and dga through its
-    // edge classes; magnetic losses (chi, dga's face classes) are not built
-    if (!is_zero(mt.chi)) throw UnsupportedError("magnetic losses (chi) on tetrahedra are outside the supported path");
+    // edge classes; magnetic losses (chi) enter dga through its face classes
+    if (!is_zero(mt.chi) && method_ != 1)
+      throw UnsupportedError("magnetic losses (chi) on tetrahedra are supported with method dga only");
   }
   // faces: packed keys when node ids fit in 21 bits, else tuple order
   const bool packed = np < (1u << 21);
@@ -742,40 +743,38 @@ void TetSim::build_ops() {
     for (uint32_t v = 0; v < L; v++)
       if (mat_det(sc_.materials.at(vol_mat_[v]).sigma) != 0) sig_tet[v] = 1, lossy_ = true;
   // N = sum of per-tet inverse magnetic blocks (Discretization.hpp:8754-8807, 9158-9255);
-  // the blocks are formed in parallel, then listed in tet order
-  {
-    std::vector<double> blk(16 * (size_t)L);
-    parallel_for(L, nth, [&](int64_t v0, int64_t v1) {
-      for (uint32_t v = (uint32_t)v0; v < (uint32_t)v1; v++) {
-        auto es = vol_edges(v);
-        V3 eb[6], fb[4];
-        for (int i = 0; i < 6; i++) eb[i] = ebar(es[i]);
-        for (int i = 0; i < 4; i++) fb[i] = fbar(vtf_[v][i]);
-        V3 vb{0, 0, 0};
-        for (int q = 0; q < 4; q++)
-          for (int a = 0; a < 3; a++) vb[a] += pts_[vols_[v][q]][a];
-        vb = {vb[0] / 4.0, vb[1] / 4.0, vb[2] / 4.0};
-        const double sgn = cell_vol_[v] < 0 ? -0.5 : 0.5;
-        const V3 fv[6] = {scale(cross(sub(vb, eb[0]), sub(fb[2], fb[3])), sgn),
-                          scale(cross(sub(vb, eb[1]), sub(fb[0], fb[3])), sgn),
-                          scale(cross(sub(vb, eb[2]), sub(fb[3], fb[1])), sgn),
-                          scale(cross(sub(vb, eb[3]), sub(fb[1], fb[2])), sgn),
-                          scale(cross(sub(vb, eb[4]), sub(fb[2], fb[0])), sgn),
-                          scale(cross(sub(vb, eb[5]), sub(fb[0], fb[1])), sgn)};
-        const Mat3& mu = sc_.materials.at(vol_mat_[v]).mu;
-        auto d = [&](int a, int b) { return dot(fv[a], mv(mu, fv[b])); };
-        const double c = 36.0 / std::fabs(cell_vol_[v]);
-        std::vector<double> M = {(d(0, 0) + d(2, 2) + d(3, 3)) * c, (-d(1, 2) - d(3, 4)) * c,
-                                 (-d(0, 1) + d(3, 5)) * c,          (d(0, 4) + d(2, 5)) * c,
-                                 0, (d(0, 0) + d(1, 1) + d(4, 4)) * c, (-d(0, 2) - d(4, 5)) * c, (d(0, 3) - d(1, 5)) * c,
-                                 0, 0, (d(1, 1) + d(2, 2) + d(5, 5)) * c, (-d(2, 3) - d(1, 4)) * c,
-                                 0, 0, 0, (d(3, 3) + d(4, 4) + d(5, 5)) * c};
-        for (int i = 0; i < 4; i++)
-          for (int j = 0; j < i; j++) M[4 * i + j] = M[4 * j + i];
-        spd_inv(M, 4);
-        std::copy(M.begin(), M.end(), blk.begin() + 16 * (size_t)v);
-      }
-    });
+  // the blocks are formed in parallel, then listed in tet order.  mag_mass is
+  // the per-tet magnetic mass M from the dual area vectors, or with chi in
+  // place of mu the magnetic-loss matrix Z (:8778-8802).
+  auto mag_mass = [&](uint32_t v, const Mat3& mat, double* M) {
+    auto es = vol_edges(v);
+    V3 eb[6], fb[4];
+    for (int i = 0; i < 6; i++) eb[i] = ebar(es[i]);
+    for (int i = 0; i < 4; i++) fb[i] = fbar(vtf_[v][i]);
+    V3 vb{0, 0, 0};
+    for (int q = 0; q < 4; q++)
+      for (int a = 0; a < 3; a++) vb[a] += pts_[vols_[v][q]][a];
+    vb = {vb[0] / 4.0, vb[1] / 4.0, vb[2] / 4.0};
+    const double sgn = cell_vol_[v] < 0 ? -0.5 : 0.5;
+    const V3 fv[6] = {scale(cross(sub(vb, eb[0]), sub(fb[2], fb[3])), sgn),
+                      scale(cross(sub(vb, eb[1]), sub(fb[0], fb[3])), sgn),
+                      scale(cross(sub(vb, eb[2]), sub(fb[3], fb[1])), sgn),
+                      scale(cross(sub(vb, eb[3]), sub(fb[1], fb[2])), sgn),
+                      scale(cross(sub(vb, eb[4]), sub(fb[2], fb[0])), sgn),
+                      scale(cross(sub(vb, eb[5]), sub(fb[0], fb[1])), sgn)};
+    auto d = [&](int a, int b) { return dot(fv[a], mv(mat, fv[b])); };
+    const double c = 36.0 / std::fabs(cell_vol_[v]);
+    const double m[16] = {(d(0, 0) + d(2, 2) + d(3, 3)) * c, (-d(1, 2) - d(3, 4)) * c,
+                          (-d(0, 1) + d(3, 5)) * c,          (d(0, 4) + d(2, 5)) * c,
+                          0, (d(0, 0) + d(1, 1) + d(4, 4)) * c, (-d(0, 2) - d(4, 5)) * c, (d(0, 3) - d(1, 5)) * c,
+                          0, 0, (d(1, 1) + d(2, 2) + d(5, 5)) * c, (-d(2, 3) - d(1, 4)) * c,
+                          0, 0, 0, (d(3, 3) + d(4, 4) + d(5, 5)) * c};
+    for (int i = 0; i < 16; i++) M[i] = m[i];
+    for (int i = 0; i < 4; i++)
+      for (int j = 0; j < i; j++) M[4 * i + j] = M[4 * j + i];
+  };
+  std::vector<double> blk(16 * (size_t)L);
+  auto build_N = [&]() {
     // nonzero entries in tet order, at positions from a prefix of the counts
     std::vector<int64_t> off(L + 1, 0);
     parallel_for(L, nth, [&](int64_t v0, int64_t v1) {
@@ -795,7 +794,16 @@ void TetSim::build_ops() {
       }
     });
     N_ = HostCsr::build(NF, NF, t, nth);
-  }
+  };
+  parallel_for(L, nth, [&](int64_t v0, int64_t v1) {
+    std::vector<double> M(16);
+    for (uint32_t v = (uint32_t)v0; v < (uint32_t)v1; v++) {
+      mag_mass(v, sc_.materials.at(vol_mat_[v]).mu, M.data());
+      spd_inv(M, 4);
+      std::copy(M.begin(), M.end(), blk.begin() + 16 * (size_t)v);
+    }
+  });
+  build_N();
   auto primal_area = [&](uint32_t v) {
     const auto& n = vols_[v];
     V3 e[6] = {sub(pts_[n[1]], pts_[n[0]]), sub(pts_[n[2]], pts_[n[1]]), sub(pts_[n[2]], pts_[n[0]]),
@@ -890,6 +898,57 @@ void TetSim::build_ops() {
     }
     HostCsr Einv = HostCsr::build(NE, NE, einv_t, nth);
     dt_est_ = sim_.courant * estimate_dt(Einv, false);
+    // magnetic losses (Discretization.hpp:6357-6542, 9128-9205), with the
+    // run's dt: a face is class 1 when its tets have chi = 0, class 2 when
+    // they share one chi (and mu); a face whose tets differ is fractured in
+    // the reference, which then reads its old values from the electric state
+    // (Old_F_c, :586), so it is refused.  A tet whose chi has a non-zero
+    // determinant gets the block N = (M + dt/2 Z)^-1 and RS = N (M - dt/2 Z);
+    // R of a class-2 face is the diagonal of RS in its last tet.  dt above
+    // comes from the lossless N, as in the reference.
+    bool chi_any = false;
+    for (uint32_t v = 0; v < L; v++) chi_any = chi_any || !is_zero(sc_.materials.at(vol_mat_[v]).chi);
+    if (chi_any) {
+      auto same = [](const Mat3& a, const Mat3& b) {
+        for (int i = 0; i < 3; i++)
+          for (int j = 0; j < 3; j++)
+            if (a.m[i][j] != b.m[i][j]) return false;
+        return true;
+      };
+      for (uint32_t f = 0; f < NF; f++) {
+        if (ftv_[f][1] < 0) continue;
+        const Material& m0 = sc_.materials.at(vol_mat_[ftv_[f][0]]);
+        const Material& m1 = sc_.materials.at(vol_mat_[ftv_[f][1]]);
+        if ((!is_zero(m0.chi) || !is_zero(m1.chi)) && (!same(m0.chi, m1.chi) || !same(m0.mu, m1.mu)))
+          throw UnsupportedError("fractured magnetic-loss faces (chi, or mu where chi is set, changing across a face) "
+                                 "are outside the supported path: the reference reads their old values from the "
+                                 "electric state");
+      }
+      double dt = dt_est_;
+      if (sim_.step != 0 && !(sim_.step > dt)) dt = sim_.step;
+      nr_.assign(NF, 1.0);
+      parallel_for(L, nth, [&](int64_t v0, int64_t v1) {
+        double M[16], Z[16];
+        std::vector<double> Nl(16);
+        for (uint32_t v = (uint32_t)v0; v < (uint32_t)v1; v++) {
+          const Mat3& chi = sc_.materials.at(vol_mat_[v]).chi;
+          if (mat_det(chi) == 0) continue;
+          mag_mass(v, sc_.materials.at(vol_mat_[v]).mu, M);
+          mag_mass(v, chi, Z);
+          for (int q = 0; q < 16; q++) Nl[q] = M[q] + 0.5 * dt * Z[q];
+          spd_inv(Nl, 4);
+          std::copy(Nl.begin(), Nl.end(), blk.begin() + 16 * (size_t)v);
+          for (int j = 0; j < 4; j++) {
+            const int32_t f = vtf_[v][j];
+            if ((int32_t)v != std::max(ftv_[f][0], ftv_[f][1])) continue;  // the face's last tet writes R
+            double acc = 0;
+            for (int m = 0; m < 4; m++) acc += Nl[4 * j + m] * (M[4 * m + j] - 0.5 * dt * Z[4 * m + j]);
+            nr_[f] = acc;
+          }
+        }
+      });
+      build_N();
+    }
     if (dga_frac_) {
       // conducting tets (Discretization.hpp:9262-9475) with the run's dt: a
       // star with a conducting tet gets H = (E + dt/2 S)^-1 and PQ =
@@ -1816,6 +1875,7 @@ void TetSim::alloc_and_upload() {
   };
   upcsr(N_, d.n_ptr, d.n_col, d.n_val);
   upcsr(H_, d.h_ptr, d.h_col, d.h_val);
+  if (!nr_.empty()) d.n_r = upT(nr_);
   if (dga_frac_) {
     d.h_p = upT(hp_);
     d.nq = (int)q_size_;

@@ -130,6 +130,7 @@ class TetSim : public Sim {
   std::vector<int64_t> frac_off_;                  // node -> U_c offset, -1 if not fractured
   uint32_t q_size_ = 0;
   std::vector<int32_t> fe_edge_, fe_a_, fe_b_;     // fractured edges and their two U_c entries
+  std::vector<double> nr_;                         // dga with chi: R per face (F = R F - dt N cu)
   std::vector<uint8_t> pec_;
   std::vector<std::vector<uint32_t>> edge_src_;
   // operators

@@ -4,7 +4,8 @@
 //
 //   tet_curl_u        cu = C U (3 signed edges per face), B -= dt cu
 //                     (Discretization.hpp:902-916)
-//   tet_nmul          F -= dt N cu (:917)
+//   tet_nmul          F = R F - dt N cu (:917-918; R = 1 without magnetic
+//                     losses)
 //   tet_curl_f        cf = C^T F + Ctb Fb - I (:878-879)
 //   tet_h_update      U = P U + dt H cf on interior edges (P = 1 when
 //                     lossless), boundary flux (:887-894)
@@ -71,7 +72,7 @@ __global__ void __launch_bounds__(kBlock) tet_nmul(DevPtrs d) {
   T s = 0;
   for (int64_t k = d.n_ptr[f]; k < d.n_ptr[f + 1]; k++) s += ld<T>(d.n_val, k) * x[d.n_col[k]];
   T* F = (T*)d.F;
-  F[f] = F[f] - (T)d.dt * s;
+  F[f] = d.n_r ? ((const T*)d.n_r)[f] * F[f] - (T)d.dt * s : F[f] - (T)d.dt * s;
 }
 
 template <typename T>

@@ -34,6 +34,7 @@ struct DevPtrs {
   // Q (U_c x U_c) and Mq (U_c x edges), and the fractured edges with their
   // two U_c entries
   const void* h_p = nullptr;
+  const void* n_r = nullptr;  // dga with chi: R per face (F = R F - dt N cu), null without
   int nq = 0, nfe = 0;
   const int64_t *q_ptr = nullptr, *mq_ptr = nullptr;
   const int32_t *q_col = nullptr, *mq_col = nullptr;
