@@ -385,11 +385,11 @@ def precision_report(script, device, steps=400, every=100):
 
 
 # DRAM traffic of the FIT class kernels measured by ncu (one launch each of
-# the 256^3 scene, state 607 MB > L2): fit_e_class 691.8 MB against 709.4 MB
-# algorithmic, fit_h_class 697.6 MB against 708.2 MB.  The ratio is per byte
+# the 256^3 scene, state 607 MB > L2, 32 x 4 blocks): fit_e_class 689.7 MB
+# against 709.4 MB algorithmic, fit_h_class 697.6 MB against 708.2 MB.  The ratio is per byte
 # (one plane per block, the same re-use at every size), reported for the
 # dominant kernel as ratio x its algorithmic bytes.
-FIT_DRAM_OVER_ALGORITHMIC = {("fit_e_class", 4): 0.975, ("fit_h_class", 4): 0.985}
+FIT_DRAM_OVER_ALGORITHMIC = {("fit_e_class", 4): 0.972, ("fit_h_class", 4): 0.985}
 FIT_TRAFFIC_NOTE = "ncu DRAM bytes / algorithmic bytes of the kernel at 256^3, times this launch's algorithmic bytes"
 
 

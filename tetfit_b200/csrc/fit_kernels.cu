@@ -1305,6 +1305,16 @@ __global__ void __launch_bounds__(256) fit_loss_finish(const double* part, int n
 }
 
 // ---------------------------------------------------------------- launchers
+// Block shape of the streamed variants (x by y node slots of one plane; at
+// most 256 threads, the kernels' launch bound).  32 x 4 and 64 x 2 measured
+// fastest at 256^3 and 512^3 (FP32, B200): 4 % below 32 x 8; 32 x 1 took twice
+// as long, 256 x 1 and 16 x 16 were slower than 32 x 8.
+#ifndef TF_FIT_SBX
+#define TF_FIT_SBX 32
+#endif
+#ifndef TF_FIT_SBY
+#define TF_FIT_SBY 4
+#endif
 // Kernel variants for the E and H halves (all compute bit-identical results):
 // 0 one thread per node slot, 1 z-march over 4 planes, 2 z-march over 16,
 // 3 one thread per node slot with per-dof coefficient arrays.
@@ -1316,6 +1326,10 @@ void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const Probe
   // loss (optional): Joule loss of the E half step
   dim3 blk(32, 8, 1);
   dim3 grd((unsigned)((g.Nx + 1 + 31) / 32), (unsigned)((g.Ny + 1 + 7) / 8), (unsigned)(g.Nz + 1));
+  // the streamed variants (3, 5): one node slot per thread, one plane per block
+  const dim3 sblk(TF_FIT_SBX, TF_FIT_SBY, 1);
+  const dim3 sgrd((unsigned)((g.Nx + TF_FIT_SBX) / TF_FIT_SBX), (unsigned)((g.Ny + TF_FIT_SBY) / TF_FIT_SBY),
+                  (unsigned)(g.Nz + 1));
   auto mgrid = [&](int kc) {
     return dim3((unsigned)((g.Nx + 1 + 31) / 32), (unsigned)((g.Ny + 1 + 7) / 8), (unsigned)((g.Nz + 1 + kc - 1) / kc));
   };
@@ -1330,8 +1344,8 @@ void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const Probe
   if (sp.n > 0) fit_special_pre<T><<<nsb, 256, 0, st>>>(g, sp, step_counter);
   if (ev) cudaEventRecord(ev[1], st);
   if (e_variant == 0) fit_e_kernel<T><<<grd, blk, 0, st>>>(g);
-  else if (e_variant == 3) fit_e_coef<T><<<grd, blk, 0, st>>>(g);
-  else if (e_variant == 5 && g.lut_e) fit_e_class<T><<<grd, blk, 0, st>>>(g);
+  else if (e_variant == 3) fit_e_coef<T><<<sgrd, sblk, 0, st>>>(g);
+  else if (e_variant == 5 && g.lut_e) fit_e_class<T><<<sgrd, sblk, 0, st>>>(g);
   else if (e_variant == 4 && tma)
     fit_e_tma<T><<<mgrid(16), dim3(kTmaTX, kTmaTY + 1), 0, st>>>(g, 16, tma->F[0], tma->F[1], tma->F[2], tma->U[0], tma->U[1], tma->U[2],
                                              tma->err);
@@ -1349,8 +1363,8 @@ void fit_launch_step(const FitGrid<T>& g, const SpecialEdges<T>& sp, const Probe
   if (pr.n > 0) fit_probe_kernel<T><<<(pr.n + 127) / 128, 128, 0, st>>>(g, pr, step_counter);
   if (ev) cudaEventRecord(ev[4], st);
   if (h_variant == 0) fit_h_kernel<T><<<grd, blk, 0, st>>>(g, step_counter);
-  else if (h_variant == 3) fit_h_coef<T><<<grd, blk, 0, st>>>(g, step_counter);
-  else if (h_variant == 5 && g.lut_f) fit_h_class<T><<<grd, blk, 0, st>>>(g, step_counter);
+  else if (h_variant == 3) fit_h_coef<T><<<sgrd, sblk, 0, st>>>(g, step_counter);
+  else if (h_variant == 5 && g.lut_f) fit_h_class<T><<<sgrd, sblk, 0, st>>>(g, step_counter);
   else if (h_variant == 4 && tma)
     fit_h_tma<T><<<mgrid(16), dim3(kTmaTX, kTmaTY + 1), 0, st>>>(g, 16, step_counter, tma->U[0], tma->U[1], tma->U[2], tma->F[0],
                                              tma->F[1], tma->F[2], tma->err);
