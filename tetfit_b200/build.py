@@ -16,7 +16,7 @@ OUT = os.path.join(HERE, "libtetfit_b200.so")
 CLI = os.path.join(HERE, "tetfit")
 CLI_SOURCE = os.path.join(CSRC, "tetfit_main.cpp")
 SOURCES = ["script.cpp", "fit.cpp", "fit_kernels.cu", "tet.cpp", "tet_kernels.cu", "tet_group.cpp",
-           "tet_group_kernels.cu", "mlp.cu", "pcg.cu", "barrier_check.cu", "capi.cpp", "capi_batch.cpp"]
+           "tet_group_kernels.cu", "mlp.cu", "pcg.cu", "dt_gpu.cu", "barrier_check.cu", "capi.cpp", "capi_batch.cpp"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
 OBJ_DIR = os.path.join(HERE, "_build")

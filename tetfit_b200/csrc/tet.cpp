@@ -23,6 +23,7 @@
 #include <stdexcept>
 
 #include "cuda_util.hpp"
+#include "dt_gpu.hpp"
 #include "host_parallel.hpp"
 #include "tet_group.hpp"
 
@@ -1298,106 +1299,30 @@ void TetSim::split_system(double scale, double sig_coef) {
 double TetSim::estimate_dt(const HostCsr& M, bool generalized) {
   const size_t n = edges_.size(), nf = faces_.size();
   if (sim_.step != 0 && (n > 3000000 || !opt_.estimate_pinned)) return sim_.step / sim_.courant;
-  // Loops run on the set-up threads: matrix products and updates row by row,
-  // inner products as sums of fixed 4096-row chunks added in chunk order, so
-  // the estimate does not depend on the thread count.
-  const int nth = opt_.setup_threads;
-  auto par = [&](size_t m, auto&& f) {
-    parallel_for((int64_t)m, nth, [&](int64_t i0, int64_t i1) {
-      for (int64_t i = i0; i < i1; i++) f((size_t)i);
-    });
-  };
-  std::vector<double> part((n + 4095) / 4096);
-  auto dot = [&](const double* a, const double* b) {
-    parallel_for((int64_t)part.size(), nth, [&](int64_t c0, int64_t c1) {
-      for (int64_t c = c0; c < c1; c++) {
-        double t = 0;
-        for (size_t i = (size_t)c * 4096; i < std::min(n, (size_t)(c + 1) * 4096); i++) t += a[i] * b[i];
-        part[c] = t;
-      }
-    }, 4);
-    double t = 0;
-    for (double x : part) t += x;
-    return t;
-  };
-  std::vector<double> cu(nf), ncu(nf);
-  auto K = [&](const double* x, double* y) {
-    par(nf, [&](size_t f) { cu[f] = x[fte_[f][0]] - x[fte_[f][1]] + x[fte_[f][2]]; });
-    N_.mul(cu.data(), ncu.data(), nth);
-    par(n, [&](size_t e) {
-      double t = 0;
-      for (int64_t k = Ct_.ptr[e]; k < Ct_.ptr[e + 1]; k++) t += Ct_.val[k] * ncu[Ct_.col[k]];
-      y[e] = t;
-    });
-  };
-  std::vector<double> pre(n), r(n), z(n), p(n), q(n);
-  if (generalized)
-    par(n, [&](size_t i) {
-      double dg = 0;
-      for (int64_t k = M.ptr[i]; k < M.ptr[i + 1]; k++)
-        if (M.col[k] == (int32_t)i) dg = M.val[k];
-      pre[i] = dg != 0 ? 1.0 / dg : 1.0;
-    });
-  auto Minv = [&](const double* x, double* y) {
-    if (!generalized) {
-      M.mul(x, y, nth);
-      return;
-    }
-    // y = E^-1 x by Jacobi-PCG from zero
-    par(n, [&](size_t i) {
-      y[i] = 0.0;
-      r[i] = x[i];
-      z[i] = pre[i] * r[i];
-      p[i] = z[i];
-    });
-    const double rr0 = dot(r.data(), r.data());
-    double rz = dot(r.data(), z.data());
-    for (int it = 0; it < 1000 && rr0 > 0; it++) {
-      M.mul(p.data(), q.data(), nth);
-      const double a = rz / dot(p.data(), q.data());
-      par(n, [&](size_t i) {
-        y[i] += a * p[i];
-        r[i] -= a * q[i];
-        z[i] = pre[i] * r[i];
-      });
-      const double rr = dot(r.data(), r.data()), rz2 = dot(r.data(), z.data());
-      if (std::sqrt(rr / rr0) < 1e-12) break;
-      const double bt = rz2 / rz;
-      par(n, [&](size_t i) { p[i] = z[i] + bt * p[i]; });
-      rz = rz2;
-    }
-  };
-  std::vector<double> x(n), v(n), Kv(n), w(n), Kw(n), vp(n, 0.0);
+  // Lanczos on the GPU (dt_gpu.cu) from a fixed pseudo-random start vector
+  std::vector<double> x(n);
   uint64_t s = 0x2545F4914F6CDD1Dull;
   for (size_t i = 0; i < n; i++) {
     s ^= s << 13; s ^= s >> 7; s ^= s << 17;
     x[i] = (double)(s >> 11) / 9007199254740992.0 - 0.5;
   }
-  K(x.data(), Kv.data());
-  Minv(Kv.data(), v.data());
-  K(v.data(), Kv.data());
-  const double nrm = std::sqrt(dot(v.data(), Kv.data()));
-  par(n, [&](size_t i) { v[i] /= nrm; Kv[i] /= nrm; });
-  std::vector<double> al, be;
-  double beta = 0, last = 0, lam = 0;
-  for (int it = 0; it < 400; it++) {
-    Minv(Kv.data(), w.data());
-    const double alpha = dot(w.data(), Kv.data());
-    par(n, [&](size_t i) { w[i] -= alpha * v[i] + beta * vp[i]; });
-    al.push_back(alpha);
-    K(w.data(), Kw.data());
-    double nb = dot(w.data(), Kw.data());
-    nb = nb > 0 ? std::sqrt(nb) : 0;
-    if (it % 10 == 9 || nb == 0 || it == 399) {
-      lam = tridiag_max(al, be);
-      if (nb == 0 || std::fabs(lam - last) <= 1e-9 * std::fabs(lam)) break;
-      last = lam;
-    }
-    be.push_back(nb);
-    beta = nb;
-    vp.swap(v);
-    par(n, [&](size_t i) { v[i] = w[i] / nb; Kv[i] = Kw[i] / nb; });
-  }
+  std::vector<int32_t> fte(3 * nf), ct(Ct_.col.size());
+  for (size_t f = 0; f < nf; f++)
+    for (int a = 0; a < 3; a++) fte[3 * f + a] = fte_[f][a];
+  for (size_t k = 0; k < ct.size(); k++)
+    ct[k] = Ct_.val[k] < 0 ? (int32_t)((uint32_t)Ct_.col[k] | 0x80000000u) : Ct_.col[k];
+  DtProblem p;
+  p.device = opt_.device;
+  p.n = (int64_t)n;
+  p.nf = (int64_t)nf;
+  p.fte = fte.data();
+  p.N = {(int64_t)N_.nrows, N_.ptr.data(), N_.col.data(), N_.val.data()};
+  p.Ct = {(int64_t)Ct_.nrows, Ct_.ptr.data(), ct.data(), nullptr};
+  p.M = {(int64_t)M.nrows, M.ptr.data(), M.col.data(), M.val.data()};
+  p.generalized = generalized;
+  p.x0 = x.data();
+  p.tridiag_max = tridiag_max;
+  const double lam = gpu_lanczos_lambda(p);
   return 2.0 / std::sqrt(lam);
 }
 
