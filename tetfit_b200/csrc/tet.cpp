@@ -854,6 +854,8 @@ void TetSim::build_ops() {
     };
     // node stars in parallel, each into its own lists, then concatenated in
     // node order (the order a sequential pass would list them)
+    // the unmasked inverses Einv only feed the dt estimate
+    const bool want_einv = dt_estimate_needed();
     const size_t NP = pts_.size();
     std::vector<HostCsr::Trips> ein_n(NP), h_n(NP);
     parallel_for((int64_t)NP, nth, [&](int64_t n0, int64_t n1) {
@@ -864,14 +866,16 @@ void TetSim::build_ops() {
         const int64_t b0 = star_ptr_[nid];
         const int n = (int)(star_ptr_[nid + 1] - b0);
         star_mass(nid, false, E);
-        std::vector<double> Hl = E;
-        spd_inv(Hl, n);
-        for (int j = 0; j < n; j++)
-          for (int k = j; k < n; k++)
-            if (Hl[j * n + k] != 0) {
-              einv_t.push_back({(uint32_t)star_edge_[b0 + j], (uint32_t)star_edge_[b0 + k], Hl[j * n + k]});
-              if (j != k) einv_t.push_back({(uint32_t)star_edge_[b0 + k], (uint32_t)star_edge_[b0 + j], Hl[j * n + k]});
-            }
+        if (want_einv) {
+          std::vector<double> Hl = E;
+          spd_inv(Hl, n);
+          for (int j = 0; j < n; j++)
+            for (int k = j; k < n; k++)
+              if (Hl[j * n + k] != 0) {
+                einv_t.push_back({(uint32_t)star_edge_[b0 + j], (uint32_t)star_edge_[b0 + k], Hl[j * n + k]});
+                if (j != k) einv_t.push_back({(uint32_t)star_edge_[b0 + k], (uint32_t)star_edge_[b0 + j], Hl[j * n + k]});
+              }
+        }
         if (dga_frac_) continue;  // the masked inverses need dt (below)
         // masked inverse (Discretization.hpp:9263-9333)
         for (int j = 0; j < n; j++)
@@ -897,7 +901,8 @@ void TetSim::build_ops() {
       einv_t.insert(einv_t.end(), ein_n[nid].begin(), ein_n[nid].end());
       HostCsr::Trips().swap(ein_n[nid]);
     }
-    HostCsr Einv = HostCsr::build(NE, NE, einv_t, nth);
+    HostCsr Einv;
+    if (want_einv) Einv = HostCsr::build(NE, NE, einv_t, nth);
     dt_est_ = sim_.courant * estimate_dt(Einv, false);
     // magnetic losses (Discretization.hpp:6357-6542, 9128-9205), with the
     // run's dt: a face is class 1 when its tets have chi = 0, class 2 when
@@ -1296,9 +1301,15 @@ void TetSim::split_system(double scale, double sig_coef) {
 // product; dt = 2 / sqrt(lambda).  Meshes above 3 M edges with a pinned step,
 // and batch members with a pinned step, skip the estimate and take the step
 // as given.
+// A pinned step skips the estimate on large meshes (and in batches); dt is
+// then the pinned step.
+bool TetSim::dt_estimate_needed() const {
+  return !(sim_.step != 0 && (edges_.size() > 3000000 || !opt_.estimate_pinned));
+}
+
 double TetSim::estimate_dt(const HostCsr& M, bool generalized) {
   const size_t n = edges_.size(), nf = faces_.size();
-  if (sim_.step != 0 && (n > 3000000 || !opt_.estimate_pinned)) return sim_.step / sim_.courant;
+  if (!dt_estimate_needed()) return sim_.step / sim_.courant;
   // Lanczos on the GPU (dt_gpu.cu) from a fixed pseudo-random start vector
   std::vector<double> x(n);
   uint64_t s = 0x2545F4914F6CDD1Dull;

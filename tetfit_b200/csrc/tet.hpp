@@ -88,6 +88,7 @@ class TetSim : public Sim {
   void classify();
   void build_ops();
   void split_system(double scale, double sig_coef = 0.0);
+  bool dt_estimate_needed() const;
   double estimate_dt(const HostCsr& Minv_or_E, bool generalized);
   void locate_probes();
   void build_sources();

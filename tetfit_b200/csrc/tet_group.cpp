@@ -547,7 +547,8 @@ void TetGroup::partition() {
   CU(cudaMemcpy(aptr.data(), d.A.ptr, sizeof(int64_t) * (nslice + 1), cudaMemcpyDeviceToHost));
   std::vector<uint16_t> ssim(nslice);
   if (nslice) CU(cudaMemcpy(ssim.data(), d.slice_sim, sizeof(uint16_t) * nslice, cudaMemcpyDeviceToHost));
-  int64_t want = (nslice + kCgWarps - 1) / kCgWarps;
+  const int warps = opt_.precision == 1 ? cg_warps<float>() : cg_warps<double>();
+  int64_t want = (nslice + warps - 1) / warps;
   int G = (int)std::max<int64_t>(1, std::min<int64_t>(cg_blocks_, want));
   std::vector<double> cum(nslice + 1, 0.0);
   for (int64_t s = 0; s < nslice; s++) cum[s + 1] = cum[s] + (double)((aptr[s + 1] - aptr[s]) >> 5) + 8.0;

@@ -615,9 +615,10 @@ __device__ __forceinline__ T p_next(T z, T pold, T beta, bool first) {
 
 // Co-resident CG blocks per SM the register budget is set for: more warps
 // in flight hide the SELL sweep's load latency better than longer load
-// chunks (measured: FP32 four blocks of 512, FP64 three, where four spill).
+// chunks (measured: FP32 two blocks of 1024 threads, 2048 per SM; FP64 three
+// of 512, where four spill).
 #ifndef TF_CG_MINB32
-#define TF_CG_MINB32 4
+#define TF_CG_MINB32 2
 #endif
 #ifndef TF_CG_MINB64
 #define TF_CG_MINB64 3
@@ -626,7 +627,7 @@ template <typename T>
 constexpr int cg_min_blocks() { return sizeof(T) == 4 ? TF_CG_MINB32 : TF_CG_MINB64; }
 
 template <typename T, bool kFused>
-__global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDev d) {
+__global__ void __launch_bounds__(cg_threads<T>(), cg_min_blocks<T>()) grp_cg(GroupDev d) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SimCg* st = reinterpret_cast<SimCg*>(smem_raw);
   auto grid_sync = [&]() { grid_barrier(d.gbar, d.err, gridDim.x); };
@@ -649,7 +650,7 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
     a3 = warp_sum(a3);
     a4 = warp_sum(a4);
     if (lane == 0) {
-      double* w = wp + ((g - g0) * kCgWarps + warp) * kPart;
+      double* w = wp + ((g - g0) * cg_warps<T>() + warp) * kPart;
       w[3] = a3;
       w[4] = a4;
     }
@@ -657,7 +658,7 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
     a1 = warp_sum(a1);
     a2 = warp_sum(a2);
     if (lane == 0) {
-      double* w = wp + ((g - g0) * kCgWarps + warp) * kPart;
+      double* w = wp + ((g - g0) * cg_warps<T>() + warp) * kPart;
       w[0] = a0;
       w[1] = a1;
       w[2] = a2;
@@ -668,7 +669,7 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
     a1 = warp_sum(a1);
     a2 = warp_sum(a2);
     if (lane == 0) {
-      double* w = wp + ((g - g0) * kCgWarps + warp) * kPart;
+      double* w = wp + ((g - g0) * cg_warps<T>() + warp) * kPart;
       w[0] = a0;
       w[1] = a1;
       w[2] = a2;
@@ -676,10 +677,10 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
   };
   auto publish = [&](int nq, int slot) {
     __syncthreads();
-    for (int gl = threadIdx.x; gl < g1 - g0; gl += kCgThreads)
+    for (int gl = threadIdx.x; gl < g1 - g0; gl += cg_threads<T>())
       for (int k = 0; k < nq; k++) {
         double a = 0.0;
-        for (int w = 0; w < kCgWarps; w++) a += wp[(gl * kCgWarps + w) * kPart + k];
+        for (int w = 0; w < cg_warps<T>(); w++) a += wp[(gl * cg_warps<T>() + w) * kPart + k];
         d.part[kCgPart * (int64_t)d.seg_of[g0 + gl] + slot + k] = a;
       }
   };
@@ -687,7 +688,7 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
   // simulation, lanes over its segments, then a fixed shuffle tree; f(s, t)
   // runs on lane 0 with the nq totals t[]
   auto totals = [&](int nq, int slot, auto&& f) {
-    for (int s = warp; s < d.S; s += kCgWarps) {
+    for (int s = warp; s < d.S; s += cg_warps<T>()) {
       double t[kPart] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
       for (int g = d.sim_seg[s] + lane; g < d.sim_seg[s + 1]; g += 32)
         for (int k = 0; k < nq; k++) t[k] += d.part[kCgPart * (int64_t)g + slot + k];
@@ -710,7 +711,7 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
     const int s = d.seg_sim[d.seg_of[g]];
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0;
     if (running(d, s))
-      for (int64_t sl = d.seg_s0[d.seg_of[g]] + warp; sl < d.seg_s1[d.seg_of[g]]; sl += kCgWarps) {
+      for (int64_t sl = d.seg_s0[d.seg_of[g]] + warp; sl < d.seg_s1[d.seg_of[g]]; sl += cg_warps<T>()) {
         const int64_t i = sl * 32 + lane;
         const T ri = b[i] - sell_dot_cg<T>(d.A, i, [&](int32_t c) { return x[c]; });
         r[i] = ri;
@@ -750,7 +751,7 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
 
   for (;;) {
     int any = 0;
-    for (int s = threadIdx.x; s < d.S; s += kCgThreads) any |= st[s].active;
+    for (int s = threadIdx.x; s < d.S; s += cg_threads<T>()) any |= st[s].active;
     if (!__syncthreads_or(any)) break;
     // p_{j+1} = z + beta p_j, x += alpha_j p_j (lazy), and in the fused
     // variant q = A p_{j+1} with p.q partials
@@ -765,7 +766,7 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
         T* pn = pbuf(c.it);
         T* xs = xs_of(c);
         const T* zs = zs_of(c);
-        for (int64_t sl = d.seg_s0[d.seg_of[g]] + warp; sl < d.seg_s1[d.seg_of[g]]; sl += kCgWarps) {
+        for (int64_t sl = d.seg_s0[d.seg_of[g]] + warp; sl < d.seg_s1[d.seg_of[g]]; sl += cg_warps<T>()) {
           const int64_t i = sl * 32 + lane;
           const T po = first ? (T)0 : pold[i];
           const T pi = p_next<T>(zs[i], po, beta, first);
@@ -790,7 +791,7 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
         double a0 = 0.0;
         if (c.active) {
           const T* pn = pbuf(c.it);
-          for (int64_t sl = d.seg_s0[d.seg_of[g]] + warp; sl < d.seg_s1[d.seg_of[g]]; sl += kCgWarps) {
+          for (int64_t sl = d.seg_s0[d.seg_of[g]] + warp; sl < d.seg_s1[d.seg_of[g]]; sl += cg_warps<T>()) {
             const int64_t i = sl * 32 + lane;
             const T qi = sell_dot_cg<T>(d.A, i, [&](int32_t cc) { return pn[cc]; });
             q[i] = qi;
@@ -814,7 +815,7 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
         const T alpha = (T)st[s].alpha;
         T* rs = rs_of(st[s]);
         T* zs = zs_of(st[s]);
-        for (int64_t sl = d.seg_s0[d.seg_of[g]] + warp; sl < d.seg_s1[d.seg_of[g]]; sl += kCgWarps) {
+        for (int64_t sl = d.seg_s0[d.seg_of[g]] + warp; sl < d.seg_s1[d.seg_of[g]]; sl += cg_warps<T>()) {
           const int64_t i = sl * 32 + lane;
           const T ri = rs[i] - alpha * q[i];
           rs[i] = ri;
@@ -850,7 +851,7 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
     const T alpha = (T)c.alpha;
     const T* pl = pbuf(c.it - 1);
     T* xs = xs_of(c);
-    for (int64_t sl = d.seg_s0[d.seg_of[g]] + warp; sl < d.seg_s1[d.seg_of[g]]; sl += kCgWarps) {
+    for (int64_t sl = d.seg_s0[d.seg_of[g]] + warp; sl < d.seg_s1[d.seg_of[g]]; sl += cg_warps<T>()) {
       const int64_t i = sl * 32 + lane;
       T v = xs[i];
       if (c.it > 0) v = fmaT(alpha, pl[i], v);
@@ -858,7 +859,7 @@ __global__ void __launch_bounds__(kCgThreads, cg_min_blocks<T>()) grp_cg(GroupDe
     }
   }
   if (blockIdx.x == 0)
-    for (int s = threadIdx.x; s < d.S; s += kCgThreads) {
+    for (int s = threadIdx.x; s < d.S; s += cg_threads<T>()) {
       if (!running(d, s)) continue;
       const SimCg c = st[s];
       const int64_t k = d.stat_off[s] + d.step[s];
@@ -985,19 +986,20 @@ __global__ void grp_bump(GroupDev d) {
 // ------------------------------------------------------------------ launch
 static inline unsigned gblk(int64_t n) { return (unsigned)(n > 0 ? (n + kGB - 1) / kGB : 1); }
 
-static size_t cg_smem(int S) { return sizeof(SimCg) * (size_t)S + sizeof(double) * kMaxSeg * kCgWarps * kPart; }
+template <typename T>
+static size_t cg_smem(int S) { return sizeof(SimCg) * (size_t)S + sizeof(double) * kMaxSeg * cg_warps<T>() * kPart; }
 
 template <typename T>
 int group_cg_blocks(int device, int S, size_t* smem) {
-  const size_t sm = cg_smem(S);
+  const size_t sm = cg_smem<T>(S);
   if (smem) *smem = sm;
   int sms = 0, a = 0, b = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (cudaFuncSetAttribute(grp_cg<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess ||
       cudaFuncSetAttribute(grp_cg<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
     return 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, grp_cg<T, true>, kCgThreads, sm);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, grp_cg<T, false>, kCgThreads, sm);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, grp_cg<T, true>, cg_threads<T>(), sm);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, grp_cg<T, false>, cg_threads<T>(), sm);
   return (a < b ? a : b) * sms;
 }
 
@@ -1066,7 +1068,7 @@ cudaError_t group_launch_step(const GroupDev& d, int cg_blocks, int cg_variant, 
   if (ev) cudaEventRecord(ev[2], st);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cg_blocks);
-  cfg.blockDim = dim3(kCgThreads);
+  cfg.blockDim = dim3(cg_threads<T>());
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
