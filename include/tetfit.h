@@ -127,16 +127,19 @@ TF_API int tf_get_flux(tf_ctx* ctx, double* flux, size_t cap, size_t* n);
 /* Per-step Joule loss, the third column of poynting.dat: 0.25 (U_old + U)^T
  * Si (U_old + U) (fdtd, Discretization.hpp:1902; dga :895; gfdtd :1519).  As
  * in the reference, the fdtd conductance vector Si is filled only for l2norm
- * outputs (:5368, :5594-5597), so the loss is zero for other outputs; the
- * tetrahedral paths accept lossless materials only, so theirs is zero.  FP64
- * accumulation on the GPU. */
+ * outputs (:5368, :5594-5597), so the loss is zero for other outputs; gfdtd
+ * and fem give the reference's list (:1518-1546, :1733-1757) with
+ * conducting materials; dga never fills its SigMat, so its loss is zero.
+ * FP64 accumulation on the GPU. */
 TF_API int tf_get_losses(tf_ctx* ctx, double* losses, size_t cap, size_t* n);
 /* Discrete leapfrog energy of the current state (U^n, F^{n+1/2}) in FP64
  * accumulation: fdtd 0.5 U^n.Me.U^n + 0.5 F^{n+1/2}.Mmu.F^{n-1/2} (F^{n-1/2}
  * recomputed from U^n); gfdtd 0.5 U^n.E.U^n + 0.5 B^{n-1/2}.N.B^{n+1/2} over the
- * free edges (B^{n+1/2} recomputed).  Both are invariants of the lossless
- * leapfrog once the sources are off.  dga returns TF_E_UNSUPPORTED (its
- * electric mass is the inverse of the assembled H). */
+ * free edges (B^{n+1/2} recomputed); dga 0.5 U^n.H^-1.U^{n+1} +
+ * 0.5 B^{n+1/2}.N.B^{n+1/2} over the class-1 edges (U^{n+1} - U^n = dt H cf
+ * from the current F; H^-1 U^n by a GPU PCG solve to 1e-15).  All are
+ * invariants of the lossless leapfrog once the sources are off.  fem, and dga
+ * with conducting or magnetically lossy materials, return TF_E_UNSUPPORTED. */
 TF_API int tf_energy(tf_ctx* ctx, double* energy);
 /* One step driven from host memory: carrier_in[n_sources] replaces the script
  * waveform's value for this step (NULL keeps it); probe_out[n_probes*6]

@@ -134,5 +134,15 @@ def test_tet_cavity_energy_drift(tmp_path, product_lib, oracle_lib, method):
             d.step(998)
             g1 = d.energy()
             assert abs(g1 - g0) / g0 <= 1e-12, f"GPU energy drift {abs(g1 - g0) / g0:.3e}"
+        else:
+            # dga: W^n = 1/2 U^n.H^-1.U^{n+1} + 1/2 B^{n+1/2}.N.B^{n+1/2} from the
+            # current state alone (tf_energy: a PCG solve with H's class-1
+            # block on the GPU): against numpy on the same states, and its drift
+            g0 = d.energy()
+            w_np = energy()
+            assert abs(g0 - w_np) / w_np <= 1e-12, (g0, w_np)
+            d.step(998)
+            g1 = d.energy()
+            assert abs(g1 - g0) / g0 <= 1e-12, f"GPU energy drift {abs(g1 - g0) / g0:.3e}"
     assert w0 > 0
     assert abs(w1 - w0) / w0 <= 1e-12, f"{method}: relative drift {abs(w1 - w0) / w0:.3e}"

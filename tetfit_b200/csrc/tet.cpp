@@ -33,6 +33,11 @@ template <typename T>
 cudaError_t tet_launch_step(const DevPtrs& d, cudaStream_t st, cudaEvent_t* ev);
 template <typename T>
 void tet_launch_initial_probes(const DevPtrs& d, cudaStream_t st);
+template <typename T>
+cudaError_t tet_launch_energy(const DevPtrs& d, DevPtrs d_cg, int cg_blocks, const int32_t* ie, int ni,
+                              double* part, double* out, cudaStream_t st);
+template <typename T>
+int tet_cg_blocks(int device);
 
 namespace {
 using V3 = std::array<double, 3>;
@@ -2055,10 +2060,95 @@ size_t TetSim::training_loss(float* loss, size_t cap) const {
 }
 
 double TetSim::energy() {
-  // gfdtd: the group engine's GPU reduction; dga's electric energy needs the
-  // inverse of the assembled H, which is not formed
-  if (method_ != 2 || !group_) throw UnsupportedError("tf_energy: dga's electric mass is the inverse of H");
+  // gfdtd: the group engine's GPU reduction; dga: H^-1 through a PCG solve
+  if (method_ == 1) return dga_energy();
+  if (method_ != 2 || !group_) throw UnsupportedError("tf_energy: fem's energy is not provided");
   return group_->energy(0);
+}
+
+// dga: W^n = 1/2 U^n.H^-1.U^{n+1} + 1/2 B.N.B over the class-1 edges
+// (tet_launch_energy), H^-1 u by the standalone PCG kernel on H's class-1
+// block in FP64 to 1e-15 relative.  Lossless runs only: the conducting
+// classes do not conserve it.
+double TetSim::dga_energy() {
+  if (dga_frac_ || !nr_.empty())
+    throw UnsupportedError("tf_energy: a dga run with conducting or magnetically lossy materials has no invariant");
+  const bool f32 = opt_.precision == 1;
+  if (!en_edges_) {
+    if (H_.ptr.empty()) throw UnsupportedError("tf_energy: the dga operators were released");
+    const uint32_t NE = (uint32_t)edges_.size();
+    std::vector<int32_t> ie, pos(NE, -1);
+    for (uint32_t e = 0; e < NE; e++)
+      if (cls_[e] == 1) {
+        pos[e] = (int32_t)ie.size();
+        ie.push_back((int32_t)e);
+      }
+    const int ni = (int)ie.size();
+    std::vector<int64_t> ptr(ni + 1, 0);
+    std::vector<int32_t> col;
+    std::vector<double> val;
+    for (int i = 0; i < ni; i++) {
+      for (int64_t k = H_.ptr[ie[i]]; k < H_.ptr[ie[i] + 1]; k++) {
+        const int32_t c = pos[H_.col[k]];
+        if (c < 0) throw CudaError("tf_energy: H has a column outside the class-1 edges");
+        col.push_back(c);
+        val.push_back(H_.val[k]);
+      }
+      ptr[i + 1] = (int64_t)col.size();
+    }
+    auto dalloc = [&](size_t bytes) -> void* {
+      void* p = nullptr;
+      CU(cudaMalloc(&p, bytes ? bytes : 16));
+      allocs_.push_back(p);
+      return p;
+    };
+    auto up = [&](const void* src, size_t bytes) -> void* {
+      void* p = dalloc(bytes);
+      if (bytes) CU(cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice));
+      return p;
+    };
+    en_blocks_ = tet_cg_blocks<double>(opt_.device);
+    if (en_blocks_ < 1) throw CudaError("tf_energy: no co-resident blocks for the CG kernel");
+    DevPtrs& c = en_cg_;
+    c.nfree = ni;
+    c.a_ptr = (const int64_t*)up(ptr.data(), ptr.size() * 8);
+    c.a_col = (const int32_t*)up(col.data(), col.size() * 4);
+    c.a_val = up(val.data(), val.size() * 8);
+    double* work = (double*)dalloc(((size_t)6 * ni + 4 * (size_t)en_blocks_ + 6) * 8);
+    c.jac = work;
+    c.r = work + ni;
+    c.p = work + 2 * (size_t)ni;
+    c.q = work + 3 * (size_t)ni;
+    c.rhs = work + 4 * (size_t)ni;
+    c.x = work + 5 * (size_t)ni;
+    c.part_a = work + 6 * (size_t)ni;
+    c.part_b = c.part_a + en_blocks_;
+    double* tail = c.part_a + 4 * (size_t)en_blocks_;
+    c.cg_resid = tail;
+    c.cg_iters = (int32_t*)(tail + 1);
+    c.step = (int*)(tail + 2);
+    c.cg_limit = (int32_t*)(tail + 3);
+    c.err = (int*)(tail + 4);
+    c.gbar = (unsigned int*)(tail + 5);
+    c.tol = 1e-15;
+    c.cg_maxiter = 5000;
+    c.cg_criterion = 1;
+    en_n_ = ni;
+    en_edges_ = (int32_t*)up(ie.data(), ie.size() * 4);
+    const size_t nparts = 2 * (((size_t)ni + 255) / 256 + 1) + ((faces_.size() + 255) / 256 + 1);
+    en_part_ = (double*)dalloc(nparts * 8);
+    en_out_ = (double*)dalloc(8);
+  }
+  cudaError_t e = f32 ? tet_launch_energy<float>(dp_, en_cg_, en_blocks_, en_edges_, en_n_, en_part_, en_out_, stream_)
+                      : tet_launch_energy<double>(dp_, en_cg_, en_blocks_, en_edges_, en_n_, en_part_, en_out_, stream_);
+  CU(e);
+  double w = 0;
+  int berr = 0;
+  CU(cudaMemcpyAsync(&w, en_out_, 8, cudaMemcpyDeviceToHost, stream_));
+  CU(cudaMemcpyAsync(&berr, en_cg_.err, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  CU(cudaStreamSynchronize(stream_));
+  if (berr) throw CudaError("tf_energy: a grid barrier wait of the CG kernel ran out of time");
+  return w;
 }
 
 }  // namespace tf

@@ -132,6 +132,13 @@ class TetSim : public Sim {
   uint32_t q_size_ = 0;
   std::vector<int32_t> fe_edge_, fe_a_, fe_b_;     // fractured edges and their two U_c entries
   std::vector<double> nr_;                         // dga with chi: R per face (F = R F - dt N cu)
+  // dga energy (tf_energy), set up on the first call: the class-1 edges, the
+  // class-1 block of H in FP64 with its PCG work, and the partial sums
+  DevPtrs en_cg_;
+  int en_blocks_ = 0, en_n_ = 0;
+  int32_t* en_edges_ = nullptr;
+  double *en_part_ = nullptr, *en_out_ = nullptr;
+  double dga_energy();
   std::vector<uint8_t> pec_;
   std::vector<std::vector<uint32_t>> edge_src_;
   // operators

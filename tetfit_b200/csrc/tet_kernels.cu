@@ -146,6 +146,63 @@ __global__ void __launch_bounds__(kBlock) tet_frac_gather(DevPtrs d, int part0) 
   if (threadIdx.x == 0) d.flux_part[part0 + blockIdx.x] = fl;
 }
 
+// dga energy (tf_energy).  W^n = 1/2 U^n.H^-1.U^{n+1} + 1/2 B.N.B over the
+// class-1 edges, the leapfrog invariant of the lossless scheme; with
+// U^{n+1} = U^n + dt H cf it is 1/2 u.x + 1/2 dt u.cf + 1/2 B.N.B, u the
+// class-1 values of U^n, x = H^-1 u (a PCG solve), cf from the current F.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) tet_energy_gather(DevPtrs d, const int32_t* ie, double* u, int ni) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ni) u[i] = (double)((const T*)d.U)[ie[i]];
+}
+
+// part[2 b] = sum of u.x, part[2 b + 1] = sum of u.cf over block b's rows
+template <typename T>
+__global__ void __launch_bounds__(kBlock) tet_energy_e(DevPtrs d, const int32_t* ie, const double* x, int ni,
+                                                      double* part) {
+  __shared__ double sh[33];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double a = 0.0, b = 0.0;
+  if (i < ni) {
+    const double u = (double)((const T*)d.U)[ie[i]];
+    a = u * x[i];
+    b = u * (double)((const T*)d.cf)[ie[i]];
+  }
+  a = block_sum(a, sh);
+  b = block_sum(b, sh);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = a;
+    part[2 * blockIdx.x + 1] = b;
+  }
+}
+
+// part[b] = sum over block b's faces of B_f (N B)_f
+template <typename T>
+__global__ void __launch_bounds__(kBlock) tet_energy_m(DevPtrs d, double* part) {
+  __shared__ double sh[33];
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  double c = 0.0;
+  if (f < d.nF) {
+    const T* B = (const T*)d.B;
+    double s = 0.0;
+    for (int64_t k = d.n_ptr[f]; k < d.n_ptr[f + 1]; k++) s += (double)ld<T>(d.n_val, k) * (double)B[d.n_col[k]];
+    c = (double)B[f] * s;
+  }
+  c = block_sum(c, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = c;
+}
+
+// out = 1/2 (sum u.x) + 1/2 dt (sum u.cf) + 1/2 (sum B.N.B), partials in order
+__global__ void tet_energy_sum(const double* pe, int nbe, const double* pm, int nbm, double dt, double* out) {
+  double a = 0.0, b = 0.0, c = 0.0;
+  for (int q = 0; q < nbe; q++) {
+    a += pe[2 * q];
+    b += pe[2 * q + 1];
+  }
+  for (int q = 0; q < nbm; q++) c += pm[q];
+  *out = 0.5 * a + 0.5 * dt * b + 0.5 * c;
+}
+
 // Source edges: E sources write U, H sources write cb (reset each step),
 // currents write I.
 template <typename T>
@@ -396,6 +453,27 @@ void tet_launch_initial_probes(const DevPtrs& d, cudaStream_t st) {
   if (d.np) tet_probes<T><<<nblk(d.np), kBlock, 0, st>>>(d, 0);
 }
 
+// dga energy: gather u, solve H x = u (d_cg: the class-1 block of H and the
+// PCG work), then the three sums; *out receives W (device)
+template <typename T>
+cudaError_t tet_launch_energy(const DevPtrs& d, DevPtrs d_cg, int cg_blocks, const int32_t* ie, int ni,
+                              double* part, double* out, cudaStream_t st) {
+  tet_curl_f<T><<<nblk(d.nE), kBlock, 0, st>>>(d);
+  tet_energy_gather<T><<<nblk(ni), kBlock, 0, st>>>(d, ie, (double*)d_cg.rhs, ni);
+  cudaMemsetAsync(d_cg.x, 0, sizeof(double) * (size_t)ni, st);
+  cudaError_t e = pcg_launch_solve(d_cg, cg_blocks, st);
+  if (e != cudaSuccess) return e;
+  const int nbe = (int)nblk(ni), nbm = (int)nblk(d.nF);
+  tet_energy_e<T><<<nbe, kBlock, 0, st>>>(d, ie, (const double*)d_cg.x, ni, part);
+  tet_energy_m<T><<<nbm, kBlock, 0, st>>>(d, part + 2 * nbe);
+  tet_energy_sum<<<1, 1, 0, st>>>(part, nbe, part + 2 * nbe, nbm, d.dt, out);
+  return cudaGetLastError();
+}
+
+template cudaError_t tet_launch_energy<double>(const DevPtrs&, DevPtrs, int, const int32_t*, int, double*, double*,
+                                               cudaStream_t);
+template cudaError_t tet_launch_energy<float>(const DevPtrs&, DevPtrs, int, const int32_t*, int, double*, double*,
+                                              cudaStream_t);
 template cudaError_t tet_launch_step<double>(const DevPtrs&, cudaStream_t, cudaEvent_t*);
 template cudaError_t tet_launch_step<float>(const DevPtrs&, cudaStream_t, cudaEvent_t*);
 template int tet_cg_blocks<double>(int);
