@@ -315,3 +315,31 @@ def test_unsupported_magnetic_losses_are_refused(tmp_path, product_lib, method, 
         with pytest.raises(tb.TetfitError) as e:
             d.prepare(1)
     assert e.value.code == tb.TF_E_UNSUPPORTED
+
+
+def test_dga_mirror_rows_of_the_first_class_edges(tmp_path, oracle_lib):
+    """The reference fills a star's class-1 (class-2) rows from the upper
+    triangle and mirrors each entry into the row h_index (p_index) of the
+    column's edge, which is 0 for an edge of another class (:6546-6547).  So
+    on a half-conducting scene every class-1 or class-2 row holds only edges
+    that share a node with it, except the rows of the first class-1 and the
+    first class-2 edge, which also collect mirror entries of fractured columns
+    from all over the mesh (CPU, oracle)."""
+    s = write_tet_case(str(tmp_path), lossy_case("dga"))
+    o = oracle.TetOracle(s)
+    edges, _, cls, _ = o.topology()
+    ptr, col, _ = o.matrix("H")
+    o.close()
+    near = {}
+    for e, (a, b) in enumerate(edges):
+        near.setdefault(int(a), set()).add(e)
+        near.setdefault(int(b), set()).add(e)
+    firsts = {int(np.flatnonzero(cls == c)[0]) for c in (1, 2)}
+    extra = {}
+    for e in np.flatnonzero((cls == 1) | (cls == 2)):
+        cols = set(col[ptr[e]:ptr[e + 1]].tolist())
+        allowed = near[int(edges[e][0])] | near[int(edges[e][1])]
+        extra[int(e)] = cols - allowed
+    assert all(not v for e, v in extra.items() if e not in firsts)
+    for e in firsts:
+        assert extra[e] and all(cls[c] in (1, 2) for c in extra[e])
