@@ -17,8 +17,11 @@
 //
 // Scope and documented divergences:
 //  * conductivity (sigma) enters gfdtd and fem through SigMat and dga through
-//    its edge classes (:6776-6905, :9262-9475); magnetic losses (chi, the face
-//    classes :6501-6542) are rejected;
+//    its edge classes (:6776-6905, :9262-9475); magnetic losses (chi) enter
+//    dga through its face classes (:6357-6542, :9128-9205) where a face's
+//    tets share chi (and mu); fractured faces, whose old values the
+//    reference reads from the electric state (:586), and chi on gfdtd and fem
+//    are rejected;
 //  * tets with material label 7 are dropped (:6091); the reference also keeps 4
 //    zero-initialised face slots per dropped tet (:6130-6152) that create a
 //    spurious face (0,0,0); here they are not created;

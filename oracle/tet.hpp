@@ -1,6 +1,7 @@
 // ORACLE — test infrastructure only.  FP64 CPU restatement of TetFIT's
-// tetrahedral DGA paths ("method dga" explicit and "method gfdtd" with the
-// Jacobi-PCG mass solve); see tet.cpp for the reference lines followed.
+// tetrahedral DGA paths ("method dga" explicit, "method gfdtd" and "method
+// fem" with the Jacobi-PCG solve); see tet.cpp for the reference lines
+// followed.
 #pragma once
 #include <array>
 #include <cstdint>
